@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Disco RK timestep (zone-updates/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload ragged64|config0]
+
+A step is one full RK2 timestep (two substeps, fused getmindt) of every disk
+of the workload, inputs resident in HBM.  Default workload `ragged64`: 64
+ragged 2D hydro disks (~5.7M cells, the config-2 batch, FP64 plain path).
+Multi-GPU: one process per GPU (torchrun), each GPU advances its own 64
+disks (same sizes, own noise seeds): the disks are independent, so there is
+no data-path collective ("scaling": "weak"); only a barrier and a max of the
+timings over ranks.
+
+--impl reference times the reference Disco serial CPU code itself
+(oracle/_ref, built from the reference's own sources) on the same disks, one
+process per disk spread over all host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+
+METRIC = "zone-updates/s"
+Q = 6                                   # NUM_C 5 + NUM_N 1 (hydro)
+B_ALG_STEP = 576                        # HBM bytes per zone-update, FP64 hydro (10Q+12 words)
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def kernel_bytes(name, first, N, Nf, Na):
+    """Algorithmic (compulsory, each element once) HBM bytes of one launch.
+    N cells, Nf r-faces, Na annuli; Q doubles per cell."""
+    w = 8
+    if name == "k_begin":
+        return N * w * ((5 * Q + 4) if first else (5 * Q + 1))
+    if name == "k_I0":
+        return N * w + Na * 4
+    if name == "k_faces":
+        return N * w * (2 * Q + 2) + N * 8 + Nf * (4 + 4 + 1 + 3 * w + Q * w)
+    if name == "k_gradr":
+        return Nf * w * (Q + 1) + N * (w * Q + 3 * w + 8)
+    if name == "k_flux_r":
+        return Nf * (4 + 4 + 2 * w + Q * w) + N * w * (3 * Q + 2)
+    if name == "k_flux_p":
+        return N * w * (3 * Q + 2)
+    if name == "k_update":
+        return N * w * (5 * Q + (6 if first else 3)) + N * 8 + Nf * w * Q
+    return 0
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1])); smax.append(float(p[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, p[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_disks(workload, rank):
+    from disco_b200 import workloads
+    if workload == "config0":
+        return [workloads.config0_disk()]
+    return workloads.ragged_disks(64, rank=rank)
+
+
+def reference_pars(workload, rank=0):
+    from disco_b200 import workloads, template_paths
+    if workload == "config0":
+        return [template_paths("c0_kepler2d")[0]], False
+    _, pars = workloads.ragged_disks(64, rank=rank, keep_pars=True)
+    return pars, True
+
+
+def time_reference(workload, nsteps, max_workers=None):
+    """The reference's serial CPU code on every disk of the workload, one
+    process per disk, statically spread over the host cores.  Returns
+    (zone-updates/s, cores, sample description)."""
+    import pyoracle
+    binary = pyoracle.ref_binary("c0_kepler2d")
+    if not os.path.exists(binary):
+        pyoracle.build_ref("c0_kepler2d")
+    pars, tmp = reference_pars(workload)
+    cores = max_workers or min(os.cpu_count() or 1, len(pars))
+    work = []
+    for p in pars:
+        d = tempfile.mkdtemp(prefix="dref_")
+        with open(p) as f, open(os.path.join(d, "in.par"), "w") as g:
+            g.write(f.read())
+        work.append(d)
+    # static round-robin assignment: worker w runs disks w, w+cores, ...
+    procs = []
+    for w in range(cores):
+        jobs = work[w::cores]
+        cmd = " ; ".join("%s %s %d --time" % (binary, d, nsteps) for d in jobs)
+        procs.append(subprocess.Popen(["bash", "-c", cmd], stdout=subprocess.PIPE, text=True))
+    per_worker, zones = [], 0
+    for pr in procs:
+        out, _ = pr.communicate()
+        s = 0.0
+        for line in out.strip().splitlines():
+            if line.startswith("{"):
+                r = json.loads(line)
+                s += r["seconds"]
+                zones += r["real_cells"] * r["steps"]
+        per_worker.append(s)
+    for d in work:
+        subprocess.run(["rm", "-rf", d])
+    if tmp:
+        for p in pars:
+            os.unlink(p)
+    wall = max(per_worker)
+    sample = "%s: all %d disks x %d step(s), %d processes on %d cores, step-loop time only" % (
+        workload, len(pars), nsteps, len(pars), cores)
+    return zones / wall, cores, sample
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    v, cores, sample = time_reference(args.workload, max(1, args.steps // 4))
+    line = {"metric": METRIC, "value": v, "unit": "zone-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": args.workload, "parallelism": "one process per disk"},
+            "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    import disco_b200 as db
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        pg = dist
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(x):
+        if not pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    disks = make_disks(args.workload, rank)
+    b = db.Batch(disks, device=local)
+    nreal = sum(d.nreal for d in disks)
+    ncell = b.ncell
+    nf = sum(int(sum(d.Np[j] + d.Np[j + 1] for j in range(d.Nr - 1))) for d in disks)
+    na = sum(d.Nr * d.Nz for d in disks)
+
+    stream = torch.cuda.Stream(device=local)
+    b.set_stream(stream.cuda_stream)
+    b.run(args.warmup)
+    b.sync()
+
+    # per-kernel device times of one step (events between launches, same stream)
+    kt = b.kernel_times()
+    launches_per_step = len(kt)
+
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        b.run(args.steps)
+        e1.record(stream)
+    e1.synchronize()
+    ck = clocks.stop()
+    barrier()
+    if b.last_error() != 0:
+        raise RuntimeError("device error during the timed region: %s" % db.STATUS.get(b.last_error()))
+    ms = allmax(e0.elapsed_time(e1))
+    value = world * nreal * args.steps / (ms / 1e3)
+
+    # roofline of the dominant kernel (sum over its launches in the step)
+    hbm, peak_kind = peaks()
+    tot, byt, seen = {}, {}, {}
+    for name, t in kt:
+        first = seen.get(name, 0) == 0
+        seen[name] = seen.get(name, 0) + 1
+        tot[name] = tot.get(name, 0.0) + t
+        byt[name] = byt.get(name, 0) + kernel_bytes(name, first, ncell, nf, na)
+    dom = max(tot, key=tot.get)
+    achieved = byt[dom] / (tot[dom] / 1e3) / 1e9
+    traffic = None
+    tfile = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            tj = json.load(open(tfile))
+            ent = tj.get(args.workload, {}).get(dom)
+            if ent:
+                traffic = ent["bytes_per_launch"]
+        except Exception:
+            traffic = None
+    step_gbs = B_ALG_STEP * (value / world) / 1e9
+
+    # end to end through the C ABI with host buffers: upload the state from
+    # host memory, K x {dt = getmindt() -> host; timestep(dt) from host},
+    # download the state.
+    st = b.get_cells()
+    h2d = (st["prim"].nbytes + st["cons"].nbytes + st["piph"].nbytes + st["dphi"].nbytes
+           + st["wiph"].nbytes + 4 * ncell)
+    d2h = h2d - 4 * ncell
+    real = np.concatenate([d.real for d in disks])
+    barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    t_wall = time.perf_counter()
+    b.set_cells(st["prim"], st["cons"], st["piph"], st["dphi"], st["wiph"], real)
+    for _ in range(args.steps):
+        dt = b.mindt()
+        b.timestep(dt)
+    out = b.get_cells()
+    f1.record(stream)
+    f1.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    e2e_ms = allmax(max(f0.elapsed_time(f1), t_wall * 1e3))
+    e2e = world * nreal * args.steps / (e2e_ms / 1e3)
+    del out
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, cores, sample = time_reference(args.workload, 1)
+            cpu = {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "reference",
+                   "sample": sample}
+        except Exception as ex:  # reference binary missing on this machine
+            cpu = {"value": None, "unit": "zone-updates/s", "cores": 0, "kind": "reference",
+                   "sample": "unavailable: %s" % ex}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "disks_per_gpu": len(disks), "real_cells_per_gpu": nreal,
+                       "cells_per_gpu_incl_ghosts": ncell, "r_faces_per_gpu": nf,
+                       "precision": "fp64 plain", "riemann": "HLLC", "timestepper": "RK2",
+                       "l2_policy": "inputs larger than L2 (%.1f GB of cell state per GPU)" %
+                                    (ncell * 8 * (6 * Q + 4) / 1e9),
+                       "parallelism": "independent disks per GPU" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                         "peak_kind": peak_kind},
+            "step_roofline": {"bytes_per_zone_update": B_ALG_STEP, "achieved": step_gbs, "peak": hbm,
+                              "unit": "GB/s", "frac": step_gbs / hbm},
+            "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(tot.items(), key=lambda x: -x[1])},
+            "e2e": {"value": e2e, "unit": "zone-updates/s",
+                    "h2d_bytes_per_step": (h2d + 8 * len(disks) * args.steps) / args.steps,
+                    "d2h_bytes_per_step": (d2h + 8 * len(disks) * args.steps) / args.steps},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": ck,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
+    if pg:
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ragged64", choices=["ragged64", "config0"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

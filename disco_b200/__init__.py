@@ -1,0 +1,317 @@
+"""disco_b200: B200-native Disco RK timestep, Python host mirror.
+
+The product is the C ABI in include/disco_b200.h (kernels + batch API) and
+include/disco_host.h (in.par / Makefile_opt.in parsing and grid set-up),
+built into disco_b200/libdisco_b200.so.  This module binds it with ctypes and
+mirrors the reference's host flow (main.c:31-83):
+
+    disk = Disk.from_files("in.par", "Makefile_opt.in")   # read_par_file, setupGrid,
+                                                          # setupDomain, setupCells
+    batch = Batch([disk])                                 # device-resident state
+    dt = batch.mindt()                                    # getmindt
+    batch.timestep(dt)                                    # timestep
+    batch.run(100)                                        # 100 x {getmindt; timestep}
+
+There is no CPU fallback: without the built library or a CUDA device every
+entry point raises DiscoError.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libdisco_b200.so")
+TEMPLATES = os.path.join(HERE, "templates")
+
+OK = 0
+STATUS = {0: "ok", 1: "bad argument", 2: "CUDA runtime error", 3: "module combination not built",
+          4: "phi wrap loop hit its cap (non-finite piph)", 5: "non-finite or non-positive dt",
+          6: "no CUDA device", 7: "call out of order"}
+HYDRO = {"euler": 0, "mhd": 1}
+BOUNDARY = {"fixed": 0, "zerograd": 1, "fixed3d": 2}
+PLANETS = {"none": 0, "sun": 1, "cm2": 2, "binary_soft": 3}
+INITIAL = {"kepler_noise": 0, "mhd_shear_noise": 1}
+PREC_FP64, PREC_MIXED = 0, 1
+
+
+class DiscoError(RuntimeError):
+    def __init__(self, status, where=""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS.get(status, status)} (status {status})")
+
+
+class Params(C.Structure):
+    """Mirror of disco_params (include/disco_b200.h)."""
+    _fields_ = [
+        ("Num_R", C.c_int), ("Num_Z", C.c_int), ("aspect", C.c_double),
+        ("rmin", C.c_double), ("rmax", C.c_double), ("zmin", C.c_double), ("zmax", C.c_double),
+        ("phimax", C.c_double),
+        ("NoBC_Rmin", C.c_int), ("NoBC_Rmax", C.c_int), ("NoBC_Zmin", C.c_int), ("NoBC_Zmax", C.c_int),
+        ("LogZoning", C.c_int), ("R_Periodic", C.c_int), ("Z_Periodic", C.c_int),
+        ("LogRadius", C.c_double),
+        ("Mesh_Motion", C.c_int), ("Riemann_Solver", C.c_int), ("Timestep", C.c_int),
+        ("CFL", C.c_double), ("PLM", C.c_double), ("maxDT", C.c_double),
+        ("Density_Floor", C.c_double), ("Pressure_Floor", C.c_double),
+        ("Exact_Mesh_Omega", C.c_int), ("Exact_Mesh_Omega_Par", C.c_double),
+        ("Energy_Omega", C.c_int), ("Energy_Omega_Par", C.c_double),
+        ("RotFrame", C.c_int), ("RotOmega", C.c_double), ("RotD", C.c_double),
+        ("Adiabatic_Index", C.c_double), ("viscosity", C.c_double),
+        ("visc_flag", C.c_int), ("alpha_flag", C.c_int), ("isothermal_flag", C.c_int),
+        ("Cs2_Profile", C.c_int), ("Cs2_Par", C.c_double),
+        ("Disk_Mach", C.c_double), ("Mass_Ratio", C.c_double),
+        ("grav2D", C.c_int), ("CT", C.c_int), ("initPar0", C.c_int),
+        ("initPar", C.c_double * 9), ("metricPar", C.c_double * 5), ("t_min", C.c_double),
+    ]
+
+
+class Modules(C.Structure):
+    """Mirror of disco_modules."""
+    _fields_ = [("hydro", C.c_int), ("boundary", C.c_int), ("planets", C.c_int),
+                ("initial", C.c_int), ("analysis", C.c_int),
+                ("num_c", C.c_int), ("num_n", C.c_int), ("ct_mode", C.c_int)]
+
+
+_lib = None
+
+_I = C.c_int
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int)
+
+
+def library():
+    """Load libdisco_b200.so (raises DiscoError if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise DiscoError(6, "libdisco_b200.so not built (run disco_b200.build.build())")
+    lib = C.CDLL(LIBPATH)
+    sig = {
+        "disco_abi_version": (_I, []),
+        "disco_strerror": (C.c_char_p, [_I]),
+        "disco_batch_create": (_I, [_I, C.POINTER(Modules), _I, _I, C.POINTER(Params), _IP, _IP, _IP,
+                                    _IP, _D, _D, C.POINTER(_P)]),
+        "disco_batch_destroy": (None, [_P]),
+        "disco_batch_sizes": (_I, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), _IP]),
+        "disco_batch_set_cells": (_I, [_P, _D, _D, _D, _D, _D, _IP, _D]),
+        "disco_batch_get_cells": (_I, [_P, _D, _D, _D, _D, _D, _D]),
+        "disco_batch_setup_cells": (_I, [_P]),
+        "disco_batch_mindt": (_I, [_P, _D]),
+        "disco_batch_timestep": (_I, [_P, _D]),
+        "disco_batch_run": (_I, [_P, _I]),
+        "disco_batch_time": (_I, [_P, _I, _D, _IP]),
+        "disco_batch_get_faces": (_I, [_P, _I, _I, _IP, _IP, _IP, _IP, _IP, _D]),
+        "disco_batch_get_diagnostics": (_I, [_P, _I, _D, _IP, _D]),
+        "disco_batch_last_error": (_I, [_P]),
+        "disco_batch_kernel_times": (_I, [_P, C.POINTER(C.c_float), C.POINTER(C.c_char_p), _I, _IP]),
+        "disco_batch_set_stream": (_I, [_P, _P]),
+        "disco_read_par": (_I, [C.c_char_p, C.POINTER(Params), _IP]),
+        "disco_read_opt": (_I, [C.c_char_p, C.POINTER(Modules)]),
+        "disco_setup_grid": (_I, [C.POINTER(Params), _IP, _IP, _IP, _IP, _D, _D]),
+        "disco_setup_phi": (_I, [C.POINTER(Params), _I, _I, _IP, _IP, _D, _D, _IP]),
+        "disco_sizeof": (_I, [_I]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(status, where):
+    if status != OK:
+        raise DiscoError(status, where)
+
+
+def dptr(a):
+    return a.ctypes.data_as(_D) if a is not None else None
+
+
+def iptr(a):
+    return a.ctypes.data_as(_IP) if a is not None else None
+
+
+def read_par(path):
+    """read_par_file (readpar.c:44-188) -> Params."""
+    p = Params()
+    miss = C.c_int(0)
+    _check(library().disco_read_par(path.encode(), C.byref(p), C.byref(miss)), "disco_read_par")
+    return p
+
+
+def read_opt(path):
+    """Makefile_opt.in module selection -> Modules."""
+    m = Modules()
+    _check(library().disco_read_opt(path.encode(), C.byref(m)), "disco_read_opt")
+    return m
+
+
+class Disk:
+    """One disk's grid and initial phi layout, built as setupGrid/setupDomain do."""
+
+    def __init__(self, params, modules):
+        lib = library()
+        self.params, self.modules = params, modules
+        Nr, Nz = C.c_int(), C.c_int()
+        Ng = np.zeros(4, np.int32)
+        _check(lib.disco_setup_grid(C.byref(params), C.byref(Nr), C.byref(Nz), iptr(Ng),
+                                    None, None, None), "disco_setup_grid")
+        self.Nr, self.Nz, self.Ng = Nr.value, Nz.value, Ng
+        self.Np = np.zeros(self.Nr * self.Nz, np.int32)
+        self.r_jph = np.zeros(self.Nr + 1)
+        self.z_kph = np.zeros(self.Nz + 1)
+        _check(lib.disco_setup_grid(C.byref(params), C.byref(Nr), C.byref(Nz), iptr(Ng),
+                                    iptr(self.Np), dptr(self.r_jph), dptr(self.z_kph)),
+               "disco_setup_grid")
+        self.ncell = int(self.Np.sum())
+        self.piph = np.zeros(self.ncell)
+        self.dphi = np.zeros(self.ncell)
+        self.real = np.zeros(self.ncell, np.int32)
+        _check(lib.disco_setup_phi(C.byref(params), self.Nr, self.Nz, iptr(self.Ng), iptr(self.Np),
+                                   dptr(self.piph), dptr(self.dphi), iptr(self.real)),
+               "disco_setup_phi")
+
+    @classmethod
+    def from_files(cls, par_path, opt_path):
+        return cls(read_par(par_path), read_opt(opt_path))
+
+    @property
+    def q(self):
+        return self.modules.num_c + self.modules.num_n
+
+    @property
+    def nreal(self):
+        return int(self.real.sum())
+
+
+class Batch:
+    """Device-resident batch of disks (disco_batch_*)."""
+
+    def __init__(self, disks, device=0, precision=PREC_FP64, setup=True):
+        lib = library()
+        self.disks = list(disks)
+        n = len(self.disks)
+        m = self.disks[0].modules
+        par = (Params * n)(*[d.params for d in self.disks])
+        Nr = np.array([d.Nr for d in self.disks], np.int32)
+        Nz = np.array([d.Nz for d in self.disks], np.int32)
+        Ng = np.concatenate([d.Ng for d in self.disks]).astype(np.int32)
+        Np = np.concatenate([d.Np for d in self.disks]).astype(np.int32)
+        rj = np.concatenate([d.r_jph for d in self.disks])
+        zk = np.concatenate([d.z_kph for d in self.disks])
+        h = C.c_void_p()
+        _check(lib.disco_batch_create(device, C.byref(m), precision, n, par, iptr(Nr), iptr(Nz),
+                                      iptr(Ng), iptr(Np), dptr(rj), dptr(zk), C.byref(h)),
+               "disco_batch_create")
+        self.h = h
+        self.q = self.disks[0].q
+        self.offsets = np.concatenate([[0], np.cumsum([d.ncell for d in self.disks])]).astype(np.int64)
+        self.ncell = int(self.offsets[-1])
+        if setup:
+            piph = np.concatenate([d.piph for d in self.disks])
+            dphi = np.concatenate([d.dphi for d in self.disks])
+            real = np.concatenate([d.real for d in self.disks]).astype(np.int32)
+            _check(lib.disco_batch_set_cells(self.h, None, None, dptr(piph), dptr(dphi), None,
+                                             iptr(real), None), "disco_batch_set_cells")
+            _check(lib.disco_batch_setup_cells(self.h), "disco_batch_setup_cells")
+
+    def close(self):
+        if getattr(self, "h", None):
+            library().disco_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_cells(self, prim, cons, piph, dphi, wiph=None, real=None):
+        prim = None if prim is None else np.ascontiguousarray(prim, np.float64)
+        cons = None if cons is None else np.ascontiguousarray(cons, np.float64)
+        piph = np.ascontiguousarray(piph, np.float64)
+        dphi = np.ascontiguousarray(dphi, np.float64)
+        wiph = None if wiph is None else np.ascontiguousarray(wiph, np.float64)
+        real = None if real is None else np.ascontiguousarray(real, np.int32)
+        _check(library().disco_batch_set_cells(self.h, dptr(prim), dptr(cons), dptr(piph),
+                                               dptr(dphi), dptr(wiph), iptr(real), None),
+               "disco_batch_set_cells")
+
+    def get_cells(self):
+        n, q = self.ncell, self.q
+        prim = np.zeros((n, q)); cons = np.zeros((n, q))
+        piph = np.zeros(n); dphi = np.zeros(n); wiph = np.zeros(n)
+        _check(library().disco_batch_get_cells(self.h, dptr(prim), dptr(cons), dptr(piph),
+                                               dptr(dphi), dptr(wiph), None),
+               "disco_batch_get_cells")
+        return dict(prim=prim, cons=cons, piph=piph, dphi=dphi, wiph=wiph)
+
+    def mindt(self):
+        dt = np.zeros(len(self.disks))
+        _check(library().disco_batch_mindt(self.h, dptr(dt)), "disco_batch_mindt")
+        return dt
+
+    def timestep(self, dt=None):
+        a = None if dt is None else np.ascontiguousarray(np.broadcast_to(dt, len(self.disks)), np.float64)
+        _check(library().disco_batch_timestep(self.h, dptr(a)), "disco_batch_timestep")
+
+    def run(self, nsteps):
+        _check(library().disco_batch_run(self.h, int(nsteps)), "disco_batch_run")
+
+    def set_stream(self, stream_handle):
+        """Launch on an external cudaStream_t (an int handle; 0/None = own stream)."""
+        _check(library().disco_batch_set_stream(self.h, C.c_void_p(stream_handle or None)),
+               "disco_batch_set_stream")
+
+    def kernel_times(self, cap=64):
+        """One instrumented step: [(kernel name, device ms), ...] in launch order."""
+        ms = (C.c_float * cap)()
+        names = (C.c_char_p * cap)()
+        n = C.c_int()
+        _check(library().disco_batch_kernel_times(self.h, ms, names, cap, C.byref(n)),
+               "disco_batch_kernel_times")
+        return [(names[i].decode(), float(ms[i])) for i in range(n.value)]
+
+    def last_error(self):
+        return library().disco_batch_last_error(self.h)
+
+    def sync(self):
+        _check(self.last_error(), "device")
+
+    def time(self, disk=0):
+        t = C.c_double(); cnt = C.c_int()
+        _check(library().disco_batch_time(self.h, disk, C.byref(t), C.byref(cnt)), "disco_batch_time")
+        return t.value, cnt.value
+
+    def faces(self, disk=0, dim=1, geom=False):
+        d = self.disks[disk]
+        ntr = (d.Nr - 1) * d.Nz if dim == 1 else (d.Nz - 1) * d.Nr
+        nf_max = int(sum(d.Np)) * 2 + 16
+        fI = np.zeros(ntr + 1, np.int32)
+        iL = np.zeros(nf_max, np.int32); iR = np.zeros(nf_max, np.int32)
+        LR = np.zeros(nf_max, np.int32)
+        g = np.zeros((nf_max, 8)) if geom else None
+        nf = C.c_int()
+        _check(library().disco_batch_get_faces(self.h, disk, dim, C.byref(nf), iptr(fI), iptr(iL),
+                                               iptr(iR), iptr(LR), dptr(g)), "disco_batch_get_faces")
+        n = nf.value
+        out = dict(fIndex=fI, iL=iL[:n], iR=iR[:n], LRtype=LR[:n])
+        if geom:
+            out["geom"] = g[:n]
+        return out
+
+    def diagnostics(self, disk=0):
+        d = self.disks[disk]
+        Qrz = np.zeros(d.Nr * d.Nz * 5)
+        nq = C.c_int(); tav = C.c_double()
+        _check(library().disco_batch_get_diagnostics(self.h, disk, dptr(Qrz), C.byref(nq),
+                                                     C.byref(tav)), "disco_batch_get_diagnostics")
+        return Qrz[: d.Nr * d.Nz * nq.value], tav.value
+
+
+def template_paths(name):
+    """(in.par, Makefile_opt.in) of a bundled configuration template."""
+    return (os.path.join(TEMPLATES, name + ".par"), os.path.join(TEMPLATES, name + ".in"))

@@ -1,0 +1,610 @@
+/*
+ * C ABI of the B200 Disco timestep (include/disco_b200.h): batch set-up,
+ * host <-> device state transfer, and the per-step launch sequence that
+ * replaces timestep()/onestep() (timestep.c:7-45, onestep.c:84-229).
+ *
+ * One batch = one or more independent disks in one set of ragged SoA
+ * arrays.  A step is ~16 kernels (two substeps of begin / I0 / faces /
+ * gradr / flux_r / flux_p / update, plus three tiny per-disk kernels); the
+ * multi-step driver captures one step in a CUDA graph and replays it with
+ * dt left on the device by the previous step's fused getmindt.
+ */
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+#include <algorithm>
+#include "disco_b200.h"
+#include "disco_kernels.cuh"
+
+using namespace disco;
+
+struct disco_batch {
+   int device;
+   disco_modules mods;
+   int prec;
+   int ndisk, Q, NC;
+   int timestep_mode;        /* 0 = RK2, 1 = forward Euler */
+   int bc_fixed;
+   int any_mm3;
+   int nq;
+   std::vector<disco_params> params;
+   /* topology (host) */
+   std::vector<int> ann_off, ann_np, ann_disk, ann_j, ann_k;
+   std::vector<int> tr_a, tr_b, tr_off, tr_flux, tr_j, tr_k;
+   std::vector<double> tr_dxL, tr_dxR;
+   std::vector<int2> cblk, fblk;
+   std::vector<int> ann_blk0, ann_nblk;
+   std::vector<double> rj, zk;
+   std::vector<DiskParams> dparams;
+   std::vector<int> disk_Nr, disk_Nz, disk_nreal;
+   int64_t ncell, nreal;
+   /* device */
+   View v;
+   void *dev_static;            /* one allocation for topology */
+   std::vector<void *> allocs;
+   int *d_ann_blk0, *d_ann_nblk;
+   double *d_Qrz;
+   int *d_err;
+   cudaStream_t stream;
+   cudaStream_t own_stream;
+   std::vector<cudaEvent_t> *tape;       /* non-NULL: record an event after each launch */
+   std::vector<const char *> *tape_names;
+   cudaGraphExec_t graph;
+   int have_cells;
+   int last_status;
+};
+
+static int cuda_status(cudaError_t e){
+   return e == cudaSuccess ? DISCO_OK : DISCO_ERR_CUDA;
+}
+#define CK(x) do{ cudaError_t _e = (x); if( _e != cudaSuccess ){ \
+   fprintf(stderr, "disco_b200: %s failed: %s (%s:%d)\n", #x, cudaGetErrorString(_e), __FILE__, __LINE__); \
+   return DISCO_ERR_CUDA; } }while(0)
+
+template<class T>
+static T *dalloc(disco_batch *b, size_t n){
+   void *p = NULL;
+   if( n == 0 ) n = 1;
+   if( cudaMalloc(&p, n*sizeof(T)) != cudaSuccess ) return NULL;
+   cudaMemset(p, 0, n*sizeof(T));
+   b->allocs.push_back(p);
+   return (T *)p;
+}
+template<class T>
+static T *dupload(disco_batch *b, const std::vector<T> &h){
+   T *p = dalloc<T>(b, h.size());
+   if( p && !h.empty() ) cudaMemcpy(p, h.data(), h.size()*sizeof(T), cudaMemcpyHostToDevice);
+   return p;
+}
+
+extern "C" int disco_abi_version(void){ return DISCO_ABI_VERSION; }
+
+extern "C" const char *disco_strerror(int s){
+   switch( s ){
+      case DISCO_OK: return "ok";
+      case DISCO_ERR_ARG: return "bad argument";
+      case DISCO_ERR_CUDA: return "CUDA runtime error";
+      case DISCO_ERR_UNSUPPORTED: return "module combination not built";
+      case DISCO_ERR_PHI_WRAP: return "phi wrap loop hit its cap (non-finite piph)";
+      case DISCO_ERR_NONFINITE: return "non-finite or non-positive dt";
+      case DISCO_ERR_NO_DEVICE: return "no CUDA device";
+      case DISCO_ERR_STATE: return "call out of order";
+   }
+   return "unknown status";
+}
+
+static void fill_disk_params(DiskParams &D, const disco_params &p, const disco_modules &m){
+   memset(&D, 0, sizeof D);
+   D.gam = p.Adiabatic_Index; D.PLM = p.PLM; D.CFL = p.CFL; D.maxDT = p.maxDT;
+   D.Pmax = p.phimax; D.rho_floor = p.Density_Floor; D.p_floor = p.Pressure_Floor;
+   D.RotOmega = p.RotOmega; D.Mach = p.Disk_Mach;
+   D.Cs2_M = p.metricPar[2]; D.Cs2_H0 = p.initPar[4]; D.Cs2_r1 = p.initPar[2];
+   D.mesh_motion = p.Mesh_Motion; D.riemann = p.Riemann_Solver; D.en_om = p.Energy_Omega;
+   D.mesh_om = p.Exact_Mesh_Omega; D.isothermal = p.isothermal_flag;
+   D.cs2_profile = p.Cs2_Profile; D.grav2D = p.grav2D; D.polar = p.NoBC_Rmin == 1;
+   D.timestep = p.Timestep;
+   D.rotframe = p.RotFrame;
+   D.planets_move = (m.planets == DISCO_PLANETS_CM2 || m.planets == DISCO_PLANETS_BINARY_SOFT);
+   D.ic.mach = p.Disk_Mach; D.ic.amp = p.initPar[1];
+   D.ic.rmin = p.rmin; D.ic.rmax = p.rmax; D.ic.phimax = p.phimax;
+   D.ic.seed = (uint64_t)(int64_t)p.initPar0;
+}
+
+static void init_planets(DiskState &S, DiskParams &D, const disco_params &p, const disco_modules &m){
+   memset(S.pl, 0, sizeof S.pl);
+   switch( m.planets ){
+      case DISCO_PLANETS_SUN:                          /* Planets/sun.c:9-17 */
+         D.npl = 1; S.pl[0].M = 1.0; break;
+      case DISCO_PLANETS_CM2: {                        /* Planets/cm2.c:14-38 */
+         D.npl = 2;
+         double a = 1.0, q = p.Mass_Ratio, mu = q/(1.+q), om = pow(a,-1.5);
+         S.pl[0].M = 1.-mu; S.pl[0].omega = om; S.pl[0].r = a*mu; S.pl[0].phi = M_PI;
+         S.pl[1].M = mu;    S.pl[1].omega = om; S.pl[1].r = a*(1.-mu);
+         break; }
+      case DISCO_PLANETS_BINARY_SOFT: {                /* new module: softened equal-mass binary */
+         D.npl = 2;
+         double a = p.initPar[5] > 0 ? p.initPar[5] : 1.0, eps = p.initPar[6];
+         double om = 1.0/(a*sqrt(a));
+         S.pl[0].M = 0.5; S.pl[0].omega = om; S.pl[0].r = 0.5*a; S.pl[0].phi = M_PI; S.pl[0].eps = eps;
+         S.pl[1].M = 0.5; S.pl[1].omega = om; S.pl[1].r = 0.5*a; S.pl[1].phi = 0.0;  S.pl[1].eps = eps;
+         break; }
+      default:                                          /* Planets/none.c:9-17 */
+         D.npl = 1; S.pl[0].M = 0.0; S.pl[0].eps = 1.0; break;
+   }
+}
+
+extern "C" int disco_batch_create(int device, const disco_modules *mods, int precision,
+                                  int ndisk, const disco_params *params,
+                                  const int *Nr, const int *Nz, const int *Ng,
+                                  const int *Np, const double *r_jph, const double *z_kph,
+                                  disco_batch **out){
+   if( !mods || !params || !Nr || !Nz || !Ng || !Np || !r_jph || !z_kph || !out || ndisk < 1 )
+      return DISCO_ERR_ARG;
+   *out = NULL;
+   int ndev = 0;
+   if( cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1 ) return DISCO_ERR_NO_DEVICE;
+   if( device < 0 || device >= ndev ) return DISCO_ERR_ARG;
+   if( mods->hydro != DISCO_HYDRO_EULER || mods->num_c != 5 || mods->num_n != 1 ||
+       mods->ct_mode != 0 || precision != DISCO_PREC_FP64 )
+      return DISCO_ERR_UNSUPPORTED;
+   if( mods->boundary != DISCO_BC_FIXED ) return DISCO_ERR_UNSUPPORTED;
+   if( mods->initial != DISCO_IC_KEPLER_NOISE ) return DISCO_ERR_UNSUPPORTED;
+   for( int d=0 ; d<ndisk ; ++d ){
+      if( Nz[d] != 1 ) return DISCO_ERR_UNSUPPORTED;          /* 3D: z faces not built */
+      if( Nr[d] < 2 ) return DISCO_ERR_ARG;
+      if( params[d].Timestep != params[0].Timestep ) return DISCO_ERR_ARG;
+      if( params[d].R_Periodic ) return DISCO_ERR_UNSUPPORTED;
+      if( params[d].Riemann_Solver > 1 ) return DISCO_ERR_UNSUPPORTED;
+      if( params[d].visc_flag || params[d].RotFrame ) return DISCO_ERR_UNSUPPORTED;
+   }
+   CK(cudaSetDevice(device));
+   disco_batch *b = new disco_batch();
+   b->device = device; b->mods = *mods; b->prec = precision; b->ndisk = ndisk;
+   b->NC = mods->num_c; b->Q = mods->num_c + mods->num_n;
+   b->timestep_mode = params[0].Timestep == 1 ? 1 : 0;
+   b->bc_fixed = mods->boundary == DISCO_BC_FIXED;
+   b->nq = mods->analysis == DISCO_DIAG_DISK2D ? 5 : 0;
+   b->params.assign(params, params + ndisk);
+   b->any_mm3 = 0;
+   b->graph = NULL;
+   b->have_cells = 0;
+   b->own_stream = NULL;
+   b->tape = NULL; b->tape_names = NULL;
+
+   /* ---- topology */
+   int cell = 0, ann = 0, face = 0, roff = 0, zoff = 0, npoff = 0;
+   b->ncell = 0; b->nreal = 0;
+   std::vector<DiskState> dstate(ndisk);
+   b->dparams.resize(ndisk);
+   for( int d=0 ; d<ndisk ; ++d ){
+      const disco_params &p = params[d];
+      DiskParams &D = b->dparams[d];
+      fill_disk_params(D, p, *mods);
+      memset(&dstate[d], 0, sizeof(DiskState));
+      init_planets(dstate[d], D, p, *mods);
+      dstate[d].t = p.t_min;
+      if( p.Mesh_Motion == 3 ) b->any_mm3 = 1;
+      int nr = Nr[d], nz = Nz[d];
+      D.Nr = nr; D.Nz = nz;
+      D.NgRa = Ng[4*d+0]; D.NgRb = Ng[4*d+1]; D.NgZa = Ng[4*d+2]; D.NgZb = Ng[4*d+3];
+      D.ann0 = ann; D.cell0 = cell;
+      D.rj0 = roff; D.zk0 = zoff;
+      for( int j=0 ; j<=nr ; ++j ) b->rj.push_back(r_jph[roff + j]);
+      for( int k=0 ; k<=nz ; ++k ) b->zk.push_back(z_kph[zoff + k]);
+      int nreal = 0;
+      for( int k=0 ; k<nz ; ++k ) for( int j=0 ; j<nr ; ++j ){
+         int np = Np[npoff + j + nr*k];
+         if( np < 4 ){ delete b; return DISCO_ERR_ARG; }
+         b->ann_off.push_back(cell); b->ann_np.push_back(np); b->ann_disk.push_back(d);
+         b->ann_j.push_back(j); b->ann_k.push_back(k);
+         b->ann_blk0.push_back((int)b->cblk.size());
+         int nb = 0;
+         for( int i0=0 ; i0<np ; i0+=CB ){ b->cblk.push_back(make_int2(ann, i0)); ++nb; }
+         b->ann_nblk.push_back(nb);
+         if( j >= D.NgRa && j < nr-D.NgRb && k >= D.NgZa && k < nz-D.NgZb ) nreal += np;
+         cell += np; ++ann;
+      }
+      /* r tracks (faces_alt.c:87-100): (Nr-1)*Nz tracks, track JK = j + (Nr-1)*k */
+      D.trr0 = (int)b->tr_a.size();
+      D.ntrr = (nr-1)*nz;
+      D.face_r0 = face;
+      const double *rj = r_jph + roff + 1;
+      int jmin = D.NgRa == 0 ? 0 : D.NgRa-1;            /* trans_flux, misc.c:459-471 */
+      int jmax = D.NgRb == 0 ? nr-1 : nr-D.NgRb;
+      for( int k=0 ; k<nz ; ++k ) for( int j=0 ; j<nr-1 ; ++j ){
+         int t = (int)b->tr_a.size();
+         int A = D.ann0 + j + nr*k, B = A + 1;
+         b->tr_a.push_back(A); b->tr_b.push_back(B); b->tr_off.push_back(face);
+         b->tr_j.push_back(j); b->tr_k.push_back(k);
+         b->tr_flux.push_back(j >= jmin && j < jmax && k >= D.NgZa && k < nz-D.NgZb);
+         /* dxL/dxR, faces_alt.c:112-118 */
+         double rm = 2.0*(rj[j]*rj[j] + rj[j]*rj[j-1] + rj[j-1]*rj[j-1]) / (3.0*(rj[j]+rj[j-1]));
+         double rp = 2.0*(rj[j+1]*rj[j+1] + rj[j+1]*rj[j] + rj[j]*rj[j]) / (3.0*(rj[j+1]+rj[j]));
+         b->tr_dxL.push_back(rj[j] - rm);
+         b->tr_dxR.push_back(rp - rj[j]);
+         int nf = b->ann_np[A] + b->ann_np[B];
+         for( int f0=0 ; f0<nf ; f0+=FB ) b->fblk.push_back(make_int2(t, f0));
+         face += nf;
+      }
+      b->disk_Nr.push_back(nr); b->disk_Nz.push_back(nz); b->disk_nreal.push_back(nreal);
+      b->nreal += nreal;
+      roff += nr+1; zoff += nz+1; npoff += nr*nz;
+   }
+   b->ann_off.push_back(cell);
+   b->tr_off.push_back(face);
+   b->ncell = cell;
+
+   View &v = b->v;
+   memset(&v, 0, sizeof v);
+   v.Ncell = cell; v.Nann = ann; v.Ntr = (int)b->tr_a.size(); v.Nf = face;
+   v.nq = b->nq;
+   v.dtfac = 1.0;
+   v.ann_off = dupload(b, b->ann_off); v.ann_np = dupload(b, b->ann_np);
+   v.ann_disk = dupload(b, b->ann_disk); v.ann_j = dupload(b, b->ann_j); v.ann_k = dupload(b, b->ann_k);
+   v.tr_a = dupload(b, b->tr_a); v.tr_b = dupload(b, b->tr_b); v.tr_off = dupload(b, b->tr_off);
+   v.tr_flux = dupload(b, b->tr_flux); v.tr_j = dupload(b, b->tr_j); v.tr_k = dupload(b, b->tr_k);
+   v.tr_dxL = dupload(b, b->tr_dxL); v.tr_dxR = dupload(b, b->tr_dxR);
+   v.cblk = dupload(b, b->cblk); v.fblk = dupload(b, b->fblk);
+   v.rj = dupload(b, b->rj); v.zk = dupload(b, b->zk);
+   v.dp = dupload(b, b->dparams);
+   v.ds = dupload(b, dstate);
+   b->d_ann_blk0 = dupload(b, b->ann_blk0); b->d_ann_nblk = dupload(b, b->ann_nblk);
+   size_t N = (size_t)cell, Qn = (size_t)b->Q*N;
+   v.prim = dalloc<double>(b, Qn); v.cons = dalloc<double>(b, Qn);
+   v.RKcons = dalloc<double>(b, Qn); v.gradp = dalloc<double>(b, Qn);
+   v.gradr = dalloc<double>(b, Qn); v.Gp = dalloc<double>(b, Qn);
+   v.piph = dalloc<double>(b, N); v.dphi = dalloc<double>(b, N);
+   v.wiph = dalloc<double>(b, N); v.piph_new = dalloc<double>(b, N);
+   v.I0 = dalloc<int>(b, ann);
+   v.consL = dalloc<int>(b, N); v.consR = dalloc<int>(b, N);
+   v.fL = dalloc<int>(b, face); v.fR = dalloc<int>(b, face);
+   v.fLR = dalloc<unsigned char>(b, face);
+   v.fphic = dalloc<double>(b, face); v.fdA = dalloc<double>(b, face); v.fdp = dalloc<double>(b, face);
+   v.fS = dalloc<double>(b, (size_t)b->Q*face); v.fG = dalloc<double>(b, (size_t)b->Q*face);
+   v.diag_part = dalloc<double>(b, b->cblk.size()*6);
+   b->d_Qrz = dalloc<double>(b, (size_t)ann*5);
+   v.err = dalloc<int>(b, 1);
+   b->d_err = v.err;
+   for( void *p : b->allocs ) if( !p ){ disco_batch_destroy(b); return DISCO_ERR_CUDA; }
+   if( cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ){
+      disco_batch_destroy(b); return DISCO_ERR_CUDA;
+   }
+   if( cudaDeviceSynchronize() != cudaSuccess ){ disco_batch_destroy(b); return DISCO_ERR_CUDA; }
+   *out = b;
+   return DISCO_OK;
+}
+
+extern "C" void disco_batch_destroy(disco_batch *b){
+   if( !b ) return;
+   cudaSetDevice(b->device);
+   if( b->graph ) cudaGraphExecDestroy(b->graph);
+   if( b->own_stream ) cudaStreamDestroy(b->own_stream);
+   else if( b->stream ) cudaStreamDestroy(b->stream);
+   for( void *p : b->allocs ) if( p ) cudaFree(p);
+   delete b;
+}
+
+extern "C" int disco_batch_sizes(const disco_batch *b, int64_t *ncell, int64_t *nreal, int *q){
+   if( !b ) return DISCO_ERR_ARG;
+   if( ncell ) *ncell = b->ncell;
+   if( nreal ) *nreal = b->nreal;
+   if( q ) *q = b->Q;
+   return DISCO_OK;
+}
+
+/* cell-major (Q per cell) host <-> SoA device */
+static int upload_q(disco_batch *b, double *dst, const double *src){
+   size_t N = b->ncell; int Q = b->Q;
+   std::vector<double> t((size_t)Q*N);
+   for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<Q ; ++q ) t[q*N + c] = src[c*Q + q];
+   CK(cudaMemcpy(dst, t.data(), t.size()*sizeof(double), cudaMemcpyHostToDevice));
+   return DISCO_OK;
+}
+static int download_q(disco_batch *b, double *dst, const double *src){
+   size_t N = b->ncell; int Q = b->Q;
+   std::vector<double> t((size_t)Q*N);
+   CK(cudaMemcpy(t.data(), src, t.size()*sizeof(double), cudaMemcpyDeviceToHost));
+   for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<Q ; ++q ) dst[c*Q + q] = t[q*N + c];
+   return DISCO_OK;
+}
+
+static unsigned nblk(size_t n, unsigned t){ return (unsigned)((n + t - 1)/t); }
+
+/* after a launch: in kernel-timing mode, an event closing that launch */
+static void mark(disco_batch *b, const char *name){
+   if( !b->tape ) return;
+   cudaEvent_t e;
+   cudaEventCreate(&e);
+   cudaEventRecord(e, b->stream);
+   b->tape->push_back(e);
+   b->tape_names->push_back(name);
+}
+
+template<int Q, int NC>
+static void launch_prim2cons(disco_batch *b){
+   k_prim2cons<Q,NC><<<(unsigned)b->cblk.size(), CB, 0, b->stream>>>(b->v);
+}
+
+extern "C" int disco_batch_set_cells(disco_batch *b, const double *prim, const double *cons,
+                                     const double *piph, const double *dphi, const double *wiph,
+                                     const int *real, const double *Phi){
+   if( !b || !piph || !dphi ) return DISCO_ERR_ARG;
+   (void)real; (void)Phi;
+   CK(cudaSetDevice(b->device));
+   size_t N = b->ncell;
+   int s;
+   if( prim && (s = upload_q(b, b->v.prim, prim)) ) return s;
+   if( cons && (s = upload_q(b, b->v.cons, cons)) ) return s;
+   CK(cudaMemcpy(b->v.piph, piph, N*sizeof(double), cudaMemcpyHostToDevice));
+   CK(cudaMemcpy(b->v.dphi, dphi, N*sizeof(double), cudaMemcpyHostToDevice));
+   if( wiph ) CK(cudaMemcpy(b->v.wiph, wiph, N*sizeof(double), cudaMemcpyHostToDevice));
+   if( prim && !cons ){
+      launch_prim2cons<6,5>(b);
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(b->stream));
+   }
+   b->have_cells = 1;
+   return DISCO_OK;
+}
+
+extern "C" int disco_batch_get_cells(disco_batch *b, double *prim, double *cons,
+                                     double *piph, double *dphi, double *wiph, double *Phi){
+   if( !b ) return DISCO_ERR_ARG;
+   (void)Phi;
+   CK(cudaSetDevice(b->device));
+   CK(cudaStreamSynchronize(b->stream));
+   size_t N = b->ncell;
+   int s;
+   if( prim && (s = download_q(b, prim, b->v.prim)) ) return s;
+   if( cons && (s = download_q(b, cons, b->v.cons)) ) return s;
+   if( piph ) CK(cudaMemcpy(piph, b->v.piph, N*sizeof(double), cudaMemcpyDeviceToHost));
+   if( dphi ) CK(cudaMemcpy(dphi, b->v.dphi, N*sizeof(double), cudaMemcpyDeviceToHost));
+   if( wiph ) CK(cudaMemcpy(wiph, b->v.wiph, N*sizeof(double), cudaMemcpyDeviceToHost));
+   return DISCO_OK;
+}
+
+static int launch_mindt(disco_batch *b){
+   View v = b->v;
+   unsigned nd = nblk(b->ndisk, 64);
+   k_mindt_begin<<<nd, 64, 0, b->stream>>>(v, b->ndisk);
+   k_mindt<6><<<(unsigned)b->cblk.size(), CB, 0, b->stream>>>(v);
+   k_mindt_end<<<nd, 64, 0, b->stream>>>(v, b->ndisk);
+   return cuda_status(cudaGetLastError());
+}
+
+extern "C" int disco_batch_setup_cells(disco_batch *b){
+   if( !b ) return DISCO_ERR_ARG;
+   CK(cudaSetDevice(b->device));
+   View v = b->v;
+   unsigned ncb = (unsigned)b->cblk.size();
+   k_setup<6,5><<<ncb, CB, 0, b->stream>>>(v, b->bc_fixed);
+   k_wcell<6><<<ncb, CB, 0, b->stream>>>(v);
+   if( b->any_mm3 ) k_wmean_nomove<<<nblk(v.Nann, 128), 128, 0, b->stream>>>(v);
+   CK(cudaGetLastError());
+   int s = launch_mindt(b);
+   if( s ) return s;
+   CK(cudaStreamSynchronize(b->stream));
+   b->have_cells = 1;
+   return DISCO_OK;
+}
+
+static int read_err(disco_batch *b){
+   int e = 0;
+   if( cudaMemcpy(&e, b->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ) return DISCO_ERR_CUDA;
+   if( e ){
+      int z = 0;
+      cudaMemcpy(b->d_err, &z, sizeof(int), cudaMemcpyHostToDevice);
+   }
+   if( e & ERRF_WRAP ) return DISCO_ERR_PHI_WRAP;
+   if( e & ERRF_NONFINITE ) return DISCO_ERR_NONFINITE;
+   return DISCO_OK;
+}
+
+extern "C" int disco_batch_mindt(disco_batch *b, double *dt){
+   if( !b ) return DISCO_ERR_ARG;
+   if( !b->have_cells ) return DISCO_ERR_STATE;
+   CK(cudaSetDevice(b->device));
+   int s = launch_mindt(b);
+   if( s ) return s;
+   CK(cudaStreamSynchronize(b->stream));
+   if( dt ){
+      std::vector<DiskState> st(b->ndisk);
+      CK(cudaMemcpy(st.data(), b->v.ds, sizeof(DiskState)*b->ndisk, cudaMemcpyDeviceToHost));
+      for( int d=0 ; d<b->ndisk ; ++d ) dt[d] = st[d].dt_next;
+   }
+   return read_err(b);
+}
+
+/* One substep of onestep() (onestep.c:84-229) for the hydro path. */
+static void launch_substep(disco_batch *b, double RK, int first, int last, double dtfac){
+   View v = b->v;
+   v.dtfac = dtfac;
+   cudaStream_t s = b->stream;
+   unsigned ncb = (unsigned)b->cblk.size(), nfb = (unsigned)b->fblk.size();
+   k_begin<6,5><<<ncb, CB, 0, s>>>(v, RK, first);                  mark(b, "k_begin");
+   if( first && b->any_mm3 ){ k_wmean<<<nblk(v.Nann, 128), 128, 0, s>>>(v); mark(b, "k_wmean"); }
+   k_I0<<<nblk((size_t)v.Nann*32, 128), 128, 0, s>>>(v);              mark(b, "k_I0");
+   k_faces<6><<<nfb, FB, 0, s>>>(v, 1);                               mark(b, "k_faces");
+   k_gradr<6><<<ncb, CB, 0, s>>>(v);                                  mark(b, "k_gradr");
+   k_flux_r<6,5><<<nfb, FB, 0, s>>>(v);                               mark(b, "k_flux_r");
+   k_flux_p<6,5><<<ncb, CB, 0, s>>>(v);                               mark(b, "k_flux_p");
+   k_update<6,5><<<ncb, CB, 0, s>>>(v, first, last, b->bc_fixed);     mark(b, "k_update");
+}
+
+/* timestep() (timestep.c:7-45). */
+static void launch_step(disco_batch *b, int use_next){
+   View v = b->v;
+   cudaStream_t s = b->stream;
+   unsigned nd = nblk(b->ndisk, 64);
+   k_disk_begin<<<nd, 64, 0, s>>>(v, b->ndisk, use_next);             mark(b, "k_disk_begin");
+   if( b->timestep_mode == 1 ){
+      launch_substep(b, 0.0, 1, 1, 1.0);
+      k_disk_mid<<<nd, 64, 0, s>>>(v, b->ndisk, 0.0, 1, 1);         mark(b, "k_disk_mid");
+   }else{
+      launch_substep(b, 0.0, 1, 0, 1.0);
+      k_disk_mid<<<nd, 64, 0, s>>>(v, b->ndisk, 0.0, 1, 1);         mark(b, "k_disk_mid");
+      launch_substep(b, 0.5, 0, 1, 0.5);
+      k_disk_mid<<<nd, 64, 0, s>>>(v, b->ndisk, 0.5, 0, 0);         mark(b, "k_disk_mid");
+   }
+   if( b->nq ){
+      k_diag_finish<<<nblk(v.Nann, 128), 128, 0, s>>>(v, b->d_Qrz, b->d_ann_blk0, b->d_ann_nblk);
+      mark(b, "k_diag_finish");
+   }
+   k_disk_end<<<nd, 64, 0, s>>>(v, b->ndisk);                        mark(b, "k_disk_end");
+}
+
+extern "C" int disco_batch_timestep(disco_batch *b, const double *dt){
+   if( !b ) return DISCO_ERR_ARG;
+   if( !b->have_cells ) return DISCO_ERR_STATE;
+   CK(cudaSetDevice(b->device));
+   if( dt ){
+      std::vector<DiskState> st(b->ndisk);
+      CK(cudaMemcpy(st.data(), b->v.ds, sizeof(DiskState)*b->ndisk, cudaMemcpyDeviceToHost));
+      for( int d=0 ; d<b->ndisk ; ++d ) st[d].dt_next = dt[d];
+      CK(cudaMemcpy(b->v.ds, st.data(), sizeof(DiskState)*b->ndisk, cudaMemcpyHostToDevice));
+   }
+   launch_step(b, 1);
+   CK(cudaGetLastError());
+   return DISCO_OK;
+}
+
+extern "C" int disco_batch_run(disco_batch *b, int nsteps){
+   if( !b || nsteps < 0 ) return DISCO_ERR_ARG;
+   if( !b->have_cells ) return DISCO_ERR_STATE;
+   CK(cudaSetDevice(b->device));
+   if( !b->graph ){
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      launch_step(b, 1);
+      CK(cudaStreamEndCapture(b->stream, &g));
+      CK(cudaGraphInstantiate(&b->graph, g, 0));
+      CK(cudaGraphDestroy(g));
+   }
+   for( int n=0 ; n<nsteps ; ++n ) CK(cudaGraphLaunch(b->graph, b->stream));
+   CK(cudaGetLastError());
+   return DISCO_OK;
+}
+
+extern "C" int disco_batch_time(const disco_batch *b, int disk, double *t, int *count){
+   if( !b || disk < 0 || disk >= b->ndisk ) return DISCO_ERR_ARG;
+   CK(cudaSetDevice(b->device));
+   CK(cudaStreamSynchronize(b->stream));
+   DiskState st;
+   CK(cudaMemcpy(&st, b->v.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
+   if( t ) *t = st.t;
+   if( count ) *count = st.count_steps;
+   return DISCO_OK;
+}
+
+extern "C" int disco_batch_get_faces(disco_batch *b, int disk, int dim, int *nfaces,
+                                     int *fIndex, int *iL, int *iR, int *LRtype, double *geom){
+   if( !b || disk < 0 || disk >= b->ndisk || (dim != 1 && dim != 2) ) return DISCO_ERR_ARG;
+   if( dim == 2 ){ if( nfaces ) *nfaces = 0; return DISCO_OK; }
+   CK(cudaSetDevice(b->device));
+   View v = b->v;
+   k_I0<<<nblk((size_t)v.Nann*32, 128), 128, 0, b->stream>>>(v);
+   k_faces<6><<<(unsigned)b->fblk.size(), FB, 0, b->stream>>>(v, 0);
+   CK(cudaGetLastError());
+   CK(cudaStreamSynchronize(b->stream));
+   const DiskParams &D = b->dparams[disk];
+   int f0 = D.face_r0;
+   int t0 = D.trr0, nt = D.ntrr;
+   int nf = b->tr_off[t0 + nt] - f0;
+   if( nfaces ) *nfaces = nf;
+   if( fIndex ) for( int t=0 ; t<=nt ; ++t ) fIndex[t] = b->tr_off[t0+t] - f0;
+   std::vector<int> tl(nf), tr(nf);
+   std::vector<unsigned char> tlr(nf);
+   if( iL || iR || LRtype ){
+      CK(cudaMemcpy(tl.data(), v.fL + f0, nf*sizeof(int), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(tr.data(), v.fR + f0, nf*sizeof(int), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(tlr.data(), v.fLR + f0, nf, cudaMemcpyDeviceToHost));
+      for( int n=0 ; n<nf ; ++n ){
+         if( iL ) iL[n] = tl[n] - D.cell0;
+         if( iR ) iR[n] = tr[n] - D.cell0;
+         if( LRtype ) LRtype[n] = tlr[n];
+      }
+   }
+   if( geom ){
+      std::vector<double> phic(nf), dA(nf), dp(nf);
+      CK(cudaMemcpy(phic.data(), v.fphic + f0, nf*sizeof(double), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(dA.data(), v.fdA + f0, nf*sizeof(double), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(dp.data(), v.fdp + f0, nf*sizeof(double), cudaMemcpyDeviceToHost));
+      const double *rj = b->rj.data() + D.rj0 + 1;
+      const double *zk = b->zk.data() + D.zk0 + 1;
+      for( int t=0 ; t<nt ; ++t ){
+         int gt = t0 + t;
+         int j = b->tr_j[gt], k = b->tr_k[gt];
+         for( int f=b->tr_off[gt]-f0 ; f<b->tr_off[gt+1]-f0 ; ++f ){
+            double *g = geom + 8*(size_t)f;
+            g[0] = b->tr_dxL[gt]; g[1] = b->tr_dxR[gt];
+            g[2] = .5*(rj[j]+rj[j]); g[3] = phic[f]; g[4] = 0.5*(zk[k]+zk[k-1]);
+            g[5] = dp[f]; g[6] = zk[k]-zk[k-1]; g[7] = dA[f];
+         }
+      }
+   }
+   return read_err(b);
+}
+
+extern "C" int disco_batch_get_diagnostics(disco_batch *b, int disk, double *Qrz, int *nq, double *t_avg){
+   if( !b || disk < 0 || disk >= b->ndisk ) return DISCO_ERR_ARG;
+   CK(cudaSetDevice(b->device));
+   CK(cudaStreamSynchronize(b->stream));
+   if( nq ) *nq = b->nq;
+   const DiskParams &D = b->dparams[disk];
+   int na = b->disk_Nr[disk]*b->disk_Nz[disk];
+   if( Qrz && b->nq ) CK(cudaMemcpy(Qrz, b->d_Qrz + (size_t)D.ann0*5, sizeof(double)*na*5, cudaMemcpyDeviceToHost));
+   if( t_avg ){
+      DiskState st;
+      CK(cudaMemcpy(&st, b->v.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
+      *t_avg = st.t_avg;
+   }
+   return DISCO_OK;
+}
+
+extern "C" int disco_batch_last_error(disco_batch *b){
+   if( !b ) return DISCO_ERR_ARG;
+   if( cudaSetDevice(b->device) != cudaSuccess ) return DISCO_ERR_CUDA;
+   cudaError_t e = cudaStreamSynchronize(b->stream);
+   if( e != cudaSuccess ) return DISCO_ERR_CUDA;
+   return read_err(b);
+}
+
+extern "C" int disco_batch_set_stream(disco_batch *b, void *stream){
+   if( !b ) return DISCO_ERR_ARG;
+   CK(cudaSetDevice(b->device));
+   CK(cudaStreamSynchronize(b->stream));
+   if( b->own_stream == NULL ) b->own_stream = b->stream;
+   b->stream = stream ? (cudaStream_t)stream : b->own_stream;
+   return DISCO_OK;
+}
+
+extern "C" int disco_batch_kernel_times(disco_batch *b, float *ms, const char **names,
+                                        int cap, int *nlaunch){
+   if( !b || !ms || !nlaunch || cap < 1 ) return DISCO_ERR_ARG;
+   if( !b->have_cells ) return DISCO_ERR_STATE;
+   CK(cudaSetDevice(b->device));
+   std::vector<cudaEvent_t> ev;
+   std::vector<const char *> nm;
+   b->tape = &ev; b->tape_names = &nm;
+   cudaEvent_t e0;
+   CK(cudaEventCreate(&e0));
+   CK(cudaEventRecord(e0, b->stream));
+   ev.push_back(e0);
+   launch_step(b, 1);
+   b->tape = NULL; b->tape_names = NULL;
+   CK(cudaGetLastError());
+   CK(cudaStreamSynchronize(b->stream));
+   int n = (int)nm.size();
+   if( n > cap ) n = cap;
+   for( int i=0 ; i<n ; ++i ){
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[i], ev[i+1]);
+      ms[i] = t;
+      if( names ) names[i] = nm[i];
+   }
+   *nlaunch = n;
+   for( cudaEvent_t e : ev ) cudaEventDestroy(e);
+   return read_err(b);
+}

@@ -1,0 +1,884 @@
+/*
+ * Kernels of the B200 Disco timestep, FP64 plain path (hydro).
+ *
+ * Layout (device, one batch of one or more disks):
+ *   cells      ragged SoA in annulus order; prim[q*Ncell + c], cons, RKcons,
+ *              gradp, gradr; piph[c], dphi[c], wiph[c]
+ *   annuli     ann_off[a] .. ann_off[a]+ann_np[a]-1 are annulus a's cells
+ *   r-tracks   track t joins annulus tr_a[t] (inner) and tr_b[t] (outer);
+ *              its faces are tr_off[t] .. tr_off[t+1]-1 (Np_a + Np_b of them,
+ *              faces_alt.c:87-100)
+ *   faces      SoA: fL, fR (global cells), fLR, fphic, fdA, fdp, fS[q], fG[q]
+ *   consume    consL[c] = face of the r-track outside c that consumes c in the
+ *              merge; consR[c] = same for the track inside c.  They give each
+ *              cell the contiguous runs of faces it belongs to, so every
+ *              scatter of the reference (plm.c:82-110, riemann.c:312-315)
+ *              becomes an order-preserving gather without atomics.
+ *
+ * Grids are block tables: cell kernels get one block per (annulus, chunk of
+ * CB cells), face kernels one block per (track, chunk of FB faces).
+ */
+#pragma once
+#include "disco_device.cuh"
+
+namespace disco {
+
+#define CB 128
+#define FB 128
+
+struct View {
+   int Ncell, Nann, Ntr, Nf;
+   const int *ann_off, *ann_np, *ann_disk, *ann_j, *ann_k;
+   const int *tr_a, *tr_b, *tr_off, *tr_flux, *tr_j, *tr_k;
+   const double *tr_dxL, *tr_dxR;
+   const int2 *cblk, *fblk;
+   const double *rj, *zk;
+   const DiskParams *dp;
+   DiskState *ds;
+   double *prim, *cons, *RKcons, *gradp, *gradr;
+   double *piph, *dphi, *wiph, *piph_new;
+   int *I0;
+   int *fL, *fR;
+   unsigned char *fLR;
+   double *fphic, *fdA, *fdp, *fS, *fG;
+   int *consL, *consR;
+   double *Gp;
+   double *diag_part;   /* per cell block: nq sums + volume */
+   int nq;
+   double dtfac;        /* 1 in the first substep, 0.5 in the second (timestep.c:39) */
+   int *err;
+};
+
+__device__ __forceinline__ void raise_err(const View &v, int e){
+   if( e ) atomicOr(v.err, e);
+}
+
+/* ------------------------------------------------------------------ k_begin
+ * First substep: RK snapshot (timestep.c:18-24), set_wcell (misc.c:101-168,
+ * modes 0/1/2/4; mode 3's mean is k_wmean), the moved-and-wrapped piph of
+ * move_cells + clean_pi (misc.c:256-268, 8-26) into piph_new.
+ * Every substep: adjust_RK_cons (misc.c:226-244) and plm_phi (plm.c:15-51). */
+template<int Q, int NC>
+__global__ void __launch_bounds__(CB) k_begin(View v, double RK, int first){
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   if( i >= np ) return;
+   const int N = v.Ncell;
+   int c0 = v.ann_off[a], c = c0 + i;
+   int cm = c0 + (i == 0 ? np-1 : i-1);
+   int cp = c0 + (i+1 == np ? 0 : i+1);
+   int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+
+   double pC[Q], pL[Q], pR[Q];
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ){
+      pC[q] = v.prim[q*N + c]; pL[q] = v.prim[q*N + cm]; pR[q] = v.prim[q*N + cp];
+   }
+   if( first ){
+      double w = 0.0;
+      if( P.mesh_motion ) w = .5*(pC[UPP] + pR[UPP]);       /* get_omega = prim[UPP] */
+      if( P.mesh_motion == 4 ){
+         int j = v.ann_j[a];
+         const double *rj = v.rj + P.rj0 + 1;
+         w = mesh_om(P, centroid_r(rj[j], rj[j-1]));
+      }
+      v.wiph[c] = w;
+      if( P.mesh_motion != 3 ){
+         int err = 0;
+         double phi = v.piph[c] + w*v.ds[d].dt;
+         int n = 0;
+         while( phi > P.Pmax ){ phi -= P.Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
+         while( phi < 0.0 ){ phi += P.Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
+         v.piph_new[c] = phi;
+         raise_err(v, err);
+      }
+   }
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ){
+      double cq = v.cons[q*N + c];
+      double rk;
+      if( first ){ rk = cq; v.RKcons[q*N + c] = cq; }
+      else rk = v.RKcons[q*N + c];
+      v.cons[q*N + c] = (1.-RK)*cq + RK*rk;
+   }
+   double dpL = v.dphi[cm], dpC = v.dphi[c], dpR = v.dphi[cp];
+   double PLM = P.PLM;
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ){
+      double sL = pC[q] - pL[q];  sL /= .5*( dpC + dpL );
+      double sR = pR[q] - pC[q];  sR /= .5*( dpR + dpC );
+      double sC = pR[q] - pL[q];  sC /= .5*( dpL + dpR ) + dpC;
+      double aa = PLM*sL, bb = sC, cc = PLM*sR;           /* minmod, plm.c:6 */
+      double m = aa;
+      if( aa*bb < 0.0 ) m = 0.0;
+      if( fabs(bb) < fabs(m) ) m = bb;
+      if( bb*cc < 0.0 ) m = 0.0;
+      if( fabs(cc) < fabs(m) ) m = cc;
+      v.gradp[q*N + c] = m;
+   }
+}
+
+/* Mesh_Motion 3 (misc.c:138-152): annulus mean of w, summed in cell order
+ * by one thread per annulus, then the move of the first substep. */
+__global__ void k_wmean(View v){
+   int a = blockIdx.x*blockDim.x + threadIdx.x;
+   if( a >= v.Nann ) return;
+   int np = v.ann_np[a], c0 = v.ann_off[a];
+   int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+   if( P.mesh_motion != 3 ) return;
+   double w = 0.0;
+   for( int i=0 ; i<np ; ++i ) w += v.wiph[c0+i];
+   w /= (double)np;
+   double dt = v.ds[d].dt;
+   int err = 0;
+   for( int i=0 ; i<np ; ++i ){
+      v.wiph[c0+i] = w;
+      double phi = v.piph[c0+i] + w*dt;
+      int n = 0;
+      while( phi > P.Pmax ){ phi -= P.Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
+      while( phi < 0.0 ){ phi += P.Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
+      v.piph_new[c0+i] = phi;
+   }
+   raise_err(v, err);
+}
+
+/* ------------------------------------------------------------------ k_I0
+ * faces_alt.c:57-79: I0 = first cell in quadrant I after any cell in
+ * quadrant IV (the cell whose upper edge is just past phi = 0).  One warp
+ * per annulus, ballots over 32-cell chunks. */
+__global__ void k_I0(View v){
+   int warp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
+   int lane = threadIdx.x & 31;
+   if( warp >= v.Nann ) return;
+   int a = warp;
+   int np = v.ann_np[a], c0 = v.ann_off[a];
+   const DiskParams &P = v.dp[v.ann_disk[a]];
+   double convert = 2.*DISCO_PI/P.Pmax;
+   int first4 = -1, res = 0;
+   for( int base=0 ; base<np ; base+=32 ){
+      int i = base + lane;
+      bool q1 = false, q4 = false;
+      if( i < np ){
+         double s, cs;
+         sincos(v.piph[c0+i]*convert, &s, &cs);
+         q1 = (s > 0. && cs > 0.);
+         q4 = (s < 0. && cs > 0.);
+      }
+      unsigned m4 = __ballot_sync(0xffffffffu, q4);
+      unsigned m1 = __ballot_sync(0xffffffffu, q1);
+      if( first4 < 0 && m4 ){
+         int l4 = __ffs(m4) - 1;
+         first4 = base + l4;
+         unsigned after = (l4 == 31) ? 0u : (m1 & (0xffffffffu << (l4+1)));
+         if( after ){ res = base + __ffs(after) - 1; break; }
+      }else if( first4 >= 0 && m1 ){
+         res = base + __ffs(m1) - 1; break;
+      }
+   }
+   if( lane == 0 ) v.I0[a] = res;
+}
+
+/* ------------------------------------------------------------------ faces
+ * buildfaces (faces_alt.c:102-177) as a merge path: face d of a track is
+ * the d-th step of the reference's two-pointer merge, found by binary
+ * search on the diagonal over the two annuli's edges unrolled from I0.
+ * Within one cell width the unrolled order equals the reference's wrapped
+ * comparison, so (iL, iR, LRtype) are the reference's; the face's own
+ * LR / LR_back and geometry are then evaluated exactly as :140-164 and
+ * addFace (:10-34) do.  Also emits the PLM face slopes S_q of plm_trans
+ * (plm.c:82-89) when with_slopes is set. */
+template<int Q>
+__global__ void __launch_bounds__(FB) k_faces(View v, int with_slopes){
+   int2 b = v.fblk[blockIdx.x];
+   int t = b.x, dd = b.y + threadIdx.x;
+   int A = v.tr_a[t], B = v.tr_b[t];
+   int NA = v.ann_np[A], NB = v.ann_np[B];
+   if( dd >= NA + NB ) return;
+   const int N = v.Ncell;
+   int f = v.tr_off[t] + dd;
+   int cA0 = v.ann_off[A], cB0 = v.ann_off[B];
+   int IA = v.I0[A], IB = v.I0[B];
+   const DiskParams &P = v.dp[v.ann_disk[A]];
+   double Pmax = P.Pmax;
+   int err = 0;
+
+   int lo = dd - NB > 0 ? dd - NB : 0;
+   int hi = dd < NA ? dd : NA;
+   while( lo < hi ){
+      int mid = (lo + hi) >> 1;
+      int ia = IA + mid;       if( ia >= NA ) ia -= NA;
+      int ib = IB + dd - mid - 1; if( ib >= NB ) ib -= NB;
+      if( v.piph[cA0+ia] > v.piph[cB0+ib] ) hi = mid; else lo = mid + 1;
+   }
+   int ka = lo, kb = dd - lo;
+   int ia = IA + ka; while( ia >= NA ) ia -= NA;
+   int ib = IB + kb; while( ib >= NB ) ib -= NB;
+   int cL = cA0 + ia, cR = cB0 + ib;
+
+   double pL = v.piph[cL], pR = v.piph[cR];
+   double dL = v.dphi[cL], dR = v.dphi[cR];
+   double dphi = pL - pR;
+   int n = 0;
+   while( dphi > .5*Pmax ){ dphi -= Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
+   while( dphi <-.5*Pmax ){ dphi += Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
+   int LR = dphi > 0. ? 1 : 0;
+   dphi = pL-dL - pR+dR;
+   n = 0;
+   while( dphi > .5*Pmax ){ dphi -= Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
+   while( dphi <-.5*Pmax ){ dphi += Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
+   int LR_back = dphi < 0. ? 1 : 0;
+   double xp1 = LR == 0 ? pL : pR;
+   double xm1 = LR_back == 0 ? pL-dL : pR-dR;
+
+   int j = v.tr_j[t], k = v.tr_k[t];
+   const double *rj = v.rj + P.rj0 + 1;
+   const double *zk = v.zk + P.zk0 + 1;
+   double dp = get_dp(xp1, xm1, Pmax, &err);
+   double phic = get_dp(xp1, .5*dp, Pmax, &err);
+   double r = .5*(rj[j]+rj[j]);
+   double dz = zk[k]-zk[k-1];
+   double dA = r*dp*dz;                                   /* get_dA(.,.,1) */
+
+   v.fL[f] = cL; v.fR[f] = cR; v.fLR[f] = (unsigned char)LR;
+   v.fphic[f] = phic; v.fdA[f] = dA; v.fdp[f] = dp;
+   if( LR == 0 ) v.consL[cL] = f; else v.consR[cR] = f;
+
+   if( with_slopes ){
+      double dxL = v.tr_dxL[t], dxR = v.tr_dxR[t];
+      double phiL = pL - .5*dL, phiR = pR - .5*dR;
+      double dpL = get_signed_dp(phic, phiL, Pmax, &err);
+      double dpR = get_signed_dp(phiR, phic, Pmax, &err);
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ){
+         double WL = v.prim[q*N + cL] + dpL*v.gradp[q*N + cL];
+         double WR = v.prim[q*N + cR] - dpR*v.gradp[q*N + cR];
+         v.fS[(size_t)q*v.Nf + f] = (WR-WL)/(dxR+dxL);
+      }
+   }
+   raise_err(v, err);
+}
+
+/* The faces of track t in which cell c (k-th edge from I0 of its annulus,
+ * cell index i) is the head on its side, in face order: run 1 is
+ * [s1, e1]; the I0 cell also heads the faces after the other annulus wraps,
+ * run 2 = [s2, e2] (empty when s2 > e2).  cons[] is consL or consR. */
+struct Runs { int s1, e1, s2, e2; };
+__device__ __forceinline__ Runs cell_runs(const View &v, const int *cons, int t,
+                                          int c0, int np, int i, int I0){
+   Runs R;
+   int c = c0 + i;
+   if( i == I0 ){
+      R.s1 = v.tr_off[t];
+      int prev = c0 + (I0 == 0 ? np-1 : I0-1);
+      R.s2 = cons[prev] + 1;
+      R.e2 = v.tr_off[t+1] - 1;
+   }else{
+      int prev = c0 + (i == 0 ? np-1 : i-1);
+      R.s1 = cons[prev] + 1;
+      R.s2 = 1; R.e2 = 0;
+   }
+   R.e1 = cons[c];
+   return R;
+}
+
+/* ------------------------------------------------------------------ k_gradr
+ * plm_trans for dim 1 (plm.c:56-195): sum S*dA over the cell's faces in the
+ * reference's face order (inner track first, then outer), divide by the
+ * cell's two face areas, then apply every face's limiter. */
+template<int Q>
+__global__ void __launch_bounds__(CB) k_gradr(View v){
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   if( i >= np ) return;
+   const int N = v.Ncell;
+   int c0 = v.ann_off[a], c = c0 + i;
+   int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+   int j = v.ann_j[a], k = v.ann_k[a];
+   int Nr = P.Nr;
+   int I0 = v.I0[a];
+   double g[Q];
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ) g[q] = 0.0;
+   if( P.PLM == 0.0 ){
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) v.gradr[q*N + c] = 0.0;
+      return;
+   }
+   int tin = j >= 1 ? P.trr0 + (j-1) + (Nr-1)*k : -1;
+   int tout = j <= Nr-2 ? P.trr0 + j + (Nr-1)*k : -1;
+   Runs Rin = {1,0,1,0}, Rout = {1,0,1,0};
+   if( tin >= 0 ) Rin = cell_runs(v, v.consR, tin, c0, np, i, I0);
+   if( tout >= 0 ) Rout = cell_runs(v, v.consL, tout, c0, np, i, I0);
+   const size_t Nf = v.Nf;
+#define ACC_RUN(s,e) for( int f=(s) ; f<=(e) ; ++f ){ double dA = v.fdA[f]; \
+      _Pragma("unroll") for( int q=0 ; q<Q ; ++q ) g[q] += v.fS[q*Nf + f]*dA; }
+   ACC_RUN(Rin.s1, Rin.e1)
+   ACC_RUN(Rin.s2, Rin.e2)
+   ACC_RUN(Rout.s1, Rout.e1)
+   ACC_RUN(Rout.s2, Rout.e2)
+#undef ACC_RUN
+   int err = 0;
+   const double *rj = v.rj + P.rj0 + 1;
+   const double *zk = v.zk + P.zk0 + 1;
+   double phip = v.piph[c];
+   double phim = phip - v.dphi[c];
+   double dph = get_dp(phip, phim, P.Pmax, &err);
+   double dz = zk[k]-zk[k-1];
+   double dAp = (.5*(rj[j]+rj[j]))*dph*dz;
+   double dAm = (.5*(rj[j-1]+rj[j-1]))*dph*dz;
+   double dAtot = dAp + dAm;
+   if( j == 0 ) dAtot = dAp;
+   if( j == Nr-1 ) dAtot = dAm;
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ) g[q] /= dAtot;
+   double PLM = P.PLM;
+#define LIM_RUN(s,e) for( int f=(s) ; f<=(e) ; ++f ){ \
+      _Pragma("unroll") for( int q=0 ; q<Q ; ++q ){ double S = v.fS[q*Nf + f]; \
+         if( S*g[q] < 0.0 ) g[q] = 0.0; else if( fabs(PLM*S) < fabs(g[q]) ) g[q] = PLM*S; } }
+   LIM_RUN(Rin.s1, Rin.e1)
+   LIM_RUN(Rin.s2, Rin.e2)
+   LIM_RUN(Rout.s1, Rout.e1)
+   LIM_RUN(Rout.s2, Rout.e2)
+#undef LIM_RUN
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ) v.gradr[q*N + c] = g[q];
+   raise_err(v, err);
+}
+
+/* ------------------------------------------------------------------ k_flux_r
+ * trans_flux dim 1 (misc.c:431-509) -> riemann_trans (riemann.c:114-170)
+ * -> solve_riemann; G_q = (F - w U*) dA dt per face. */
+template<int Q, int NC>
+__global__ void __launch_bounds__(FB) k_flux_r(View v){
+   int2 b = v.fblk[blockIdx.x];
+   int t = b.x;
+   if( !v.tr_flux[t] ) return;
+   int dd = b.y + threadIdx.x;
+   int f = v.tr_off[t] + dd;
+   if( f >= v.tr_off[t+1] ) return;
+   const int N = v.Ncell;
+   int cL = v.fL[f], cR = v.fR[f];
+   int d = v.ann_disk[v.tr_a[t]];
+   const DiskParams &P = v.dp[d];
+   int err = 0;
+   double dt = v.ds[d].dt*v.dtfac;
+   double dAdt = v.fdA[f]*dt;
+   double dxL = v.tr_dxL[t], dxR = v.tr_dxR[t];
+   double phi = v.fphic[f];
+   double phiL = v.piph[cL] - .5*v.dphi[cL];
+   double phiR = v.piph[cR] - .5*v.dphi[cR];
+   double dpL = get_signed_dp(phi, phiL, P.Pmax, &err);
+   double dpR = get_signed_dp(phiR, phi, P.Pmax, &err);
+   double primL[Q], primR[Q];
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ){
+      primL[q] = v.prim[q*N+cL] + v.gradr[q*N+cL]*dxL + v.gradp[q*N+cL]*dpL;
+      primR[q] = v.prim[q*N+cR] - v.gradr[q*N+cR]*dxR - v.gradp[q*N+cR]*dpR;
+   }
+   int j = v.tr_j[t];
+   const double *rj = v.rj + P.rj0 + 1;
+   double r = .5*(rj[j]+rj[j]);                 /* face cm[0] */
+   double G[Q];
+   solve_riemann<Q,NC,1>(P, primL, primR, r, get_om(P, r), 0.0, dAdt, G);
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ) v.fG[(size_t)q*v.Nf + f] = G[q];
+   raise_err(v, err);
+}
+
+/* ------------------------------------------------------------------ k_flux_p
+ * phi_flux (misc.c:368-426) -> riemann_phi (riemann.c:39-65): the face
+ * between cell i and i+1 of a real annulus, stored at cell i. */
+template<int Q, int NC>
+__global__ void __launch_bounds__(CB) k_flux_p(View v){
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   if( i >= np ) return;
+   int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+   int j = v.ann_j[a], k = v.ann_k[a];
+   if( j < P.NgRa || j >= P.Nr - P.NgRb || k < P.NgZa || k >= P.Nz - P.NgZb ) return;
+   const int N = v.Ncell;
+   int c0 = v.ann_off[a], cL = c0 + i, cR = c0 + (i < np-1 ? i+1 : 0);
+   const double *rj = v.rj + P.rj0 + 1;
+   const double *zk = v.zk + P.zk0 + 1;
+   double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
+   double r = centroid_r(rp, rm);
+   double dA = (rp-rm)*(zp-zm);                      /* get_dA(.,.,0) */
+   double dt = v.ds[d].dt*v.dtfac;
+   double primL[Q], primR[Q];
+   double dL = v.dphi[cL], dR = v.dphi[cR];
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ){
+      primL[q] = v.prim[q*N+cL] + .5*v.gradp[q*N+cL]*dL;
+      primR[q] = v.prim[q*N+cR] - .5*v.gradp[q*N+cR]*dR;
+   }
+   double w = r*v.wiph[cL];
+   double G[Q];
+   solve_riemann<Q,NC,0>(P, primL, primR, r, get_om(P, r), w, dA*dt, G);
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ) v.Gp[q*N + cL] = G[q];
+}
+
+/* ------------------------------------------------------------------ k_update
+ * Everything after the fluxes, per cell, in the reference's order:
+ *   flux gather  riemann.c:312-315 applied as phi_flux then trans_flux do
+ *   add_source   misc.c:538-580 (euler source + planet_src), old piph
+ *   move/clean/calc_dp   misc.c:256-288 (first substep; piph_new from k_begin)
+ *   calc_prim    misc.c:290-325 (euler cons2prim)
+ *   boundary     Boundary/fixed.c:11-60 (r ghosts re-initialised)
+ * and, on the last substep, the next step's getmindt (misc.c:39-84) and the
+ * diagnostics sums of add_diagnostics (analysis.c:52-107). */
+template<int Q, int NC>
+__global__ void __launch_bounds__(CB) k_update(View v, int first, int last, int bc_fixed){
+   __shared__ double s_red[CB/32][8];
+   __shared__ unsigned long long s_dt[CB/32];
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   bool active = i < np;
+   const int N = v.Ncell;
+   int c0 = v.ann_off[a], c = c0 + (active ? i : 0);
+   int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+   DiskState &S = v.ds[d];
+   int j = v.ann_j[a], k = v.ann_k[a];
+   const double *rj = v.rj + P.rj0 + 1;
+   const double *zk = v.zk + P.zk0 + 1;
+   bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
+   int err = 0;
+   double dt = S.dt*v.dtfac;
+   double prim[Q];
+   double dtc = 1.0e300;
+   double dq[6] = {0,0,0,0,0,0};
+   if( active ){
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) prim[q] = v.prim[q*N + c];
+      double piph = v.piph[c], dphi = v.dphi[c];
+      if( real ){
+         double cons[Q];
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ) cons[q] = v.cons[q*N + c];
+         /* phi faces: loop order of phi_flux */
+         int cprev = c0 + (i == 0 ? np-1 : i-1);
+         if( i > 0 ){
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ){ cons[q] += v.Gp[q*N+cprev]; cons[q] -= v.Gp[q*N+c]; }
+         }else{
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ){ cons[q] -= v.Gp[q*N+c]; cons[q] += v.Gp[q*N+cprev]; }
+         }
+         /* r faces: inner track (cell is R) then outer track (cell is L) */
+         int I0 = v.I0[a];
+         int tin = P.trr0 + (j-1) + (P.Nr-1)*k;
+         int tout = P.trr0 + j + (P.Nr-1)*k;
+         Runs Rin = cell_runs(v, v.consR, tin, c0, np, i, I0);
+         Runs Rout = cell_runs(v, v.consL, tout, c0, np, i, I0);
+         const size_t Nf = v.Nf;
+#define ADD_RUN(s,e,op) for( int f=(s) ; f<=(e) ; ++f ){ \
+         _Pragma("unroll") for( int q=0 ; q<Q ; ++q ) cons[q] op v.fG[q*Nf + f]; }
+         ADD_RUN(Rin.s1, Rin.e1, +=)
+         ADD_RUN(Rin.s2, Rin.e2, +=)
+         ADD_RUN(Rout.s1, Rout.e1, -=)
+         ADD_RUN(Rout.s2, Rout.e2, -=)
+#undef ADD_RUN
+         /* add_source with the pre-move cell */
+         double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
+         double phim = piph - dphi;
+         double dph = get_dp(piph, phim, P.Pmax, &err);
+         double dV = dV_of(rp, rm, dph, zp, zm);
+         double dVdt = dV*dt;
+         {  /* euler source, euler.c:171-215 */
+            double rho = prim[RHO], Pp = prim[PPP];
+            double r = centroid_r(rp, rm);
+            double r_1 = .5*(rp+rm);
+            double vr = prim[URR], omega = prim[UPP], vz = prim[UZZ];
+            double centrifugal = rho*omega*omega*r;
+            if( P.polar ) centrifugal *= sin(0.5*dph) / (0.5*dph);
+            double press_bal = Pp/r_1;
+            cons[SRR] += dVdt*( centrifugal + press_bal );
+            double om = get_om(P, r);
+            double om_r = get_om1(P, r);
+            double om_z = 0.0;
+            cons[TAU] += dVdt*rho*( r*vr*om*om - r*r*(omega-om)*(vr*om_r + vz*om_z));
+         }
+         for( int p=0 ; p<P.npl ; ++p ){   /* planet_src, planet.c:152-196 */
+            double rho = prim[RHO], vr = prim[URR], vz = prim[UZZ], omega = prim[UPP];
+            double phi = phim + 0.5*dph;
+            double x0 = centroid_r(rp, rm), x2 = centroid_z(zp, zm);
+            double F0, F1, F2;
+            planetary_force(P.grav2D, S.pl[p], x0, phi, x2, &F0, &F1, &F2);
+            double hr = 1.0, hp = x0, hz = 1.0;
+            if( P.polar ){ double adj = sin(0.5*dph)/(0.5*dph); F0 *= adj; F1 *= adj; }
+            cons[SRR] += rho*hr*F0*dVdt;
+            cons[LLL] += rho*hp*F1*dVdt;
+            cons[SZZ] += rho*hz*F2*dVdt;
+            cons[TAU] += rho*( hr*F0*vr + hz*F2*vz + hp*F1*omega )*dVdt;
+         }
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ) v.cons[q*N + c] = cons[q];
+         if( first ){
+            piph = v.piph_new[c];
+            dphi = get_dp(piph, v.piph_new[cprev], P.Pmax, &err);
+            v.piph[c] = piph; v.dphi[c] = dphi;
+         }
+         /* calc_prim */
+         double phim2 = piph - dphi;
+         double dph2 = get_dp(piph, phim2, P.Pmax, &err);
+         double dV2 = dV_of(rp, rm, dph2, zp, zm);
+         double r = centroid_r(rp, rm);
+         cons2prim<Q,NC>(P, cons, prim, r, get_om(P, r), dV2);
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ) v.prim[q*N + c] = prim[q];
+      }else{
+         if( first ){
+            int cprev = c0 + (i == 0 ? np-1 : i-1);
+            piph = v.piph_new[c];
+            dphi = get_dp(piph, v.piph_new[cprev], P.Pmax, &err);
+            v.piph[c] = piph; v.dphi[c] = dphi;
+         }
+         bool rghost = j < P.NgRa || j >= P.Nr - P.NgRb;
+         if( bc_fixed && rghost ){
+            double x[3] = { .5*(rj[j]+rj[j-1]), piph - .5*dphi, .5*(zk[k]+zk[k-1]) };
+            initial<Q,NC>(P, prim, x);
+            if( P.rotframe ) prim[UPP] -= P.RotOmega;       /* subtract_omega, rotframe.c:11 */
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ) v.prim[q*N + c] = prim[q];
+         }
+      }
+      if( last ){
+         double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
+         double phim = piph - dphi;
+         if( real ){                              /* mindt, euler.c:332-380 */
+            int cprev = c0 + (i == 0 ? np-1 : i-1);
+            double w = .5*(v.wiph[cprev] + v.wiph[c]);
+            double r = centroid_r(rp, rm);
+            double vp = (prim[UPP]-w)*r;
+            double cs = sqrt(P.gam*prim[PPP]/prim[RHO]);
+            double maxvr = cs + fabs(prim[URR]);
+            double maxvp = cs + fabs(vp);
+            double maxvz = cs + fabs(prim[UZZ]);
+            double dtr = (rp-rm)/maxvr;
+            double dtp = (.5*(rp+rm))*get_dp(piph, phim, P.Pmax, &err)/maxvp;
+            double dtz = (zp-zm)/maxvz;
+            double dtm = dtr;
+            if( dtm > dtp ) dtm = dtp;
+            if( dtm > dtz ) dtm = dtz;
+            if( dtm == dtm ) dtc = dtm;
+         }
+         if( v.nq ){                              /* diag_disk2d.c:17-38 */
+            double dph = get_dp(piph, phim, P.Pmax, &err);
+            double dV = dV_of(rp, rm, dph, zp, zm);
+            double r = .5*(rp+rm), phi = .5*(piph+phim);
+            double rho = prim[RHO], vr = prim[URR], omega = prim[UPP];
+            double Fp = 0.0;
+            if( P.npl > 1 ){
+               double Fr, Fz;
+               planetary_force(P.grav2D, S.pl[1], r, phi, 0.0, &Fr, &Fp, &Fz);
+            }
+            dq[0] = rho*dV;
+            dq[1] = 2.*DISCO_PI*r*rho*vr*dV;
+            dq[2] = 2.*DISCO_PI*r*rho*(r*Fp)*dV;
+            dq[3] = 2.*DISCO_PI*r*rho*( r*r*omega*vr )*dV;
+            dq[4] = omega*dV;
+            dq[5] = dV;
+         }
+      }
+   }
+   raise_err(v, err);
+   if( !last ) return;
+   /* block reductions (one annulus per block) */
+   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+   unsigned long long bits = dbits(dtc);
+#pragma unroll
+   for( int o=16 ; o>0 ; o>>=1 ){
+      unsigned long long ob = __shfl_down_sync(0xffffffffu, bits, o);
+      bits = ob < bits ? ob : bits;
+   }
+   if( lane == 0 ) s_dt[wid] = bits;
+   if( v.nq ){
+#pragma unroll
+      for( int m=0 ; m<6 ; ++m ){
+         double x = dq[m];
+#pragma unroll
+         for( int o=16 ; o>0 ; o>>=1 ) x += __shfl_down_sync(0xffffffffu, x, o);
+         if( lane == 0 ) s_red[wid][m] = x;
+      }
+   }
+   __syncthreads();
+   if( threadIdx.x == 0 ){
+      unsigned long long mb = s_dt[0];
+      for( int w=1 ; w<CB/32 ; ++w ) mb = s_dt[w] < mb ? s_dt[w] : mb;
+      if( real ) atomicMin(&S.dtmin, mb);
+      if( v.nq ){
+         for( int m=0 ; m<6 ; ++m ){
+            double x = 0.0;
+            for( int w=0 ; w<CB/32 ; ++w ) x += s_red[w][m];
+            v.diag_part[(size_t)blockIdx.x*6 + m] = x;
+         }
+      }
+   }
+}
+
+/* ------------------------------------------------------------------ per disk */
+/* Start of timestep(): planet_RK_copy, reset of the dt reduction. */
+__global__ void k_disk_begin(View v, int ndisk, int use_next){
+   int d = blockIdx.x*blockDim.x + threadIdx.x;
+   if( d >= ndisk ) return;
+   DiskState &S = v.ds[d];
+   const DiskParams &P = v.dp[d];
+   if( use_next ) S.dt = S.dt_next;
+   for( int p=0 ; p<P.npl ; ++p ){
+      Planet &pl = S.pl[p];
+      pl.RK_r = pl.r; pl.RK_phi = pl.phi; pl.RK_M = pl.M; pl.RK_omega = pl.omega; pl.RK_vr = pl.vr;
+   }
+   double dt0 = P.maxDT / P.CFL;
+   if( dt0 <= 0.0 ) dt0 = 1.0e100;
+   S.dtmin = dbits(dt0);
+}
+
+/* After substep 1 (onestep.c:163-166, timestep.c:38): planet adjust/move,
+ * planet phi wrap (clean_pi, misc.c:27-34), t += dt. */
+__global__ void k_disk_mid(View v, int ndisk, double RK, int first, int advance_t){
+   int d = blockIdx.x*blockDim.x + threadIdx.x;
+   if( d >= ndisk ) return;
+   DiskState &S = v.ds[d];
+   const DiskParams &P = v.dp[d];
+   double dt = S.dt;
+   double dts = first ? dt : 0.5*dt;
+   if( first ){
+      for( int p=0 ; p<P.npl ; ++p ){
+         Planet &pl = S.pl[p];
+         pl.r     = (1.-RK)*pl.r     + RK*pl.RK_r;
+         pl.phi   = (1.-RK)*pl.phi   + RK*pl.RK_phi;
+         pl.M     = (1.-RK)*pl.M     + RK*pl.RK_M;
+         pl.omega = (1.-RK)*pl.omega + RK*pl.RK_omega;
+         pl.vr    = (1.-RK)*pl.vr    + RK*pl.RK_vr;
+         if( P.planets_move ) pl.phi += pl.omega*dts;
+      }
+   }
+   for( int p=0 ; p<P.npl ; ++p ){
+      Planet &pl = S.pl[p];
+      double phi = pl.phi;
+      int n = 0;
+      while( phi > P.Pmax && n++ < WRAP_CAP ){ phi -= P.Pmax; pl.RK_phi -= P.Pmax; }
+      while( phi < 0.0 && n++ < WRAP_CAP ){ phi += P.Pmax; pl.RK_phi += P.Pmax; }
+      pl.phi = phi;
+   }
+   if( advance_t ) S.t += dt;
+}
+
+/* End of timestep(): dt of the next step, diagnostics (analysis.c:97-105),
+ * count_steps. */
+__global__ void k_disk_end(View v, int ndisk){
+   int d = blockIdx.x*blockDim.x + threadIdx.x;
+   if( d >= ndisk ) return;
+   DiskState &S = v.ds[d];
+   const DiskParams &P = v.dp[d];
+   double mn = __longlong_as_double((long long)S.dtmin);
+   S.dt_next = mn*P.CFL;
+   S.t_avg += S.dt;
+   S.count_steps += 1;
+   if( !(S.dt_next > 0.0) || S.dt_next != S.dt_next || S.dt_next >= 1.0e99 )
+      atomicOr(v.err, ERRF_NONFINITE);
+}
+
+/* Per annulus: sum its blocks' diagnostic partials in block order. */
+__global__ void k_diag_finish(View v, double *Qrz, const int *ann_blk0, const int *ann_nblk){
+   int a = blockIdx.x*blockDim.x + threadIdx.x;
+   if( a >= v.Nann ) return;
+   int d = v.ann_disk[a];
+   double dt = v.ds[d].dt;
+   double s[6] = {0,0,0,0,0,0};
+   for( int bb=0 ; bb<ann_nblk[a] ; ++bb ){
+      const double *p = v.diag_part + (size_t)(ann_blk0[a]+bb)*6;
+      for( int m=0 ; m<6 ; ++m ) s[m] += p[m];
+   }
+   for( int m=0 ; m<5 ; ++m ) Qrz[(size_t)a*5 + m] += s[m]*dt / s[5];
+}
+
+/* ------------------------------------------------------------------ setup
+ * setupCells (domain.c:319-383): initial(), prim2cons, cons2prim on real
+ * cells; then main.c's boundary_trans for ghosts. */
+template<int Q, int NC>
+__global__ void __launch_bounds__(CB) k_setup(View v, int bc_fixed){
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   if( i >= np ) return;
+   const int N = v.Ncell;
+   int c = v.ann_off[a] + i;
+   int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+   int j = v.ann_j[a], k = v.ann_k[a];
+   const double *rj = v.rj + P.rj0 + 1;
+   const double *zk = v.zk + P.zk0 + 1;
+   bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
+   int err = 0;
+   double piph = v.piph[c], dphi = v.dphi[c];
+   double prim[Q], cons[Q];
+   if( real ){
+      double z = centroid_z(zk[k], zk[k-1]);
+      double r = centroid_r(rj[j], rj[j-1]);
+      double phim = piph - dphi;
+      double dph = get_dp(piph, phim, P.Pmax, &err);
+      double dV = dV_of(rj[j], rj[j-1], dph, zk[k], zk[k-1]);
+      double x[3] = {r, piph - .5*dphi, z};
+      initial<Q,NC>(P, prim, x);
+      if( P.rotframe ) prim[UPP] -= P.RotOmega;
+      double om = get_om(P, r);
+      prim2cons<Q,NC>(P, prim, cons, r, om, dV);
+      cons2prim<Q,NC>(P, cons, prim, r, om, dV);
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ){ v.prim[q*N+c] = prim[q]; v.cons[q*N+c] = cons[q]; }
+   }else{
+      bool rghost = j < P.NgRa || j >= P.Nr - P.NgRb;
+      if( bc_fixed && rghost ){
+         double x[3] = { .5*(rj[j]+rj[j-1]), piph - .5*dphi, .5*(zk[k]+zk[k-1]) };
+         initial<Q,NC>(P, prim, x);
+         if( P.rotframe ) prim[UPP] -= P.RotOmega;
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ) v.prim[q*N+c] = prim[q];
+      }
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) v.cons[q*N+c] = 0.0;
+   }
+   raise_err(v, err);
+}
+
+/* prim2cons on real cells for an upload without cons (domain.c:349). */
+template<int Q, int NC>
+__global__ void __launch_bounds__(CB) k_prim2cons(View v){
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   if( i >= np ) return;
+   const int N = v.Ncell;
+   int c = v.ann_off[a] + i;
+   const DiskParams &P = v.dp[v.ann_disk[a]];
+   int j = v.ann_j[a], k = v.ann_k[a];
+   const double *rj = v.rj + P.rj0 + 1;
+   const double *zk = v.zk + P.zk0 + 1;
+   int err = 0;
+   double piph = v.piph[c], dphi = v.dphi[c];
+   double r = centroid_r(rj[j], rj[j-1]);
+   double dph = get_dp(piph, piph - dphi, P.Pmax, &err);
+   double dV = dV_of(rj[j], rj[j-1], dph, zk[k], zk[k-1]);
+   double prim[Q], cons[Q];
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ) prim[q] = v.prim[q*N+c];
+   prim2cons<Q,NC>(P, prim, cons, r, get_om(P, r), dV);
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ) v.cons[q*N+c] = cons[q];
+   raise_err(v, err);
+}
+
+/* set_wcell alone (setupCells' last call, domain.c:385). */
+template<int Q>
+__global__ void __launch_bounds__(CB) k_wcell(View v){
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   if( i >= np ) return;
+   const int N = v.Ncell;
+   int c0 = v.ann_off[a], c = c0 + i;
+   int cp = c0 + (i+1 == np ? 0 : i+1);
+   const DiskParams &P = v.dp[v.ann_disk[a]];
+   double w = 0.0;
+   if( P.mesh_motion ) w = .5*(v.prim[UPP*N + c] + v.prim[UPP*N + cp]);
+   if( P.mesh_motion == 4 ){
+      int j = v.ann_j[a];
+      const double *rj = v.rj + P.rj0 + 1;
+      w = mesh_om(P, centroid_r(rj[j], rj[j-1]));
+   }
+   v.wiph[c] = w;
+}
+
+/* Mesh_Motion 3 mean without a move (set-up only). */
+__global__ void k_wmean_nomove(View v){
+   int a = blockIdx.x*blockDim.x + threadIdx.x;
+   if( a >= v.Nann ) return;
+   const DiskParams &P = v.dp[v.ann_disk[a]];
+   if( P.mesh_motion != 3 ) return;
+   int np = v.ann_np[a], c0 = v.ann_off[a];
+   double w = 0.0;
+   for( int i=0 ; i<np ; ++i ) w += v.wiph[c0+i];
+   w /= (double)np;
+   for( int i=0 ; i<np ; ++i ) v.wiph[c0+i] = w;
+}
+
+/* Stand-alone getmindt (misc.c:39-84) into ds[d].dt_next. */
+template<int Q>
+__global__ void __launch_bounds__(CB) k_mindt(View v){
+   __shared__ unsigned long long s_dt[CB/32];
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   const int N = v.Ncell;
+   int c0 = v.ann_off[a];
+   int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+   int j = v.ann_j[a], k = v.ann_k[a];
+   bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
+   double dtc = 1.0e300;
+   int err = 0;
+   if( i < np && real ){
+      int c = c0 + i;
+      const double *rj = v.rj + P.rj0 + 1;
+      const double *zk = v.zk + P.zk0 + 1;
+      double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
+      double piph = v.piph[c], phim = piph - v.dphi[c];
+      int cprev = c0 + (i == 0 ? np-1 : i-1);
+      double w = .5*(v.wiph[cprev] + v.wiph[c]);
+      double r = centroid_r(rp, rm);
+      double vp = (v.prim[UPP*N+c]-w)*r;
+      double cs = sqrt(P.gam*v.prim[PPP*N+c]/v.prim[RHO*N+c]);
+      double maxvr = cs + fabs(v.prim[URR*N+c]);
+      double maxvp = cs + fabs(vp);
+      double maxvz = cs + fabs(v.prim[UZZ*N+c]);
+      double dtr = (rp-rm)/maxvr;
+      double dtp = (.5*(rp+rm))*get_dp(piph, phim, P.Pmax, &err)/maxvp;
+      double dtz = (zp-zm)/maxvz;
+      double dtm = dtr;
+      if( dtm > dtp ) dtm = dtp;
+      if( dtm > dtz ) dtm = dtz;
+      if( dtm == dtm ) dtc = dtm;
+   }
+   raise_err(v, err);
+   unsigned long long bits = dbits(dtc);
+   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+   for( int o=16 ; o>0 ; o>>=1 ){
+      unsigned long long ob = __shfl_down_sync(0xffffffffu, bits, o);
+      bits = ob < bits ? ob : bits;
+   }
+   if( lane == 0 ) s_dt[wid] = bits;
+   __syncthreads();
+   if( threadIdx.x == 0 && real ){
+      unsigned long long mb = s_dt[0];
+      for( int w=1 ; w<CB/32 ; ++w ) mb = s_dt[w] < mb ? s_dt[w] : mb;
+      atomicMin(&v.ds[d].dtmin, mb);
+   }
+}
+
+__global__ void k_mindt_begin(View v, int ndisk){
+   int d = blockIdx.x*blockDim.x + threadIdx.x;
+   if( d >= ndisk ) return;
+   const DiskParams &P = v.dp[d];
+   double dt0 = P.maxDT / P.CFL;
+   if( dt0 <= 0.0 ) dt0 = 1.0e100;
+   v.ds[d].dtmin = dbits(dt0);
+}
+__global__ void k_mindt_end(View v, int ndisk){
+   int d = blockIdx.x*blockDim.x + threadIdx.x;
+   if( d >= ndisk ) return;
+   double mn = __longlong_as_double((long long)v.ds[d].dtmin);
+   v.ds[d].dt_next = mn*v.dp[d].CFL;
+}
+
+} // namespace disco

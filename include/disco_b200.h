@@ -1,0 +1,212 @@
+/*
+ * disco_b200 -- C ABI of the B200-native Disco RK timestep.
+ *
+ * This is the drop-in boundary for the serial (USE_MPI=0) Disco hot path.
+ * In the reference, main.c calls two functions per step:
+ *
+ *     double getmindt( struct domain * );          misc.c:39-84   (main.c:12,72)
+ *     void   timestep( struct domain * , double ); timestep.c:7-45 (main.c:7,81)
+ *
+ * and timestep() calls onestep() twice (onestep.c:84-229).  Physics modules
+ * are link-time selected C files (hydro.h, geometry.h, boundary.h, omega.h,
+ * Planets/*.c, Initial/*.c) chosen in Makefile_opt.in; run-time parameters
+ * come from in.par (readpar.c:44-188).
+ *
+ * Here the whole state lives on one GPU between calls, laid out as ragged
+ * structure-of-arrays (cells in annulus order jk = j + Nr*k, i = 0..Np-1).
+ * The functions below take plain pointers and sizes; no struct of the
+ * reference crosses the boundary, so a C, cgo, ctypes or JNI caller can bind
+ * them directly.  Every function returns an int status: DISCO_OK (0) or one
+ * of the DISCO_ERR_* codes; disco_strerror() names it.  Device-side failures
+ * that the reference would hang or NaN on (unbounded phi-wrap loops on a
+ * non-finite piph, misc.c:22-23 / cylindrical.c:12-13) set an error word
+ * that the next call reports as DISCO_ERR_PHI_WRAP or DISCO_ERR_NONFINITE.
+ *
+ * A "batch" holds one or more independent disks (each its own in.par grid,
+ * parameters and dt) advanced together in the same kernels.  A single-disk
+ * batch is exactly the reference's serial domain.
+ */
+#ifndef DISCO_B200_H
+#define DISCO_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DISCO_ABI_VERSION 1
+
+enum disco_status {
+   DISCO_OK = 0,
+   DISCO_ERR_ARG = 1,          /* bad argument (null pointer, size, unknown module) */
+   DISCO_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+   DISCO_ERR_UNSUPPORTED = 3,  /* module combination not built */
+   DISCO_ERR_PHI_WRAP = 4,     /* phi wrap loop hit its iteration cap (non-finite piph) */
+   DISCO_ERR_NONFINITE = 5,    /* non-finite dt or state detected */
+   DISCO_ERR_NO_DEVICE = 6,    /* no CUDA device / library built without one */
+   DISCO_ERR_STATE = 7         /* call out of order (e.g. step before set_cells) */
+};
+
+/* Module choices, one per Makefile_opt.in line (Makefile:11-26).  The names
+ * match the reference's module file names. */
+enum disco_hydro    { DISCO_HYDRO_EULER = 0, DISCO_HYDRO_MHD = 1 };
+enum disco_boundary { DISCO_BC_FIXED = 0, DISCO_BC_ZEROGRAD = 1, DISCO_BC_FIXED3D = 2 };
+enum disco_planets  { DISCO_PLANETS_NONE = 0, DISCO_PLANETS_SUN = 1, DISCO_PLANETS_CM2 = 2,
+                      DISCO_PLANETS_BINARY_SOFT = 3 };
+enum disco_initial  { DISCO_IC_KEPLER_NOISE = 0, DISCO_IC_MHD_SHEAR_NOISE = 1 };
+enum disco_analysis { DISCO_DIAG_NONE = 0, DISCO_DIAG_DISK2D = 1 };
+enum disco_precision{ DISCO_PREC_FP64 = 0, DISCO_PREC_MIXED = 1 };
+
+/* Compile-time module selection (Makefile_opt.in).  num_c/num_n/ct_mode are
+ * the reference's NUM_C, NUM_N and CT_MODE (paul.h:26-49). */
+typedef struct disco_modules {
+   int hydro, boundary, planets, initial, analysis;
+   int num_c, num_n, ct_mode;
+} disco_modules;
+
+/* Run-time parameters: the subset of struct param_list (paul.h:51-127) that
+ * the step reads, with read_par_file's 2*pi scalings already applied
+ * (readpar.c:162-172).  Field names follow param_list. */
+typedef struct disco_params {
+   int    Num_R, Num_Z;
+   double aspect;
+   double rmin, rmax, zmin, zmax, phimax;
+   int    NoBC_Rmin, NoBC_Rmax, NoBC_Zmin, NoBC_Zmax;
+   int    LogZoning, R_Periodic, Z_Periodic;
+   double LogRadius;
+   int    Mesh_Motion, Riemann_Solver, Timestep;
+   double CFL, PLM, maxDT;
+   double Density_Floor, Pressure_Floor;
+   int    Exact_Mesh_Omega;
+   double Exact_Mesh_Omega_Par;
+   int    Energy_Omega;
+   double Energy_Omega_Par;
+   int    RotFrame;
+   double RotOmega, RotD;
+   double Adiabatic_Index;
+   double viscosity;
+   int    visc_flag, alpha_flag;
+   int    isothermal_flag;
+   int    Cs2_Profile;
+   double Cs2_Par;
+   double Disk_Mach;
+   double Mass_Ratio;
+   int    grav2D;
+   int    CT;
+   int    initPar0;
+   double initPar[9];          /* initPar[1..8] = Init_Par1..8; [0] unused */
+   double metricPar[5];        /* metricPar[1..4] = Metric_Par1..4 */
+   double t_min;
+} disco_params;
+
+typedef struct disco_batch disco_batch;   /* opaque device-resident batch */
+
+/* Version of this ABI (DISCO_ABI_VERSION). */
+int disco_abi_version(void);
+const char *disco_strerror(int status);
+
+/*
+ * Create a batch of `ndisk` independent disks on CUDA device `device`.
+ *
+ * Per disk d: params[d], and its grid exactly as setupGrid() builds it
+ * (gridsetup.c:15-142): Nr[d], Nz[d] (annuli incl. ghosts), Ng[4*d+0..3] =
+ * NgRa, NgRb, NgZa, NgZb, and concatenated arrays
+ *   Np      : Nr*Nz ints per disk            (cells per annulus)
+ *   r_jph   : Nr+1 doubles per disk, element 0 is the reference's r_jph[-1]
+ *   z_kph   : Nz+1 doubles per disk, element 0 is z_kph[-1]
+ * All disks share one module selection `mods` and one precision.
+ * Replaces: setupGrid + setupDomain allocation (gridsetup.c:90-95,
+ * domain.c:34-38,112-113).
+ */
+int disco_batch_create(int device, const disco_modules *mods, int precision,
+                       int ndisk, const disco_params *params,
+                       const int *Nr, const int *Nz, const int *Ng,
+                       const int *Np, const double *r_jph, const double *z_kph,
+                       disco_batch **out);
+void disco_batch_destroy(disco_batch *b);
+
+/* Total cells (incl. ghosts) and real cells of the batch; Q = num_c+num_n. */
+int disco_batch_sizes(const disco_batch *b, int64_t *ncell, int64_t *nreal, int *q);
+
+/*
+ * Upload cell state from host memory.  All arrays hold ncell entries in
+ * annulus order (disk-major); prim/cons are cell-major, Q doubles per cell
+ * (the reference's struct cell prim[NUM_Q] / cons[NUM_Q], paul.h:185-186).
+ * real[] is the reference's cell->real flag.  cons may be NULL (then cons is
+ * rebuilt from prim with prim2cons on the device, as setupCells does,
+ * domain.c:205).  Phi (num_faces doubles per cell) may be NULL when CT is off.
+ */
+int disco_batch_set_cells(disco_batch *b, const double *prim, const double *cons,
+                          const double *piph, const double *dphi, const double *wiph,
+                          const int *real, const double *Phi);
+
+/* Download cell state (same layout); any pointer may be NULL to skip it. */
+int disco_batch_get_cells(disco_batch *b, double *prim, double *cons,
+                          double *piph, double *dphi, double *wiph, double *Phi);
+
+/*
+ * Device set-up of a fresh batch after set_cells with prim unset: evaluates
+ * the Initial module on every real cell, prim2cons, cons2prim, set_wcell
+ * (domain.c:283-386) and the boundary (main.c:53-62).  piph/dphi must have
+ * been uploaded (the reference draws them from rand(), domain.c:206-233).
+ */
+int disco_batch_setup_cells(disco_batch *b);
+
+/* getmindt (misc.c:39-84) for every disk: dt[d] = CFL * min over real cells. */
+int disco_batch_mindt(disco_batch *b, double *dt);
+
+/*
+ * One full step of every disk: timestep() (timestep.c:7-45) with the given
+ * per-disk dt (NULL = use the dt that the last mindt/step left on the
+ * device, i.e. getmindt of the current state, with no host round trip).
+ */
+int disco_batch_timestep(disco_batch *b, const double *dt);
+
+/*
+ * nsteps repetitions of { dt = getmindt; timestep(dt) } (main.c:69-83
+ * without output), all on the device, replayed from a CUDA graph.
+ */
+int disco_batch_run(disco_batch *b, int nsteps);
+
+/* Simulation time and step count of disk d (theDomain->t, count_steps). */
+int disco_batch_time(const disco_batch *b, int disk, double *t, int *count_steps);
+
+/*
+ * Face list of disk `disk` for dim 1 (r) or 2 (z), built from the current
+ * state exactly as setup_faces/buildfaces build it (misc.c:512-532,
+ * faces_alt.c:36-179).  fIndex has N_ftracks+1 entries (the reference's
+ * fIndex_r / fIndex_z); iL/iR are cell indices within the disk (annulus
+ * order); LRtype as struct face.  Any output pointer may be NULL; *nfaces
+ * receives the count.  geom (8 doubles per face: dxL dxR cm0 cm1 cm2 dphi dl
+ * dA) may be NULL.
+ */
+int disco_batch_get_faces(disco_batch *b, int disk, int dim, int *nfaces,
+                          int *fIndex, int *iL, int *iR, int *LRtype, double *geom);
+
+/* Time-averaged diagnostics Qrz of disk d (analysis.c:52-107): Nr*Nz*nq. */
+int disco_batch_get_diagnostics(disco_batch *b, int disk, double *Qrz, int *nq, double *t_avg);
+
+/* Device error word accumulated since the last call (DISCO_OK if none). */
+int disco_batch_last_error(disco_batch *b);
+
+/*
+ * Launch all further work of the batch on `stream` (a cudaStream_t, passed
+ * as void* so this header needs no CUDA include; NULL restores the batch's
+ * own stream).  Lets a caller time the step with events on its own stream.
+ */
+int disco_batch_set_stream(disco_batch *b, void *stream);
+
+/*
+ * Run one full step with a CUDA event between every kernel launch and
+ * return each launch's device time: ms[i] and the kernel's name in
+ * names[i] (static strings), for i < *nlaunch (at most cap).  The
+ * reference's profiler (profiler.c:188-206) labels the same phases.
+ */
+int disco_batch_kernel_times(disco_batch *b, float *ms, const char **names, int cap, int *nlaunch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,59 @@
+/*
+ * disco_b200 host side (C): the parts of Disco's start-up that stay on the
+ * host -- in.par and Makefile_opt.in parsing, grid construction and the
+ * per-annulus phi offsets -- restated so a batch can be built without the
+ * reference tree.  Each function names the reference routine it replaces.
+ */
+#ifndef DISCO_HOST_H
+#define DISCO_HOST_H
+
+#include "disco_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/*
+ * Parse an in.par file (readpar.c:6-42 readvar, :44-188 read_par_file).
+ * Same key names, same "first matching line wins" rule, same separators
+ * ("\t :=>_"), same 2*pi / pi scalings of T_*, Phi_Max and Z_* (:162-172).
+ * Missing keys keep their zero value, as in the reference (main.c:31 zero-
+ * initialises the domain); *nmissing receives how many were absent.
+ */
+int disco_read_par(const char *path, disco_params *p, int *nmissing);
+
+/*
+ * Parse a Makefile_opt.in module selection (INITIAL, HYDRO, BOUNDARY,
+ * PLANETS, ANALYSIS, NUM_C, NUM_N, CT_MODE; Makefile:11-26).  Unknown module
+ * names give DISCO_ERR_UNSUPPORTED.
+ */
+int disco_read_opt(const char *path, disco_modules *m);
+
+/*
+ * setupGrid (gridsetup.c:15-142) for the serial single-rank case: fills
+ * Nr, Nz (annuli incl. ghosts), Ng[4] = {NgRa, NgRb, NgZa, NgZb}, and, when
+ * the pointers are non-NULL, Np[Nr*Nz], r_jph[Nr+1], z_kph[Nz+1] (element 0
+ * is index -1 of the reference's arrays).  Call once with NULL arrays to
+ * get the sizes.
+ */
+int disco_setup_grid(const disco_params *p, int *Nr, int *Nz, int *Ng,
+                     int *Np, double *r_jph, double *z_kph);
+
+/*
+ * The per-annulus phi offsets of setupDomain (domain.c:172-233): glibc
+ * srand(314159), one discarded rand(), then p0 = Pmax*rand()/RAND_MAX per
+ * annulus, piph_i = p0 + i*Pmax/Np (wrapped once), and dphi from calc_dp
+ * (misc.c:271-288) as setupCells does first (domain.c:290).  Also sets
+ * real[] (1 for cells outside the ghost annuli, domain.c:307-351).
+ */
+int disco_setup_phi(const disco_params *p, int Nr, int Nz, const int *Ng,
+                    const int *Np, double *piph, double *dphi, int *real);
+
+/* sizeof(disco_params) for which = 0, sizeof(disco_modules) for 1: lets a
+ * foreign-language mirror of the structs check its layout. */
+int disco_sizeof(int which);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

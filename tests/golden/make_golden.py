@@ -1,0 +1,70 @@
+"""Generate the golden fixtures of tests/golden/ by running the reference.
+
+The reference Disco has no test vectors of its own (no tests/, no golden
+data), so its behaviour is pinned by running it: oracle/Makefile compiles the
+reference's unmodified serial sources with a fixed-step driver
+(oracle/ref_driver.c), and this script records its state after 0 and N steps
+for a few small configurations.  Run it where the reference tree is
+available:
+
+    python tests/golden/make_golden.py
+
+Each case writes <case>.npz with the step-0 state (s0_*), the step-N state
+(sN_*), the dt sequence, the r-face list after N steps and the diagnostics.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+import pyoracle  # noqa: E402
+
+TEMPLATES = os.path.join(REPO, "disco_b200", "templates")
+
+# case -> (module config, in.par overrides, steps)
+CASES = {
+    "c0_log16": ("c0_kepler2d", {"Num_R": 16}, 8),
+    "c0_lin20": ("c0_kepler2d", {"Num_R": 20, "Log_Zoning": 0, "Mach_Number": 12.0,
+                                 "Init_Par0": 27}, 8),
+    "c0_hll_fe_mm3": ("c0_kepler2d", {"Num_R": 10, "Riemann_Solver": 0, "Timestep": 1,
+                                      "Mesh_Motion": 3, "PLM": 1.2}, 6),
+    "c0_cm2": ("c0_cm2", {"Num_R": 24, "Mass_Ratio": 1.0e-3}, 6),
+}
+
+
+def par_text(cfg_par, overrides):
+    out = []
+    with open(os.path.join(TEMPLATES, cfg_par + ".par")) as f:
+        for line in f:
+            key = line.split()[0] if line.split() else ""
+            if key in overrides:
+                line = "%s\t\t%s\n" % (key, repr(overrides[key]) if isinstance(overrides[key], float)
+                                       else overrides[key])
+            out.append(line)
+    return "".join(out)
+
+
+def main():
+    for case, (cfg, over, n) in CASES.items():
+        text = par_text("c0_kepler2d", over)
+        with open(os.path.join(HERE, case + ".par"), "w") as f:
+            f.write(text)
+        d0 = pyoracle.run_ref(cfg, text, 0)
+        dn = pyoracle.run_ref(cfg, text, n)
+        F = dn["faces_1"]
+        np.savez_compressed(
+            os.path.join(HERE, case + ".npz"), cfg=cfg, nsteps=n,
+            s0_prim=d0["prim"], s0_cons=d0["cons"], s0_piph=d0["piph"], s0_dphi=d0["dphi"],
+            s0_wiph=d0["wiph"], real=d0["real"], s0_dt_next=d0["dt_next"],
+            sN_prim=dn["prim"], sN_cons=dn["cons"], sN_piph=dn["piph"], sN_dphi=dn["dphi"],
+            sN_wiph=dn["wiph"], dt=dn["dt"], sN_dt_next=dn["dt_next"], Qrz=dn["Qrz"],
+            t=dn["meta"]["t"], fIndex=F["fIndex"], iL=F["iL"], iR=F["iR"], LRtype=F["LRtype"],
+            fgeom=F["geom"], Np=d0["Np"], r_jph=d0["r_jph"], z_kph=d0["z_kph"])
+        print(case, "cells", d0["meta"]["Ncell"], "faces", len(F["iL"]))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,196 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+Bar (north_star): face lists bit-exact; FP64 fields within 1e-12 relative L1
+of the serial CPU build after N steps.  Everything except libm calls is
+compiled to round exactly as the reference (--fmad=false, same operation
+order, order-preserving gathers), so most quantities are in fact bit-exact;
+the tolerance covers the ulp-level differences of CUDA's pow/sin/cos.
+"""
+import numpy as np
+import pytest
+
+import disco_b200 as db
+from helpers import CASES, case_disk, golden, oracle_for, rel_l1, rel_l1_cols
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12          # relative L1, FP64 fields (north_star)
+
+
+def _real(g):
+    return g["real"] == 1
+
+
+def _batch_from_golden(disk, g):
+    b = db.Batch([disk], setup=False)
+    b.set_cells(g["s0_prim"], g["s0_cons"], g["s0_piph"], g["s0_dphi"], g["s0_wiph"], g["real"])
+    return b
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_setup_matches_reference(case):
+    """Device setupCells (initial, prim2cons, cons2prim, set_wcell, boundary)
+    reproduces the reference's step-0 state on real cells bit for bit."""
+    disk, g = case_disk(case)
+    b = db.Batch([disk])
+    st = b.get_cells()
+    r = _real(g)
+    assert np.array_equal(st["prim"][r], g["s0_prim"][r])
+    assert np.array_equal(st["cons"][r], g["s0_cons"][r])
+    assert np.array_equal(st["wiph"][r], g["s0_wiph"][r])
+    assert np.array_equal(st["piph"], g["s0_piph"])
+    # ghost prim comes from the same Initial module at ghost centres
+    assert np.array_equal(st["prim"][~r], g["s0_prim"][~r])
+    dt = b.mindt()[0]
+    assert dt == g["s0_dt_next"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_steps_match_reference(case):
+    """N full RK steps from the reference's step-0 state vs the reference."""
+    disk, g = case_disk(case)
+    b = _batch_from_golden(disk, g)
+    dts = []
+    for _ in range(int(g["nsteps"])):
+        dt = b.mindt()[0]
+        dts.append(dt)
+        b.timestep(dt)
+    b.sync()
+    assert np.max(np.abs(np.array(dts) / g["dt"] - 1.0)) < TOL
+    st = b.get_cells()
+    r = _real(g)
+    for q, e in enumerate(rel_l1_cols(st["prim"][r], g["sN_prim"][r])):
+        assert e < TOL, ("prim", q, e)
+    for q, e in enumerate(rel_l1_cols(st["cons"][r], g["sN_cons"][r])):
+        assert e < TOL, ("cons", q, e)
+    assert rel_l1(st["piph"], g["sN_piph"]) < 1e-14
+    f = b.faces(0, 1, geom=True)
+    for k in ("fIndex", "iL", "iR", "LRtype"):
+        assert np.array_equal(f[k], g[k]), k
+    assert rel_l1(f["geom"], g["fgeom"]) < 1e-14
+    t, n = b.time()
+    assert n == int(g["nsteps"]) and abs(t / g["t"] - 1) < TOL
+    Q, _ = b.diagnostics()
+    assert rel_l1(Q, g["Qrz"]) < TOL
+
+
+@pytest.mark.parametrize("case", ["c0_log16", "c0_lin20"])
+def test_lockstep_one_step(case):
+    """One step from the same state: mesh quantities (wiph, piph, dphi) are
+    bit-exact; fields differ only through the libm calls of the point-mass
+    source (pow, sin, cos in planet.c:56-150)."""
+    disk, g = case_disk(case)
+    o = oracle_for(disk)
+    o.set_cells(g["s0_prim"], g["s0_cons"], g["s0_piph"], g["s0_dphi"], g["s0_wiph"], g["real"])
+    b = _batch_from_golden(disk, g)
+    dt = o.mindt()
+    assert b.mindt()[0] == dt
+    o.timestep(dt)
+    b.timestep(dt)
+    so, sg = o.get_cells(), b.get_cells()
+    r = _real(g)
+    assert np.array_equal(sg["piph"], so["piph"])
+    assert np.array_equal(sg["dphi"], so["dphi"])
+    assert np.array_equal(sg["wiph"], so["wiph"])
+    # only the planet source goes through libm (pow, sin, cos)
+    for q, e in enumerate(rel_l1_cols(sg["prim"][r], so["prim"][r])):
+        assert e < 1e-14, (q, e)
+
+
+def test_config0_full_100_steps():
+    """Config 0 (Nr=128 log r in [0.5,3], Np=452, 57,856 cells), 100 steps:
+    GPU vs the CPU oracle (bit-pinned to the reference)."""
+    par, opt = db.template_paths("c0_kepler2d")
+    disk = db.Disk.from_files(par, opt)
+    b = db.Batch([disk])
+    st0 = b.get_cells()
+    o = oracle_for(disk)
+    o.set_cells(st0["prim"], st0["cons"], st0["piph"], st0["dphi"], st0["wiph"], disk.real)
+    nsteps = 100
+    dto = []
+    for _ in range(nsteps):
+        dt = o.mindt()
+        dto.append(dt)
+        o.timestep(dt)
+    b.run(nsteps)
+    b.sync()
+    sg, so = b.get_cells(), o.get_cells()
+    r = disk.real == 1
+    ep = rel_l1_cols(sg["prim"][r], so["prim"][r])
+    ec = rel_l1_cols(sg["cons"][r], so["cons"][r])
+    assert max(ep) < TOL and max(ec) < TOL, (ep, ec)
+    fo, fg = o.faces(1), b.faces(0, 1)
+    for k in ("fIndex", "iL", "iR", "LRtype"):
+        assert np.array_equal(fg[k], fo[k]), k
+    t, n = b.time()
+    assert n == nsteps and abs(t / o.time() - 1) < TOL
+    # total mass drift vs the oracle
+    m_g, m_o = sg["cons"][r, 0].sum(), so["cons"][r, 0].sum()
+    assert abs(m_g / m_o - 1) < TOL
+
+
+def test_batch_of_ragged_disks_matches_single_runs():
+    """Disks of different Nr/Np/params in one batch advance exactly as each
+    would alone (config-2 style ragged batch)."""
+    disks, golds = zip(*[case_disk(c) for c in CASES])
+    b = db.Batch(list(disks), setup=False)
+    b.set_cells(np.concatenate([g["s0_prim"] for g in golds]),
+                np.concatenate([g["s0_cons"] for g in golds]),
+                np.concatenate([g["s0_piph"] for g in golds]),
+                np.concatenate([g["s0_dphi"] for g in golds]),
+                np.concatenate([g["s0_wiph"] for g in golds]),
+                np.concatenate([g["real"] for g in golds]))
+    singles = []
+    for d, g in zip(disks, golds):
+        s = _batch_from_golden(d, g)
+        s.run(5)
+        singles.append(s.get_cells())
+    b.run(5)
+    sb = b.get_cells()
+    for i, s in enumerate(singles):
+        lo, hi = b.offsets[i], b.offsets[i + 1]
+        assert np.array_equal(sb["prim"][lo:hi], s["prim"]), i
+        assert np.array_equal(sb["piph"][lo:hi], s["piph"]), i
+        assert b.time(i)[1] == 5
+
+
+def test_graph_replay_equals_eager_steps():
+    disk, g = case_disk("c0_lin20")
+    a = _batch_from_golden(disk, g)
+    c = _batch_from_golden(disk, g)
+    for _ in range(7):
+        a.timestep(None)          # dt left on the device by the previous mindt
+    a.sync()
+    c.mindt()
+    c.run(7)
+    c.sync()
+    sa, sc = a.get_cells(), c.get_cells()
+    for k in ("prim", "cons", "piph", "dphi", "wiph"):
+        assert np.array_equal(sa[k], sc[k]), k
+
+
+def test_nonfinite_piph_reports_error_status():
+    """A poisoned cell (piph = inf, injected on the host) makes the bounded
+    phi-wrap loops give up and report DISCO_ERR_PHI_WRAP instead of hanging
+    (the reference's unbounded loops spin forever, misc.c:22-23)."""
+    disk, g = case_disk("c0_log16")
+    piph = g["s0_piph"].copy()
+    piph[200] = np.inf
+    b = db.Batch([disk], setup=False)
+    b.set_cells(g["s0_prim"], g["s0_cons"], piph, g["s0_dphi"], g["s0_wiph"], g["real"])
+    b.timestep(np.array([0.01]))
+    assert b.last_error() in (4, 5)
+    # the context stays usable: a clean state steps without error
+    b.set_cells(g["s0_prim"], g["s0_cons"], g["s0_piph"], g["s0_dphi"], g["s0_wiph"], g["real"])
+    b.timestep(np.array([0.01]))
+    assert b.last_error() == 0
+
+
+def test_kernel_times_cover_the_step():
+    disk, g = case_disk("c0_lin20")
+    b = _batch_from_golden(disk, g)
+    kt = b.kernel_times()
+    names = [k for k, _ in kt]
+    for k in ("k_begin", "k_I0", "k_faces", "k_gradr", "k_flux_r", "k_flux_p", "k_update"):
+        assert names.count(k) == 2, k
+    assert all(ms >= 0 for _, ms in kt)
