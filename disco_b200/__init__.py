@@ -107,6 +107,7 @@ def library():
         "disco_batch_last_error": (_I, [_P]),
         "disco_batch_kernel_times": (_I, [_P, C.POINTER(C.c_float), C.POINTER(C.c_char_p), _I, _IP]),
         "disco_batch_set_stream": (_I, [_P, _P]),
+        "disco_batch_debug_get": (_I, [_P, _I, _D]),
         "disco_read_par": (_I, [C.c_char_p, C.POINTER(Params), _IP]),
         "disco_read_opt": (_I, [C.c_char_p, C.POINTER(Modules)]),
         "disco_setup_grid": (_I, [C.POINTER(Params), _IP, _IP, _IP, _IP, _D, _D]),
@@ -274,6 +275,12 @@ class Batch:
         _check(library().disco_batch_kernel_times(self.h, ms, names, cap, C.byref(n)),
                "disco_batch_kernel_times")
         return [(names[i].decode(), float(ms[i])) for i in range(n.value)]
+
+    def debug_array(self, which):
+        """Internal per-cell array after the last step: 0 gradp, 1 gradr, 2 RKcons."""
+        out = np.zeros((self.ncell, self.q))
+        _check(library().disco_batch_debug_get(self.h, which, dptr(out)), "disco_batch_debug_get")
+        return out
 
     def last_error(self):
         return library().disco_batch_last_error(self.h)

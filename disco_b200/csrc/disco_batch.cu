@@ -110,6 +110,7 @@ static void fill_disk_params(DiskParams &D, const disco_params &p, const disco_m
    D.ic.mach = p.Disk_Mach; D.ic.amp = p.initPar[1];
    D.ic.rmin = p.rmin; D.ic.rmax = p.rmax; D.ic.phimax = p.phimax;
    D.ic.seed = (uint64_t)(int64_t)p.initPar0;
+   D.ic.kind = (int)p.initPar[2];
 }
 
 static void init_planets(DiskState &S, DiskParams &D, const disco_params &p, const disco_modules &m){
@@ -294,18 +295,26 @@ extern "C" int disco_batch_sizes(const disco_batch *b, int64_t *ncell, int64_t *
    return DISCO_OK;
 }
 
+/* Host <-> device copy ordered on the batch's stream (which may be a
+ * non-blocking stream of the caller), completed before returning. */
+static cudaError_t xfer(const disco_batch *b, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind){
+   cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, b->stream);
+   if( e != cudaSuccess ) return e;
+   return cudaStreamSynchronize(b->stream);
+}
+
 /* cell-major (Q per cell) host <-> SoA device */
 static int upload_q(disco_batch *b, double *dst, const double *src){
    size_t N = b->ncell; int Q = b->Q;
    std::vector<double> t((size_t)Q*N);
    for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<Q ; ++q ) t[q*N + c] = src[c*Q + q];
-   CK(cudaMemcpy(dst, t.data(), t.size()*sizeof(double), cudaMemcpyHostToDevice));
+   CK(xfer(b, dst, t.data(), t.size()*sizeof(double), cudaMemcpyHostToDevice));
    return DISCO_OK;
 }
 static int download_q(disco_batch *b, double *dst, const double *src){
    size_t N = b->ncell; int Q = b->Q;
    std::vector<double> t((size_t)Q*N);
-   CK(cudaMemcpy(t.data(), src, t.size()*sizeof(double), cudaMemcpyDeviceToHost));
+   CK(xfer(b, t.data(), src, t.size()*sizeof(double), cudaMemcpyDeviceToHost));
    for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<Q ; ++q ) dst[c*Q + q] = t[q*N + c];
    return DISCO_OK;
 }
@@ -337,9 +346,9 @@ extern "C" int disco_batch_set_cells(disco_batch *b, const double *prim, const d
    int s;
    if( prim && (s = upload_q(b, b->v.prim, prim)) ) return s;
    if( cons && (s = upload_q(b, b->v.cons, cons)) ) return s;
-   CK(cudaMemcpy(b->v.piph, piph, N*sizeof(double), cudaMemcpyHostToDevice));
-   CK(cudaMemcpy(b->v.dphi, dphi, N*sizeof(double), cudaMemcpyHostToDevice));
-   if( wiph ) CK(cudaMemcpy(b->v.wiph, wiph, N*sizeof(double), cudaMemcpyHostToDevice));
+   CK(xfer(b, b->v.piph, piph, N*sizeof(double), cudaMemcpyHostToDevice));
+   CK(xfer(b, b->v.dphi, dphi, N*sizeof(double), cudaMemcpyHostToDevice));
+   if( wiph ) CK(xfer(b, b->v.wiph, wiph, N*sizeof(double), cudaMemcpyHostToDevice));
    if( prim && !cons ){
       launch_prim2cons<6,5>(b);
       CK(cudaGetLastError());
@@ -359,9 +368,9 @@ extern "C" int disco_batch_get_cells(disco_batch *b, double *prim, double *cons,
    int s;
    if( prim && (s = download_q(b, prim, b->v.prim)) ) return s;
    if( cons && (s = download_q(b, cons, b->v.cons)) ) return s;
-   if( piph ) CK(cudaMemcpy(piph, b->v.piph, N*sizeof(double), cudaMemcpyDeviceToHost));
-   if( dphi ) CK(cudaMemcpy(dphi, b->v.dphi, N*sizeof(double), cudaMemcpyDeviceToHost));
-   if( wiph ) CK(cudaMemcpy(wiph, b->v.wiph, N*sizeof(double), cudaMemcpyDeviceToHost));
+   if( piph ) CK(xfer(b, piph, b->v.piph, N*sizeof(double), cudaMemcpyDeviceToHost));
+   if( dphi ) CK(xfer(b, dphi, b->v.dphi, N*sizeof(double), cudaMemcpyDeviceToHost));
+   if( wiph ) CK(xfer(b, wiph, b->v.wiph, N*sizeof(double), cudaMemcpyDeviceToHost));
    return DISCO_OK;
 }
 
@@ -392,10 +401,10 @@ extern "C" int disco_batch_setup_cells(disco_batch *b){
 
 static int read_err(disco_batch *b){
    int e = 0;
-   if( cudaMemcpy(&e, b->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ) return DISCO_ERR_CUDA;
+   if( xfer(b, &e, b->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ) return DISCO_ERR_CUDA;
    if( e ){
       int z = 0;
-      cudaMemcpy(b->d_err, &z, sizeof(int), cudaMemcpyHostToDevice);
+      xfer(b, b->d_err, &z, sizeof(int), cudaMemcpyHostToDevice);
    }
    if( e & ERRF_WRAP ) return DISCO_ERR_PHI_WRAP;
    if( e & ERRF_NONFINITE ) return DISCO_ERR_NONFINITE;
@@ -411,7 +420,7 @@ extern "C" int disco_batch_mindt(disco_batch *b, double *dt){
    CK(cudaStreamSynchronize(b->stream));
    if( dt ){
       std::vector<DiskState> st(b->ndisk);
-      CK(cudaMemcpy(st.data(), b->v.ds, sizeof(DiskState)*b->ndisk, cudaMemcpyDeviceToHost));
+      CK(xfer(b, st.data(), b->v.ds, sizeof(DiskState)*b->ndisk, cudaMemcpyDeviceToHost));
       for( int d=0 ; d<b->ndisk ; ++d ) dt[d] = st[d].dt_next;
    }
    return read_err(b);
@@ -461,9 +470,9 @@ extern "C" int disco_batch_timestep(disco_batch *b, const double *dt){
    CK(cudaSetDevice(b->device));
    if( dt ){
       std::vector<DiskState> st(b->ndisk);
-      CK(cudaMemcpy(st.data(), b->v.ds, sizeof(DiskState)*b->ndisk, cudaMemcpyDeviceToHost));
+      CK(xfer(b, st.data(), b->v.ds, sizeof(DiskState)*b->ndisk, cudaMemcpyDeviceToHost));
       for( int d=0 ; d<b->ndisk ; ++d ) st[d].dt_next = dt[d];
-      CK(cudaMemcpy(b->v.ds, st.data(), sizeof(DiskState)*b->ndisk, cudaMemcpyHostToDevice));
+      CK(xfer(b, b->v.ds, st.data(), sizeof(DiskState)*b->ndisk, cudaMemcpyHostToDevice));
    }
    launch_step(b, 1);
    CK(cudaGetLastError());
@@ -492,7 +501,7 @@ extern "C" int disco_batch_time(const disco_batch *b, int disk, double *t, int *
    CK(cudaSetDevice(b->device));
    CK(cudaStreamSynchronize(b->stream));
    DiskState st;
-   CK(cudaMemcpy(&st, b->v.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
+   CK(xfer(b, &st, b->v.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
    if( t ) *t = st.t;
    if( count ) *count = st.count_steps;
    return DISCO_OK;
@@ -517,9 +526,9 @@ extern "C" int disco_batch_get_faces(disco_batch *b, int disk, int dim, int *nfa
    std::vector<int> tl(nf), tr(nf);
    std::vector<unsigned char> tlr(nf);
    if( iL || iR || LRtype ){
-      CK(cudaMemcpy(tl.data(), v.fL + f0, nf*sizeof(int), cudaMemcpyDeviceToHost));
-      CK(cudaMemcpy(tr.data(), v.fR + f0, nf*sizeof(int), cudaMemcpyDeviceToHost));
-      CK(cudaMemcpy(tlr.data(), v.fLR + f0, nf, cudaMemcpyDeviceToHost));
+      CK(xfer(b, tl.data(), v.fL + f0, nf*sizeof(int), cudaMemcpyDeviceToHost));
+      CK(xfer(b, tr.data(), v.fR + f0, nf*sizeof(int), cudaMemcpyDeviceToHost));
+      CK(xfer(b, tlr.data(), v.fLR + f0, nf, cudaMemcpyDeviceToHost));
       for( int n=0 ; n<nf ; ++n ){
          if( iL ) iL[n] = tl[n] - D.cell0;
          if( iR ) iR[n] = tr[n] - D.cell0;
@@ -528,9 +537,9 @@ extern "C" int disco_batch_get_faces(disco_batch *b, int disk, int dim, int *nfa
    }
    if( geom ){
       std::vector<double> phic(nf), dA(nf), dp(nf);
-      CK(cudaMemcpy(phic.data(), v.fphic + f0, nf*sizeof(double), cudaMemcpyDeviceToHost));
-      CK(cudaMemcpy(dA.data(), v.fdA + f0, nf*sizeof(double), cudaMemcpyDeviceToHost));
-      CK(cudaMemcpy(dp.data(), v.fdp + f0, nf*sizeof(double), cudaMemcpyDeviceToHost));
+      CK(xfer(b, phic.data(), v.fphic + f0, nf*sizeof(double), cudaMemcpyDeviceToHost));
+      CK(xfer(b, dA.data(), v.fdA + f0, nf*sizeof(double), cudaMemcpyDeviceToHost));
+      CK(xfer(b, dp.data(), v.fdp + f0, nf*sizeof(double), cudaMemcpyDeviceToHost));
       const double *rj = b->rj.data() + D.rj0 + 1;
       const double *zk = b->zk.data() + D.zk0 + 1;
       for( int t=0 ; t<nt ; ++t ){
@@ -554,10 +563,10 @@ extern "C" int disco_batch_get_diagnostics(disco_batch *b, int disk, double *Qrz
    if( nq ) *nq = b->nq;
    const DiskParams &D = b->dparams[disk];
    int na = b->disk_Nr[disk]*b->disk_Nz[disk];
-   if( Qrz && b->nq ) CK(cudaMemcpy(Qrz, b->d_Qrz + (size_t)D.ann0*5, sizeof(double)*na*5, cudaMemcpyDeviceToHost));
+   if( Qrz && b->nq ) CK(xfer(b, Qrz, b->d_Qrz + (size_t)D.ann0*5, sizeof(double)*na*5, cudaMemcpyDeviceToHost));
    if( t_avg ){
       DiskState st;
-      CK(cudaMemcpy(&st, b->v.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
+      CK(xfer(b, &st, b->v.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
       *t_avg = st.t_avg;
    }
    return DISCO_OK;
@@ -569,6 +578,16 @@ extern "C" int disco_batch_last_error(disco_batch *b){
    cudaError_t e = cudaStreamSynchronize(b->stream);
    if( e != cudaSuccess ) return DISCO_ERR_CUDA;
    return read_err(b);
+}
+
+extern "C" int disco_batch_debug_get(disco_batch *b, int which, double *out){
+   if( !b || !out ) return DISCO_ERR_ARG;
+   CK(cudaSetDevice(b->device));
+   const double *src = which == 0 ? b->v.gradp : which == 1 ? b->v.gradr :
+                       which == 2 ? b->v.RKcons : NULL;
+   if( !src ) return DISCO_ERR_ARG;
+   CK(cudaStreamSynchronize(b->stream));
+   return download_q(b, out, src);
 }
 
 extern "C" int disco_batch_set_stream(disco_batch *b, void *stream){

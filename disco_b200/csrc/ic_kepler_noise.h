@@ -14,6 +14,12 @@
  *   P     = Sigma * (v_phi / Mach)^2 ,  v_phi = r^-1/2
  *   X     = 4 (phi/Pmax)(1 - phi/Pmax)          (passive scalar, NUM_N>0)
  *
+ * With Init_Par2 = 1 the disk instead rotates rigidly (Omega = 1) and is
+ * held by pressure, P = 1/Mach^2 + r^2/2, with no gravity needed: run with
+ * PLANETS = none and Energy_Omega 0, a step then calls no libm function
+ * whose value matters, which makes a CPU and a GPU build comparable bit for
+ * bit.
+ *
  * Noise is applied only inside [rmin, rmax]: ghost annuli lie outside, so
  * their boundary values stay a smooth function of x and cannot flip a hash
  * bucket when a ghost cell's phi differs by an ulp between two builds.
@@ -45,6 +51,8 @@ typedef struct {
    double rmin, rmax;
    double phimax;
    uint64_t seed;
+   int kind;          /* Init_Par2: 0 Keplerian, 1 rigid rotation held by pressure */
+   int pad;
 } disco_ic_kepler_noise;
 
 /* splitmix64 finaliser (Steele, Lea & Flood 2014). */
@@ -76,12 +84,21 @@ DISCO_HD void disco_ic_kepler_noise_eval(const disco_ic_kepler_noise *p,
    double sig = 1.0;
    if( r >= p->rmin && r <= p->rmax && p->amp != 0.0 )
       sig = 1.0 * (1.0 + p->amp * disco_hash_unit(p->seed, r, phi, p->phimax));
-   double sr = sqrt(r);
-   double omega = 1.0 / (r * sr);
-   double vphi = 1.0 / sr;
-   double cs = vphi / p->mach;
+   double omega, press;
+   if( p->kind == 1 ){
+      /* rigid rotation Omega = 1 balanced by a pressure gradient,
+       * dP/dr = rho Omega^2 r with rho = 1: P = 1/Mach^2 + r^2/2 (no gravity) */
+      omega = 1.0;
+      press = 1.0 / (p->mach * p->mach) + 0.5 * r * r;
+   }else{
+      double sr = sqrt(r);
+      double vphi = 1.0 / sr;
+      double cs = vphi / p->mach;
+      omega = 1.0 / (r * sr);
+      press = sig * cs * cs;
+   }
    prim[0] = sig;
-   prim[1] = sig * cs * cs;
+   prim[1] = press;
    prim[2] = 0.0;
    prim[3] = omega;
    prim[4] = 0.0;

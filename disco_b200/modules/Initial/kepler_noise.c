@@ -20,6 +20,7 @@ void setICparams( struct domain * theDomain ){
    icp.rmax   = theDomain->theParList.rmax;
    icp.phimax = theDomain->theParList.phimax;
    icp.seed   = (uint64_t)(int64_t)theDomain->theParList.initPar0;
+   icp.kind   = (int)theDomain->theParList.initPar2;
 }
 
 void initial( double * prim , double * x ){

@@ -192,6 +192,13 @@ int disco_batch_get_diagnostics(disco_batch *b, int disk, double *Qrz, int *nq, 
 int disco_batch_last_error(disco_batch *b);
 
 /*
+ * Diagnostic read of an internal per-cell array left by the last step, cell-
+ * major Q doubles per cell: which = 0 gradp, 1 gradr (the phi and r slopes of
+ * plm_phi / plm_trans, plm.c:15-195, from the last substep), 2 RKcons.
+ */
+int disco_batch_debug_get(disco_batch *b, int which, double *out);
+
+/*
  * Launch all further work of the batch on `stream` (a cudaStream_t, passed
  * as void* so this header needs no CUDA include; NULL restores the batch's
  * own stream).  Lets a caller time the step with events on its own stream.

@@ -431,6 +431,7 @@ orc_domain *orc_create(const disco_params *p, const disco_modules *m,
    d->ic.mach = p->Disk_Mach; d->ic.amp = p->initPar[1];
    d->ic.rmin = p->rmin; d->ic.rmax = p->rmax; d->ic.phimax = p->phimax;
    d->ic.seed = (uint64_t)(int64_t)p->initPar0;
+   d->ic.kind = (int)p->initPar[2];
    return d;
 }
 

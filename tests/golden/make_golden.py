@@ -31,7 +31,10 @@ CASES = {
                                  "Init_Par0": 27}, 8),
     "c0_hll_fe_mm3": ("c0_kepler2d", {"Num_R": 10, "Riemann_Solver": 0, "Timestep": 1,
                                       "Mesh_Motion": 3, "PLM": 1.2}, 6),
-    "c0_cm2": ("c0_cm2", {"Num_R": 24, "Mass_Ratio": 1.0e-3}, 6),
+    "c0_cm2": ("c0_cm2", {"Num_R": 24, "Mass_Ratio": 1.0e-3, "Energy_Omega": 0}, 6),
+    # libm-free: rigid rotation held by pressure, no gravity, lab energy frame
+    "c0_rigid": ("c0_nograv", {"Num_R": 20, "Log_Zoning": 0, "Init_Par2": 1,
+                               "Energy_Omega": 0, "Mach_Number": 5.0}, 8),
 }
 
 

@@ -10,7 +10,7 @@ import pyoracle
 TESTS = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(TESTS, "golden")
 TEMPLATES = db.TEMPLATES
-CASES = ["c0_log16", "c0_lin20", "c0_hll_fe_mm3", "c0_cm2"]
+CASES = ["c0_log16", "c0_lin20", "c0_hll_fe_mm3", "c0_cm2", "c0_rigid"]
 
 
 def golden(case):
