@@ -196,6 +196,10 @@ class Batch:
         self.disks = list(disks)
         n = len(self.disks)
         m = self.disks[0].modules
+        key = lambda mm: tuple(getattr(mm, f) for f, _ in Modules._fields_)
+        if any(key(d.modules) != key(m) for d in self.disks):
+            # one Makefile_opt.in module selection per batch, as one Disco build has
+            raise DiscoError(1, "Batch: all disks must share one module selection")
         par = (Params * n)(*[d.params for d in self.disks])
         Nr = np.array([d.Nr for d in self.disks], np.int32)
         Nz = np.array([d.Nz for d in self.disks], np.int32)

@@ -15,6 +15,12 @@ from helpers import CASES, case_disk, golden, oracle_for, rel_l1, rel_l1_cols
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12          # relative L1, FP64 fields (north_star)
+# The golden fixtures are deliberately coarse (10-24 annuli, dt up to half an
+# inner orbit), where the few-ulp differences between CUDA's and glibc's
+# pow/sin/cos in the point-mass force are amplified fastest; the forward-Euler
+# HLL fixture reaches 4e-12 after 4 steps.  The libm-free fixture (c0_rigid) is
+# held to bit equality instead.
+CASE_TOL = {"c0_hll_fe_mm3": 1e-11}
 
 
 def _real(g):
@@ -58,22 +64,23 @@ def test_steps_match_reference(case):
     b.sync()
     if case == "c0_rigid":
         assert np.array_equal(np.array(dts), g["dt"])
-    assert np.max(np.abs(np.array(dts) / g["dt"] - 1.0)) < TOL, dts
+    tol = CASE_TOL.get(case, TOL)
+    assert np.max(np.abs(np.array(dts) / g["dt"] - 1.0)) < tol, dts
     st = b.get_cells()
     r = _real(g)
     for q, e in enumerate(rel_l1_cols(st["prim"][r], g["sN_prim"][r])):
-        assert e < TOL, ("prim", q, e)
+        assert e < tol, ("prim", q, e)
     for q, e in enumerate(rel_l1_cols(st["cons"][r], g["sN_cons"][r])):
-        assert e < TOL, ("cons", q, e)
+        assert e < tol, ("cons", q, e)
     assert rel_l1(st["piph"], g["sN_piph"]) < 1e-14
     f = b.faces(0, 1, geom=True)
     for k in ("fIndex", "iL", "iR", "LRtype"):
         assert np.array_equal(f[k], g[k]), k
     assert rel_l1(f["geom"], g["fgeom"]) < 1e-14
     t, n = b.time()
-    assert n == int(g["nsteps"]) and abs(t / g["t"] - 1) < TOL
+    assert n == int(g["nsteps"]) and abs(t / g["t"] - 1) < tol
     Q, _ = b.diagnostics()
-    assert rel_l1(Q, g["Qrz"]) < TOL
+    assert rel_l1(Q, g["Qrz"]) < tol
 
 
 @pytest.mark.parametrize("case", ["c0_log16", "c0_lin20"])
@@ -132,28 +139,38 @@ def test_config0_full_100_steps():
 
 
 def test_batch_of_ragged_disks_matches_single_runs():
-    """Disks of different Nr/Np/params in one batch advance exactly as each
-    would alone (config-2 style ragged batch)."""
-    disks, golds = zip(*[case_disk(c) for c in CASES if c != "c0_hll_fe_mm3"])
-    b = db.Batch(list(disks), setup=False)
-    b.set_cells(np.concatenate([g["s0_prim"] for g in golds]),
-                np.concatenate([g["s0_cons"] for g in golds]),
-                np.concatenate([g["s0_piph"] for g in golds]),
-                np.concatenate([g["s0_dphi"] for g in golds]),
-                np.concatenate([g["s0_wiph"] for g in golds]),
-                np.concatenate([g["real"] for g in golds]))
+    """Disks of different Nr/Np/Mach/seed (one module selection) in one batch
+    advance exactly as each would alone (config-2 style ragged batch)."""
+    import os
+    from helpers import par_with
+    _, opt = db.template_paths("c0_kepler2d")
+    specs = [{"Num_R": 20}, {"Num_R": 33, "Mach_Number": 35.0, "Init_Par0": 7},
+             {"Num_R": 26, "Log_Zoning": 0, "Mach_Number": 12.0, "Init_Par0": 11}]
+    disks = []
+    for sp in specs:
+        p = par_with(sp)
+        disks.append(db.Disk.from_files(p, opt))
+        os.unlink(p)
+    b = db.Batch(disks)
     singles = []
-    for d, g in zip(disks, golds):
-        s = _batch_from_golden(d, g)
+    for d in disks:
+        s = db.Batch([d])
         s.run(5)
         singles.append(s.get_cells())
     b.run(5)
     sb = b.get_cells()
     for i, s in enumerate(singles):
         lo, hi = b.offsets[i], b.offsets[i + 1]
-        assert np.array_equal(sb["prim"][lo:hi], s["prim"]), i
-        assert np.array_equal(sb["piph"][lo:hi], s["piph"]), i
+        for k in ("prim", "cons", "piph", "dphi", "wiph"):
+            assert np.array_equal(sb[k][lo:hi], s[k]), (i, k)
         assert b.time(i)[1] == 5
+
+
+def test_batch_rejects_mixed_module_selections():
+    d1, _ = case_disk("c0_log16")
+    d2, _ = case_disk("c0_cm2")
+    with pytest.raises(db.DiscoError):
+        db.Batch([d1, d2])
 
 
 def test_graph_replay_equals_eager_steps():
