@@ -126,6 +126,8 @@ def make_disks(workload, rank):
     from disco_b200 import workloads
     if workload == "config0":
         return [workloads.config0_disk()]
+    if workload == "ragged8":
+        return workloads.ragged_disks(8, rank=rank)
     return workloads.ragged_disks(64, rank=rank)
 
 
@@ -133,7 +135,7 @@ def reference_pars(workload, rank=0):
     from disco_b200 import workloads, template_paths
     if workload == "config0":
         return [template_paths("c0_kepler2d")[0]], False
-    _, pars = workloads.ragged_disks(64, rank=rank, keep_pars=True)
+    _, pars = workloads.ragged_disks(8 if workload == "ragged8" else 64, rank=rank, keep_pars=True)
     return pars, True
 
 
@@ -348,7 +350,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ragged64", choices=["ragged64", "config0"])
+    ap.add_argument("--workload", default="ragged64", choices=["ragged64", "ragged8", "config0"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
