@@ -1,0 +1,149 @@
+/*
+ * Drop-in replacement of Disco's timestep() and getmindt() for the serial
+ * (USE_MPI=0) build, running the step on a B200 through the disco_b200 C ABI.
+ *
+ * It is compiled inside a Disco tree (it includes the tree's paul.h and
+ * sees the Makefile's -DHYDRO=... -DNUM_C=... definitions) and replaces, at
+ * link time:
+ *     void   timestep( struct domain * , double )   timestep.c:7-45
+ *     double getmindt( struct domain * )            misc.c:39-84
+ * main.c's loop (main.c:69-83) is unchanged.  The first call uploads the
+ * domain (cells, grid, parameters) to the GPU; afterwards the state stays on
+ * the device and struct domain's cells are stale until
+ * disco_gpu_sync_to_host() copies them back (call it before report/output,
+ * e.g. at the top of possiblyOutput, domain.c:317).
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "paul.h"
+#include "disco_b200.h"
+
+static disco_batch *g_batch = NULL;
+
+static int module_id(const char *name, const char *const *names, int n){
+   int i;
+   for( i=0 ; i<n ; ++i ) if( strcmp(name, names[i]) == 0 ) return i;
+   return -1;
+}
+
+static void fill_params(const struct domain *d, disco_params *p){
+   const struct param_list *L = &d->theParList;
+   memset(p, 0, sizeof *p);
+   p->Num_R = L->Num_R; p->Num_Z = L->Num_Z; p->aspect = L->aspect;
+   p->rmin = L->rmin; p->rmax = L->rmax; p->zmin = L->zmin; p->zmax = L->zmax;
+   p->phimax = L->phimax;
+   p->NoBC_Rmin = L->NoBC_Rmin; p->NoBC_Rmax = L->NoBC_Rmax;
+   p->NoBC_Zmin = L->NoBC_Zmin; p->NoBC_Zmax = L->NoBC_Zmax;
+   p->LogZoning = L->LogZoning; p->R_Periodic = L->R_Periodic; p->Z_Periodic = L->Z_Periodic;
+   p->LogRadius = L->LogRadius;
+   p->Mesh_Motion = L->Mesh_Motion; p->Riemann_Solver = L->Riemann_Solver;
+   p->Timestep = L->Timestep;
+   p->CFL = L->CFL; p->PLM = L->PLM; p->maxDT = L->maxDT;
+   p->Density_Floor = L->Density_Floor; p->Pressure_Floor = L->Pressure_Floor;
+   p->Exact_Mesh_Omega = L->Exact_Mesh_Omega; p->Exact_Mesh_Omega_Par = L->Exact_Mesh_Omega_Par;
+   p->Energy_Omega = L->Energy_Omega; p->Energy_Omega_Par = L->Energy_Omega_Par;
+   p->RotFrame = L->RotFrame; p->RotOmega = L->RotOmega; p->RotD = L->RotD;
+   p->Adiabatic_Index = L->Adiabatic_Index; p->viscosity = L->viscosity;
+   p->visc_flag = L->visc_flag; p->alpha_flag = L->alpha_flag;
+   p->isothermal_flag = L->isothermal_flag; p->Cs2_Profile = L->Cs2_Profile; p->Cs2_Par = L->Cs2_Par;
+   p->Disk_Mach = L->Disk_Mach; p->Mass_Ratio = L->Mass_Ratio; p->grav2D = L->grav2D;
+   p->CT = L->CT;
+   p->initPar0 = L->initPar0;
+   p->initPar[1] = L->initPar1; p->initPar[2] = L->initPar2; p->initPar[3] = L->initPar3;
+   p->initPar[4] = L->initPar4; p->initPar[5] = L->initPar5; p->initPar[6] = L->initPar6;
+   p->initPar[7] = L->initPar7; p->initPar[8] = L->initPar8;
+   p->metricPar[1] = L->metricPar1; p->metricPar[2] = L->metricPar2;
+   p->metricPar[3] = L->metricPar3; p->metricPar[4] = L->metricPar4;
+   p->t_min = d->t;
+}
+
+static void fail(const char *what, int s){
+   fprintf(stderr, "disco_b200 shim: %s: %s\n", what, disco_strerror(s));
+   exit(1);
+}
+
+static void gpu_init(struct domain *d){
+   static const char *const hydros[] = {"euler", "mhd"};
+   static const char *const bcs[] = {"fixed", "zerograd", "fixed3d"};
+   static const char *const pls[] = {"none", "sun", "cm2", "binary_soft"};
+   static const char *const ics[] = {"kepler_noise", "mhd_shear_noise"};
+   disco_modules m;
+   memset(&m, 0, sizeof m);
+   m.hydro = module_id(HYDRO, hydros, 2);
+   m.boundary = module_id(BOUNDARY, bcs, 3);
+   m.planets = module_id(PLANETS, pls, 4);
+   m.initial = module_id(INITIAL, ics, 2);
+   m.analysis = strcmp(ANALYSIS, "diag_disk2d") == 0 ? DISCO_DIAG_DISK2D : DISCO_DIAG_NONE;
+   m.num_c = NUM_C; m.num_n = NUM_N; m.ct_mode = CT_MODE;
+   if( m.hydro < 0 || m.boundary < 0 || m.planets < 0 || m.initial < 0 )
+      fail("module selection", DISCO_ERR_UNSUPPORTED);
+   disco_params p;
+   fill_params(d, &p);
+   int Nr = d->Nr, Nz = d->Nz, jk, i, q;
+   int Ng[4] = {d->NgRa, d->NgRb, d->NgZa, d->NgZb};
+   int s = disco_batch_create(0, &m, DISCO_PREC_FP64, 1, &p, &Nr, &Nz, Ng, d->Np,
+                              d->r_jph - 1, d->z_kph - 1, &g_batch);
+   if( s ) fail("disco_batch_create", s);
+   int64_t ncell;
+   disco_batch_sizes(g_batch, &ncell, NULL, NULL);
+   double *prim = malloc(sizeof(double)*NUM_Q*ncell), *cons = malloc(sizeof(double)*NUM_Q*ncell);
+   double *piph = malloc(sizeof(double)*ncell), *dphi = malloc(sizeof(double)*ncell);
+   double *wiph = malloc(sizeof(double)*ncell);
+   int *real = malloc(sizeof(int)*ncell);
+   int64_t n = 0;
+   for( jk=0 ; jk<Nr*Nz ; ++jk ) for( i=0 ; i<d->Np[jk] ; ++i, ++n ){
+      struct cell *c = &d->theCells[jk][i];
+      for( q=0 ; q<NUM_Q ; ++q ){ prim[NUM_Q*n+q] = c->prim[q]; cons[NUM_Q*n+q] = c->cons[q]; }
+      piph[n] = c->piph; dphi[n] = c->dphi; wiph[n] = c->wiph; real[n] = c->real;
+   }
+   s = disco_batch_set_cells(g_batch, prim, cons, piph, dphi, wiph, real, NULL);
+   free(prim); free(cons); free(piph); free(dphi); free(wiph); free(real);
+   if( s ) fail("disco_batch_set_cells", s);
+}
+
+/* getmindt replacement (misc.c:39-84): the device min-reduction. */
+double getmindt( struct domain * theDomain ){
+   if( !g_batch ) gpu_init(theDomain);
+   double dt = 0.0;
+   int s = disco_batch_mindt(g_batch, &dt);
+   if( s ) fail("disco_batch_mindt", s);
+   return dt;
+}
+
+/* timestep replacement (timestep.c:7-45). */
+void timestep( struct domain * theDomain , double dt ){
+   if( !g_batch ) gpu_init(theDomain);
+   int s = disco_batch_timestep(g_batch, &dt);
+   if( s ) fail("disco_batch_timestep", s);
+   theDomain->t += dt;
+   theDomain->count_steps += 1;
+}
+
+/* Copy the device state back into struct domain's cells (before output). */
+void disco_gpu_sync_to_host( struct domain * theDomain ){
+   if( !g_batch ) return;
+   int64_t ncell;
+   disco_batch_sizes(g_batch, &ncell, NULL, NULL);
+   double *prim = malloc(sizeof(double)*NUM_Q*ncell), *cons = malloc(sizeof(double)*NUM_Q*ncell);
+   double *piph = malloc(sizeof(double)*ncell), *dphi = malloc(sizeof(double)*ncell);
+   double *wiph = malloc(sizeof(double)*ncell);
+   int s = disco_batch_get_cells(g_batch, prim, cons, piph, dphi, wiph, NULL);
+   if( s ) fail("disco_batch_get_cells", s);
+   s = disco_batch_last_error(g_batch);
+   if( s ) fail("device step", s);
+   int jk, i, q;
+   int64_t n = 0;
+   for( jk=0 ; jk<theDomain->Nr*theDomain->Nz ; ++jk ) for( i=0 ; i<theDomain->Np[jk] ; ++i, ++n ){
+      struct cell *c = &theDomain->theCells[jk][i];
+      for( q=0 ; q<NUM_Q ; ++q ){ c->prim[q] = prim[NUM_Q*n+q]; c->cons[q] = cons[NUM_Q*n+q]; }
+      c->piph = piph[n]; c->dphi = dphi[n]; c->wiph = wiph[n];
+   }
+   free(prim); free(cons); free(piph); free(dphi); free(wiph);
+   /* time-averaged diagnostics accumulated on the device (analysis.c:52-107) */
+   int nq = 0;
+   double tavg = 0.0;
+   if( theDomain->num_tools > 0 &&
+       disco_batch_get_diagnostics(g_batch, 0, theDomain->theTools.Qrz, &nq, &tavg) == DISCO_OK )
+      theDomain->theTools.t_avg = tavg;
+}

@@ -32,6 +32,9 @@ double getmindt( struct domain * );
 int read_par_file( struct domain * );
 void setup_faces( struct domain * , int );
 void freeDomain( struct domain * );
+/* Present only when this driver is linked with the GPU drop-in
+ * (disco_b200/shim): copies the device state back into the cells. */
+void disco_gpu_sync_to_host( struct domain * ) __attribute__((weak));
 
 static double wall(void){
    struct timeval tv; gettimeofday(&tv, NULL);
@@ -146,6 +149,7 @@ int main(int argc, char *argv[]){
       return 0;
    }
    if( !dumpdir ) return 0;
+   if( disco_gpu_sync_to_host ) disco_gpu_sync_to_host( &theDomain );
 
    int Q = NUM_Q;
    double *prim = malloc(sizeof(double)*Q*(size_t)Ncell);

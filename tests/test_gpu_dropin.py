@@ -1,0 +1,67 @@
+"""The drop-in: the reference's own host code (read_par_file, setupGrid,
+setupDomain, setupCells, boundary_trans -- everything but timestep() and
+getmindt()) linked with disco_b200/shim, i.e. exactly the link-time
+substitution of INTEGRATION.md, against the unmodified reference binary.
+
+Both binaries are built from the reference sources by oracle/Makefile
+(targets disco_ref and hybrid) wherever the reference tree is available."""
+import os
+import shutil
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import pyoracle
+from helpers import GOLDEN, rel_l1_cols
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(binary, par, nsteps):
+    work = tempfile.mkdtemp(prefix="dropin_")
+    try:
+        shutil.copy(par, os.path.join(work, "in.par"))
+        dump = os.path.join(work, "dump")
+        subprocess.run([binary, work, str(nsteps), dump], check=True,
+                       stdout=subprocess.DEVNULL, timeout=600)
+        return pyoracle.load_dump(dump)
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def _binaries(cfg):
+    ref = pyoracle.ref_binary(cfg)
+    hyb = os.path.join(os.path.dirname(ref), "disco_hybrid")
+    if not (os.path.exists(ref) and os.path.exists(hyb)):
+        pytest.skip("reference / hybrid binaries for %s not built" % cfg)
+    return ref, hyb
+
+
+def test_dropin_bitexact_libm_free():
+    ref, hyb = _binaries("c0_nograv")
+    par = os.path.join(GOLDEN, "c0_rigid.par")
+    a, b = _run(ref, par, 10), _run(hyb, par, 10)
+    assert np.array_equal(a["dt"], b["dt"])
+    for k in ("prim", "piph", "dphi", "wiph"):
+        assert np.array_equal(a[k], b[k]), k
+    r = a["real"] == 1
+    assert np.array_equal(a["cons"][r], b["cons"][r])
+    for k in ("iL", "iR", "LRtype"):
+        assert np.array_equal(a["faces_1"][k], b["faces_1"][k]), k
+    assert a["dt_next"] == b["dt_next"]
+
+
+def test_dropin_config0_20_steps():
+    ref, hyb = _binaries("c0_kepler2d")
+    import disco_b200 as db
+    par, _ = db.template_paths("c0_kepler2d")
+    a, b = _run(ref, par, 20), _run(hyb, par, 20)
+    assert np.max(np.abs(b["dt"] / a["dt"] - 1)) < 1e-12
+    r = a["real"] == 1
+    assert max(rel_l1_cols(b["prim"][r], a["prim"][r])) < 1e-12
+    assert max(rel_l1_cols(b["cons"][r], a["cons"][r])) < 1e-12
+    for k in ("iL", "iR", "LRtype"):
+        assert np.array_equal(a["faces_1"][k], b["faces_1"][k]), k
+    assert np.max(np.abs(b["Qrz"] - a["Qrz"])) <= 1e-12 * np.max(np.abs(a["Qrz"]))
