@@ -213,6 +213,33 @@ int disco_batch_set_stream(disco_batch *b, void *stream);
  */
 int disco_batch_kernel_times(disco_batch *b, float *ms, const char **names, int cap, int *nlaunch);
 
+/*
+ * getmindt for one disk whose state the caller already keeps in device
+ * memory, computed without allocating any device memory.  No counterpart in
+ * the reference: it exists for callers that may not call cudaMalloc (a host
+ * code that owns all device memory through its own pool, or a loop that runs
+ * while allocation is forbidden), since disco_batch_mindt needs a batch and
+ * creating a batch allocates.
+ *
+ * Inputs: the disk's params, hydro module (DISCO_HYDRO_EULER only), grid as
+ * for disco_batch_create (host arrays: Ng[4], Np[Nr*Nz], r_jph[Nr+1],
+ * z_kph[Nz+1]) and device pointers to its cells in annulus order: prim as
+ * structure-of-arrays (prim[q*ncell + c], q < 6), piph, dphi, wiph.  Work is
+ * issued on `stream` (a cudaStream_t; NULL = default stream) and *dt (host)
+ * receives CFL * min over real cells, the reference's getmindt value.
+ *
+ * Limits: Nr*Nz <= 65536 annuli, Nr+1 and Nz+1 <= 8192, ncell <= 2^26;
+ * larger grids return DISCO_ERR_ARG.  Working memory is one static device
+ * array of about 3.2 MiB that every GPU using the library holds until exit.
+ * The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress); make it before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race and must be serialised.
+ */
+int disco_mindt_noalloc(const disco_params *p, int hydro, int Nr, int Nz,
+                        const int *Ng, const int *Np, const double *r_jph,
+                        const double *z_kph, const double *prim, const double *piph,
+                        const double *dphi, const double *wiph, void *stream, double *dt);
+
 #ifdef __cplusplus
 }
 #endif
