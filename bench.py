@@ -49,6 +49,9 @@ def kernel_bytes(name, first, N, Nf, Na):
     w = 8
     if name == "k_begin":
         return N * w * ((5 * Q + 4) if first else (5 * Q + 1))
+    if name == "k_c2p":
+        # reads cons, piph, dphi (+wiph on the last substep); writes prim
+        return N * w * (2 * Q + 2) + (N * w if not first else 0)
     if name == "k_I0":
         return N * w + Na * 4
     if name == "k_faces":
@@ -60,7 +63,9 @@ def kernel_bytes(name, first, N, Nf, Na):
     if name == "k_flux_p":
         return N * w * (3 * Q + 2)
     if name == "k_update":
-        return N * w * (5 * Q + (6 if first else 3)) + N * 8 + Nf * w * Q
+        # reads cons, prim, phi fluxes, piph, dphi, consL/consR, r-face fluxes;
+        # writes cons (+ reads piph_new, writes piph and dphi in the first substep)
+        return N * w * (4 * Q + (5 if first else 2)) + N * 8 + Nf * w * Q
     return 0
 
 

@@ -63,6 +63,8 @@ static int cuda_status(cudaError_t e){
    fprintf(stderr, "disco_b200: %s failed: %s (%s:%d)\n", #x, cudaGetErrorString(_e), __FILE__, __LINE__); \
    return DISCO_ERR_CUDA; } }while(0)
 
+static unsigned nblk(size_t n, unsigned t);
+
 template<class T>
 static T *dalloc(disco_batch *b, size_t n){
    void *p = NULL;
@@ -265,12 +267,18 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.fphic = dalloc<double>(b, face); v.fdA = dalloc<double>(b, face); v.fdp = dalloc<double>(b, face);
    v.fS = dalloc<double>(b, (size_t)b->Q*face); v.fG = dalloc<double>(b, (size_t)b->Q*face);
    v.diag_part = dalloc<double>(b, b->cblk.size()*6);
+   v.ann_om = dalloc<double>(b, ann); v.ann_om1 = dalloc<double>(b, ann);
+   v.tr_om = dalloc<double>(b, v.Ntr);
    b->d_Qrz = dalloc<double>(b, (size_t)ann*5);
    v.err = dalloc<int>(b, 1);
    b->d_err = v.err;
    for( void *p : b->allocs ) if( !p ){ disco_batch_destroy(b); return DISCO_ERR_CUDA; }
    if( cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ){
       disco_batch_destroy(b); return DISCO_ERR_CUDA;
+   }
+   {
+      int nx = ann > v.Ntr ? ann : v.Ntr;
+      k_precompute<<<nblk(nx, 128), 128, 0, b->stream>>>(v);
    }
    if( cudaDeviceSynchronize() != cudaSuccess ){ disco_batch_destroy(b); return DISCO_ERR_CUDA; }
    *out = b;
@@ -439,7 +447,8 @@ static void launch_substep(disco_batch *b, double RK, int first, int last, doubl
    k_gradr<6><<<ncb, CB, 0, s>>>(v);                                  mark(b, "k_gradr");
    k_flux_r<6,5><<<nfb, FB, 0, s>>>(v);                               mark(b, "k_flux_r");
    k_flux_p<6,5><<<ncb, CB, 0, s>>>(v);                               mark(b, "k_flux_p");
-   k_update<6,5><<<ncb, CB, 0, s>>>(v, first, last, b->bc_fixed);     mark(b, "k_update");
+   k_update<6,5,1><<<ncb, CB, 0, s>>>(v, first);                      mark(b, "k_update");
+   k_c2p<6,5><<<ncb, CB, 0, s>>>(v, last, b->bc_fixed);               mark(b, "k_c2p");
 }
 
 /* timestep() (timestep.c:7-45). */

@@ -44,6 +44,10 @@ struct View {
    int *consL, *consR;
    double *Gp;
    double *diag_part;   /* per cell block: nq sums + volume */
+   /* energy-frame Omega of omega.c:62-110, evaluated once by k_precompute at
+    * the radii the step uses (same device expressions, so bit-identical to
+    * evaluating them in place): annulus centroid (om, dOm/dr) and r-face */
+   double *ann_om, *ann_om1, *tr_om;
    int nq;
    double dtfac;        /* 1 in the first substep, 0.5 in the second (timestep.c:39) */
    int *err;
@@ -117,6 +121,26 @@ __global__ void __launch_bounds__(CB) k_begin(View v, double RK, int first){
       if( bb*cc < 0.0 ) m = 0.0;
       if( fabs(cc) < fabs(m) ) m = cc;
       v.gradp[q*N + c] = m;
+   }
+}
+
+/* Energy-frame Omega at the radii the step evaluates it (omega.c:62-110):
+ * annulus centroids (sources, phi faces, c2p) and r-faces (trans_flux). */
+__global__ void k_precompute(View v){
+   int x = blockIdx.x*blockDim.x + threadIdx.x;
+   if( x < v.Nann ){
+      const DiskParams &P = v.dp[v.ann_disk[x]];
+      const double *rj = v.rj + P.rj0 + 1;
+      int j = v.ann_j[x];
+      double r = centroid_r(rj[j], rj[j-1]);
+      v.ann_om[x] = get_om(P, r);
+      v.ann_om1[x] = get_om1(P, r);
+   }
+   if( x < v.Ntr ){
+      const DiskParams &P = v.dp[v.ann_disk[v.tr_a[x]]];
+      const double *rj = v.rj + P.rj0 + 1;
+      int j = v.tr_j[x];
+      v.tr_om[x] = get_om(P, .5*(rj[j]+rj[j]));
    }
 }
 
@@ -384,7 +408,7 @@ __global__ void __launch_bounds__(FB) k_flux_r(View v){
    const double *rj = v.rj + P.rj0 + 1;
    double r = .5*(rj[j]+rj[j]);                 /* face cm[0] */
    double G[Q];
-   solve_riemann<Q,NC,1>(P, primL, primR, r, get_om(P, r), 0.0, dAdt, G);
+   solve_riemann<Q,NC,1>(P, primL, primR, r, v.tr_om[t], 0.0, dAdt, G);
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) v.fG[(size_t)q*v.Nf + f] = G[q];
    raise_err(v, err);
@@ -420,22 +444,119 @@ __global__ void __launch_bounds__(CB) k_flux_p(View v){
    }
    double w = r*v.wiph[cL];
    double G[Q];
-   solve_riemann<Q,NC,0>(P, primL, primR, r, get_om(P, r), w, dA*dt, G);
+   solve_riemann<Q,NC,0>(P, primL, primR, r, v.ann_om[a], w, dA*dt, G);
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) v.Gp[q*N + cL] = G[q];
 }
 
 /* ------------------------------------------------------------------ k_update
- * Everything after the fluxes, per cell, in the reference's order:
+ * The flux gather and sources, per cell, in the reference's order:
  *   flux gather  riemann.c:312-315 applied as phi_flux then trans_flux do
- *   add_source   misc.c:538-580 (euler source + planet_src), old piph
+ *                (phi faces from k_flux_p's Gp when PHI is set)
+ *   add_source   misc.c:538-580 (euler source + planet_src), pre-move cell
  *   move/clean/calc_dp   misc.c:256-288 (first substep; piph_new from k_begin)
- *   calc_prim    misc.c:290-325 (euler cons2prim)
+ * calc_prim, the boundary, and the fused getmindt / diagnostics follow in
+ * k_c2p. */
+template<int Q, int NC, int PHI>
+__global__ void __launch_bounds__(CB) k_update(View v, int first){
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   if( i >= np ) return;
+   const int N = v.Ncell;
+   int c0 = v.ann_off[a], c = c0 + i;
+   int cprev = c0 + (i == 0 ? np-1 : i-1);
+   int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+   int j = v.ann_j[a], k = v.ann_k[a];
+   bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
+   int err = 0;
+   double piph = v.piph[c], dphi = v.dphi[c];
+   if( real ){
+      const DiskState &S = v.ds[d];
+      const double *rj = v.rj + P.rj0 + 1;
+      const double *zk = v.zk + P.zk0 + 1;
+      double dt = S.dt*v.dtfac;
+      double cons[Q];
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) cons[q] = v.cons[q*N + c];
+      if( PHI ){                          /* phi faces: loop order of phi_flux */
+         if( i > 0 ){
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ){ cons[q] += v.Gp[q*N+cprev]; cons[q] -= v.Gp[q*N+c]; }
+         }else{
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ){ cons[q] -= v.Gp[q*N+c]; cons[q] += v.Gp[q*N+cprev]; }
+         }
+      }
+      /* r faces: inner track (cell is R) then outer track (cell is L) */
+      int I0 = v.I0[a];
+      int tin = P.trr0 + (j-1) + (P.Nr-1)*k;
+      int tout = P.trr0 + j + (P.Nr-1)*k;
+      Runs Rin = cell_runs(v, v.consR, tin, c0, np, i, I0);
+      Runs Rout = cell_runs(v, v.consL, tout, c0, np, i, I0);
+      const size_t Nf = v.Nf;
+#define ADD_RUN(s,e,op) for( int f=(s) ; f<=(e) ; ++f ){ \
+      _Pragma("unroll") for( int q=0 ; q<Q ; ++q ) cons[q] op v.fG[q*Nf + f]; }
+      ADD_RUN(Rin.s1, Rin.e1, +=)
+      ADD_RUN(Rin.s2, Rin.e2, +=)
+      ADD_RUN(Rout.s1, Rout.e1, -=)
+      ADD_RUN(Rout.s2, Rout.e2, -=)
+#undef ADD_RUN
+      /* add_source with the pre-move cell */
+      double prim[Q];
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) prim[q] = v.prim[q*N + c];
+      double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
+      double phim = piph - dphi;
+      double dph = get_dp(piph, phim, P.Pmax, &err);
+      double dV = dV_of(rp, rm, dph, zp, zm);
+      double dVdt = dV*dt;
+      double r = centroid_r(rp, rm);
+      {  /* euler source, euler.c:171-215 */
+         double rho = prim[RHO], Pp = prim[PPP];
+         double r_1 = .5*(rp+rm);
+         double vr = prim[URR], omega = prim[UPP], vz = prim[UZZ];
+         double centrifugal = rho*omega*omega*r;
+         if( P.polar ) centrifugal *= sin(0.5*dph) / (0.5*dph);
+         double press_bal = Pp/r_1;
+         cons[SRR] += dVdt*( centrifugal + press_bal );
+         double om = v.ann_om[a];
+         double om_r = v.ann_om1[a];
+         double om_z = 0.0;
+         cons[TAU] += dVdt*rho*( r*vr*om*om - r*r*(omega-om)*(vr*om_r + vz*om_z));
+      }
+      for( int p=0 ; p<P.npl ; ++p ){   /* planet_src, planet.c:152-196 */
+         double rho = prim[RHO], vr = prim[URR], vz = prim[UZZ], omega = prim[UPP];
+         double phi = phim + 0.5*dph;
+         double x2 = centroid_z(zp, zm);
+         double F0, F1, F2;
+         planetary_force(P.grav2D, S.pl[p], r, phi, x2, &F0, &F1, &F2);
+         double hr = 1.0, hp = r, hz = 1.0;
+         if( P.polar ){ double adj = sin(0.5*dph)/(0.5*dph); F0 *= adj; F1 *= adj; }
+         cons[SRR] += rho*hr*F0*dVdt;
+         cons[LLL] += rho*hp*F1*dVdt;
+         cons[SZZ] += rho*hz*F2*dVdt;
+         cons[TAU] += rho*( hr*F0*vr + hz*F2*vz + hp*F1*omega )*dVdt;
+      }
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) v.cons[q*N + c] = cons[q];
+   }
+   if( first ){
+      piph = v.piph_new[c];
+      dphi = get_dp(piph, v.piph_new[cprev], P.Pmax, &err);
+      v.piph[c] = piph; v.dphi[c] = dphi;
+   }
+   raise_err(v, err);
+}
+
+/* ------------------------------------------------------------------ k_c2p
+ *   calc_prim    misc.c:290-325 (euler cons2prim) on real cells
  *   boundary     Boundary/fixed.c:11-60 (r ghosts re-initialised)
  * and, on the last substep, the next step's getmindt (misc.c:39-84) and the
- * diagnostics sums of add_diagnostics (analysis.c:52-107). */
+ * per-block sums of add_diagnostics (analysis.c:52-107). */
 template<int Q, int NC>
-__global__ void __launch_bounds__(CB) k_update(View v, int first, int last, int bc_fixed){
+__global__ void __launch_bounds__(CB) k_c2p(View v, int last, int bc_fixed){
    __shared__ double s_red[CB/32][8];
    __shared__ unsigned long long s_dt[CB/32];
    int2 b = v.cblk[blockIdx.x];
@@ -446,102 +567,28 @@ __global__ void __launch_bounds__(CB) k_update(View v, int first, int last, int 
    int c0 = v.ann_off[a], c = c0 + (active ? i : 0);
    int d = v.ann_disk[a];
    const DiskParams &P = v.dp[d];
-   DiskState &S = v.ds[d];
    int j = v.ann_j[a], k = v.ann_k[a];
    const double *rj = v.rj + P.rj0 + 1;
    const double *zk = v.zk + P.zk0 + 1;
    bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
    int err = 0;
-   double dt = S.dt*v.dtfac;
    double prim[Q];
    double dtc = 1.0e300;
    double dq[6] = {0,0,0,0,0,0};
+   double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
    if( active ){
-#pragma unroll
-      for( int q=0 ; q<Q ; ++q ) prim[q] = v.prim[q*N + c];
       double piph = v.piph[c], dphi = v.dphi[c];
+      double phim = piph - dphi;
       if( real ){
          double cons[Q];
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) cons[q] = v.cons[q*N + c];
-         /* phi faces: loop order of phi_flux */
-         int cprev = c0 + (i == 0 ? np-1 : i-1);
-         if( i > 0 ){
-#pragma unroll
-            for( int q=0 ; q<Q ; ++q ){ cons[q] += v.Gp[q*N+cprev]; cons[q] -= v.Gp[q*N+c]; }
-         }else{
-#pragma unroll
-            for( int q=0 ; q<Q ; ++q ){ cons[q] -= v.Gp[q*N+c]; cons[q] += v.Gp[q*N+cprev]; }
-         }
-         /* r faces: inner track (cell is R) then outer track (cell is L) */
-         int I0 = v.I0[a];
-         int tin = P.trr0 + (j-1) + (P.Nr-1)*k;
-         int tout = P.trr0 + j + (P.Nr-1)*k;
-         Runs Rin = cell_runs(v, v.consR, tin, c0, np, i, I0);
-         Runs Rout = cell_runs(v, v.consL, tout, c0, np, i, I0);
-         const size_t Nf = v.Nf;
-#define ADD_RUN(s,e,op) for( int f=(s) ; f<=(e) ; ++f ){ \
-         _Pragma("unroll") for( int q=0 ; q<Q ; ++q ) cons[q] op v.fG[q*Nf + f]; }
-         ADD_RUN(Rin.s1, Rin.e1, +=)
-         ADD_RUN(Rin.s2, Rin.e2, +=)
-         ADD_RUN(Rout.s1, Rout.e1, -=)
-         ADD_RUN(Rout.s2, Rout.e2, -=)
-#undef ADD_RUN
-         /* add_source with the pre-move cell */
-         double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
-         double phim = piph - dphi;
-         double dph = get_dp(piph, phim, P.Pmax, &err);
-         double dV = dV_of(rp, rm, dph, zp, zm);
-         double dVdt = dV*dt;
-         {  /* euler source, euler.c:171-215 */
-            double rho = prim[RHO], Pp = prim[PPP];
-            double r = centroid_r(rp, rm);
-            double r_1 = .5*(rp+rm);
-            double vr = prim[URR], omega = prim[UPP], vz = prim[UZZ];
-            double centrifugal = rho*omega*omega*r;
-            if( P.polar ) centrifugal *= sin(0.5*dph) / (0.5*dph);
-            double press_bal = Pp/r_1;
-            cons[SRR] += dVdt*( centrifugal + press_bal );
-            double om = get_om(P, r);
-            double om_r = get_om1(P, r);
-            double om_z = 0.0;
-            cons[TAU] += dVdt*rho*( r*vr*om*om - r*r*(omega-om)*(vr*om_r + vz*om_z));
-         }
-         for( int p=0 ; p<P.npl ; ++p ){   /* planet_src, planet.c:152-196 */
-            double rho = prim[RHO], vr = prim[URR], vz = prim[UZZ], omega = prim[UPP];
-            double phi = phim + 0.5*dph;
-            double x0 = centroid_r(rp, rm), x2 = centroid_z(zp, zm);
-            double F0, F1, F2;
-            planetary_force(P.grav2D, S.pl[p], x0, phi, x2, &F0, &F1, &F2);
-            double hr = 1.0, hp = x0, hz = 1.0;
-            if( P.polar ){ double adj = sin(0.5*dph)/(0.5*dph); F0 *= adj; F1 *= adj; }
-            cons[SRR] += rho*hr*F0*dVdt;
-            cons[LLL] += rho*hp*F1*dVdt;
-            cons[SZZ] += rho*hz*F2*dVdt;
-            cons[TAU] += rho*( hr*F0*vr + hz*F2*vz + hp*F1*omega )*dVdt;
-         }
-#pragma unroll
-         for( int q=0 ; q<Q ; ++q ) v.cons[q*N + c] = cons[q];
-         if( first ){
-            piph = v.piph_new[c];
-            dphi = get_dp(piph, v.piph_new[cprev], P.Pmax, &err);
-            v.piph[c] = piph; v.dphi[c] = dphi;
-         }
-         /* calc_prim */
-         double phim2 = piph - dphi;
-         double dph2 = get_dp(piph, phim2, P.Pmax, &err);
+         double dph2 = get_dp(piph, phim, P.Pmax, &err);
          double dV2 = dV_of(rp, rm, dph2, zp, zm);
-         double r = centroid_r(rp, rm);
-         cons2prim<Q,NC>(P, cons, prim, r, get_om(P, r), dV2);
+         cons2prim<Q,NC>(P, cons, prim, centroid_r(rp, rm), v.ann_om[a], dV2);
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) v.prim[q*N + c] = prim[q];
       }else{
-         if( first ){
-            int cprev = c0 + (i == 0 ? np-1 : i-1);
-            piph = v.piph_new[c];
-            dphi = get_dp(piph, v.piph_new[cprev], P.Pmax, &err);
-            v.piph[c] = piph; v.dphi[c] = dphi;
-         }
          bool rghost = j < P.NgRa || j >= P.Nr - P.NgRb;
          if( bc_fixed && rghost ){
             double x[3] = { .5*(rj[j]+rj[j-1]), piph - .5*dphi, .5*(zk[k]+zk[k-1]) };
@@ -549,11 +596,12 @@ __global__ void __launch_bounds__(CB) k_update(View v, int first, int last, int 
             if( P.rotframe ) prim[UPP] -= P.RotOmega;       /* subtract_omega, rotframe.c:11 */
 #pragma unroll
             for( int q=0 ; q<Q ; ++q ) v.prim[q*N + c] = prim[q];
+         }else if( last ){
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ) prim[q] = v.prim[q*N + c];
          }
       }
       if( last ){
-         double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
-         double phim = piph - dphi;
          if( real ){                              /* mindt, euler.c:332-380 */
             int cprev = c0 + (i == 0 ? np-1 : i-1);
             double w = .5*(v.wiph[cprev] + v.wiph[c]);
@@ -579,7 +627,7 @@ __global__ void __launch_bounds__(CB) k_update(View v, int first, int last, int 
             double Fp = 0.0;
             if( P.npl > 1 ){
                double Fr, Fz;
-               planetary_force(P.grav2D, S.pl[1], r, phi, 0.0, &Fr, &Fp, &Fz);
+               planetary_force(P.grav2D, v.ds[d].pl[1], r, phi, 0.0, &Fr, &Fp, &Fz);
             }
             dq[0] = rho*dV;
             dq[1] = 2.*DISCO_PI*r*rho*vr*dV;
@@ -614,7 +662,7 @@ __global__ void __launch_bounds__(CB) k_update(View v, int first, int last, int 
    if( threadIdx.x == 0 ){
       unsigned long long mb = s_dt[0];
       for( int w=1 ; w<CB/32 ; ++w ) mb = s_dt[w] < mb ? s_dt[w] : mb;
-      if( real ) atomicMin(&S.dtmin, mb);
+      if( real ) atomicMin(&v.ds[d].dtmin, mb);
       if( v.nq ){
          for( int m=0 ; m<6 ; ++m ){
             double x = 0.0;
