@@ -308,6 +308,31 @@ def run_ours(args, world, rank, local):
     e2e = world * nreal * args.steps / (e2e_ms / 1e3)
     del out
 
+    # the mixed-precision form on the same disks, timed the same way
+    mixed = None
+    if not args.no_mixed:
+        bm = db.Batch(disks, device=local, precision=db.PREC_MIXED)
+        bm.set_stream(stream.cuda_stream)
+        bm.run(args.warmup)
+        bm.sync()
+        barrier()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            g0.record(stream)
+            bm.run(args.steps)
+            g1.record(stream)
+        g1.synchronize()
+        barrier()
+        if bm.last_error() != 0:
+            raise RuntimeError("device error in the mixed-form timed region")
+        mms = allmax(g0.elapsed_time(g1))
+        mv = world * nreal * args.steps / (mms / 1e3)
+        mixed = {"value": mv, "unit": "zone-updates/s", "ms_per_step": mms / args.steps,
+                 "speedup_vs_fp64": mv / value,
+                 "precision": "FP32 prim/slopes/fluxes, FP64 mesh/dt/Kahan cons"}
+        bm.close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -340,6 +365,7 @@ def run_ours(args, world, rank, local):
                     "h2d_bytes_per_step": (h2d + 8 * len(disks) * args.steps) / args.steps,
                     "d2h_bytes_per_step": (d2h + 8 * len(disks) * args.steps) / args.steps},
             "gpu_launches": launches_per_step * args.steps,
+            "mixed_form": mixed,
             "clocks": ck,
             "cpu_baseline": cpu,
         }
@@ -357,6 +383,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ragged64", choices=["ragged64", "ragged8", "config0"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -67,7 +67,10 @@ def build(force=False, verbose=False):
     objs = []
     for src in cu:
         obj = os.path.join(bdir, os.path.basename(src) + ".o")
-        _run([nvcc] + ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17",
+        # the FP64 parity path must not contract a*b+c into FMA (the reference's
+        # x86-64 build does not); the FP32 mixed form (*_mixed.cu) may
+        fmad = "--fmad=true" if src.endswith("_mixed.cu") else "--fmad=false"
+        _run([nvcc] + ARCH + ["-O3", "-lineinfo", fmad, "-std=c++17",
                               "-Xcompiler", "-fPIC", "-Xptxas", "-v"] + inc +
              ["-c", src, "-o", obj], verbose)
         objs.append(obj)

@@ -4,10 +4,14 @@
  * replaces timestep()/onestep() (timestep.c:7-45, onestep.c:84-229).
  *
  * One batch = one or more independent disks in one set of ragged SoA
- * arrays.  A step is ~16 kernels (two substeps of begin / I0 / faces /
- * gradr / flux_r / flux_p / update, plus three tiny per-disk kernels); the
+ * arrays.  A substep is begin / I0 / faces / gradr / flux_r / flux_p /
+ * update / c2p, a step two substeps plus three tiny per-disk kernels; the
  * multi-step driver captures one step in a CUDA graph and replays it with
  * dt left on the device by the previous step's fused getmindt.
+ *
+ * Two precisions share the code: DISCO_PREC_FP64 (ViewT<double>, the
+ * reference's arithmetic) and DISCO_PREC_MIXED (ViewT<float>: FP32 prim,
+ * slopes and fluxes; FP64 geometry, mesh, dt and Kahan-compensated cons).
  */
 #include <cuda_runtime.h>
 #include <stdio.h>
@@ -15,46 +19,7 @@
 #include <string.h>
 #include <vector>
 #include <algorithm>
-#include "disco_b200.h"
-#include "disco_kernels.cuh"
-
-using namespace disco;
-
-struct disco_batch {
-   int device;
-   disco_modules mods;
-   int prec;
-   int ndisk, Q, NC;
-   int timestep_mode;        /* 0 = RK2, 1 = forward Euler */
-   int bc_fixed;
-   int any_mm3;
-   int nq;
-   std::vector<disco_params> params;
-   /* topology (host) */
-   std::vector<int> ann_off, ann_np, ann_disk, ann_j, ann_k;
-   std::vector<int> tr_a, tr_b, tr_off, tr_flux, tr_j, tr_k;
-   std::vector<double> tr_dxL, tr_dxR;
-   std::vector<int2> cblk, fblk;
-   std::vector<int> ann_blk0, ann_nblk;
-   std::vector<double> rj, zk;
-   std::vector<DiskParams> dparams;
-   std::vector<int> disk_Nr, disk_Nz, disk_nreal;
-   int64_t ncell, nreal;
-   /* device */
-   View v;
-   void *dev_static;            /* one allocation for topology */
-   std::vector<void *> allocs;
-   int *d_ann_blk0, *d_ann_nblk;
-   double *d_Qrz;
-   int *d_err;
-   cudaStream_t stream;
-   cudaStream_t own_stream;
-   std::vector<cudaEvent_t> *tape;       /* non-NULL: record an event after each launch */
-   std::vector<const char *> *tape_names;
-   cudaGraphExec_t graph;
-   int have_cells;
-   int last_status;
-};
+#include "disco_batch_impl.cuh"
 
 static int cuda_status(cudaError_t e){
    return e == cudaSuccess ? DISCO_OK : DISCO_ERR_CUDA;
@@ -63,17 +28,17 @@ static int cuda_status(cudaError_t e){
    fprintf(stderr, "disco_b200: %s failed: %s (%s:%d)\n", #x, cudaGetErrorString(_e), __FILE__, __LINE__); \
    return DISCO_ERR_CUDA; } }while(0)
 
-static unsigned nblk(size_t n, unsigned t);
 
-template<class T>
-static T *dalloc(disco_batch *b, size_t n){
+static void *dalloc_bytes(disco_batch *b, size_t bytes){
    void *p = NULL;
-   if( n == 0 ) n = 1;
-   if( cudaMalloc(&p, n*sizeof(T)) != cudaSuccess ) return NULL;
-   cudaMemset(p, 0, n*sizeof(T));
+   if( bytes == 0 ) bytes = 8;
+   if( cudaMalloc(&p, bytes) != cudaSuccess ) return NULL;
+   cudaMemset(p, 0, bytes);
    b->allocs.push_back(p);
-   return (T *)p;
+   return p;
 }
+template<class T>
+static T *dalloc(disco_batch *b, size_t n){ return (T *)dalloc_bytes(b, n*sizeof(T)); }
 template<class T>
 static T *dupload(disco_batch *b, const std::vector<T> &h){
    T *p = dalloc<T>(b, h.size());
@@ -138,6 +103,17 @@ static void init_planets(DiskState &S, DiskParams &D, const disco_params &p, con
    }
 }
 
+/* the FP32 view: same allocations, R* pointers reinterpreted */
+static void make_float_view(disco_batch *b){
+   ViewT<double> &d = b->vd;
+   ViewT<float> &f = b->vf;
+   memcpy(&f, &d, sizeof f);
+   f.prim = (float *)d.prim; f.gradp = (float *)d.gradp; f.gradr = (float *)d.gradr;
+   f.fS = (float *)d.fS; f.fG = (float *)d.fG; f.Gp = (float *)d.Gp;
+}
+
+extern "C" void disco_batch_destroy(disco_batch *b);
+
 extern "C" int disco_batch_create(int device, const disco_modules *mods, int precision,
                                   int ndisk, const disco_params *params,
                                   const int *Nr, const int *Nz, const int *Ng,
@@ -149,8 +125,9 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    int ndev = 0;
    if( cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1 ) return DISCO_ERR_NO_DEVICE;
    if( device < 0 || device >= ndev ) return DISCO_ERR_ARG;
+   if( precision != DISCO_PREC_FP64 && precision != DISCO_PREC_MIXED ) return DISCO_ERR_ARG;
    if( mods->hydro != DISCO_HYDRO_EULER || mods->num_c != 5 || mods->num_n != 1 ||
-       mods->ct_mode != 0 || precision != DISCO_PREC_FP64 )
+       mods->ct_mode != 0 )
       return DISCO_ERR_UNSUPPORTED;
    if( mods->boundary != DISCO_BC_FIXED ) return DISCO_ERR_UNSUPPORTED;
    if( mods->initial != DISCO_IC_KEPLER_NOISE ) return DISCO_ERR_UNSUPPORTED;
@@ -173,6 +150,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->any_mm3 = 0;
    b->graph = NULL;
    b->have_cells = 0;
+   b->stream = NULL;
    b->own_stream = NULL;
    b->tape = NULL; b->tape_names = NULL;
 
@@ -239,7 +217,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->tr_off.push_back(face);
    b->ncell = cell;
 
-   View &v = b->v;
+   ViewT<double> &v = b->vd;
    memset(&v, 0, sizeof v);
    v.Ncell = cell; v.Nann = ann; v.Ntr = (int)b->tr_a.size(); v.Nf = face;
    v.nq = b->nq;
@@ -254,10 +232,16 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.dp = dupload(b, b->dparams);
    v.ds = dupload(b, dstate);
    b->d_ann_blk0 = dupload(b, b->ann_blk0); b->d_ann_nblk = dupload(b, b->ann_nblk);
-   size_t N = (size_t)cell, Qn = (size_t)b->Q*N;
-   v.prim = dalloc<double>(b, Qn); v.cons = dalloc<double>(b, Qn);
-   v.RKcons = dalloc<double>(b, Qn); v.gradp = dalloc<double>(b, Qn);
-   v.gradr = dalloc<double>(b, Qn); v.Gp = dalloc<double>(b, Qn);
+   size_t N = (size_t)cell, Qn = (size_t)b->Q*N, Qf = (size_t)b->Q*face;
+   size_t rs = precision == DISCO_PREC_MIXED ? sizeof(float) : sizeof(double);
+   v.prim = (double *)dalloc_bytes(b, Qn*rs);
+   v.gradp = (double *)dalloc_bytes(b, Qn*rs);
+   v.gradr = (double *)dalloc_bytes(b, Qn*rs);
+   v.Gp = (double *)dalloc_bytes(b, Qn*rs);
+   v.fS = (double *)dalloc_bytes(b, Qf*rs);
+   v.fG = (double *)dalloc_bytes(b, Qf*rs);
+   v.cons = dalloc<double>(b, Qn); v.RKcons = dalloc<double>(b, Qn);
+   v.ccarry = precision == DISCO_PREC_MIXED ? dalloc<double>(b, Qn) : NULL;
    v.piph = dalloc<double>(b, N); v.dphi = dalloc<double>(b, N);
    v.wiph = dalloc<double>(b, N); v.piph_new = dalloc<double>(b, N);
    v.I0 = dalloc<int>(b, ann);
@@ -265,17 +249,18 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.fL = dalloc<int>(b, face); v.fR = dalloc<int>(b, face);
    v.fLR = dalloc<unsigned char>(b, face);
    v.fphic = dalloc<double>(b, face); v.fdA = dalloc<double>(b, face); v.fdp = dalloc<double>(b, face);
-   v.fS = dalloc<double>(b, (size_t)b->Q*face); v.fG = dalloc<double>(b, (size_t)b->Q*face);
    v.diag_part = dalloc<double>(b, b->cblk.size()*6);
    v.ann_om = dalloc<double>(b, ann); v.ann_om1 = dalloc<double>(b, ann);
    v.tr_om = dalloc<double>(b, v.Ntr);
    b->d_Qrz = dalloc<double>(b, (size_t)ann*5);
    v.err = dalloc<int>(b, 1);
    b->d_err = v.err;
+   make_float_view(b);
    for( void *p : b->allocs ) if( !p ){ disco_batch_destroy(b); return DISCO_ERR_CUDA; }
-   if( cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ){
+   if( cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) != cudaSuccess ){
       disco_batch_destroy(b); return DISCO_ERR_CUDA;
    }
+   b->stream = b->own_stream;
    {
       int nx = ann > v.Ntr ? ann : v.Ntr;
       k_precompute<<<nblk(nx, 128), 128, 0, b->stream>>>(v);
@@ -290,7 +275,6 @@ extern "C" void disco_batch_destroy(disco_batch *b){
    cudaSetDevice(b->device);
    if( b->graph ) cudaGraphExecDestroy(b->graph);
    if( b->own_stream ) cudaStreamDestroy(b->own_stream);
-   else if( b->stream ) cudaStreamDestroy(b->stream);
    for( void *p : b->allocs ) if( p ) cudaFree(p);
    delete b;
 }
@@ -311,37 +295,31 @@ static cudaError_t xfer(const disco_batch *b, void *dst, const void *src, size_t
    return cudaStreamSynchronize(b->stream);
 }
 
-/* cell-major (Q per cell) host <-> SoA device */
-static int upload_q(disco_batch *b, double *dst, const double *src){
+/* cell-major FP64 (Q per cell) host <-> SoA device of element type T */
+template<class T>
+static int upload_q(disco_batch *b, T *dst, const double *src){
    size_t N = b->ncell; int Q = b->Q;
-   std::vector<double> t((size_t)Q*N);
-   for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<Q ; ++q ) t[q*N + c] = src[c*Q + q];
-   CK(xfer(b, dst, t.data(), t.size()*sizeof(double), cudaMemcpyHostToDevice));
+   std::vector<T> t((size_t)Q*N);
+   for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<Q ; ++q ) t[q*N + c] = (T)src[c*Q + q];
+   CK(xfer(b, dst, t.data(), t.size()*sizeof(T), cudaMemcpyHostToDevice));
    return DISCO_OK;
 }
-static int download_q(disco_batch *b, double *dst, const double *src){
+template<class T>
+static int download_q(disco_batch *b, double *dst, const T *src){
    size_t N = b->ncell; int Q = b->Q;
-   std::vector<double> t((size_t)Q*N);
-   CK(xfer(b, t.data(), src, t.size()*sizeof(double), cudaMemcpyDeviceToHost));
-   for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<Q ; ++q ) dst[c*Q + q] = t[q*N + c];
+   std::vector<T> t((size_t)Q*N);
+   CK(xfer(b, t.data(), src, t.size()*sizeof(T), cudaMemcpyDeviceToHost));
+   for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<Q ; ++q ) dst[c*Q + q] = (double)t[q*N + c];
    return DISCO_OK;
 }
-
-static unsigned nblk(size_t n, unsigned t){ return (unsigned)((n + t - 1)/t); }
-
-/* after a launch: in kernel-timing mode, an event closing that launch */
-static void mark(disco_batch *b, const char *name){
-   if( !b->tape ) return;
-   cudaEvent_t e;
-   cudaEventCreate(&e);
-   cudaEventRecord(e, b->stream);
-   b->tape->push_back(e);
-   b->tape_names->push_back(name);
+/* an R-typed cell array of the batch (prim, gradp, gradr) */
+static int upload_r(disco_batch *b, double *dev, const double *src){
+   if( b->prec == DISCO_PREC_MIXED ) return upload_q<float>(b, (float *)dev, src);
+   return upload_q<double>(b, dev, src);
 }
-
-template<int Q, int NC>
-static void launch_prim2cons(disco_batch *b){
-   k_prim2cons<Q,NC><<<(unsigned)b->cblk.size(), CB, 0, b->stream>>>(b->v);
+static int download_r(disco_batch *b, double *dst, const double *dev){
+   if( b->prec == DISCO_PREC_MIXED ) return download_q<float>(b, dst, (const float *)dev);
+   return download_q<double>(b, dst, dev);
 }
 
 extern "C" int disco_batch_set_cells(disco_batch *b, const double *prim, const double *cons,
@@ -352,16 +330,19 @@ extern "C" int disco_batch_set_cells(disco_batch *b, const double *prim, const d
    CK(cudaSetDevice(b->device));
    size_t N = b->ncell;
    int s;
-   if( prim && (s = upload_q(b, b->v.prim, prim)) ) return s;
-   if( cons && (s = upload_q(b, b->v.cons, cons)) ) return s;
-   CK(xfer(b, b->v.piph, piph, N*sizeof(double), cudaMemcpyHostToDevice));
-   CK(xfer(b, b->v.dphi, dphi, N*sizeof(double), cudaMemcpyHostToDevice));
-   if( wiph ) CK(xfer(b, b->v.wiph, wiph, N*sizeof(double), cudaMemcpyHostToDevice));
+   if( prim && (s = upload_r(b, b->vd.prim, prim)) ) return s;
+   if( cons && (s = upload_q<double>(b, b->vd.cons, cons)) ) return s;
+   CK(xfer(b, b->vd.piph, piph, N*sizeof(double), cudaMemcpyHostToDevice));
+   CK(xfer(b, b->vd.dphi, dphi, N*sizeof(double), cudaMemcpyHostToDevice));
+   if( wiph ) CK(xfer(b, b->vd.wiph, wiph, N*sizeof(double), cudaMemcpyHostToDevice));
+   if( b->vd.ccarry ) CK(cudaMemsetAsync(b->vd.ccarry, 0, (size_t)b->Q*N*sizeof(double), b->stream));
    if( prim && !cons ){
-      launch_prim2cons<6,5>(b);
+      unsigned ncb = (unsigned)b->cblk.size();
+      if( b->prec == DISCO_PREC_MIXED ) mixed_launch_prim2cons(b);
+      else k_prim2cons<6,5,double><<<ncb, CB, 0, b->stream>>>(b->vd);
       CK(cudaGetLastError());
-      CK(cudaStreamSynchronize(b->stream));
    }
+   CK(cudaStreamSynchronize(b->stream));
    b->have_cells = 1;
    return DISCO_OK;
 }
@@ -374,31 +355,25 @@ extern "C" int disco_batch_get_cells(disco_batch *b, double *prim, double *cons,
    CK(cudaStreamSynchronize(b->stream));
    size_t N = b->ncell;
    int s;
-   if( prim && (s = download_q(b, prim, b->v.prim)) ) return s;
-   if( cons && (s = download_q(b, cons, b->v.cons)) ) return s;
-   if( piph ) CK(xfer(b, piph, b->v.piph, N*sizeof(double), cudaMemcpyDeviceToHost));
-   if( dphi ) CK(xfer(b, dphi, b->v.dphi, N*sizeof(double), cudaMemcpyDeviceToHost));
-   if( wiph ) CK(xfer(b, wiph, b->v.wiph, N*sizeof(double), cudaMemcpyDeviceToHost));
+   if( prim && (s = download_r(b, prim, b->vd.prim)) ) return s;
+   if( cons && (s = download_q<double>(b, cons, b->vd.cons)) ) return s;
+   if( piph ) CK(xfer(b, piph, b->vd.piph, N*sizeof(double), cudaMemcpyDeviceToHost));
+   if( dphi ) CK(xfer(b, dphi, b->vd.dphi, N*sizeof(double), cudaMemcpyDeviceToHost));
+   if( wiph ) CK(xfer(b, wiph, b->vd.wiph, N*sizeof(double), cudaMemcpyDeviceToHost));
    return DISCO_OK;
 }
 
 static int launch_mindt(disco_batch *b){
-   View v = b->v;
-   unsigned nd = nblk(b->ndisk, 64);
-   k_mindt_begin<<<nd, 64, 0, b->stream>>>(v, b->ndisk);
-   k_mindt<6><<<(unsigned)b->cblk.size(), CB, 0, b->stream>>>(v);
-   k_mindt_end<<<nd, 64, 0, b->stream>>>(v, b->ndisk);
+   if( b->prec == DISCO_PREC_MIXED ) mixed_launch_mindt(b);
+   else launch_mindt_t(b, b->vd);
    return cuda_status(cudaGetLastError());
 }
 
 extern "C" int disco_batch_setup_cells(disco_batch *b){
    if( !b ) return DISCO_ERR_ARG;
    CK(cudaSetDevice(b->device));
-   View v = b->v;
-   unsigned ncb = (unsigned)b->cblk.size();
-   k_setup<6,5><<<ncb, CB, 0, b->stream>>>(v, b->bc_fixed);
-   k_wcell<6><<<ncb, CB, 0, b->stream>>>(v);
-   if( b->any_mm3 ) k_wmean_nomove<<<nblk(v.Nann, 128), 128, 0, b->stream>>>(v);
+   if( b->prec == DISCO_PREC_MIXED ) mixed_launch_setup(b);
+   else launch_setup_t(b, b->vd);
    CK(cudaGetLastError());
    int s = launch_mindt(b);
    if( s ) return s;
@@ -428,49 +403,15 @@ extern "C" int disco_batch_mindt(disco_batch *b, double *dt){
    CK(cudaStreamSynchronize(b->stream));
    if( dt ){
       std::vector<DiskState> st(b->ndisk);
-      CK(xfer(b, st.data(), b->v.ds, sizeof(DiskState)*b->ndisk, cudaMemcpyDeviceToHost));
+      CK(xfer(b, st.data(), b->vd.ds, sizeof(DiskState)*b->ndisk, cudaMemcpyDeviceToHost));
       for( int d=0 ; d<b->ndisk ; ++d ) dt[d] = st[d].dt_next;
    }
    return read_err(b);
 }
 
-/* One substep of onestep() (onestep.c:84-229) for the hydro path. */
-static void launch_substep(disco_batch *b, double RK, int first, int last, double dtfac){
-   View v = b->v;
-   v.dtfac = dtfac;
-   cudaStream_t s = b->stream;
-   unsigned ncb = (unsigned)b->cblk.size(), nfb = (unsigned)b->fblk.size();
-   k_begin<6,5><<<ncb, CB, 0, s>>>(v, RK, first);                  mark(b, "k_begin");
-   if( first && b->any_mm3 ){ k_wmean<<<nblk(v.Nann, 128), 128, 0, s>>>(v); mark(b, "k_wmean"); }
-   k_I0<<<nblk((size_t)v.Nann*32, 128), 128, 0, s>>>(v);              mark(b, "k_I0");
-   k_faces<6><<<nfb, FB, 0, s>>>(v, 1);                               mark(b, "k_faces");
-   k_gradr<6><<<ncb, CB, 0, s>>>(v);                                  mark(b, "k_gradr");
-   k_flux_r<6,5><<<nfb, FB, 0, s>>>(v);                               mark(b, "k_flux_r");
-   k_flux_p<6,5><<<ncb, CB, 0, s>>>(v);                               mark(b, "k_flux_p");
-   k_update<6,5,1><<<ncb, CB, 0, s>>>(v, first);                      mark(b, "k_update");
-   k_c2p<6,5><<<ncb, CB, 0, s>>>(v, last, b->bc_fixed);               mark(b, "k_c2p");
-}
-
-/* timestep() (timestep.c:7-45). */
 static void launch_step(disco_batch *b, int use_next){
-   View v = b->v;
-   cudaStream_t s = b->stream;
-   unsigned nd = nblk(b->ndisk, 64);
-   k_disk_begin<<<nd, 64, 0, s>>>(v, b->ndisk, use_next);             mark(b, "k_disk_begin");
-   if( b->timestep_mode == 1 ){
-      launch_substep(b, 0.0, 1, 1, 1.0);
-      k_disk_mid<<<nd, 64, 0, s>>>(v, b->ndisk, 0.0, 1, 1);         mark(b, "k_disk_mid");
-   }else{
-      launch_substep(b, 0.0, 1, 0, 1.0);
-      k_disk_mid<<<nd, 64, 0, s>>>(v, b->ndisk, 0.0, 1, 1);         mark(b, "k_disk_mid");
-      launch_substep(b, 0.5, 0, 1, 0.5);
-      k_disk_mid<<<nd, 64, 0, s>>>(v, b->ndisk, 0.5, 0, 0);         mark(b, "k_disk_mid");
-   }
-   if( b->nq ){
-      k_diag_finish<<<nblk(v.Nann, 128), 128, 0, s>>>(v, b->d_Qrz, b->d_ann_blk0, b->d_ann_nblk);
-      mark(b, "k_diag_finish");
-   }
-   k_disk_end<<<nd, 64, 0, s>>>(v, b->ndisk);                        mark(b, "k_disk_end");
+   if( b->prec == DISCO_PREC_MIXED ) mixed_launch_step(b, use_next);
+   else launch_step_t(b, b->vd, use_next);
 }
 
 extern "C" int disco_batch_timestep(disco_batch *b, const double *dt){
@@ -479,9 +420,9 @@ extern "C" int disco_batch_timestep(disco_batch *b, const double *dt){
    CK(cudaSetDevice(b->device));
    if( dt ){
       std::vector<DiskState> st(b->ndisk);
-      CK(xfer(b, st.data(), b->v.ds, sizeof(DiskState)*b->ndisk, cudaMemcpyDeviceToHost));
+      CK(xfer(b, st.data(), b->vd.ds, sizeof(DiskState)*b->ndisk, cudaMemcpyDeviceToHost));
       for( int d=0 ; d<b->ndisk ; ++d ) st[d].dt_next = dt[d];
-      CK(xfer(b, b->v.ds, st.data(), sizeof(DiskState)*b->ndisk, cudaMemcpyHostToDevice));
+      CK(xfer(b, b->vd.ds, st.data(), sizeof(DiskState)*b->ndisk, cudaMemcpyHostToDevice));
    }
    launch_step(b, 1);
    CK(cudaGetLastError());
@@ -510,7 +451,7 @@ extern "C" int disco_batch_time(const disco_batch *b, int disk, double *t, int *
    CK(cudaSetDevice(b->device));
    CK(cudaStreamSynchronize(b->stream));
    DiskState st;
-   CK(xfer(b, &st, b->v.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
+   CK(xfer(b, &st, b->vd.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
    if( t ) *t = st.t;
    if( count ) *count = st.count_steps;
    return DISCO_OK;
@@ -521,9 +462,14 @@ extern "C" int disco_batch_get_faces(disco_batch *b, int disk, int dim, int *nfa
    if( !b || disk < 0 || disk >= b->ndisk || (dim != 1 && dim != 2) ) return DISCO_ERR_ARG;
    if( dim == 2 ){ if( nfaces ) *nfaces = 0; return DISCO_OK; }
    CK(cudaSetDevice(b->device));
-   View v = b->v;
-   k_I0<<<nblk((size_t)v.Nann*32, 128), 128, 0, b->stream>>>(v);
-   k_faces<6><<<(unsigned)b->fblk.size(), FB, 0, b->stream>>>(v, 0);
+   const ViewT<double> &v = b->vd;
+   unsigned nib = nblk((size_t)v.Nann*32, 128), nfb = (unsigned)b->fblk.size();
+   if( b->prec == DISCO_PREC_MIXED ){
+      mixed_launch_faces(b);
+   }else{
+      k_I0<double><<<nib, 128, 0, b->stream>>>(v);
+      k_faces<6,double><<<nfb, FB, 0, b->stream>>>(v, 0);
+   }
    CK(cudaGetLastError());
    CK(cudaStreamSynchronize(b->stream));
    const DiskParams &D = b->dparams[disk];
@@ -575,7 +521,7 @@ extern "C" int disco_batch_get_diagnostics(disco_batch *b, int disk, double *Qrz
    if( Qrz && b->nq ) CK(xfer(b, Qrz, b->d_Qrz + (size_t)D.ann0*5, sizeof(double)*na*5, cudaMemcpyDeviceToHost));
    if( t_avg ){
       DiskState st;
-      CK(xfer(b, &st, b->v.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
+      CK(xfer(b, &st, b->vd.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
       *t_avg = st.t_avg;
    }
    return DISCO_OK;
@@ -592,18 +538,17 @@ extern "C" int disco_batch_last_error(disco_batch *b){
 extern "C" int disco_batch_debug_get(disco_batch *b, int which, double *out){
    if( !b || !out ) return DISCO_ERR_ARG;
    CK(cudaSetDevice(b->device));
-   const double *src = which == 0 ? b->v.gradp : which == 1 ? b->v.gradr :
-                       which == 2 ? b->v.RKcons : NULL;
-   if( !src ) return DISCO_ERR_ARG;
    CK(cudaStreamSynchronize(b->stream));
-   return download_q(b, out, src);
+   if( which == 0 ) return download_r(b, out, b->vd.gradp);
+   if( which == 1 ) return download_r(b, out, b->vd.gradr);
+   if( which == 2 ) return download_q<double>(b, out, b->vd.RKcons);
+   return DISCO_ERR_ARG;
 }
 
 extern "C" int disco_batch_set_stream(disco_batch *b, void *stream){
    if( !b ) return DISCO_ERR_ARG;
    CK(cudaSetDevice(b->device));
    CK(cudaStreamSynchronize(b->stream));
-   if( b->own_stream == NULL ) b->own_stream = b->stream;
    b->stream = stream ? (cudaStream_t)stream : b->own_stream;
    return DISCO_OK;
 }

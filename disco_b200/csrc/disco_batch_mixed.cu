@@ -1,0 +1,17 @@
+/*
+ * The FP32 mixed form's launches (DISCO_PREC_MIXED): the templated kernels of
+ * disco_kernels.cuh instantiated with R = float.  This file is compiled with
+ * FMA contraction (--fmad=true); the FP64 path in disco_batch.cu is not.
+ */
+#include "disco_batch_impl.cuh"
+
+void mixed_launch_mindt(disco_batch *b){ launch_mindt_t(b, b->vf); }
+void mixed_launch_setup(disco_batch *b){ launch_setup_t(b, b->vf); }
+void mixed_launch_step(disco_batch *b, int use_next){ launch_step_t(b, b->vf, use_next); }
+void mixed_launch_prim2cons(disco_batch *b){
+   k_prim2cons<6,5,float><<<(unsigned)b->cblk.size(), CB, 0, b->stream>>>(b->vf);
+}
+void mixed_launch_faces(disco_batch *b){
+   k_I0<float><<<nblk((size_t)b->vf.Nann*32, 128), 128, 0, b->stream>>>(b->vf);
+   k_faces<6,float><<<(unsigned)b->fblk.size(), FB, 0, b->stream>>>(b->vf, 0);
+}

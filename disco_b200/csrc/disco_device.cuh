@@ -1,5 +1,5 @@
 /*
- * Device-side physics of the B200 Disco timestep (FP64).
+ * Device-side physics of the B200 Disco timestep.
  *
  * Per-state algebra of the selected modules, written with the same
  * floating-point operation order as the reference so that, compiled with
@@ -78,8 +78,12 @@ __device__ __forceinline__ double get_signed_dp(double phip, double phim, double
    while( dp >  .5*Pmax ){ dp -= Pmax; if( ++n > WRAP_CAP ){ *err |= ERRF_WRAP; break; } }
    return dp;
 }
+/* cylindrical.c:24-30; the sum is spelled with round-to-nearest intrinsics so
+ * that no translation unit (the mixed form is built with FMA contraction)
+ * turns it into an FMA: the mesh must be the same in every form. */
 __device__ __forceinline__ double centroid_r(double xp, double xm){
-   return 2.0*(xp*xp + xp*xm + xm*xm) / (3.0*(xp+xm));
+   double s = __dadd_rn(__dadd_rn(__dmul_rn(xp, xp), __dmul_rn(xp, xm)), __dmul_rn(xm, xm));
+   return 2.0*s / (3.0*(xp+xm));
 }
 __device__ __forceinline__ double centroid_z(double xp, double xm){ return 0.5*(xp+xm); }
 /* get_dV(xp,xm) given dphi = get_dp(xp1,xm1) already evaluated */
@@ -129,17 +133,21 @@ __device__ __forceinline__ double mesh_om(const DiskParams &P, double r){
 }
 
 /* ------------------------------------------------------------ euler.c
- * x[0] is the radius used by the state algebra; om = get_om(x). */
-template<int Q, int NC>
-__device__ __forceinline__ void prim2cons(const DiskParams &P, const double *prim, double *cons,
-                                          double r, double om, double dV){
-   double rho = prim[RHO], Pp = prim[PPP], vr = prim[URR];
-   double vp = prim[UPP]*r, vz = prim[UZZ];
-   double vp_off = vp - om*r;
-   double v2 = vr*vr + vp_off*vp_off + vz*vz;
-   double rhoe = Pp/(P.gam - 1.);
+ * Templated on the bulk real type R: R = double is the reference's FP64
+ * arithmetic (constants written R(...) so the double instantiation rounds
+ * exactly as before); R = float is the mixed form's FP32 flux arithmetic.
+ * r is the radius used by the state algebra and om = get_om(x) there. */
+template<int Q, int NC, class R>
+__device__ __forceinline__ void prim2cons(const DiskParams &P, const R *prim, R *cons,
+                                          R r, R om, R dV){
+   const R gam = (R)P.gam;
+   R rho = prim[RHO], Pp = prim[PPP], vr = prim[URR];
+   R vp = prim[UPP]*r, vz = prim[UZZ];
+   R vp_off = vp - om*r;
+   R v2 = vr*vr + vp_off*vp_off + vz*vz;
+   R rhoe = Pp/(gam - R(1.));
    cons[DDD] = rho*dV;
-   cons[TAU] = (.5*rho*v2 + rhoe )*dV;
+   cons[TAU] = (R(.5)*rho*v2 + rhoe )*dV;
    cons[SRR] = rho*vr*dV;
    cons[LLL] = r*rho*vp*dV;
    cons[SZZ] = rho*vz*dV;
@@ -147,6 +155,7 @@ __device__ __forceinline__ void prim2cons(const DiskParams &P, const double *pri
    for( int q=NC ; q<Q ; ++q ) cons[q] = prim[q]*cons[DDD];
 }
 
+/* cons2prim (euler.c:102-139), always FP64 */
 template<int Q, int NC>
 __device__ __forceinline__ void cons2prim(const DiskParams &P, const double *cons, double *prim,
                                           double r, double om, double dV){
@@ -178,62 +187,64 @@ __device__ __forceinline__ void cons2prim(const DiskParams &P, const double *con
 }
 
 /* flux(), euler.c:141, for a normal n = e_dim (dim 0: phi, 1: r, 2: z) */
-template<int Q, int NC, int DIM>
-__device__ __forceinline__ void flux(const DiskParams &P, const double *prim, double *F,
-                                     double r, double om){
-   const double n0 = DIM==1 ? 1.0 : 0.0, n1 = DIM==0 ? 1.0 : 0.0, n2 = DIM==2 ? 1.0 : 0.0;
-   double rho = prim[RHO], Pp = prim[PPP], vr = prim[URR];
-   double vp = prim[UPP]*r, vz = prim[UZZ];
-   double vn = vr*n0 + vp*n1 + vz*n2;
-   double wn = om*r*n1;
-   double vp_off = vp - om*r;
-   double rhoe = Pp/(P.gam - 1.);
-   double v2 = vr*vr + vp_off*vp_off + vz*vz;
+template<int Q, int NC, int DIM, class R>
+__device__ __forceinline__ void flux(const DiskParams &P, const R *prim, R *F, R r, R om){
+   const R n0 = DIM==1 ? R(1.0) : R(0.0), n1 = DIM==0 ? R(1.0) : R(0.0), n2 = DIM==2 ? R(1.0) : R(0.0);
+   const R gam = (R)P.gam;
+   R rho = prim[RHO], Pp = prim[PPP], vr = prim[URR];
+   R vp = prim[UPP]*r, vz = prim[UZZ];
+   R vn = vr*n0 + vp*n1 + vz*n2;
+   R wn = om*r*n1;
+   R vp_off = vp - om*r;
+   R rhoe = Pp/(gam - R(1.));
+   R v2 = vr*vr + vp_off*vp_off + vz*vz;
    F[DDD] = rho*vn;
    F[SRR] = rho*vr*vn + Pp*n0;
    F[LLL] = r*(rho*vp*vn + Pp*n1);
    F[SZZ] = rho*vz*vn + Pp*n2;
-   F[TAU] = ( .5*rho*v2 + rhoe + Pp )*vn - Pp*wn;
+   F[TAU] = ( R(.5)*rho*v2 + rhoe + Pp )*vn - Pp*wn;
 #pragma unroll
    for( int q=NC ; q<Q ; ++q ) F[q] = prim[q]*F[DDD];
 }
 
 /* getUstar(), euler.c:64 */
-template<int Q, int NC, int DIM>
-__device__ __forceinline__ void getUstar(const DiskParams &P, const double *prim, double *Ustar,
-                                         double r, double om, double Sk, double Ss){
-   const double n0 = DIM==1 ? 1.0 : 0.0, n1 = DIM==0 ? 1.0 : 0.0, n2 = DIM==2 ? 1.0 : 0.0;
-   double rho = prim[RHO], vr = prim[URR], vp = prim[UPP]*r, vz = prim[UZZ];
-   double Pp = prim[PPP];
-   double vp_off = vp - om*r;
-   double v2 = vr*vr+vp_off*vp_off+vz*vz;
-   double vn = vr*n0 + vp*n1 + vz*n2;
-   double vn_off = vn - om*r*n1;
-   double Ss_off = Ss + vn_off - vn;
-   double rhoe = Pp/(P.gam - 1.);
-   double rhostar = rho*(Sk - vn)/(Sk - Ss);
-   double Pstar = Pp*(Ss - vn)/(Sk - Ss);
-   double Us = rhoe*(Sk - vn)/(Sk - Ss);
+template<int Q, int NC, int DIM, class R>
+__device__ __forceinline__ void getUstar(const DiskParams &P, const R *prim, R *Ustar,
+                                         R r, R om, R Sk, R Ss){
+   const R n0 = DIM==1 ? R(1.0) : R(0.0), n1 = DIM==0 ? R(1.0) : R(0.0), n2 = DIM==2 ? R(1.0) : R(0.0);
+   const R gam = (R)P.gam;
+   R rho = prim[RHO], vr = prim[URR], vp = prim[UPP]*r, vz = prim[UZZ];
+   R Pp = prim[PPP];
+   R vp_off = vp - om*r;
+   R v2 = vr*vr+vp_off*vp_off+vz*vz;
+   R vn = vr*n0 + vp*n1 + vz*n2;
+   R vn_off = vn - om*r*n1;
+   R Ss_off = Ss + vn_off - vn;
+   R rhoe = Pp/(gam - R(1.));
+   R rhostar = rho*(Sk - vn)/(Sk - Ss);
+   R Pstar = Pp*(Ss - vn)/(Sk - Ss);
+   R Us = rhoe*(Sk - vn)/(Sk - Ss);
    Ustar[DDD] = rhostar;
    Ustar[SRR] =   rhostar*( vr + (Ss-vn)*n0 );
    Ustar[LLL] = r*rhostar*( vp + (Ss-vn)*n1 );
    Ustar[SZZ] =   rhostar*( vz + (Ss-vn)*n2 );
-   Ustar[TAU] = .5*rhostar*v2 + Us + rhostar*Ss_off*(Ss - vn) + Pstar;
+   Ustar[TAU] = R(.5)*rhostar*v2 + Us + rhostar*Ss_off*(Ss - vn) + Pstar;
 #pragma unroll
    for( int q=NC ; q<Q ; ++q ) Ustar[q] = prim[q]*Ustar[DDD];
 }
 
 /* vel(), euler.c:305 */
-template<int DIM>
-__device__ __forceinline__ void vel(const DiskParams &P, const double *p1, const double *p2,
-                                    double r, double *Sl, double *Sr, double *Ss){
-   const double n0 = DIM==1 ? 1.0 : 0.0, n1 = DIM==0 ? 1.0 : 0.0, n2 = DIM==2 ? 1.0 : 0.0;
-   double P1 = p1[PPP], rho1 = p1[RHO];
-   double vn1 = p1[URR]*n0 + p1[UPP]*n1*r + p1[UZZ]*n2;
-   double cs1 = sqrt(P.gam*P1/rho1);
-   double P2 = p2[PPP], rho2 = p2[RHO];
-   double vn2 = p2[URR]*n0 + p2[UPP]*n1*r + p2[UZZ]*n2;
-   double cs2 = sqrt(P.gam*P2/rho2);
+template<int DIM, class R>
+__device__ __forceinline__ void vel(const DiskParams &P, const R *p1, const R *p2,
+                                    R r, R *Sl, R *Sr, R *Ss){
+   const R n0 = DIM==1 ? R(1.0) : R(0.0), n1 = DIM==0 ? R(1.0) : R(0.0), n2 = DIM==2 ? R(1.0) : R(0.0);
+   const R gam = (R)P.gam;
+   R P1 = p1[PPP], rho1 = p1[RHO];
+   R vn1 = p1[URR]*n0 + p1[UPP]*n1*r + p1[UZZ]*n2;
+   R cs1 = sqrt(gam*P1/rho1);
+   R P2 = p2[PPP], rho2 = p2[RHO];
+   R vn2 = p2[URR]*n0 + p2[UPP]*n1*r + p2[UZZ]*n2;
+   R cs2 = sqrt(gam*P2/rho2);
    *Ss = ( P2 - P1 + rho1*vn1*(-cs1) - rho2*vn2*cs2 )/( rho1*(-cs1) - rho2*cs2 );
    *Sr =  cs1 + vn1;
    *Sl = -cs1 + vn1;
@@ -244,40 +255,40 @@ __device__ __forceinline__ void vel(const DiskParams &P, const double *p1, const
 /* solve_riemann(), riemann.c:216-318, HLL / HLLC.  Returns
  * G_q = (Flux_q - w*Ustr_q)*dAdt, the amount subtracted from cons_L and
  * added to cons_R (riemann.c:312-315). */
-template<int Q, int NC, int DIM>
-__device__ __forceinline__ void solve_riemann(const DiskParams &P, const double *primL,
-                                              const double *primR, double r, double om,
-                                              double w, double dAdt, double *G){
-   double Flux[Q], Ustr[Q];
+template<int Q, int NC, int DIM, class R>
+__device__ __forceinline__ void solve_riemann(const DiskParams &P, const R *primL,
+                                              const R *primR, R r, R om,
+                                              R w, R dAdt, R *G){
+   R Flux[Q], Ustr[Q];
 #pragma unroll
-   for( int q=0 ; q<Q ; ++q ){ Flux[q] = 0.0; Ustr[q] = 0.0; }
-   double Sl, Sr, Ss;
-   vel<DIM>(P, primL, primR, r, &Sl, &Sr, &Ss);
+   for( int q=0 ; q<Q ; ++q ){ Flux[q] = R(0.0); Ustr[q] = R(0.0); }
+   R Sl, Sr, Ss;
+   vel<DIM,R>(P, primL, primR, r, &Sl, &Sr, &Ss);
    if( w < Sl ){
-      flux<Q,NC,DIM>(P, primL, Flux, r, om);
-      prim2cons<Q,NC>(P, primL, Ustr, r, om, 1.0);
+      flux<Q,NC,DIM,R>(P, primL, Flux, r, om);
+      prim2cons<Q,NC,R>(P, primL, Ustr, r, om, R(1.0));
    }else if( w > Sr ){
-      flux<Q,NC,DIM>(P, primR, Flux, r, om);
-      prim2cons<Q,NC>(P, primR, Ustr, r, om, 1.0);
+      flux<Q,NC,DIM,R>(P, primR, Flux, r, om);
+      prim2cons<Q,NC,R>(P, primR, Ustr, r, om, R(1.0));
    }else if( P.riemann == 0 ){
-      double Fl[Q], Fr[Q], Ul[Q], Ur[Q];
-      double aL = Sr, aR = -Sl;
-      prim2cons<Q,NC>(P, primL, Ul, r, om, 1.0);
-      prim2cons<Q,NC>(P, primR, Ur, r, om, 1.0);
-      flux<Q,NC,DIM>(P, primL, Fl, r, om);
-      flux<Q,NC,DIM>(P, primR, Fr, r, om);
+      R Fl[Q], Fr[Q], Ul[Q], Ur[Q];
+      R aL = Sr, aR = -Sl;
+      prim2cons<Q,NC,R>(P, primL, Ul, r, om, R(1.0));
+      prim2cons<Q,NC,R>(P, primR, Ur, r, om, R(1.0));
+      flux<Q,NC,DIM,R>(P, primL, Fl, r, om);
+      flux<Q,NC,DIM,R>(P, primR, Fr, r, om);
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){
          Flux[q] = ( aL*Fl[q] + aR*Fr[q] + aL*aR*( Ul[q] - Ur[q] ) )/( aL + aR );
          Ustr[q] = ( aR*Ul[q] + aL*Ur[q] + Fl[q] - Fr[q] )/( aL + aR );
       }
    }else{
-      double Uk[Q], Fk[Q];
-      const double *pk = (w < Ss) ? primL : primR;
-      double Sk = (w < Ss) ? Sl : Sr;
-      prim2cons<Q,NC>(P, pk, Uk, r, om, 1.0);
-      getUstar<Q,NC,DIM>(P, pk, Ustr, r, om, Sk, Ss);
-      flux<Q,NC,DIM>(P, pk, Fk, r, om);
+      R Uk[Q], Fk[Q];
+      const R *pk = (w < Ss) ? primL : primR;
+      R Sk = (w < Ss) ? Sl : Sr;
+      prim2cons<Q,NC,R>(P, pk, Uk, r, om, R(1.0));
+      getUstar<Q,NC,DIM,R>(P, pk, Ustr, r, om, Sk, Ss);
+      flux<Q,NC,DIM,R>(P, pk, Fk, r, om);
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ) Flux[q] = Fk[q] + Sk*( Ustr[q] - Uk[q] );
    }

@@ -1,14 +1,22 @@
 /*
- * Kernels of the B200 Disco timestep, FP64 plain path (hydro).
+ * Kernels of the B200 Disco timestep (hydro), templated on the bulk real
+ * type R of the primitive variables, slopes and fluxes:
+ *   R = double   the plain FP64 path, arithmetic identical to the reference
+ *                (built with --fmad=false, same operation order);
+ *   R = float    the mixed form: FP32 prim / PLM / Riemann arithmetic, FP64
+ *                phi positions, mesh motion, face endpoints, dt reduction and
+ *                a Kahan-compensated FP64 conserved update.
  *
  * Layout (device, one batch of one or more disks):
- *   cells      ragged SoA in annulus order; prim[q*Ncell + c], cons, RKcons,
- *              gradp, gradr; piph[c], dphi[c], wiph[c]
+ *   cells      ragged SoA in annulus order; prim[q*Ncell + c] (R), cons (FP64),
+ *              RKcons, ccarry (Kahan carry, mixed form), gradp, gradr (R);
+ *              piph[c], dphi[c], wiph[c] (FP64)
  *   annuli     ann_off[a] .. ann_off[a]+ann_np[a]-1 are annulus a's cells
  *   r-tracks   track t joins annulus tr_a[t] (inner) and tr_b[t] (outer);
  *              its faces are tr_off[t] .. tr_off[t+1]-1 (Np_a + Np_b of them,
  *              faces_alt.c:87-100)
- *   faces      SoA: fL, fR (global cells), fLR, fphic, fdA, fdp, fS[q], fG[q]
+ *   faces      SoA: fL, fR (global cells), fLR, fphic, fdA, fdp (FP64),
+ *              fS[q], fG[q] (R)
  *   consume    consL[c] = face of the r-track outside c that consumes c in the
  *              merge; consR[c] = same for the track inside c.  They give each
  *              cell the contiguous runs of faces it belongs to, so every
@@ -26,7 +34,8 @@ namespace disco {
 #define CB 128
 #define FB 128
 
-struct View {
+template<class R>
+struct ViewT {
    int Ncell, Nann, Ntr, Nf;
    const int *ann_off, *ann_np, *ann_disk, *ann_j, *ann_k;
    const int *tr_a, *tr_b, *tr_off, *tr_flux, *tr_j, *tr_k;
@@ -35,14 +44,16 @@ struct View {
    const double *rj, *zk;
    const DiskParams *dp;
    DiskState *ds;
-   double *prim, *cons, *RKcons, *gradp, *gradr;
+   R *prim, *gradp, *gradr;
+   double *cons, *RKcons, *ccarry;
    double *piph, *dphi, *wiph, *piph_new;
    int *I0;
    int *fL, *fR;
    unsigned char *fLR;
-   double *fphic, *fdA, *fdp, *fS, *fG;
+   double *fphic, *fdA, *fdp;
+   R *fS, *fG;
    int *consL, *consR;
-   double *Gp;
+   R *Gp;
    double *diag_part;   /* per cell block: nq sums + volume */
    /* energy-frame Omega of omega.c:62-110, evaluated once by k_precompute at
     * the radii the step uses (same device expressions, so bit-identical to
@@ -53,8 +64,22 @@ struct View {
    int *err;
 };
 
-__device__ __forceinline__ void raise_err(const View &v, int e){
+template<class R>
+__device__ __forceinline__ void raise_err(const ViewT<R> &v, int e){
    if( e ) atomicOr(v.err, e);
+}
+
+/* cons += x, plain in the FP64 path, Kahan-compensated in the mixed form */
+template<class R>
+__device__ __forceinline__ void acc(double &s, double &cc, double x){
+   if constexpr ( sizeof(R) == sizeof(double) ){
+      s += x;
+   }else{
+      double y = x - cc;
+      double t = s + y;
+      cc = (t - s) - y;
+      s = t;
+   }
 }
 
 /* ------------------------------------------------------------------ k_begin
@@ -62,8 +87,8 @@ __device__ __forceinline__ void raise_err(const View &v, int e){
  * modes 0/1/2/4; mode 3's mean is k_wmean), the moved-and-wrapped piph of
  * move_cells + clean_pi (misc.c:256-268, 8-26) into piph_new.
  * Every substep: adjust_RK_cons (misc.c:226-244) and plm_phi (plm.c:15-51). */
-template<int Q, int NC>
-__global__ void __launch_bounds__(CB) k_begin(View v, double RK, int first){
+template<int Q, int NC, class R>
+__global__ void __launch_bounds__(CB) k_begin(ViewT<R> v, double RK, int first){
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -75,14 +100,14 @@ __global__ void __launch_bounds__(CB) k_begin(View v, double RK, int first){
    int d = v.ann_disk[a];
    const DiskParams &P = v.dp[d];
 
-   double pC[Q], pL[Q], pR[Q];
+   R pC[Q], pL[Q], pR[Q];
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ){
       pC[q] = v.prim[q*N + c]; pL[q] = v.prim[q*N + cm]; pR[q] = v.prim[q*N + cp];
    }
    if( first ){
       double w = 0.0;
-      if( P.mesh_motion ) w = .5*(pC[UPP] + pR[UPP]);       /* get_omega = prim[UPP] */
+      if( P.mesh_motion ) w = .5*((double)pC[UPP] + (double)pR[UPP]);   /* get_omega = prim[UPP] */
       if( P.mesh_motion == 4 ){
          int j = v.ann_j[a];
          const double *rj = v.rj + P.rj0 + 1;
@@ -91,7 +116,8 @@ __global__ void __launch_bounds__(CB) k_begin(View v, double RK, int first){
       v.wiph[c] = w;
       if( P.mesh_motion != 3 ){
          int err = 0;
-         double phi = v.piph[c] + w*v.ds[d].dt;
+         /* move_cells: never contracted to an FMA, so both forms move alike */
+         double phi = __dadd_rn(v.piph[c], __dmul_rn(w, v.ds[d].dt));
          int n = 0;
          while( phi > P.Pmax ){ phi -= P.Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
          while( phi < 0.0 ){ phi += P.Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
@@ -106,19 +132,23 @@ __global__ void __launch_bounds__(CB) k_begin(View v, double RK, int first){
       if( first ){ rk = cq; v.RKcons[q*N + c] = cq; }
       else rk = v.RKcons[q*N + c];
       v.cons[q*N + c] = (1.-RK)*cq + RK*rk;
+      if constexpr ( sizeof(R) != sizeof(double) ){
+         /* the carry belongs to cons; averaged with it (RKcons keeps none) */
+         if( !first ) v.ccarry[q*N + c] = (1.-RK)*v.ccarry[q*N + c];
+      }
    }
-   double dpL = v.dphi[cm], dpC = v.dphi[c], dpR = v.dphi[cp];
-   double PLM = P.PLM;
+   const R dpL = (R)v.dphi[cm], dpC = (R)v.dphi[c], dpR = (R)v.dphi[cp];
+   const R PLM = (R)P.PLM;
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ){
-      double sL = pC[q] - pL[q];  sL /= .5*( dpC + dpL );
-      double sR = pR[q] - pC[q];  sR /= .5*( dpR + dpC );
-      double sC = pR[q] - pL[q];  sC /= .5*( dpL + dpR ) + dpC;
-      double aa = PLM*sL, bb = sC, cc = PLM*sR;           /* minmod, plm.c:6 */
-      double m = aa;
-      if( aa*bb < 0.0 ) m = 0.0;
+      R sL = pC[q] - pL[q];  sL /= R(.5)*( dpC + dpL );
+      R sR = pR[q] - pC[q];  sR /= R(.5)*( dpR + dpC );
+      R sC = pR[q] - pL[q];  sC /= R(.5)*( dpL + dpR ) + dpC;
+      R aa = PLM*sL, bb = sC, cc = PLM*sR;                /* minmod, plm.c:6 */
+      R m = aa;
+      if( aa*bb < R(0.0) ) m = R(0.0);
       if( fabs(bb) < fabs(m) ) m = bb;
-      if( bb*cc < 0.0 ) m = 0.0;
+      if( bb*cc < R(0.0) ) m = R(0.0);
       if( fabs(cc) < fabs(m) ) m = cc;
       v.gradp[q*N + c] = m;
    }
@@ -126,7 +156,8 @@ __global__ void __launch_bounds__(CB) k_begin(View v, double RK, int first){
 
 /* Energy-frame Omega at the radii the step evaluates it (omega.c:62-110):
  * annulus centroids (sources, phi faces, c2p) and r-faces (trans_flux). */
-__global__ void k_precompute(View v){
+template<class R>
+__global__ void k_precompute(ViewT<R> v){
    int x = blockIdx.x*blockDim.x + threadIdx.x;
    if( x < v.Nann ){
       const DiskParams &P = v.dp[v.ann_disk[x]];
@@ -146,7 +177,8 @@ __global__ void k_precompute(View v){
 
 /* Mesh_Motion 3 (misc.c:138-152): annulus mean of w, summed in cell order
  * by one thread per annulus, then the move of the first substep. */
-__global__ void k_wmean(View v){
+template<class R>
+__global__ void k_wmean(ViewT<R> v){
    int a = blockIdx.x*blockDim.x + threadIdx.x;
    if( a >= v.Nann ) return;
    int np = v.ann_np[a], c0 = v.ann_off[a];
@@ -160,7 +192,7 @@ __global__ void k_wmean(View v){
    int err = 0;
    for( int i=0 ; i<np ; ++i ){
       v.wiph[c0+i] = w;
-      double phi = v.piph[c0+i] + w*dt;
+      double phi = __dadd_rn(v.piph[c0+i], __dmul_rn(w, dt));
       int n = 0;
       while( phi > P.Pmax ){ phi -= P.Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
       while( phi < 0.0 ){ phi += P.Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
@@ -173,7 +205,8 @@ __global__ void k_wmean(View v){
  * faces_alt.c:57-79: I0 = first cell in quadrant I after any cell in
  * quadrant IV (the cell whose upper edge is just past phi = 0).  One warp
  * per annulus, ballots over 32-cell chunks. */
-__global__ void k_I0(View v){
+template<class R>
+__global__ void k_I0(ViewT<R> v){
    int warp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
    int lane = threadIdx.x & 31;
    if( warp >= v.Nann ) return;
@@ -212,10 +245,10 @@ __global__ void k_I0(View v){
  * Within one cell width the unrolled order equals the reference's wrapped
  * comparison, so (iL, iR, LRtype) are the reference's; the face's own
  * LR / LR_back and geometry are then evaluated exactly as :140-164 and
- * addFace (:10-34) do.  Also emits the PLM face slopes S_q of plm_trans
- * (plm.c:82-89) when with_slopes is set. */
-template<int Q>
-__global__ void __launch_bounds__(FB) k_faces(View v, int with_slopes){
+ * addFace (:10-34) do (FP64 in both forms).  Also emits the PLM face slopes
+ * S_q of plm_trans (plm.c:82-89) when with_slopes is set. */
+template<int Q, class R>
+__global__ void __launch_bounds__(FB) k_faces(ViewT<R> v, int with_slopes){
    int2 b = v.fblk[blockIdx.x];
    int t = b.x, dd = b.y + threadIdx.x;
    int A = v.tr_a[t], B = v.tr_b[t];
@@ -271,14 +304,14 @@ __global__ void __launch_bounds__(FB) k_faces(View v, int with_slopes){
    if( LR == 0 ) v.consL[cL] = f; else v.consR[cR] = f;
 
    if( with_slopes ){
-      double dxL = v.tr_dxL[t], dxR = v.tr_dxR[t];
+      R dxL = (R)v.tr_dxL[t], dxR = (R)v.tr_dxR[t];
       double phiL = pL - .5*dL, phiR = pR - .5*dR;
-      double dpL = get_signed_dp(phic, phiL, Pmax, &err);
-      double dpR = get_signed_dp(phiR, phic, Pmax, &err);
+      R dpL = (R)get_signed_dp(phic, phiL, Pmax, &err);
+      R dpR = (R)get_signed_dp(phiR, phic, Pmax, &err);
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){
-         double WL = v.prim[q*N + cL] + dpL*v.gradp[q*N + cL];
-         double WR = v.prim[q*N + cR] - dpR*v.gradp[q*N + cR];
+         R WL = v.prim[q*N + cL] + dpL*v.gradp[q*N + cL];
+         R WR = v.prim[q*N + cR] - dpR*v.gradp[q*N + cR];
          v.fS[(size_t)q*v.Nf + f] = (WR-WL)/(dxR+dxL);
       }
    }
@@ -290,30 +323,31 @@ __global__ void __launch_bounds__(FB) k_faces(View v, int with_slopes){
  * [s1, e1]; the I0 cell also heads the faces after the other annulus wraps,
  * run 2 = [s2, e2] (empty when s2 > e2).  cons[] is consL or consR. */
 struct Runs { int s1, e1, s2, e2; };
-__device__ __forceinline__ Runs cell_runs(const View &v, const int *cons, int t,
+template<class R>
+__device__ __forceinline__ Runs cell_runs(const ViewT<R> &v, const int *cons, int t,
                                           int c0, int np, int i, int I0){
-   Runs R;
+   Runs RR;
    int c = c0 + i;
    if( i == I0 ){
-      R.s1 = v.tr_off[t];
+      RR.s1 = v.tr_off[t];
       int prev = c0 + (I0 == 0 ? np-1 : I0-1);
-      R.s2 = cons[prev] + 1;
-      R.e2 = v.tr_off[t+1] - 1;
+      RR.s2 = cons[prev] + 1;
+      RR.e2 = v.tr_off[t+1] - 1;
    }else{
       int prev = c0 + (i == 0 ? np-1 : i-1);
-      R.s1 = cons[prev] + 1;
-      R.s2 = 1; R.e2 = 0;
+      RR.s1 = cons[prev] + 1;
+      RR.s2 = 1; RR.e2 = 0;
    }
-   R.e1 = cons[c];
-   return R;
+   RR.e1 = cons[c];
+   return RR;
 }
 
 /* ------------------------------------------------------------------ k_gradr
  * plm_trans for dim 1 (plm.c:56-195): sum S*dA over the cell's faces in the
  * reference's face order (inner track first, then outer), divide by the
  * cell's two face areas, then apply every face's limiter. */
-template<int Q>
-__global__ void __launch_bounds__(CB) k_gradr(View v){
+template<int Q, class R>
+__global__ void __launch_bounds__(CB) k_gradr(ViewT<R> v){
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -325,12 +359,12 @@ __global__ void __launch_bounds__(CB) k_gradr(View v){
    int j = v.ann_j[a], k = v.ann_k[a];
    int Nr = P.Nr;
    int I0 = v.I0[a];
-   double g[Q];
+   R g[Q];
 #pragma unroll
-   for( int q=0 ; q<Q ; ++q ) g[q] = 0.0;
+   for( int q=0 ; q<Q ; ++q ) g[q] = R(0.0);
    if( P.PLM == 0.0 ){
 #pragma unroll
-      for( int q=0 ; q<Q ; ++q ) v.gradr[q*N + c] = 0.0;
+      for( int q=0 ; q<Q ; ++q ) v.gradr[q*N + c] = R(0.0);
       return;
    }
    int tin = j >= 1 ? P.trr0 + (j-1) + (Nr-1)*k : -1;
@@ -339,7 +373,7 @@ __global__ void __launch_bounds__(CB) k_gradr(View v){
    if( tin >= 0 ) Rin = cell_runs(v, v.consR, tin, c0, np, i, I0);
    if( tout >= 0 ) Rout = cell_runs(v, v.consL, tout, c0, np, i, I0);
    const size_t Nf = v.Nf;
-#define ACC_RUN(s,e) for( int f=(s) ; f<=(e) ; ++f ){ double dA = v.fdA[f]; \
+#define ACC_RUN(s,e) for( int f=(s) ; f<=(e) ; ++f ){ R dA = (R)v.fdA[f]; \
       _Pragma("unroll") for( int q=0 ; q<Q ; ++q ) g[q] += v.fS[q*Nf + f]*dA; }
    ACC_RUN(Rin.s1, Rin.e1)
    ACC_RUN(Rin.s2, Rin.e2)
@@ -358,12 +392,13 @@ __global__ void __launch_bounds__(CB) k_gradr(View v){
    double dAtot = dAp + dAm;
    if( j == 0 ) dAtot = dAp;
    if( j == Nr-1 ) dAtot = dAm;
+   const R rdAtot = (R)dAtot;
 #pragma unroll
-   for( int q=0 ; q<Q ; ++q ) g[q] /= dAtot;
-   double PLM = P.PLM;
+   for( int q=0 ; q<Q ; ++q ) g[q] /= rdAtot;
+   const R PLM = (R)P.PLM;
 #define LIM_RUN(s,e) for( int f=(s) ; f<=(e) ; ++f ){ \
-      _Pragma("unroll") for( int q=0 ; q<Q ; ++q ){ double S = v.fS[q*Nf + f]; \
-         if( S*g[q] < 0.0 ) g[q] = 0.0; else if( fabs(PLM*S) < fabs(g[q]) ) g[q] = PLM*S; } }
+      _Pragma("unroll") for( int q=0 ; q<Q ; ++q ){ R S = v.fS[q*Nf + f]; \
+         if( S*g[q] < R(0.0) ) g[q] = R(0.0); else if( fabs(PLM*S) < fabs(g[q]) ) g[q] = PLM*S; } }
    LIM_RUN(Rin.s1, Rin.e1)
    LIM_RUN(Rin.s2, Rin.e2)
    LIM_RUN(Rout.s1, Rout.e1)
@@ -377,8 +412,8 @@ __global__ void __launch_bounds__(CB) k_gradr(View v){
 /* ------------------------------------------------------------------ k_flux_r
  * trans_flux dim 1 (misc.c:431-509) -> riemann_trans (riemann.c:114-170)
  * -> solve_riemann; G_q = (F - w U*) dA dt per face. */
-template<int Q, int NC>
-__global__ void __launch_bounds__(FB) k_flux_r(View v){
+template<int Q, int NC, class R>
+__global__ void __launch_bounds__(FB) k_flux_r(ViewT<R> v){
    int2 b = v.fblk[blockIdx.x];
    int t = b.x;
    if( !v.tr_flux[t] ) return;
@@ -392,13 +427,13 @@ __global__ void __launch_bounds__(FB) k_flux_r(View v){
    int err = 0;
    double dt = v.ds[d].dt*v.dtfac;
    double dAdt = v.fdA[f]*dt;
-   double dxL = v.tr_dxL[t], dxR = v.tr_dxR[t];
+   R dxL = (R)v.tr_dxL[t], dxR = (R)v.tr_dxR[t];
    double phi = v.fphic[f];
    double phiL = v.piph[cL] - .5*v.dphi[cL];
    double phiR = v.piph[cR] - .5*v.dphi[cR];
-   double dpL = get_signed_dp(phi, phiL, P.Pmax, &err);
-   double dpR = get_signed_dp(phiR, phi, P.Pmax, &err);
-   double primL[Q], primR[Q];
+   R dpL = (R)get_signed_dp(phi, phiL, P.Pmax, &err);
+   R dpR = (R)get_signed_dp(phiR, phi, P.Pmax, &err);
+   R primL[Q], primR[Q];
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ){
       primL[q] = v.prim[q*N+cL] + v.gradr[q*N+cL]*dxL + v.gradp[q*N+cL]*dpL;
@@ -407,8 +442,8 @@ __global__ void __launch_bounds__(FB) k_flux_r(View v){
    int j = v.tr_j[t];
    const double *rj = v.rj + P.rj0 + 1;
    double r = .5*(rj[j]+rj[j]);                 /* face cm[0] */
-   double G[Q];
-   solve_riemann<Q,NC,1>(P, primL, primR, r, v.tr_om[t], 0.0, dAdt, G);
+   R G[Q];
+   solve_riemann<Q,NC,1,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G);
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) v.fG[(size_t)q*v.Nf + f] = G[q];
    raise_err(v, err);
@@ -417,8 +452,8 @@ __global__ void __launch_bounds__(FB) k_flux_r(View v){
 /* ------------------------------------------------------------------ k_flux_p
  * phi_flux (misc.c:368-426) -> riemann_phi (riemann.c:39-65): the face
  * between cell i and i+1 of a real annulus, stored at cell i. */
-template<int Q, int NC>
-__global__ void __launch_bounds__(CB) k_flux_p(View v){
+template<int Q, int NC, class R>
+__global__ void __launch_bounds__(CB) k_flux_p(ViewT<R> v){
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -435,16 +470,16 @@ __global__ void __launch_bounds__(CB) k_flux_p(View v){
    double r = centroid_r(rp, rm);
    double dA = (rp-rm)*(zp-zm);                      /* get_dA(.,.,0) */
    double dt = v.ds[d].dt*v.dtfac;
-   double primL[Q], primR[Q];
-   double dL = v.dphi[cL], dR = v.dphi[cR];
+   R primL[Q], primR[Q];
+   R dL = (R)v.dphi[cL], dR = (R)v.dphi[cR];
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ){
-      primL[q] = v.prim[q*N+cL] + .5*v.gradp[q*N+cL]*dL;
-      primR[q] = v.prim[q*N+cR] - .5*v.gradp[q*N+cR]*dR;
+      primL[q] = v.prim[q*N+cL] + R(.5)*v.gradp[q*N+cL]*dL;
+      primR[q] = v.prim[q*N+cR] - R(.5)*v.gradp[q*N+cR]*dR;
    }
    double w = r*v.wiph[cL];
-   double G[Q];
-   solve_riemann<Q,NC,0>(P, primL, primR, r, v.ann_om[a], w, dA*dt, G);
+   R G[Q];
+   solve_riemann<Q,NC,0,R>(P, primL, primR, (R)r, (R)v.ann_om[a], (R)w, (R)(dA*dt), G);
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) v.Gp[q*N + cL] = G[q];
 }
@@ -452,13 +487,13 @@ __global__ void __launch_bounds__(CB) k_flux_p(View v){
 /* ------------------------------------------------------------------ k_update
  * The flux gather and sources, per cell, in the reference's order:
  *   flux gather  riemann.c:312-315 applied as phi_flux then trans_flux do
- *                (phi faces from k_flux_p's Gp when PHI is set)
- *   add_source   misc.c:538-580 (euler source + planet_src), pre-move cell
+ *   add_source   misc.c:538-580 (euler source + planet_src), pre-move cell,
+ *                FP64 in both forms (the disk's force balance)
  *   move/clean/calc_dp   misc.c:256-288 (first substep; piph_new from k_begin)
  * calc_prim, the boundary, and the fused getmindt / diagnostics follow in
  * k_c2p. */
-template<int Q, int NC, int PHI>
-__global__ void __launch_bounds__(CB) k_update(View v, int first){
+template<int Q, int NC, class R>
+__global__ void __launch_bounds__(CB) k_update(ViewT<R> v, int first){
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -477,16 +512,25 @@ __global__ void __launch_bounds__(CB) k_update(View v, int first){
       const double *rj = v.rj + P.rj0 + 1;
       const double *zk = v.zk + P.zk0 + 1;
       double dt = S.dt*v.dtfac;
-      double cons[Q];
+      double cons[Q], cc[Q];
 #pragma unroll
-      for( int q=0 ; q<Q ; ++q ) cons[q] = v.cons[q*N + c];
-      if( PHI ){                          /* phi faces: loop order of phi_flux */
-         if( i > 0 ){
+      for( int q=0 ; q<Q ; ++q ){
+         cons[q] = v.cons[q*N + c];
+         if constexpr ( sizeof(R) != sizeof(double) ) cc[q] = v.ccarry[q*N + c];
+         else cc[q] = 0.0;
+      }
+      /* phi faces: loop order of phi_flux */
+      if( i > 0 ){
 #pragma unroll
-            for( int q=0 ; q<Q ; ++q ){ cons[q] += v.Gp[q*N+cprev]; cons[q] -= v.Gp[q*N+c]; }
-         }else{
+         for( int q=0 ; q<Q ; ++q ){
+            acc<R>(cons[q], cc[q], (double)v.Gp[q*N+cprev]);
+            acc<R>(cons[q], cc[q], -(double)v.Gp[q*N+c]);
+         }
+      }else{
 #pragma unroll
-            for( int q=0 ; q<Q ; ++q ){ cons[q] -= v.Gp[q*N+c]; cons[q] += v.Gp[q*N+cprev]; }
+         for( int q=0 ; q<Q ; ++q ){
+            acc<R>(cons[q], cc[q], -(double)v.Gp[q*N+c]);
+            acc<R>(cons[q], cc[q], (double)v.Gp[q*N+cprev]);
          }
       }
       /* r faces: inner track (cell is R) then outer track (cell is L) */
@@ -496,17 +540,17 @@ __global__ void __launch_bounds__(CB) k_update(View v, int first){
       Runs Rin = cell_runs(v, v.consR, tin, c0, np, i, I0);
       Runs Rout = cell_runs(v, v.consL, tout, c0, np, i, I0);
       const size_t Nf = v.Nf;
-#define ADD_RUN(s,e,op) for( int f=(s) ; f<=(e) ; ++f ){ \
-      _Pragma("unroll") for( int q=0 ; q<Q ; ++q ) cons[q] op v.fG[q*Nf + f]; }
-      ADD_RUN(Rin.s1, Rin.e1, +=)
-      ADD_RUN(Rin.s2, Rin.e2, +=)
-      ADD_RUN(Rout.s1, Rout.e1, -=)
-      ADD_RUN(Rout.s2, Rout.e2, -=)
+#define ADD_RUN(s,e,sg) for( int f=(s) ; f<=(e) ; ++f ){ \
+      _Pragma("unroll") for( int q=0 ; q<Q ; ++q ) acc<R>(cons[q], cc[q], sg (double)v.fG[q*Nf + f]); }
+      ADD_RUN(Rin.s1, Rin.e1, +)
+      ADD_RUN(Rin.s2, Rin.e2, +)
+      ADD_RUN(Rout.s1, Rout.e1, -)
+      ADD_RUN(Rout.s2, Rout.e2, -)
 #undef ADD_RUN
       /* add_source with the pre-move cell */
       double prim[Q];
 #pragma unroll
-      for( int q=0 ; q<Q ; ++q ) prim[q] = v.prim[q*N + c];
+      for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N + c];
       double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
       double phim = piph - dphi;
       double dph = get_dp(piph, phim, P.Pmax, &err);
@@ -520,11 +564,11 @@ __global__ void __launch_bounds__(CB) k_update(View v, int first){
          double centrifugal = rho*omega*omega*r;
          if( P.polar ) centrifugal *= sin(0.5*dph) / (0.5*dph);
          double press_bal = Pp/r_1;
-         cons[SRR] += dVdt*( centrifugal + press_bal );
+         acc<R>(cons[SRR], cc[SRR], dVdt*( centrifugal + press_bal ));
          double om = v.ann_om[a];
          double om_r = v.ann_om1[a];
          double om_z = 0.0;
-         cons[TAU] += dVdt*rho*( r*vr*om*om - r*r*(omega-om)*(vr*om_r + vz*om_z));
+         acc<R>(cons[TAU], cc[TAU], dVdt*rho*( r*vr*om*om - r*r*(omega-om)*(vr*om_r + vz*om_z)));
       }
       for( int p=0 ; p<P.npl ; ++p ){   /* planet_src, planet.c:152-196 */
          double rho = prim[RHO], vr = prim[URR], vz = prim[UZZ], omega = prim[UPP];
@@ -534,13 +578,16 @@ __global__ void __launch_bounds__(CB) k_update(View v, int first){
          planetary_force(P.grav2D, S.pl[p], r, phi, x2, &F0, &F1, &F2);
          double hr = 1.0, hp = r, hz = 1.0;
          if( P.polar ){ double adj = sin(0.5*dph)/(0.5*dph); F0 *= adj; F1 *= adj; }
-         cons[SRR] += rho*hr*F0*dVdt;
-         cons[LLL] += rho*hp*F1*dVdt;
-         cons[SZZ] += rho*hz*F2*dVdt;
-         cons[TAU] += rho*( hr*F0*vr + hz*F2*vz + hp*F1*omega )*dVdt;
+         acc<R>(cons[SRR], cc[SRR], rho*hr*F0*dVdt);
+         acc<R>(cons[LLL], cc[LLL], rho*hp*F1*dVdt);
+         acc<R>(cons[SZZ], cc[SZZ], rho*hz*F2*dVdt);
+         acc<R>(cons[TAU], cc[TAU], rho*( hr*F0*vr + hz*F2*vz + hp*F1*omega )*dVdt);
       }
 #pragma unroll
-      for( int q=0 ; q<Q ; ++q ) v.cons[q*N + c] = cons[q];
+      for( int q=0 ; q<Q ; ++q ){
+         v.cons[q*N + c] = cons[q];
+         if constexpr ( sizeof(R) != sizeof(double) ) v.ccarry[q*N + c] = cc[q];
+      }
    }
    if( first ){
       piph = v.piph_new[c];
@@ -551,12 +598,12 @@ __global__ void __launch_bounds__(CB) k_update(View v, int first){
 }
 
 /* ------------------------------------------------------------------ k_c2p
- *   calc_prim    misc.c:290-325 (euler cons2prim) on real cells
+ *   calc_prim    misc.c:290-325 (euler cons2prim, FP64) on real cells
  *   boundary     Boundary/fixed.c:11-60 (r ghosts re-initialised)
  * and, on the last substep, the next step's getmindt (misc.c:39-84) and the
  * per-block sums of add_diagnostics (analysis.c:52-107). */
-template<int Q, int NC>
-__global__ void __launch_bounds__(CB) k_c2p(View v, int last, int bc_fixed){
+template<int Q, int NC, class R>
+__global__ void __launch_bounds__(CB) k_c2p(ViewT<R> v, int last, int bc_fixed){
    __shared__ double s_red[CB/32][8];
    __shared__ unsigned long long s_dt[CB/32];
    int2 b = v.cblk[blockIdx.x];
@@ -587,7 +634,11 @@ __global__ void __launch_bounds__(CB) k_c2p(View v, int last, int bc_fixed){
          double dV2 = dV_of(rp, rm, dph2, zp, zm);
          cons2prim<Q,NC>(P, cons, prim, centroid_r(rp, rm), v.ann_om[a], dV2);
 #pragma unroll
-         for( int q=0 ; q<Q ; ++q ) v.prim[q*N + c] = prim[q];
+         for( int q=0 ; q<Q ; ++q ){
+            R pq = (R)prim[q];
+            v.prim[q*N + c] = pq;
+            prim[q] = (double)pq;       /* the stored state is what the next step sees */
+         }
       }else{
          bool rghost = j < P.NgRa || j >= P.Nr - P.NgRb;
          if( bc_fixed && rghost ){
@@ -595,10 +646,14 @@ __global__ void __launch_bounds__(CB) k_c2p(View v, int last, int bc_fixed){
             initial<Q,NC>(P, prim, x);
             if( P.rotframe ) prim[UPP] -= P.RotOmega;       /* subtract_omega, rotframe.c:11 */
 #pragma unroll
-            for( int q=0 ; q<Q ; ++q ) v.prim[q*N + c] = prim[q];
+            for( int q=0 ; q<Q ; ++q ){
+               R pq = (R)prim[q];
+               v.prim[q*N + c] = pq;
+               prim[q] = (double)pq;
+            }
          }else if( last ){
 #pragma unroll
-            for( int q=0 ; q<Q ; ++q ) prim[q] = v.prim[q*N + c];
+            for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N + c];
          }
       }
       if( last ){
@@ -675,7 +730,8 @@ __global__ void __launch_bounds__(CB) k_c2p(View v, int last, int bc_fixed){
 
 /* ------------------------------------------------------------------ per disk */
 /* Start of timestep(): planet_RK_copy, reset of the dt reduction. */
-__global__ void k_disk_begin(View v, int ndisk, int use_next){
+template<class R>
+__global__ void k_disk_begin(ViewT<R> v, int ndisk, int use_next){
    int d = blockIdx.x*blockDim.x + threadIdx.x;
    if( d >= ndisk ) return;
    DiskState &S = v.ds[d];
@@ -692,7 +748,8 @@ __global__ void k_disk_begin(View v, int ndisk, int use_next){
 
 /* After substep 1 (onestep.c:163-166, timestep.c:38): planet adjust/move,
  * planet phi wrap (clean_pi, misc.c:27-34), t += dt. */
-__global__ void k_disk_mid(View v, int ndisk, double RK, int first, int advance_t){
+template<class R>
+__global__ void k_disk_mid(ViewT<R> v, int ndisk, double RK, int first, int advance_t){
    int d = blockIdx.x*blockDim.x + threadIdx.x;
    if( d >= ndisk ) return;
    DiskState &S = v.ds[d];
@@ -721,9 +778,10 @@ __global__ void k_disk_mid(View v, int ndisk, double RK, int first, int advance_
    if( advance_t ) S.t += dt;
 }
 
-/* End of timestep(): dt of the next step, diagnostics (analysis.c:97-105),
+/* End of timestep(): dt of the next step, diagnostics time (analysis.c:105),
  * count_steps. */
-__global__ void k_disk_end(View v, int ndisk){
+template<class R>
+__global__ void k_disk_end(ViewT<R> v, int ndisk){
    int d = blockIdx.x*blockDim.x + threadIdx.x;
    if( d >= ndisk ) return;
    DiskState &S = v.ds[d];
@@ -737,7 +795,8 @@ __global__ void k_disk_end(View v, int ndisk){
 }
 
 /* Per annulus: sum its blocks' diagnostic partials in block order. */
-__global__ void k_diag_finish(View v, double *Qrz, const int *ann_blk0, const int *ann_nblk){
+template<class R>
+__global__ void k_diag_finish(ViewT<R> v, double *Qrz, const int *ann_blk0, const int *ann_nblk){
    int a = blockIdx.x*blockDim.x + threadIdx.x;
    if( a >= v.Nann ) return;
    int d = v.ann_disk[a];
@@ -752,9 +811,9 @@ __global__ void k_diag_finish(View v, double *Qrz, const int *ann_blk0, const in
 
 /* ------------------------------------------------------------------ setup
  * setupCells (domain.c:319-383): initial(), prim2cons, cons2prim on real
- * cells; then main.c's boundary_trans for ghosts. */
-template<int Q, int NC>
-__global__ void __launch_bounds__(CB) k_setup(View v, int bc_fixed){
+ * cells (FP64); then main.c's boundary_trans for ghosts. */
+template<int Q, int NC, class R>
+__global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc_fixed){
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -780,10 +839,10 @@ __global__ void __launch_bounds__(CB) k_setup(View v, int bc_fixed){
       initial<Q,NC>(P, prim, x);
       if( P.rotframe ) prim[UPP] -= P.RotOmega;
       double om = get_om(P, r);
-      prim2cons<Q,NC>(P, prim, cons, r, om, dV);
+      prim2cons<Q,NC,double>(P, prim, cons, r, om, dV);
       cons2prim<Q,NC>(P, cons, prim, r, om, dV);
 #pragma unroll
-      for( int q=0 ; q<Q ; ++q ){ v.prim[q*N+c] = prim[q]; v.cons[q*N+c] = cons[q]; }
+      for( int q=0 ; q<Q ; ++q ){ v.prim[q*N+c] = (R)prim[q]; v.cons[q*N+c] = cons[q]; }
    }else{
       bool rghost = j < P.NgRa || j >= P.Nr - P.NgRb;
       if( bc_fixed && rghost ){
@@ -791,17 +850,21 @@ __global__ void __launch_bounds__(CB) k_setup(View v, int bc_fixed){
          initial<Q,NC>(P, prim, x);
          if( P.rotframe ) prim[UPP] -= P.RotOmega;
 #pragma unroll
-         for( int q=0 ; q<Q ; ++q ) v.prim[q*N+c] = prim[q];
+         for( int q=0 ; q<Q ; ++q ) v.prim[q*N+c] = (R)prim[q];
       }
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ) v.cons[q*N+c] = 0.0;
+   }
+   if constexpr ( sizeof(R) != sizeof(double) ){
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) v.ccarry[q*N+c] = 0.0;
    }
    raise_err(v, err);
 }
 
 /* prim2cons on real cells for an upload without cons (domain.c:349). */
-template<int Q, int NC>
-__global__ void __launch_bounds__(CB) k_prim2cons(View v){
+template<int Q, int NC, class R>
+__global__ void __launch_bounds__(CB) k_prim2cons(ViewT<R> v){
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -819,16 +882,16 @@ __global__ void __launch_bounds__(CB) k_prim2cons(View v){
    double dV = dV_of(rj[j], rj[j-1], dph, zk[k], zk[k-1]);
    double prim[Q], cons[Q];
 #pragma unroll
-   for( int q=0 ; q<Q ; ++q ) prim[q] = v.prim[q*N+c];
-   prim2cons<Q,NC>(P, prim, cons, r, get_om(P, r), dV);
+   for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N+c];
+   prim2cons<Q,NC,double>(P, prim, cons, r, get_om(P, r), dV);
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) v.cons[q*N+c] = cons[q];
    raise_err(v, err);
 }
 
 /* set_wcell alone (setupCells' last call, domain.c:385). */
-template<int Q>
-__global__ void __launch_bounds__(CB) k_wcell(View v){
+template<int Q, class R>
+__global__ void __launch_bounds__(CB) k_wcell(ViewT<R> v){
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -838,7 +901,7 @@ __global__ void __launch_bounds__(CB) k_wcell(View v){
    int cp = c0 + (i+1 == np ? 0 : i+1);
    const DiskParams &P = v.dp[v.ann_disk[a]];
    double w = 0.0;
-   if( P.mesh_motion ) w = .5*(v.prim[UPP*N + c] + v.prim[UPP*N + cp]);
+   if( P.mesh_motion ) w = .5*((double)v.prim[UPP*N + c] + (double)v.prim[UPP*N + cp]);
    if( P.mesh_motion == 4 ){
       int j = v.ann_j[a];
       const double *rj = v.rj + P.rj0 + 1;
@@ -848,7 +911,8 @@ __global__ void __launch_bounds__(CB) k_wcell(View v){
 }
 
 /* Mesh_Motion 3 mean without a move (set-up only). */
-__global__ void k_wmean_nomove(View v){
+template<class R>
+__global__ void k_wmean_nomove(ViewT<R> v){
    int a = blockIdx.x*blockDim.x + threadIdx.x;
    if( a >= v.Nann ) return;
    const DiskParams &P = v.dp[v.ann_disk[a]];
@@ -860,9 +924,9 @@ __global__ void k_wmean_nomove(View v){
    for( int i=0 ; i<np ; ++i ) v.wiph[c0+i] = w;
 }
 
-/* Stand-alone getmindt (misc.c:39-84) into ds[d].dt_next. */
-template<int Q>
-__global__ void __launch_bounds__(CB) k_mindt(View v){
+/* Stand-alone getmindt (misc.c:39-84) into ds[d].dtmin. */
+template<int Q, class R>
+__global__ void __launch_bounds__(CB) k_mindt(ViewT<R> v){
    __shared__ unsigned long long s_dt[CB/32];
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
@@ -884,11 +948,11 @@ __global__ void __launch_bounds__(CB) k_mindt(View v){
       int cprev = c0 + (i == 0 ? np-1 : i-1);
       double w = .5*(v.wiph[cprev] + v.wiph[c]);
       double r = centroid_r(rp, rm);
-      double vp = (v.prim[UPP*N+c]-w)*r;
-      double cs = sqrt(P.gam*v.prim[PPP*N+c]/v.prim[RHO*N+c]);
-      double maxvr = cs + fabs(v.prim[URR*N+c]);
+      double vp = ((double)v.prim[UPP*N+c]-w)*r;
+      double cs = sqrt(P.gam*(double)v.prim[PPP*N+c]/(double)v.prim[RHO*N+c]);
+      double maxvr = cs + fabs((double)v.prim[URR*N+c]);
       double maxvp = cs + fabs(vp);
-      double maxvz = cs + fabs(v.prim[UZZ*N+c]);
+      double maxvz = cs + fabs((double)v.prim[UZZ*N+c]);
       double dtr = (rp-rm)/maxvr;
       double dtp = (.5*(rp+rm))*get_dp(piph, phim, P.Pmax, &err)/maxvp;
       double dtz = (zp-zm)/maxvz;
@@ -914,7 +978,8 @@ __global__ void __launch_bounds__(CB) k_mindt(View v){
    }
 }
 
-__global__ void k_mindt_begin(View v, int ndisk){
+template<class R>
+__global__ void k_mindt_begin(ViewT<R> v, int ndisk){
    int d = blockIdx.x*blockDim.x + threadIdx.x;
    if( d >= ndisk ) return;
    const DiskParams &P = v.dp[d];
@@ -922,7 +987,8 @@ __global__ void k_mindt_begin(View v, int ndisk){
    if( dt0 <= 0.0 ) dt0 = 1.0e100;
    v.ds[d].dtmin = dbits(dt0);
 }
-__global__ void k_mindt_end(View v, int ndisk){
+template<class R>
+__global__ void k_mindt_end(ViewT<R> v, int ndisk){
    int d = blockIdx.x*blockDim.x + threadIdx.x;
    if( d >= ndisk ) return;
    double mn = __longlong_as_double((long long)v.ds[d].dtmin);

@@ -1,0 +1,86 @@
+"""The mixed-precision form (DISCO_PREC_MIXED) against the FP64 path.
+
+FP32 prim, PLM slopes and Riemann fluxes (with FMA); FP64 phi positions, mesh
+motion, face endpoints, dt reduction and a Kahan-compensated conserved
+update.  Stated tolerance after 100 steps of config 0: relative L1 <= 1e-5 on
+density, pressure, Omega and the passive scalar; v_r (zero in equilibrium,
+so its own L1 is noise-sized) is measured against |v|.  With an analytic mesh
+(Mesh_Motion 4) the face positions never see the FP32 state, so the face
+topology is bit-identical to the FP64 run; with the by-cell mesh (Mesh_Motion
+1) it is compared too.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import disco_b200 as db
+from helpers import par_with, rel_l1
+
+pytestmark = pytest.mark.gpu
+
+TOL_MIXED = 1e-5
+
+
+def _pair(overrides, nsteps):
+    _, opt = db.template_paths("c0_kepler2d")
+    p = par_with(overrides)
+    disk = db.Disk.from_files(p, opt)
+    os.unlink(p)
+    a = db.Batch([disk], precision=db.PREC_FP64)
+    m = db.Batch([disk], precision=db.PREC_MIXED)
+    a.run(nsteps)
+    m.run(nsteps)
+    a.sync()
+    m.sync()
+    return disk, a, m
+
+
+def _field_errors(disk, sa, sm):
+    r = disk.real == 1
+    pa, pm = sa["prim"][r], sm["prim"][r]
+    vmag = np.abs(pa[:, 2]) + np.abs(pa[:, 3] * 1.0)
+    return {
+        "rho": rel_l1(pm[:, 0], pa[:, 0]),
+        "P": rel_l1(pm[:, 1], pa[:, 1]),
+        "vr_over_v": float(np.sum(np.abs(pm[:, 2] - pa[:, 2])) / np.sum(vmag)),
+        "omega": rel_l1(pm[:, 3], pa[:, 3]),
+        "X": rel_l1(pm[:, 5], pa[:, 5]),
+        "mass": abs(sm["cons"][r, 0].sum() / sa["cons"][r, 0].sum() - 1.0),
+    }
+
+
+def test_mixed_config0_analytic_mesh_faces_bitexact():
+    # Max_DT below every cell's CFL step makes dt = Max_DT in both runs, so the
+    # analytic mesh moves identically and the face lists must match bit for bit
+    disk, a, m = _pair({"Mesh_Motion": 4, "Exact_Mesh_Omega": 2, "Max_DT": 0.01}, 100)
+    sa, sm = a.get_cells(), m.get_cells()
+    assert np.array_equal(sa["piph"], sm["piph"])
+    assert np.array_equal(sa["dphi"], sm["dphi"])
+    fa, fm = a.faces(0, 1), m.faces(0, 1)
+    for k in ("fIndex", "iL", "iR", "LRtype"):
+        assert np.array_equal(fa[k], fm[k]), k
+    err = _field_errors(disk, sa, sm)
+    assert max(err.values()) < TOL_MIXED, err
+    assert abs(m.time()[0] / a.time()[0] - 1) < TOL_MIXED
+
+
+def test_mixed_config0_cell_mesh():
+    disk, a, m = _pair({}, 100)
+    sa, sm = a.get_cells(), m.get_cells()
+    err = _field_errors(disk, sa, sm)
+    assert max(err.values()) < TOL_MIXED, err
+    fa, fm = a.faces(0, 1), m.faces(0, 1)
+    assert np.array_equal(fa["fIndex"], fm["fIndex"])
+    mism = int(np.sum((fa["iL"] != fm["iL"]) | (fa["iR"] != fm["iR"])))
+    assert mism == 0, mism
+
+
+def test_mixed_state_is_float32():
+    disk, a, m = _pair({"Num_R": 16}, 2)
+    sm = m.get_cells()
+    r = disk.real == 1
+    p = sm["prim"][r]
+    assert np.array_equal(p, p.astype(np.float32).astype(np.float64))
+    g = m.debug_array(0)
+    assert np.array_equal(g, g.astype(np.float32).astype(np.float64))
