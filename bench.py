@@ -203,6 +203,105 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+C2P_GRID = {"Nr": 192, "Nz": 96, "Np": 462, "rmin": 1.5, "rmax": 50.0, "zmin": -20.0, "zmax": 20.0}
+C2P_TOL, C2P_NEXTRA, C2P_MAXIT = 1e-10, 10, 30
+C2P_BYTES = 8 * (9 + 3 + 5 + 9)         # read cons, x, the 5 prims of the warm start; write prims
+
+
+def c2p_leg(args, local, stream):
+    """GRMHD cons -> prim on the torus workload (Kerr-KS a = 0.9): the
+    network is trained on pairs written by plain solves of four perturbation
+    sizes, then plain (previous prims) and learned guesses are timed on fresh
+    states, both finished by Newton to |d eta/eta| < 1e-10 with the
+    reference's tail of 10 and cap of 30."""
+    import numpy as np
+    import torch
+    from disco_b200.gr import GR
+
+    g = C2P_GRID
+    gr = GR(device=local, metric="kerr", a=0.9, tol=C2P_TOL, nextra=C2P_NEXTRA, max_iter=C2P_MAXIT)
+    gr.set_stream(stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    out = {"workload": "GRMHD torus, Kerr-KS a=0.9, %dx%dx%d cells (r %.1f-%.0f log, z +-%.0f)" %
+                       (g["Nr"], g["Nz"], g["Np"], g["rmin"], g["rmax"], g["zmax"]),
+           "tol": C2P_TOL, "nextra": C2P_NEXTRA, "max_iter": C2P_MAXIT}
+    with torch.cuda.stream(stream):
+        x = gr.grid(g["Nr"], g["Nz"], g["Np"], g["rmin"], g["rmax"], g["zmin"], g["zmax"])
+        p0 = gr.torus(x)
+        n = x.shape[1]
+        out["ncell"] = n
+        pairs = []
+        for seed, eps in ((101, 1e-3), (102, 3e-2), (103, 0.1), (104, 0.3)):
+            cons = gr.prim2cons(gr.perturb(p0, seed, eps), x)
+            pr = p0.clone()
+            pairs.append(gr.cons2prim(cons, x, pr, pairs=True, stats=False)["pairs"])
+            del cons, pr
+        pairs = torch.cat(pairs)
+        gr.mlp_init(3)
+        gr.mlp_fit_norm(pairs)
+        steps, batch = 3000, 8192
+        ev[0].record(stream)
+        hist = gr.mlp_train(pairs, steps=steps, batch=batch, lr=2e-3, seed=9)
+        ev[1].record(stream)
+        ev[1].synchronize()
+        out["train"] = {"pairs": int(pairs.shape[0]), "steps": steps, "batch": batch,
+                        "ms": ev[0].elapsed_time(ev[1]), "loss_first": float(hist[:10].mean()),
+                        "loss_last": float(hist[-50:].mean())}
+        del pairs
+        # the same network in a solver without the tail (tol only)
+        gr0 = GR(device=local, metric="kerr", a=0.9, tol=C2P_TOL, nextra=0, max_iter=C2P_MAXIT)
+        gr0.set_stream(stream)
+        gr0.mlp_set(*gr.mlp_get())
+        work = torch.empty_like(p0)
+        hbm, _ = peaks()
+        for name, eps in (("warm", 1e-3), ("jump", 0.3)):
+            cons = gr.prim2cons(gr.perturb(p0, 777, eps), x)
+            for solver, tail in ((gr, ""), (gr0, "_tail0")):
+                row = {"eps": eps, "nextra": C2P_NEXTRA if solver is gr else 0}
+                for guess, key in (("previous", "plain"), ("learned", "learned")):
+                    ts = []
+                    for r in range(4):
+                        work.copy_(p0)
+                        ev[0].record(stream)
+                        solver.cons2prim(cons, x, work, guess=guess, stats=False)
+                        ev[1].record(stream)
+                        ev[1].synchronize()
+                        if r:
+                            ts.append(ev[0].elapsed_time(ev[1]))
+                    work.copy_(p0)
+                    rep = solver.cons2prim(cons, x, work, guess=guess)
+                    ms = statistics.median(ts)
+                    gbs = C2P_BYTES * n / (ms / 1e3) / 1e9
+                    row[key] = {"ms": ms, "cells_per_s": n / (ms / 1e3), "iters_mean": rep["iters_mean"],
+                                "iters_max": rep["iters_max"], "n_fallback": rep["n_fallback"],
+                                "n_fail": rep["n_fail"], "hbm_gbs": gbs, "hbm_frac": gbs / hbm}
+                row["learned_speedup"] = row["plain"]["ms"] / row["learned"]["ms"]
+                row["learned_iteration_ratio"] = row["learned"]["iters_mean"] / row["plain"]["iters_mean"]
+                out[name + tail] = row
+            del cons
+        del gr0
+        out["bytes_per_cell"] = C2P_BYTES
+        # CPU baseline: the oracle restatement (same tol/tail/cap), one core,
+        # on the first 50k cells of the warm case
+        if not args.no_cpu_baseline:
+            try:
+                from oracle import pyc2p
+                m = 50000
+                xs = x[:, :m].T.cpu().numpy().copy()
+                pp = p0[:, :m].T.cpu().numpy().copy()
+                cs = gr.prim2cons(gr.perturb(p0, 777, 1e-3), x)[:, :m].T.cpu().numpy().copy()
+                orc = pyc2p.C2POracle(metric=1, a=0.9, tol=C2P_TOL, nextra=C2P_NEXTRA, max_iter=C2P_MAXIT)
+                t0 = time.perf_counter()
+                orc.cons2prim(cs, xs, pp)
+                dt = time.perf_counter() - t0
+                out["cpu_baseline"] = {"value": m / dt, "unit": "cells/s", "cores": 1, "kind": "port",
+                                       "sample": "%d cells of the warm case, oracle restatement" % m}
+            except Exception as ex:
+                out["cpu_baseline"] = {"value": None, "sample": "unavailable: %s" % ex}
+    del gr
+    return out
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -333,6 +432,11 @@ def run_ours(args, world, rank, local):
                  "precision": "FP32 prim/slopes/fluxes, FP64 mesh/dt/Kahan cons"}
         bm.close()
 
+    c2p = None
+    if not args.no_c2p:
+        c2p = c2p_leg(args, local, stream)
+        barrier()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -366,6 +470,7 @@ def run_ours(args, world, rank, local):
                     "d2h_bytes_per_step": (d2h + 8 * len(disks) * args.steps) / args.steps},
             "gpu_launches": launches_per_step * args.steps,
             "mixed_form": mixed,
+            "c2p": c2p,
             "clocks": ck,
             "cpu_baseline": cpu,
         }
@@ -384,6 +489,7 @@ def main():
     ap.add_argument("--workload", default="ragged64", choices=["ragged64", "ragged8", "config0"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
+    ap.add_argument("--no-c2p", action="store_true", help="skip the GRMHD cons->prim leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -285,18 +285,32 @@ void orc_gr_newton_from(long n, const double *cons, const double *x, const doubl
    }
 }
 
-/* The network's 8 raw features from a state's invariants and warm start:
- * log D, log e, log1p s2, log1p Q, log1p|psi|, alpha, v2_0, log eta_0 */
+/* The network's 8 raw features of a state and its warm start: log e,
+ * log(1+s2), log(1+Q), log(1+|psi|), log eta_0, log sigma, ra/sigma,
+ * rb/sigma, with ra = fa/(eta_0+Q)^2 and rb = fb/eta_0 the scaled Newton
+ * residuals (grmhd2.c:1185-1187) at the warm start and sigma = |ra| + |rb|
+ * + 1e-14; sig (nullable) receives sigma and warm (nullable, 2 per state)
+ * the warm start (v2_0, eta_0).  Float logs, as the device. */
 void orc_gr_features(long n, const double *cons, const double *x, const double *prim,
-                     float *feat){
+                     float *feat, double *sig, double *warm){
    long i;
    for( i=0 ; i<n ; ++i ){
       geo_t g; inv_t I; float *f = feat + 8*i;
+      double v2, eta, w, fa, fb, ra, rb, sg;
       geo_at(x + 3*i, &g);
       invariants(cons + 9*i, prim + 9*i, x + 3*i, &g, &I);
-      f[0] = (float)log(I.D); f[1] = (float)log(I.e); f[2] = (float)log1p(I.s2);
-      f[3] = (float)log1p(I.Q); f[4] = (float)log1p(fabs(I.psi)); f[5] = (float)g.al;
-      f[6] = (float)I.v20; f[7] = (float)log(I.eta0);
+      v2 = I.v20; eta = I.eta0;
+      w = 1.0/sqrt(1.0-v2);
+      fa = (eta+I.Q)*(eta+I.Q)*v2 - I.psi*(2*eta+I.Q)/(eta*eta) - I.s2;
+      fb = eta - I.n*(1-v2)*(eta-w) + 0.5*I.Q*(1+v2) - 0.5*I.psi/(eta*eta) - I.e;
+      ra = fa/((eta+I.Q)*(eta+I.Q));
+      rb = fb/eta;
+      sg = fabs(ra) + fabs(rb) + 1e-14;
+      f[0] = logf((float)I.e); f[1] = logf(1.0f + (float)I.s2); f[2] = logf(1.0f + (float)I.Q);
+      f[3] = logf(1.0f + (float)fabs(I.psi)); f[4] = logf((float)eta);
+      f[5] = logf((float)sg); f[6] = (float)(ra/sg); f[7] = (float)(rb/sg);
+      if( sig ) sig[i] = sg;
+      if( warm ){ warm[2*i] = v2; warm[2*i+1] = eta; }
    }
 }
 

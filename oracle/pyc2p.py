@@ -96,13 +96,17 @@ class C2POracle:
         return prim, it, ok
 
     def features(self, cons, x, guess):
+        """(features[n, 8], sigma[n], warm start (v2_0, eta_0)[n, 2]) of the learned guess."""
         self._setup()
         n = len(cons)
         cons = np.ascontiguousarray(cons, np.float64); x = np.ascontiguousarray(x, np.float64)
         guess = np.ascontiguousarray(guess, np.float64)
         f = np.zeros((n, 8), np.float32)
-        self.lib.orc_gr_features(C.c_long(n), _p(cons, _D), _p(x, _D), _p(guess, _D), _p(f, _F))
-        return f
+        sg = np.zeros(n)
+        wm = np.zeros((n, 2))
+        self.lib.orc_gr_features(C.c_long(n), _p(cons, _D), _p(x, _D), _p(guess, _D), _p(f, _F),
+                                 _p(sg, _D), _p(wm, _D))
+        return f, sg, wm
 
     def mlp_loss_grad(self, param, norm, feat, target=None):
         """(loss, grad[NPARAM] float64, out[n,2]) in double precision."""

@@ -72,8 +72,19 @@ def test_mixed_config0_cell_mesh():
     assert max(err.values()) < TOL_MIXED, err
     fa, fm = a.faces(0, 1), m.faces(0, 1)
     assert np.array_equal(fa["fIndex"], fm["fIndex"])
-    mism = int(np.sum((fa["iL"] != fm["iL"]) | (fa["iR"] != fm["iR"])))
-    assert mism == 0, mism
+    # The by-cell mesh moves with the FP32 state, so a track's list may start
+    # at a different cell (I0 is the first cell past phi = 0, and an edge
+    # within rounding of 0 can land on either side); its faces, the cell
+    # pairs each track connects, must be the same.
+    order = int(np.sum((fa["iL"] != fm["iL"]) | (fa["iR"] != fm["iR"])))
+    fi = fa["fIndex"]
+    differ = 0
+    for t in range(len(fi) - 1):
+        sa = sorted(zip(fa["iL"][fi[t]:fi[t + 1]], fa["iR"][fi[t]:fi[t + 1]], fa["LRtype"][fi[t]:fi[t + 1]]))
+        sb = sorted(zip(fm["iL"][fi[t]:fi[t + 1]], fm["iR"][fi[t]:fi[t + 1]], fm["LRtype"][fi[t]:fi[t + 1]]))
+        differ += sum(p != q for p, q in zip(sa, sb))
+    print("faces listed in a different order: %d of %d; different faces: %d" % (order, fi[-1], differ))
+    assert differ == 0, (order, differ)
 
 
 def test_mixed_state_is_float32():
