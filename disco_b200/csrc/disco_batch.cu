@@ -78,6 +78,11 @@ static void fill_disk_params(DiskParams &D, const disco_params &p, const disco_m
    D.ic.rmin = p.rmin; D.ic.rmax = p.rmax; D.ic.phimax = p.phimax;
    D.ic.seed = (uint64_t)(int64_t)p.initPar0;
    D.ic.kind = (int)p.initPar[2];
+   D.ic_module = m.initial == DISCO_IC_MHD_SHEAR_NOISE ? 1 : 0;
+   D.ic_mhd.seed = (uint64_t)(int64_t)p.initPar0; D.ic_mhd.amp = p.initPar[1];
+   D.ic_mhd.cs = p.initPar[3]; D.ic_mhd.beta = p.initPar[4]; D.ic_mhd.gam = p.Adiabatic_Index;
+   D.ic_mhd.rmin = p.rmin; D.ic_mhd.rmax = p.rmax; D.ic_mhd.zmin = p.zmin; D.ic_mhd.zmax = p.zmax;
+   D.ic_mhd.phimax = p.phimax; D.ic_mhd.kind = (int)p.initPar[2];
 }
 
 static void init_planets(DiskState &S, DiskParams &D, const disco_params &p, const disco_modules &m){
@@ -126,17 +131,27 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    if( cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1 ) return DISCO_ERR_NO_DEVICE;
    if( device < 0 || device >= ndev ) return DISCO_ERR_ARG;
    if( precision != DISCO_PREC_FP64 && precision != DISCO_PREC_MIXED ) return DISCO_ERR_ARG;
-   if( mods->hydro != DISCO_HYDRO_EULER || mods->num_c != 5 || mods->num_n != 1 ||
-       mods->ct_mode != 0 )
+   /* euler (NUM_C 5) or mhd (NUM_C 8), NUM_N 1.  Constrained transport
+    * (in.par Constrained_Transport) is not built: B evolves through the
+    * fluxes.  CT_MODE 1/2 only sizes the reference's face-flux storage,
+    * which without Constrained_Transport never reaches the cells; MHD
+    * builds need it (with CT_MODE 0, flip_fluxes, bfields.c:760-814, writes
+    * through zero-length Phi arrays into the cell's real flag and the next
+    * cell's prims), so it is accepted. */
+   bool mhd = mods->hydro == DISCO_HYDRO_MHD;
+   if( !((mods->hydro == DISCO_HYDRO_EULER && mods->num_c == 5) || (mhd && mods->num_c == 8)) ||
+       mods->num_n != 1 || mods->ct_mode < 0 || mods->ct_mode > 2 )
       return DISCO_ERR_UNSUPPORTED;
+   for( int d=0 ; d<ndisk ; ++d ) if( params[d].CT ) return DISCO_ERR_UNSUPPORTED;
    if( mods->boundary != DISCO_BC_FIXED ) return DISCO_ERR_UNSUPPORTED;
-   if( mods->initial != DISCO_IC_KEPLER_NOISE ) return DISCO_ERR_UNSUPPORTED;
+   if( mods->initial != DISCO_IC_KEPLER_NOISE && mods->initial != DISCO_IC_MHD_SHEAR_NOISE )
+      return DISCO_ERR_UNSUPPORTED;
    for( int d=0 ; d<ndisk ; ++d ){
       if( Nz[d] != 1 ) return DISCO_ERR_UNSUPPORTED;          /* 3D: z faces not built */
       if( Nr[d] < 2 ) return DISCO_ERR_ARG;
       if( params[d].Timestep != params[0].Timestep ) return DISCO_ERR_ARG;
       if( params[d].R_Periodic ) return DISCO_ERR_UNSUPPORTED;
-      if( params[d].Riemann_Solver > 1 ) return DISCO_ERR_UNSUPPORTED;
+      if( params[d].Riemann_Solver > (mhd ? 2 : 1) ) return DISCO_ERR_UNSUPPORTED;   /* HLLD needs B */
       if( params[d].visc_flag || params[d].RotFrame ) return DISCO_ERR_UNSUPPORTED;
    }
    CK(cudaSetDevice(device));
@@ -339,7 +354,7 @@ extern "C" int disco_batch_set_cells(disco_batch *b, const double *prim, const d
    if( prim && !cons ){
       unsigned ncb = (unsigned)b->cblk.size();
       if( b->prec == DISCO_PREC_MIXED ) mixed_launch_prim2cons(b);
-      else k_prim2cons<6,5,double><<<ncb, CB, 0, b->stream>>>(b->vd);
+      else launch_prim2cons_t(b, b->vd);
       CK(cudaGetLastError());
    }
    CK(cudaStreamSynchronize(b->stream));

@@ -9,7 +9,7 @@ void mixed_launch_mindt(disco_batch *b){ launch_mindt_t(b, b->vf); }
 void mixed_launch_setup(disco_batch *b){ launch_setup_t(b, b->vf); }
 void mixed_launch_step(disco_batch *b, int use_next){ launch_step_t(b, b->vf, use_next); }
 void mixed_launch_prim2cons(disco_batch *b){
-   k_prim2cons<6,5,float><<<(unsigned)b->cblk.size(), CB, 0, b->stream>>>(b->vf);
+   launch_prim2cons_t(b, b->vf);
 }
 void mixed_launch_faces(disco_batch *b){
    k_I0<float><<<nblk((size_t)b->vf.Nann*32, 128), 128, 0, b->stream>>>(b->vf);

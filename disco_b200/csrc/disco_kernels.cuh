@@ -439,6 +439,10 @@ __global__ void __launch_bounds__(FB) k_flux_r(ViewT<R> v){
       primL[q] = v.prim[q*N+cL] + v.gradr[q*N+cL]*dxL + v.gradp[q*N+cL]*dpL;
       primR[q] = v.prim[q*N+cR] - v.gradr[q*N+cR]*dxR - v.gradp[q*N+cR]*dpR;
    }
+   if constexpr ( NC == 8 ){                     /* normal B averaged, riemann.c:146-152 */
+      R Bavg = R(.5)*(primL[BRR]+primR[BRR]);
+      primL[BRR] = Bavg; primR[BRR] = Bavg;
+   }
    int j = v.tr_j[t];
    const double *rj = v.rj + P.rj0 + 1;
    double r = .5*(rj[j]+rj[j]);                 /* face cm[0] */
@@ -476,6 +480,10 @@ __global__ void __launch_bounds__(CB) k_flux_p(ViewT<R> v){
    for( int q=0 ; q<Q ; ++q ){
       primL[q] = v.prim[q*N+cL] + R(.5)*v.gradp[q*N+cL]*dL;
       primR[q] = v.prim[q*N+cR] - R(.5)*v.gradp[q*N+cR]*dR;
+   }
+   if constexpr ( NC == 8 ){                     /* B_phi averaged, riemann.c:54-58 */
+      R Bp = R(.5)*(primL[BPP]+primR[BPP]);
+      primL[BPP] = Bp; primR[BPP] = Bp;
    }
    double w = r*v.wiph[cL];
    R G[Q];
@@ -557,7 +565,26 @@ __global__ void __launch_bounds__(CB) k_update(ViewT<R> v, int first){
       double dV = dV_of(rp, rm, dph, zp, zm);
       double dVdt = dV*dt;
       double r = centroid_r(rp, rm);
-      {  /* euler source, euler.c:171-215 */
+      if constexpr ( NC == 8 ){  /* mhd source, mhd.c:225-263 */
+         double rho = prim[RHO], Pp = prim[PPP];
+         double r_1 = .5*(rp+rm);
+         double r2_3 = (rp*rp + rp*rm + rm*rm)/3.;
+         double vr = prim[URR], omega = prim[UPP];
+         double Br = prim[BRR], Bp = prim[BPP], Bz = prim[BZZ];
+         double B2 = Br*Br+Bp*Bp+Bz*Bz;
+         double centrifugal;
+         if( P.polar ){
+            centrifugal = ( rho*omega*omega*r2_3 )/r_1*sin(.5*dph)/(.5*dph);
+            centrifugal -= Bp*Bp/r_1;
+         }else{
+            centrifugal = rho*omega*omega*r - Bp*Bp/r;
+         }
+         double press_bal = (Pp+.5*B2)/r_1;
+         acc<R>(cons[SRR], cc[SRR], dVdt*( centrifugal + press_bal ));
+         double om = v.ann_om[a];
+         double om1 = v.ann_om1[a];
+         acc<R>(cons[TAU], cc[TAU], dVdt*rho*vr*( om*om*r2_3/r_1 - om1*(omega-om)*r2_3 ));
+      }else{  /* euler source, euler.c:171-215 */
          double rho = prim[RHO], Pp = prim[PPP];
          double r_1 = .5*(rp+rm);
          double vr = prim[URR], omega = prim[UPP], vz = prim[UZZ];
@@ -657,12 +684,16 @@ __global__ void __launch_bounds__(CB) k_c2p(ViewT<R> v, int last, int bc_fixed){
          }
       }
       if( last ){
-         if( real ){                              /* mindt, euler.c:332-380 */
+         if( real ){                              /* mindt, euler.c:332-380, mhd.c:452-486 */
             int cprev = c0 + (i == 0 ? np-1 : i-1);
             double w = .5*(v.wiph[cprev] + v.wiph[c]);
             double r = centroid_r(rp, rm);
             double vp = (prim[UPP]-w)*r;
             double cs = sqrt(P.gam*prim[PPP]/prim[RHO]);
+            if constexpr ( NC == 8 ){
+               double b2 = (prim[BRR]*prim[BRR]+prim[BPP]*prim[BPP]+prim[BZZ]*prim[BZZ])/prim[RHO];
+               cs = sqrt(cs*cs + b2);
+            }
             double maxvr = cs + fabs(prim[URR]);
             double maxvp = cs + fabs(vp);
             double maxvz = cs + fabs(prim[UZZ]);
@@ -925,7 +956,7 @@ __global__ void k_wmean_nomove(ViewT<R> v){
 }
 
 /* Stand-alone getmindt (misc.c:39-84) into ds[d].dtmin. */
-template<int Q, class R>
+template<int Q, int NC, class R>
 __global__ void __launch_bounds__(CB) k_mindt(ViewT<R> v){
    __shared__ unsigned long long s_dt[CB/32];
    int2 b = v.cblk[blockIdx.x];
@@ -950,6 +981,11 @@ __global__ void __launch_bounds__(CB) k_mindt(ViewT<R> v){
       double r = centroid_r(rp, rm);
       double vp = ((double)v.prim[UPP*N+c]-w)*r;
       double cs = sqrt(P.gam*(double)v.prim[PPP*N+c]/(double)v.prim[RHO*N+c]);
+      if constexpr ( NC == 8 ){                  /* mhd.c:452-486: fast speed */
+         double Br = v.prim[BRR*N+c], Bp = v.prim[BPP*N+c], Bz = v.prim[BZZ*N+c];
+         double b2 = (Br*Br+Bp*Bp+Bz*Bz)/(double)v.prim[RHO*N+c];
+         cs = sqrt(cs*cs + b2);
+      }
       double maxvr = cs + fabs((double)v.prim[URR*N+c]);
       double maxvp = cs + fabs(vp);
       double maxvz = cs + fabs((double)v.prim[UZZ*N+c]);

@@ -1,0 +1,92 @@
+/*
+ * Magnetised Keplerian shearing disk with seeded, hash-based velocity noise.
+ *
+ * A new initial-condition module for the MHD workloads (the reference's MHD
+ * disk ICs, e.g. Initial/flock.c, draw their noise from rand() in cell
+ * order, which a device cannot evaluate per cell).  Like kepler_noise, the
+ * noise is a pure function of the cell position, so the host build, the
+ * device set-up and the boundary kernels agree for the same x.
+ *
+ *   rho   = 1
+ *   P     = rho cs^2 / gamma                      (sound speed cs)
+ *   Omega = r^-3/2 + amp cs u_phi / r
+ *   v_r   = amp cs u_r,   v_z = amp cs u_z        (u in [-1,1), hashed)
+ *   B     = (0, 0, Bz),   Bz = sqrt(2 P / beta)   (vertical field, plasma beta)
+ *   X     = (z - zmin)/(zmax - zmin)              (passive scalar, NUM_N>0)
+ *
+ * With Init_Par2 = 1 the disk rotates rigidly instead (Omega = 1 + noise),
+ * held by pressure, P = rho cs^2/gamma + r^2/2, so no gravity is needed:
+ * with PLANETS = none and Energy_Omega 0 a step calls no libm function
+ * whose value matters, and a CPU and a GPU build agree bit for bit.
+ *
+ * Noise only inside [rmin, rmax] x [zmin, zmax] (ghost cells stay smooth).
+ * Uses +,-,*,/ and sqrt only, so host and device values are bit-identical.
+ *
+ * Parameters (in.par): Init_Par0 = seed, Init_Par1 = amp (fraction of cs),
+ * Init_Par2 = kind (0 Keplerian, 1 rigid), Init_Par3 = cs, Init_Par4 = beta,
+ * Adiabatic_Index, R_Min/R_Max,
+ * Z_Min/Z_Max, Phi_Max.
+ */
+#ifndef DISCO_IC_MHD_SHEAR_H
+#define DISCO_IC_MHD_SHEAR_H
+
+#include "ic_kepler_noise.h"
+
+typedef struct {
+   double cs, beta, amp, gam;
+   double rmin, rmax, zmin, zmax, phimax;
+   uint64_t seed;
+   int kind;
+   int pad;
+} disco_ic_mhd_shear;
+
+/* Uniform in [-1,1) from the seed, a salt and the cell position (r, phi, z
+ * bucketed as disco_hash_unit does). */
+DISCO_HD double disco_hash_unit3(uint64_t seed, uint64_t salt, double r, double phi, double z,
+                                 double phimax){
+   int64_t qr = (int64_t)(r * 1048576.0);
+   int64_t qp = (int64_t)((phi / phimax) * 16777216.0);
+   int64_t qz = (int64_t)((z + 1024.0) * 1048576.0);
+   uint64_t h = disco_mix64(seed ^ disco_mix64(salt * 0x9E3779B97F4A7C15ull
+                                               ^ (uint64_t)qr * 0x100000001B3ull
+                                               ^ ((uint64_t)qp << 1)
+                                               ^ ((uint64_t)qz << 29)));
+   double u = (double)(h >> 11) * (1.0 / 9007199254740992.0);
+   return 2.0 * u - 1.0;
+}
+
+/* prim layout: RHO, PPP, URR, UPP, UZZ, BRR, BPP, BZZ, passive... */
+DISCO_HD void disco_ic_mhd_shear_eval(const disco_ic_mhd_shear *p, int num_c, int num_q,
+                                      double *prim, const double *x){
+   double r = x[0], phi = x[1], z = x[2];
+   double sr = sqrt(r);
+   double omega = 1.0 / (r * sr);
+   double rho = 1.0;
+   double press = rho * p->cs * p->cs / p->gam;
+   if( p->kind == 1 ){
+      omega = 1.0;
+      press = press + 0.5 * r * r;
+   }
+   double vr = 0.0, vz = 0.0;
+   if( r >= p->rmin && r <= p->rmax && z >= p->zmin && z <= p->zmax && p->amp != 0.0 ){
+      double a = p->amp * p->cs;
+      vr = a * disco_hash_unit3(p->seed, 1, r, phi, z, p->phimax);
+      vz = a * disco_hash_unit3(p->seed, 2, r, phi, z, p->phimax);
+      omega += a * disco_hash_unit3(p->seed, 3, r, phi, z, p->phimax) / r;
+   }
+   prim[0] = rho;
+   prim[1] = press;
+   prim[2] = vr;
+   prim[3] = omega;
+   prim[4] = vz;
+   int q;
+   for( q=5 ; q<num_c ; ++q ) prim[q] = 0.0;
+   if( num_c >= 8 ) prim[7] = sqrt(2.0 * (rho * p->cs * p->cs / p->gam) / p->beta);
+   if( num_q > num_c ){
+      double zr = p->zmax > p->zmin ? (z - p->zmin) / (p->zmax - p->zmin) : 0.5;
+      prim[num_c] = zr;
+      for( q=num_c+1 ; q<num_q ; ++q ) prim[q] = 0.0;
+   }
+}
+
+#endif

@@ -35,7 +35,18 @@ CASES = {
     # libm-free: rigid rotation held by pressure, no gravity, lab energy frame
     "c0_rigid": ("c0_nograv", {"Num_R": 20, "Log_Zoning": 0, "Init_Par2": 1,
                                "Energy_Omega": 0, "Mach_Number": 5.0}, 8),
+    # Newtonian MHD (mhd.c, no CT): HLLD, HLLC-MHD and HLL + forward Euler
+    "c1_mhd_hlld": ("c1_mhd2d", {}, 8),
+    "c1_mhd_hllc": ("c1_mhd2d", {"Num_R": 12, "Riemann_Solver": 1, "Init_Par0": 99}, 6),
+    "c1_mhd_hll_fe": ("c1_mhd2d", {"Num_R": 10, "Riemann_Solver": 0, "Timestep": 1,
+                                   "Mesh_Motion": 1, "Init_Par1": 0.05}, 6),
+    # libm-free MHD: rigid rotation held by pressure, no gravity, HLLD
+    "c1_mhd_rigid": ("c1_mhd2d_nograv", {"Num_R": 14, "Init_Par2": 1, "Init_Par4": 10.0}, 8),
 }
+
+# the in.par template each module configuration starts from
+BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": "c0_kepler2d",
+            "c1_mhd2d": "c1_mhd2d", "c1_mhd2d_nograv": "c1_mhd2d"}
 
 
 def par_text(cfg_par, overrides):
@@ -51,8 +62,11 @@ def par_text(cfg_par, overrides):
 
 
 def main():
+    only = set(sys.argv[1:])
     for case, (cfg, over, n) in CASES.items():
-        text = par_text("c0_kepler2d", over)
+        if only and case not in only:
+            continue
+        text = par_text(BASE_PAR[cfg], over)
         with open(os.path.join(HERE, case + ".par"), "w") as f:
             f.write(text)
         d0 = pyoracle.run_ref(cfg, text, 0)
