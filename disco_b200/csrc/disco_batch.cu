@@ -114,6 +114,7 @@ static void make_float_view(disco_batch *b){
    ViewT<float> &f = b->vf;
    memcpy(&f, &d, sizeof f);
    f.prim = (float *)d.prim; f.gradp = (float *)d.gradp; f.gradr = (float *)d.gradr;
+   f.gradz = (float *)d.gradz;
    f.fS = (float *)d.fS; f.fG = (float *)d.fG; f.Gp = (float *)d.Gp;
 }
 
@@ -143,11 +144,12 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
        mods->num_n != 1 || mods->ct_mode < 0 || mods->ct_mode > 2 )
       return DISCO_ERR_UNSUPPORTED;
    for( int d=0 ; d<ndisk ; ++d ) if( params[d].CT ) return DISCO_ERR_UNSUPPORTED;
-   if( mods->boundary != DISCO_BC_FIXED ) return DISCO_ERR_UNSUPPORTED;
+   if( mods->boundary != DISCO_BC_FIXED && mods->boundary != DISCO_BC_ZEROGRAD &&
+       mods->boundary != DISCO_BC_FIXED3D )
+      return DISCO_ERR_UNSUPPORTED;
    if( mods->initial != DISCO_IC_KEPLER_NOISE && mods->initial != DISCO_IC_MHD_SHEAR_NOISE )
       return DISCO_ERR_UNSUPPORTED;
    for( int d=0 ; d<ndisk ; ++d ){
-      if( Nz[d] != 1 ) return DISCO_ERR_UNSUPPORTED;          /* 3D: z faces not built */
       if( Nr[d] < 2 ) return DISCO_ERR_ARG;
       if( params[d].Timestep != params[0].Timestep ) return DISCO_ERR_ARG;
       if( params[d].R_Periodic ) return DISCO_ERR_UNSUPPORTED;
@@ -159,10 +161,14 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->device = device; b->mods = *mods; b->prec = precision; b->ndisk = ndisk;
    b->NC = mods->num_c; b->Q = mods->num_c + mods->num_n;
    b->timestep_mode = params[0].Timestep == 1 ? 1 : 0;
-   b->bc_fixed = mods->boundary == DISCO_BC_FIXED;
+   b->bc_fixed = mods->boundary == DISCO_BC_FIXED ? 1 : mods->boundary == DISCO_BC_FIXED3D ? 2 : 0;
+   b->bc_zerograd = mods->boundary == DISCO_BC_ZEROGRAD;
+   b->d_zg_pairs = NULL;
+   b->zg_smem = 0;
    b->nq = mods->analysis == DISCO_DIAG_DISK2D ? 5 : 0;
    b->params.assign(params, params + ndisk);
    b->any_mm3 = 0;
+   b->any_3d = 0;
    b->graph = NULL;
    b->have_cells = 0;
    b->stream = NULL;
@@ -220,6 +226,31 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
          double rp = 2.0*(rj[j+1]*rj[j+1] + rj[j+1]*rj[j] + rj[j]*rj[j]) / (3.0*(rj[j+1]+rj[j]));
          b->tr_dxL.push_back(rj[j] - rm);
          b->tr_dxR.push_back(rp - rj[j]);
+         b->tr_dim.push_back(1);
+         int nf = b->ann_np[A] + b->ann_np[B];
+         for( int f0=0 ; f0<nf ; f0+=FB ) b->fblk.push_back(make_int2(t, f0));
+         face += nf;
+      }
+      /* z tracks (faces_alt.c:83-100 with dim 2): Nr*(Nz-1) tracks, track
+       * JK = j + Nr*k joins (j,k) and (j,k+1) */
+      D.trz0 = (int)b->tr_a.size();
+      D.ntrz = nr*(nz-1);
+      if( nz > 1 ) b->any_3d = 1;
+      const double *zkp = z_kph + zoff + 1;
+      int kminz = D.NgZa == 0 ? 0 : D.NgZa-1;           /* trans_flux dim 2, misc.c:474-489 */
+      int kmaxz = D.NgZb == 0 ? nz-1 : nz-D.NgZb;
+      for( int k=0 ; k<nz-1 ; ++k ) for( int j=0 ; j<nr ; ++j ){
+         int t = (int)b->tr_a.size();
+         int A = D.ann0 + j + nr*k, B = A + nr;
+         b->tr_a.push_back(A); b->tr_b.push_back(B); b->tr_off.push_back(face);
+         b->tr_j.push_back(j); b->tr_k.push_back(k);
+         b->tr_flux.push_back(j >= D.NgRa && j < nr-D.NgRb && k >= kminz && k < kmaxz);
+         /* dxL/dxR, faces_alt.c:119-125 */
+         double zm = 0.5*(zkp[k]+zkp[k-1]);
+         double zp = 0.5*(zkp[k+1]+zkp[k]);
+         b->tr_dxL.push_back(zkp[k] - zm);
+         b->tr_dxR.push_back(zp - zkp[k]);
+         b->tr_dim.push_back(2);
          int nf = b->ann_np[A] + b->ann_np[B];
          for( int f0=0 ; f0<nf ; f0+=FB ) b->fblk.push_back(make_int2(t, f0));
          face += nf;
@@ -232,6 +263,49 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->tr_off.push_back(face);
    b->ncell = cell;
 
+   /* zerograd layers (boundary_functions.c:269-440): r ghosts from the real
+    * cells outwards, then z ghosts (all j, ghosts included) */
+   if( b->bc_zerograd ){
+      int maxr = 0, maxz = 0;
+      for( int d=0 ; d<ndisk ; ++d ){
+         const DiskParams &D = b->dparams[d];
+         maxr = std::max(maxr, std::max(D.NgRa, D.NgRb));
+         if( D.Nz > 1 && !params[d].Z_Periodic ) maxz = std::max(maxz, std::max(D.NgZa, D.NgZb));
+      }
+      for( int l=0 ; l<maxr ; ++l ){
+         b->zg_off.push_back((int)b->zg_pairs.size());
+         for( int d=0 ; d<ndisk ; ++d ){
+            const DiskParams &D = b->dparams[d];
+            for( int k=0 ; k<D.Nz ; ++k ){
+               int base = D.ann0 + D.Nr*k;
+               if( l < D.NgRa ){ int j = D.NgRa-1-l; b->zg_pairs.push_back(make_int2(base+j, base+j+1)); }
+               if( l < D.NgRb ){ int j = D.Nr-D.NgRb+l; b->zg_pairs.push_back(make_int2(base+j, base+j-1)); }
+            }
+         }
+      }
+      for( int l=0 ; l<maxz ; ++l ){
+         b->zg_off.push_back((int)b->zg_pairs.size());
+         for( int d=0 ; d<ndisk ; ++d ){
+            const DiskParams &D = b->dparams[d];
+            if( D.Nz < 2 || params[d].Z_Periodic ) continue;
+            for( int j=0 ; j<D.Nr ; ++j ){
+               if( l < D.NgZa ){ int k = D.NgZa-1-l;
+                  b->zg_pairs.push_back(make_int2(D.ann0 + j + D.Nr*k, D.ann0 + j + D.Nr*(k+1))); }
+               if( l < D.NgZb ){ int k = D.Nz-D.NgZb+l;
+                  b->zg_pairs.push_back(make_int2(D.ann0 + j + D.Nr*k, D.ann0 + j + D.Nr*(k-1))); }
+            }
+         }
+      }
+      b->zg_off.push_back((int)b->zg_pairs.size());
+      size_t sm = 0;
+      for( const int2 &pr : b->zg_pairs ){
+         size_t n0 = b->ann_np[pr.x], n1 = b->ann_np[pr.y];
+         sm = std::max(sm, 16*(n0 + n1) + 8*n0);
+      }
+      b->zg_smem = (sm + 15) & ~(size_t)15;
+      if( b->zg_smem > 200*1024 ){ delete b; return DISCO_ERR_UNSUPPORTED; }
+   }
+
    ViewT<double> &v = b->vd;
    memset(&v, 0, sizeof v);
    v.Ncell = cell; v.Nann = ann; v.Ntr = (int)b->tr_a.size(); v.Nf = face;
@@ -242,6 +316,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.tr_a = dupload(b, b->tr_a); v.tr_b = dupload(b, b->tr_b); v.tr_off = dupload(b, b->tr_off);
    v.tr_flux = dupload(b, b->tr_flux); v.tr_j = dupload(b, b->tr_j); v.tr_k = dupload(b, b->tr_k);
    v.tr_dxL = dupload(b, b->tr_dxL); v.tr_dxR = dupload(b, b->tr_dxR);
+   v.tr_dim = dupload(b, b->tr_dim);
    v.cblk = dupload(b, b->cblk); v.fblk = dupload(b, b->fblk);
    v.rj = dupload(b, b->rj); v.zk = dupload(b, b->zk);
    v.dp = dupload(b, b->dparams);
@@ -252,6 +327,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.prim = (double *)dalloc_bytes(b, Qn*rs);
    v.gradp = (double *)dalloc_bytes(b, Qn*rs);
    v.gradr = (double *)dalloc_bytes(b, Qn*rs);
+   v.gradz = b->any_3d ? (double *)dalloc_bytes(b, Qn*rs) : NULL;
    v.Gp = (double *)dalloc_bytes(b, Qn*rs);
    v.fS = (double *)dalloc_bytes(b, Qf*rs);
    v.fG = (double *)dalloc_bytes(b, Qf*rs);
@@ -261,6 +337,8 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.wiph = dalloc<double>(b, N); v.piph_new = dalloc<double>(b, N);
    v.I0 = dalloc<int>(b, ann);
    v.consL = dalloc<int>(b, N); v.consR = dalloc<int>(b, N);
+   v.consZL = b->any_3d ? dalloc<int>(b, N) : NULL;
+   v.consZR = b->any_3d ? dalloc<int>(b, N) : NULL;
    v.fL = dalloc<int>(b, face); v.fR = dalloc<int>(b, face);
    v.fLR = dalloc<unsigned char>(b, face);
    v.fphic = dalloc<double>(b, face); v.fdA = dalloc<double>(b, face); v.fdp = dalloc<double>(b, face);
@@ -270,7 +348,12 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->d_Qrz = dalloc<double>(b, (size_t)ann*5);
    v.err = dalloc<int>(b, 1);
    b->d_err = v.err;
+   if( b->bc_zerograd && !b->zg_pairs.empty() ) b->d_zg_pairs = dupload(b, b->zg_pairs);
    make_float_view(b);
+   if( prepare_zerograd<6,double>(b) || prepare_zerograd<9,double>(b) ||
+       (precision == DISCO_PREC_MIXED && mixed_prepare_zerograd(b)) ){
+      disco_batch_destroy(b); return DISCO_ERR_CUDA;
+   }
    for( void *p : b->allocs ) if( !p ){ disco_batch_destroy(b); return DISCO_ERR_CUDA; }
    if( cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) != cudaSuccess ){
       disco_batch_destroy(b); return DISCO_ERR_CUDA;
@@ -475,7 +558,7 @@ extern "C" int disco_batch_time(const disco_batch *b, int disk, double *t, int *
 extern "C" int disco_batch_get_faces(disco_batch *b, int disk, int dim, int *nfaces,
                                      int *fIndex, int *iL, int *iR, int *LRtype, double *geom){
    if( !b || disk < 0 || disk >= b->ndisk || (dim != 1 && dim != 2) ) return DISCO_ERR_ARG;
-   if( dim == 2 ){ if( nfaces ) *nfaces = 0; return DISCO_OK; }
+   if( dim == 2 && b->disk_Nz[disk] < 2 ){ if( nfaces ) *nfaces = 0; return DISCO_OK; }
    CK(cudaSetDevice(b->device));
    const ViewT<double> &v = b->vd;
    unsigned nib = nblk((size_t)v.Nann*32, 128), nfb = (unsigned)b->fblk.size();
@@ -488,8 +571,8 @@ extern "C" int disco_batch_get_faces(disco_batch *b, int disk, int dim, int *nfa
    CK(cudaGetLastError());
    CK(cudaStreamSynchronize(b->stream));
    const DiskParams &D = b->dparams[disk];
-   int f0 = D.face_r0;
-   int t0 = D.trr0, nt = D.ntrr;
+   int t0 = dim == 1 ? D.trr0 : D.trz0, nt = dim == 1 ? D.ntrr : D.ntrz;
+   int f0 = b->tr_off[t0];
    int nf = b->tr_off[t0 + nt] - f0;
    if( nfaces ) *nfaces = nf;
    if( fIndex ) for( int t=0 ; t<=nt ; ++t ) fIndex[t] = b->tr_off[t0+t] - f0;
@@ -516,10 +599,17 @@ extern "C" int disco_batch_get_faces(disco_batch *b, int disk, int dim, int *nfa
          int gt = t0 + t;
          int j = b->tr_j[gt], k = b->tr_k[gt];
          for( int f=b->tr_off[gt]-f0 ; f<b->tr_off[gt+1]-f0 ; ++f ){
+            /* dxL, dxR, cm[0..2], dphi, dl, dA as addFace (faces_alt.c:10-34) */
             double *g = geom + 8*(size_t)f;
             g[0] = b->tr_dxL[gt]; g[1] = b->tr_dxR[gt];
-            g[2] = .5*(rj[j]+rj[j]); g[3] = phic[f]; g[4] = 0.5*(zk[k]+zk[k-1]);
-            g[5] = dp[f]; g[6] = zk[k]-zk[k-1]; g[7] = dA[f];
+            if( dim == 1 ){
+               g[2] = .5*(rj[j]+rj[j]); g[3] = phic[f]; g[4] = 0.5*(zk[k]+zk[k-1]);
+               g[5] = dp[f]; g[6] = zk[k]-zk[k-1]; g[7] = dA[f];
+            }else{
+               g[2] = 2.0*(rj[j]*rj[j] + rj[j]*rj[j-1] + rj[j-1]*rj[j-1])/(3.0*(rj[j]+rj[j-1]));
+               g[3] = phic[f]; g[4] = .5*(zk[k]+zk[k]);
+               g[5] = dp[f]; g[6] = rj[j]-rj[j-1]; g[7] = dA[f];
+            }
          }
       }
    }

@@ -18,13 +18,20 @@ struct disco_batch {
    int prec;
    int ndisk, Q, NC;
    int timestep_mode;        /* 0 = RK2, 1 = forward Euler */
-   int bc_fixed;
+   int bc_fixed;             /* 0 none / zerograd, 1 fixed, 2 fixed3d */
    int any_mm3;
+   int any_3d;               /* some disk has Nz > 1: z faces, gradz, z fluxes */
+   int bc_zerograd;          /* Boundary/zerograd.c */
+   std::vector<int2> zg_pairs;          /* (ghost annulus, source annulus), by layer */
+   std::vector<int> zg_off;             /* layer groups: r layers, then z layers */
+   int2 *d_zg_pairs;
+   size_t zg_smem;                      /* dynamic shared memory of k_zerograd */
    int nq;
    std::vector<disco_params> params;
    /* topology (host) */
    std::vector<int> ann_off, ann_np, ann_disk, ann_j, ann_k;
    std::vector<int> tr_a, tr_b, tr_off, tr_flux, tr_j, tr_k;
+   std::vector<unsigned char> tr_dim;
    std::vector<double> tr_dxL, tr_dxR;
    std::vector<int2> cblk, fblk;
    std::vector<int> ann_blk0, ann_nblk;
@@ -59,6 +66,24 @@ static inline void mark(disco_batch *b, const char *name){
    b->tape_names->push_back(name);
 }
 
+/* boundary_trans of Boundary/zerograd.c (r layers, then z layers, each
+ * layer from the real cells outwards), onestep.c:196-222 and main.c:53-62 */
+template<int Q, class R>
+static void launch_zerograd(disco_batch *b, const ViewT<R> &v){
+   if( !b->bc_zerograd ) return;
+   for( size_t g=0 ; g+1<b->zg_off.size() ; ++g ){
+      int n = b->zg_off[g+1] - b->zg_off[g];
+      if( n > 0 ) k_zerograd<Q,R><<<n, 128, b->zg_smem, b->stream>>>(v, b->d_zg_pairs + b->zg_off[g]);
+   }
+   mark(b, "k_zerograd");
+}
+template<int Q, class R>
+static int prepare_zerograd(disco_batch *b){
+   if( !b->bc_zerograd ) return 0;
+   return cudaFuncSetAttribute(k_zerograd<Q,R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)b->zg_smem) != cudaSuccess;
+}
+
 template<int Q, int NC, class R>
 static void launch_mindt_qt(disco_batch *b, const ViewT<R> &v){
    unsigned nd = nblk(b->ndisk, 64);
@@ -72,6 +97,7 @@ static void launch_setup_qt(disco_batch *b, const ViewT<R> &v){
    k_setup<Q,NC,R><<<ncb, CB, 0, b->stream>>>(v, b->bc_fixed);
    k_wcell<Q,R><<<ncb, CB, 0, b->stream>>>(v);
    if( b->any_mm3 ) k_wmean_nomove<R><<<nblk(v.Nann, 128), 128, 0, b->stream>>>(v);
+   launch_zerograd<Q,R>(b, v);                   /* main.c:53-62 */
 }
 
 /* One substep of onestep() (onestep.c:84-229). */
@@ -84,11 +110,17 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    if( first && b->any_mm3 ){ k_wmean<R><<<nblk(v.Nann, 128), 128, 0, s>>>(v); mark(b, "k_wmean"); }
    k_I0<R><<<nblk((size_t)v.Nann*32, 128), 128, 0, s>>>(v);           mark(b, "k_I0");
    k_faces<Q,R><<<nfb, FB, 0, s>>>(v, 1);                             mark(b, "k_faces");
-   k_gradr<Q,R><<<ncb, CB, 0, s>>>(v);                                mark(b, "k_gradr");
-   k_flux_r<Q,NC,R><<<nfb, FB, 0, s>>>(v);                            mark(b, "k_flux_r");
+   k_grad<Q,1,R><<<ncb, CB, 0, s>>>(v);                               mark(b, "k_gradr");
+   if( b->any_3d ){ k_grad<Q,2,R><<<ncb, CB, 0, s>>>(v);              mark(b, "k_gradz"); }
+   k_flux_t<Q,NC,1,R><<<nfb, FB, 0, s>>>(v);                          mark(b, "k_flux_r");
+   if( b->any_3d ){ k_flux_t<Q,NC,2,R><<<nfb, FB, 0, s>>>(v);         mark(b, "k_flux_z"); }
    k_flux_p<Q,NC,R><<<ncb, CB, 0, s>>>(v);                            mark(b, "k_flux_p");
    k_update<Q,NC,R><<<ncb, CB, 0, s>>>(v, first);                     mark(b, "k_update");
-   k_c2p<Q,NC,R><<<ncb, CB, 0, s>>>(v, last, b->bc_fixed);            mark(b, "k_c2p");
+   k_c2p<Q,NC,R><<<ncb, CB, 0, s>>>(v, last, b->bc_fixed, !b->bc_zerograd); mark(b, "k_c2p");
+   launch_zerograd<Q,R>(b, v);
+   if( last && b->nq && b->bc_zerograd ){
+      k_diag_part<Q,R><<<ncb, CB, 0, s>>>(v);                         mark(b, "k_diag_part");
+   }
 }
 
 /* timestep() (timestep.c:7-45). */
@@ -139,3 +171,4 @@ void mixed_launch_setup(disco_batch *b);
 void mixed_launch_step(disco_batch *b, int use_next);
 void mixed_launch_prim2cons(disco_batch *b);
 void mixed_launch_faces(disco_batch *b);
+int mixed_prepare_zerograd(disco_batch *b);

@@ -15,3 +15,6 @@ void mixed_launch_faces(disco_batch *b){
    k_I0<float><<<nblk((size_t)b->vf.Nann*32, 128), 128, 0, b->stream>>>(b->vf);
    k_faces<6,float><<<(unsigned)b->fblk.size(), FB, 0, b->stream>>>(b->vf, 0);
 }
+int mixed_prepare_zerograd(disco_batch *b){
+   return prepare_zerograd<6,float>(b) || prepare_zerograd<9,float>(b);
+}

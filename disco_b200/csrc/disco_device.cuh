@@ -50,6 +50,7 @@ struct DiskParams {
    int cell0;         /* first global cell */
    int trr0, ntrr;    /* first global r-track, count */
    int face_r0;       /* first global r-face */
+   int trz0, ntrz;    /* first global z-track, count (Nr*(Nz-1)) */
    int npl;
    int ic_module;     /* DISCO_IC_KEPLER_NOISE or DISCO_IC_MHD_SHEAR_NOISE */
    int pad_ic;

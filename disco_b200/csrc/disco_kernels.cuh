@@ -12,13 +12,16 @@
  *              RKcons, ccarry (Kahan carry, mixed form), gradp, gradr (R);
  *              piph[c], dphi[c], wiph[c] (FP64)
  *   annuli     ann_off[a] .. ann_off[a]+ann_np[a]-1 are annulus a's cells
- *   r-tracks   track t joins annulus tr_a[t] (inner) and tr_b[t] (outer);
- *              its faces are tr_off[t] .. tr_off[t+1]-1 (Np_a + Np_b of them,
- *              faces_alt.c:87-100)
+ *   tracks     track t joins annulus tr_a[t] (inner / lower) and tr_b[t]
+ *              (outer / upper); its faces are tr_off[t] .. tr_off[t+1]-1
+ *              (Np_a + Np_b of them, faces_alt.c:87-100).  Per disk the
+ *              (Nr-1)*Nz r-tracks (tr_dim 1) come first, then the
+ *              Nr*(Nz-1) z-tracks (tr_dim 2)
  *   faces      SoA: fL, fR (global cells), fLR, fphic, fdA, fdp (FP64),
  *              fS[q], fG[q] (R)
  *   consume    consL[c] = face of the r-track outside c that consumes c in the
- *              merge; consR[c] = same for the track inside c.  They give each
+ *              merge; consR[c] = same for the track inside c (consZL/consZR:
+ *              the z-tracks above / below c).  They give each
  *              cell the contiguous runs of faces it belongs to, so every
  *              scatter of the reference (plm.c:82-110, riemann.c:312-315)
  *              becomes an order-preserving gather without atomics.
@@ -39,12 +42,13 @@ struct ViewT {
    int Ncell, Nann, Ntr, Nf;
    const int *ann_off, *ann_np, *ann_disk, *ann_j, *ann_k;
    const int *tr_a, *tr_b, *tr_off, *tr_flux, *tr_j, *tr_k;
+   const unsigned char *tr_dim;      /* 1: r-track (j,k)-(j+1,k); 2: z-track (j,k)-(j,k+1) */
    const double *tr_dxL, *tr_dxR;
    const int2 *cblk, *fblk;
    const double *rj, *zk;
    const DiskParams *dp;
    DiskState *ds;
-   R *prim, *gradp, *gradr;
+   R *prim, *gradp, *gradr, *gradz;   /* gradz only when a disk has Nz > 1 */
    double *cons, *RKcons, *ccarry;
    double *piph, *dphi, *wiph, *piph_new;
    int *I0;
@@ -52,7 +56,8 @@ struct ViewT {
    unsigned char *fLR;
    double *fphic, *fdA, *fdp;
    R *fS, *fG;
-   int *consL, *consR;
+   int *consL, *consR;                /* r-tracks outside / inside the cell */
+   int *consZL, *consZR;              /* z-tracks above / below the cell */
    R *Gp;
    double *diag_part;   /* per cell block: nq sums + volume */
    /* energy-frame Omega of omega.c:62-110, evaluated once by k_precompute at
@@ -171,7 +176,7 @@ __global__ void k_precompute(ViewT<R> v){
       const DiskParams &P = v.dp[v.ann_disk[v.tr_a[x]]];
       const double *rj = v.rj + P.rj0 + 1;
       int j = v.tr_j[x];
-      v.tr_om[x] = get_om(P, .5*(rj[j]+rj[j]));
+      v.tr_om[x] = get_om(P, v.tr_dim[x] == 1 ? .5*(rj[j]+rj[j]) : centroid_r(rj[j], rj[j-1]));
    }
 }
 
@@ -295,13 +300,21 @@ __global__ void __launch_bounds__(FB) k_faces(ViewT<R> v, int with_slopes){
    const double *zk = v.zk + P.zk0 + 1;
    double dp = get_dp(xp1, xm1, Pmax, &err);
    double phic = get_dp(xp1, .5*dp, Pmax, &err);
-   double r = .5*(rj[j]+rj[j]);
-   double dz = zk[k]-zk[k-1];
-   double dA = r*dp*dz;                                   /* get_dA(.,.,1) */
+   double dA;
+   if( v.tr_dim[t] == 1 ){
+      double r = .5*(rj[j]+rj[j]);
+      double dz = zk[k]-zk[k-1];
+      dA = r*dp*dz;                                       /* get_dA(.,.,1) */
+   }else{
+      double r = .5*(rj[j]+rj[j-1]);
+      double dr = rj[j]-rj[j-1];
+      dA = r*dr*dp;                                       /* get_dA(.,.,2) */
+   }
 
    v.fL[f] = cL; v.fR[f] = cR; v.fLR[f] = (unsigned char)LR;
    v.fphic[f] = phic; v.fdA[f] = dA; v.fdp[f] = dp;
-   if( LR == 0 ) v.consL[cL] = f; else v.consR[cR] = f;
+   if( v.tr_dim[t] == 1 ){ if( LR == 0 ) v.consL[cL] = f; else v.consR[cR] = f; }
+   else                  { if( LR == 0 ) v.consZL[cL] = f; else v.consZR[cR] = f; }
 
    if( with_slopes ){
       R dxL = (R)v.tr_dxL[t], dxR = (R)v.tr_dxR[t];
@@ -342,12 +355,13 @@ __device__ __forceinline__ Runs cell_runs(const ViewT<R> &v, const int *cons, in
    return RR;
 }
 
-/* ------------------------------------------------------------------ k_gradr
- * plm_trans for dim 1 (plm.c:56-195): sum S*dA over the cell's faces in the
- * reference's face order (inner track first, then outer), divide by the
- * cell's two face areas, then apply every face's limiter. */
-template<int Q, class R>
-__global__ void __launch_bounds__(CB) k_gradr(ViewT<R> v){
+/* ------------------------------------------------------------------ k_grad
+ * plm_trans (plm.c:56-195) for dim 1 (r) or 2 (z): sum S*dA over the
+ * cell's faces in the reference's face order (inner / lower track first,
+ * then outer / upper), divide by the cell's two face areas, then apply
+ * every face's limiter. */
+template<int Q, int DIM, class R>
+__global__ void __launch_bounds__(CB) k_grad(ViewT<R> v){
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -356,22 +370,33 @@ __global__ void __launch_bounds__(CB) k_gradr(ViewT<R> v){
    int c0 = v.ann_off[a], c = c0 + i;
    int d = v.ann_disk[a];
    const DiskParams &P = v.dp[d];
+   if( DIM == 2 && P.Nz == 1 ) return;
+   R *grad = DIM == 1 ? v.gradr : v.gradz;
    int j = v.ann_j[a], k = v.ann_k[a];
-   int Nr = P.Nr;
+   int Nr = P.Nr, Nz = P.Nz;
    int I0 = v.I0[a];
    R g[Q];
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) g[q] = R(0.0);
    if( P.PLM == 0.0 ){
 #pragma unroll
-      for( int q=0 ; q<Q ; ++q ) v.gradr[q*N + c] = R(0.0);
+      for( int q=0 ; q<Q ; ++q ) grad[q*N + c] = R(0.0);
       return;
    }
-   int tin = j >= 1 ? P.trr0 + (j-1) + (Nr-1)*k : -1;
-   int tout = j <= Nr-2 ? P.trr0 + j + (Nr-1)*k : -1;
+   int tin, tout;
+   const int *cin, *cout;
+   if( DIM == 1 ){
+      tin = j >= 1 ? P.trr0 + (j-1) + (Nr-1)*k : -1;
+      tout = j <= Nr-2 ? P.trr0 + j + (Nr-1)*k : -1;
+      cin = v.consR; cout = v.consL;
+   }else{
+      tin = k >= 1 ? P.trz0 + j + Nr*(k-1) : -1;
+      tout = k <= Nz-2 ? P.trz0 + j + Nr*k : -1;
+      cin = v.consZR; cout = v.consZL;
+   }
    Runs Rin = {1,0,1,0}, Rout = {1,0,1,0};
-   if( tin >= 0 ) Rin = cell_runs(v, v.consR, tin, c0, np, i, I0);
-   if( tout >= 0 ) Rout = cell_runs(v, v.consL, tout, c0, np, i, I0);
+   if( tin >= 0 ) Rin = cell_runs(v, cin, tin, c0, np, i, I0);
+   if( tout >= 0 ) Rout = cell_runs(v, cout, tout, c0, np, i, I0);
    const size_t Nf = v.Nf;
 #define ACC_RUN(s,e) for( int f=(s) ; f<=(e) ; ++f ){ R dA = (R)v.fdA[f]; \
       _Pragma("unroll") for( int q=0 ; q<Q ; ++q ) g[q] += v.fS[q*Nf + f]*dA; }
@@ -386,12 +411,19 @@ __global__ void __launch_bounds__(CB) k_gradr(ViewT<R> v){
    double phip = v.piph[c];
    double phim = phip - v.dphi[c];
    double dph = get_dp(phip, phim, P.Pmax, &err);
-   double dz = zk[k]-zk[k-1];
-   double dAp = (.5*(rj[j]+rj[j]))*dph*dz;
-   double dAm = (.5*(rj[j-1]+rj[j-1]))*dph*dz;
+   double dAp, dAm;
+   if( DIM == 1 ){
+      double dz = zk[k]-zk[k-1];
+      dAp = (.5*(rj[j]+rj[j]))*dph*dz;
+      dAm = (.5*(rj[j-1]+rj[j-1]))*dph*dz;
+   }else{
+      double r = .5*(rj[j]+rj[j-1]), dr = rj[j]-rj[j-1];
+      dAp = r*dr*dph;
+      dAm = r*dr*dph;
+   }
    double dAtot = dAp + dAm;
-   if( j == 0 ) dAtot = dAp;
-   if( j == Nr-1 ) dAtot = dAm;
+   if( (DIM == 1 && j == 0) || (DIM == 2 && k == 0) ) dAtot = dAp;
+   if( (DIM == 1 && j == Nr-1) || (DIM == 2 && k == Nz-1) ) dAtot = dAm;
    const R rdAtot = (R)dAtot;
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) g[q] /= rdAtot;
@@ -405,18 +437,21 @@ __global__ void __launch_bounds__(CB) k_gradr(ViewT<R> v){
    LIM_RUN(Rout.s2, Rout.e2)
 #undef LIM_RUN
 #pragma unroll
-   for( int q=0 ; q<Q ; ++q ) v.gradr[q*N + c] = g[q];
+   for( int q=0 ; q<Q ; ++q ) grad[q*N + c] = g[q];
    raise_err(v, err);
 }
 
-/* ------------------------------------------------------------------ k_flux_r
- * trans_flux dim 1 (misc.c:431-509) -> riemann_trans (riemann.c:114-170)
- * -> solve_riemann; G_q = (F - w U*) dA dt per face. */
-template<int Q, int NC, class R>
-__global__ void __launch_bounds__(FB) k_flux_r(ViewT<R> v){
+/* ------------------------------------------------------------------ k_flux_t
+ * trans_flux (misc.c:431-509) -> riemann_trans (riemann.c:114-170) ->
+ * solve_riemann for the faces of r-tracks (DIM 1) or z-tracks (DIM 2);
+ * G_q = (F - w U*) dA dt per face.  The face centre cm is (r_{j+1/2}, phic,
+ * z centroid) for r-faces and (r centroid, phic, z_{k+1/2}) for z-faces
+ * (addFace, faces_alt.c:10-16). */
+template<int Q, int NC, int DIM, class R>
+__global__ void __launch_bounds__(FB) k_flux_t(ViewT<R> v){
    int2 b = v.fblk[blockIdx.x];
    int t = b.x;
-   if( !v.tr_flux[t] ) return;
+   if( v.tr_dim[t] != DIM || !v.tr_flux[t] ) return;
    int dd = b.y + threadIdx.x;
    int f = v.tr_off[t] + dd;
    if( f >= v.tr_off[t+1] ) return;
@@ -433,21 +468,23 @@ __global__ void __launch_bounds__(FB) k_flux_r(ViewT<R> v){
    double phiR = v.piph[cR] - .5*v.dphi[cR];
    R dpL = (R)get_signed_dp(phi, phiL, P.Pmax, &err);
    R dpR = (R)get_signed_dp(phiR, phi, P.Pmax, &err);
+   const R *grad = DIM == 1 ? v.gradr : v.gradz;
    R primL[Q], primR[Q];
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ){
-      primL[q] = v.prim[q*N+cL] + v.gradr[q*N+cL]*dxL + v.gradp[q*N+cL]*dpL;
-      primR[q] = v.prim[q*N+cR] - v.gradr[q*N+cR]*dxR - v.gradp[q*N+cR]*dpR;
+      primL[q] = v.prim[q*N+cL] + grad[q*N+cL]*dxL + v.gradp[q*N+cL]*dpL;
+      primR[q] = v.prim[q*N+cR] - grad[q*N+cR]*dxR - v.gradp[q*N+cR]*dpR;
    }
    if constexpr ( NC == 8 ){                     /* normal B averaged, riemann.c:146-152 */
-      R Bavg = R(.5)*(primL[BRR]+primR[BRR]);
-      primL[BRR] = Bavg; primR[BRR] = Bavg;
+      const int BT = DIM == 1 ? BRR : BZZ;
+      R Bavg = R(.5)*(primL[BT]+primR[BT]);
+      primL[BT] = Bavg; primR[BT] = Bavg;
    }
    int j = v.tr_j[t];
    const double *rj = v.rj + P.rj0 + 1;
-   double r = .5*(rj[j]+rj[j]);                 /* face cm[0] */
+   double r = DIM == 1 ? .5*(rj[j]+rj[j]) : centroid_r(rj[j], rj[j-1]);    /* face cm[0] */
    R G[Q];
-   solve_riemann<Q,NC,1,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G);
+   solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G);
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) v.fG[(size_t)q*v.Nf + f] = G[q];
    raise_err(v, err);
@@ -554,6 +591,19 @@ __global__ void __launch_bounds__(CB) k_update(ViewT<R> v, int first){
       ADD_RUN(Rin.s2, Rin.e2, +)
       ADD_RUN(Rout.s1, Rout.e1, -)
       ADD_RUN(Rout.s2, Rout.e2, -)
+      /* z faces (trans_flux dim 2): lower track (cell is R) then upper */
+      if( P.Nz > 1 ){
+         if( k >= 1 ){
+            Runs Zin = cell_runs(v, v.consZR, P.trz0 + j + P.Nr*(k-1), c0, np, i, I0);
+            ADD_RUN(Zin.s1, Zin.e1, +)
+            ADD_RUN(Zin.s2, Zin.e2, +)
+         }
+         if( k <= P.Nz-2 ){
+            Runs Zout = cell_runs(v, v.consZL, P.trz0 + j + P.Nr*k, c0, np, i, I0);
+            ADD_RUN(Zout.s1, Zout.e1, -)
+            ADD_RUN(Zout.s2, Zout.e2, -)
+         }
+      }
 #undef ADD_RUN
       /* add_source with the pre-move cell */
       double prim[Q];
@@ -624,13 +674,106 @@ __global__ void __launch_bounds__(CB) k_update(ViewT<R> v, int first){
    raise_err(v, err);
 }
 
+/* One cell's terms of add_diagnostics (analysis.c:52-107) with the
+ * diag_disk2d quantities (Diagnostics/diag_disk2d.c:17-38), times dV, and
+ * dV itself: every cell of the annulus, ghosts included, at the midpoint xc. */
+__device__ __forceinline__ void diag_cell(const DiskParams &P, const DiskState &S, const double *prim,
+                                          double rp, double rm, double zp, double zm,
+                                          double piph, double phim, double *dq, int *err){
+   double dph = get_dp(piph, phim, P.Pmax, err);
+   double dV = dV_of(rp, rm, dph, zp, zm);
+   double r = .5*(rp+rm), phi = .5*(piph+phim);
+   double rho = prim[RHO], vr = prim[URR], omega = prim[UPP];
+   double Fp = 0.0;
+   if( P.npl > 1 ){
+      double Fr, Fz;
+      planetary_force(P.grav2D, S.pl[1], r, phi, 0.0, &Fr, &Fp, &Fz);
+   }
+   dq[0] = rho*dV;
+   dq[1] = 2.*DISCO_PI*r*rho*vr*dV;
+   dq[2] = 2.*DISCO_PI*r*rho*(r*Fp)*dV;
+   dq[3] = 2.*DISCO_PI*r*rho*( r*r*omega*vr )*dV;
+   dq[4] = omega*dV;
+   dq[5] = dV;
+}
+
+/* The per-block diagnostic sums as a pass of their own, for boundaries that
+ * change ghost prims after calc_prim (zerograd): add_diagnostics sees the
+ * state after the last boundary pass (timestep.c:40-42). */
+template<int Q, class R>
+__global__ void __launch_bounds__(CB) k_diag_part(ViewT<R> v){
+   __shared__ double s_red[CB/32][6];
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   const int N = v.Ncell;
+   int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+   int j = v.ann_j[a], k = v.ann_k[a];
+   const double *rj = v.rj + P.rj0 + 1;
+   const double *zk = v.zk + P.zk0 + 1;
+   double dq[6] = {0,0,0,0,0,0};
+   int err = 0;
+   if( i < np ){
+      int c = v.ann_off[a] + i;
+      double prim[Q];
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N + c];
+      double piph = v.piph[c];
+      diag_cell(P, v.ds[d], prim, rj[j], rj[j-1], zk[k], zk[k-1], piph, piph - v.dphi[c], dq, &err);
+   }
+   raise_err(v, err);
+   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+   for( int m=0 ; m<6 ; ++m ){
+      double x = dq[m];
+#pragma unroll
+      for( int o=16 ; o>0 ; o>>=1 ) x += __shfl_down_sync(0xffffffffu, x, o);
+      if( lane == 0 ) s_red[wid][m] = x;
+   }
+   __syncthreads();
+   if( threadIdx.x == 0 ){
+      for( int m=0 ; m<6 ; ++m ){
+         double x = 0.0;
+         for( int w=0 ; w<CB/32 ; ++w ) x += s_red[w][m];
+         v.diag_part[(size_t)blockIdx.x*6 + m] = x;
+      }
+   }
+}
+
+/* The ghost cells a fixed boundary re-initialises from the Initial module,
+ * and where it evaluates it:
+ *   bc 1  Boundary/fixed.c:11-60: r ghosts (all k) at (midpoint r,
+ *         piph - dphi/2, midpoint z)
+ *   bc 2  Boundary/fixed3d.c -> boundary_functions.c:20-31, 161-265: r ghosts
+ *         (all k) and z ghosts (all j) at the centroid (get_centroid_arr)
+ * then subtract_omega (rotframe.c:15-17).  Returns whether prim was set. */
+template<int Q, int NC>
+__device__ __forceinline__ bool fixed_ghost_init(const DiskParams &P, int bc, int j, int k,
+                                                 const double *rj, const double *zk,
+                                                 double piph, double dphi, double *prim){
+   bool rghost = j < P.NgRa || j >= P.Nr - P.NgRb;
+   bool zghost = k < P.NgZa || k >= P.Nz - P.NgZb;
+   if( bc == 1 && rghost ){
+      double x[3] = { .5*(rj[j]+rj[j-1]), piph - .5*dphi, .5*(zk[k]+zk[k-1]) };
+      initial<Q,NC>(P, prim, x);
+   }else if( bc == 2 && (rghost || zghost) ){
+      double x[3] = { centroid_r(rj[j], rj[j-1]), 0.5*(piph + (piph - dphi)), 0.5*(zk[k]+zk[k-1]) };
+      initial<Q,NC>(P, prim, x);
+   }else{
+      return false;
+   }
+   if( P.rotframe ) prim[UPP] -= P.RotOmega;
+   return true;
+}
+
 /* ------------------------------------------------------------------ k_c2p
  *   calc_prim    misc.c:290-325 (euler cons2prim, FP64) on real cells
  *   boundary     Boundary/fixed.c:11-60 (r ghosts re-initialised)
  * and, on the last substep, the next step's getmindt (misc.c:39-84) and the
  * per-block sums of add_diagnostics (analysis.c:52-107). */
 template<int Q, int NC, class R>
-__global__ void __launch_bounds__(CB) k_c2p(ViewT<R> v, int last, int bc_fixed){
+__global__ void __launch_bounds__(CB) k_c2p(ViewT<R> v, int last, int bc, int diag){
    __shared__ double s_red[CB/32][8];
    __shared__ unsigned long long s_dt[CB/32];
    int2 b = v.cblk[blockIdx.x];
@@ -667,11 +810,7 @@ __global__ void __launch_bounds__(CB) k_c2p(ViewT<R> v, int last, int bc_fixed){
             prim[q] = (double)pq;       /* the stored state is what the next step sees */
          }
       }else{
-         bool rghost = j < P.NgRa || j >= P.Nr - P.NgRb;
-         if( bc_fixed && rghost ){
-            double x[3] = { .5*(rj[j]+rj[j-1]), piph - .5*dphi, .5*(zk[k]+zk[k-1]) };
-            initial<Q,NC>(P, prim, x);
-            if( P.rotframe ) prim[UPP] -= P.RotOmega;       /* subtract_omega, rotframe.c:11 */
+         if( fixed_ghost_init<Q,NC>(P, bc, j, k, rj, zk, piph, dphi, prim) ){
 #pragma unroll
             for( int q=0 ; q<Q ; ++q ){
                R pq = (R)prim[q];
@@ -705,23 +844,7 @@ __global__ void __launch_bounds__(CB) k_c2p(ViewT<R> v, int last, int bc_fixed){
             if( dtm > dtz ) dtm = dtz;
             if( dtm == dtm ) dtc = dtm;
          }
-         if( v.nq ){                              /* diag_disk2d.c:17-38 */
-            double dph = get_dp(piph, phim, P.Pmax, &err);
-            double dV = dV_of(rp, rm, dph, zp, zm);
-            double r = .5*(rp+rm), phi = .5*(piph+phim);
-            double rho = prim[RHO], vr = prim[URR], omega = prim[UPP];
-            double Fp = 0.0;
-            if( P.npl > 1 ){
-               double Fr, Fz;
-               planetary_force(P.grav2D, v.ds[d].pl[1], r, phi, 0.0, &Fr, &Fp, &Fz);
-            }
-            dq[0] = rho*dV;
-            dq[1] = 2.*DISCO_PI*r*rho*vr*dV;
-            dq[2] = 2.*DISCO_PI*r*rho*(r*Fp)*dV;
-            dq[3] = 2.*DISCO_PI*r*rho*( r*r*omega*vr )*dV;
-            dq[4] = omega*dV;
-            dq[5] = dV;
-         }
+         if( v.nq && diag ) diag_cell(P, v.ds[d], prim, rp, rm, zp, zm, piph, phim, dq, &err);
       }
    }
    raise_err(v, err);
@@ -735,7 +858,7 @@ __global__ void __launch_bounds__(CB) k_c2p(ViewT<R> v, int last, int bc_fixed){
       bits = ob < bits ? ob : bits;
    }
    if( lane == 0 ) s_dt[wid] = bits;
-   if( v.nq ){
+   if( v.nq && diag ){
 #pragma unroll
       for( int m=0 ; m<6 ; ++m ){
          double x = dq[m];
@@ -749,13 +872,95 @@ __global__ void __launch_bounds__(CB) k_c2p(ViewT<R> v, int last, int bc_fixed){
       unsigned long long mb = s_dt[0];
       for( int w=1 ; w<CB/32 ; ++w ) mb = s_dt[w] < mb ? s_dt[w] : mb;
       if( real ) atomicMin(&v.ds[d].dtmin, mb);
-      if( v.nq ){
+      if( v.nq && diag ){
          for( int m=0 ; m<6 ; ++m ){
             double x = 0.0;
             for( int w=0 ; w<CB/32 ; ++w ) x += s_red[w][m];
             v.diag_part[(size_t)blockIdx.x*6 + m] = x;
          }
       }
+   }
+}
+
+/* ------------------------------------------------------------------ zerograd
+ * boundary_zerograd_{rinn,rout,zbot,ztop} (boundary_functions.c:269-440):
+ * a ghost annulus takes the phi-overlap-weighted average of the adjacent
+ * annulus (set_cells_copy_distant, :90-158).  One block per (ghost, source)
+ * annulus pair of one layer: thread 0 replays the reference's traversal on
+ * the two annuli's edges in shared memory and records, per ghost cell, the
+ * source cell it starts from and how many it visits; then every thread sums
+ * its ghost cell's overlaps in that order and divides by its dphi.  Loops
+ * are capped; a cap hit raises ERRF_WRAP. */
+template<int Q, class R>
+__global__ void k_zerograd(ViewT<R> v, const int2 *pairs){
+   extern __shared__ __align__(16) unsigned char zg_smem[];
+   int2 pr = pairs[blockIdx.x];
+   const int a = pr.x, a1 = pr.y;
+   const int np = v.ann_np[a], np1 = v.ann_np[a1];
+   const int c0 = v.ann_off[a], c10 = v.ann_off[a1];
+   const DiskParams &P = v.dp[v.ann_disk[a]];
+   const double Pmax = P.Pmax;
+   double *sp = reinterpret_cast<double*>(zg_smem);          /* ghost piph, dphi */
+   double *sd = sp + np;
+   double *sp1 = sd + np;                                    /* source piph, dphi */
+   double *sd1 = sp1 + np1;
+   int *st = reinterpret_cast<int*>(sd1 + np1);              /* start, count */
+   int *cnt = st + np;
+   for( int i=threadIdx.x ; i<np ; i+=blockDim.x ){ sp[i] = v.piph[c0+i]; sd[i] = v.dphi[c0+i]; }
+   for( int i=threadIdx.x ; i<np1 ; i+=blockDim.x ){ sp1[i] = v.piph[c10+i]; sd1[i] = v.dphi[c10+i]; }
+   __syncthreads();
+   if( threadIdx.x == 0 ){
+      int err = 0;
+      /* the source cell containing the ghost annulus's first edge */
+      int i1 = 0;
+      double phi0 = sp[0] - sd[0];
+      for( i1=0 ; i1<np1 ; ++i1 ){
+         double dphip = get_signed_dp(sp1[i1], phi0, Pmax, &err);
+         double dphim = dphip - sd1[i1];
+         if( dphip > 0 && dphim <= 0.0 ) break;
+      }
+      if( i1 >= np1 ) i1 = 0;
+      for( int i=0 ; i<np ; ++i ){
+         double phip = sp[i], phim = sp[i] - sd[i];
+         double phip1;
+         int n = 0;
+         st[i] = i1;
+         do{
+            phip1 = sp1[i1];
+            double phim1 = sp1[i1] - sd1[i1];
+            int w = 0;
+            while( phip1 < phim ){ phip1 += Pmax; phim1 += Pmax; if( ++w > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
+            while( phim1 > phip ){ phip1 -= Pmax; phim1 -= Pmax; if( ++w > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
+            i1 = i1 < np1-1 ? i1+1 : 0;
+            if( ++n > np1 + 1 ){ err |= ERRF_WRAP; break; }
+         }while( phip1 < phip );
+         cnt[i] = n;
+         i1 = i1 > 0 ? i1-1 : np1-1;
+      }
+      raise_err(v, err);
+   }
+   __syncthreads();
+   const int N = v.Ncell;
+   for( int i=threadIdx.x ; i<np ; i+=blockDim.x ){
+      double phip = sp[i], phim = sp[i] - sd[i];
+      double acc[Q];
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) acc[q] = 0.0;
+      int i1 = st[i];
+      for( int n=0 ; n<cnt[i] ; ++n ){
+         double phip1 = sp1[i1], phim1 = sp1[i1] - sd1[i1];
+         int w = 0;
+         while( phip1 < phim && w <= WRAP_CAP ){ phip1 += Pmax; phim1 += Pmax; ++w; }
+         while( phim1 > phip && w <= 2*WRAP_CAP ){ phip1 -= Pmax; phim1 -= Pmax; ++w; }
+         double phi1 = phip < phip1 ? phip : phip1;
+         double phi2 = phim > phim1 ? phim : phim1;
+         double dphi = phi1 - phi2;
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ) acc[q] += (double)v.prim[q*N + c10 + i1]*dphi;
+         i1 = i1 < np1-1 ? i1+1 : 0;
+      }
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) v.prim[q*N + c0 + i] = (R)(acc[q]/sd[i]);
    }
 }
 
@@ -844,7 +1049,7 @@ __global__ void k_diag_finish(ViewT<R> v, double *Qrz, const int *ann_blk0, cons
  * setupCells (domain.c:319-383): initial(), prim2cons, cons2prim on real
  * cells (FP64); then main.c's boundary_trans for ghosts. */
 template<int Q, int NC, class R>
-__global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc_fixed){
+__global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc){
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -875,11 +1080,7 @@ __global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc_fixed){
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){ v.prim[q*N+c] = (R)prim[q]; v.cons[q*N+c] = cons[q]; }
    }else{
-      bool rghost = j < P.NgRa || j >= P.Nr - P.NgRb;
-      if( bc_fixed && rghost ){
-         double x[3] = { .5*(rj[j]+rj[j-1]), piph - .5*dphi, .5*(zk[k]+zk[k-1]) };
-         initial<Q,NC>(P, prim, x);
-         if( P.rotframe ) prim[UPP] -= P.RotOmega;
+      if( fixed_ghost_init<Q,NC>(P, bc, j, k, rj, zk, piph, dphi, prim) ){
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) v.prim[q*N+c] = (R)prim[q];
       }

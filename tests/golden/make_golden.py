@@ -42,11 +42,20 @@ CASES = {
                                    "Mesh_Motion": 1, "Init_Par1": 0.05}, 6),
     # libm-free MHD: rigid rotation held by pressure, no gravity, HLLD
     "c1_mhd_rigid": ("c1_mhd2d_nograv", {"Num_R": 14, "Init_Par2": 1, "Init_Par4": 10.0}, 8),
+    # zero-gradient boundaries (Boundary/zerograd.c), 2D hydro
+    "c0_zg": ("c0_zerograd", {"Num_R": 16, "Init_Par0": 4242}, 6),
+    # 3D: z faces, z slopes and fluxes (hydro, fixed; MHD HLLD, zerograd)
+    "c0_3d": ("c0_fixed3d", {"Num_R": 10, "Num_Z": 4, "Grav2D": 1, "Z_Min": -0.3,
+                             "Z_Max": 0.3}, 4),
+    "c1_mhd3d": ("c1_mhd3d", {"Num_R": 8, "Num_Z": 6}, 5),
+    "c1_mhd3d_rigid": ("c1_mhd3d_nograv", {"Num_R": 8, "Num_Z": 6, "Init_Par2": 1,
+                                           "Init_Par4": 10.0}, 6),
 }
 
 # the in.par template each module configuration starts from
 BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": "c0_kepler2d",
-            "c1_mhd2d": "c1_mhd2d", "c1_mhd2d_nograv": "c1_mhd2d"}
+            "c1_mhd2d": "c1_mhd2d", "c1_mhd2d_nograv": "c1_mhd2d", "c0_zerograd": "c0_kepler2d", "c0_fixed3d": "c0_kepler2d",
+            "c1_mhd3d": "c1_mhd3d", "c1_mhd3d_nograv": "c1_mhd3d"}
 
 
 def par_text(cfg_par, overrides):
@@ -72,6 +81,11 @@ def main():
         d0 = pyoracle.run_ref(cfg, text, 0)
         dn = pyoracle.run_ref(cfg, text, n)
         F = dn["faces_1"]
+        extra = {}
+        if "faces_2" in dn:
+            Z = dn["faces_2"]
+            extra = dict(z_fIndex=Z["fIndex"], z_iL=Z["iL"], z_iR=Z["iR"], z_LRtype=Z["LRtype"],
+                         z_fgeom=Z["geom"])
         np.savez_compressed(
             os.path.join(HERE, case + ".npz"), cfg=cfg, nsteps=n,
             s0_prim=d0["prim"], s0_cons=d0["cons"], s0_piph=d0["piph"], s0_dphi=d0["dphi"],
@@ -79,7 +93,7 @@ def main():
             sN_prim=dn["prim"], sN_cons=dn["cons"], sN_piph=dn["piph"], sN_dphi=dn["dphi"],
             sN_wiph=dn["wiph"], dt=dn["dt"], sN_dt_next=dn["dt_next"], Qrz=dn["Qrz"],
             t=dn["meta"]["t"], fIndex=F["fIndex"], iL=F["iL"], iR=F["iR"], LRtype=F["LRtype"],
-            fgeom=F["geom"], Np=d0["Np"], r_jph=d0["r_jph"], z_kph=d0["z_kph"])
+            fgeom=F["geom"], Np=d0["Np"], r_jph=d0["r_jph"], z_kph=d0["z_kph"], **extra)
         print(case, "cells", d0["meta"]["Ncell"], "faces", len(F["iL"]))
 
 

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import disco_b200 as db
-from helpers import CASES, MHD_CASES, case_disk, golden, oracle_for, rel_l1, rel_l1_cols
+from helpers import CASES, EXT_CASES, MHD_CASES, case_disk, golden, oracle_for, rel_l1, rel_l1_cols
 
 pytestmark = pytest.mark.gpu
 
@@ -24,8 +24,8 @@ TOL = 1e-12          # relative L1, FP64 fields (north_star)
 # noise-sized and carries the same libm differences at 1.3e-12; their
 # libm-free twin (c1_mhd_rigid) is held to bit equality.
 CASE_TOL = {"c0_hll_fe_mm3": 1e-11, "c1_mhd_hlld": 1e-11, "c1_mhd_hllc": 1e-11,
-            "c1_mhd_hll_fe": 1e-11}
-BITEXACT = ("c0_rigid", "c1_mhd_rigid")
+            "c1_mhd_hll_fe": 1e-11, "c1_mhd3d": 1e-11, "c0_3d": 1e-11}
+BITEXACT = ("c0_rigid", "c1_mhd_rigid", "c1_mhd3d_rigid")
 
 
 def _real(g):
@@ -38,7 +38,7 @@ def _batch_from_golden(disk, g):
     return b
 
 
-@pytest.mark.parametrize("case", CASES + MHD_CASES)
+@pytest.mark.parametrize("case", CASES + MHD_CASES + EXT_CASES)
 def test_setup_matches_reference(case):
     """Device setupCells (initial, prim2cons, cons2prim, set_wcell, boundary)
     reproduces the reference's step-0 state on real cells bit for bit."""
@@ -56,7 +56,7 @@ def test_setup_matches_reference(case):
     assert dt == g["s0_dt_next"]
 
 
-@pytest.mark.parametrize("case", CASES + MHD_CASES)
+@pytest.mark.parametrize("case", CASES + MHD_CASES + EXT_CASES)
 def test_steps_match_reference(case):
     """N full RK steps from the reference's step-0 state vs the reference."""
     disk, g = case_disk(case)
@@ -77,11 +77,22 @@ def test_steps_match_reference(case):
         assert e < tol, ("prim", q, e)
     for q, e in enumerate(rel_l1_cols(st["cons"][r], g["sN_cons"][r])):
         assert e < tol, ("cons", q, e)
-    assert rel_l1(st["piph"], g["sN_piph"]) < 1e-14
+    # piph follows the cells' own Omega (Mesh_Motion 1/3), so it carries the
+    # libm noise of the state, scaled down by w dt / piph
+    assert rel_l1(st["piph"], g["sN_piph"]) < 1e-13
     f = b.faces(0, 1, geom=True)
     for k in ("fIndex", "iL", "iR", "LRtype"):
         assert np.array_equal(f[k], g[k]), k
     assert rel_l1(f["geom"], g["fgeom"]) < 1e-14
+    if "z_iL" in g:                       # 3D: the z-face lists too
+        fz = b.faces(0, 2, geom=True)
+        for k in ("fIndex", "iL", "iR", "LRtype"):
+            assert np.array_equal(fz[k], g["z_" + k]), ("z", k)
+        assert rel_l1(fz["geom"], g["z_fgeom"]) < 1e-14
+    if case in BITEXACT:
+        for k in ("prim", "piph", "dphi", "wiph"):
+            assert np.array_equal(st[k], g["sN_" + k]), k
+        assert np.array_equal(st["cons"][r], g["sN_cons"][r])
     t, n = b.time()
     assert n == int(g["nsteps"]) and abs(t / g["t"] - 1) < tol
     Q, _ = b.diagnostics()
