@@ -55,17 +55,19 @@ def kernel_bytes(name, first, N, Nf, Na):
     if name == "k_I0":
         return N * w + Na * 4
     if name == "k_faces":
+        # reads piph, dphi, prim, gradp; writes the face lists, geometry,
+        # PLM face slopes and consL/consR
         return N * w * (2 * Q + 2) + N * 8 + Nf * (4 + 4 + 1 + 3 * w + Q * w)
     if name == "k_gradr":
+        # reads the face slopes and areas, the cell's geometry; writes gradr
         return Nf * w * (Q + 1) + N * (w * Q + 3 * w + 8)
     if name == "k_flux_r":
         return Nf * (4 + 4 + 2 * w + Q * w) + N * w * (3 * Q + 2)
-    if name == "k_flux_p":
-        return N * w * (3 * Q + 2)
     if name == "k_update":
-        # reads cons, prim, phi fluxes, piph, dphi, consL/consR, r-face fluxes;
-        # writes cons (+ reads piph_new, writes piph and dphi in the first substep)
-        return N * w * (4 * Q + (5 if first else 2)) + N * 8 + Nf * w * Q
+        # reads cons, prim, gradp (phi faces), piph, dphi, wiph, the consume
+        # indices and the r-face fluxes; writes cons (+ piph_new -> piph,
+        # dphi in the first substep)
+        return N * w * (4 * Q + (6 if first else 3)) + N * 8 + Nf * w * Q
     return 0
 
 

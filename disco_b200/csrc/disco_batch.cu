@@ -115,7 +115,7 @@ static void make_float_view(disco_batch *b){
    memcpy(&f, &d, sizeof f);
    f.prim = (float *)d.prim; f.gradp = (float *)d.gradp; f.gradr = (float *)d.gradr;
    f.gradz = (float *)d.gradz;
-   f.fS = (float *)d.fS; f.fG = (float *)d.fG; f.Gp = (float *)d.Gp;
+   f.fS = (float *)d.fS; f.fG = (float *)d.fG;
 }
 
 extern "C" void disco_batch_destroy(disco_batch *b);
@@ -328,7 +328,6 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.gradp = (double *)dalloc_bytes(b, Qn*rs);
    v.gradr = (double *)dalloc_bytes(b, Qn*rs);
    v.gradz = b->any_3d ? (double *)dalloc_bytes(b, Qn*rs) : NULL;
-   v.Gp = (double *)dalloc_bytes(b, Qn*rs);
    v.fS = (double *)dalloc_bytes(b, Qf*rs);
    v.fG = (double *)dalloc_bytes(b, Qf*rs);
    v.cons = dalloc<double>(b, Qn); v.RKcons = dalloc<double>(b, Qn);

@@ -114,7 +114,6 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    if( b->any_3d ){ k_grad<Q,2,R><<<ncb, CB, 0, s>>>(v);              mark(b, "k_gradz"); }
    k_flux_t<Q,NC,1,R><<<nfb, FB, 0, s>>>(v);                          mark(b, "k_flux_r");
    if( b->any_3d ){ k_flux_t<Q,NC,2,R><<<nfb, FB, 0, s>>>(v);         mark(b, "k_flux_z"); }
-   k_flux_p<Q,NC,R><<<ncb, CB, 0, s>>>(v);                            mark(b, "k_flux_p");
    k_update<Q,NC,R><<<ncb, CB, 0, s>>>(v, first);                     mark(b, "k_update");
    k_c2p<Q,NC,R><<<ncb, CB, 0, s>>>(v, last, b->bc_fixed, !b->bc_zerograd); mark(b, "k_c2p");
    launch_zerograd<Q,R>(b, v);

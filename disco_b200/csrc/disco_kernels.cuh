@@ -58,7 +58,6 @@ struct ViewT {
    R *fS, *fG;
    int *consL, *consR;                /* r-tracks outside / inside the cell */
    int *consZL, *consZR;              /* z-tracks above / below the cell */
-   R *Gp;
    double *diag_part;   /* per cell block: nq sums + volume */
    /* energy-frame Omega of omega.c:62-110, evaluated once by k_precompute at
     * the radii the step uses (same device expressions, so bit-identical to
@@ -250,8 +249,10 @@ __global__ void k_I0(ViewT<R> v){
  * Within one cell width the unrolled order equals the reference's wrapped
  * comparison, so (iL, iR, LRtype) are the reference's; the face's own
  * LR / LR_back and geometry are then evaluated exactly as :140-164 and
- * addFace (:10-34) do (FP64 in both forms).  Also emits the PLM face slopes
- * S_q of plm_trans (plm.c:82-89) when with_slopes is set. */
+ * addFace (:10-34) do (FP64 in both forms).  Also stores the PLM face
+ * slopes S_q of plm_trans (plm.c:82-89) when with_slopes is set: the
+ * gather reads each twice (sum, limiter), and recomputing them there from
+ * the two cells' scattered states was measured 5x slower than storing. */
 template<int Q, class R>
 __global__ void __launch_bounds__(FB) k_faces(ViewT<R> v, int with_slopes){
    int2 b = v.fblk[blockIdx.x];
@@ -490,27 +491,15 @@ __global__ void __launch_bounds__(FB) k_flux_t(ViewT<R> v){
    raise_err(v, err);
 }
 
-/* ------------------------------------------------------------------ k_flux_p
+/* ------------------------------------------------------------------ phi faces
  * phi_flux (misc.c:368-426) -> riemann_phi (riemann.c:39-65): the face
- * between cell i and i+1 of a real annulus, stored at cell i. */
+ * between cells cL = i and cR = i+1 of a real annulus a, G_q = (F - w U*)
+ * dA dt, with x = (annulus centroid r, phi, centroid z), dA = dr dz,
+ * w = r wiph[cL]. */
 template<int Q, int NC, class R>
-__global__ void __launch_bounds__(CB) k_flux_p(ViewT<R> v){
-   int2 b = v.cblk[blockIdx.x];
-   int a = b.x, i = b.y + threadIdx.x;
-   int np = v.ann_np[a];
-   if( i >= np ) return;
-   int d = v.ann_disk[a];
-   const DiskParams &P = v.dp[d];
-   int j = v.ann_j[a], k = v.ann_k[a];
-   if( j < P.NgRa || j >= P.Nr - P.NgRb || k < P.NgZa || k >= P.Nz - P.NgZb ) return;
+__device__ __forceinline__ void phi_face_flux(const ViewT<R> &v, const DiskParams &P, int a,
+                                              int cL, int cR, double r, double dAdt, R *G){
    const int N = v.Ncell;
-   int c0 = v.ann_off[a], cL = c0 + i, cR = c0 + (i < np-1 ? i+1 : 0);
-   const double *rj = v.rj + P.rj0 + 1;
-   const double *zk = v.zk + P.zk0 + 1;
-   double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
-   double r = centroid_r(rp, rm);
-   double dA = (rp-rm)*(zp-zm);                      /* get_dA(.,.,0) */
-   double dt = v.ds[d].dt*v.dtfac;
    R primL[Q], primR[Q];
    R dL = (R)v.dphi[cL], dR = (R)v.dphi[cR];
 #pragma unroll
@@ -523,10 +512,7 @@ __global__ void __launch_bounds__(CB) k_flux_p(ViewT<R> v){
       primL[BPP] = Bp; primR[BPP] = Bp;
    }
    double w = r*v.wiph[cL];
-   R G[Q];
-   solve_riemann<Q,NC,0,R>(P, primL, primR, (R)r, (R)v.ann_om[a], (R)w, (R)(dA*dt), G);
-#pragma unroll
-   for( int q=0 ; q<Q ; ++q ) v.Gp[q*N + cL] = G[q];
+   solve_riemann<Q,NC,0,R>(P, primL, primR, (R)r, (R)v.ann_om[a], (R)w, (R)dAdt, G);
 }
 
 /* ------------------------------------------------------------------ k_update
@@ -539,10 +525,10 @@ __global__ void __launch_bounds__(CB) k_flux_p(ViewT<R> v){
  * k_c2p. */
 template<int Q, int NC, class R>
 __global__ void __launch_bounds__(CB) k_update(ViewT<R> v, int first){
+   __shared__ R sG[Q][CB+1];      /* sG[q][t+1]: face (i, i+1); sG[q][0]: face (i0-1, i0) */
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
-   if( i >= np ) return;
    const int N = v.Ncell;
    int c0 = v.ann_off[a], c = c0 + i;
    int cprev = c0 + (i == 0 ? np-1 : i-1);
@@ -550,12 +536,31 @@ __global__ void __launch_bounds__(CB) k_update(ViewT<R> v, int first){
    const DiskParams &P = v.dp[d];
    int j = v.ann_j[a], k = v.ann_k[a];
    bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
+   const double *rj = v.rj + P.rj0 + 1;
+   const double *zk = v.zk + P.zk0 + 1;
+   if( real ){                      /* uniform over the block: one annulus */
+      double dA = (rj[j]-rj[j-1])*(zk[k]-zk[k-1]);       /* get_dA(.,.,0) */
+      double dAdtp = dA*(v.ds[d].dt*v.dtfac);
+      double rc = centroid_r(rj[j], rj[j-1]);
+      if( i < np ){
+         R G[Q];
+         phi_face_flux<Q,NC,R>(v, P, a, c, c0 + (i < np-1 ? i+1 : 0), rc, dAdtp, G);
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ) sG[q][threadIdx.x+1] = G[q];
+      }
+      if( threadIdx.x == 0 ){
+         R G[Q];
+         phi_face_flux<Q,NC,R>(v, P, a, cprev, c, rc, dAdtp, G);
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ) sG[q][0] = G[q];
+      }
+      __syncthreads();
+   }
+   if( i >= np ) return;
    int err = 0;
    double piph = v.piph[c], dphi = v.dphi[c];
    if( real ){
       const DiskState &S = v.ds[d];
-      const double *rj = v.rj + P.rj0 + 1;
-      const double *zk = v.zk + P.zk0 + 1;
       double dt = S.dt*v.dtfac;
       double cons[Q], cc[Q];
 #pragma unroll
@@ -565,17 +570,18 @@ __global__ void __launch_bounds__(CB) k_update(ViewT<R> v, int first){
          else cc[q] = 0.0;
       }
       /* phi faces: loop order of phi_flux */
+      const int t = threadIdx.x;
       if( i > 0 ){
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ){
-            acc<R>(cons[q], cc[q], (double)v.Gp[q*N+cprev]);
-            acc<R>(cons[q], cc[q], -(double)v.Gp[q*N+c]);
+            acc<R>(cons[q], cc[q], (double)sG[q][t]);
+            acc<R>(cons[q], cc[q], -(double)sG[q][t+1]);
          }
       }else{
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ){
-            acc<R>(cons[q], cc[q], -(double)v.Gp[q*N+c]);
-            acc<R>(cons[q], cc[q], (double)v.Gp[q*N+cprev]);
+            acc<R>(cons[q], cc[q], -(double)sG[q][t+1]);
+            acc<R>(cons[q], cc[q], (double)sG[q][t]);
          }
       }
       /* r faces: inner track (cell is R) then outer track (cell is L) */

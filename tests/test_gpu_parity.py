@@ -227,7 +227,7 @@ def test_kernel_times_cover_the_step():
     b = _batch_from_golden(disk, g)
     kt = b.kernel_times()
     names = [k for k, _ in kt]
-    for k in ("k_begin", "k_I0", "k_faces", "k_gradr", "k_flux_r", "k_flux_p", "k_update", "k_c2p"):
+    for k in ("k_begin", "k_I0", "k_faces", "k_gradr", "k_flux_r", "k_update", "k_c2p"):
         assert names.count(k) == 2, k
     assert all(ms >= 0 for _, ms in kt)
 
