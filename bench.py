@@ -205,6 +205,104 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def div_b(disk, batch, st):
+    """Discrete div B of every real cell from the face fluxes of the
+    cell-centred field: sum over the cell's phi, r and z faces of the
+    face-averaged normal B times the face area, over the cell volume.
+    Returns (sum |div B| dV, sum |B| dV) over the real cells."""
+    import numpy as np
+    p = st["prim"]
+    Br, Bp, Bz = p[:, 5], p[:, 6], p[:, 7]
+    nc = len(p)
+    flux = np.zeros(nc)
+    off = np.concatenate([[0], np.cumsum(disk.Np)])
+    rj, zk = disk.r_jph, disk.z_kph          # index 0 is edge -1
+    vol = np.zeros(nc)
+    for a in range(disk.Nr * disk.Nz):
+        j, k = a % disk.Nr, a // disk.Nr
+        c = np.arange(off[a], off[a + 1])
+        cn = np.roll(c, -1)
+        dr, dz = rj[j + 1] - rj[j], zk[k + 1] - zk[k]
+        f = 0.5 * (Bp[c] + Bp[cn]) * dr * dz
+        flux[c] += f
+        flux[cn] -= f
+        vol[c] = 0.5 * (rj[j + 1] + rj[j]) * dr * st["dphi"][c] * dz
+    for dim, comp in ((1, Br), (2, Bz)):
+        fa = batch.faces(0, dim, geom=True)
+        if len(fa["iL"]) == 0:
+            continue
+        f = 0.5 * (comp[fa["iL"]] + comp[fa["iR"]]) * fa["geom"][:, 7]
+        np.add.at(flux, fa["iL"], f)
+        np.add.at(flux, fa["iR"], -f)
+    r = disk.real == 1
+    bmag = np.sqrt(Br ** 2 + Bp ** 2 + Bz ** 2)
+    return float(np.abs(flux[r]).sum()), float((bmag[r] * vol[r]).sum())
+
+
+def config1_leg(args, local, stream):
+    """3D Newtonian MHD shearing disk (HLLD, zerograd, no constrained
+    transport: B evolves through the fluxes): FP64 and the mixed form for
+    200 steps from the same state; throughput of both, the mixed form's
+    error and drifts against FP64."""
+    import numpy as np
+    import torch
+    import disco_b200 as db
+    par, opt = db.template_paths("c1_mhd3d")
+    disk = db.Disk.from_files(par, opt)
+    nsteps = 200
+    out = {"workload": "3D MHD shearing disk, HLLD, zerograd, Nr=%d Nz=%d, Np max %d, %d real cells"
+                       % (disk.Nr, disk.Nz, int(np.max(disk.Np)), disk.nreal),
+           "steps": nsteps, "warmup": 3,
+           "note": "errors and drifts after warm-up + timed steps, both forms from the same set-up"}
+    states = {}
+    for prec, key in ((db.PREC_FP64, "fp64"), (db.PREC_MIXED, "mixed")):
+        b = db.Batch([disk], device=local, precision=prec)
+        b.set_stream(stream.cuda_stream)
+        if key == "fp64":
+            states["s0"] = b.get_cells()
+            states["div0"] = div_b(disk, b, states["s0"])
+        b.run(3)                    # warm-up (and the step graph's capture)
+        b.sync()
+        if key == "fp64":
+            kt = {}
+            for name, t in b.kernel_times():
+                kt[name] = kt.get(name, 0.0) + t
+            out["fp64_kernels_ms_per_step"] = {k: round(v, 4) for k, v in
+                                               sorted(kt.items(), key=lambda x: -x[1])}
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.run(nsteps)
+        e1.record(stream)
+        e1.synchronize()
+        if b.last_error() != 0:
+            raise RuntimeError("device error in the config-1 leg")
+        ms = e0.elapsed_time(e1)
+        st = b.get_cells()
+        states[key] = st
+        out[key] = {"zone_updates_per_s": disk.nreal * nsteps / (ms / 1e3), "ms_per_step": ms / nsteps,
+                    "div_b": div_b(disk, b, st)}
+        b.close()
+    r = disk.real == 1
+    a, m, s0 = states["fp64"], states["mixed"], states["s0"]
+    names = ["rho", "P", "v_r", "omega", "v_z", "B_r", "B_phi", "B_z", "X"]
+    err = {}
+    for q, nm in enumerate(names):
+        den = np.abs(a["prim"][r, q]).sum()
+        err[nm] = float(np.abs(m["prim"][r, q] - a["prim"][r, q]).sum() / den) if den > 0 else None
+    out["mixed_rel_l1_vs_fp64"] = err
+    tot = lambda st, q: float(st["cons"][r, q].sum())
+    out["drift"] = {
+        "mass_fp64": tot(a, 0) / tot(s0, 0) - 1.0, "mass_mixed": tot(m, 0) / tot(s0, 0) - 1.0,
+        "ang_mom_fp64": tot(a, 3) / tot(s0, 3) - 1.0, "ang_mom_mixed": tot(m, 3) / tot(s0, 3) - 1.0,
+        "mixed_vs_fp64_mass": tot(m, 0) / tot(a, 0) - 1.0,
+        "div_b_rel_step0": states["div0"][0] / states["div0"][1],
+        "div_b_rel_fp64": out["fp64"]["div_b"][0] / out["fp64"]["div_b"][1],
+        "div_b_rel_mixed": out["mixed"]["div_b"][0] / out["mixed"]["div_b"][1]}
+    out["mixed_speedup_vs_fp64"] = out["mixed"]["zone_updates_per_s"] / out["fp64"]["zone_updates_per_s"]
+    return out
+
+
 C2P_GRID = {"Nr": 192, "Nz": 96, "Np": 462, "rmin": 1.5, "rmax": 50.0, "zmin": -20.0, "zmax": 20.0}
 C2P_TOL, C2P_NEXTRA, C2P_MAXIT = 1e-10, 10, 30
 C2P_BYTES = 8 * (9 + 3 + 5 + 9)         # read cons, x, the 5 prims of the warm start; write prims
@@ -434,6 +532,11 @@ def run_ours(args, world, rank, local):
                  "precision": "FP32 prim/slopes/fluxes, FP64 mesh/dt/Kahan cons"}
         bm.close()
 
+    config1 = None
+    if not args.no_config1:
+        config1 = config1_leg(args, local, stream)
+        barrier()
+
     c2p = None
     if not args.no_c2p:
         c2p = c2p_leg(args, local, stream)
@@ -472,6 +575,7 @@ def run_ours(args, world, rank, local):
                     "d2h_bytes_per_step": (d2h + 8 * len(disks) * args.steps) / args.steps},
             "gpu_launches": launches_per_step * args.steps,
             "mixed_form": mixed,
+            "config1_mhd3d": config1,
             "c2p": c2p,
             "clocks": ck,
             "cpu_baseline": cpu,
@@ -492,6 +596,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--no-c2p", action="store_true", help="skip the GRMHD cons->prim leg")
+    ap.add_argument("--no-config1", action="store_true", help="skip the 3D MHD (config 1) leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

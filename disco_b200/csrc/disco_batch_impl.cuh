@@ -96,7 +96,7 @@ static void launch_setup_qt(disco_batch *b, const ViewT<R> &v){
    unsigned ncb = (unsigned)b->cblk.size();
    k_setup<Q,NC,R><<<ncb, CB, 0, b->stream>>>(v, b->bc_fixed);
    k_wcell<Q,R><<<ncb, CB, 0, b->stream>>>(v);
-   if( b->any_mm3 ) k_wmean_nomove<R><<<nblk(v.Nann, 128), 128, 0, b->stream>>>(v);
+   if( b->any_mm3 ) k_wmean<R><<<nblk(v.Nann, WM_WARPS), 32*WM_WARPS, 0, b->stream>>>(v, 0);
    launch_zerograd<Q,R>(b, v);                   /* main.c:53-62 */
 }
 
@@ -107,7 +107,7 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    cudaStream_t s = b->stream;
    unsigned ncb = (unsigned)b->cblk.size(), nfb = (unsigned)b->fblk.size();
    k_begin<Q,NC,R><<<ncb, CB, 0, s>>>(v, RK, first);                  mark(b, "k_begin");
-   if( first && b->any_mm3 ){ k_wmean<R><<<nblk(v.Nann, 128), 128, 0, s>>>(v); mark(b, "k_wmean"); }
+   if( first && b->any_mm3 ){ k_wmean<R><<<nblk(v.Nann, WM_WARPS), 32*WM_WARPS, 0, s>>>(v, 1); mark(b, "k_wmean"); }
    k_I0<R><<<nblk((size_t)v.Nann*32, 128), 128, 0, s>>>(v);           mark(b, "k_I0");
    k_faces<Q,R><<<nfb, FB, 0, s>>>(v, 1);                             mark(b, "k_faces");
    k_grad<Q,1,R><<<ncb, CB, 0, s>>>(v);                               mark(b, "k_gradr");

@@ -180,27 +180,42 @@ __global__ void k_precompute(ViewT<R> v){
 }
 
 /* Mesh_Motion 3 (misc.c:138-152): annulus mean of w, summed in cell order
- * by one thread per annulus, then the move of the first substep. */
+ * (one warp per annulus: lane 0 adds the values in cell order from shared
+ * memory, the warp loads and writes), then the move of the first substep
+ * (move != 0) or not (set-up). */
+#define WM_WARPS 4
+#define WM_CHUNK 256
 template<class R>
-__global__ void k_wmean(ViewT<R> v){
-   int a = blockIdx.x*blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(32*WM_WARPS) k_wmean(ViewT<R> v, int move){
+   __shared__ double s_w[WM_WARPS][WM_CHUNK];
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int a = blockIdx.x*WM_WARPS + warp;
    if( a >= v.Nann ) return;
-   int np = v.ann_np[a], c0 = v.ann_off[a];
-   int d = v.ann_disk[a];
+   const int np = v.ann_np[a], c0 = v.ann_off[a];
+   const int d = v.ann_disk[a];
    const DiskParams &P = v.dp[d];
    if( P.mesh_motion != 3 ) return;
    double w = 0.0;
-   for( int i=0 ; i<np ; ++i ) w += v.wiph[c0+i];
+   for( int base=0 ; base<np ; base+=WM_CHUNK ){
+      const int n = np - base < WM_CHUNK ? np - base : WM_CHUNK;
+      for( int t=lane ; t<n ; t+=32 ) s_w[warp][t] = v.wiph[c0+base+t];
+      __syncwarp();
+      if( lane == 0 ) for( int t=0 ; t<n ; ++t ) w += s_w[warp][t];
+      __syncwarp();
+   }
+   w = __shfl_sync(0xffffffffu, w, 0);
    w /= (double)np;
-   double dt = v.ds[d].dt;
+   const double dt = v.ds[d].dt;
    int err = 0;
-   for( int i=0 ; i<np ; ++i ){
+   for( int i=lane ; i<np ; i+=32 ){
       v.wiph[c0+i] = w;
-      double phi = __dadd_rn(v.piph[c0+i], __dmul_rn(w, dt));
-      int n = 0;
-      while( phi > P.Pmax ){ phi -= P.Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
-      while( phi < 0.0 ){ phi += P.Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
-      v.piph_new[c0+i] = phi;
+      if( move ){
+         double phi = __dadd_rn(v.piph[c0+i], __dmul_rn(w, dt));
+         int n = 0;
+         while( phi > P.Pmax ){ phi -= P.Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
+         while( phi < 0.0 ){ phi += P.Pmax; if( ++n > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
+         v.piph_new[c0+i] = phi;
+      }
    }
    raise_err(v, err);
 }
@@ -888,6 +903,33 @@ __global__ void __launch_bounds__(CB) k_c2p(ViewT<R> v, int last, int bc, int di
    }
 }
 
+/* The sequential walk of set_cells_copy_distant (boundary_functions.c:
+ * 90-158) over ghost cells lo..hi-1 starting at source cell i1: records the
+ * start and the number of source cells visited per ghost cell, returns the
+ * cell the next ghost cell starts from.  Loops capped (ERRF_WRAP). */
+__device__ __forceinline__ int zg_walk(const double *sp, const double *sd, const double *sp1,
+                                       const double *sd1, int np1, double Pmax, int lo, int hi,
+                                       int i1, int *st, int *cnt, int *err){
+   for( int i=lo ; i<hi ; ++i ){
+      double phip = sp[i], phim = sp[i] - sd[i];
+      double phip1;
+      int n = 0;
+      st[i] = i1;
+      do{
+         phip1 = sp1[i1];
+         double phim1 = sp1[i1] - sd1[i1];
+         int w = 0;
+         while( phip1 < phim ){ phip1 += Pmax; phim1 += Pmax; if( ++w > WRAP_CAP ){ *err |= ERRF_WRAP; break; } }
+         while( phim1 > phip ){ phip1 -= Pmax; phim1 -= Pmax; if( ++w > WRAP_CAP ){ *err |= ERRF_WRAP; break; } }
+         i1 = i1 < np1-1 ? i1+1 : 0;
+         if( ++n > np1 + 1 ){ *err |= ERRF_WRAP; break; }
+      }while( phip1 < phip );
+      cnt[i] = n;
+      i1 = i1 > 0 ? i1-1 : np1-1;
+   }
+   return i1;
+}
+
 /* ------------------------------------------------------------------ zerograd
  * boundary_zerograd_{rinn,rout,zbot,ztop} (boundary_functions.c:269-440):
  * a ghost annulus takes the phi-overlap-weighted average of the adjacent
@@ -912,36 +954,61 @@ __global__ void k_zerograd(ViewT<R> v, const int2 *pairs){
    double *sd1 = sp1 + np1;
    int *st = reinterpret_cast<int*>(sd1 + np1);              /* start, count */
    int *cnt = st + np;
+   __shared__ int s_first;
    for( int i=threadIdx.x ; i<np ; i+=blockDim.x ){ sp[i] = v.piph[c0+i]; sd[i] = v.dphi[c0+i]; }
    for( int i=threadIdx.x ; i<np1 ; i+=blockDim.x ){ sp1[i] = v.piph[c10+i]; sd1[i] = v.dphi[c10+i]; }
+   if( threadIdx.x == 0 ) s_first = np1;
    __syncthreads();
-   if( threadIdx.x == 0 ){
+   {  /* the first source cell (in index order) containing the ghost
+       * annulus's first edge: every thread tests its cells, the minimum
+       * index wins, as the reference's search loop would stop there */
       int err = 0;
-      /* the source cell containing the ghost annulus's first edge */
-      int i1 = 0;
       double phi0 = sp[0] - sd[0];
-      for( i1=0 ; i1<np1 ; ++i1 ){
-         double dphip = get_signed_dp(sp1[i1], phi0, Pmax, &err);
-         double dphim = dphip - sd1[i1];
-         if( dphip > 0 && dphim <= 0.0 ) break;
+      for( int k=threadIdx.x ; k<np1 ; k+=blockDim.x ){
+         double dphip = get_signed_dp(sp1[k], phi0, Pmax, &err);
+         double dphim = dphip - sd1[k];
+         if( dphip > 0 && dphim <= 0.0 ){ atomicMin(&s_first, k); break; }
       }
-      if( i1 >= np1 ) i1 = 0;
-      for( int i=0 ; i<np ; ++i ){
-         double phip = sp[i], phim = sp[i] - sd[i];
-         double phip1;
-         int n = 0;
-         st[i] = i1;
-         do{
-            phip1 = sp1[i1];
-            double phim1 = sp1[i1] - sd1[i1];
-            int w = 0;
-            while( phip1 < phim ){ phip1 += Pmax; phim1 += Pmax; if( ++w > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
-            while( phim1 > phip ){ phip1 -= Pmax; phim1 -= Pmax; if( ++w > WRAP_CAP ){ err |= ERRF_WRAP; break; } }
-            i1 = i1 < np1-1 ? i1+1 : 0;
-            if( ++n > np1 + 1 ){ err |= ERRF_WRAP; break; }
-         }while( phip1 < phip );
-         cnt[i] = n;
-         i1 = i1 > 0 ? i1-1 : np1-1;
+      raise_err(v, err);
+   }
+   __syncthreads();
+   /* The walk of set_cells_copy_distant: ghost cell i starts at source cell
+    * st[i] and visits cnt[i] cells; the next starts where it stopped.  Warp 0
+    * splits the ghost cells into 32 runs; lane l walks run l from a guess of
+    * its start (the source cell holding the upper edge of the cell before
+    * the run).  Then each guess is checked against the end of the previous
+    * run; from the first wrong guess on, lane 0 walks the rest again, so
+    * st/cnt are those of the sequential walk in every case. */
+   if( threadIdx.x < 32 ){
+      const int lane = threadIdx.x;
+      const int seg = (np + 31)/32;
+      const int lo = lane*seg, hi = lo + seg < np ? lo + seg : np;
+      __shared__ int s_guess[32], s_end[32], s_err[32];
+      int err = 0, werr = 0;
+      int start = -1;
+      if( lo < np ){
+         if( lane == 0 ){
+            start = s_first < np1 ? s_first : 0;
+         }else{
+            const double pt = sp[lo-1];
+            for( int k=0 ; k<np1 ; ++k ){
+               double dd = get_signed_dp(sp1[k], pt, Pmax, &err);
+               if( dd >= 0.0 && dd - sd1[k] < 0.0 ){ start = k; break; }
+            }
+         }
+      }
+      s_guess[lane] = start;
+      int endi = -1;
+      if( lo < np && start >= 0 ) endi = zg_walk(sp, sd, sp1, sd1, np1, Pmax, lo, hi, start, st, cnt, &werr);
+      s_end[lane] = endi;
+      s_err[lane] = werr;           /* counts only if this run's start is confirmed */
+      __syncwarp();
+      if( lane == 0 ){
+         int bad = 32;
+         for( int l=1 ; l<32 && l*seg < np ; ++l )
+            if( s_guess[l] < 0 || s_guess[l] != s_end[l-1] ){ bad = l; break; }
+         for( int l=0 ; l<bad ; ++l ) err |= s_err[l];
+         if( bad < 32 ) zg_walk(sp, sd, sp1, sd1, np1, Pmax, bad*seg, np, s_end[bad-1], st, cnt, &err);
       }
       raise_err(v, err);
    }
@@ -1146,20 +1213,6 @@ __global__ void __launch_bounds__(CB) k_wcell(ViewT<R> v){
       w = mesh_om(P, centroid_r(rj[j], rj[j-1]));
    }
    v.wiph[c] = w;
-}
-
-/* Mesh_Motion 3 mean without a move (set-up only). */
-template<class R>
-__global__ void k_wmean_nomove(ViewT<R> v){
-   int a = blockIdx.x*blockDim.x + threadIdx.x;
-   if( a >= v.Nann ) return;
-   const DiskParams &P = v.dp[v.ann_disk[a]];
-   if( P.mesh_motion != 3 ) return;
-   int np = v.ann_np[a], c0 = v.ann_off[a];
-   double w = 0.0;
-   for( int i=0 ; i<np ; ++i ) w += v.wiph[c0+i];
-   w /= (double)np;
-   for( int i=0 ; i<np ; ++i ) v.wiph[c0+i] = w;
 }
 
 /* Stand-alone getmindt (misc.c:39-84) into ds[d].dtmin. */
