@@ -36,6 +36,34 @@ namespace disco {
 
 #define CB 128
 #define FB 128
+/* Resident blocks per SM asked of the compiler for the step kernels (the
+ * register budget per thread follows: 65536 / (128 * MB)).  The kernels
+ * are latency-bound, so warps in flight matter more than the spills the
+ * tighter budget costs: on ragged64 the hydro step went from 7.26 to
+ * 5.41 ms (FP64) and 5.60 to 4.57 ms (mixed) with these values against
+ * the compiler's choice (MB 1).  The MHD instantiations (HLLD needs about
+ * 160 registers) keep MB_MHD. */
+#ifndef MB_STEP
+#define MB_STEP 8
+#endif
+#ifndef MB_MHD
+#define MB_MHD 4
+#endif
+#ifndef MB_BEGIN
+#define MB_BEGIN 10
+#endif
+#ifndef MB_GRAD
+#define MB_GRAD 12
+#endif
+#ifndef MB_FLUX
+#define MB_FLUX MB_STEP
+#endif
+#ifndef MB_UPDATE
+#define MB_UPDATE MB_STEP
+#endif
+#ifndef MB_C2P
+#define MB_C2P MB_STEP
+#endif
 
 template<class R>
 struct ViewT {
@@ -92,7 +120,7 @@ __device__ __forceinline__ void acc(double &s, double &cc, double x){
  * move_cells + clean_pi (misc.c:256-268, 8-26) into piph_new.
  * Every substep: adjust_RK_cons (misc.c:226-244) and plm_phi (plm.c:15-51). */
 template<int Q, int NC, class R>
-__global__ void __launch_bounds__(CB) k_begin(ViewT<R> v, double RK, int first){
+__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_BEGIN) k_begin(ViewT<R> v, double RK, int first){
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -377,7 +405,7 @@ __device__ __forceinline__ Runs cell_runs(const ViewT<R> &v, const int *cons, in
  * then outer / upper), divide by the cell's two face areas, then apply
  * every face's limiter. */
 template<int Q, int DIM, class R>
-__global__ void __launch_bounds__(CB) k_grad(ViewT<R> v){
+__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_GRAD) k_grad(ViewT<R> v){
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -464,7 +492,7 @@ __global__ void __launch_bounds__(CB) k_grad(ViewT<R> v){
  * z centroid) for r-faces and (r centroid, phic, z_{k+1/2}) for z-faces
  * (addFace, faces_alt.c:10-16). */
 template<int Q, int NC, int DIM, class R>
-__global__ void __launch_bounds__(FB) k_flux_t(ViewT<R> v){
+__global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R> v){
    int2 b = v.fblk[blockIdx.x];
    int t = b.x;
    if( v.tr_dim[t] != DIM || !v.tr_flux[t] ) return;
@@ -539,7 +567,7 @@ __device__ __forceinline__ void phi_face_flux(const ViewT<R> &v, const DiskParam
  * calc_prim, the boundary, and the fused getmindt / diagnostics follow in
  * k_c2p. */
 template<int Q, int NC, class R>
-__global__ void __launch_bounds__(CB) k_update(ViewT<R> v, int first){
+__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT<R> v, int first){
    __shared__ R sG[Q][CB+1];      /* sG[q][t+1]: face (i, i+1); sG[q][0]: face (i0-1, i0) */
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
@@ -794,7 +822,7 @@ __device__ __forceinline__ bool fixed_ghost_init(const DiskParams &P, int bc, in
  * and, on the last substep, the next step's getmindt (misc.c:39-84) and the
  * per-block sums of add_diagnostics (analysis.c:52-107). */
 template<int Q, int NC, class R>
-__global__ void __launch_bounds__(CB) k_c2p(ViewT<R> v, int last, int bc, int diag){
+__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v, int last, int bc, int diag){
    __shared__ double s_red[CB/32][8];
    __shared__ unsigned long long s_dt[CB/32];
    int2 b = v.cblk[blockIdx.x];
