@@ -83,12 +83,13 @@ def test_steps_match_reference(case):
     f = b.faces(0, 1, geom=True)
     for k in ("fIndex", "iL", "iR", "LRtype"):
         assert np.array_equal(f[k], g[k]), k
-    assert rel_l1(f["geom"], g["fgeom"]) < 1e-14
+    # the face geometry follows piph (same libm noise, same bound)
+    assert rel_l1(f["geom"], g["fgeom"]) < 1e-13
     if "z_iL" in g:                       # 3D: the z-face lists too
         fz = b.faces(0, 2, geom=True)
         for k in ("fIndex", "iL", "iR", "LRtype"):
             assert np.array_equal(fz[k], g["z_" + k]), ("z", k)
-        assert rel_l1(fz["geom"], g["z_fgeom"]) < 1e-14
+        assert rel_l1(fz["geom"], g["z_fgeom"]) < 1e-13
     if case in BITEXACT:
         for k in ("prim", "piph", "dphi", "wiph"):
             assert np.array_equal(st[k], g["sN_" + k]), k
