@@ -234,25 +234,39 @@ class Batch:
         except Exception:
             pass
 
-    def set_cells(self, prim, cons, piph, dphi, wiph=None, real=None):
+    @property
+    def ct(self):
+        """Constrained transport on (in.par Constrained_Transport)."""
+        return bool(self.disks[0].params.CT)
+
+    def set_cells(self, prim, cons, piph, dphi, wiph=None, real=None, Phi=None):
+        """Upload a state; Phi (ncell x 3 face fluxes) is the constrained-transport
+        state and is taken only when CT is on (zeros when omitted)."""
         prim = None if prim is None else np.ascontiguousarray(prim, np.float64)
         cons = None if cons is None else np.ascontiguousarray(cons, np.float64)
         piph = np.ascontiguousarray(piph, np.float64)
         dphi = np.ascontiguousarray(dphi, np.float64)
         wiph = None if wiph is None else np.ascontiguousarray(wiph, np.float64)
         real = None if real is None else np.ascontiguousarray(real, np.int32)
+        Phi = None if Phi is None else np.ascontiguousarray(Phi, np.float64)
+        if Phi is not None and Phi.shape != (self.ncell, 3):
+            raise ValueError("Phi must be ncell x 3")
         _check(library().disco_batch_set_cells(self.h, dptr(prim), dptr(cons), dptr(piph),
-                                               dptr(dphi), dptr(wiph), iptr(real), None),
+                                               dptr(dphi), dptr(wiph), iptr(real), dptr(Phi)),
                "disco_batch_set_cells")
 
     def get_cells(self):
         n, q = self.ncell, self.q
         prim = np.zeros((n, q)); cons = np.zeros((n, q))
         piph = np.zeros(n); dphi = np.zeros(n); wiph = np.zeros(n)
+        Phi = np.zeros((n, 3)) if self.ct else None
         _check(library().disco_batch_get_cells(self.h, dptr(prim), dptr(cons), dptr(piph),
-                                               dptr(dphi), dptr(wiph), None),
+                                               dptr(dphi), dptr(wiph), dptr(Phi)),
                "disco_batch_get_cells")
-        return dict(prim=prim, cons=cons, piph=piph, dphi=dphi, wiph=wiph)
+        out = dict(prim=prim, cons=cons, piph=piph, dphi=dphi, wiph=wiph)
+        if Phi is not None:
+            out["Phi"] = Phi
+        return out
 
     def mindt(self):
         dt = np.zeros(len(self.disks))

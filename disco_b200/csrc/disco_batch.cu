@@ -83,6 +83,7 @@ static void fill_disk_params(DiskParams &D, const disco_params &p, const disco_m
    D.ic_mhd.cs = p.initPar[3]; D.ic_mhd.beta = p.initPar[4]; D.ic_mhd.gam = p.Adiabatic_Index;
    D.ic_mhd.rmin = p.rmin; D.ic_mhd.rmax = p.rmax; D.ic_mhd.zmin = p.zmin; D.ic_mhd.zmax = p.zmax;
    D.ic_mhd.phimax = p.phimax; D.ic_mhd.kind = (int)p.initPar[2];
+   D.ic_mhd.beta_phi = p.initPar[5]; D.ic_mhd.b_r = p.initPar[6];
 }
 
 static void init_planets(DiskState &S, DiskParams &D, const disco_params &p, const disco_modules &m){
@@ -132,18 +133,24 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    if( cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1 ) return DISCO_ERR_NO_DEVICE;
    if( device < 0 || device >= ndev ) return DISCO_ERR_ARG;
    if( precision != DISCO_PREC_FP64 && precision != DISCO_PREC_MIXED ) return DISCO_ERR_ARG;
-   /* euler (NUM_C 5) or mhd (NUM_C 8), NUM_N 1.  Constrained transport
-    * (in.par Constrained_Transport) is not built: B evolves through the
-    * fluxes.  CT_MODE 1/2 only sizes the reference's face-flux storage,
-    * which without Constrained_Transport never reaches the cells; MHD
-    * builds need it (with CT_MODE 0, flip_fluxes, bfields.c:760-814, writes
-    * through zero-length Phi arrays into the cell's real flag and the next
-    * cell's prims), so it is accepted. */
+   /* euler (NUM_C 5) or mhd (NUM_C 8), NUM_N 1.  Without in.par
+    * Constrained_Transport, B evolves through the fluxes and CT_MODE 1/2 only
+    * sizes the reference's face-flux storage, which then never reaches the
+    * cells; MHD builds need it (with CT_MODE 0, flip_fluxes, bfields.c:
+    * 760-814, writes through zero-length Phi arrays into the cell's real
+    * flag and the next cell's prims), so it is accepted.  Constrained
+    * transport itself is built for 2D disks (CT_MODE 1, Nz = 1) in FP64,
+    * for every disk of the batch or none. */
    bool mhd = mods->hydro == DISCO_HYDRO_MHD;
    if( !((mods->hydro == DISCO_HYDRO_EULER && mods->num_c == 5) || (mhd && mods->num_c == 8)) ||
        mods->num_n != 1 || mods->ct_mode < 0 || mods->ct_mode > 2 )
       return DISCO_ERR_UNSUPPORTED;
-   for( int d=0 ; d<ndisk ; ++d ) if( params[d].CT ) return DISCO_ERR_UNSUPPORTED;
+   int ct = params[0].CT ? 1 : 0;
+   for( int d=0 ; d<ndisk ; ++d ) if( (params[d].CT ? 1 : 0) != ct ) return DISCO_ERR_ARG;
+   if( ct ){
+      if( !mhd || mods->ct_mode != 1 || precision != DISCO_PREC_FP64 ) return DISCO_ERR_UNSUPPORTED;
+      for( int d=0 ; d<ndisk ; ++d ) if( Nz[d] != 1 ) return DISCO_ERR_UNSUPPORTED;
+   }
    if( mods->boundary != DISCO_BC_FIXED && mods->boundary != DISCO_BC_ZEROGRAD &&
        mods->boundary != DISCO_BC_FIXED3D )
       return DISCO_ERR_UNSUPPORTED;
@@ -174,6 +181,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->stream = NULL;
    b->own_stream = NULL;
    b->tape = NULL; b->tape_names = NULL;
+   b->ct = ct;
 
    /* ---- topology */
    int cell = 0, ann = 0, face = 0, roff = 0, zoff = 0, npoff = 0;
@@ -347,6 +355,15 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->d_Qrz = dalloc<double>(b, (size_t)ann*5);
    v.err = dalloc<int>(b, 1);
    b->d_err = v.err;
+   if( ct ){
+      v.ct = 1;
+      v.Phi = dalloc<double>(b, 3*N); v.RKPhi = dalloc<double>(b, 3*N);
+      v.ctE = dalloc<double>(b, 4*N); v.ctB = dalloc<double>(b, 4*N);
+      v.pE = dalloc<double>(b, N); v.pB = dalloc<double>(b, N);
+      v.fEt = dalloc<double>(b, face); v.fBt = dalloc<double>(b, face);
+      v.fX = dalloc<double>(b, face);
+      v.fFlip = dalloc<unsigned char>(b, face);
+   }
    if( b->bc_zerograd && !b->zg_pairs.empty() ) b->d_zg_pairs = dupload(b, b->zg_pairs);
    make_float_view(b);
    if( prepare_zerograd<6,double>(b) || prepare_zerograd<9,double>(b) ||
@@ -423,12 +440,17 @@ extern "C" int disco_batch_set_cells(disco_batch *b, const double *prim, const d
                                      const double *piph, const double *dphi, const double *wiph,
                                      const int *real, const double *Phi){
    if( !b || !piph || !dphi ) return DISCO_ERR_ARG;
-   (void)real; (void)Phi;
+   (void)real;
    CK(cudaSetDevice(b->device));
    size_t N = b->ncell;
    int s;
    if( prim && (s = upload_r(b, b->vd.prim, prim)) ) return s;
    if( cons && (s = upload_q<double>(b, b->vd.cons, cons)) ) return s;
+   if( b->ct ){                     /* Phi[0..2] per cell, cell-major */
+      std::vector<double> t(3*N, 0.0);
+      if( Phi ) for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<3 ; ++q ) t[q*N + c] = Phi[3*c + q];
+      CK(xfer(b, b->vd.Phi, t.data(), t.size()*sizeof(double), cudaMemcpyHostToDevice));
+   }
    CK(xfer(b, b->vd.piph, piph, N*sizeof(double), cudaMemcpyHostToDevice));
    CK(xfer(b, b->vd.dphi, dphi, N*sizeof(double), cudaMemcpyHostToDevice));
    if( wiph ) CK(xfer(b, b->vd.wiph, wiph, N*sizeof(double), cudaMemcpyHostToDevice));
@@ -447,11 +469,15 @@ extern "C" int disco_batch_set_cells(disco_batch *b, const double *prim, const d
 extern "C" int disco_batch_get_cells(disco_batch *b, double *prim, double *cons,
                                      double *piph, double *dphi, double *wiph, double *Phi){
    if( !b ) return DISCO_ERR_ARG;
-   (void)Phi;
    CK(cudaSetDevice(b->device));
    CK(cudaStreamSynchronize(b->stream));
    size_t N = b->ncell;
    int s;
+   if( Phi && b->ct ){
+      std::vector<double> t(3*N);
+      CK(xfer(b, t.data(), b->vd.Phi, t.size()*sizeof(double), cudaMemcpyDeviceToHost));
+      for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<3 ; ++q ) Phi[3*c + q] = t[q*N + c];
+   }
    if( prim && (s = download_r(b, prim, b->vd.prim)) ) return s;
    if( cons && (s = download_q<double>(b, cons, b->vd.cons)) ) return s;
    if( piph ) CK(xfer(b, piph, b->vd.piph, N*sizeof(double), cudaMemcpyDeviceToHost));

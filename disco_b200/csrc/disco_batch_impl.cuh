@@ -9,6 +9,7 @@
 #include <vector>
 #include "disco_b200.h"
 #include "disco_kernels.cuh"
+#include "disco_ct.cuh"
 
 using namespace disco;
 
@@ -52,6 +53,7 @@ struct disco_batch {
    std::vector<const char *> *tape_names;
    cudaGraphExec_t graph;
    int have_cells;
+   int ct;                   /* 2D constrained transport (FP64 view only) */
 };
 
 static inline unsigned nblk(size_t n, unsigned t){ return (unsigned)((n + t - 1)/t); }
@@ -95,6 +97,15 @@ template<int Q, int NC, class R>
 static void launch_setup_qt(disco_batch *b, const ViewT<R> &v){
    unsigned ncb = (unsigned)b->cblk.size();
    k_setup<Q,NC,R><<<ncb, CB, 0, b->stream>>>(v, b->bc_fixed);
+   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+      if( b->ct ){                  /* set_B_fields (bfields.c:12-86), then cons2prim */
+         unsigned nfb = (unsigned)b->fblk.size();
+         k_I0<R><<<nblk((size_t)v.Nann*32, 128), 128, 0, b->stream>>>(v);
+         k_faces<Q,R><<<nfb, FB, 0, b->stream>>>(v, 0);
+         k_ct_face_init<Q,NC,R><<<nfb, FB, 0, b->stream>>>(v);
+         k_c2p<Q,NC,R><<<ncb, CB, 0, b->stream>>>(v, 0, b->bc_fixed, 0);
+      }
+   }
    k_wcell<Q,R><<<ncb, CB, 0, b->stream>>>(v);
    if( b->any_mm3 ) k_wmean<R><<<nblk(v.Nann, WM_WARPS), 32*WM_WARPS, 0, b->stream>>>(v, 0);
    launch_zerograd<Q,R>(b, v);                   /* main.c:53-62 */
@@ -115,6 +126,17 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    k_flux_t<Q,NC,1,R><<<nfb, FB, 0, s>>>(v);                          mark(b, "k_flux_r");
    if( b->any_3d ){ k_flux_t<Q,NC,2,R><<<nfb, FB, 0, s>>>(v);         mark(b, "k_flux_z"); }
    k_update<Q,NC,R><<<ncb, CB, 0, s>>>(v, first);                     mark(b, "k_update");
+   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+      if( b->ct ){                  /* onestep.c:140-146 and 160-167 */
+         k_ct_edges<R><<<ncb, CB, 0, s>>>(v);                           mark(b, "k_ct_edges");
+         k_ct_faces<R><<<nfb, FB, 0, s>>>(v);                           mark(b, "k_ct_faces");
+         k_ct_update<R><<<ncb, CB, 0, s>>>(v, first);                   mark(b, "k_ct_update");
+         if( first ){
+            k_ct_flag<R><<<nfb, FB, 0, s>>>(v);                         mark(b, "k_ct_flag");
+            k_ct_flip<R><<<nblk((size_t)v.Ntr*32, 128), 128, 0, s>>>(v); mark(b, "k_ct_flip");
+         }
+      }
+   }
    k_c2p<Q,NC,R><<<ncb, CB, 0, s>>>(v, last, b->bc_fixed, !b->bc_zerograd); mark(b, "k_c2p");
    launch_zerograd<Q,R>(b, v);
    if( last && b->nq && b->bc_zerograd ){

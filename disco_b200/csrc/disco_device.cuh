@@ -617,11 +617,13 @@ __device__ __forceinline__ void hlld_solve(const DiskParams &P, R w, const R *pr
 
 /* solve_riemann(), riemann.c:216-318, HLL / HLLC / HLLD (riemann 0 / 1 /
  * 2; HLLD needs MHD).  Returns G_q = (Flux_q - w*Ustr_q)*dAdt, the amount
- * subtracted from cons_L and added to cons_R (riemann.c:312-315). */
+ * subtracted from cons_L and added to cons_R (riemann.c:312-315), and, when
+ * eb is given (MHD), the inputs of flux_to_E (Hydro/mhd.c:293-316):
+ * eb = (Flux[BRR], Flux[BPP], Ustr[BRR]). */
 template<int Q, int NC, int DIM, class R>
 __device__ __forceinline__ void solve_riemann(const DiskParams &P, const R *primL,
                                               const R *primR, R r, R om,
-                                              R w, R dAdt, R *G){
+                                              R w, R dAdt, R *G, R *eb = nullptr){
    R Flux[Q], Ustr[Q];
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ){ Flux[q] = R(0.0); Ustr[q] = R(0.0); }
@@ -630,6 +632,7 @@ __device__ __forceinline__ void solve_riemann(const DiskParams &P, const R *prim
          hlld_solve<Q,DIM,R>(P, w, primL, primR, Flux, Ustr, r);
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) G[q] = (Flux[q] - w*Ustr[q])*dAdt;
+         if( eb ){ eb[0] = Flux[BRR]; eb[1] = Flux[BPP]; eb[2] = Ustr[BRR]; }
          return;
       }
    }
@@ -665,6 +668,9 @@ __device__ __forceinline__ void solve_riemann(const DiskParams &P, const R *prim
    }
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) G[q] = (Flux[q] - w*Ustr[q])*dAdt;
+   if constexpr ( NC == 8 ){
+      if( eb ){ eb[0] = Flux[BRR]; eb[1] = Flux[BPP]; eb[2] = Ustr[BRR]; }
+   }
 }
 
 /* ------------------------------------------------------------ planets */

@@ -94,6 +94,17 @@ struct ViewT {
    int nq;
    double dtfac;        /* 1 in the first substep, 0.5 in the second (timestep.c:39) */
    int *err;
+   /* 2D constrained transport (Constrained_Transport 1, CT_MODE 1; bfields.c).
+    * Per cell, SoA [s*Ncell + c]: Phi / RKPhi, s = 0 the magnetic flux through
+    * the cell's phi face at piph, s = 1 / 2 the flux through the r-face the cell
+    * owns in the track inside / outside it (the face ending at its piph,
+    * LRtype 1 / 0); ctE / ctB the four edge values E[0..3], B[0..3]
+    * (riemann.c:73-85, 175-187) before averaging; pE / pB the phi face's
+    * (Ez, Br) from flux_to_E.  Per r-face: fEt / fBt (Erz, Brz), fX the
+    * E dl dt of update_B_fluxes, fFlip the flag of check_flipped. */
+   int ct;
+   double *Phi, *RKPhi, *ctE, *ctB, *pE, *pB, *fEt, *fBt, *fX;
+   unsigned char *fFlip;
 };
 
 template<class R>
@@ -167,6 +178,18 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_BEGIN) k_begin(ViewT<R
       if constexpr ( sizeof(R) != sizeof(double) ){
          /* the carry belongs to cons; averaged with it (RKcons keeps none) */
          if( !first ) v.ccarry[q*N + c] = (1.-RK)*v.ccarry[q*N + c];
+      }
+   }
+   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+      if( v.ct ){                   /* timestep.c:22 and adjust_RK_cons, misc.c:239-241 */
+#pragma unroll
+         for( int s=0 ; s<3 ; ++s ){
+            double ph = v.Phi[s*N + c];
+            double rk;
+            if( first ){ rk = ph; v.RKPhi[s*N + c] = ph; }
+            else rk = v.RKPhi[s*N + c];
+            v.Phi[s*N + c] = (1.-RK)*ph + RK*rk;
+         }
       }
    }
    const R dpL = (R)v.dphi[cm], dpC = (R)v.dphi[c], dpR = (R)v.dphi[cp];
@@ -528,7 +551,19 @@ __global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R
    const double *rj = v.rj + P.rj0 + 1;
    double r = DIM == 1 ? .5*(rj[j]+rj[j]) : centroid_r(rj[j], rj[j-1]);    /* face cm[0] */
    R G[Q];
-   solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G);
+   if constexpr ( NC == 8 && DIM == 1 && sizeof(R) == sizeof(double) ){
+      if( v.ct ){                    /* flux_to_E dim 1, Hydro/mhd.c:304-308 */
+         R eb[3];
+         solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G, eb);
+         double irfac = 1.0/(1.0/r);
+         v.fEt[f] = -eb[1]*r;
+         v.fBt[f] = eb[2]*irfac;
+      }else{
+         solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G);
+      }
+   }else{
+      solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G);
+   }
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) v.fG[(size_t)q*v.Nf + f] = G[q];
    raise_err(v, err);
@@ -541,7 +576,8 @@ __global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R
  * w = r wiph[cL]. */
 template<int Q, int NC, class R>
 __device__ __forceinline__ void phi_face_flux(const ViewT<R> &v, const DiskParams &P, int a,
-                                              int cL, int cR, double r, double dAdt, R *G){
+                                              int cL, int cR, double r, double dAdt, R *G,
+                                              R *eb = nullptr){
    const int N = v.Ncell;
    R primL[Q], primR[Q];
    R dL = (R)v.dphi[cL], dR = (R)v.dphi[cR];
@@ -555,7 +591,7 @@ __device__ __forceinline__ void phi_face_flux(const ViewT<R> &v, const DiskParam
       primL[BPP] = Bp; primR[BPP] = Bp;
    }
    double w = r*v.wiph[cL];
-   solve_riemann<Q,NC,0,R>(P, primL, primR, (R)r, (R)v.ann_om[a], (R)w, (R)dAdt, G);
+   solve_riemann<Q,NC,0,R>(P, primL, primR, (R)r, (R)v.ann_om[a], (R)w, (R)dAdt, G, eb);
 }
 
 /* ------------------------------------------------------------------ k_update
@@ -581,17 +617,37 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
    bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
    const double *rj = v.rj + P.rj0 + 1;
    const double *zk = v.zk + P.zk0 + 1;
-   if( real ){                      /* uniform over the block: one annulus */
+   /* With constrained transport phi_flux also runs on the ghost annuli next
+    * to the real ones (misc.c:382-397): their faces' E is needed, their cons
+    * updates are not (the ghosts' cons never reach a real cell). */
+   bool ctE = false;
+   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+      if( v.ct ){
+         int jmin = P.NgRa == 0 ? 0 : P.NgRa-1, jmax = P.NgRb == 0 ? P.Nr : P.Nr-P.NgRb+1;
+         int kmin = P.NgZa == 0 ? 0 : P.NgZa-1, kmax = P.NgZb == 0 ? P.Nz : P.Nz-P.NgZb+1;
+         ctE = j >= jmin && j < jmax && k >= kmin && k < kmax;
+      }
+   }
+   if( real || ctE ){               /* uniform over the block: one annulus */
       double dA = (rj[j]-rj[j-1])*(zk[k]-zk[k-1]);       /* get_dA(.,.,0) */
       double dAdtp = dA*(v.ds[d].dt*v.dtfac);
       double rc = centroid_r(rj[j], rj[j-1]);
       if( i < np ){
          R G[Q];
-         phi_face_flux<Q,NC,R>(v, P, a, c, c0 + (i < np-1 ? i+1 : 0), rc, dAdtp, G);
+         int cn = c0 + (i < np-1 ? i+1 : 0);
+         if( ctE ){                 /* flux_to_E dim 0, Hydro/mhd.c:298-303 */
+            R eb[3];
+            phi_face_flux<Q,NC,R>(v, P, a, c, cn, rc, dAdtp, G, eb);
+            double irfac = 1.0/(1.0/rc);
+            v.pE[c] = eb[0]*irfac;
+            v.pB[c] = eb[2]*irfac;
+         }else{
+            phi_face_flux<Q,NC,R>(v, P, a, c, cn, rc, dAdtp, G);
+         }
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) sG[q][threadIdx.x+1] = G[q];
       }
-      if( threadIdx.x == 0 ){
+      if( threadIdx.x == 0 && real ){
          R G[Q];
          phi_face_flux<Q,NC,R>(v, P, a, cprev, c, rc, dAdtp, G);
 #pragma unroll
@@ -715,7 +771,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
          if constexpr ( sizeof(R) != sizeof(double) ) v.ccarry[q*N + c] = cc[q];
       }
    }
-   if( first ){
+   if( first && !v.ct ){            /* with CT the edge fields read the old piph first */
       piph = v.piph_new[c];
       dphi = get_dp(piph, v.piph_new[cprev], P.Pmax, &err);
       v.piph[c] = piph; v.dphi[c] = dphi;
@@ -816,6 +872,12 @@ __device__ __forceinline__ bool fixed_ghost_init(const DiskParams &P, int bc, in
    return true;
 }
 
+/* B_faces_to_cells type 1 under constrained transport (disco_ct.cuh) */
+template<class R>
+__device__ void ct_cons_B(const ViewT<R> &v, const DiskParams &P, int a, int c0, int np, int i,
+                          int j, int k, double rp, double rm, double zp, double zm, double *cons,
+                          int *err);
+
 /* ------------------------------------------------------------------ k_c2p
  *   calc_prim    misc.c:290-325 (euler cons2prim, FP64) on real cells
  *   boundary     Boundary/fixed.c:11-60 (r ghosts re-initialised)
@@ -849,6 +911,13 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v,
          double cons[Q];
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) cons[q] = v.cons[q*N + c];
+         if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+            if( v.ct ){                  /* onestep.c:183-185 */
+               ct_cons_B(v, P, a, c0, np, i, j, k, rp, rm, zp, zm, cons, &err);
+               v.cons[BRR*N + c] = cons[BRR];
+               v.cons[BPP*N + c] = cons[BPP];
+            }
+         }
          double dph2 = get_dp(piph, phim, P.Pmax, &err);
          double dV2 = dV_of(rp, rm, dph2, zp, zm);
          cons2prim<Q,NC>(P, cons, prim, centroid_r(rp, rm), v.ann_om[a], dV2);
@@ -1177,7 +1246,8 @@ __global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc){
       if( P.rotframe ) prim[UPP] -= P.RotOmega;
       double om = get_om(P, r);
       prim2cons<Q,NC,double>(P, prim, cons, r, om, dV);
-      cons2prim<Q,NC>(P, cons, prim, r, om, dV);
+      /* with CT, cons2prim follows set_B_fields (domain.c:211-237): k_c2p */
+      if( !v.ct ) cons2prim<Q,NC>(P, cons, prim, r, om, dV);
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){ v.prim[q*N+c] = (R)prim[q]; v.cons[q*N+c] = cons[q]; }
    }else{
@@ -1191,6 +1261,17 @@ __global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc){
    if constexpr ( sizeof(R) != sizeof(double) ){
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ) v.ccarry[q*N+c] = 0.0;
+   }
+   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+      if( v.ct ){                        /* set_B_fields, bfields.c:22-42 */
+         double x[3] = { centroid_r(rj[j], rj[j-1]), piph, centroid_z(zk[k], zk[k-1]) };
+         double pb[Q];
+         initial<Q,NC>(P, pb, x);
+         double dA = (rj[j]-rj[j-1])*(zk[k]-zk[k-1]);
+         v.Phi[c] = pb[BPP]*dA;
+         v.Phi[N + c] = 0.0;
+         v.Phi[2*N + c] = 0.0;
+      }
    }
    raise_err(v, err);
 }

@@ -11,7 +11,13 @@
  *   P     = rho cs^2 / gamma                      (sound speed cs)
  *   Omega = r^-3/2 + amp cs u_phi / r
  *   v_r   = amp cs u_r,   v_z = amp cs u_z        (u in [-1,1), hashed)
- *   B     = (0, 0, Bz),   Bz = sqrt(2 P / beta)   (vertical field, plasma beta)
+ *   B     = (Br, Bphi, Bz)
+ *           Bz   = sqrt(2 P / beta)               (vertical field, plasma beta)
+ *           Bphi = sqrt(2 P / beta_phi)           (uniform toroidal field; 0 when
+ *                                                  beta_phi = 0)
+ *           Br   = b_r (rmin / r) u(phi),  u = 4 s (1 - s) - 2/3,  s = phi/phimax
+ *                                                 (mod 1): r Br is independent of r
+ *                                                  and Bphi of phi, so div B = 0
  *   X     = (z - zmin)/(zmax - zmin)              (passive scalar, NUM_N>0)
  *
  * With Init_Par2 = 1 the disk rotates rigidly instead (Omega = 1 + noise),
@@ -20,11 +26,12 @@
  * whose value matters, and a CPU and a GPU build agree bit for bit.
  *
  * Noise only inside [rmin, rmax] x [zmin, zmax] (ghost cells stay smooth).
- * Uses +,-,*,/ and sqrt only, so host and device values are bit-identical.
+ * Uses +,-,*,/, sqrt and floor only, so host and device values are
+ * bit-identical.
  *
  * Parameters (in.par): Init_Par0 = seed, Init_Par1 = amp (fraction of cs),
  * Init_Par2 = kind (0 Keplerian, 1 rigid), Init_Par3 = cs, Init_Par4 = beta,
- * Adiabatic_Index, R_Min/R_Max,
+ * Init_Par5 = beta_phi, Init_Par6 = b_r, Adiabatic_Index, R_Min/R_Max,
  * Z_Min/Z_Max, Phi_Max.
  */
 #ifndef DISCO_IC_MHD_SHEAR_H
@@ -34,6 +41,7 @@
 
 typedef struct {
    double cs, beta, amp, gam;
+   double beta_phi, b_r;
    double rmin, rmax, zmin, zmax, phimax;
    uint64_t seed;
    int kind;
@@ -81,7 +89,16 @@ DISCO_HD void disco_ic_mhd_shear_eval(const disco_ic_mhd_shear *p, int num_c, in
    prim[4] = vz;
    int q;
    for( q=5 ; q<num_c ; ++q ) prim[q] = 0.0;
-   if( num_c >= 8 ) prim[7] = sqrt(2.0 * (rho * p->cs * p->cs / p->gam) / p->beta);
+   if( num_c >= 8 ){
+      double p0 = rho * p->cs * p->cs / p->gam;
+      prim[7] = sqrt(2.0 * p0 / p->beta);
+      if( p->beta_phi > 0.0 ) prim[6] = sqrt(2.0 * p0 / p->beta_phi);
+      if( p->b_r != 0.0 ){
+         double s = phi / p->phimax;
+         s = s - floor(s);
+         prim[5] = p->b_r * (p->rmin / r) * (4.0 * s * (1.0 - s) - 2.0 / 3.0);
+      }
+   }
    if( num_q > num_c ){
       double zr = p->zmax > p->zmin ? (z - p->zmin) / (p->zmax - p->zmin) : 0.5;
       prim[num_c] = zr;

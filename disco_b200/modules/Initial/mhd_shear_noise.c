@@ -1,7 +1,9 @@
 /*
  * Disco Initial module `mhd_shear_noise`: a magnetised Keplerian shearing
- * disk (vertical field of plasma beta Init_Par4, sound speed Init_Par3) with
- * seeded, hash-based velocity noise of amplitude Init_Par1 * cs.  Drop this
+ * disk (vertical field of plasma beta Init_Par4, sound speed Init_Par3;
+ * optional toroidal field of beta Init_Par5 and radial field of amplitude
+ * Init_Par6) with seeded, hash-based velocity noise of amplitude
+ * Init_Par1 * cs.  Drop this
  * file into a Disco tree's Initial/ directory and select it with
  * `INITIAL = mhd_shear_noise`; it follows the Initial-module contract
  * (setICparams/initial, e.g. Initial/flock.c) and evaluates the same
@@ -19,6 +21,8 @@ void setICparams( struct domain * theDomain ){
    icp.amp    = theDomain->theParList.initPar1;
    icp.cs     = theDomain->theParList.initPar3;
    icp.beta   = theDomain->theParList.initPar4;
+   icp.beta_phi = theDomain->theParList.initPar5;
+   icp.b_r    = theDomain->theParList.initPar6;
    icp.gam    = theDomain->theParList.Adiabatic_Index;
    icp.rmin   = theDomain->theParList.rmin;
    icp.rmax   = theDomain->theParList.rmax;

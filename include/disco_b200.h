@@ -136,13 +136,19 @@ int disco_batch_sizes(const disco_batch *b, int64_t *ncell, int64_t *nreal, int 
  * (the reference's struct cell prim[NUM_Q] / cons[NUM_Q], paul.h:185-186).
  * real[] is the reference's cell->real flag.  cons may be NULL (then cons is
  * rebuilt from prim with prim2cons on the device, as setupCells does,
- * domain.c:205).  Phi (num_faces doubles per cell) may be NULL when CT is off.
+ * domain.c:205).  Phi is the constrained-transport state (in.par
+ * Constrained_Transport 1, built for CT_MODE 1 in 2D): 3 doubles per cell,
+ * the reference's cell->Phi[NUM_FACES] (paul.h:198) -- Phi[0] the magnetic
+ * flux through the phi face at piph, Phi[1] / Phi[2] that through the r face
+ * the cell owns in the track inside / outside it (bfields.c:734-758).  It
+ * is ignored when CT is off and may be NULL (zeros) when CT is on.
  */
 int disco_batch_set_cells(disco_batch *b, const double *prim, const double *cons,
                           const double *piph, const double *dphi, const double *wiph,
                           const int *real, const double *Phi);
 
-/* Download cell state (same layout); any pointer may be NULL to skip it. */
+/* Download cell state (same layout; Phi only when CT is on); any pointer
+ * may be NULL to skip it. */
 int disco_batch_get_cells(disco_batch *b, double *prim, double *cons,
                           double *piph, double *dphi, double *wiph, double *Phi);
 

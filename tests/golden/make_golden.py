@@ -50,6 +50,17 @@ CASES = {
     "c1_mhd3d": ("c1_mhd3d", {"Num_R": 8, "Num_Z": 6}, 5),
     "c1_mhd3d_rigid": ("c1_mhd3d_nograv", {"Num_R": 8, "Num_Z": 6, "Init_Par2": 1,
                                            "Init_Par4": 10.0}, 6),
+    # 2D constrained transport (bfields.c) with toroidal and radial field:
+    # Keplerian HLLD, libm-free rigid HLLD, and HLL + forward Euler with the
+    # by-cell mesh
+    "c1_ct2d": ("c1_mhd2d", {"Num_R": 12, "Constrained_Transport": 1, "Init_Par5": 20.0,
+                             "Init_Par6": 0.05}, 8),
+    "c1_ct_rigid": ("c1_mhd2d_nograv", {"Num_R": 14, "Init_Par2": 1, "Init_Par4": 10.0,
+                                        "Constrained_Transport": 1, "Init_Par5": 20.0,
+                                        "Init_Par6": 0.05}, 8),
+    "c1_ct_hll_fe": ("c1_mhd2d", {"Num_R": 10, "Riemann_Solver": 0, "Timestep": 1,
+                                  "Mesh_Motion": 1, "Constrained_Transport": 1,
+                                  "Init_Par5": 10.0, "Init_Par6": 0.1}, 6),
 }
 
 # the in.par template each module configuration starts from
@@ -82,6 +93,8 @@ def main():
         dn = pyoracle.run_ref(cfg, text, n)
         F = dn["faces_1"]
         extra = {}
+        if "Phi" in d0 and over.get("Constrained_Transport"):
+            extra.update(s0_Phi=d0["Phi"], sN_Phi=dn["Phi"])
         if "faces_2" in dn:
             Z = dn["faces_2"]
             extra = dict(z_fIndex=Z["fIndex"], z_iL=Z["iL"], z_iR=Z["iR"], z_LRtype=Z["LRtype"],

@@ -1,0 +1,154 @@
+"""GPU parity of 2D constrained transport (Constrained_Transport 1, CT_MODE 1)
+against the reference's own build (bfields.c, riemann.c edge bookkeeping,
+onestep.c:140-185), from the fixtures of tests/golden/make_golden.py.
+
+The CT state is the per-cell face-flux array Phi[3] (Phi[0] the phi face at
+piph, Phi[1] / Phi[2] the r face the cell owns in the track inside / outside
+it).  The comparison covers every slot a real cell reads: Phi[0] of real
+cells and the owned-face slots of every track next to a real annulus; the
+remaining slots (ghost cells' own faces towards further ghosts) follow edge
+fields the reference leaves stale and reach nothing.
+
+- c1_ct_rigid (no gravity, so no libm call whose value matters): bit-exact,
+  state, slots, dt sequence and face lists.
+- c1_ct2d (Keplerian, point-mass gravity) and c1_ct_hll_fe (HLL, forward
+  Euler, by-cell mesh): relative L1 1e-11 (the libm differences of the
+  point-mass force, as for the other MHD fixtures), face lists bit-exact.
+- At full size, the property CT exists for: each real cell's discrete
+  divergence (net flux through its faces) stays at its initial value to
+  round-off (the reference's own runs keep it to 1e-17 of 1e-4).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import disco_b200 as db
+from helpers import case_disk, par_with, rel_l1, rel_l1_cols
+
+pytestmark = pytest.mark.gpu
+
+CT_CASES = ["c1_ct2d", "c1_ct_rigid", "c1_ct_hll_fe"]
+CT_TOL = {"c1_ct2d": 1e-11, "c1_ct_hll_fe": 1e-11}
+
+
+def _observed_slots(disk):
+    """Mask (ncell x 3) of the Phi slots real cells read."""
+    Nr, Ng = disk.Nr, disk.Ng
+    j = np.repeat(np.arange(disk.Nr * disk.Nz) % Nr, disk.Np)
+    m = np.zeros((disk.ncell, 3), bool)
+    m[:, 0] = disk.real == 1
+    m[:, 1] = (j >= Ng[0]) & (j <= Nr - Ng[1])
+    m[:, 2] = (j >= Ng[0] - 1) & (j <= Nr - Ng[1] - 1)
+    return m
+
+
+def _from_golden(disk, g):
+    b = db.Batch([disk], setup=False)
+    b.set_cells(g["s0_prim"], g["s0_cons"], g["s0_piph"], g["s0_dphi"], g["s0_wiph"], g["real"],
+                Phi=g["s0_Phi"])
+    return b
+
+
+def divergence(b, disk):
+    """Net magnetic flux out of each cell through its current faces: outer
+    r faces - inner r faces + Phi[0](c) - Phi[0](c-1)."""
+    st = b.get_cells()
+    Phi = st["Phi"]
+    F = b.faces(0, 1)
+    L, R, lr = F["iL"], F["iR"], F["LRtype"]
+    v = np.where(lr == 0, Phi[L, 2], Phi[R, 1])
+    div = np.zeros(disk.ncell)
+    np.add.at(div, L, v)
+    np.add.at(div, R, -v)
+    off = np.concatenate([[0], np.cumsum(disk.Np)])
+    for a in range(len(disk.Np)):
+        c = np.arange(off[a], off[a + 1])
+        div[c] += Phi[c, 0] - Phi[np.roll(c, 1), 0]
+    return div, Phi
+
+
+@pytest.mark.parametrize("case", CT_CASES)
+def test_ct_setup_matches_reference(case):
+    """set_B_fields + B_faces_to_cells + cons2prim on the device reproduce the
+    reference's step-0 state bit for bit."""
+    disk, g = case_disk(case)
+    b = db.Batch([disk])
+    st = b.get_cells()
+    r = disk.real == 1
+    assert np.array_equal(st["prim"][r], g["s0_prim"][r])
+    assert np.array_equal(st["cons"][r], g["s0_cons"][r])
+    m = _observed_slots(disk)
+    assert np.array_equal(st["Phi"][m], g["s0_Phi"][m])
+    assert b.mindt()[0] == g["s0_dt_next"]
+
+
+@pytest.mark.parametrize("case", CT_CASES)
+def test_ct_steps_match_reference(case):
+    disk, g = case_disk(case)
+    b = _from_golden(disk, g)
+    dts = []
+    for _ in range(int(g["nsteps"])):
+        dt = b.mindt()[0]
+        dts.append(dt)
+        b.timestep(dt)
+    b.sync()
+    st = b.get_cells()
+    r = disk.real == 1
+    m = _observed_slots(disk)
+    F = b.faces(0, 1)
+    for k in ("fIndex", "iL", "iR", "LRtype"):
+        assert np.array_equal(F[k], g[k]), k
+    if case not in CT_TOL:
+        assert np.array_equal(np.array(dts), g["dt"])
+        assert np.array_equal(st["prim"][r], g["sN_prim"][r])
+        assert np.array_equal(st["cons"][r], g["sN_cons"][r])
+        assert np.array_equal(st["Phi"][m], g["sN_Phi"][m])
+        return
+    tol = CT_TOL[case]
+    assert np.max(np.abs(np.array(dts) / g["dt"] - 1.0)) < tol
+    for q, e in enumerate(rel_l1_cols(st["prim"][r], g["sN_prim"][r])):
+        assert e < tol, ("prim", q, e)
+    for q, e in enumerate(rel_l1_cols(st["cons"][r], g["sN_cons"][r])):
+        assert e < tol, ("cons", q, e)
+    for s in range(3):
+        e = rel_l1(st["Phi"][m[:, s], s], g["sN_Phi"][m[:, s], s])
+        assert e < tol, ("Phi", s, e)
+
+
+def _ct_disk(nr, ct):
+    _, opt = db.template_paths("c1_mhd2d")
+    p = par_with({"Num_R": nr, "Constrained_Transport": ct, "Init_Par5": 20.0,
+                  "Init_Par6": 0.05, "Init_Par1": 0.05}, base="c1_mhd2d")
+    disk = db.Disk.from_files(p, opt)
+    os.unlink(p)
+    return disk
+
+
+def test_ct_preserves_divergence():
+    """128 annuli (about 70k cells), 40 steps of the Keplerian disk with
+    shear, so faces flip in every step: the discrete divergence of each
+    real cell is unchanged to round-off under CT."""
+    disk = _ct_disk(128, 1)
+    b = db.Batch([disk])
+    d0, P0 = divergence(b, disk)
+    F0 = b.faces(0, 1)
+    b.run(40)
+    b.sync()
+    d1, P1 = divergence(b, disk)
+    F1 = b.faces(0, 1)
+    # the sliding annuli have re-paired their faces (flips happened)
+    assert not np.array_equal(F0["iR"], F1["iR"])
+    r = disk.real == 1
+    scale = np.abs(P1).max()
+    drift = np.abs(d1 - d0)[r].max()
+    print("div drift %.3e of max |Phi| %.3e (initial max |div| %.3e)" % (drift, scale, np.abs(d0[r]).max()))
+    assert drift <= 1e-12 * scale
+    assert np.abs(P1[r, 1:]).max() > 1.5 * np.abs(P0[r, 1:]).max()   # the field did evolve
+
+
+def test_ct_refuses_unsupported():
+    disk = _ct_disk(16, 1)
+    with pytest.raises(db.DiscoError) as e:
+        db.Batch([disk], precision=db.PREC_MIXED)
+    assert e.value.status == 3
