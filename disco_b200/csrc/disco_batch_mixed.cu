@@ -3,6 +3,7 @@
  * disco_kernels.cuh instantiated with R = float.  This file is compiled with
  * FMA contraction (--fmad=true); the FP64 path in disco_batch.cu is not.
  */
+#define DISCO_MIXED_TU 1
 #include "disco_batch_impl.cuh"
 
 void mixed_launch_mindt(disco_batch *b){ launch_mindt_t(b, b->vf); }

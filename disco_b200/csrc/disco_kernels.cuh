@@ -40,9 +40,16 @@ namespace disco {
  * register budget per thread follows: 65536 / (128 * MB)).  The kernels
  * are latency-bound, so warps in flight matter more than the spills the
  * tighter budget costs: on ragged64 the hydro step went from 7.26 to
- * 5.41 ms (FP64) and 5.60 to 4.57 ms (mixed) with these values against
- * the compiler's choice (MB 1).  The MHD instantiations (HLLD needs about
- * 160 registers) keep MB_MHD. */
+ * 5.41 ms (FP64) and 5.60 to 4.57 ms (mixed) with MB 8-12 against the
+ * compiler's choice (MB 1).  tuned.h holds the per-kernel values the
+ * autotuner (disco_b200/autotune.py) measured on a B200, per precision
+ * (DISCO_MIXED_TU marks the FP32 translation unit); a -DMB_x on the
+ * command line overrides them, and the defaults below fill the rest.  The
+ * MHD instantiations (HLLD needs about 160 registers) keep MB_MHD. */
+#include "tuned.h"
+#ifndef MB_FACES
+#define MB_FACES 1
+#endif
 #ifndef MB_STEP
 #define MB_STEP 8
 #endif
@@ -320,7 +327,7 @@ __global__ void k_I0(ViewT<R> v){
  * gather reads each twice (sum, limiter), and recomputing them there from
  * the two cells' scattered states was measured 5x slower than storing. */
 template<int Q, class R>
-__global__ void __launch_bounds__(FB) k_faces(ViewT<R> v, int with_slopes){
+__global__ void __launch_bounds__(FB, MB_FACES) k_faces(ViewT<R> v, int with_slopes){
    int2 b = v.fblk[blockIdx.x];
    int t = b.x, dd = b.y + threadIdx.x;
    int A = v.tr_a[t], B = v.tr_b[t];

@@ -1,0 +1,46 @@
+"""The autotuner's selection and header output (CPU; the measurement itself
+runs on the GPU: python -m disco_b200.autotune measure)."""
+import os
+import re
+import subprocess
+
+from disco_b200 import autotune as at
+from disco_b200 import build as native
+
+
+def _table():
+    # ms per step per kernel for three candidates; each kernel has its own best
+    return {"fp64": {4: {"k_begin": 1.0, "k_faces": 2.0, "k_update": 1.5},
+                     8: {"k_begin": 0.8, "k_faces": 2.1, "k_update": 1.2},
+                     16: {"k_begin": 0.9, "k_faces": 1.7, "k_update": 2.0}},
+            "mixed": {4: {"k_begin": 0.7, "k_faces": 1.0, "k_update": 1.0},
+                      8: {"k_begin": 0.9, "k_faces": 0.9, "k_update": 1.1},
+                      16: {"k_begin": 0.8, "k_faces": 1.2, "k_update": 0.9}}}
+
+
+def test_choose_per_kernel_and_precision():
+    best = at.choose(_table())
+    assert best["fp64"] == {"k_begin": 8, "k_faces": 16, "k_update": 8}
+    assert best["mixed"] == {"k_begin": 4, "k_faces": 8, "k_update": 16}
+
+
+def test_header_defines_each_precision(tmp_path):
+    res = _table()
+    path = str(tmp_path / "tuned.h")
+    at.write_header(res, at.choose(res), "test", path=path)
+    src = open(path).read()
+    # the header must select the values by translation unit
+    for tu, expect in (("", {"MB_BEGIN": 8, "MB_FACES": 16, "MB_UPDATE": 8}),
+                       ("-DDISCO_MIXED_TU", {"MB_BEGIN": 4, "MB_FACES": 8, "MB_UPDATE": 16})):
+        cmd = ["gcc", "-E", "-dM", "-x", "c"] + ([tu] if tu else []) + [path]
+        out = subprocess.run(cmd, capture_output=True, text=True, check=True).stdout
+        got = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define (MB_\w+) (\d+)", out)}
+        assert got == expect, (tu, got)
+    assert "-> 16" in src
+
+
+def test_committed_header_covers_every_tuned_kernel():
+    src = open(at.TUNED).read()
+    for macro in at.MACROS.values():
+        assert src.count("#define %s " % macro) == 2, macro   # one per precision
+    assert os.path.dirname(at.TUNED) == os.path.join(native.HERE, "csrc")
