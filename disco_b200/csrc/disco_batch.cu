@@ -355,6 +355,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->d_Qrz = dalloc<double>(b, (size_t)ann*5);
    v.err = dalloc<int>(b, 1);
    b->d_err = v.err;
+   v.topo = dalloc<int>(b, 1);
    if( ct ){
       v.ct = 1;
       v.Phi = dalloc<double>(b, 3*N); v.RKPhi = dalloc<double>(b, 3*N);
@@ -455,6 +456,7 @@ extern "C" int disco_batch_set_cells(disco_batch *b, const double *prim, const d
    CK(xfer(b, b->vd.dphi, dphi, N*sizeof(double), cudaMemcpyHostToDevice));
    if( wiph ) CK(xfer(b, b->vd.wiph, wiph, N*sizeof(double), cudaMemcpyHostToDevice));
    if( b->vd.ccarry ) CK(cudaMemsetAsync(b->vd.ccarry, 0, (size_t)b->Q*N*sizeof(double), b->stream));
+   CK(cudaMemsetAsync(b->vd.topo, 0, sizeof(int), b->stream));      /* new piph: faces stale */
    if( prim && !cons ){
       unsigned ncb = (unsigned)b->cblk.size();
       if( b->prec == DISCO_PREC_MIXED ) mixed_launch_prim2cons(b);
@@ -495,6 +497,7 @@ static int launch_mindt(disco_batch *b){
 extern "C" int disco_batch_setup_cells(disco_batch *b){
    if( !b ) return DISCO_ERR_ARG;
    CK(cudaSetDevice(b->device));
+   CK(cudaMemsetAsync(b->vd.topo, 0, sizeof(int), b->stream));
    if( b->prec == DISCO_PREC_MIXED ) mixed_launch_setup(b);
    else launch_setup_t(b, b->vd);
    CK(cudaGetLastError());
