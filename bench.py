@@ -53,10 +53,14 @@ def kernel_bytes(name, first, N, Nf, Na):
         # reads cons, piph, dphi (+wiph on the last substep); writes prim
         return N * w * (2 * Q + 2) + (N * w if not first else 0)
     if name == "k_I0":
-        return N * w + Na * 4
+        # RK2 keeps the faces in the first substep (k_I0 returns at once)
+        return 0 if first else N * w + Na * 4
     if name == "k_faces":
         # reads piph, dphi, prim, gradp; writes the face lists, geometry,
-        # PLM face slopes and consL/consR
+        # PLM face slopes and consL/consR -- or, in the first substep, reads
+        # the kept face cells and centres and writes the slopes only
+        if first:
+            return N * w * (2 * Q + 2) + Nf * (4 + 4 + w + Q * w)
         return N * w * (2 * Q + 2) + N * 8 + Nf * (4 + 4 + 1 + 3 * w + Q * w)
     if name == "k_gradr":
         # reads the face slopes and areas, the cell's geometry; writes gradr

@@ -115,6 +115,10 @@ static void launch_setup_qt(disco_batch *b, const ViewT<R> &v){
 template<int Q, int NC, class R>
 static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int last, double dtfac){
    v.dtfac = dtfac;
+   /* RK2: the first substep keeps the faces the previous step's second
+    * substep built from the same piph; that substep marks them valid */
+   v.topo_reuse = first && b->timestep_mode == 0;
+   v.topo_set = !first;
    cudaStream_t s = b->stream;
    unsigned ncb = (unsigned)b->cblk.size(), nfb = (unsigned)b->fblk.size();
    k_begin<Q,NC,R><<<ncb, CB, 0, s>>>(v, RK, first);                  mark(b, "k_begin");

@@ -94,6 +94,13 @@ struct ViewT {
    int *consL, *consR;                /* r-tracks outside / inside the cell */
    int *consZL, *consZR;              /* z-tracks above / below the cell */
    double *diag_part;   /* per cell block: nq sums + volume */
+   /* *topo = 1 when the face lists and geometry were built from the current
+    * piph (the second RK2 substep builds them after the cells have moved, so
+    * the next step's first substep, with the same piph, keeps them and only
+    * re-evaluates the face slopes); topo_reuse / topo_set select the
+    * behaviour of one launch sequence. */
+   int *topo;
+   int topo_reuse, topo_set;
    /* energy-frame Omega of omega.c:62-110, evaluated once by k_precompute at
     * the radii the step uses (same device expressions, so bit-identical to
     * evaluating them in place): annulus centroid (om, dOm/dr) and r-face */
@@ -287,6 +294,7 @@ __global__ void k_I0(ViewT<R> v){
    int warp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
    int lane = threadIdx.x & 31;
    if( warp >= v.Nann ) return;
+   if( v.topo_reuse && *v.topo ) return;
    int a = warp;
    int np = v.ann_np[a], c0 = v.ann_off[a];
    const DiskParams &P = v.dp[v.ann_disk[a]];
@@ -341,6 +349,23 @@ __global__ void __launch_bounds__(FB, MB_FACES) k_faces(ViewT<R> v, int with_slo
    double Pmax = P.Pmax;
    int err = 0;
 
+   if( v.topo_reuse && *v.topo ){   /* same piph as the last build: slopes only */
+      if( !with_slopes ) return;
+      int cL = v.fL[f], cR = v.fR[f];
+      double phic = v.fphic[f];
+      R dxL = (R)v.tr_dxL[t], dxR = (R)v.tr_dxR[t];
+      double phiL = v.piph[cL] - .5*v.dphi[cL], phiR = v.piph[cR] - .5*v.dphi[cR];
+      R dpL = (R)get_signed_dp(phic, phiL, Pmax, &err);
+      R dpR = (R)get_signed_dp(phiR, phic, Pmax, &err);
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ){
+         R WL = v.prim[q*N + cL] + dpL*v.gradp[q*N + cL];
+         R WR = v.prim[q*N + cR] - dpR*v.gradp[q*N + cR];
+         v.fS[(size_t)q*v.Nf + f] = (WR-WL)/(dxR+dxL);
+      }
+      raise_err(v, err);
+      return;
+   }
    int lo = dd - NB > 0 ? dd - NB : 0;
    int hi = dd < NA ? dd : NA;
    while( lo < hi ){
@@ -608,7 +633,8 @@ __device__ __forceinline__ void phi_face_flux(const ViewT<R> &v, const DiskParam
  *                FP64 in both forms (the disk's force balance)
  *   move/clean/calc_dp   misc.c:256-288 (first substep; piph_new from k_begin)
  * calc_prim, the boundary, and the fused getmindt / diagnostics follow in
- * k_c2p. */
+ * k_c2p (run inside this kernel instead, the extra registers cost more than
+ * the saved re-read of cons: 1.73 against 1.69 ms per ragged64 step). */
 template<int Q, int NC, class R>
 __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT<R> v, int first){
    __shared__ R sG[Q][CB+1];      /* sG[q][t+1]: face (i, i+1); sG[q][0]: face (i0-1, i0) */
@@ -885,46 +911,30 @@ __device__ void ct_cons_B(const ViewT<R> &v, const DiskParams &P, int a, int c0,
                           int j, int k, double rp, double rm, double zp, double zm, double *cons,
                           int *err);
 
-/* ------------------------------------------------------------------ k_c2p
- *   calc_prim    misc.c:290-325 (euler cons2prim, FP64) on real cells
- *   boundary     Boundary/fixed.c:11-60 (r ghosts re-initialised)
+/* ------------------------------------------------------------------ c2p
+ *   calc_prim    misc.c:290-325 (cons2prim, FP64) on real cells, from cons
+ *   boundary     Boundary/fixed.c:11-60 / fixed3d (ghosts re-initialised)
  * and, on the last substep, the next step's getmindt (misc.c:39-84) and the
- * per-block sums of add_diagnostics (analysis.c:52-107). */
+ * per-block sums of add_diagnostics (analysis.c:52-107).  Every thread of the
+ * block (one annulus chunk) must call it: it ends in block reductions.
+ * piph / dphi are the moved cell's; cons is read only on real cells. */
 template<int Q, int NC, class R>
-__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v, int last, int bc, int diag){
+__device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P, int a, int c,
+                                         int c0, int np, int i, int j, int k, int d, bool real,
+                                         bool active, double piph, double dphi, double *cons,
+                                         int last, int bc, int diag, int err){
    __shared__ double s_red[CB/32][8];
    __shared__ unsigned long long s_dt[CB/32];
-   int2 b = v.cblk[blockIdx.x];
-   int a = b.x, i = b.y + threadIdx.x;
-   int np = v.ann_np[a];
-   bool active = i < np;
    const int N = v.Ncell;
-   int c0 = v.ann_off[a], c = c0 + (active ? i : 0);
-   int d = v.ann_disk[a];
-   const DiskParams &P = v.dp[d];
-   int j = v.ann_j[a], k = v.ann_k[a];
    const double *rj = v.rj + P.rj0 + 1;
    const double *zk = v.zk + P.zk0 + 1;
-   bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
-   int err = 0;
    double prim[Q];
    double dtc = 1.0e300;
    double dq[6] = {0,0,0,0,0,0};
    double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
    if( active ){
-      double piph = v.piph[c], dphi = v.dphi[c];
       double phim = piph - dphi;
       if( real ){
-         double cons[Q];
-#pragma unroll
-         for( int q=0 ; q<Q ; ++q ) cons[q] = v.cons[q*N + c];
-         if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
-            if( v.ct ){                  /* onestep.c:183-185 */
-               ct_cons_B(v, P, a, c0, np, i, j, k, rp, rm, zp, zm, cons, &err);
-               v.cons[BRR*N + c] = cons[BRR];
-               v.cons[BPP*N + c] = cons[BPP];
-            }
-         }
          double dph2 = get_dp(piph, phim, P.Pmax, &err);
          double dV2 = dV_of(rp, rm, dph2, zp, zm);
          cons2prim<Q,NC>(P, cons, prim, centroid_r(rp, rm), v.ann_om[a], dV2);
@@ -973,6 +983,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v,
       }
    }
    raise_err(v, err);
+   if( v.topo_set && blockIdx.x == 0 && threadIdx.x == 0 ) *v.topo = 1;
    if( !last ) return;
    /* block reductions (one annulus per block) */
    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1005,6 +1016,44 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v,
          }
       }
    }
+}
+
+/* ------------------------------------------------------------------ k_c2p
+ * c2p_tail on each cell after k_update, with constrained transport first
+ * rebuilding B from the face fluxes (onestep.c:183-185). */
+template<int Q, int NC, class R>
+__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v, int last, int bc, int diag){
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   bool active = i < np;
+   const int N = v.Ncell;
+   int c0 = v.ann_off[a], c = c0 + (active ? i : 0);
+   int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+   int j = v.ann_j[a], k = v.ann_k[a];
+   bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
+   int err = 0;
+   double cons[Q];
+   double piph = 0.0, dphi = 0.0;
+   if( active ){
+      piph = v.piph[c]; dphi = v.dphi[c];
+      if( real ){
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ) cons[q] = v.cons[q*N + c];
+         if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+            if( v.ct ){                  /* onestep.c:183-185 */
+               const double *rj = v.rj + P.rj0 + 1;
+               const double *zk = v.zk + P.zk0 + 1;
+               ct_cons_B(v, P, a, c0, np, i, j, k, rj[j], rj[j-1], zk[k], zk[k-1], cons, &err);
+               v.cons[BRR*N + c] = cons[BRR];
+               v.cons[BPP*N + c] = cons[BPP];
+            }
+         }
+      }
+   }
+   c2p_tail<Q,NC,R>(v, P, a, c, c0, np, i, j, k, d, real, active, piph, dphi, cons, last, bc, diag,
+                    err);
 }
 
 /* The sequential walk of set_cells_copy_distant (boundary_functions.c:
