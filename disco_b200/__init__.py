@@ -255,11 +255,22 @@ class Batch:
                                                dptr(dphi), dptr(wiph), iptr(real), dptr(Phi)),
                "disco_batch_set_cells")
 
-    def get_cells(self):
+    def get_cells(self, out=None):
+        """Download the state; `out` may supply the arrays (e.g. pinned host
+        memory) as a dict with the keys this returns."""
         n, q = self.ncell, self.q
-        prim = np.zeros((n, q)); cons = np.zeros((n, q))
-        piph = np.zeros(n); dphi = np.zeros(n); wiph = np.zeros(n)
-        Phi = np.zeros((n, 3)) if self.ct else None
+        o = out or {}
+        prim = o.get("prim"); cons = o.get("cons")
+        piph = o.get("piph"); dphi = o.get("dphi"); wiph = o.get("wiph")
+        prim = np.zeros((n, q)) if prim is None else prim
+        cons = np.zeros((n, q)) if cons is None else cons
+        piph = np.zeros(n) if piph is None else piph
+        dphi = np.zeros(n) if dphi is None else dphi
+        wiph = np.zeros(n) if wiph is None else wiph
+        for a, shape in ((prim, (n, q)), (cons, (n, q)), (piph, (n,)), (dphi, (n,)), (wiph, (n,))):
+            if a.shape != shape or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("get_cells: output arrays must be C-contiguous float64 of the state's shape")
+        Phi = (o.get("Phi") if o.get("Phi") is not None else np.zeros((n, 3))) if self.ct else None
         _check(library().disco_batch_get_cells(self.h, dptr(prim), dptr(cons), dptr(piph),
                                                dptr(dphi), dptr(wiph), dptr(Phi)),
                "disco_batch_get_cells")

@@ -391,6 +391,7 @@ extern "C" void disco_batch_destroy(disco_batch *b){
    if( b->graph ) cudaGraphExecDestroy(b->graph);
    if( b->own_stream ) cudaStreamDestroy(b->own_stream);
    for( void *p : b->allocs ) if( p ) cudaFree(p);
+   if( b->d_stage ) cudaFree(b->d_stage);
    delete b;
 }
 
@@ -410,21 +411,48 @@ static cudaError_t xfer(const disco_batch *b, void *dst, const void *src, size_t
    return cudaStreamSynchronize(b->stream);
 }
 
-/* cell-major FP64 (Q per cell) host <-> SoA device of element type T */
+/* cell-major FP64 (Q per cell) host <-> SoA device of element type T: one
+ * contiguous copy through a device staging array (DMA at full speed when the
+ * host buffer is pinned), transposed on the device, one thread per cell. */
+template<class T>
+__global__ void k_aos_to_soa(const double *src, T *dst, size_t N, int Q){
+   size_t c = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+   if( c >= N ) return;
+   for( int q=0 ; q<Q ; ++q ) dst[q*N + c] = (T)src[c*Q + q];
+}
+template<class T>
+__global__ void k_soa_to_aos(const T *src, double *dst, size_t N, int Q){
+   size_t c = blockIdx.x*(size_t)blockDim.x + threadIdx.x;
+   if( c >= N ) return;
+   for( int q=0 ; q<Q ; ++q ) dst[c*Q + q] = (double)src[q*N + c];
+}
+static int staging(disco_batch *b){
+   if( b->d_stage ) return DISCO_OK;
+   if( cudaMalloc(&b->d_stage, (size_t)b->Q*b->ncell*sizeof(double)) != cudaSuccess ){
+      b->d_stage = NULL;
+      return DISCO_ERR_CUDA;
+   }
+   return DISCO_OK;
+}
 template<class T>
 static int upload_q(disco_batch *b, T *dst, const double *src){
    size_t N = b->ncell; int Q = b->Q;
-   std::vector<T> t((size_t)Q*N);
-   for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<Q ; ++q ) t[q*N + c] = (T)src[c*Q + q];
-   CK(xfer(b, dst, t.data(), t.size()*sizeof(T), cudaMemcpyHostToDevice));
+   int s = staging(b);
+   if( s ) return s;
+   CK(cudaMemcpyAsync(b->d_stage, src, (size_t)Q*N*sizeof(double), cudaMemcpyHostToDevice, b->stream));
+   k_aos_to_soa<T><<<nblk(N, 256), 256, 0, b->stream>>>(b->d_stage, dst, N, Q);
+   CK(cudaGetLastError());
+   CK(cudaStreamSynchronize(b->stream));
    return DISCO_OK;
 }
 template<class T>
 static int download_q(disco_batch *b, double *dst, const T *src){
    size_t N = b->ncell; int Q = b->Q;
-   std::vector<T> t((size_t)Q*N);
-   CK(xfer(b, t.data(), src, t.size()*sizeof(T), cudaMemcpyDeviceToHost));
-   for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<Q ; ++q ) dst[c*Q + q] = (double)t[q*N + c];
+   int s = staging(b);
+   if( s ) return s;
+   k_soa_to_aos<T><<<nblk(N, 256), 256, 0, b->stream>>>(src, b->d_stage, N, Q);
+   CK(cudaGetLastError());
+   CK(xfer(b, dst, b->d_stage, (size_t)Q*N*sizeof(double), cudaMemcpyDeviceToHost));
    return DISCO_OK;
 }
 /* an R-typed cell array of the batch (prim, gradp, gradr) */

@@ -46,6 +46,7 @@ struct disco_batch {
    std::vector<void *> allocs;
    int *d_ann_blk0, *d_ann_nblk;
    double *d_Qrz;
+   double *d_stage;          /* Q x ncell FP64, set/get_cells staging (lazy) */
    int *d_err;
    cudaStream_t stream;
    cudaStream_t own_stream;
