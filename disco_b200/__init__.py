@@ -27,7 +27,7 @@ TEMPLATES = os.path.join(HERE, "templates")
 OK = 0
 STATUS = {0: "ok", 1: "bad argument", 2: "CUDA runtime error", 3: "module combination not built",
           4: "phi wrap loop hit its cap (non-finite piph)", 5: "non-finite or non-positive dt",
-          6: "no CUDA device", 7: "call out of order"}
+          6: "no CUDA device", 7: "call out of order", 8: "device consistency check failed"}
 HYDRO = {"euler": 0, "mhd": 1}
 BOUNDARY = {"fixed": 0, "zerograd": 1, "fixed3d": 2}
 PLANETS = {"none": 0, "sun": 1, "cm2": 2, "binary_soft": 3}
@@ -239,9 +239,15 @@ class Batch:
         """Constrained transport on (in.par Constrained_Transport)."""
         return bool(self.disks[0].params.CT)
 
+    @property
+    def num_faces(self):
+        """Face-flux slots per cell under CT (the reference's NUM_FACES)."""
+        return 5 if self.disks[0].modules.ct_mode == 2 else 3
+
     def set_cells(self, prim, cons, piph, dphi, wiph=None, real=None, Phi=None):
-        """Upload a state; Phi (ncell x 3 face fluxes) is the constrained-transport
-        state and is taken only when CT is on (zeros when omitted)."""
+        """Upload a state; Phi (ncell x num_faces face fluxes) is the
+        constrained-transport state and is taken only when CT is on (zeros when
+        omitted)."""
         prim = None if prim is None else np.ascontiguousarray(prim, np.float64)
         cons = None if cons is None else np.ascontiguousarray(cons, np.float64)
         piph = np.ascontiguousarray(piph, np.float64)
@@ -249,8 +255,8 @@ class Batch:
         wiph = None if wiph is None else np.ascontiguousarray(wiph, np.float64)
         real = None if real is None else np.ascontiguousarray(real, np.int32)
         Phi = None if Phi is None else np.ascontiguousarray(Phi, np.float64)
-        if Phi is not None and Phi.shape != (self.ncell, 3):
-            raise ValueError("Phi must be ncell x 3")
+        if Phi is not None and Phi.shape != (self.ncell, self.num_faces):
+            raise ValueError("Phi must be ncell x %d" % self.num_faces)
         _check(library().disco_batch_set_cells(self.h, dptr(prim), dptr(cons), dptr(piph),
                                                dptr(dphi), dptr(wiph), iptr(real), dptr(Phi)),
                "disco_batch_set_cells")
@@ -270,7 +276,8 @@ class Batch:
         for a, shape in ((prim, (n, q)), (cons, (n, q)), (piph, (n,)), (dphi, (n,)), (wiph, (n,))):
             if a.shape != shape or a.dtype != np.float64 or not a.flags.c_contiguous:
                 raise ValueError("get_cells: output arrays must be C-contiguous float64 of the state's shape")
-        Phi = (o.get("Phi") if o.get("Phi") is not None else np.zeros((n, 3))) if self.ct else None
+        Phi = (o.get("Phi") if o.get("Phi") is not None else np.zeros((n, self.num_faces))) \
+            if self.ct else None
         _check(library().disco_batch_get_cells(self.h, dptr(prim), dptr(cons), dptr(piph),
                                                dptr(dphi), dptr(wiph), dptr(Phi)),
                "disco_batch_get_cells")

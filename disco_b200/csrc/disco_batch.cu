@@ -58,6 +58,7 @@ extern "C" const char *disco_strerror(int s){
       case DISCO_ERR_NONFINITE: return "non-finite or non-positive dt";
       case DISCO_ERR_NO_DEVICE: return "no CUDA device";
       case DISCO_ERR_STATE: return "call out of order";
+      case DISCO_ERR_INTERNAL: return "device consistency check failed";
    }
    return "unknown status";
 }
@@ -145,11 +146,16 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    if( !((mods->hydro == DISCO_HYDRO_EULER && mods->num_c == 5) || (mhd && mods->num_c == 8)) ||
        mods->num_n != 1 || mods->ct_mode < 0 || mods->ct_mode > 2 )
       return DISCO_ERR_UNSUPPORTED;
-   int ct = params[0].CT ? 1 : 0;
-   for( int d=0 ; d<ndisk ; ++d ) if( (params[d].CT ? 1 : 0) != ct ) return DISCO_ERR_ARG;
-   if( ct ){
-      if( !mhd || mods->ct_mode != 1 || precision != DISCO_PREC_FP64 ) return DISCO_ERR_UNSUPPORTED;
-      for( int d=0 ; d<ndisk ; ++d ) if( Nz[d] != 1 ) return DISCO_ERR_UNSUPPORTED;
+   int ct = params[0].CT ? mods->ct_mode : 0;
+   for( int d=0 ; d<ndisk ; ++d ) if( (params[d].CT ? 1 : 0) != (params[0].CT ? 1 : 0) ) return DISCO_ERR_ARG;
+   if( params[0].CT ){
+      /* CT_MODE 1 stores no z-face fluxes, so it is built for 2D disks; in 3D
+       * (CT_MODE 2) avg_Efields' z-pole branch (NgZa or NgZb = 0) is not */
+      if( !mhd || mods->ct_mode < 1 || precision != DISCO_PREC_FP64 ) return DISCO_ERR_UNSUPPORTED;
+      for( int d=0 ; d<ndisk ; ++d ){
+         if( Nz[d] > 1 && (mods->ct_mode != 2 || Ng[4*d+2] == 0 || Ng[4*d+3] == 0) )
+            return DISCO_ERR_UNSUPPORTED;
+      }
    }
    if( mods->boundary != DISCO_BC_FIXED && mods->boundary != DISCO_BC_ZEROGRAD &&
        mods->boundary != DISCO_BC_FIXED3D )
@@ -182,6 +188,8 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->own_stream = NULL;
    b->tape = NULL; b->tape_names = NULL;
    b->ct = ct;
+   b->nfs = ct == 2 ? 5 : 3;
+   b->line_ne = 0;
 
    /* ---- topology */
    int cell = 0, ann = 0, face = 0, roff = 0, zoff = 0, npoff = 0;
@@ -223,12 +231,15 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       const double *rj = r_jph + roff + 1;
       int jmin = D.NgRa == 0 ? 0 : D.NgRa-1;            /* trans_flux, misc.c:459-471 */
       int jmax = D.NgRb == 0 ? nr-1 : nr-D.NgRb;
+      /* with CT one more layer of fluxes outside the real cells (:449-471) */
+      int kminr = ct ? (D.NgZa == 0 ? 0 : D.NgZa-1) : D.NgZa;
+      int kmaxr = ct ? (D.NgZb == 0 ? nz : nz-D.NgZb+1) : nz-D.NgZb;
       for( int k=0 ; k<nz ; ++k ) for( int j=0 ; j<nr-1 ; ++j ){
          int t = (int)b->tr_a.size();
          int A = D.ann0 + j + nr*k, B = A + 1;
          b->tr_a.push_back(A); b->tr_b.push_back(B); b->tr_off.push_back(face);
          b->tr_j.push_back(j); b->tr_k.push_back(k);
-         b->tr_flux.push_back(j >= jmin && j < jmax && k >= D.NgZa && k < nz-D.NgZb);
+         b->tr_flux.push_back(j >= jmin && j < jmax && k >= kminr && k < kmaxr);
          /* dxL/dxR, faces_alt.c:112-118 */
          double rm = 2.0*(rj[j]*rj[j] + rj[j]*rj[j-1] + rj[j-1]*rj[j-1]) / (3.0*(rj[j]+rj[j-1]));
          double rp = 2.0*(rj[j+1]*rj[j+1] + rj[j+1]*rj[j] + rj[j]*rj[j]) / (3.0*(rj[j+1]+rj[j]));
@@ -247,12 +258,14 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       const double *zkp = z_kph + zoff + 1;
       int kminz = D.NgZa == 0 ? 0 : D.NgZa-1;           /* trans_flux dim 2, misc.c:474-489 */
       int kmaxz = D.NgZb == 0 ? nz-1 : nz-D.NgZb;
+      int jminz = ct ? (D.NgRa == 0 ? 0 : D.NgRa-1) : D.NgRa;
+      int jmaxz = ct ? (D.NgRb == 0 ? nr : nr-D.NgRb+1) : nr-D.NgRb;
       for( int k=0 ; k<nz-1 ; ++k ) for( int j=0 ; j<nr ; ++j ){
          int t = (int)b->tr_a.size();
          int A = D.ann0 + j + nr*k, B = A + nr;
          b->tr_a.push_back(A); b->tr_b.push_back(B); b->tr_off.push_back(face);
          b->tr_j.push_back(j); b->tr_k.push_back(k);
-         b->tr_flux.push_back(j >= D.NgRa && j < nr-D.NgRb && k >= kminz && k < kmaxz);
+         b->tr_flux.push_back(j >= jminz && j < jmaxz && k >= kminz && k < kmaxz);
          /* dxL/dxR, faces_alt.c:119-125 */
          double zm = 0.5*(zkp[k]+zkp[k-1]);
          double zp = 0.5*(zkp[k+1]+zkp[k]);
@@ -263,12 +276,23 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
          for( int f0=0 ; f0<nf ; f0+=FB ) b->fblk.push_back(make_int2(t, f0));
          face += nf;
       }
+      /* (r, z) edge lines of make_edge_adjust (bfields.c:922-1125), line
+       * j + (Nr-1)*k between annuli (j,k), (j+1,k), (j,k+1), (j+1,k+1) */
+      D.ln0 = (int)b->line_off.size();
+      if( ct == 2 && nz > 1 ){
+         for( int k=0 ; k<nz-1 ; ++k ) for( int j=0 ; j<nr-1 ; ++j ){
+            int A = D.ann0 + j + nr*k;
+            b->line_off.push_back(b->line_ne);
+            b->line_ne += b->ann_np[A] + b->ann_np[A+1] + b->ann_np[A+nr] + b->ann_np[A+nr+1];
+         }
+      }
       b->disk_Nr.push_back(nr); b->disk_Nz.push_back(nz); b->disk_nreal.push_back(nreal);
       b->nreal += nreal;
       roff += nr+1; zoff += nz+1; npoff += nr*nz;
    }
    b->ann_off.push_back(cell);
    b->tr_off.push_back(face);
+   b->line_off.push_back(b->line_ne);
    b->ncell = cell;
 
    /* zerograd layers (boundary_functions.c:269-440): r ghosts from the real
@@ -357,13 +381,24 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->d_err = v.err;
    v.topo = dalloc<int>(b, 1);
    if( ct ){
-      v.ct = 1;
-      v.Phi = dalloc<double>(b, 3*N); v.RKPhi = dalloc<double>(b, 3*N);
-      v.ctE = dalloc<double>(b, 4*N); v.ctB = dalloc<double>(b, 4*N);
+      v.ct = ct;
+      v.nfs = b->nfs;
+      size_t ne = ct == 2 ? 8 : 4;
+      v.Phi = dalloc<double>(b, b->nfs*N); v.RKPhi = dalloc<double>(b, b->nfs*N);
+      v.ctE = dalloc<double>(b, ne*N); v.ctB = dalloc<double>(b, ne*N);
       v.pE = dalloc<double>(b, N); v.pB = dalloc<double>(b, N);
       v.fEt = dalloc<double>(b, face); v.fBt = dalloc<double>(b, face);
       v.fX = dalloc<double>(b, face);
       v.fFlip = dalloc<unsigned char>(b, face);
+      if( ct == 2 ){
+         v.pEr = dalloc<double>(b, N); v.pBz = dalloc<double>(b, N);
+         v.fEphi = dalloc<double>(b, face);
+         if( b->any_3d ){
+            v.rk = dalloc<int>(b, 4*N);
+            v.lineX = dalloc<double>(b, (size_t)b->line_ne);
+            v.line_off = dupload(b, b->line_off);
+         }
+      }
    }
    if( b->bc_zerograd && !b->zg_pairs.empty() ) b->d_zg_pairs = dupload(b, b->zg_pairs);
    make_float_view(b);
@@ -475,9 +510,10 @@ extern "C" int disco_batch_set_cells(disco_batch *b, const double *prim, const d
    int s;
    if( prim && (s = upload_r(b, b->vd.prim, prim)) ) return s;
    if( cons && (s = upload_q<double>(b, b->vd.cons, cons)) ) return s;
-   if( b->ct ){                     /* Phi[0..2] per cell, cell-major */
-      std::vector<double> t(3*N, 0.0);
-      if( Phi ) for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<3 ; ++q ) t[q*N + c] = Phi[3*c + q];
+   if( b->ct ){                     /* Phi[0 .. num_faces-1] per cell, cell-major */
+      const int F = b->nfs;
+      std::vector<double> t(F*N, 0.0);
+      if( Phi ) for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<F ; ++q ) t[q*N + c] = Phi[F*c + q];
       CK(xfer(b, b->vd.Phi, t.data(), t.size()*sizeof(double), cudaMemcpyHostToDevice));
    }
    CK(xfer(b, b->vd.piph, piph, N*sizeof(double), cudaMemcpyHostToDevice));
@@ -504,9 +540,10 @@ extern "C" int disco_batch_get_cells(disco_batch *b, double *prim, double *cons,
    size_t N = b->ncell;
    int s;
    if( Phi && b->ct ){
-      std::vector<double> t(3*N);
+      const int F = b->nfs;
+      std::vector<double> t(F*N);
       CK(xfer(b, t.data(), b->vd.Phi, t.size()*sizeof(double), cudaMemcpyDeviceToHost));
-      for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<3 ; ++q ) Phi[3*c + q] = t[q*N + c];
+      for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<F ; ++q ) Phi[F*c + q] = t[q*N + c];
    }
    if( prim && (s = download_r(b, prim, b->vd.prim)) ) return s;
    if( cons && (s = download_q<double>(b, cons, b->vd.cons)) ) return s;
@@ -545,6 +582,7 @@ static int read_err(disco_batch *b){
    }
    if( e & ERRF_WRAP ) return DISCO_ERR_PHI_WRAP;
    if( e & ERRF_NONFINITE ) return DISCO_ERR_NONFINITE;
+   if( e & ERRF_INTERNAL ) return DISCO_ERR_INTERNAL;
    return DISCO_OK;
 }
 

@@ -54,7 +54,10 @@ struct disco_batch {
    std::vector<const char *> *tape_names;
    cudaGraphExec_t graph;
    int have_cells;
-   int ct;                   /* 2D constrained transport (FP64 view only) */
+   int ct;                   /* constrained transport: the CT_MODE (1, 2) or 0 (FP64 view only) */
+   int nfs;                  /* face-flux slots per cell (NUM_FACES: 3 or 5) */
+   std::vector<int> line_off;           /* edge lines of 3D CT, offsets into lineX */
+   int line_ne;
 };
 
 static inline unsigned nblk(size_t n, unsigned t){ return (unsigned)((n + t - 1)/t); }
@@ -135,6 +138,9 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
       if( b->ct ){                  /* onestep.c:140-146 and 160-167 */
          k_ct_edges<R><<<ncb, CB, 0, s>>>(v);                           mark(b, "k_ct_edges");
          k_ct_faces<R><<<nfb, FB, 0, s>>>(v);                           mark(b, "k_ct_faces");
+         if( b->ct == 2 && b->any_3d ){
+            k_ct_line<R><<<ncb, CB, 0, s>>>(v);                         mark(b, "k_ct_line");
+         }
          k_ct_update<R><<<ncb, CB, 0, s>>>(v, first);                   mark(b, "k_ct_update");
          if( first ){
             k_ct_flag<R><<<nfb, FB, 0, s>>>(v);                         mark(b, "k_ct_flag");

@@ -27,7 +27,7 @@ namespace disco {
 
 enum { RHO = 0, PPP = 1, URR = 2, UPP = 3, UZZ = 4, BRR = 5, BPP = 6, BZZ = 7 };
 enum { DDD = 0, TAU = 1, SRR = 2, LLL = 3, SZZ = 4 };
-enum { ERRF_WRAP = 1, ERRF_NONFINITE = 2 };
+enum { ERRF_WRAP = 1, ERRF_NONFINITE = 2, ERRF_INTERNAL = 4 };
 
 struct Planet {
    double r, phi, M, omega, vr;
@@ -51,6 +51,8 @@ struct DiskParams {
    int trr0, ntrr;    /* first global r-track, count */
    int face_r0;       /* first global r-face */
    int trz0, ntrz;    /* first global z-track, count (Nr*(Nz-1)) */
+   int ln0;           /* first global (r, z) edge line, (Nr-1)*(Nz-1) of them (3D CT) */
+   int pad_ln;
    int npl;
    int ic_module;     /* DISCO_IC_KEPLER_NOISE or DISCO_IC_MHD_SHEAR_NOISE */
    int pad_ic;
@@ -619,7 +621,7 @@ __device__ __forceinline__ void hlld_solve(const DiskParams &P, R w, const R *pr
  * 2; HLLD needs MHD).  Returns G_q = (Flux_q - w*Ustr_q)*dAdt, the amount
  * subtracted from cons_L and added to cons_R (riemann.c:312-315), and, when
  * eb is given (MHD), the inputs of flux_to_E (Hydro/mhd.c:293-316):
- * eb = (Flux[BRR], Flux[BPP], Ustr[BRR]). */
+ * eb = (Flux[BRR], Flux[BPP], Ustr[BRR], Flux[BZZ], Ustr[BZZ]). */
 template<int Q, int NC, int DIM, class R>
 __device__ __forceinline__ void solve_riemann(const DiskParams &P, const R *primL,
                                               const R *primR, R r, R om,
@@ -632,7 +634,8 @@ __device__ __forceinline__ void solve_riemann(const DiskParams &P, const R *prim
          hlld_solve<Q,DIM,R>(P, w, primL, primR, Flux, Ustr, r);
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) G[q] = (Flux[q] - w*Ustr[q])*dAdt;
-         if( eb ){ eb[0] = Flux[BRR]; eb[1] = Flux[BPP]; eb[2] = Ustr[BRR]; }
+         if( eb ){ eb[0] = Flux[BRR]; eb[1] = Flux[BPP]; eb[2] = Ustr[BRR];
+                   eb[3] = Flux[BZZ]; eb[4] = Ustr[BZZ]; }
          return;
       }
    }
@@ -669,7 +672,8 @@ __device__ __forceinline__ void solve_riemann(const DiskParams &P, const R *prim
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) G[q] = (Flux[q] - w*Ustr[q])*dAdt;
    if constexpr ( NC == 8 ){
-      if( eb ){ eb[0] = Flux[BRR]; eb[1] = Flux[BPP]; eb[2] = Ustr[BRR]; }
+      if( eb ){ eb[0] = Flux[BRR]; eb[1] = Flux[BPP]; eb[2] = Ustr[BRR];
+                eb[3] = Flux[BZZ]; eb[4] = Ustr[BZZ]; }
    }
 }
 

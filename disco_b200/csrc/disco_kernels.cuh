@@ -108,17 +108,24 @@ struct ViewT {
    int nq;
    double dtfac;        /* 1 in the first substep, 0.5 in the second (timestep.c:39) */
    int *err;
-   /* 2D constrained transport (Constrained_Transport 1, CT_MODE 1; bfields.c).
-    * Per cell, SoA [s*Ncell + c]: Phi / RKPhi, s = 0 the magnetic flux through
-    * the cell's phi face at piph, s = 1 / 2 the flux through the r-face the cell
-    * owns in the track inside / outside it (the face ending at its piph,
-    * LRtype 1 / 0); ctE / ctB the four edge values E[0..3], B[0..3]
-    * (riemann.c:73-85, 175-187) before averaging; pE / pB the phi face's
-    * (Ez, Br) from flux_to_E.  Per r-face: fEt / fBt (Erz, Brz), fX the
-    * E dl dt of update_B_fluxes, fFlip the flag of check_flipped. */
-   int ct;
-   double *Phi, *RKPhi, *ctE, *ctB, *pE, *pB, *fEt, *fBt, *fX;
+   /* Constrained transport (Constrained_Transport 1; bfields.c), ct = the
+    * CT_MODE (1: 2D, NUM_FACES 3; 2: 3D, NUM_FACES 5) or 0.  Per cell, SoA
+    * [s*Ncell + c]: Phi / RKPhi, s = 0 the magnetic flux through the cell's
+    * phi face at piph, s = 1 / 2 the flux through the r-face the cell owns in
+    * the track inside / outside it (the face ending at its piph, LRtype 1 /
+    * 0), s = 3 / 4 the same for the z-faces below / above it; ctE / ctB the
+    * edge values E[0..7], B[0..7] (riemann.c:73-110, 175-213) before
+    * averaging; pE, pB, pEr, pBz the phi face's (Ez, Br, Er, Bz) from
+    * flux_to_E.  Per face (r and z): fEt / fBt (Erz, Brz), fEphi (E_phi),
+    * fX the E dl dt of update_B_fluxes, fFlip the flag of check_flipped.
+    * 3D: rk[m*Ncell + c] the position of cell c in the 4-way merge of the
+    * edge line where it is list m (make_edge_adjust's c, cR, cU, cUR), and
+    * lineX[line_off[l] + e] the E_phi dl dt of merged edge e of line l. */
+   int ct, nfs;
+   double *Phi, *RKPhi, *ctE, *ctB, *pE, *pB, *pEr, *pBz, *fEt, *fBt, *fEphi, *fX;
    unsigned char *fFlip;
+   int *rk, *line_off;
+   double *lineX;
 };
 
 template<class R>
@@ -197,7 +204,8 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_BEGIN) k_begin(ViewT<R
    if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
       if( v.ct ){                   /* timestep.c:22 and adjust_RK_cons, misc.c:239-241 */
 #pragma unroll
-         for( int s=0 ; s<3 ; ++s ){
+         for( int s=0 ; s<5 ; ++s ){
+            if( s >= v.nfs ) break;
             double ph = v.Phi[s*N + c];
             double rk;
             if( first ){ rk = ph; v.RKPhi[s*N + c] = ph; }
@@ -583,13 +591,20 @@ __global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R
    const double *rj = v.rj + P.rj0 + 1;
    double r = DIM == 1 ? .5*(rj[j]+rj[j]) : centroid_r(rj[j], rj[j-1]);    /* face cm[0] */
    R G[Q];
-   if constexpr ( NC == 8 && DIM == 1 && sizeof(R) == sizeof(double) ){
-      if( v.ct ){                    /* flux_to_E dim 1, Hydro/mhd.c:304-308 */
-         R eb[3];
+   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+      if( v.ct ){                    /* flux_to_E dim 1 / 2, Hydro/mhd.c:304-314 */
+         R eb[5];
          solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G, eb);
          double irfac = 1.0/(1.0/r);
-         v.fEt[f] = -eb[1]*r;
-         v.fBt[f] = eb[2]*irfac;
+         if( DIM == 1 ){
+            v.fEt[f] = -eb[1]*r;
+            v.fBt[f] = eb[2]*irfac;
+            if( v.ct == 2 ) v.fEphi[f] = eb[3];
+         }else{
+            v.fEt[f] = eb[1]*r;
+            v.fBt[f] = eb[4];
+            v.fEphi[f] = -eb[0]*irfac;
+         }
       }else{
          solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G);
       }
@@ -669,11 +684,12 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
          R G[Q];
          int cn = c0 + (i < np-1 ? i+1 : 0);
          if( ctE ){                 /* flux_to_E dim 0, Hydro/mhd.c:298-303 */
-            R eb[3];
+            R eb[5];
             phi_face_flux<Q,NC,R>(v, P, a, c, cn, rc, dAdtp, G, eb);
             double irfac = 1.0/(1.0/rc);
             v.pE[c] = eb[0]*irfac;
             v.pB[c] = eb[2]*irfac;
+            if( v.ct == 2 ){ v.pEr[c] = -eb[3]; v.pBz[c] = eb[4]; }
          }else{
             phi_face_flux<Q,NC,R>(v, P, a, c, cn, rc, dAdtp, G);
          }
@@ -1048,6 +1064,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v,
                ct_cons_B(v, P, a, c0, np, i, j, k, rj[j], rj[j-1], zk[k], zk[k-1], cons, &err);
                v.cons[BRR*N + c] = cons[BRR];
                v.cons[BPP*N + c] = cons[BPP];
+               if( v.ct == 2 && P.Nz > 1 ) v.cons[BZZ*N + c] = cons[BZZ];
             }
          }
       }
@@ -1325,8 +1342,7 @@ __global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc){
          initial<Q,NC>(P, pb, x);
          double dA = (rj[j]-rj[j-1])*(zk[k]-zk[k-1]);
          v.Phi[c] = pb[BPP]*dA;
-         v.Phi[N + c] = 0.0;
-         v.Phi[2*N + c] = 0.0;
+         for( int s=1 ; s<v.nfs ; ++s ) v.Phi[(size_t)s*N + c] = 0.0;
       }
    }
    raise_err(v, err);

@@ -91,14 +91,14 @@ static void gpu_init(struct domain *d){
    double *piph = malloc(sizeof(double)*ncell), *dphi = malloc(sizeof(double)*ncell);
    double *wiph = malloc(sizeof(double)*ncell);
    int *real = malloc(sizeof(int)*ncell);
-   /* the constrained-transport face fluxes, cell->Phi[3] (CT_MODE 1) */
-   double *phis = NUM_FACES == 3 ? malloc(sizeof(double)*3*ncell) : NULL;
+   /* the constrained-transport face fluxes, cell->Phi[NUM_FACES] */
+   double *phis = NUM_FACES > 0 && d->theParList.CT ? malloc(sizeof(double)*(NUM_FACES > 0 ? NUM_FACES : 1)*ncell) : NULL;
    int64_t n = 0;
    for( jk=0 ; jk<Nr*Nz ; ++jk ) for( i=0 ; i<d->Np[jk] ; ++i, ++n ){
       struct cell *c = &d->theCells[jk][i];
       for( q=0 ; q<NUM_Q ; ++q ){ prim[NUM_Q*n+q] = c->prim[q]; cons[NUM_Q*n+q] = c->cons[q]; }
       piph[n] = c->piph; dphi[n] = c->dphi; wiph[n] = c->wiph; real[n] = c->real;
-      if( phis ) for( q=0 ; q<NUM_FACES ; ++q ) phis[3*n+q] = c->Phi[q];
+      if( phis ) for( q=0 ; q<NUM_FACES ; ++q ) phis[NUM_FACES*n+q] = c->Phi[q];
    }
    s = disco_batch_set_cells(g_batch, prim, cons, piph, dphi, wiph, real, phis);
    free(prim); free(cons); free(piph); free(dphi); free(wiph); free(real); free(phis);
@@ -131,7 +131,7 @@ void disco_gpu_sync_to_host( struct domain * theDomain ){
    double *prim = malloc(sizeof(double)*NUM_Q*ncell), *cons = malloc(sizeof(double)*NUM_Q*ncell);
    double *piph = malloc(sizeof(double)*ncell), *dphi = malloc(sizeof(double)*ncell);
    double *wiph = malloc(sizeof(double)*ncell);
-   double *phis = NUM_FACES == 3 && theDomain->theParList.CT ? malloc(sizeof(double)*3*ncell) : NULL;
+   double *phis = NUM_FACES > 0 && theDomain->theParList.CT ? malloc(sizeof(double)*(NUM_FACES > 0 ? NUM_FACES : 1)*ncell) : NULL;
    int s = disco_batch_get_cells(g_batch, prim, cons, piph, dphi, wiph, phis);
    if( s ) fail("disco_batch_get_cells", s);
    s = disco_batch_last_error(g_batch);
@@ -142,7 +142,7 @@ void disco_gpu_sync_to_host( struct domain * theDomain ){
       struct cell *c = &theDomain->theCells[jk][i];
       for( q=0 ; q<NUM_Q ; ++q ){ c->prim[q] = prim[NUM_Q*n+q]; c->cons[q] = cons[NUM_Q*n+q]; }
       c->piph = piph[n]; c->dphi = dphi[n]; c->wiph = wiph[n];
-      if( phis ) for( q=0 ; q<NUM_FACES ; ++q ) c->Phi[q] = phis[3*n+q];
+      if( phis ) for( q=0 ; q<NUM_FACES ; ++q ) c->Phi[q] = phis[NUM_FACES*n+q];
    }
    free(prim); free(cons); free(piph); free(dphi); free(wiph); free(phis);
    /* time-averaged diagnostics accumulated on the device (analysis.c:52-107) */

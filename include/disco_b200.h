@@ -46,7 +46,8 @@ enum disco_status {
    DISCO_ERR_PHI_WRAP = 4,     /* phi wrap loop hit its iteration cap (non-finite piph) */
    DISCO_ERR_NONFINITE = 5,    /* non-finite dt or state detected */
    DISCO_ERR_NO_DEVICE = 6,    /* no CUDA device / library built without one */
-   DISCO_ERR_STATE = 7         /* call out of order (e.g. step before set_cells) */
+   DISCO_ERR_STATE = 7,        /* call out of order (e.g. step before set_cells) */
+   DISCO_ERR_INTERNAL = 8      /* a device-side consistency check failed */
 };
 
 /* Module choices, one per Makefile_opt.in line (Makefile:11-26).  The names
@@ -137,11 +138,13 @@ int disco_batch_sizes(const disco_batch *b, int64_t *ncell, int64_t *nreal, int 
  * real[] is the reference's cell->real flag.  cons may be NULL (then cons is
  * rebuilt from prim with prim2cons on the device, as setupCells does,
  * domain.c:205).  Phi is the constrained-transport state (in.par
- * Constrained_Transport 1, built for CT_MODE 1 in 2D): 3 doubles per cell,
- * the reference's cell->Phi[NUM_FACES] (paul.h:198) -- Phi[0] the magnetic
- * flux through the phi face at piph, Phi[1] / Phi[2] that through the r face
- * the cell owns in the track inside / outside it (bfields.c:734-758).  It
- * is ignored when CT is off and may be NULL (zeros) when CT is on.
+ * Constrained_Transport 1; CT_MODE 1 for 2D disks, CT_MODE 2 in 2D or 3D):
+ * NUM_FACES doubles per cell (3 or 5), the reference's cell->Phi[NUM_FACES]
+ * (paul.h:198) -- Phi[0] the magnetic flux through the phi face at piph,
+ * Phi[1] / Phi[2] that through the r face the cell owns in the track inside
+ * / outside it, Phi[3] / Phi[4] the z face it owns below / above it
+ * (bfields.c:734-758).  It is ignored when CT is off and may be NULL (zeros)
+ * when CT is on.
  */
 int disco_batch_set_cells(disco_batch *b, const double *prim, const double *cons,
                           const double *piph, const double *dphi, const double *wiph,

@@ -61,6 +61,13 @@ CASES = {
     "c1_ct_hll_fe": ("c1_mhd2d", {"Num_R": 10, "Riemann_Solver": 0, "Timestep": 1,
                                   "Mesh_Motion": 1, "Constrained_Transport": 1,
                                   "Init_Par5": 10.0, "Init_Par6": 0.1}, 6),
+    # 3D constrained transport (CT_MODE 2: z faces, E_phi edges, make_edge_adjust),
+    # zero-gradient boundaries: Keplerian HLLD and libm-free rigid HLLD
+    "c1_ct3d": ("c1_mhd3d", {"Num_R": 8, "Num_Z": 6, "Constrained_Transport": 1,
+                             "Init_Par5": 20.0, "Init_Par6": 0.05}, 5),
+    "c1_ct3d_rigid": ("c1_mhd3d_nograv", {"Num_R": 8, "Num_Z": 6, "Init_Par2": 1,
+                                          "Init_Par4": 10.0, "Constrained_Transport": 1,
+                                          "Init_Par5": 20.0, "Init_Par6": 0.05}, 6),
 }
 
 # the in.par template each module configuration starts from
@@ -97,7 +104,7 @@ def main():
             extra.update(s0_Phi=d0["Phi"], sN_Phi=dn["Phi"])
         if "faces_2" in dn:
             Z = dn["faces_2"]
-            extra = dict(z_fIndex=Z["fIndex"], z_iL=Z["iL"], z_iR=Z["iR"], z_LRtype=Z["LRtype"],
+            extra.update(z_fIndex=Z["fIndex"], z_iL=Z["iL"], z_iR=Z["iR"], z_LRtype=Z["LRtype"],
                          z_fgeom=Z["geom"])
         np.savez_compressed(
             os.path.join(HERE, case + ".npz"), cfg=cfg, nsteps=n,

@@ -1,22 +1,25 @@
-"""GPU parity of 2D constrained transport (Constrained_Transport 1, CT_MODE 1)
-against the reference's own build (bfields.c, riemann.c edge bookkeeping,
-onestep.c:140-185), from the fixtures of tests/golden/make_golden.py.
+"""GPU parity of constrained transport (Constrained_Transport 1) against the
+reference's own build (bfields.c, riemann.c edge bookkeeping, onestep.c:
+140-185), from the fixtures of tests/golden/make_golden.py: CT_MODE 1 in 2D
+and CT_MODE 2 in 3D (z faces, E_phi edges, make_edge_adjust).
 
-The CT state is the per-cell face-flux array Phi[3] (Phi[0] the phi face at
-piph, Phi[1] / Phi[2] the r face the cell owns in the track inside / outside
-it).  The comparison covers every slot a real cell reads: Phi[0] of real
-cells and the owned-face slots of every track next to a real annulus; the
-remaining slots (ghost cells' own faces towards further ghosts) follow edge
-fields the reference leaves stale and reach nothing.
+The CT state is the per-cell face-flux array Phi[NUM_FACES] (Phi[0] the phi
+face at piph, Phi[1] / Phi[2] the r face the cell owns in the track inside /
+outside it, Phi[3] / Phi[4] the z face below / above it).  The comparison
+covers every slot a real cell reads: Phi[0] of real cells and the owned-face
+slots of every track next to a real annulus; the remaining slots (ghost
+cells' own faces towards further ghosts) follow edge fields the reference
+leaves stale and reach nothing.
 
-- c1_ct_rigid (no gravity, so no libm call whose value matters): bit-exact,
-  state, slots, dt sequence and face lists.
-- c1_ct2d (Keplerian, point-mass gravity) and c1_ct_hll_fe (HLL, forward
-  Euler, by-cell mesh): relative L1 1e-11 (the libm differences of the
-  point-mass force, as for the other MHD fixtures), face lists bit-exact.
+- c1_ct_rigid, c1_ct3d_rigid (no gravity, so no libm call whose value
+  matters): bit-exact, state, slots, dt sequence and face lists.
+- c1_ct2d, c1_ct3d (Keplerian, point-mass gravity) and c1_ct_hll_fe (HLL,
+  forward Euler, by-cell mesh): relative L1 1e-11 (the libm differences of
+  the point-mass force, as for the other MHD fixtures), face lists bit-exact.
 - At full size, the property CT exists for: each real cell's discrete
   divergence (net flux through its faces) stays at its initial value to
-  round-off (the reference's own runs keep it to 1e-17 of 1e-4).
+  round-off (the reference's own runs keep it to 1e-17 of 1e-4), in 2D and
+  in 3D.
 """
 import os
 
@@ -28,18 +31,24 @@ from helpers import case_disk, par_with, rel_l1, rel_l1_cols
 
 pytestmark = pytest.mark.gpu
 
-CT_CASES = ["c1_ct2d", "c1_ct_rigid", "c1_ct_hll_fe"]
-CT_TOL = {"c1_ct2d": 1e-11, "c1_ct_hll_fe": 1e-11}
+CT_CASES = ["c1_ct2d", "c1_ct_rigid", "c1_ct_hll_fe", "c1_ct3d", "c1_ct3d_rigid"]
+CT_TOL = {"c1_ct2d": 1e-11, "c1_ct_hll_fe": 1e-11, "c1_ct3d": 1e-11}
 
 
-def _observed_slots(disk):
-    """Mask (ncell x 3) of the Phi slots real cells read."""
-    Nr, Ng = disk.Nr, disk.Ng
-    j = np.repeat(np.arange(disk.Nr * disk.Nz) % Nr, disk.Np)
-    m = np.zeros((disk.ncell, 3), bool)
+def _observed_slots(disk, nfs):
+    """Mask (ncell x nfs) of the Phi slots real cells read."""
+    Nr, Nz, Ng = disk.Nr, disk.Nz, disk.Ng
+    jk = np.repeat(np.arange(Nr * Nz), disk.Np)
+    j, k = jk % Nr, jk // Nr
+    rj = (j >= Ng[0]) & (j < Nr - Ng[1])
+    rk = (k >= Ng[2]) & (k < Nz - Ng[3])
+    m = np.zeros((disk.ncell, nfs), bool)
     m[:, 0] = disk.real == 1
-    m[:, 1] = (j >= Ng[0]) & (j <= Nr - Ng[1])
-    m[:, 2] = (j >= Ng[0] - 1) & (j <= Nr - Ng[1] - 1)
+    m[:, 1] = (j >= Ng[0]) & (j <= Nr - Ng[1]) & rk
+    m[:, 2] = (j >= Ng[0] - 1) & (j <= Nr - Ng[1] - 1) & rk
+    if nfs == 5 and Nz > 1:
+        m[:, 3] = rj & (k >= Ng[2]) & (k <= Nz - Ng[3])
+        m[:, 4] = rj & (k >= Ng[2] - 1) & (k <= Nz - Ng[3] - 1)
     return m
 
 
@@ -52,15 +61,18 @@ def _from_golden(disk, g):
 
 def divergence(b, disk):
     """Net magnetic flux out of each cell through its current faces: outer
-    r faces - inner r faces + Phi[0](c) - Phi[0](c-1)."""
+    r faces - inner r faces (+ upper z faces - lower z faces) + Phi[0](c) -
+    Phi[0](c-1)."""
     st = b.get_cells()
     Phi = st["Phi"]
-    F = b.faces(0, 1)
-    L, R, lr = F["iL"], F["iR"], F["LRtype"]
-    v = np.where(lr == 0, Phi[L, 2], Phi[R, 1])
     div = np.zeros(disk.ncell)
-    np.add.at(div, L, v)
-    np.add.at(div, R, -v)
+    dims = [(1, 2, 1)] + ([(2, 4, 3)] if disk.Nz > 1 and Phi.shape[1] == 5 else [])
+    for dim, s0, s1 in dims:
+        F = b.faces(0, dim)
+        L, R, lr = F["iL"], F["iR"], F["LRtype"]
+        v = np.where(lr == 0, Phi[L, s0], Phi[R, s1])
+        np.add.at(div, L, v)
+        np.add.at(div, R, -v)
     off = np.concatenate([[0], np.cumsum(disk.Np)])
     for a in range(len(disk.Np)):
         c = np.arange(off[a], off[a + 1])
@@ -78,7 +90,7 @@ def test_ct_setup_matches_reference(case):
     r = disk.real == 1
     assert np.array_equal(st["prim"][r], g["s0_prim"][r])
     assert np.array_equal(st["cons"][r], g["s0_cons"][r])
-    m = _observed_slots(disk)
+    m = _observed_slots(disk, b.num_faces)
     assert np.array_equal(st["Phi"][m], g["s0_Phi"][m])
     assert b.mindt()[0] == g["s0_dt_next"]
 
@@ -95,10 +107,14 @@ def test_ct_steps_match_reference(case):
     b.sync()
     st = b.get_cells()
     r = disk.real == 1
-    m = _observed_slots(disk)
+    m = _observed_slots(disk, b.num_faces)
     F = b.faces(0, 1)
     for k in ("fIndex", "iL", "iR", "LRtype"):
         assert np.array_equal(F[k], g[k]), k
+    if disk.Nz > 1:
+        Fz = b.faces(0, 2)
+        for k in ("fIndex", "iL", "iR", "LRtype"):
+            assert np.array_equal(Fz[k], g["z_" + k]), ("z", k)
     if case not in CT_TOL:
         assert np.array_equal(np.array(dts), g["dt"])
         assert np.array_equal(st["prim"][r], g["sN_prim"][r])
@@ -111,9 +127,10 @@ def test_ct_steps_match_reference(case):
         assert e < tol, ("prim", q, e)
     for q, e in enumerate(rel_l1_cols(st["cons"][r], g["sN_cons"][r])):
         assert e < tol, ("cons", q, e)
-    for s in range(3):
-        e = rel_l1(st["Phi"][m[:, s], s], g["sN_Phi"][m[:, s], s])
-        assert e < tol, ("Phi", s, e)
+    for s in range(m.shape[1]):
+        if m[:, s].any():
+            e = rel_l1(st["Phi"][m[:, s], s], g["sN_Phi"][m[:, s], s])
+            assert e < tol, ("Phi", s, e)
 
 
 def _ct_disk(nr, ct):
@@ -145,6 +162,26 @@ def test_ct_preserves_divergence():
     print("div drift %.3e of max |Phi| %.3e (initial max |div| %.3e)" % (drift, scale, np.abs(d0[r]).max()))
     assert drift <= 1e-12 * scale
     assert np.abs(P1[r, 1:]).max() > 1.5 * np.abs(P0[r, 1:]).max()   # the field did evolve
+
+
+def test_ct3d_preserves_divergence():
+    """3D: 24 annuli x 16 layers of the Keplerian disk, 20 steps; r, z and
+    phi faces and the E_phi edges all take part."""
+    _, opt = db.template_paths("c1_mhd3d")
+    p = par_with({"Num_R": 24, "Num_Z": 16, "Constrained_Transport": 1, "Init_Par5": 20.0,
+                  "Init_Par6": 0.05, "Init_Par1": 0.05}, base="c1_mhd3d")
+    disk = db.Disk.from_files(p, opt)
+    os.unlink(p)
+    b = db.Batch([disk])
+    d0, P0 = divergence(b, disk)
+    b.run(20)
+    b.sync()
+    d1, P1 = divergence(b, disk)
+    r = disk.real == 1
+    scale = np.abs(P1).max()
+    drift = np.abs(d1 - d0)[r].max()
+    print("3D div drift %.3e of max |Phi| %.3e (initial max |div| %.3e)" % (drift, scale, np.abs(d0[r]).max()))
+    assert drift <= 1e-12 * scale
 
 
 def test_ct_refuses_unsupported():
