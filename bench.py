@@ -244,10 +244,11 @@ def div_b(disk, batch, st):
 
 
 def config1_leg(args, local, stream):
-    """3D Newtonian MHD shearing disk (HLLD, zerograd, no constrained
-    transport: B evolves through the fluxes): FP64 and the mixed form for
-    200 steps from the same state; throughput of both, the mixed form's
-    error and drifts against FP64."""
+    """3D Newtonian MHD shearing disk (HLLD, zerograd): FP64 and the mixed
+    form for 200 steps from the same state without constrained transport (B
+    through the fluxes), their throughput, the mixed form's error and drifts
+    against FP64; then FP64 with constrained transport (the configuration's
+    stated form) and its face-flux divergence drift."""
     import numpy as np
     import torch
     import disco_b200 as db
@@ -304,7 +305,61 @@ def config1_leg(args, local, stream):
         "div_b_rel_fp64": out["fp64"]["div_b"][0] / out["fp64"]["div_b"][1],
         "div_b_rel_mixed": out["mixed"]["div_b"][0] / out["mixed"]["div_b"][1]}
     out["mixed_speedup_vs_fp64"] = out["mixed"]["zone_updates_per_s"] / out["fp64"]["zone_updates_per_s"]
+
+    # The configuration's stated form: constrained transport (CT_MODE 2,
+    # Constrained_Transport 1), FP64.  Its invariant is each cell's net face
+    # flux (the discrete div B of the face fluxes), which CT keeps.
+    from disco_b200.workloads import write_par
+    p = write_par({"Constrained_Transport": 1}, base="c1_mhd3d")
+    diskc = db.Disk.from_files(p, opt)
+    os.unlink(p)
+    b = db.Batch([diskc], device=local)
+    b.set_stream(stream.cuda_stream)
+    d0, _ = face_flux_div(diskc, b)
+    b.run(3)
+    b.sync()
+    kt = {}
+    for name, t in b.kernel_times():
+        kt[name] = kt.get(name, 0.0) + t
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.run(nsteps)
+    e1.record(stream)
+    e1.synchronize()
+    if b.last_error() != 0:
+        raise RuntimeError("device error in the config-1 CT leg")
+    ms = e0.elapsed_time(e1)
+    d1, phimax = face_flux_div(diskc, b)
+    rc = diskc.real == 1
+    out["fp64_ct"] = {"zone_updates_per_s": diskc.nreal * nsteps / (ms / 1e3), "ms_per_step": ms / nsteps,
+                      "kernels_ms_per_step": {k: round(v, 4) for k, v in
+                                              sorted(kt.items(), key=lambda x: -x[1])},
+                      "face_div_b_drift_rel": float(np.abs(d1 - d0)[rc].max() / phimax),
+                      "note": "max over real cells of |net face flux(t) - net face flux(0)| / max |Phi|"}
+    b.close()
     return out
+
+
+def face_flux_div(disk, batch):
+    """Net magnetic flux out of each cell through its faces under CT (the
+    face-flux slots Phi), and max |Phi|."""
+    import numpy as np
+    st = batch.get_cells()
+    Phi = st["Phi"]
+    div = np.zeros(disk.ncell)
+    dims = [(1, 2, 1)] + ([(2, 4, 3)] if disk.Nz > 1 and Phi.shape[1] == 5 else [])
+    for dim, s0, s1 in dims:
+        F = batch.faces(0, dim)
+        L, R, lr = F["iL"], F["iR"], F["LRtype"]
+        v = np.where(lr == 0, Phi[L, s0], Phi[R, s1])
+        np.add.at(div, L, v)
+        np.add.at(div, R, -v)
+    off = np.concatenate([[0], np.cumsum(disk.Np)])
+    for a in range(len(disk.Np)):
+        c = np.arange(off[a], off[a + 1])
+        div[c] += Phi[c, 0] - Phi[np.roll(c, 1), 0]
+    return div, float(np.abs(Phi).max())
 
 
 C2P_GRID = {"Nr": 192, "Nz": 96, "Np": 462, "rmin": 1.5, "rmax": 50.0, "zmin": -20.0, "zmax": 20.0}

@@ -67,13 +67,15 @@ def test_dropin_config0_20_steps():
     assert np.max(np.abs(b["Qrz"] - a["Qrz"])) <= 1e-12 * np.max(np.abs(a["Qrz"]))
 
 
-def test_dropin_constrained_transport_bitexact():
-    """2D constrained transport through the drop-in: the reference's own
-    set_B_fields on the host, then the device steps; the face-flux slots
-    real cells read travel both ways through the shim."""
-    ref, hyb = _binaries("c1_mhd2d_nograv")
-    par = os.path.join(GOLDEN, "c1_ct_rigid.par")
-    a, b = _run(ref, par, 8), _run(hyb, par, 8)
+@pytest.mark.parametrize("cfg,case,n", [("c1_mhd2d_nograv", "c1_ct_rigid", 8),
+                                        ("c1_mhd3d_nograv", "c1_ct3d_rigid", 6)])
+def test_dropin_constrained_transport_bitexact(cfg, case, n):
+    """Constrained transport through the drop-in (2D CT_MODE 1, 3D CT_MODE 2):
+    the reference's own set_B_fields on the host, then the device steps; the
+    face-flux slots real cells read travel both ways through the shim."""
+    ref, hyb = _binaries(cfg)
+    par = os.path.join(GOLDEN, case + ".par")
+    a, b = _run(ref, par, n), _run(hyb, par, n)
     assert np.array_equal(a["dt"], b["dt"])
     r = a["real"] == 1
     for k in ("prim", "cons"):
@@ -81,9 +83,16 @@ def test_dropin_constrained_transport_bitexact():
     for k in ("piph", "dphi", "wiph"):
         assert np.array_equal(a[k], b[k]), k
     m = a["meta"]
-    j = np.repeat(np.arange(m["Nr"] * m["Nz"]) % m["Nr"], a["Np"])
+    Nr, Nz = m["Nr"], m["Nz"]
+    jk = np.repeat(np.arange(Nr * Nz), a["Np"])
+    j, k = jk % Nr, jk // Nr
+    rj = (j >= m["NgRa"]) & (j < Nr - m["NgRb"])
+    rk = (k >= m["NgZa"]) & (k < Nz - m["NgZb"])
     assert np.array_equal(a["Phi"][r, 0], b["Phi"][r, 0])
-    s1 = (j >= m["NgRa"]) & (j <= m["Nr"] - m["NgRb"])
-    s2 = (j >= m["NgRa"] - 1) & (j <= m["Nr"] - m["NgRb"] - 1)
-    assert np.array_equal(a["Phi"][s1, 1], b["Phi"][s1, 1])
-    assert np.array_equal(a["Phi"][s2, 2], b["Phi"][s2, 2])
+    masks = {1: (j >= m["NgRa"]) & (j <= Nr - m["NgRb"]) & rk,
+             2: (j >= m["NgRa"] - 1) & (j <= Nr - m["NgRb"] - 1) & rk}
+    if a["Phi"].shape[1] == 5:
+        masks[3] = rj & (k >= m["NgZa"]) & (k <= Nz - m["NgZb"])
+        masks[4] = rj & (k >= m["NgZa"] - 1) & (k <= Nz - m["NgZb"] - 1)
+    for s, mk in masks.items():
+        assert np.array_equal(a["Phi"][mk, s], b["Phi"][mk, s]), s
