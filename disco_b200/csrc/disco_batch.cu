@@ -118,6 +118,9 @@ static void make_float_view(disco_batch *b){
    f.prim = (float *)d.prim; f.gradp = (float *)d.gradp; f.gradr = (float *)d.gradr;
    f.gradz = (float *)d.gradz;
    f.fS = (float *)d.fS; f.fG = (float *)d.fG;
+   f.ctE = (float *)d.ctE; f.ctB = (float *)d.ctB;
+   f.pE = (float *)d.pE; f.pB = (float *)d.pB; f.pEr = (float *)d.pEr; f.pBz = (float *)d.pBz;
+   f.fEt = (float *)d.fEt; f.fBt = (float *)d.fBt; f.fEphi = (float *)d.fEphi;
 }
 
 extern "C" void disco_batch_destroy(disco_batch *b);
@@ -140,8 +143,8 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
     * cells; MHD builds need it (with CT_MODE 0, flip_fluxes, bfields.c:
     * 760-814, writes through zero-length Phi arrays into the cell's real
     * flag and the next cell's prims), so it is accepted.  Constrained
-    * transport itself is built for 2D disks (CT_MODE 1, Nz = 1) in FP64,
-    * for every disk of the batch or none. */
+    * transport itself is built in both forms, for every disk of the batch
+    * or none. */
    bool mhd = mods->hydro == DISCO_HYDRO_MHD;
    if( !((mods->hydro == DISCO_HYDRO_EULER && mods->num_c == 5) || (mhd && mods->num_c == 8)) ||
        mods->num_n != 1 || mods->ct_mode < 0 || mods->ct_mode > 2 )
@@ -151,7 +154,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    if( params[0].CT ){
       /* CT_MODE 1 stores no z-face fluxes, so it is built for 2D disks; in 3D
        * (CT_MODE 2) avg_Efields' z-pole branch (NgZa or NgZb = 0) is not */
-      if( !mhd || mods->ct_mode < 1 || precision != DISCO_PREC_FP64 ) return DISCO_ERR_UNSUPPORTED;
+      if( !mhd || mods->ct_mode < 1 ) return DISCO_ERR_UNSUPPORTED;
       for( int d=0 ; d<ndisk ; ++d ){
          if( Nz[d] > 1 && (mods->ct_mode != 2 || Ng[4*d+2] == 0 || Ng[4*d+3] == 0) )
             return DISCO_ERR_UNSUPPORTED;
@@ -384,15 +387,16 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       v.ct = ct;
       v.nfs = b->nfs;
       size_t ne = ct == 2 ? 8 : 4;
+      auto ralloc = [&](size_t n){ return (double *)dalloc_bytes(b, n*rs); };   /* R-typed */
       v.Phi = dalloc<double>(b, b->nfs*N); v.RKPhi = dalloc<double>(b, b->nfs*N);
-      v.ctE = dalloc<double>(b, ne*N); v.ctB = dalloc<double>(b, ne*N);
-      v.pE = dalloc<double>(b, N); v.pB = dalloc<double>(b, N);
-      v.fEt = dalloc<double>(b, face); v.fBt = dalloc<double>(b, face);
+      v.ctE = ralloc(ne*N); v.ctB = ralloc(ne*N);
+      v.pE = ralloc(N); v.pB = ralloc(N);
+      v.fEt = ralloc(face); v.fBt = ralloc(face);
       v.fX = dalloc<double>(b, face);
       v.fFlip = dalloc<unsigned char>(b, face);
       if( ct == 2 ){
-         v.pEr = dalloc<double>(b, N); v.pBz = dalloc<double>(b, N);
-         v.fEphi = dalloc<double>(b, face);
+         v.pEr = ralloc(N); v.pBz = ralloc(N);
+         v.fEphi = ralloc(face);
          if( b->any_3d ){
             v.rk = dalloc<int>(b, 4*N);
             v.lineX = dalloc<double>(b, (size_t)b->line_ne);

@@ -101,7 +101,7 @@ template<int Q, int NC, class R>
 static void launch_setup_qt(disco_batch *b, const ViewT<R> &v){
    unsigned ncb = (unsigned)b->cblk.size();
    k_setup<Q,NC,R><<<ncb, CB, 0, b->stream>>>(v, b->bc_fixed);
-   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+   if constexpr ( NC == 8 ){
       if( b->ct ){                  /* set_B_fields (bfields.c:12-86), then cons2prim */
          unsigned nfb = (unsigned)b->fblk.size();
          k_I0<R><<<nblk((size_t)v.Nann*32, 128), 128, 0, b->stream>>>(v);
@@ -134,7 +134,7 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    k_flux_t<Q,NC,1,R><<<nfb, FB, 0, s>>>(v);                          mark(b, "k_flux_r");
    if( b->any_3d ){ k_flux_t<Q,NC,2,R><<<nfb, FB, 0, s>>>(v);         mark(b, "k_flux_z"); }
    k_update<Q,NC,R><<<ncb, CB, 0, s>>>(v, first);                     mark(b, "k_update");
-   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+   if constexpr ( NC == 8 ){
       if( b->ct ){                  /* onestep.c:140-146 and 160-167 */
          k_ct_edges<R><<<ncb, CB, 0, s>>>(v);                           mark(b, "k_ct_edges");
          k_ct_faces<R><<<nfb, FB, 0, s>>>(v);                           mark(b, "k_ct_faces");

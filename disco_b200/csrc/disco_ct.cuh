@@ -1,8 +1,11 @@
 /*
  * Constrained transport (in.par Constrained_Transport 1; bfields.c,
- * riemann.c:73-110 and 175-213, onestep.c:140-185), FP64, as order-preserving
+ * riemann.c:73-110 and 175-213, onestep.c:140-185) as order-preserving
  * per-cell and per-face kernels.  CT_MODE 1 (2D: the in-plane field) and
  * CT_MODE 2 (3D: also the z faces, the E_phi edges and make_edge_adjust).
+ * The edge arithmetic runs in the bulk real type R (FP32 in the mixed form);
+ * the face fluxes Phi and their updates E dl dt stay FP64, so CT keeps the
+ * discrete div B in both forms.
  *
  * The reference keeps the magnetic flux of every r- or z-face in one slot of
  * the cell that "owns" the face (the face ending at the cell's piph: r faces
@@ -84,29 +87,29 @@ __global__ void __launch_bounds__(CB) k_ct_edges(ViewT<R> v){
    const DiskParams &P = v.dp[v.ann_disk[a]];
    int j = v.ann_j[a], k = v.ann_k[a];
    const int ne = v.ct == 2 ? 8 : 4;
-   double E[8] = {0,0,0,0,0,0,0,0}, B[8] = {0,0,0,0,0,0,0,0};
+   R E[8] = {0,0,0,0,0,0,0,0}, B[8] = {0,0,0,0,0,0,0,0};
    if( ct_phi_annulus(P, j, k) ){
       /* riemann_phi: cL->E[0], E[1] (E[4], E[5]) and cR->E[2], E[3] (E[6],
        * E[7]) = .5 Ez (.5 Er), riemann.c:73-110 */
-      double eR = .5*v.pE[c], eL = .5*v.pE[cm];
-      double bR = .5*v.pB[c], bL = .5*v.pB[cm];
+      R eR = R(.5)*v.pE[c], eL = R(.5)*v.pE[cm];
+      R bR = R(.5)*v.pB[c], bL = R(.5)*v.pB[cm];
       E[0] = eR; E[1] = eR; E[2] = eL; E[3] = eL;
       B[0] = bR; B[1] = bR; B[2] = bL; B[3] = bL;
       if( v.ct == 2 ){
-         double zR = .5*v.pEr[c], zL = .5*v.pEr[cm];
-         double wR = .5*v.pBz[c], wL = .5*v.pBz[cm];
+         R zR = R(.5)*v.pEr[c], zL = R(.5)*v.pEr[cm];
+         R wR = R(.5)*v.pBz[c], wL = R(.5)*v.pBz[cm];
          E[4] = zR; E[5] = zR; E[6] = zL; E[7] = zL;
          B[4] = wR; B[5] = wR; B[6] = wL; B[7] = wL;
       }
-      double dph = v.dphi[c];
+      R dph = (R)v.dphi[c];
       int I0 = v.I0[a];
       /* riemann_trans (riemann.c:175-205): as R of the inner (lower) track
        * E[0], E[2] (E[4], E[6]) += .5 Erz fracR; as L of the outer (upper)
        * track E[1], E[3] (E[5], E[7]) += .5 Erz fracL */
       auto add = [&](int lo, int hi) {
          return [&, lo, hi](int f) {
-            double fr = v.fdp[f] / dph;
-            double xe = .5*v.fEt[f]*fr, xb = .5*v.fBt[f]*fr;
+            R fr = (R)v.fdp[f] / dph;
+            R xe = R(.5)*v.fEt[f]*fr, xb = R(.5)*v.fBt[f]*fr;
             E[lo] += xe; E[hi] += xe; B[lo] += xb; B[hi] += xb;
          };
       };
@@ -163,7 +166,7 @@ __global__ void __launch_bounds__(FB) k_ct_faces(ViewT<R> v){
    int ao = lr == 0 ? A : Bn, a2 = lr == 0 ? Bn : A;
    int on = ct_next(v, ao, o);
    int c2n = ct_next(v, a2, c2), c2p = ct_prev(v, a2, c2);
-   const double *E = v.ctE, *B = v.ctB;
+   const R *E = v.ctE, *B = v.ctB;
    const size_t s0 = zf ? 4 : 0;          /* r faces use edges 0-3, z faces 4-7 */
    /* the phi average of avg_Efields: edge s of cell c becomes
     * .5 (E[s](c) + E[s+2](c+1)) for the right edges s = 0, 1 and
@@ -171,16 +174,17 @@ __global__ void __launch_bounds__(FB) k_ct_faces(ViewT<R> v){
    double p1 = v.piph[o], p2 = v.piph[c2];
    double dp1 = get_dp(p2, p1, P.Pmax, &err);
    double dp2 = v.dphi[c2] - dp1;
+   const R w1 = (R)dp1, w2 = (R)dp2;
    /* owner edge s_o (and its left twin s_o+2); c2's edges s_c, s_c+2 */
    size_t so = lr == 0 ? s0+1 : s0, sc = lr == 0 ? s0 : s0+1;
-   double Eo = .5*(E[so*N + o] + E[(so+2)*N + on]);
-   double Bo = .5*(B[so*N + o] + B[(so+2)*N + on]);
-   double ea = .5*(E[sc*N + c2] + E[(sc+2)*N + c2n]), eb = .5*(E[sc*N + c2p] + E[(sc+2)*N + c2]);
-   double ba = .5*(B[sc*N + c2] + B[(sc+2)*N + c2n]), bb = .5*(B[sc*N + c2p] + B[(sc+2)*N + c2]);
-   double Eav = ( dp2*ea + dp1*eb )/(dp1+dp2);
-   double Bav = ( dp2*ba + dp1*bb )/(dp1+dp2);
-   double fE = .5*(Eo + Eav);
-   double fB = .5*(Bo + Bav);
+   R Eo = R(.5)*(E[so*N + o] + E[(so+2)*N + on]);
+   R Bo = R(.5)*(B[so*N + o] + B[(so+2)*N + on]);
+   R ea = R(.5)*(E[sc*N + c2] + E[(sc+2)*N + c2n]), eb = R(.5)*(E[sc*N + c2p] + E[(sc+2)*N + c2]);
+   R ba = R(.5)*(B[sc*N + c2] + B[(sc+2)*N + c2n]), bb = R(.5)*(B[sc*N + c2p] + B[(sc+2)*N + c2]);
+   R Eav = ( w2*ea + w1*eb )/(w1+w2);
+   R Bav = ( w2*ba + w1*bb )/(w1+w2);
+   R fE = R(.5)*(Eo + Eav);
+   R fB = R(.5)*(Bo + Bav);
    /* subtract_advective_B_fluxes: the owner's edge moves with its wiph; an
     * r face's edge sits at r_jph[j] (E -= h w B), a z face's at the
     * annulus centroid (E += h w B) */
@@ -188,18 +192,19 @@ __global__ void __launch_bounds__(FB) k_ct_faces(ViewT<R> v){
    const double *rj = v.rj + P.rj0 + 1;
    const double *zk = v.zk + P.zk0 + 1;
    double w = v.wiph[o];
-   double Ef, dl;
+   R Ef;
+   double dl;
    if( !zf ){
       double h = rj[j];
-      Ef = fE - h*w*fB;
+      Ef = fE - (R)(h*w)*fB;
       dl = zk[k]-zk[k-1];                         /* r-face dl = dz, faces_alt.c:26-27 */
    }else{
       double h = centroid_r(rj[j], rj[j-1]);
-      Ef = fE + h*w*fB;
+      Ef = fE + (R)(h*w)*fB;
       dl = rj[j]-rj[j-1];                         /* z-face dl = dr */
    }
    double dt = v.ds[d].dt*v.dtfac;
-   v.fX[f] = Ef*dl*dt;
+   v.fX[f] = (double)Ef*dl*dt;
    raise_err(v, err);
 }
 
@@ -232,14 +237,14 @@ __device__ __forceinline__ int ct_which4(double phi, double phiR, double phiU, d
 /* E_phi of the face cell c owns on side s (0 inner r, 1 outer r, 2 lower z,
  * 3 upper z), as riemann_trans left it (riemann.c:188-212); cell (jc, kc) */
 template<class R>
-__device__ __forceinline__ double ct_ephi(const ViewT<R> &v, const DiskParams &P, int c, int jc,
-                                          int kc, int s){
+__device__ __forceinline__ R ct_ephi(const ViewT<R> &v, const DiskParams &P, int c, int jc,
+                                     int kc, int s){
    int t, f;
    if( s == 0 ){ t = P.trr0 + (jc-1) + (P.Nr-1)*kc; f = v.consR[c]; }
    else if( s == 1 ){ t = P.trr0 + jc + (P.Nr-1)*kc; f = v.consL[c]; }
    else if( s == 2 ){ t = P.trz0 + jc + P.Nr*(kc-1); f = v.consZR[c]; }
    else { t = P.trz0 + jc + P.Nr*kc; f = v.consZL[c]; }
-   return v.tr_flux[t] ? v.fEphi[f] : 0.0;
+   return v.tr_flux[t] ? v.fEphi[f] : R(0.0);
 }
 
 /* make_edge_adjust, one thread per (cell, list): the line (jl, kl) is the
@@ -319,28 +324,29 @@ __global__ void __launch_bounds__(CB) k_ct_line(ViewT<R> v){
       if( w4 != m ) err |= ERRF_INTERNAL;
       /* E_phi of the cells' owned faces: c [3],[1]; cR [3],[0]; cU [1],[2]; cUR [0],[2] */
       auto eph = [&](int n, int s){ return ct_ephi(v, P, cur[n], jl + (n & 1), kl + (n >> 1), s); };
-      double E;
+      const R q4 = R(.25);
+      R E;
       if( w4 == 0 ){
-         E = .25*( eph(0,3) + eph(0,1) );
-         if( LR_alt == 0 ) E += .25*eph(2,1); else E += .25*eph(3,0);
-         if( UD_alt == 0 ) E += .25*eph(1,3); else E += .25*eph(3,2);
+         E = q4*( eph(0,3) + eph(0,1) );
+         if( LR_alt == 0 ) E += q4*eph(2,1); else E += q4*eph(3,0);
+         if( UD_alt == 0 ) E += q4*eph(1,3); else E += q4*eph(3,2);
       }else if( w4 == 1 ){
-         E = .25*( eph(1,3) + eph(1,0) );
-         if( LR_alt == 0 ) E += .25*eph(2,1); else E += .25*eph(3,0);
-         if( UD_alt == 0 ) E += .25*eph(0,3); else E += .25*eph(2,2);
+         E = q4*( eph(1,3) + eph(1,0) );
+         if( LR_alt == 0 ) E += q4*eph(2,1); else E += q4*eph(3,0);
+         if( UD_alt == 0 ) E += q4*eph(0,3); else E += q4*eph(2,2);
       }else if( w4 == 2 ){
-         E = .25*( eph(2,2) + eph(2,1) );
-         if( LR_alt == 0 ) E += .25*eph(0,1); else E += .25*eph(1,0);
-         if( UD_alt == 0 ) E += .25*eph(1,3); else E += .25*eph(3,2);
+         E = q4*( eph(2,2) + eph(2,1) );
+         if( LR_alt == 0 ) E += q4*eph(0,1); else E += q4*eph(1,0);
+         if( UD_alt == 0 ) E += q4*eph(1,3); else E += q4*eph(3,2);
       }else{
-         E = .25*( eph(3,2) + eph(3,0) );
-         if( LR_alt == 0 ) E += .25*eph(0,1); else E += .25*eph(1,0);
-         if( UD_alt == 0 ) E += .25*eph(0,3); else E += .25*eph(2,2);
+         E = q4*( eph(3,2) + eph(3,0) );
+         if( LR_alt == 0 ) E += q4*eph(0,1); else E += q4*eph(1,0);
+         if( UD_alt == 0 ) E += q4*eph(0,3); else E += q4*eph(2,2);
       }
       double xp1 = v.piph[cur[w4]];
       double xm1 = v.piph[cur[w4b]] - v.dphi[cur[w4b]];
       double dl = (.5*(rj[jl]+rj[jl]))*get_dp(xp1, xm1, Pmax, &err);   /* get_dL(.,.,0) */
-      v.lineX[v.line_off[line] + e] = E*dl*dt;
+      v.lineX[v.line_off[line] + e] = (double)E*dl*dt;
    }
    raise_err(v, err);
 }

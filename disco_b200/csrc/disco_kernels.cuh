@@ -115,14 +115,15 @@ struct ViewT {
     * the track inside / outside it (the face ending at its piph, LRtype 1 /
     * 0), s = 3 / 4 the same for the z-faces below / above it; ctE / ctB the
     * edge values E[0..7], B[0..7] (riemann.c:73-110, 175-213) before
-    * averaging; pE, pB, pEr, pBz the phi face's (Ez, Br, Er, Bz) from
+    * averaging (FP32 in the mixed form, whose face fluxes stay FP64); pE, pB, pEr, pBz the phi face's (Ez, Br, Er, Bz) from
     * flux_to_E.  Per face (r and z): fEt / fBt (Erz, Brz), fEphi (E_phi),
     * fX the E dl dt of update_B_fluxes, fFlip the flag of check_flipped.
     * 3D: rk[m*Ncell + c] the position of cell c in the 4-way merge of the
     * edge line where it is list m (make_edge_adjust's c, cR, cU, cUR), and
     * lineX[line_off[l] + e] the E_phi dl dt of merged edge e of line l. */
    int ct, nfs;
-   double *Phi, *RKPhi, *ctE, *ctB, *pE, *pB, *pEr, *pBz, *fEt, *fBt, *fEphi, *fX;
+   double *Phi, *RKPhi, *fX;            /* the face fluxes stay FP64 in both forms */
+   R *ctE, *ctB, *pE, *pB, *pEr, *pBz, *fEt, *fBt, *fEphi;   /* edge arithmetic: R */
    unsigned char *fFlip;
    int *rk, *line_off;
    double *lineX;
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_BEGIN) k_begin(ViewT<R
          if( !first ) v.ccarry[q*N + c] = (1.-RK)*v.ccarry[q*N + c];
       }
    }
-   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+   if constexpr ( NC == 8 ){
       if( v.ct ){                   /* timestep.c:22 and adjust_RK_cons, misc.c:239-241 */
 #pragma unroll
          for( int s=0 ; s<5 ; ++s ){
@@ -591,17 +592,18 @@ __global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R
    const double *rj = v.rj + P.rj0 + 1;
    double r = DIM == 1 ? .5*(rj[j]+rj[j]) : centroid_r(rj[j], rj[j-1]);    /* face cm[0] */
    R G[Q];
-   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+   if constexpr ( NC == 8 ){
       if( v.ct ){                    /* flux_to_E dim 1 / 2, Hydro/mhd.c:304-314 */
          R eb[5];
          solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G, eb);
-         double irfac = 1.0/(1.0/r);
+         const R rr = (R)r;
+         const R irfac = (R)(1.0/(1.0/r));
          if( DIM == 1 ){
-            v.fEt[f] = -eb[1]*r;
+            v.fEt[f] = -eb[1]*rr;
             v.fBt[f] = eb[2]*irfac;
             if( v.ct == 2 ) v.fEphi[f] = eb[3];
          }else{
-            v.fEt[f] = eb[1]*r;
+            v.fEt[f] = eb[1]*rr;
             v.fBt[f] = eb[4];
             v.fEphi[f] = -eb[0]*irfac;
          }
@@ -669,7 +671,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
     * to the real ones (misc.c:382-397): their faces' E is needed, their cons
     * updates are not (the ghosts' cons never reach a real cell). */
    bool ctE = false;
-   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+   if constexpr ( NC == 8 ){
       if( v.ct ){
          int jmin = P.NgRa == 0 ? 0 : P.NgRa-1, jmax = P.NgRb == 0 ? P.Nr : P.Nr-P.NgRb+1;
          int kmin = P.NgZa == 0 ? 0 : P.NgZa-1, kmax = P.NgZb == 0 ? P.Nz : P.Nz-P.NgZb+1;
@@ -686,7 +688,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
          if( ctE ){                 /* flux_to_E dim 0, Hydro/mhd.c:298-303 */
             R eb[5];
             phi_face_flux<Q,NC,R>(v, P, a, c, cn, rc, dAdtp, G, eb);
-            double irfac = 1.0/(1.0/rc);
+            const R irfac = (R)(1.0/(1.0/rc));
             v.pE[c] = eb[0]*irfac;
             v.pB[c] = eb[2]*irfac;
             if( v.ct == 2 ){ v.pEr[c] = -eb[3]; v.pBz[c] = eb[4]; }
@@ -1057,7 +1059,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v,
       if( real ){
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) cons[q] = v.cons[q*N + c];
-         if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+         if constexpr ( NC == 8 ){
             if( v.ct ){                  /* onestep.c:183-185 */
                const double *rj = v.rj + P.rj0 + 1;
                const double *zk = v.zk + P.zk0 + 1;
@@ -1335,7 +1337,7 @@ __global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc){
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ) v.ccarry[q*N+c] = 0.0;
    }
-   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+   if constexpr ( NC == 8 ){
       if( v.ct ){                        /* set_B_fields, bfields.c:22-42 */
          double x[3] = { centroid_r(rj[j], rj[j-1]), piph, centroid_z(zk[k], zk[k-1]) };
          double pb[Q];
