@@ -341,6 +341,63 @@ def config1_leg(args, local, stream):
     return out
 
 
+B_ALG_MHD_CT = {"fp64": 1056, "mixed": 1200}   # HBM bytes per zone-update, MHD Q=9 with CT (5 faces)
+
+
+def config4_leg(args, local, stream):
+    """3D MHD circumbinary disk with constrained transport (softened
+    equal-mass binary, HLLD, CT_MODE 2, zerograd; Nr 384 x Nz 128, Np up to
+    1536, 39.5M real cells): 50 steps of the mixed form (FP32 bulk, FP64
+    phi/mesh/Kahan update, FP64 face fluxes) against the FP64 plain path,
+    from the same set-up; throughput, step-level fraction of the HBM
+    roofline, and the mixed form's density / pressure error."""
+    import numpy as np
+    import torch
+    import disco_b200 as db
+    par, opt = db.template_paths("c4_binary3d")
+    disk = db.Disk.from_files(par, opt)
+    nsteps = 50
+    hbm, kind = peaks()
+    out = {"workload": "3D MHD circumbinary disk, softened equal-mass binary, HLLD + CT, zerograd, "
+                       "Nr=%d Nz=%d (incl. ghosts), Np max %d, %d real cells"
+                       % (disk.Nr, disk.Nz, int(np.max(disk.Np)), disk.nreal),
+           "steps": nsteps, "warmup": 3}
+    ref = None
+    r = disk.real == 1
+    for prec, key in ((db.PREC_FP64, "fp64"), (db.PREC_MIXED, "mixed")):
+        b = db.Batch([disk], device=local, precision=prec)
+        b.set_stream(stream.cuda_stream)
+        b.run(3)
+        b.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.run(nsteps)
+        e1.record(stream)
+        e1.synchronize()
+        if b.last_error() != 0:
+            raise RuntimeError("device error in the config-4 leg")
+        ms = e0.elapsed_time(e1)
+        zu = disk.nreal * nsteps / (ms / 1e3)
+        out[key] = {"zone_updates_per_s": zu, "ms_per_step": ms / nsteps,
+                    "step_roofline": {"bytes_per_zone_update": B_ALG_MHD_CT[key],
+                                      "achieved": B_ALG_MHD_CT[key] * zu / 1e9, "peak": hbm,
+                                      "unit": "GB/s", "frac": B_ALG_MHD_CT[key] * zu / 1e9 / hbm,
+                                      "peak_kind": kind}}
+        st = b.get_cells()
+        if key == "fp64":
+            ref = st["prim"][r][:, :2].copy()
+        else:
+            pm = st["prim"][r][:, :2]
+            out["mixed_rel_l1_vs_fp64"] = {
+                nm: float(np.abs(pm[:, q] - ref[:, q]).sum() / np.abs(ref[:, q]).sum())
+                for q, nm in ((0, "rho"), (1, "P"))}
+        del st
+        b.close()
+    out["mixed_speedup_vs_fp64"] = out["mixed"]["zone_updates_per_s"] / out["fp64"]["zone_updates_per_s"]
+    return out
+
+
 def face_flux_div(disk, batch):
     """Net magnetic flux out of each cell through its faces under CT (the
     face-flux slots Phi), and max |Phi|."""
@@ -606,6 +663,11 @@ def run_ours(args, world, rank, local):
         config1 = config1_leg(args, local, stream)
         barrier()
 
+    config4 = None
+    if not args.no_config4:
+        config4 = config4_leg(args, local, stream)
+        barrier()
+
     c2p = None
     if not args.no_c2p:
         c2p = c2p_leg(args, local, stream)
@@ -645,6 +707,7 @@ def run_ours(args, world, rank, local):
             "gpu_launches": launches_per_step * args.steps,
             "mixed_form": mixed,
             "config1_mhd3d": config1,
+            "config4_binary3d": config4,
             "c2p": c2p,
             "clocks": ck,
             "cpu_baseline": cpu,
@@ -666,6 +729,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--no-c2p", action="store_true", help="skip the GRMHD cons->prim leg")
     ap.add_argument("--no-config1", action="store_true", help="skip the 3D MHD (config 1) leg")
+    ap.add_argument("--no-config4", action="store_true",
+                    help="skip the 40M-cell 3D MHD circumbinary (config 4) leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -99,8 +99,10 @@ static void init_planets(DiskState &S, DiskParams &D, const disco_params &p, con
          S.pl[1].M = mu;    S.pl[1].omega = om; S.pl[1].r = a*(1.-mu);
          break; }
       case DISCO_PLANETS_BINARY_SOFT: {                /* new module: softened equal-mass binary */
+         /* separation 1, circular, softening Init_Par8 (Init_Par5-7 belong
+          * to the disk's initial conditions) */
          D.npl = 2;
-         double a = p.initPar[5] > 0 ? p.initPar[5] : 1.0, eps = p.initPar[6];
+         double a = 1.0, eps = p.initPar[8];
          double om = 1.0/(a*sqrt(a));
          S.pl[0].M = 0.5; S.pl[0].omega = om; S.pl[0].r = 0.5*a; S.pl[0].phi = M_PI; S.pl[0].eps = eps;
          S.pl[1].M = 0.5; S.pl[1].omega = om; S.pl[1].r = 0.5*a; S.pl[1].phi = 0.0;  S.pl[1].eps = eps;

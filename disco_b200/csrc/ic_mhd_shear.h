@@ -24,13 +24,17 @@
  * held by pressure, P = rho cs^2/gamma + r^2/2, so no gravity is needed:
  * with PLANETS = none and Energy_Omega 0 a step calls no libm function
  * whose value matters, and a CPU and a GPU build agree bit for bit.
+ * With Init_Par2 = 2 it is a circumbinary disk: surface density
+ * rho = (rmin/r)^(1/2) (1 + amp u_rho), P = rho cs^2/gamma, Keplerian Omega
+ * about the unit total mass, no velocity noise (Bphi's beta then follows the
+ * local pressure).
  *
  * Noise only inside [rmin, rmax] x [zmin, zmax] (ghost cells stay smooth).
  * Uses +,-,*,/, sqrt and floor only, so host and device values are
  * bit-identical.
  *
  * Parameters (in.par): Init_Par0 = seed, Init_Par1 = amp (fraction of cs),
- * Init_Par2 = kind (0 Keplerian, 1 rigid), Init_Par3 = cs, Init_Par4 = beta,
+ * Init_Par2 = kind (0 Keplerian, 1 rigid, 2 circumbinary), Init_Par3 = cs, Init_Par4 = beta,
  * Init_Par5 = beta_phi, Init_Par6 = b_r, Adiabatic_Index, R_Min/R_Max,
  * Z_Min/Z_Max, Phi_Max.
  */
@@ -76,7 +80,12 @@ DISCO_HD void disco_ic_mhd_shear_eval(const disco_ic_mhd_shear *p, int num_c, in
       press = press + 0.5 * r * r;
    }
    double vr = 0.0, vz = 0.0;
-   if( r >= p->rmin && r <= p->rmax && z >= p->zmin && z <= p->zmax && p->amp != 0.0 ){
+   int inside = r >= p->rmin && r <= p->rmax && z >= p->zmin && z <= p->zmax;
+   if( p->kind == 2 ){
+      rho = sqrt(p->rmin / r);
+      if( inside && p->amp != 0.0 ) rho *= 1.0 + p->amp * disco_hash_unit3(p->seed, 4, r, phi, z, p->phimax);
+      press = rho * p->cs * p->cs / p->gam;
+   }else if( inside && p->amp != 0.0 ){
       double a = p->amp * p->cs;
       vr = a * disco_hash_unit3(p->seed, 1, r, phi, z, p->phimax);
       vz = a * disco_hash_unit3(p->seed, 2, r, phi, z, p->phimax);
@@ -90,7 +99,7 @@ DISCO_HD void disco_ic_mhd_shear_eval(const disco_ic_mhd_shear *p, int num_c, in
    int q;
    for( q=5 ; q<num_c ; ++q ) prim[q] = 0.0;
    if( num_c >= 8 ){
-      double p0 = rho * p->cs * p->cs / p->gam;
+      double p0 = rho * p->cs * p->cs / p->gam;     /* the disk's gas pressure */
       prim[7] = sqrt(2.0 * p0 / p->beta);
       if( p->beta_phi > 0.0 ) prim[6] = sqrt(2.0 * p0 / p->beta_phi);
       if( p->b_r != 0.0 ){
