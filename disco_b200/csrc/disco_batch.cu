@@ -368,7 +368,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.fS = (double *)dalloc_bytes(b, Qf*rs);
    v.fG = (double *)dalloc_bytes(b, Qf*rs);
    v.cons = dalloc<double>(b, Qn); v.RKcons = dalloc<double>(b, Qn);
-   v.ccarry = precision == DISCO_PREC_MIXED ? dalloc<double>(b, Qn) : NULL;
+   v.ccarry = precision == DISCO_PREC_MIXED ? dalloc<float>(b, Qn) : NULL;
    v.piph = dalloc<double>(b, N); v.dphi = dalloc<double>(b, N);
    v.wiph = dalloc<double>(b, N); v.piph_new = dalloc<double>(b, N);
    v.I0 = dalloc<int>(b, ann);
@@ -525,7 +525,7 @@ extern "C" int disco_batch_set_cells(disco_batch *b, const double *prim, const d
    CK(xfer(b, b->vd.piph, piph, N*sizeof(double), cudaMemcpyHostToDevice));
    CK(xfer(b, b->vd.dphi, dphi, N*sizeof(double), cudaMemcpyHostToDevice));
    if( wiph ) CK(xfer(b, b->vd.wiph, wiph, N*sizeof(double), cudaMemcpyHostToDevice));
-   if( b->vd.ccarry ) CK(cudaMemsetAsync(b->vd.ccarry, 0, (size_t)b->Q*N*sizeof(double), b->stream));
+   if( b->vd.ccarry ) CK(cudaMemsetAsync(b->vd.ccarry, 0, (size_t)b->Q*N*sizeof(float), b->stream));
    CK(cudaMemsetAsync(b->vd.topo, 0, sizeof(int), b->stream));      /* new piph: faces stale */
    if( prim && !cons ){
       unsigned ncb = (unsigned)b->cblk.size();

@@ -9,7 +9,8 @@
  *
  * Layout (device, one batch of one or more disks):
  *   cells      ragged SoA in annulus order; prim[q*Ncell + c] (R), cons (FP64),
- *              RKcons, ccarry (Kahan carry, mixed form), gradp, gradr (R);
+ *              RKcons (FP64), ccarry (FP32 Kahan carry, mixed form), gradp,
+ *              gradr (R);
  *              piph[c], dphi[c], wiph[c] (FP64)
  *   annuli     ann_off[a] .. ann_off[a]+ann_np[a]-1 are annulus a's cells
  *   tracks     track t joins annulus tr_a[t] (inner / lower) and tr_b[t]
@@ -84,7 +85,9 @@ struct ViewT {
    const DiskParams *dp;
    DiskState *ds;
    R *prim, *gradp, *gradr, *gradz;   /* gradz only when a disk has Nz > 1 */
-   double *cons, *RKcons, *ccarry;
+   double *cons, *RKcons;
+   float *ccarry;       /* Kahan carry of cons (mixed form): below half an ulp of cons,
+                         * so FP32 keeps 24 more bits of the sum than cons has */
    double *piph, *dphi, *wiph, *piph_new;
    int *I0;
    int *fL, *fR;
@@ -199,7 +202,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_BEGIN) k_begin(ViewT<R
       v.cons[q*N + c] = (1.-RK)*cq + RK*rk;
       if constexpr ( sizeof(R) != sizeof(double) ){
          /* the carry belongs to cons; averaged with it (RKcons keeps none) */
-         if( !first ) v.ccarry[q*N + c] = (1.-RK)*v.ccarry[q*N + c];
+         if( !first ) v.ccarry[q*N + c] = (float)((1.-RK)*(double)v.ccarry[q*N + c]);
       }
    }
    if constexpr ( NC == 8 ){
@@ -716,7 +719,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){
          cons[q] = v.cons[q*N + c];
-         if constexpr ( sizeof(R) != sizeof(double) ) cc[q] = v.ccarry[q*N + c];
+         if constexpr ( sizeof(R) != sizeof(double) ) cc[q] = (double)v.ccarry[q*N + c];
          else cc[q] = 0.0;
       }
       /* phi faces: loop order of phi_flux */
@@ -819,7 +822,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){
          v.cons[q*N + c] = cons[q];
-         if constexpr ( sizeof(R) != sizeof(double) ) v.ccarry[q*N + c] = cc[q];
+         if constexpr ( sizeof(R) != sizeof(double) ) v.ccarry[q*N + c] = (float)cc[q];
       }
    }
    if( first && !v.ct ){            /* with CT the edge fields read the old piph first */
@@ -1335,7 +1338,7 @@ __global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc){
    }
    if constexpr ( sizeof(R) != sizeof(double) ){
 #pragma unroll
-      for( int q=0 ; q<Q ; ++q ) v.ccarry[q*N+c] = 0.0;
+      for( int q=0 ; q<Q ; ++q ) v.ccarry[q*N+c] = 0.0f;
    }
    if constexpr ( NC == 8 ){
       if( v.ct ){                        /* set_B_fields, bfields.c:22-42 */
