@@ -536,12 +536,10 @@ def run_ours(args, world, rank, local):
             pg.barrier()
         torch.cuda.synchronize()
 
+    from disco_b200.replicas import job_rate, max_over_ranks
+
     def allmax(x):
-        if not pg:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(x, pg, device="cuda")
 
     disks = make_disks(args.workload, rank)
     b = db.Batch(disks, device=local)
@@ -574,7 +572,7 @@ def run_ours(args, world, rank, local):
     if b.last_error() != 0:
         raise RuntimeError("device error during the timed region: %s" % db.STATUS.get(b.last_error()))
     ms = allmax(e0.elapsed_time(e1))
-    value = world * nreal * args.steps / (ms / 1e3)
+    value = job_rate(world, nreal, args.steps, ms)
 
     # roofline of the dominant kernel (sum over its launches in the step)
     hbm, peak_kind = peaks()
