@@ -1,23 +1,28 @@
 """Autotuner for the step kernels' launch shapes.
 
-The step kernels are bound by memory latency: how many blocks an SM keeps
-resident (which __launch_bounds__ turns into each kernel's register budget)
-decides how many loads are in flight, and the best value differs per kernel,
-per precision and per GPU.  This tool
+The step kernels are bound by memory latency: the block size and how many
+blocks an SM keeps resident (which __launch_bounds__ turns into each
+kernel's register budget) decide how many loads are in flight, and the best
+values differ per kernel, per precision and per GPU.  This tool
 
-  1. builds the library once per candidate occupancy target MB (every
-     kernel's macro set to MB, both precisions) into a cache directory,
+  1. builds the library once per candidate shape -- a block size CB (cell
+     and face kernels alike) and an occupancy target MB for every kernel,
+     both precisions -- into a cache directory,
   2. times each kernel of one step of a workload with CUDA events
      (disco_batch_kernel_times, median of several instrumented steps), one
      child process per candidate and precision,
-  3. keeps, per kernel and precision, the fastest candidate and writes them
-     to csrc/tuned.h (with the measured table), which the kernels include.
+  3. keeps the block size whose per-kernel best times add up to the fastest
+     FP64 step (the host's block tables serve both precisions, so there is
+     one), then per kernel and precision the fastest MB at that block size,
+     and writes them to csrc/tuned.h with the measured table.
 
-    python -m disco_b200.autotune build   [--cache DIR] [--mb 4,6,8,...]   (no GPU needed)
+    python -m disco_b200.autotune build   [--cache DIR] [--mb 4,6,...] [--cb 128]   (no GPU)
     python -m disco_b200.autotune measure [--cache DIR] [--workload ragged64] [--write]
 
-Kernels are independent of each other's launch shape, so one sweep over MB
-picks every kernel's value at once.
+The MB list is given for 128-thread blocks and scaled for other block sizes
+so that every block size sees the same register budgets.  Kernels are
+independent of each other's launch shape, so one sweep picks every kernel's
+value at once.
 """
 import argparse
 import json
@@ -39,12 +44,17 @@ MACROS = {"k_begin": "MB_BEGIN", "k_faces": "MB_FACES", "k_gradr": "MB_GRAD",
 PRECISIONS = {"fp64": 0, "mixed": 1}
 
 
-def _variant_dir(cache, mb):
-    return os.path.join(cache, "mb%d" % mb)
+def _variant_dir(cache, cb, mb):
+    return os.path.join(cache, "cb%d_mb%d" % (cb, mb))
 
 
-def build_variants(cache=DEFAULT_CACHE, mbs=DEFAULT_MB, verbose=False):
-    """Compile one library per candidate; returns {mb: path}."""
+def _parse_variant(name):
+    cb, mb = name[2:].split("_mb")
+    return int(cb), int(mb)
+
+
+def build_variants(cache=DEFAULT_CACHE, mbs=DEFAULT_MB, cbs=(128,), verbose=False):
+    """Compile one library per candidate shape; returns {(cb, mb): path}."""
     nvcc = native.nvcc_path()
     native.build()                                 # objects of the untuned TUs
     bdir = os.path.join(HERE, "_build")
@@ -55,11 +65,12 @@ def build_variants(cache=DEFAULT_CACHE, mbs=DEFAULT_MB, verbose=False):
               if os.path.basename(s) not in tuned]
     shared += [os.path.join(bdir, os.path.basename(s) + ".o") for s in c]
     out = {}
-    for mb in mbs:
-        vdir = _variant_dir(cache, mb)
+    shapes = sorted({(cb, max(1, min(2048 // cb, mb * 128 // cb))) for cb in cbs for mb in mbs})
+    for cb, mb in shapes:
+        vdir = _variant_dir(cache, cb, mb)
         os.makedirs(vdir, exist_ok=True)
         lib = os.path.join(vdir, "libdisco_b200.so")
-        defs = ["-D%s=%d" % (m, mb) for m in MACROS.values()]
+        defs = ["-D%s=%d" % (m, mb) for m in MACROS.values()] + ["-DCB=%d" % cb, "-DFB=%d" % cb]
         objs = []
         for name in tuned:
             src = os.path.join(CSRC, name)
@@ -73,7 +84,7 @@ def build_variants(cache=DEFAULT_CACHE, mbs=DEFAULT_MB, verbose=False):
                     objs + shared + ["-lm"], verbose)
         for o in objs:
             os.unlink(o)
-        out[mb] = lib
+        out[(cb, mb)] = lib
     return out
 
 
@@ -100,49 +111,62 @@ def _child(lib, workload, precision, reps):
 
 
 def measure(cache=DEFAULT_CACHE, workload="ragged64", reps=7):
-    """{precision: {mb: {kernel: ms per step}}} for every built candidate."""
+    """{precision: {(cb, mb): {kernel: ms per step}}} for every built candidate."""
     res = {}
-    mbs = sorted(int(d[2:]) for d in os.listdir(cache) if d.startswith("mb") and
-                 os.path.exists(os.path.join(cache, d, "libdisco_b200.so")))
+    shapes = sorted(_parse_variant(d) for d in os.listdir(cache) if d.startswith("cb") and
+                    os.path.exists(os.path.join(cache, d, "libdisco_b200.so")))
     for pname, prec in PRECISIONS.items():
         res[pname] = {}
-        for mb in mbs:
-            lib = os.path.join(_variant_dir(cache, mb), "libdisco_b200.so")
+        for cb, mb in shapes:
+            lib = os.path.join(_variant_dir(cache, cb, mb), "libdisco_b200.so")
             r = subprocess.run([sys.executable, "-m", "disco_b200.autotune", "_child", lib, workload,
                                 str(prec), str(reps)], capture_output=True, text=True,
                                cwd=native.REPO, timeout=900)
             if r.returncode != 0:
                 sys.stderr.write(r.stderr[-2000:])
-                raise RuntimeError("autotune child failed for mb %d (%s)" % (mb, pname))
-            res[pname][mb] = json.loads(r.stdout.strip().splitlines()[-1])
+                raise RuntimeError("autotune child failed for cb %d mb %d (%s)" % (cb, mb, pname))
+            res[pname][(cb, mb)] = json.loads(r.stdout.strip().splitlines()[-1])
     return res
 
 
 def choose(res):
-    """Fastest candidate per (precision, kernel)."""
-    best = {}
+    """The block size, then the fastest MB per (precision, kernel) at it:
+    {"cb": CB, "fp64": {kernel: MB}, "mixed": {...}}."""
+    def best_total(table, cb):
+        tot = 0.0
+        for k in MACROS:
+            cand = [t[k] for (c, _), t in table.items() if c == cb and k in t]
+            tot += min(cand) if cand else 0.0
+        return tot
+    ref = res.get("fp64") or next(iter(res.values()))
+    cbs = sorted({c for c, _ in ref})
+    cb = min(cbs, key=lambda c: best_total(ref, c))
+    best = {"cb": cb}
     for pname, table in res.items():
         best[pname] = {}
         for k in MACROS:
-            cand = [(t[k], mb) for mb, t in table.items() if k in t]
+            cand = [(t[k], mb) for (c, mb), t in table.items() if c == cb and k in t]
             if cand:
                 best[pname][k] = min(cand)[1]
     return best
 
 
 def write_header(res, best, workload, path=TUNED):
+    cb = best["cb"]
     lines = ["/*",
-             " * Per-kernel occupancy targets (resident blocks per SM of 128 threads; the",
-             " * register budget is 65536 / (128 * MB)), written by disco_b200/autotune.py",
-             " * from CUDA-event kernel times of one step of the %s workload" % workload,
-             " * (median of the instrumented steps, ms per step):", " *"]
+             " * Launch shapes of the step kernels: CB threads per block and, per kernel,",
+             " * the resident blocks per SM MB (register budget 65536 / (CB * MB)), written",
+             " * by disco_b200/autotune.py from CUDA-event kernel times of one step of the",
+             " * %s workload (median of the instrumented steps, ms per step;" % workload,
+             " * columns CB/MB):", " *"]
     for pname, table in res.items():
-        mbs = sorted(table)
-        lines.append(" *   %-6s %-10s %s" % (pname, "kernel", " ".join("%8s" % ("MB %d" % m) for m in mbs)))
+        shapes = sorted(table)
+        lines.append(" *   %-6s %-10s %s" % (pname, "kernel", " ".join("%8s" % ("%d/%d" % s) for s in shapes)))
         for k in MACROS:
-            row = " ".join("%8.4f" % table[m].get(k, float("nan")) for m in mbs)
+            row = " ".join("%8.4f" % table[s].get(k, float("nan")) for s in shapes)
             lines.append(" *   %-6s %-10s %s   -> %d" % ("", k, row, best[pname].get(k, 0)))
-    lines += [" *", " * Values given with -D on the command line win.", " */", "#pragma once"]
+    lines += [" *", " * Values given with -D on the command line win.", " */", "#pragma once",
+              "#ifndef CB", "#define CB %d" % cb, "#endif", "#ifndef FB", "#define FB %d" % cb, "#endif"]
     for pname, cond in (("mixed", "#ifdef DISCO_MIXED_TU"), ("fp64", "#else")):
         lines.append(cond)
         for k, m in MACROS.items():
@@ -158,7 +182,9 @@ def main(argv=None):
     sub = ap.add_subparsers(dest="cmd", required=True)
     b = sub.add_parser("build")
     b.add_argument("--cache", default=DEFAULT_CACHE)
-    b.add_argument("--mb", default=",".join(str(m) for m in DEFAULT_MB))
+    b.add_argument("--mb", default=",".join(str(m) for m in DEFAULT_MB),
+                   help="occupancy targets for 128-thread blocks (scaled for other sizes)")
+    b.add_argument("--cb", default="128", help="block sizes, e.g. 64,128,256")
     m = sub.add_parser("measure")
     m.add_argument("--cache", default=DEFAULT_CACHE)
     m.add_argument("--workload", default="ragged64", choices=["ragged64", "ragged8", "config0"])
@@ -170,14 +196,17 @@ def main(argv=None):
     c.add_argument("reps", type=int)
     a = ap.parse_args(argv)
     if a.cmd == "build":
-        for mb, lib in build_variants(a.cache, [int(x) for x in a.mb.split(",")]).items():
-            print(mb, lib)
+        for shape, lib in build_variants(a.cache, [int(x) for x in a.mb.split(",")],
+                                         [int(x) for x in a.cb.split(",")]).items():
+            print(shape, lib)
     elif a.cmd == "measure":
         res = measure(a.cache, a.workload, a.reps)
         best = choose(res)
         if a.json:
             with open(a.json, "w") as f:
-                json.dump({"workload": a.workload, "res": res, "best": best}, f, indent=1)
+                json.dump({"workload": a.workload, "best": best,
+                           "res": {p: {"%d/%d" % s: t for s, t in tab.items()} for p, tab in res.items()}},
+                          f, indent=1)
         print(json.dumps(best))
         if a.write:
             write_header(res, best, a.workload)

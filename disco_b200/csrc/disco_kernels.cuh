@@ -33,12 +33,21 @@
 #pragma once
 #include "disco_device.cuh"
 
+#include "tuned.h"
+
 namespace disco {
 
+/* threads per block of the cell kernels (one block per annulus chunk of CB
+ * cells) and of the face kernels (FB faces of one track); tuned.h may set
+ * them, the host's block tables and every launch follow */
+#ifndef CB
 #define CB 128
-#define FB 128
+#endif
+#ifndef FB
+#define FB CB
+#endif
 /* Resident blocks per SM asked of the compiler for the step kernels (the
- * register budget per thread follows: 65536 / (128 * MB)).  The kernels
+ * register budget per thread follows: 65536 / (CB * MB)).  The kernels
  * are latency-bound, so warps in flight matter more than the spills the
  * tighter budget costs: on ragged64 the hydro step went from 7.26 to
  * 5.41 ms (FP64) and 5.60 to 4.57 ms (mixed) with MB 8-12 against the
@@ -47,7 +56,6 @@ namespace disco {
  * (DISCO_MIXED_TU marks the FP32 translation unit); a -DMB_x on the
  * command line overrides them, and the defaults below fill the rest.  The
  * MHD instantiations (HLLD needs about 160 registers) keep MB_MHD. */
-#include "tuned.h"
 #ifndef MB_FACES
 #define MB_FACES 1
 #endif

@@ -9,17 +9,22 @@ from disco_b200 import build as native
 
 
 def _table():
-    # ms per step per kernel for three candidates; each kernel has its own best
-    return {"fp64": {4: {"k_begin": 1.0, "k_faces": 2.0, "k_update": 1.5},
-                     8: {"k_begin": 0.8, "k_faces": 2.1, "k_update": 1.2},
-                     16: {"k_begin": 0.9, "k_faces": 1.7, "k_update": 2.0}},
-            "mixed": {4: {"k_begin": 0.7, "k_faces": 1.0, "k_update": 1.0},
-                      8: {"k_begin": 0.9, "k_faces": 0.9, "k_update": 1.1},
-                      16: {"k_begin": 0.8, "k_faces": 1.2, "k_update": 0.9}}}
+    # ms per step per kernel for (block size, MB) candidates; each kernel has
+    # its own best; 256-thread blocks are slower in total
+    t = {"fp64": {(128, 4): {"k_begin": 1.0, "k_faces": 2.0, "k_update": 1.5},
+                  (128, 8): {"k_begin": 0.8, "k_faces": 2.1, "k_update": 1.2},
+                  (128, 16): {"k_begin": 0.9, "k_faces": 1.7, "k_update": 2.0},
+                  (256, 4): {"k_begin": 0.7, "k_faces": 2.5, "k_update": 1.6}},
+         "mixed": {(128, 4): {"k_begin": 0.7, "k_faces": 1.0, "k_update": 1.0},
+                   (128, 8): {"k_begin": 0.9, "k_faces": 0.9, "k_update": 1.1},
+                   (128, 16): {"k_begin": 0.8, "k_faces": 1.2, "k_update": 0.9},
+                   (256, 4): {"k_begin": 0.1, "k_faces": 0.1, "k_update": 0.1}}}
+    return t
 
 
 def test_choose_per_kernel_and_precision():
     best = at.choose(_table())
+    assert best["cb"] == 128                      # decided by the FP64 step
     assert best["fp64"] == {"k_begin": 8, "k_faces": 16, "k_update": 8}
     assert best["mixed"] == {"k_begin": 4, "k_faces": 8, "k_update": 16}
 
@@ -36,6 +41,7 @@ def test_header_defines_each_precision(tmp_path):
         out = subprocess.run(cmd, capture_output=True, text=True, check=True).stdout
         got = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define (MB_\w+) (\d+)", out)}
         assert got == expect, (tu, got)
+        assert re.search(r"#define CB 128", out) and re.search(r"#define FB 128", out)
     assert "-> 16" in src
 
 
@@ -43,4 +49,5 @@ def test_committed_header_covers_every_tuned_kernel():
     src = open(at.TUNED).read()
     for macro in at.MACROS.values():
         assert src.count("#define %s " % macro) == 2, macro   # one per precision
+    assert src.count("#define CB ") == 1
     assert os.path.dirname(at.TUNED) == os.path.join(native.HERE, "csrc")
