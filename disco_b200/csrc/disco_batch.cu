@@ -225,6 +225,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
          b->ann_blk0.push_back((int)b->cblk.size());
          int nb = 0;
          for( int i0=0 ; i0<np ; i0+=CB ){ b->cblk.push_back(make_int2(ann, i0)); ++nb; }
+         for( int i0=0 ; i0<np ; i0+=CB-1 ) b->ublk.push_back(make_int2(ann, i0));
          b->ann_nblk.push_back(nb);
          if( j >= D.NgRa && j < nr-D.NgRb && k >= D.NgZa && k < nz-D.NgZb ) nreal += np;
          cell += np; ++ann;
@@ -354,7 +355,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.tr_flux = dupload(b, b->tr_flux); v.tr_j = dupload(b, b->tr_j); v.tr_k = dupload(b, b->tr_k);
    v.tr_dxL = dupload(b, b->tr_dxL); v.tr_dxR = dupload(b, b->tr_dxR);
    v.tr_dim = dupload(b, b->tr_dim);
-   v.cblk = dupload(b, b->cblk); v.fblk = dupload(b, b->fblk);
+   v.cblk = dupload(b, b->cblk); v.fblk = dupload(b, b->fblk); v.ublk = dupload(b, b->ublk);
    v.rj = dupload(b, b->rj); v.zk = dupload(b, b->zk);
    v.dp = dupload(b, b->dparams);
    v.ds = dupload(b, dstate);

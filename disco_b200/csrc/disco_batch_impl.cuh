@@ -35,6 +35,7 @@ struct disco_batch {
    std::vector<unsigned char> tr_dim;
    std::vector<double> tr_dxL, tr_dxR;
    std::vector<int2> cblk, fblk;
+   std::vector<int2> ublk;              /* k_update's blocks: chunks of CB-1 cells */
    std::vector<int> ann_blk0, ann_nblk;
    std::vector<double> rj, zk;
    std::vector<DiskParams> dparams;
@@ -133,7 +134,7 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    if( b->any_3d ){ k_grad<Q,2,R><<<ncb, CB, 0, s>>>(v);              mark(b, "k_gradz"); }
    k_flux_t<Q,NC,1,R><<<nfb, FB, 0, s>>>(v);                          mark(b, "k_flux_r");
    if( b->any_3d ){ k_flux_t<Q,NC,2,R><<<nfb, FB, 0, s>>>(v);         mark(b, "k_flux_z"); }
-   k_update<Q,NC,R><<<ncb, CB, 0, s>>>(v, first);                     mark(b, "k_update");
+   k_update<Q,NC,R><<<(unsigned)b->ublk.size(), CB, 0, s>>>(v, first); mark(b, "k_update");
    if constexpr ( NC == 8 ){
       if( b->ct ){                  /* onestep.c:140-146 and 160-167 */
          k_ct_edges<R><<<ncb, CB, 0, s>>>(v);                           mark(b, "k_ct_edges");

@@ -89,6 +89,7 @@ struct ViewT {
    const unsigned char *tr_dim;      /* 1: r-track (j,k)-(j+1,k); 2: z-track (j,k)-(j,k+1) */
    const double *tr_dxL, *tr_dxR;
    const int2 *cblk, *fblk;
+   const int2 *ublk;                  /* k_update: (annulus, first cell) of chunks of CB-1 cells */
    const double *rj, *zk;
    const DiskParams *dp;
    DiskState *ds;
@@ -665,8 +666,12 @@ __device__ __forceinline__ void phi_face_flux(const ViewT<R> &v, const DiskParam
  * the saved re-read of cons: 1.73 against 1.69 ms per ragged64 step). */
 template<int Q, int NC, class R>
 __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT<R> v, int first){
-   __shared__ R sG[Q][CB+1];      /* sG[q][t+1]: face (i, i+1); sG[q][0]: face (i0-1, i0) */
-   int2 b = v.cblk[blockIdx.x];
+   /* The block updates CB-1 cells i0 .. i0+CB-2 and its thread t solves the
+    * phi face (i0+t-1, i0+t) into sG[.][t]: every thread one face, the
+    * chunk's two outer faces included (the left one is also the previous
+    * chunk's last). */
+   __shared__ R sG[Q][CB];
+   int2 b = v.ublk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
    const int N = v.Ncell;
@@ -693,31 +698,27 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
       double dA = (rj[j]-rj[j-1])*(zk[k]-zk[k-1]);       /* get_dA(.,.,0) */
       double dAdtp = dA*(v.ds[d].dt*v.dtfac);
       double rc = centroid_r(rj[j], rj[j-1]);
-      if( i < np ){
+      if( i <= np ){                 /* face (i-1, i): left cell cprev, right cell c (mod np) */
          R G[Q];
-         int cn = c0 + (i < np-1 ? i+1 : 0);
+         int cr = i < np ? c : c0;
          if( ctE ){                 /* flux_to_E dim 0, Hydro/mhd.c:298-303 */
             R eb[5];
-            phi_face_flux<Q,NC,R>(v, P, a, c, cn, rc, dAdtp, G, eb);
-            const R irfac = (R)(1.0/(1.0/rc));
-            v.pE[c] = eb[0]*irfac;
-            v.pB[c] = eb[2]*irfac;
-            if( v.ct == 2 ){ v.pEr[c] = -eb[3]; v.pBz[c] = eb[4]; }
+            phi_face_flux<Q,NC,R>(v, P, a, cprev, cr, rc, dAdtp, G, eb);
+            if( threadIdx.x > 0 ){  /* stored once: t = 0's face is the previous chunk's */
+               const R irfac = (R)(1.0/(1.0/rc));
+               v.pE[cprev] = eb[0]*irfac;
+               v.pB[cprev] = eb[2]*irfac;
+               if( v.ct == 2 ){ v.pEr[cprev] = -eb[3]; v.pBz[cprev] = eb[4]; }
+            }
          }else{
-            phi_face_flux<Q,NC,R>(v, P, a, c, cn, rc, dAdtp, G);
+            phi_face_flux<Q,NC,R>(v, P, a, cprev, cr, rc, dAdtp, G);
          }
 #pragma unroll
-         for( int q=0 ; q<Q ; ++q ) sG[q][threadIdx.x+1] = G[q];
-      }
-      if( threadIdx.x == 0 && real ){
-         R G[Q];
-         phi_face_flux<Q,NC,R>(v, P, a, cprev, c, rc, dAdtp, G);
-#pragma unroll
-         for( int q=0 ; q<Q ; ++q ) sG[q][0] = G[q];
+         for( int q=0 ; q<Q ; ++q ) sG[q][threadIdx.x] = G[q];
       }
       __syncthreads();
    }
-   if( i >= np ) return;
+   if( threadIdx.x == CB-1 || i >= np ) return;
    int err = 0;
    double piph = v.piph[c], dphi = v.dphi[c];
    if( real ){
