@@ -33,6 +33,7 @@ struct Planet {
    double r, phi, M, omega, vr;
    double RK_r, RK_phi, RK_M, RK_omega, RK_vr;
    double eps;
+   double cphi, sphi;    /* cos(phi), sin(phi), set on the device whenever phi changes */
    int type;
    int pad;
 };
@@ -682,11 +683,13 @@ __device__ __forceinline__ double fgrav(double M, double r, double eps, int type
    if( type == 0 ){                                   /* PLPOINTMASS, planet.c:58-62 */
       /* M*pow(r,n-1.)/pow( pow(r,n) + pow(eps,n) ,1.+1./n) with n = PHI_ORDER
        * = 2 (a global in planet.c, so the reference calls pow at run time):
-       * pow(r,1.) is r exactly, and pow(x,2.) is written x*x, which glibc's
-       * pow(x,2.) equals except for a last-bit difference in about 1e-3 of
-       * arguments -- the same order as CUDA's pow against glibc's, which
-       * the parity tolerance already covers.  Three pow calls fewer per cell. */
-      return( M*r/pow( r*r + eps*eps , 1.5) );
+       * pow(r,1.) is r exactly, pow(x,2.) is written x*x (glibc's pow(x,2.)
+       * equals it except for a last-bit difference in about 1e-3 of
+       * arguments) and pow(x,1.5) is x*sqrt(x) (within about an ulp of
+       * glibc's correctly rounded pow) -- differences of the order of CUDA's
+       * pow against glibc's, which the parity tolerance covers. */
+      double x = r*r + eps*eps;
+      return( M*r/(x*sqrt(x)) );
    }
    return 0.0;
 }
@@ -694,12 +697,14 @@ __device__ __forceinline__ double fgrav(double M, double r, double eps, int type
 __device__ __forceinline__ void planetary_force(int grav2D, const Planet &pl, double r,
                                                 double phi, double z, double *fr,
                                                 double *fp, double *fz){
-   double rp = pl.r, pp = pl.phi;
+   double rp = pl.r;
+   double sinp, cosp;
+   sincos(phi, &sinp, &cosp);
+   double cpp = pl.cphi, spp = pl.sphi;             /* cos, sin of the planet's phi */
    if( grav2D == 1 ) z = 0.0;
-   else if( grav2D == 2 ){ rp = r; pp = phi; z = 1.0; }
-   double cosp = cos(phi), sinp = sin(phi);
-   double dx = r*cosp-rp*cos(pp);
-   double dy = r*sinp-rp*sin(pp);
+   else if( grav2D == 2 ){ rp = r; cpp = cosp; spp = sinp; z = 1.0; }
+   double dx = r*cosp-rp*cpp;
+   double dy = r*sinp-rp*spp;
    double script_r = sqrt(dx*dx+dy*dy+z*z);
    double script_r_perp = sqrt(dx*dx+dy*dy);
    double f1 = -fgrav( pl.M , script_r , pl.eps , pl.type );

@@ -1233,6 +1233,7 @@ __global__ void k_disk_begin(ViewT<R> v, int ndisk, int use_next){
    for( int p=0 ; p<P.npl ; ++p ){
       Planet &pl = S.pl[p];
       pl.RK_r = pl.r; pl.RK_phi = pl.phi; pl.RK_M = pl.M; pl.RK_omega = pl.omega; pl.RK_vr = pl.vr;
+      sincos(pl.phi, &pl.sphi, &pl.cphi);
    }
    double dt0 = P.maxDT / P.CFL;
    if( dt0 <= 0.0 ) dt0 = 1.0e100;
@@ -1267,6 +1268,7 @@ __global__ void k_disk_mid(ViewT<R> v, int ndisk, double RK, int first, int adva
       while( phi > P.Pmax && n++ < WRAP_CAP ){ phi -= P.Pmax; pl.RK_phi -= P.Pmax; }
       while( phi < 0.0 && n++ < WRAP_CAP ){ phi += P.Pmax; pl.RK_phi += P.Pmax; }
       pl.phi = phi;
+      sincos(phi, &pl.sphi, &pl.cphi);
    }
    if( advance_t ) S.t += dt;
 }
