@@ -166,21 +166,33 @@ __device__ __forceinline__ void acc(double &s, double &cc, double x){
  * Every substep: adjust_RK_cons (misc.c:226-244) and plm_phi (plm.c:15-51). */
 template<int Q, int NC, class R>
 __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_BEGIN) k_begin(ViewT<R> v, double RK, int first){
+   /* the chunk's prims and dphi staged once, with one neighbour cell on each
+    * side (slot t+1 = cell i0+t) */
+   __shared__ R sp[Q][CB+2];
+   __shared__ double sd[CB+2];
    int2 b = v.cblk[blockIdx.x];
-   int a = b.x, i = b.y + threadIdx.x;
+   int a = b.x, i0 = b.y, t = threadIdx.x, i = i0 + t;
    int np = v.ann_np[a];
-   if( i >= np ) return;
    const int N = v.Ncell;
    int c0 = v.ann_off[a], c = c0 + i;
-   int cm = c0 + (i == 0 ? np-1 : i-1);
-   int cp = c0 + (i+1 == np ? 0 : i+1);
+   int nact = np - i0 < CB ? np - i0 : CB;
+   auto stage = [&](int slot, int cell){
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) sp[q][slot] = v.prim[q*N + cell];
+      sd[slot] = v.dphi[cell];
+   };
+   if( t < nact ) stage(t+1, c);
+   if( t == 0 ) stage(0, c0 + (i0 == 0 ? np-1 : i0-1));
+   if( t == nact-1 ) stage(nact+1, c0 + (i0+nact == np ? 0 : i0+nact));
+   __syncthreads();
+   if( t >= nact ) return;
    int d = v.ann_disk[a];
    const DiskParams &P = v.dp[d];
 
    R pC[Q], pL[Q], pR[Q];
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ){
-      pC[q] = v.prim[q*N + c]; pL[q] = v.prim[q*N + cm]; pR[q] = v.prim[q*N + cp];
+      pC[q] = sp[q][t+1]; pL[q] = sp[q][t]; pR[q] = sp[q][t+2];
    }
    if( first ){
       double w = 0.0;
@@ -227,7 +239,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_BEGIN) k_begin(ViewT<R
          }
       }
    }
-   const R dpL = (R)v.dphi[cm], dpC = (R)v.dphi[c], dpR = (R)v.dphi[cp];
+   const R dpL = (R)sd[t], dpC = (R)sd[t+1], dpR = (R)sd[t+2];
    const R PLM = (R)P.PLM;
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ){
@@ -655,6 +667,23 @@ __device__ __forceinline__ void phi_face_flux(const ViewT<R> &v, const DiskParam
    solve_riemann<Q,NC,0,R>(P, primL, primR, (R)r, (R)v.ann_om[a], (R)w, (R)dAdt, G, eb);
 }
 
+/* the same from the two edge states already extrapolated (primL: cell cL's
+ * right edge, primR: the next cell's left edge); primR is overwritten */
+template<int Q, int NC, class R>
+__device__ __forceinline__ void phi_face_flux_states(const ViewT<R> &v, const DiskParams &P, int a,
+                                                     int cL, double r, double dAdt, const R *eL,
+                                                     R *primR, R *G, R *eb = nullptr){
+   R primL[Q];
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ) primL[q] = eL[q];
+   if constexpr ( NC == 8 ){                     /* B_phi averaged, riemann.c:54-58 */
+      R Bp = R(.5)*(primL[BPP]+primR[BPP]);
+      primL[BPP] = Bp; primR[BPP] = Bp;
+   }
+   double w = r*v.wiph[cL];
+   solve_riemann<Q,NC,0,R>(P, primL, primR, (R)r, (R)v.ann_om[a], (R)w, (R)dAdt, G, eb);
+}
+
 /* ------------------------------------------------------------------ k_update
  * The flux gather and sources, per cell, in the reference's order:
  *   flux gather  riemann.c:312-315 applied as phi_flux then trans_flux do
@@ -671,6 +700,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
     * chunk's two outer faces included (the left one is also the previous
     * chunk's last). */
    __shared__ R sG[Q][CB];
+   __shared__ R sW[Q][CB+1];      /* sW[.][s]: left-edge state of cell i0+s-1 */
    int2 b = v.ublk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -698,12 +728,39 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
       double dA = (rj[j]-rj[j-1])*(zk[k]-zk[k-1]);       /* get_dA(.,.,0) */
       double dAdtp = dA*(v.ds[d].dt*v.dtfac);
       double rc = centroid_r(rj[j], rj[j-1]);
+      /* riemann_phi's edge states (riemann.c:45-50): thread t extrapolates
+       * cell i-1 to both of its phi edges; the left-edge state goes to its
+       * neighbour through shared memory (the last thread also does cell i) */
+      R eR[Q];
+      const int tt = threadIdx.x;
+      auto edges = [&](int cell, R *right, int slot){
+         R dph = (R)v.dphi[cell];
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ){
+            R pq = v.prim[q*N + cell], gq = v.gradp[q*N + cell];
+            if( right ) right[q] = pq + R(.5)*gq*dph;
+            sW[q][slot] = pq - R(.5)*gq*dph;
+         }
+      };
+      /* slot s holds cell i0+s-1 (periodic); slots 0 .. smax are read */
+      const int i0 = b.y;
+      const int smax = (np - i0 < CB-1 ? np - i0 : CB-1) + 1;
+      auto cell_of = [&](int sl){
+         int x = i0 + sl - 1;
+         if( x < 0 ) x += np; else if( x >= np ) x -= np;
+         return c0 + x;
+      };
+      if( tt <= smax ) edges(cell_of(tt), eR, tt);
+      if( tt == CB-1 && CB <= smax ) edges(cell_of(CB), nullptr, CB);
+      __syncthreads();
       if( i <= np ){                 /* face (i-1, i): left cell cprev, right cell c (mod np) */
          R G[Q];
-         int cr = i < np ? c : c0;
+         R primR[Q];
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ) primR[q] = sW[q][tt+1];
          if( ctE ){                 /* flux_to_E dim 0, Hydro/mhd.c:298-303 */
             R eb[5];
-            phi_face_flux<Q,NC,R>(v, P, a, cprev, cr, rc, dAdtp, G, eb);
+            phi_face_flux_states<Q,NC,R>(v, P, a, cprev, rc, dAdtp, eR, primR, G, eb);
             if( threadIdx.x > 0 ){  /* stored once: t = 0's face is the previous chunk's */
                const R irfac = (R)(1.0/(1.0/rc));
                v.pE[cprev] = eb[0]*irfac;
@@ -711,7 +768,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
                if( v.ct == 2 ){ v.pEr[cprev] = -eb[3]; v.pBz[cprev] = eb[4]; }
             }
          }else{
-            phi_face_flux<Q,NC,R>(v, P, a, cprev, cr, rc, dAdtp, G);
+            phi_face_flux_states<Q,NC,R>(v, P, a, cprev, rc, dAdtp, eR, primR, G);
          }
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) sG[q][threadIdx.x] = G[q];
