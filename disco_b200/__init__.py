@@ -101,6 +101,7 @@ def library():
         "disco_batch_mindt": (_I, [_P, _D]),
         "disco_batch_timestep": (_I, [_P, _D]),
         "disco_batch_run": (_I, [_P, _I]),
+        "disco_batch_report": (_I, [_P, _I, _D]),
         "disco_batch_time": (_I, [_P, _I, _D, _IP]),
         "disco_batch_get_faces": (_I, [_P, _I, _I, _IP, _IP, _IP, _IP, _IP, _D]),
         "disco_batch_get_diagnostics": (_I, [_P, _I, _D, _IP, _D]),
@@ -344,6 +345,16 @@ class Batch:
         out = dict(fIndex=fI, iL=iL[:n], iR=iR[:n], LRtype=LR[:n])
         if geom:
             out["geom"] = g[:n]
+        return out
+
+    REPORT_FIELDS = ("t", "Torque", "Power", "Fr", "rho_min", "rhoavg_min", "PsiR", "PsiI", "Mass",
+                     "Mdot", "S_R", "L1_rho", "L1_isen", "L1_B", "Br2", "aM", "bM")
+
+    def report(self, disk=0):
+        """report() on the device: the 17 numbers of the disk's report.dat line
+        (names in REPORT_FIELDS)."""
+        out = np.zeros(17)
+        _check(library().disco_batch_report(self.h, disk, dptr(out)), "disco_batch_report")
         return out
 
     def diagnostics(self, disk=0):

@@ -421,6 +421,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    {
       int nx = ann > v.Ntr ? ann : v.Ntr;
       k_precompute<<<nblk(nx, 128), 128, 0, b->stream>>>(v);
+      k_planet_trig<double><<<nblk(ndisk, 64), 64, 0, b->stream>>>(v, ndisk);
    }
    if( cudaDeviceSynchronize() != cudaSuccess ){ disco_batch_destroy(b); return DISCO_ERR_CUDA; }
    *out = b;
@@ -434,6 +435,8 @@ extern "C" void disco_batch_destroy(disco_batch *b){
    if( b->own_stream ) cudaStreamDestroy(b->own_stream);
    for( void *p : b->allocs ) if( p ) cudaFree(p);
    if( b->d_stage ) cudaFree(b->d_stage);
+   if( b->d_rpart ) cudaFree(b->d_rpart);
+   if( b->d_rout ) cudaFree(b->d_rout);
    delete b;
 }
 
@@ -654,6 +657,22 @@ extern "C" int disco_batch_time(const disco_batch *b, int disk, double *t, int *
    if( t ) *t = st.t;
    if( count ) *count = st.count_steps;
    return DISCO_OK;
+}
+
+extern "C" int disco_batch_report(disco_batch *b, int disk, double *out){
+   if( !b || !out || disk < 0 || disk >= b->ndisk ) return DISCO_ERR_ARG;
+   if( !b->have_cells ) return DISCO_ERR_STATE;
+   CK(cudaSetDevice(b->device));
+   if( !b->d_rpart ){
+      if( cudaMalloc(&b->d_rpart, b->cblk.size()*RP_N*sizeof(double)) != cudaSuccess ||
+          cudaMalloc(&b->d_rout, (size_t)b->ndisk*17*sizeof(double)) != cudaSuccess )
+         return DISCO_ERR_CUDA;
+   }
+   if( b->prec == DISCO_PREC_MIXED ) mixed_launch_report(b);
+   else launch_report_t(b, b->vd);
+   CK(cudaGetLastError());
+   CK(xfer(b, out, b->d_rout + (size_t)disk*17, 17*sizeof(double), cudaMemcpyDeviceToHost));
+   return read_err(b);
 }
 
 extern "C" int disco_batch_get_faces(disco_batch *b, int disk, int dim, int *nfaces,

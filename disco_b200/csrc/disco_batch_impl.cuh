@@ -48,6 +48,7 @@ struct disco_batch {
    int *d_ann_blk0, *d_ann_nblk;
    double *d_Qrz;
    double *d_stage;          /* Q x ncell FP64, set/get_cells staging (lazy) */
+   double *d_rpart, *d_rout; /* report partials per cell block, lines per disk (lazy) */
    int *d_err;
    cudaStream_t stream;
    cudaStream_t own_stream;
@@ -198,7 +199,18 @@ static void launch_prim2cons_t(disco_batch *b, const ViewT<R> &v){
    else k_prim2cons<6,5,R><<<ncb, CB, 0, b->stream>>>(v);
 }
 
+/* report() (report.c:7-202) on the device: per-block partials, then per-disk lines */
+template<class R>
+static void launch_report_t(disco_batch *b, const ViewT<R> &v){
+   unsigned ncb = (unsigned)b->cblk.size();
+   if( b->NC == 8 ) k_report_part<9,8,R><<<ncb, CB, 0, b->stream>>>(v, b->d_rpart);
+   else k_report_part<6,5,R><<<ncb, CB, 0, b->stream>>>(v, b->d_rpart);
+   k_report_finish<R><<<nblk(b->ndisk, 64), 64, 0, b->stream>>>(v, b->d_rpart, b->d_ann_blk0,
+                                                                b->d_ann_nblk, b->d_rout, b->ndisk);
+}
+
 /* FP32 mixed-form launches, defined in disco_batch_mixed.cu */
+void mixed_launch_report(disco_batch *b);
 void mixed_launch_mindt(disco_batch *b);
 void mixed_launch_setup(disco_batch *b);
 void mixed_launch_step(disco_batch *b, int use_next);

@@ -9,6 +9,7 @@
 void mixed_launch_mindt(disco_batch *b){ launch_mindt_t(b, b->vf); }
 void mixed_launch_setup(disco_batch *b){ launch_setup_t(b, b->vf); }
 void mixed_launch_step(disco_batch *b, int use_next){ launch_step_t(b, b->vf, use_next); }
+void mixed_launch_report(disco_batch *b){ launch_report_t(b, b->vf); }
 void mixed_launch_prim2cons(disco_batch *b){
    launch_prim2cons_t(b, b->vf);
 }

@@ -693,10 +693,10 @@ __device__ __forceinline__ double fgrav(double M, double r, double eps, int type
    }
    return 0.0;
 }
-/* planetaryForce(), planet.c:99-150, mode 0 */
+/* planetaryForce(), planet.c:99-150, modes 0 and 1 */
 __device__ __forceinline__ void planetary_force(int grav2D, const Planet &pl, double r,
                                                 double phi, double z, double *fr,
-                                                double *fp, double *fz){
+                                                double *fp, double *fz, int mode = 0){
    double rp = pl.r;
    double sinp, cosp;
    sincos(phi, &sinp, &cosp);
@@ -712,6 +712,10 @@ __device__ __forceinline__ void planetary_force(int grav2D, const Planet &pl, do
    double sina = dy/script_r_perp;
    double cosap = cosa*cosp+sina*sinp;
    double sinap = sina*cosp-cosa*sinp;
+   if( mode == 1 ){                    /* components along the planet's direction */
+      cosap = cosa*cpp+sina*spp;
+      sinap = sina*cpp-cosa*spp;
+   }
    if( script_r_perp <= 0.0 ){ cosap = 0.0; sinap = 0.0; }
    double sint = script_r_perp/script_r;
    double cost = z/script_r;

@@ -1297,6 +1297,15 @@ __global__ void k_disk_begin(ViewT<R> v, int ndisk, int use_next){
    S.dtmin = dbits(dt0);
 }
 
+/* cos / sin of the planets' phi at set-up (later kept by k_disk_begin/mid) */
+template<class R>
+__global__ void k_planet_trig(ViewT<R> v, int ndisk){
+   int d = blockIdx.x*blockDim.x + threadIdx.x;
+   if( d >= ndisk ) return;
+   DiskState &S = v.ds[d];
+   for( int p=0 ; p<v.dp[d].npl ; ++p ) sincos(S.pl[p].phi, &S.pl[p].sphi, &S.pl[p].cphi);
+}
+
 /* After substep 1 (onestep.c:163-166, timestep.c:38): planet adjust/move,
  * planet phi wrap (clean_pi, misc.c:27-34), t += dt. */
 template<class R>
@@ -1359,6 +1368,145 @@ __global__ void k_diag_finish(ViewT<R> v, double *Qrz, const int *ann_blk0, cons
       for( int m=0 ; m<6 ; ++m ) s[m] += p[m];
    }
    for( int m=0 ; m<5 ; ++m ) Qrz[(size_t)a*5 + m] += s[m]*dt / s[5];
+}
+
+/* ------------------------------------------------------------------ report
+ * report() (report.c:7-202) as device reductions: per cell block the sums
+ * (and minimum) of its real cells' terms, then per disk the totals, the
+ * annulus-mean minimum and the derived values, so a report needs no copy of
+ * the state.  Sums are block trees in a fixed order, not the reference's
+ * serial loop (agreement to rounding, about 1e-15 relative). */
+enum { RP_PSIR, RP_PSII, RP_L1ISEN, RP_L1RHO, RP_L1P, RP_L1B, RP_BR2, RP_BRBP, RP_B2, RP_PDV,
+       RP_MDOT, RP_VOL, RP_MASS, RP_SR, RP_S0, RP_TORQUE, RP_POWER, RP_TORQUE2, RP_FR,
+       RP_RHOMIN, RP_ARHO, RP_AVOL, RP_N };
+
+template<int Q, int NC, class R>
+__global__ void __launch_bounds__(CB) k_report_part(ViewT<R> v, double *part){
+   __shared__ double s_red[CB/32][RP_N];
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   const int N = v.Ncell;
+   int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+   const DiskState &S = v.ds[d];
+   int j = v.ann_j[a], k = v.ann_k[a];
+   bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
+   double x[RP_N];
+#pragma unroll
+   for( int m=0 ; m<RP_N ; ++m ) x[m] = 0.0;
+   x[RP_RHOMIN] = HUGE_VAL;
+   int err = 0;
+   if( real && i < np ){
+      int c = v.ann_off[a] + i;
+      const double *rj = v.rj + P.rj0 + 1;
+      const double *zk = v.zk + P.zk0 + 1;
+      double phip = v.piph[c], dphi = v.dphi[c];
+      double phi = phip - .5*dphi;
+      double phim = phip - dphi;
+      double dV = dV_of(rj[j], rj[j-1], get_dp(phip, phim, P.Pmax, &err), zk[k], zk[k-1]);
+      double r = centroid_r(rj[j], rj[j-1]);
+      double rho = (double)v.prim[RHO*N + c], Pp = (double)v.prim[PPP*N + c];
+      double vr = (double)v.prim[URR*N + c];
+      double sn, cs;
+      sincos(phi, &sn, &cs);
+      const double rho0 = 1.0;
+      x[RP_PSIR] = rho*dV*cs;
+      x[RP_PSII] = rho*dV*sn;
+      x[RP_L1ISEN] = fabs(Pp/pow(rho, P.gam)-1.)*dV;
+      x[RP_L1RHO] = fabs(rho/rho0-1.)*dV;
+      x[RP_L1P] = fabs(Pp/pow(rho, 5./3.)/0.01-1.)*dV;
+      if constexpr ( NC == 8 ){
+         double Br = (double)v.prim[BRR*N + c], Bp = (double)v.prim[BPP*N + c];
+         double Bz = (double)v.prim[BZZ*N + c];
+         x[RP_L1B] = fabs(Br)*dV;
+         x[RP_BR2] = .5*Br*Br*dV;
+         x[RP_BRBP] = Br*Bp*dV;
+         x[RP_B2] = .5*(Br*Br+Bp*Bp+Bz*Bz)*dV;
+      }
+      x[RP_PDV] = Pp*dV;
+      x[RP_MDOT] = 2.*DISCO_PI*r*rho*dV*vr;
+      x[RP_VOL] = dV;
+      x[RP_RHOMIN] = rho/rho0;
+      x[RP_ARHO] = rho*dV;
+      x[RP_AVOL] = dV;
+      x[RP_MASS] = rho*dV;
+      double r4 = pow(rho, 4.);
+      x[RP_SR] = r4*r*dV;
+      x[RP_S0] = r4*dV;
+      if( P.npl > 1 ){
+         double fr, fp, fz, fp2;
+         const Planet &p1 = S.pl[1];
+         planetary_force(P.grav2D, S.pl[0], r, phi, 0.0, &fr, &fp2, &fz, 1);
+         planetary_force(P.grav2D, p1, r, phi, 0.0, &fr, &fp, &fz, 1);
+         x[RP_TORQUE] = -(rho-1.0)*p1.r*fp*dV;
+         x[RP_POWER] = -(rho-1.0)*( p1.r*p1.omega*fp + p1.vr*fr )*dV;
+         x[RP_TORQUE2] = -(rho-1.0)*p1.r*fp2*dV;
+         x[RP_FR] = -(rho-1.0)*fr*dV;
+      }
+   }
+   raise_err(v, err);
+   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+   for( int m=0 ; m<RP_N ; ++m ){
+      double y = x[m];
+#pragma unroll
+      for( int o=16 ; o>0 ; o>>=1 ){
+         double z = __shfl_down_sync(0xffffffffu, y, o);
+         y = m == RP_RHOMIN ? (z < y ? z : y) : y + z;
+      }
+      if( lane == 0 ) s_red[wid][m] = y;
+   }
+   __syncthreads();
+   if( threadIdx.x == 0 ){
+      for( int m=0 ; m<RP_N ; ++m ){
+         double y = s_red[0][m];
+         for( int w=1 ; w<CB/32 ; ++w ) y = m == RP_RHOMIN ? (s_red[w][m] < y ? s_red[w][m] : y) : y + s_red[w][m];
+         part[(size_t)blockIdx.x*RP_N + m] = y;
+      }
+   }
+}
+
+/* one thread per disk: totals over its blocks in annulus order, the minimum
+ * over radii of the annulus (all z) mean density, the derived values; out =
+ * the 17 numbers of a report.dat line (report.c:189-193) */
+template<class R>
+__global__ void k_report_finish(ViewT<R> v, const double *part, const int *ann_blk0,
+                                const int *ann_nblk, double *out, int ndisk){
+   int d = blockIdx.x*blockDim.x + threadIdx.x;
+   if( d >= ndisk ) return;
+   const DiskParams &P = v.dp[d];
+   const DiskState &S = v.ds[d];
+   double tot[RP_N];
+   for( int m=0 ; m<RP_N ; ++m ) tot[m] = 0.0;
+   tot[RP_RHOMIN] = HUGE_VAL;
+   double rhoavg_min = HUGE_VAL;
+   for( int j=P.NgRa ; j<P.Nr-P.NgRb ; ++j ){
+      double arho = 0.0, avol = 0.0;
+      for( int k=P.NgZa ; k<P.Nz-P.NgZb ; ++k ){
+         int a = P.ann0 + j + P.Nr*k;
+         for( int bb=0 ; bb<ann_nblk[a] ; ++bb ){
+            const double *p = part + (size_t)(ann_blk0[a]+bb)*RP_N;
+            for( int m=0 ; m<RP_RHOMIN ; ++m ) tot[m] += p[m];
+            if( p[RP_RHOMIN] < tot[RP_RHOMIN] ) tot[RP_RHOMIN] = p[RP_RHOMIN];
+            arho += p[RP_ARHO]; avol += p[RP_AVOL];
+         }
+      }
+      double rho_avg = arho/avol;
+      const double rho0 = 1.0;
+      if( rhoavg_min > rho_avg/rho0 ) rhoavg_min = rho_avg/rho0;
+   }
+   double Vol = tot[RP_VOL];
+   double *o = out + (size_t)d*17;
+   o[0] = S.t;
+   o[1] = tot[RP_TORQUE]; o[2] = tot[RP_POWER]; o[3] = tot[RP_FR];
+   o[4] = tot[RP_RHOMIN]; o[5] = rhoavg_min;
+   o[6] = tot[RP_PSIR]; o[7] = tot[RP_PSII]; o[8] = tot[RP_MASS];
+   o[9] = tot[RP_MDOT]/Vol; o[10] = tot[RP_SR]/tot[RP_S0];
+   o[11] = tot[RP_L1RHO]/Vol; o[12] = tot[RP_L1ISEN]/Vol; o[13] = tot[RP_L1B]/Vol;
+   o[14] = tot[RP_BR2];
+   o[15] = tot[RP_BRBP]/tot[RP_PDV];             /* aM */
+   o[16] = tot[RP_PDV]/tot[RP_B2];               /* bM */
 }
 
 /* ------------------------------------------------------------------ setup

@@ -183,6 +183,15 @@ int disco_batch_run(disco_batch *b, int nsteps);
 int disco_batch_time(const disco_batch *b, int disk, double *t, int *count_steps);
 
 /*
+ * report() (report.c:7-202) on the device, without copying the state: the
+ * 17 numbers of the disk's report.dat line, in the reference's order --
+ * t, Torque, Power, Fr, rho_min, rhoavg_min, PsiR, PsiI, Mass, Mdot, S_R,
+ * L1_rho, L1_isen, L1_B, Br2, aM, bM (report.c:189-193).  The sums run as
+ * block trees, so they agree with the reference's serial loop to rounding.
+ */
+int disco_batch_report(disco_batch *b, int disk, double *out);
+
+/*
  * Face list of disk `disk` for dim 1 (r) or 2 (z), built from the current
  * state exactly as setup_faces/buildfaces build it (misc.c:512-532,
  * faces_alt.c:36-179).  fIndex has N_ftracks+1 entries (the reference's

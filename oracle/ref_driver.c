@@ -29,6 +29,7 @@ void timestep( struct domain * , double );
 void boundary_trans( struct domain * , int );
 void exchangeData( struct domain * , int );
 double getmindt( struct domain * );
+void report( struct domain * );
 int read_par_file( struct domain * );
 void setup_faces( struct domain * , int );
 void freeDomain( struct domain * );
@@ -148,6 +149,9 @@ int main(int argc, char *argv[]){
              secs, nsteps, Nreal, secs > 0 ? (double)Nreal*nsteps/secs : 0.0);
       return 0;
    }
+   /* DISCO_REF_REPORT set: one report() of the final state into report.dat
+    * of RUNDIR (the current directory), as possiblyOutput would write it */
+   if( getenv("DISCO_REF_REPORT") ) report( &theDomain );
    if( !dumpdir ) return 0;
    if( disco_gpu_sync_to_host ) disco_gpu_sync_to_host( &theDomain );
 

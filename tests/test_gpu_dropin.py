@@ -19,14 +19,21 @@ from helpers import GOLDEN, rel_l1_cols
 pytestmark = pytest.mark.gpu
 
 
-def _run(binary, par, nsteps):
+def _run(binary, par, nsteps, report=False):
     work = tempfile.mkdtemp(prefix="dropin_")
     try:
         shutil.copy(par, os.path.join(work, "in.par"))
         dump = os.path.join(work, "dump")
+        env = dict(os.environ)
+        if report:
+            env["DISCO_REF_REPORT"] = "1"
         subprocess.run([binary, work, str(nsteps), dump], check=True,
-                       stdout=subprocess.DEVNULL, timeout=600)
-        return pyoracle.load_dump(dump)
+                       stdout=subprocess.DEVNULL, timeout=600, env=env)
+        out = pyoracle.load_dump(dump)
+        if report:
+            with open(os.path.join(work, "report.dat")) as f:
+                out["report"] = np.array([float(x) for x in f.read().split()])
+        return out
     finally:
         shutil.rmtree(work, ignore_errors=True)
 
@@ -96,3 +103,21 @@ def test_dropin_constrained_transport_bitexact(cfg, case, n):
         masks[4] = rj & (k >= m["NgZa"] - 1) & (k <= Nz - m["NgZb"] - 1)
     for s, mk in masks.items():
         assert np.array_equal(a["Phi"][mk, s], b["Phi"][mk, s]), s
+
+
+@pytest.mark.parametrize("cfg,par", [("c0_cm2", "c0_cm2.par"), ("c1_mhd2d_nograv", "c1_ct_rigid.par")])
+def test_dropin_report(cfg, par):
+    """report() through the drop-in: the line computed on the device from the
+    resident state against the reference's report.c on its own state (both
+    printed with %le, 6 significant digits): binary torque terms (cm2) and
+    the magnetic terms (MHD with CT)."""
+    ref, hyb = _binaries(cfg)
+    p = os.path.join(GOLDEN, par)
+    a, b = _run(ref, p, 6, report=True), _run(hyb, p, 6, report=True)
+    ra, rb = a["report"], b["report"]
+    assert len(ra) == len(rb) == 17
+    for n, (x, y) in enumerate(zip(ra, rb)):
+        if np.isinf(x) or np.isinf(y):          # bM = PdV / B2 without a field
+            assert x == y, (n, x, y)
+        else:
+            assert abs(x - y) <= 5e-6 * abs(x) + 1e-300, (n, x, y)
