@@ -25,9 +25,11 @@ LIBPATH = os.path.join(HERE, "libdisco_b200.so")
 TEMPLATES = os.path.join(HERE, "templates")
 
 OK = 0
+PLANET_COLS = 7
 STATUS = {0: "ok", 1: "bad argument", 2: "CUDA runtime error", 3: "module combination not built",
           4: "phi wrap loop hit its cap (non-finite piph)", 5: "non-finite or non-positive dt",
-          6: "no CUDA device", 7: "call out of order", 8: "device consistency check failed"}
+          6: "no CUDA device", 7: "call out of order", 8: "device consistency check failed",
+          9: "file not written, read or parsed"}
 HYDRO = {"euler": 0, "mhd": 1}
 BOUNDARY = {"fixed": 0, "zerograd": 1, "fixed3d": 2}
 PLANETS = {"none": 0, "sun": 1, "cm2": 2, "binary_soft": 3}
@@ -114,6 +116,22 @@ def library():
         "disco_setup_grid": (_I, [C.POINTER(Params), _IP, _IP, _IP, _IP, _D, _D]),
         "disco_setup_phi": (_I, [C.POINTER(Params), _I, _I, _IP, _IP, _D, _D, _IP]),
         "disco_sizeof": (_I, [_I]),
+        "disco_batch_set_time": (_I, [_P, _I, C.c_double]),
+        "disco_batch_get_planets": (_I, [_P, _I, _D, _I, _IP]),
+        "disco_batch_set_planets": (_I, [_P, _I, _D, _I]),
+        "disco_batch_restart_cells": (_I, [_P, _D, _D, _D]),
+        "disco_batch_write_checkpoint": (_I, [_P, _I, C.c_char_p]),
+        "disco_batch_write_ascii": (_I, [_P, _I, C.c_char_p]),
+        "disco_batch_restart": (_I, [_P, C.POINTER(C.c_char_p)]),
+        "disco_npz_create": (_I, [C.c_char_p, C.POINTER(_P)]),
+        "disco_npz_put": (_I, [_P, C.c_char_p, C.c_char_p, _I, C.POINTER(C.c_int64), _P]),
+        "disco_npz_begin": (_I, [_P, C.c_char_p, C.c_char_p, _I, C.POINTER(C.c_int64)]),
+        "disco_npz_append": (_I, [_P, _P, C.c_size_t]),
+        "disco_npz_end": (_I, [_P]),
+        "disco_npz_open": (_I, [C.c_char_p, C.POINTER(_P)]),
+        "disco_npz_info": (_I, [_P, C.c_char_p, C.c_char_p, _IP, C.POINTER(C.c_int64)]),
+        "disco_npz_read": (_I, [_P, C.c_char_p, C.c_uint64, _P, C.c_size_t]),
+        "disco_npz_close": (_I, [_P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -356,6 +374,62 @@ class Batch:
         out = np.zeros(17)
         _check(library().disco_batch_report(self.h, disk, dptr(out)), "disco_batch_report")
         return out
+
+    def set_time(self, t, disk=0):
+        """Set the disk's simulation time (a restart's T)."""
+        _check(library().disco_batch_set_time(self.h, disk, float(t)), "disco_batch_set_time")
+
+    def planets(self, disk=0):
+        """The disk's planets: rows of M, vr, omega, r, phi, eps, type (the
+        checkpoint's Data/Planets columns)."""
+        n = C.c_int()
+        lib = library()
+        _check(lib.disco_batch_get_planets(self.h, disk, None, 0, C.byref(n)), "disco_batch_get_planets")
+        rows = np.zeros((n.value, PLANET_COLS))
+        _check(lib.disco_batch_get_planets(self.h, disk, dptr(rows), n.value, C.byref(n)),
+               "disco_batch_get_planets")
+        return rows
+
+    def set_planets(self, rows, disk=0):
+        rows = np.ascontiguousarray(rows, np.float64)
+        if rows.ndim != 2 or rows.shape[1] != PLANET_COLS:
+            raise ValueError("planet rows must be npl x %d" % PLANET_COLS)
+        _check(library().disco_batch_set_planets(self.h, disk, dptr(rows), rows.shape[0]),
+               "disco_batch_set_planets")
+
+    def restart_cells(self, prim, piph, Phi=None):
+        """setupCells after a restart from prim / Phi / piph of every cell
+        (disco_batch_restart_cells)."""
+        prim = np.ascontiguousarray(prim, np.float64)
+        piph = np.ascontiguousarray(piph, np.float64)
+        Phi = None if Phi is None else np.ascontiguousarray(Phi, np.float64)
+        if prim.shape != (self.ncell, self.q) or piph.shape != (self.ncell,):
+            raise ValueError("restart_cells: prim must be ncell x q, piph ncell")
+        _check(library().disco_batch_restart_cells(self.h, dptr(prim), dptr(Phi), dptr(piph)),
+               "disco_batch_restart_cells")
+
+    def write_checkpoint(self, filestart, disk=0):
+        """Write the disk's checkpoint, <filestart>.npz (the datasets of the
+        reference's HDF5 checkpoint under their paths); returns the path."""
+        _check(library().disco_batch_write_checkpoint(self.h, disk, os.fsencode(filestart)),
+               "disco_batch_write_checkpoint")
+        return os.fsdecode(filestart) + ".npz"
+
+    def write_ascii(self, filestart, disk=0):
+        """Write the ascii output module's <filestart>.dat; returns the path."""
+        _check(library().disco_batch_write_ascii(self.h, disk, os.fsencode(filestart)),
+               "disco_batch_write_ascii")
+        return os.fsdecode(filestart) + ".dat"
+
+    def restart(self, paths):
+        """Restart every disk from its checkpoint file (one path per disk, or
+        one path for a one-disk batch)."""
+        if isinstance(paths, (str, bytes, os.PathLike)):
+            paths = [paths]
+        if len(paths) != len(self.disks):
+            raise ValueError("restart: one checkpoint per disk")
+        arr = (C.c_char_p * len(paths))(*[os.fsencode(p) for p in paths])
+        _check(library().disco_batch_restart(self.h, arr), "disco_batch_restart")
 
     def diagnostics(self, disk=0):
         d = self.disks[disk]

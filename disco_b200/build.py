@@ -79,7 +79,7 @@ def build(force=False, verbose=False):
         _run(["gcc", "-O2", "-fPIC", "-std=gnu11"] + inc + ["-c", src, "-o", obj], verbose)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    _run([nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lm"], verbose)
+    _run([nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lm", "-lz"], verbose)
     os.replace(tmp, LIB)
     return LIB
 

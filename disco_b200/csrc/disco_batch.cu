@@ -59,6 +59,7 @@ extern "C" const char *disco_strerror(int s){
       case DISCO_ERR_NO_DEVICE: return "no CUDA device";
       case DISCO_ERR_STATE: return "call out of order";
       case DISCO_ERR_INTERNAL: return "device consistency check failed";
+      case DISCO_ERR_IO: return "file not written, read or parsed";
    }
    return "unknown status";
 }
@@ -657,6 +658,91 @@ extern "C" int disco_batch_time(const disco_batch *b, int disk, double *t, int *
    if( t ) *t = st.t;
    if( count ) *count = st.count_steps;
    return DISCO_OK;
+}
+
+cudaError_t batch_xfer(const disco_batch *b, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind){
+   return xfer(b, dst, src, bytes, kind);
+}
+
+extern "C" int disco_batch_get_planets(disco_batch *b, int disk, double *rows, int cap, int *npl){
+   if( !b || disk < 0 || disk >= b->ndisk ) return DISCO_ERR_ARG;
+   CK(cudaSetDevice(b->device));
+   int n = b->dparams[disk].npl;
+   if( npl ) *npl = n;
+   if( !rows ) return DISCO_OK;
+   if( cap < n ) return DISCO_ERR_ARG;
+   DiskState st;
+   CK(xfer(b, &st, b->vd.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
+   for( int p=0 ; p<n ; ++p ){                     /* h5out.c:444-455 */
+      const Planet &pl = st.pl[p];
+      double *r = rows + DISCO_PLANET_COLS*p;
+      r[0] = pl.M; r[1] = pl.vr; r[2] = pl.omega; r[3] = pl.r; r[4] = pl.phi; r[5] = pl.eps;
+      r[6] = (double)pl.type;
+   }
+   return DISCO_OK;
+}
+
+extern "C" int disco_batch_set_planets(disco_batch *b, int disk, const double *rows, int npl){
+   if( !b || !rows || disk < 0 || disk >= b->ndisk ) return DISCO_ERR_ARG;
+   if( npl != b->dparams[disk].npl ) return DISCO_ERR_ARG;
+   for( int p=0 ; p<npl ; ++p )
+      if( rows[DISCO_PLANET_COLS*p + 6] != 0.0 ) return DISCO_ERR_UNSUPPORTED;   /* PLPOINTMASS only */
+   CK(cudaSetDevice(b->device));
+   DiskState st;
+   CK(xfer(b, &st, b->vd.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
+   for( int p=0 ; p<npl ; ++p ){                   /* h5in.c:305-317 */
+      Planet &pl = st.pl[p];
+      const double *r = rows + DISCO_PLANET_COLS*p;
+      pl.M = r[0]; pl.vr = r[1]; pl.omega = r[2]; pl.r = r[3]; pl.phi = r[4]; pl.eps = r[5];
+      pl.type = 0;
+   }
+   CK(xfer(b, b->vd.ds + disk, &st, sizeof st, cudaMemcpyHostToDevice));
+   k_planet_trig<double><<<nblk(b->ndisk, 64), 64, 0, b->stream>>>(b->vd, b->ndisk);
+   CK(cudaGetLastError());
+   CK(cudaStreamSynchronize(b->stream));
+   return DISCO_OK;
+}
+
+extern "C" int disco_batch_set_time(disco_batch *b, int disk, double t){
+   if( !b || disk < 0 || disk >= b->ndisk ) return DISCO_ERR_ARG;
+   CK(cudaSetDevice(b->device));
+   DiskState st;
+   CK(xfer(b, &st, b->vd.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
+   st.t = t;
+   CK(xfer(b, b->vd.ds + disk, &st, sizeof st, cudaMemcpyHostToDevice));
+   return DISCO_OK;
+}
+
+extern "C" int disco_batch_restart_cells(disco_batch *b, const double *prim, const double *Phi,
+                                         const double *piph){
+   if( !b || !prim || !piph || (b->ct && !Phi) ) return DISCO_ERR_ARG;
+   CK(cudaSetDevice(b->device));
+   size_t N = b->ncell;
+   int s;
+   if( (s = upload_r(b, b->vd.prim, prim)) ) return s;
+   if( b->ct ){
+      const int F = b->nfs;
+      std::vector<double> t(F*N);
+      for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<F ; ++q ) t[q*N + c] = Phi[F*c + q];
+      CK(xfer(b, b->vd.Phi, t.data(), t.size()*sizeof(double), cudaMemcpyHostToDevice));
+   }
+   CK(xfer(b, b->vd.piph, piph, N*sizeof(double), cudaMemcpyHostToDevice));
+   CK(cudaMemsetAsync(b->vd.topo, 0, sizeof(int), b->stream));
+   /* diagnostics restart from zero (h5in.c:329-333), as does the step count
+    * of a new process (domain.c:99) */
+   std::vector<DiskState> st(b->ndisk);
+   CK(xfer(b, st.data(), b->vd.ds, sizeof(DiskState)*b->ndisk, cudaMemcpyDeviceToHost));
+   for( int d=0 ; d<b->ndisk ; ++d ){ st[d].t_avg = 0.0; st[d].count_steps = 0; }
+   CK(xfer(b, b->vd.ds, st.data(), sizeof(DiskState)*b->ndisk, cudaMemcpyHostToDevice));
+   if( b->nq ) CK(cudaMemsetAsync(b->d_Qrz, 0, sizeof(double)*5*b->ann_np.size(), b->stream));
+   if( b->prec == DISCO_PREC_MIXED ) mixed_launch_restart(b);
+   else launch_restart_t(b, b->vd);
+   CK(cudaGetLastError());
+   s = launch_mindt(b);
+   if( s ) return s;
+   CK(cudaStreamSynchronize(b->stream));
+   b->have_cells = 1;
+   return read_err(b);
 }
 
 extern "C" int disco_batch_report(disco_batch *b, int disk, double *out){

@@ -117,6 +117,16 @@ static void launch_setup_qt(disco_batch *b, const ViewT<R> &v){
    launch_zerograd<Q,R>(b, v);                   /* main.c:53-62 */
 }
 
+/* setupCells with restart_flag set, then main.c's boundaries (main.c:53-62) */
+template<int Q, int NC, class R>
+static void launch_restart_qt(disco_batch *b, const ViewT<R> &v){
+   unsigned ncb = (unsigned)b->cblk.size();
+   k_restart<Q,NC,R><<<ncb, CB, 0, b->stream>>>(v, b->bc_fixed);
+   k_wcell<Q,R><<<ncb, CB, 0, b->stream>>>(v);
+   if( b->any_mm3 ) k_wmean<R><<<nblk(v.Nann, WM_WARPS), 32*WM_WARPS, 0, b->stream>>>(v, 0);
+   launch_zerograd<Q,R>(b, v);
+}
+
 /* One substep of onestep() (onestep.c:84-229). */
 template<int Q, int NC, class R>
 static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int last, double dtfac){
@@ -189,6 +199,10 @@ static void launch_setup_t(disco_batch *b, const ViewT<R> &v){
    if( b->NC == 8 ) launch_setup_qt<9,8,R>(b, v); else launch_setup_qt<6,5,R>(b, v);
 }
 template<class R>
+static void launch_restart_t(disco_batch *b, const ViewT<R> &v){
+   if( b->NC == 8 ) launch_restart_qt<9,8,R>(b, v); else launch_restart_qt<6,5,R>(b, v);
+}
+template<class R>
 static void launch_step_t(disco_batch *b, const ViewT<R> &v, int use_next){
    if( b->NC == 8 ) launch_step_qt<9,8,R>(b, v, use_next); else launch_step_qt<6,5,R>(b, v, use_next);
 }
@@ -213,7 +227,12 @@ static void launch_report_t(disco_batch *b, const ViewT<R> &v){
 void mixed_launch_report(disco_batch *b);
 void mixed_launch_mindt(disco_batch *b);
 void mixed_launch_setup(disco_batch *b);
+void mixed_launch_restart(disco_batch *b);
 void mixed_launch_step(disco_batch *b, int use_next);
 void mixed_launch_prim2cons(disco_batch *b);
 void mixed_launch_faces(disco_batch *b);
 int mixed_prepare_zerograd(disco_batch *b);
+
+/* host <-> device copy on the batch's stream, completed on return
+ * (disco_batch.cu; used by the writers of disco_output.cu) */
+cudaError_t batch_xfer(const disco_batch *b, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind);

@@ -8,6 +8,7 @@
 
 void mixed_launch_mindt(disco_batch *b){ launch_mindt_t(b, b->vf); }
 void mixed_launch_setup(disco_batch *b){ launch_setup_t(b, b->vf); }
+void mixed_launch_restart(disco_batch *b){ launch_restart_t(b, b->vf); }
 void mixed_launch_step(disco_batch *b, int use_next){ launch_step_t(b, b->vf, use_next); }
 void mixed_launch_report(disco_batch *b){ launch_report_t(b, b->vf); }
 void mixed_launch_prim2cons(disco_batch *b){

@@ -1569,6 +1569,60 @@ __global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc){
    raise_err(v, err);
 }
 
+/* setupCells after restart() (domain.c:139-240 with restart_flag set): the
+ * checkpoint's prim, Phi and piph are in place (Doub2Cell, h5in.c:72-77).
+ * calc_dp (misc.c:271-288), wiph = 0, and on real cells prim2cons then
+ * cons2prim -- no initial(), subtract_omega or set_B_fields, so the stored
+ * face fluxes stand; ghosts as after set-up (main.c:53-62): the fixed
+ * boundary's values, cons zero (h5in.c leaves the ghosts' cons unset and
+ * nothing reads them). */
+template<int Q, int NC, class R>
+__global__ void __launch_bounds__(CB) k_restart(ViewT<R> v, int bc){
+   int2 b = v.cblk[blockIdx.x];
+   int a = b.x, i = b.y + threadIdx.x;
+   int np = v.ann_np[a];
+   if( i >= np ) return;
+   const int N = v.Ncell;
+   int c0 = v.ann_off[a], c = c0 + i;
+   int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+   int j = v.ann_j[a], k = v.ann_k[a];
+   const double *rj = v.rj + P.rj0 + 1;
+   const double *zk = v.zk + P.zk0 + 1;
+   bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
+   int err = 0;
+   double piph = v.piph[c];
+   double dphi = get_dp(piph, v.piph[c0 + (i == 0 ? np-1 : i-1)], P.Pmax, &err);
+   v.dphi[c] = dphi;
+   v.wiph[c] = 0.0;
+   double prim[Q], cons[Q];
+   if( real ){
+      double z = centroid_z(zk[k], zk[k-1]);
+      double r = centroid_r(rj[j], rj[j-1]);
+      double dph = get_dp(piph, piph - dphi, P.Pmax, &err);
+      double dV = dV_of(rj[j], rj[j-1], dph, zk[k], zk[k-1]);
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N+c];
+      double om = get_om(P, r);
+      prim2cons<Q,NC,double>(P, prim, cons, r, om, dV);
+      cons2prim<Q,NC>(P, cons, prim, r, om, dV);
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ){ v.prim[q*N+c] = (R)prim[q]; v.cons[q*N+c] = cons[q]; }
+   }else{
+      if( fixed_ghost_init<Q,NC>(P, bc, j, k, rj, zk, piph, dphi, prim) ){
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ) v.prim[q*N+c] = (R)prim[q];
+      }
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) v.cons[q*N+c] = 0.0;
+   }
+   if constexpr ( sizeof(R) != sizeof(double) ){
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) v.ccarry[q*N+c] = 0.0f;
+   }
+   raise_err(v, err);
+}
+
 /* prim2cons on real cells for an upload without cons (domain.c:349). */
 template<int Q, int NC, class R>
 __global__ void __launch_bounds__(CB) k_prim2cons(ViewT<R> v){

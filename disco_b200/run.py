@@ -2,13 +2,17 @@
 
     python -m disco_b200.run --template c1_mhd3d --set Constrained_Transport=1 --steps 20
     python -m disco_b200.run --par in.par --opt Makefile_opt.in --steps 100 --mixed
+    python -m disco_b200.run --template c0_kepler2d --steps 50 --checkpoint checkpoint_0001
+    python -m disco_b200.run --template c0_kepler2d --restart checkpoint_0001.npz --steps 50
 
 The in.par / Makefile_opt.in pair (or a bundled template, with --set
 overrides) is read with the reference's semantics, set up on the device as
 setupCells does, and advanced by `steps` full timesteps (getmindt + timestep,
 as main.c's loop) captured in a CUDA graph.  Prints one JSON line: real
 cells, device time per step, zone-updates/s and, with --kernels, the device
-time of each kernel of one instrumented step.
+time of each kernel of one instrumented step.  --restart starts from a
+checkpoint (the Restart path of setupCells), --checkpoint / --ascii write the
+output modules' files after the run.
 """
 import argparse
 import json
@@ -29,6 +33,11 @@ def main(argv=None):
     ap.add_argument("--mixed", action="store_true", help="the mixed-precision form")
     ap.add_argument("--kernels", action="store_true", help="per-kernel times of one step")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--restart", metavar="PATH", help="start from this checkpoint (.npz) instead of "
+                    "the Initial module (in.par Restart 1)")
+    ap.add_argument("--checkpoint", metavar="FILESTART",
+                    help="write FILESTART.npz after the run (the checkpoint datasets)")
+    ap.add_argument("--ascii", metavar="FILESTART", help="write FILESTART.dat after the run (ascii output)")
     a = ap.parse_args(argv)
     if a.template:
         par, opt = template_paths(a.template)
@@ -50,7 +59,10 @@ def main(argv=None):
         if tmp:
             os.unlink(tmp)
     import torch
-    b = Batch([disk], device=a.device, precision=PREC_MIXED if a.mixed else PREC_FP64)
+    b = Batch([disk], device=a.device, precision=PREC_MIXED if a.mixed else PREC_FP64,
+              setup=a.restart is None)
+    if a.restart:
+        b.restart(a.restart)
     stream = torch.cuda.Stream(device=a.device)
     b.set_stream(stream.cuda_stream)          # the events below time the batch's own launches
     b.run(a.warmup)
@@ -75,6 +87,11 @@ def main(argv=None):
            "ms_per_step": ms, "zone_updates_per_s": disk.nreal / (ms / 1e3)}
     if kt is not None:
         out["kernels_ms_per_step"] = dict(sorted(kt.items(), key=lambda x: -x[1]))
+    out["t"], out["count_steps"] = b.time()
+    if a.checkpoint:
+        out["checkpoint"] = b.write_checkpoint(a.checkpoint)
+    if a.ascii:
+        out["ascii"] = b.write_ascii(a.ascii)
     print(json.dumps(out))
 
 

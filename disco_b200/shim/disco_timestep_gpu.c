@@ -9,9 +9,12 @@
  *     double getmindt( struct domain * )            misc.c:39-84
  * main.c's loop (main.c:69-83) is unchanged.  The first call uploads the
  * domain (cells, grid, parameters) to the GPU; afterwards the state stays on
- * the device and struct domain's cells are stale until
- * disco_gpu_sync_to_host() copies them back (call it before report/output,
- * e.g. at the top of possiblyOutput, domain.c:317).
+ * the device and struct domain's cells and planets are stale until
+ * disco_gpu_sync_to_host() copies them back (call it before output, e.g. at
+ * the top of possiblyOutput, domain.c:317; report() is replaced here and
+ * needs no copy).  The first call also uploads the domain's planets, so a
+ * run restarted by the reference's own restart() (h5in.c) continues from
+ * the checkpoint's planets.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -103,6 +106,19 @@ static void gpu_init(struct domain *d){
    s = disco_batch_set_cells(g_batch, prim, cons, piph, dphi, wiph, real, phis);
    free(prim); free(cons); free(piph); free(dphi); free(wiph); free(real); free(phis);
    if( s ) fail("disco_batch_set_cells", s);
+   /* the planets as the host domain holds them: a restart reads them from
+    * the checkpoint (h5in.c:291-318), not from initializePlanets */
+   double *pl = malloc(sizeof(double)*DISCO_PLANET_COLS*(d->Npl > 0 ? d->Npl : 1));
+   int ip;
+   for( ip=0 ; ip<d->Npl ; ++ip ){
+      const struct planet *P = d->thePlanets + ip;
+      double *r = pl + DISCO_PLANET_COLS*ip;
+      r[0] = P->M; r[1] = P->vr; r[2] = P->omega; r[3] = P->r; r[4] = P->phi; r[5] = P->eps;
+      r[6] = (double)P->type;
+   }
+   s = disco_batch_set_planets(g_batch, 0, pl, d->Npl);
+   free(pl);
+   if( s ) fail("disco_batch_set_planets", s);
 }
 
 /* getmindt replacement (misc.c:39-84): the device min-reduction. */
@@ -163,6 +179,18 @@ void disco_gpu_sync_to_host( struct domain * theDomain ){
       if( phis ) for( q=0 ; q<NUM_FACES ; ++q ) c->Phi[q] = phis[NUM_FACES*n+q];
    }
    free(prim); free(cons); free(piph); free(dphi); free(wiph); free(phis);
+   /* the planets, moved on the device (planet data of a checkpoint) */
+   double *pl = malloc(sizeof(double)*DISCO_PLANET_COLS*(theDomain->Npl > 0 ? theDomain->Npl : 1));
+   int npl = 0;
+   if( disco_batch_get_planets(g_batch, 0, pl, theDomain->Npl, &npl) == DISCO_OK && npl == theDomain->Npl ){
+      int p;
+      for( p=0 ; p<npl ; ++p ){
+         struct planet *P = theDomain->thePlanets + p;
+         const double *r = pl + DISCO_PLANET_COLS*p;
+         P->M = r[0]; P->vr = r[1]; P->omega = r[2]; P->r = r[3]; P->phi = r[4]; P->eps = r[5];
+      }
+   }
+   free(pl);
    /* time-averaged diagnostics accumulated on the device (analysis.c:52-107) */
    int nq = 0;
    double tavg = 0.0;

@@ -9,7 +9,7 @@
  *
  * and timestep() calls onestep() twice (onestep.c:84-229).  Physics modules
  * are link-time selected C files (hydro.h, geometry.h, boundary.h, omega.h,
- * Planets/*.c, Initial/*.c) chosen in Makefile_opt.in; run-time parameters
+ * Planets/<name>.c, Initial/<name>.c) chosen in Makefile_opt.in; run-time parameters
  * come from in.par (readpar.c:44-188).
  *
  * Here the whole state lives on one GPU between calls, laid out as ragged
@@ -47,7 +47,8 @@ enum disco_status {
    DISCO_ERR_NONFINITE = 5,    /* non-finite dt or state detected */
    DISCO_ERR_NO_DEVICE = 6,    /* no CUDA device / library built without one */
    DISCO_ERR_STATE = 7,        /* call out of order (e.g. step before set_cells) */
-   DISCO_ERR_INTERNAL = 8      /* a device-side consistency check failed */
+   DISCO_ERR_INTERNAL = 8,     /* a device-side consistency check failed */
+   DISCO_ERR_IO = 9            /* a file could not be written, read or parsed */
 };
 
 /* Module choices, one per Makefile_opt.in line (Makefile:11-26).  The names
@@ -181,6 +182,72 @@ int disco_batch_run(disco_batch *b, int nsteps);
 
 /* Simulation time and step count of disk d (theDomain->t, count_steps). */
 int disco_batch_time(const disco_batch *b, int disk, double *t, int *count_steps);
+
+/* Set disk d's simulation time (theDomain->t; restart sets it from the
+ * checkpoint, h5in.c:159). */
+int disco_batch_set_time(disco_batch *b, int disk, double t);
+
+/*
+ * Planets of disk d as rows of DISCO_PLANET_COLS doubles -- M, vr, omega, r,
+ * phi, eps, type -- the columns of the checkpoint's Data/Planets
+ * (h5out.c:444-455) and of restart (h5in.c:305-317).  get: *npl receives the
+ * module's planet count (theDomain->Npl); rows (may be NULL) needs cap >= it.
+ * set: npl must equal that count; type must be 0 (PLPOINTMASS, the only
+ * planet force built), else DISCO_ERR_UNSUPPORTED.  Set after a restart, or
+ * by a drop-in whose host domain has moved the planets.
+ */
+#define DISCO_PLANET_COLS 7
+int disco_batch_get_planets(disco_batch *b, int disk, double *rows, int cap, int *npl);
+int disco_batch_set_planets(disco_batch *b, int disk, const double *rows, int npl);
+
+/*
+ * Restart set-up (setupCells with restart_flag set, domain.c:139-240, after
+ * restart()'s Doub2Cell, h5in.c:72-77): uploads, for every cell of the batch
+ * in annulus order, prim (NUM_Q per cell), Phi (NUM_FACES per cell; required
+ * when constrained transport is on, ignored otherwise) and piph, then on the
+ * device: dphi by calc_dp, wiph = 0, prim2cons and cons2prim on real cells,
+ * ghosts' boundary values (main.c:53-62), the mesh velocities, and getmindt.
+ * Diagnostics and step counts restart from zero (h5in.c:329-333).  Time and
+ * planets are set separately (disco_batch_set_time / _set_planets).
+ */
+int disco_batch_restart_cells(disco_batch *b, const double *prim, const double *Phi,
+                              const double *piph);
+
+/*
+ * Checkpoint of disk d (Output/h5out.c:349-598, serial): the file
+ * "<filestart>.npz" (the container of disco_host.h: disco_npz_*) holds the
+ * reference's datasets under their HDF5 paths --
+ *   Grid/T [1], Grid/r_jph [Nr+1], Grid/z_kph [Nz+1] (ghost edges included),
+ *   Grid/Index, Grid/Np, Grid/Id_phi0 [Nz][Nr] (int32),
+ *   Data/Cells [ncell][NUM_Q+NUM_FACES+1] (prim, Phi, piph per cell, annulus
+ *   order), Data/Planets [Npl][7], Data/Diagnostics [Nz][Nr][Ntools],
+ *   Pars/<in.par key> [1], Opts/<module> [1]
+ * -- and, as output() does, averages the diagnostics over their window
+ * (avg_diagnostics) and then zeroes them (zero_diagnostics).  NUM_FACES is
+ * that of CT_MODE (0, 3 or 5), with zero face fluxes when constrained
+ * transport is off.  The rows are packed on the device and streamed to the
+ * file through a pinned buffer.
+ */
+int disco_batch_write_checkpoint(disco_batch *b, int disk, const char *filestart);
+
+/*
+ * The ascii output module (Output/ascii.c:7-77) for disk d: "<filestart>.dat"
+ * with one line per cell -- r phi z dr dphi dz prim[NUM_Q], "%e " each --
+ * annuli j outer, layers k inner (the ghost layers left out when
+ * Z_Periodic), the same text the reference writes for the same state.
+ */
+int disco_batch_write_ascii(disco_batch *b, int disk, const char *filestart);
+
+/*
+ * Restart every disk of the batch from its checkpoint file (paths[d], as
+ * written by disco_batch_write_checkpoint): the reads of restart()
+ * (h5in.c:100-354: T, Planets, Cells by Index/Np) and the set-up of
+ * disco_batch_restart_cells.  The file's grid (Np, r_jph, z_kph) must be the
+ * disk's -- the reference rebuilds its grid from the file, this batch was
+ * built for one -- and its column count NUM_Q+NUM_FACES+1; otherwise
+ * DISCO_ERR_ARG.  A file that cannot be read gives DISCO_ERR_IO.
+ */
+int disco_batch_restart(disco_batch *b, const char *const *paths);
 
 /*
  * report() (report.c:7-202) on the device, without copying the state: the

@@ -53,6 +53,35 @@ int disco_setup_phi(const disco_params *p, int Nr, int Nz, const int *Ng,
  * foreign-language mirror of the structs check its layout. */
 int disco_sizeof(int which);
 
+/*
+ * The checkpoint container (disco_npz.c): a NumPy .npz archive -- an
+ * uncompressed ZIP64 archive of .npy arrays -- standing in for the HDF5 file
+ * of Output/h5out.c and Restart/h5in.c, which this build has no library for.
+ * A member is named by the reference's dataset path ("Grid/T",
+ * "Data/Cells", ...); numpy.load(path)[name] reads it.  descr is a NumPy
+ * type string: "<f8", "<i4", "|S<n>".  All calls return a disco_status;
+ * DISCO_ERR_IO for a file that cannot be opened, written or parsed.
+ *
+ * Writing: disco_npz_create, then per member disco_npz_put (whole array) or
+ * disco_npz_begin / disco_npz_append (any number of pieces, exactly the
+ * array's bytes in total) / disco_npz_end, then disco_npz_close.  Reading:
+ * disco_npz_open, disco_npz_info (descr, ndim <= 8, shape), disco_npz_read
+ * (a byte range of the array data, C order), disco_npz_close.  Compressed
+ * members (numpy.savez_compressed) are refused with DISCO_ERR_UNSUPPORTED.
+ */
+typedef struct disco_npz disco_npz;
+int disco_npz_create(const char *path, disco_npz **z);
+int disco_npz_begin(disco_npz *z, const char *name, const char *descr, int ndim,
+                    const int64_t *shape);
+int disco_npz_append(disco_npz *z, const void *data, size_t nbytes);
+int disco_npz_end(disco_npz *z);
+int disco_npz_put(disco_npz *z, const char *name, const char *descr, int ndim,
+                  const int64_t *shape, const void *data);
+int disco_npz_open(const char *path, disco_npz **z);
+int disco_npz_info(disco_npz *z, const char *name, char *descr, int *ndim, int64_t *shape);
+int disco_npz_read(disco_npz *z, const char *name, uint64_t offset, void *dst, size_t nbytes);
+int disco_npz_close(disco_npz *z);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,6 +65,8 @@ def load_dump(d):
                wiph=rd("wiph.f64", np.float64), real=rd("real.i32", np.int32),
                dt=rd("dt.f64", np.float64), Qrz=rd("Qrz.f64", np.float64),
                dt_next=rd("dt_next.f64", np.float64)[0])
+    if os.path.exists(os.path.join(d, "planets.f64")):
+        out["planets"] = rd("planets.f64", np.float64).reshape(-1, 7)
     if meta.get("num_faces", 0) > 0 and os.path.exists(os.path.join(d, "Phi.f64")):
         out["Phi"] = rd("Phi.f64", np.float64).reshape(N, meta["num_faces"])
     for dim in (1, 2):

@@ -10,6 +10,10 @@
  *
  * usage:  disco_ref RUNDIR NSTEPS [DUMPDIR]      dump state after N steps
  *         disco_ref RUNDIR NSTEPS --time          print wall-time JSON only
+ * environment: DISCO_REF_REPORT (report.dat line), DISCO_REF_ASCII=<filestart>
+ * (ascii output of the final state), DISCO_REF_CHECKPOINT=<dir> (checkpoint
+ * datasets as raw files), DISCO_REF_RESTART=<dir> (with Restart 1 in in.par:
+ * start from such a checkpoint)
  *
  * RUNDIR must hold in.par (read_par_file reads "in.par" from the CWD,
  * readpar.c:62).  Dumps are raw little-endian arrays, one file each,
@@ -36,6 +40,10 @@ void freeDomain( struct domain * );
 /* Present only when this driver is linked with the GPU drop-in
  * (disco_b200/shim): copies the device state back into the cells. */
 void disco_gpu_sync_to_host( struct domain * ) __attribute__((weak));
+/* oracle/ref_checkpoint.c: h5out.c's datasets as raw files */
+void disco_ref_checkpoint( struct domain * , const char * );
+/* the output module (Output/ascii.c in the oracle build) */
+void output( struct domain * , char * );
 
 static double wall(void){
    struct timeval tv; gettimeofday(&tv, NULL);
@@ -152,8 +160,21 @@ int main(int argc, char *argv[]){
    /* DISCO_REF_REPORT set: one report() of the final state into report.dat
     * of RUNDIR (the current directory), as possiblyOutput would write it */
    if( getenv("DISCO_REF_REPORT") ) report( &theDomain );
-   if( !dumpdir ) return 0;
-   if( disco_gpu_sync_to_host ) disco_gpu_sync_to_host( &theDomain );
+   /* DISCO_REF_ASCII=<filestart>: the output module's file of the final
+    * state; DISCO_REF_CHECKPOINT=<dir>: its checkpoint (after the dump,
+    * since output() averages and then zeroes the diagnostics) */
+   const char *ascii = getenv("DISCO_REF_ASCII");
+   const char *ckpt = getenv("DISCO_REF_CHECKPOINT");
+   if( (ascii || ckpt || dumpdir) && disco_gpu_sync_to_host ) disco_gpu_sync_to_host( &theDomain );
+   if( ascii ){
+      char fs[4096];
+      snprintf(fs, sizeof fs, "%s", ascii);
+      output( &theDomain , fs );
+   }
+   if( !dumpdir ){
+      if( ckpt ) disco_ref_checkpoint( &theDomain , ckpt );
+      return 0;
+   }
 
    int Q = NUM_Q;
    double *prim = malloc(sizeof(double)*Q*(size_t)Ncell);
@@ -177,9 +198,10 @@ int main(int argc, char *argv[]){
    snprintf(fn, sizeof fn, "%s/meta.txt", absdump);
    m = fopen(fn, "w");
    fprintf(m, "Nr %d\nNz %d\nNgRa %d\nNgRb %d\nNgZa %d\nNgZb %d\nQ %d\nNcell %d\n"
-              "Nreal %d\nnsteps %d\nt %.17g\nnum_faces %d\nnum_tools %d\n",
+              "Nreal %d\nnsteps %d\nt %.17g\nnum_faces %d\nnum_tools %d\nt_avg %.17g\nNpl %d\n",
            Nr, Nz, theDomain.NgRa, theDomain.NgRb, theDomain.NgZa, theDomain.NgZb,
-           Q, Ncell, Nreal, nsteps, theDomain.t, NUM_FACES, theDomain.num_tools);
+           Q, Ncell, Nreal, nsteps, theDomain.t, NUM_FACES, theDomain.num_tools,
+           theDomain.theTools.t_avg, theDomain.Npl);
    fclose(m);
    dump(absdump, "Np.i32", theDomain.Np, sizeof(int)*Nr*Nz);
    dump(absdump, "r_jph.f64", theDomain.r_jph-1, sizeof(double)*(Nr+1));
@@ -196,8 +218,19 @@ int main(int argc, char *argv[]){
         sizeof(double)*(size_t)Nr*Nz*theDomain.num_tools);
    if( Nr > 1 ) dump_faces(&theDomain, 1, absdump, cell_off);
    if( Nz > 1 ) dump_faces(&theDomain, 2, absdump, cell_off);
+   /* planets: M vr omega r phi eps type (h5out.c:444-455) */
+   double *pl = malloc(sizeof(double)*7*(size_t)theDomain.Npl);
+   int p;
+   for( p=0 ; p<theDomain.Npl ; ++p ){
+      struct planet *P = theDomain.thePlanets + p;
+      double *r = pl + 7*p;
+      r[0] = P->M; r[1] = P->vr; r[2] = P->omega; r[3] = P->r; r[4] = P->phi; r[5] = P->eps;
+      r[6] = (double)P->type;
+   }
+   dump(absdump, "planets.f64", pl, sizeof(double)*7*(size_t)theDomain.Npl);
    /* the dt the next step would take */
    double dt_next = getmindt(&theDomain);
    dump(absdump, "dt_next.f64", &dt_next, sizeof(double));
+   if( ckpt ) disco_ref_checkpoint( &theDomain , ckpt );
    return 0;
 }

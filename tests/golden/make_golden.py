@@ -11,6 +11,10 @@ available:
 
 Each case writes <case>.npz with the step-0 state (s0_*), the step-N state
 (sN_*), the dt sequence, the r-face list after N steps and the diagnostics.
+The checkpoint cases (ck_*) hold the state after N steps with its planets,
+the reference's checkpoint datasets (ck_*) and ascii output of that state,
+and the state after restarting from that checkpoint, 0 steps (r0_*) and M
+steps (rM_*) later.
 """
 import os
 import sys
@@ -88,8 +92,96 @@ def par_text(cfg_par, overrides):
     return "".join(out)
 
 
+# Checkpoint and restart (Output/h5out.c, Output/ascii.c, Restart/h5in.c
+# through oracle/ref_checkpoint.c): case -> (module config, in.par overrides,
+# steps before the checkpoint N, steps after the restart M)
+CKPT_CASES = {
+    # moving binary (planets in the checkpoint), point-mass gravity, diagnostics
+    "ck_cm2": ("c0_cm2", {"Num_R": 24, "Mass_Ratio": 1.0e-3, "Energy_Omega": 0}, 6, 4),
+    # libm-free: hydro without face fluxes (NUM_FACES 0), 2D CT (3), 3D CT (5)
+    "ck_rigid": ("c0_nograv", {"Num_R": 20, "Log_Zoning": 0, "Init_Par2": 1,
+                               "Energy_Omega": 0, "Mach_Number": 5.0}, 8, 4),
+    "ck_ct_rigid": ("c1_mhd2d_nograv", {"Num_R": 14, "Init_Par2": 1, "Init_Par4": 10.0,
+                                        "Constrained_Transport": 1, "Init_Par5": 20.0,
+                                        "Init_Par6": 0.05}, 8, 4),
+    "ck_ct3d_rigid": ("c1_mhd3d_nograv", {"Num_R": 6, "Num_Z": 5, "Init_Par2": 1,
+                                          "Init_Par4": 10.0, "Constrained_Transport": 1,
+                                          "Init_Par5": 20.0, "Init_Par6": 0.05}, 4, 3),
+}
+
+CK_FILES = (("T", "f64"), ("r_jph", "f64"), ("z_kph", "f64"), ("Index", "i32"), ("Np", "i32"),
+            ("Id_phi0", "i32"), ("Cells", "f64"), ("Planets", "f64"), ("Diagnostics", "f64"))
+
+
+def read_ck(d):
+    """oracle/ref_checkpoint.c's raw datasets as arrays of their shapes."""
+    NrT, NzT, Nc, Nq, Npl, NpDat, Nt = (int(x) for x in open(os.path.join(d, "dims.txt")).read().split())
+    shapes = {"T": (1,), "r_jph": (NrT + 1,), "z_kph": (NzT + 1,), "Index": (NzT, NrT),
+              "Np": (NzT, NrT), "Id_phi0": (NzT, NrT), "Cells": (Nc, Nq), "Planets": (Npl, NpDat),
+              "Diagnostics": (NzT, NrT, Nt)}
+    out = {}
+    for name, t in CK_FILES:
+        a = np.fromfile(os.path.join(d, name + "." + t), np.float64 if t == "f64" else np.int32)
+        out[name] = a.reshape(shapes[name])
+    return out
+
+
+def run_env(cfg, text, nsteps, env):
+    """Run the reference with extra environment; returns (dump, workdir)."""
+    import subprocess
+    import tempfile
+    binary = pyoracle.build_ref(cfg)
+    work = tempfile.mkdtemp(prefix="disco_ck_")
+    with open(os.path.join(work, "in.par"), "w") as f:
+        f.write(text)
+    subprocess.run([binary, work, str(nsteps), os.path.join(work, "dump")], check=True,
+                   stdout=subprocess.DEVNULL, env=dict(os.environ, **env))
+    return pyoracle.load_dump(os.path.join(work, "dump")), work
+
+
+def make_ckpt(case):
+    import shutil
+    cfg, over, n, m = CKPT_CASES[case]
+    text = par_text(BASE_PAR[cfg], over)
+    with open(os.path.join(HERE, case + ".par"), "w") as f:
+        f.write(text)
+    d0 = pyoracle.run_ref(cfg, text, 0)
+    probe = os.path.join(HERE, "_ck_tmp")
+    os.makedirs(probe, exist_ok=True)
+    dn, w = run_env(cfg, text, n, {"DISCO_REF_CHECKPOINT": os.path.join(probe, "ck"),
+                                   "DISCO_REF_ASCII": os.path.join(probe, "ascii")})
+    ck = read_ck(os.path.join(probe, "ck"))
+    with open(os.path.join(probe, "ascii.dat"), "rb") as f:
+        ascii_bytes = np.frombuffer(f.read(), np.uint8)
+    rtext = par_text(BASE_PAR[cfg], dict(over, Restart=1))
+    r0, w0 = run_env(cfg, rtext, 0, {"DISCO_REF_RESTART": os.path.join(probe, "ck")})
+    rm, wm = run_env(cfg, rtext, m, {"DISCO_REF_RESTART": os.path.join(probe, "ck")})
+    for x in (w, w0, wm):
+        shutil.rmtree(x, ignore_errors=True)
+    shutil.rmtree(probe, ignore_errors=True)
+    # the step-N prim, Phi and piph are the checkpoint's Cells columns
+    keep = {"s0_": ("prim", "cons", "piph", "dphi", "wiph", "Phi"), "sN_": ("dphi", "wiph"),
+            "r0_": ("prim", "cons", "piph", "dphi", "wiph", "Phi"), "rM_": ("prim", "cons", "piph", "Phi")}
+    extra = {}
+    for p, d in (("s0_", d0), ("sN_", dn), ("r0_", r0), ("rM_", rm)):
+        for k in keep[p]:
+            if k in d and (k != "Phi" or over.get("Constrained_Transport")):
+                extra[p + k] = d[k]
+    np.savez_compressed(
+        os.path.join(HERE, case + ".npz"), cfg=cfg, nsteps=n, msteps=m, real=d0["real"],
+        Np=d0["Np"], r_jph=d0["r_jph"], z_kph=d0["z_kph"],
+        sN_t=dn["meta"]["t"], sN_planets=dn["planets"], sN_t_avg=dn["meta"]["t_avg"], sN_Qrz=dn["Qrz"],
+        r0_dt_next=r0["dt_next"], r0_planets=r0["planets"], r0_t=r0["meta"]["t"],
+        rM_dt=rm["dt"], rM_dt_next=rm["dt_next"], rM_t=rm["meta"]["t"], rM_planets=rm["planets"],
+        ascii=ascii_bytes, **{"ck_" + k: v for k, v in ck.items()}, **extra)
+    print(case, "cells", d0["meta"]["Ncell"], "ascii bytes", ascii_bytes.size)
+
+
 def main():
     only = set(sys.argv[1:])
+    for case in CKPT_CASES:
+        if not only or case in only:
+            make_ckpt(case)
     for case, (cfg, over, n) in CASES.items():
         if only and case not in only:
             continue

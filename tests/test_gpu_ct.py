@@ -27,29 +27,12 @@ import numpy as np
 import pytest
 
 import disco_b200 as db
-from helpers import case_disk, par_with, rel_l1, rel_l1_cols
+from helpers import case_disk, observed_slots as _observed_slots, par_with, rel_l1, rel_l1_cols
 
 pytestmark = pytest.mark.gpu
 
 CT_CASES = ["c1_ct2d", "c1_ct_rigid", "c1_ct_hll_fe", "c1_ct3d", "c1_ct3d_rigid"]
 CT_TOL = {"c1_ct2d": 1e-11, "c1_ct_hll_fe": 1e-11, "c1_ct3d": 1e-11}
-
-
-def _observed_slots(disk, nfs):
-    """Mask (ncell x nfs) of the Phi slots real cells read."""
-    Nr, Nz, Ng = disk.Nr, disk.Nz, disk.Ng
-    jk = np.repeat(np.arange(Nr * Nz), disk.Np)
-    j, k = jk % Nr, jk // Nr
-    rj = (j >= Ng[0]) & (j < Nr - Ng[1])
-    rk = (k >= Ng[2]) & (k < Nz - Ng[3])
-    m = np.zeros((disk.ncell, nfs), bool)
-    m[:, 0] = disk.real == 1
-    m[:, 1] = (j >= Ng[0]) & (j <= Nr - Ng[1]) & rk
-    m[:, 2] = (j >= Ng[0] - 1) & (j <= Nr - Ng[1] - 1) & rk
-    if nfs == 5 and Nz > 1:
-        m[:, 3] = rj & (k >= Ng[2]) & (k <= Nz - Ng[3])
-        m[:, 4] = rj & (k >= Ng[2] - 1) & (k <= Nz - Ng[3] - 1)
-    return m
 
 
 def _from_golden(disk, g):

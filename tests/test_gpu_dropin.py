@@ -14,17 +14,23 @@ import numpy as np
 import pytest
 
 import pyoracle
-from helpers import GOLDEN, rel_l1_cols
+from helpers import GOLDEN, ck_to_raw, golden, rel_l1_cols
 
 pytestmark = pytest.mark.gpu
 
 
-def _run(binary, par, nsteps, report=False):
+def _run(binary, par, nsteps, report=False, env_extra=None, par_over=None):
     work = tempfile.mkdtemp(prefix="dropin_")
     try:
-        shutil.copy(par, os.path.join(work, "in.par"))
+        with open(par) as f:
+            text = f.read()
+        for k, v in (par_over or {}).items():     # e.g. Restart 1
+            text = "".join("%s\t\t%s\n" % (k, v) if line.split()[:1] == [k] else line
+                           for line in text.splitlines(True))
+        with open(os.path.join(work, "in.par"), "w") as f:
+            f.write(text)
         dump = os.path.join(work, "dump")
-        env = dict(os.environ)
+        env = dict(os.environ, **(env_extra or {}))
         if report:
             env["DISCO_REF_REPORT"] = "1"
         subprocess.run([binary, work, str(nsteps), dump], check=True,
@@ -121,3 +127,37 @@ def test_dropin_report(cfg, par):
             assert x == y, (n, x, y)
         else:
             assert abs(x - y) <= 5e-6 * abs(x) + 1e-300, (n, x, y)
+
+
+def test_dropin_restart_from_checkpoint(tmp_path):
+    """A run restarted by the reference's own set-up (setupCells with Restart
+    1; the checkpoint read by oracle/ref_checkpoint.c in place of h5in.c) and
+    continued through the drop-in: the shim uploads the checkpoint's planets
+    (the binary has moved since initializePlanets), so 4 steps match the
+    reference restarted from the same file, planets included."""
+    ref, hyb = _binaries("c0_cm2")
+    g = golden("ck_cm2")
+    raw = ck_to_raw(g, str(tmp_path / "ck"))
+    par = os.path.join(GOLDEN, "ck_cm2.par")
+    b = _run(hyb, par, int(g["msteps"]), env_extra={"DISCO_REF_RESTART": raw},
+             par_over={"Restart": 1})
+    r = g["real"] == 1
+    assert np.max(np.abs(b["dt"] / g["rM_dt"] - 1)) < 1e-11
+    assert max(rel_l1_cols(b["prim"][r], g["rM_prim"][r])) < 1e-11
+    assert abs(b["meta"]["t"] / g["rM_t"] - 1) < 1e-12
+    assert np.abs(b["planets"] - g["rM_planets"]).max() < 1e-11
+    # the planets really moved: a restart that re-initialised them would not match
+    assert np.abs(g["rM_planets"][:, 4] - np.array([np.pi, 0.0])).min() > 0.1
+
+
+def test_dropin_ascii_output(tmp_path):
+    """The reference's ascii output module through the drop-in, after the
+    device state is copied back (disco_gpu_sync_to_host): byte for byte the
+    reference's file for the libm-free case."""
+    ref, hyb = _binaries("c0_nograv")
+    g = golden("ck_rigid")
+    out = str(tmp_path / "ascii")
+    _run(hyb, os.path.join(GOLDEN, "ck_rigid.par"), int(g["nsteps"]),
+         env_extra={"DISCO_REF_ASCII": out})
+    with open(out + ".dat", "rb") as f:
+        assert f.read() == bytes(g["ascii"])
