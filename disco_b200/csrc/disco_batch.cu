@@ -164,8 +164,13 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       }
    }
    if( mods->boundary != DISCO_BC_FIXED && mods->boundary != DISCO_BC_ZEROGRAD &&
-       mods->boundary != DISCO_BC_FIXED3D )
+       mods->boundary != DISCO_BC_FIXED3D && mods->boundary != DISCO_BC_POLAR )
       return DISCO_ERR_UNSUPPORTED;
+   /* Boundary/polar.c sets the outer r and the z ghosts only: it is meant
+    * for a grid whose inner edge is the axis (NoBC_Rmin 1, no inner ghosts);
+    * with inner ghosts their prims would never be set */
+   if( mods->boundary == DISCO_BC_POLAR )
+      for( int d=0 ; d<ndisk ; ++d ) if( Ng[4*d+0] != 0 ) return DISCO_ERR_UNSUPPORTED;
    if( mods->initial != DISCO_IC_KEPLER_NOISE && mods->initial != DISCO_IC_MHD_SHEAR_NOISE )
       return DISCO_ERR_UNSUPPORTED;
    for( int d=0 ; d<ndisk ; ++d ){
@@ -180,7 +185,8 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->device = device; b->mods = *mods; b->prec = precision; b->ndisk = ndisk;
    b->NC = mods->num_c; b->Q = mods->num_c + mods->num_n;
    b->timestep_mode = params[0].Timestep == 1 ? 1 : 0;
-   b->bc_fixed = mods->boundary == DISCO_BC_FIXED ? 1 : mods->boundary == DISCO_BC_FIXED3D ? 2 : 0;
+   b->bc_fixed = mods->boundary == DISCO_BC_FIXED ? 1 : mods->boundary == DISCO_BC_FIXED3D ? 2 :
+                 mods->boundary == DISCO_BC_POLAR ? 3 : 0;
    b->bc_zerograd = mods->boundary == DISCO_BC_ZEROGRAD;
    b->d_zg_pairs = NULL;
    b->zg_smem = 0;

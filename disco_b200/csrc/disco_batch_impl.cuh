@@ -19,7 +19,7 @@ struct disco_batch {
    int prec;
    int ndisk, Q, NC;
    int timestep_mode;        /* 0 = RK2, 1 = forward Euler */
-   int bc_fixed;             /* 0 none / zerograd, 1 fixed, 2 fixed3d */
+   int bc_fixed;             /* 0 none / zerograd, 1 fixed, 2 fixed3d, 3 polar */
    int any_mm3;
    int any_3d;               /* some disk has Nz > 1: z faces, gradz, z fluxes */
    int bc_zerograd;          /* Boundary/zerograd.c */

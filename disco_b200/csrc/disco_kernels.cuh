@@ -568,6 +568,28 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_GRAD) k_grad(ViewT<R> 
    LIM_RUN(Rout.s1, Rout.e1)
    LIM_RUN(Rout.s2, Rout.e2)
 #undef LIM_RUN
+   /* plm_geom_boundary at the axis (plm.c:184-185 -> geom_grad,
+    * cylindrical.c:141-173): with no ghosts inside (NgRa 0) and the inner
+    * edge at r = 0, the first annulus keeps only its v_r (and B_r) slope,
+    * limited against prim/r at the centroid; the other slopes are zero.
+    * (At an outer or z edge without ghosts geom_grad changes nothing.) */
+   if( DIM == 1 && j == 0 && P.NgRa == 0 ){
+      double xp0 = rj[0], xm0 = rj[-1];
+      if( !(xp0 < 0.0 || fabs(xm0) > 1.0e-10*xp0) ){
+         double r = centroid_r(xp0, xm0);
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ){
+            if( q == URR || (Q > 6 && q == BRR) ){
+               double SL = (double)v.prim[q*N + c]/r;
+               double S = (double)g[q];
+               if( S*SL < 0.0 ) g[q] = R(0.0);
+               else if( fabs(P.PLM*SL) < fabs(S) ) g[q] = (R)(P.PLM*SL);
+            }else{
+               g[q] = R(0.0);
+            }
+         }
+      }
+   }
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) grad[q*N + c] = g[q];
    raise_err(v, err);
@@ -805,10 +827,11 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
       }
       /* r faces: inner track (cell is R) then outer track (cell is L) */
       int I0 = v.I0[a];
-      int tin = P.trr0 + (j-1) + (P.Nr-1)*k;
-      int tout = P.trr0 + j + (P.Nr-1)*k;
-      Runs Rin = cell_runs(v, v.consR, tin, c0, np, i, I0);
-      Runs Rout = cell_runs(v, v.consL, tout, c0, np, i, I0);
+      /* a real annulus at the axis (NoBC_Rmin, j = 0) has no inner track, one
+       * at an outer edge without ghosts (NoBC_Rmax, j = Nr-1) no outer one */
+      Runs Rin = {1,0,1,0}, Rout = {1,0,1,0};
+      if( j >= 1 ) Rin = cell_runs(v, v.consR, P.trr0 + (j-1) + (P.Nr-1)*k, c0, np, i, I0);
+      if( j <= P.Nr-2 ) Rout = cell_runs(v, v.consL, P.trr0 + j + (P.Nr-1)*k, c0, np, i, I0);
       const size_t Nf = v.Nf;
 #define ADD_RUN(s,e,sg) for( int f=(s) ; f<=(e) ; ++f ){ \
       _Pragma("unroll") for( int q=0 ; q<Q ; ++q ) acc<R>(cons[q], cc[q], sg (double)v.fG[q*Nf + f]); }
@@ -972,7 +995,9 @@ __global__ void __launch_bounds__(CB) k_diag_part(ViewT<R> v){
  *         piph - dphi/2, midpoint z)
  *   bc 2  Boundary/fixed3d.c -> boundary_functions.c:20-31, 161-265: r ghosts
  *         (all k) and z ghosts (all j) at the centroid (get_centroid_arr)
- * then subtract_omega (rotframe.c:15-17).  Returns whether prim was set. */
+ * then subtract_omega (rotframe.c:15-17);
+ *   bc 3  Boundary/polar.c: outer r ghosts and z ghosts at the centroid,
+ *         without subtract_omega.  Returns whether prim was set. */
 template<int Q, int NC>
 __device__ __forceinline__ bool fixed_ghost_init(const DiskParams &P, int bc, int j, int k,
                                                  const double *rj, const double *zk,
@@ -985,6 +1010,13 @@ __device__ __forceinline__ bool fixed_ghost_init(const DiskParams &P, int bc, in
    }else if( bc == 2 && (rghost || zghost) ){
       double x[3] = { centroid_r(rj[j], rj[j-1]), 0.5*(piph + (piph - dphi)), 0.5*(zk[k]+zk[k-1]) };
       initial<Q,NC>(P, prim, x);
+   }else if( bc == 3 && (j >= P.Nr - P.NgRb || zghost) ){
+      /* Boundary/polar.c:10-77: the outer r ghosts, then every annulus of
+       * the z ghost layers, re-evaluated at their centroids (the z pass
+       * rewrites the corners with the same values); no subtract_omega */
+      double x[3] = { centroid_r(rj[j], rj[j-1]), piph - .5*dphi, centroid_z(zk[k], zk[k-1]) };
+      initial<Q,NC>(P, prim, x);
+      return true;
    }else{
       return false;
    }

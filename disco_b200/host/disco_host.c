@@ -138,6 +138,7 @@ int disco_read_opt(const char *path, disco_modules *m){
    if( !strcmp(v, "fixed") ) m->boundary = DISCO_BC_FIXED;
    else if( !strcmp(v, "zerograd") ) m->boundary = DISCO_BC_ZEROGRAD;
    else if( !strcmp(v, "fixed3d") ) m->boundary = DISCO_BC_FIXED3D;
+   else if( !strcmp(v, "polar") ) m->boundary = DISCO_BC_POLAR;
    else return DISCO_ERR_UNSUPPORTED;
    if( opt_value(path, "PLANETS", v, sizeof v) ) return DISCO_ERR_ARG;
    if( !strcmp(v, "none") ) m->planets = DISCO_PLANETS_NONE;

@@ -183,12 +183,15 @@ int main(int argc, char *argv[]){
    double *dphi = malloc(sizeof(double)*(size_t)Ncell);
    double *wiph = malloc(sizeof(double)*(size_t)Ncell);
    double *phis = malloc(sizeof(double)*(size_t)Ncell*(NUM_FACES>0?NUM_FACES:1));
+   double *grr = malloc(sizeof(double)*Q*(size_t)Ncell);
+   double *grp = malloc(sizeof(double)*Q*(size_t)Ncell);
    int *real = malloc(sizeof(int)*(size_t)Ncell);
    int i, q, n = 0;
    for( jk=0 ; jk<Nr*Nz ; ++jk ){
       for( i=0 ; i<theDomain.Np[jk] ; ++i, ++n ){
          struct cell *c = &theDomain.theCells[jk][i];
-         for( q=0 ; q<Q ; ++q ){ prim[Q*n+q] = c->prim[q]; cons[Q*n+q] = c->cons[q]; }
+         for( q=0 ; q<Q ; ++q ){ prim[Q*n+q] = c->prim[q]; cons[Q*n+q] = c->cons[q];
+                                 grr[Q*n+q] = c->gradr[q]; grp[Q*n+q] = c->gradp[q]; }
          piph[n] = c->piph; dphi[n] = c->dphi; wiph[n] = c->wiph; real[n] = c->real;
          for( q=0 ; q<NUM_FACES ; ++q ) phis[NUM_FACES*n+q] = c->Phi[q];
       }
@@ -212,6 +215,9 @@ int main(int argc, char *argv[]){
    dump(absdump, "dphi.f64", dphi, sizeof(double)*(size_t)Ncell);
    dump(absdump, "wiph.f64", wiph, sizeof(double)*(size_t)Ncell);
    dump(absdump, "real.i32", real, sizeof(int)*(size_t)Ncell);
+   /* the last substep's slopes (plm_phi, plm_trans), for diagnosing */
+   dump(absdump, "gradr.f64", grr, sizeof(double)*Q*(size_t)Ncell);
+   dump(absdump, "gradp.f64", grp, sizeof(double)*Q*(size_t)Ncell);
    if( NUM_FACES > 0 ) dump(absdump, "Phi.f64", phis, sizeof(double)*NUM_FACES*(size_t)Ncell);
    dump(absdump, "dt.f64", dts, sizeof(double)*(size_t)nsteps);
    dump(absdump, "Qrz.f64", theDomain.theTools.Qrz,

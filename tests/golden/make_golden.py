@@ -72,12 +72,26 @@ CASES = {
     "c1_ct3d_rigid": ("c1_mhd3d_nograv", {"Num_R": 8, "Num_Z": 6, "Init_Par2": 1,
                                           "Init_Par4": 10.0, "Constrained_Transport": 1,
                                           "Init_Par5": 20.0, "Init_Par6": 0.05}, 6),
+    # the polar boundary module (Boundary/polar.c) on grids down to the axis
+    # (NoBC_Rmin 1, R_Min 0): no inner ghosts, the axis gradient fix
+    # (plm_geom_boundary -> geom_grad) and the polar source terms; rigid
+    # rotation without gravity, hydro 2D, MHD 2D with CT, MHD 3D with CT
+    "c0_polar": ("c0_polar", {"Num_R": 16, "R_Min": 0.0, "R_Max": 2.0, "NoBC_Rmin": 1,
+                              "Log_Zoning": 0, "Init_Par2": 1, "Init_Par1": 0.05,
+                              "Energy_Omega": 0, "Mach_Number": 5.0}, 8),
+    "c1_polar_ct": ("c1_polar", {"Num_R": 14, "R_Min": 0.0, "R_Max": 2.0, "NoBC_Rmin": 1,
+                                 "Init_Par2": 1, "Init_Par4": 10.0, "Constrained_Transport": 1,
+                                 "Init_Par5": 20.0}, 8),
+    "c1_polar3d": ("c1_polar3d", {"Num_R": 8, "Num_Z": 6, "R_Min": 0.0, "R_Max": 2.0,
+                                  "NoBC_Rmin": 1, "Init_Par2": 1, "Init_Par4": 10.0,
+                                  "Constrained_Transport": 1, "Init_Par5": 20.0}, 5),
 }
 
 # the in.par template each module configuration starts from
 BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": "c0_kepler2d",
             "c1_mhd2d": "c1_mhd2d", "c1_mhd2d_nograv": "c1_mhd2d", "c0_zerograd": "c0_kepler2d", "c0_fixed3d": "c0_kepler2d",
-            "c1_mhd3d": "c1_mhd3d", "c1_mhd3d_nograv": "c1_mhd3d"}
+            "c1_mhd3d": "c1_mhd3d", "c1_mhd3d_nograv": "c1_mhd3d", "c0_polar": "c0_kepler2d",
+            "c1_polar": "c1_mhd2d", "c1_polar3d": "c1_mhd3d"}
 
 
 def par_text(cfg_par, overrides):

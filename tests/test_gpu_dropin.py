@@ -161,3 +161,16 @@ def test_dropin_ascii_output(tmp_path):
          env_extra={"DISCO_REF_ASCII": out})
     with open(out + ".dat", "rb") as f:
         assert f.read() == bytes(g["ascii"])
+
+
+def test_dropin_polar():
+    """A grid down to the axis with the polar boundary module through the
+    drop-in (the shim maps BOUNDARY polar), against the reference binary."""
+    ref, hyb = _binaries("c0_polar")
+    par = os.path.join(GOLDEN, "c0_polar.par")
+    a, b = _run(ref, par, 10), _run(hyb, par, 10)
+    assert np.max(np.abs(b["dt"] / a["dt"] - 1)) < 1e-12
+    r = a["real"] == 1
+    assert max(rel_l1_cols(b["prim"][r], a["prim"][r])) < 1e-12
+    for k in ("iL", "iR", "LRtype"):
+        assert np.array_equal(a["faces_1"][k], b["faces_1"][k]), k

@@ -1,0 +1,82 @@
+"""Grids down to the axis (NoBC_Rmin 1, R_Min 0) with the polar boundary
+module (Boundary/polar.c), against the reference binary: no inner ghosts,
+the first annulus's r slopes fixed by plm_geom_boundary -> geom_grad
+(plm.c:184-185, cylindrical.c:141-173), the polar source terms (euler.c,
+mhd.c, planet.c with NoBC_Rmin), and the outer r and z ghosts re-evaluated
+from the Initial module each substep.  2D hydro, 2D MHD with constrained
+transport and 3D MHD with constrained transport, rigid rotation without
+gravity.  The polar source terms call sin(dphi/2), whose CUDA and glibc
+values may differ in the last bit, so the state is compared at 1e-12
+relative L1 (in practice far below); the face lists bit for bit."""
+import os
+
+import numpy as np
+import pytest
+
+import disco_b200 as db
+from helpers import case_disk, observed_slots, par_with, rel_l1, rel_l1_cols
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["c0_polar", "c1_polar_ct", "c1_polar3d"]
+TOL = 1e-12
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_polar_setup(case):
+    """setupCells and the polar boundary's ghost values on the device."""
+    disk, g = case_disk(case)
+    assert disk.Ng[0] == 0 and disk.r_jph[0] == 0.0
+    b = db.Batch([disk])
+    st = b.get_cells()
+    r = disk.real == 1
+    assert np.array_equal(st["piph"], g["s0_piph"])
+    assert max(rel_l1_cols(st["prim"][r], g["s0_prim"][r])) <= TOL
+    # ghosts: the outer r layers and the z layers, set from the Initial module
+    gh = ~r
+    if gh.any():
+        assert max(rel_l1_cols(st["prim"][gh], g["s0_prim"][gh])) <= TOL
+    assert abs(b.mindt()[0] / g["s0_dt_next"] - 1) <= TOL
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_polar_steps(case):
+    disk, g = case_disk(case)
+    b = db.Batch([disk], setup=False)
+    b.set_cells(g["s0_prim"], g["s0_cons"], g["s0_piph"], g["s0_dphi"], g["s0_wiph"], g["real"],
+                Phi=g.get("s0_Phi"))
+    dts = []
+    for _ in range(int(g["nsteps"])):
+        dt = b.mindt()[0]
+        dts.append(dt)
+        b.timestep(dt)
+    b.sync()
+    st = b.get_cells()
+    F = b.faces(0, 1)
+    for k in ("fIndex", "iL", "iR", "LRtype"):
+        assert np.array_equal(F[k], g[k]), k
+    r = disk.real == 1
+    assert np.max(np.abs(np.array(dts) / g["dt"] - 1)) <= TOL
+    ep = rel_l1_cols(st["prim"][r], g["sN_prim"][r])
+    ec = rel_l1_cols(st["cons"][r], g["sN_cons"][r])
+    print("%s: prim %.2e cons %.2e" % (case, max(ep), max(ec)))
+    assert max(ep) <= TOL and max(ec) <= TOL
+    # the axis annulus itself (its slopes are the geometric ones)
+    a0 = slice(0, int(disk.Np[0]))
+    assert max(rel_l1_cols(st["prim"][a0], g["sN_prim"][a0])) <= TOL
+    if "sN_Phi" in g:
+        m = observed_slots(disk, b.num_faces)
+        for s in range(m.shape[1]):
+            if m[:, s].any():
+                assert rel_l1(st["Phi"][m[:, s], s], g["sN_Phi"][m[:, s], s]) <= TOL, s
+
+
+def test_polar_needs_the_axis():
+    """The polar module leaves inner ghosts unset: refused on a grid that
+    has them (NoBC_Rmin 0)."""
+    p = par_with({"Num_R": 12}, base="c0_kepler2d")
+    disk = db.Disk.from_files(p, os.path.join(db.TEMPLATES, "c0_polar.in"))
+    os.unlink(p)
+    with pytest.raises(db.DiscoError) as e:
+        db.Batch([disk])
+    assert e.value.status == 3
