@@ -31,7 +31,8 @@ STATUS = {0: "ok", 1: "bad argument", 2: "CUDA runtime error", 3: "module combin
           6: "no CUDA device", 7: "call out of order", 8: "device consistency check failed",
           9: "file not written, read or parsed"}
 HYDRO = {"euler": 0, "mhd": 1}
-BOUNDARY = {"fixed": 0, "zerograd": 1, "fixed3d": 2, "polar": 3}
+BOUNDARY = {"fixed": 0, "zerograd": 1, "fixed3d": 2, "polar": 3, "outflow3d": 4, "zerograd_omk": 5,
+            "accrete3d": 6}
 PLANETS = {"none": 0, "sun": 1, "cm2": 2, "binary_soft": 3}
 INITIAL = {"kepler_noise": 0, "mhd_shear_noise": 1}
 PREC_FP64, PREC_MIXED = 0, 1

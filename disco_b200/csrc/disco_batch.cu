@@ -163,8 +163,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
             return DISCO_ERR_UNSUPPORTED;
       }
    }
-   if( mods->boundary != DISCO_BC_FIXED && mods->boundary != DISCO_BC_ZEROGRAD &&
-       mods->boundary != DISCO_BC_FIXED3D && mods->boundary != DISCO_BC_POLAR )
+   if( mods->boundary < DISCO_BC_FIXED || mods->boundary > DISCO_BC_ACCRETE3D )
       return DISCO_ERR_UNSUPPORTED;
    /* Boundary/polar.c sets the outer r and the z ghosts only: it is meant
     * for a grid whose inner edge is the axis (NoBC_Rmin 1, no inner ghosts);
@@ -186,8 +185,16 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->NC = mods->num_c; b->Q = mods->num_c + mods->num_n;
    b->timestep_mode = params[0].Timestep == 1 ? 1 : 0;
    b->bc_fixed = mods->boundary == DISCO_BC_FIXED ? 1 : mods->boundary == DISCO_BC_FIXED3D ? 2 :
-                 mods->boundary == DISCO_BC_POLAR ? 3 : 0;
-   b->bc_zerograd = mods->boundary == DISCO_BC_ZEROGRAD;
+                 mods->boundary == DISCO_BC_POLAR ? 3 : mods->boundary == DISCO_BC_ACCRETE3D ? 6 : 0;
+   /* modules built from boundary_functions.c's zero-gradient copies: all four
+    * sides (zerograd; with the diode outflow3d, zerograd_omk), or the inner r
+    * side only (accrete3d, whose other sides are fixed) */
+   b->bc_zerograd = mods->boundary == DISCO_BC_ZEROGRAD || mods->boundary == DISCO_BC_OUTFLOW3D ||
+                    mods->boundary == DISCO_BC_ZEROGRAD_OMK || mods->boundary == DISCO_BC_ACCRETE3D;
+   b->zg_diode = mods->boundary == DISCO_BC_OUTFLOW3D || mods->boundary == DISCO_BC_ZEROGRAD_OMK ||
+                 mods->boundary == DISCO_BC_ACCRETE3D;
+   b->zg_omk = mods->boundary == DISCO_BC_ZEROGRAD_OMK;
+   b->d_zg_side = NULL;
    b->d_zg_pairs = NULL;
    b->zg_smem = 0;
    b->nq = mods->analysis == DISCO_DIAG_DISK2D ? 5 : 0;
@@ -309,8 +316,10 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->ncell = cell;
 
    /* zerograd layers (boundary_functions.c:269-440): r ghosts from the real
-    * cells outwards, then z ghosts (all j, ghosts included) */
+    * cells outwards, then z ghosts (all j, ghosts included); sides[] of each
+    * pair: 0 inner r, 1 outer r, 2 lower z, 3 upper z */
    if( b->bc_zerograd ){
+      const bool acc3 = mods->boundary == DISCO_BC_ACCRETE3D;
       int maxr = 0, maxz = 0;
       for( int d=0 ; d<ndisk ; ++d ){
          const DiskParams &D = b->dparams[d];
@@ -323,8 +332,13 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
             const DiskParams &D = b->dparams[d];
             for( int k=0 ; k<D.Nz ; ++k ){
                int base = D.ann0 + D.Nr*k;
-               if( l < D.NgRa ){ int j = D.NgRa-1-l; b->zg_pairs.push_back(make_int2(base+j, base+j+1)); }
-               if( l < D.NgRb ){ int j = D.Nr-D.NgRb+l; b->zg_pairs.push_back(make_int2(base+j, base+j-1)); }
+               /* accrete3d: the z ghost layers end fixed (boundary_fixed_zbot /
+                * _ztop run after the r copies), so their inner r ghosts need no copy */
+               if( acc3 && (k < D.NgZa || k >= D.Nz - D.NgZb) ) continue;
+               if( l < D.NgRa ){ int j = D.NgRa-1-l; b->zg_pairs.push_back(make_int2(base+j, base+j+1));
+                                 b->zg_side.push_back(0); }
+               if( l < D.NgRb && !acc3 ){ int j = D.Nr-D.NgRb+l;
+                                 b->zg_pairs.push_back(make_int2(base+j, base+j-1)); b->zg_side.push_back(1); }
             }
          }
       }
@@ -332,12 +346,14 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
          b->zg_off.push_back((int)b->zg_pairs.size());
          for( int d=0 ; d<ndisk ; ++d ){
             const DiskParams &D = b->dparams[d];
-            if( D.Nz < 2 || params[d].Z_Periodic ) continue;
+            if( D.Nz < 2 || params[d].Z_Periodic || acc3 ) continue;
             for( int j=0 ; j<D.Nr ; ++j ){
                if( l < D.NgZa ){ int k = D.NgZa-1-l;
-                  b->zg_pairs.push_back(make_int2(D.ann0 + j + D.Nr*k, D.ann0 + j + D.Nr*(k+1))); }
+                  b->zg_pairs.push_back(make_int2(D.ann0 + j + D.Nr*k, D.ann0 + j + D.Nr*(k+1)));
+                  b->zg_side.push_back(2); }
                if( l < D.NgZb ){ int k = D.Nz-D.NgZb+l;
-                  b->zg_pairs.push_back(make_int2(D.ann0 + j + D.Nr*k, D.ann0 + j + D.Nr*(k-1))); }
+                  b->zg_pairs.push_back(make_int2(D.ann0 + j + D.Nr*k, D.ann0 + j + D.Nr*(k-1)));
+                  b->zg_side.push_back(3); }
             }
          }
       }
@@ -414,7 +430,10 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
          }
       }
    }
-   if( b->bc_zerograd && !b->zg_pairs.empty() ) b->d_zg_pairs = dupload(b, b->zg_pairs);
+   if( b->bc_zerograd && !b->zg_pairs.empty() ){
+      b->d_zg_pairs = dupload(b, b->zg_pairs);
+      b->d_zg_side = dupload(b, b->zg_side);
+   }
    make_float_view(b);
    if( prepare_zerograd<6,double>(b) || prepare_zerograd<9,double>(b) ||
        (precision == DISCO_PREC_MIXED && mixed_prepare_zerograd(b)) ){

@@ -24,6 +24,9 @@ struct disco_batch {
    int any_3d;               /* some disk has Nz > 1: z faces, gradz, z fluxes */
    int bc_zerograd;          /* Boundary/zerograd.c */
    std::vector<int2> zg_pairs;          /* (ghost annulus, source annulus), by layer */
+   std::vector<unsigned char> zg_side;  /* per pair: 0 inner r, 1 outer r, 2 lower z, 3 upper z */
+   unsigned char *d_zg_side;
+   int zg_diode, zg_omk;                /* outflow diode; Omega from initial() in r ghosts */
    std::vector<int> zg_off;             /* layer groups: r layers, then z layers */
    int2 *d_zg_pairs;
    size_t zg_smem;                      /* dynamic shared memory of k_zerograd */
@@ -81,7 +84,9 @@ static void launch_zerograd(disco_batch *b, const ViewT<R> &v){
    if( !b->bc_zerograd ) return;
    for( size_t g=0 ; g+1<b->zg_off.size() ; ++g ){
       int n = b->zg_off[g+1] - b->zg_off[g];
-      if( n > 0 ) k_zerograd<Q,R><<<n, 128, b->zg_smem, b->stream>>>(v, b->d_zg_pairs + b->zg_off[g]);
+      if( n > 0 ) k_zerograd<Q,R><<<n, 128, b->zg_smem, b->stream>>>(v, b->d_zg_pairs + b->zg_off[g],
+                                                                     b->d_zg_side + b->zg_off[g],
+                                                                     b->zg_diode, b->zg_omk);
    }
    mark(b, "k_zerograd");
 }

@@ -996,6 +996,10 @@ __global__ void __launch_bounds__(CB) k_diag_part(ViewT<R> v){
  *   bc 2  Boundary/fixed3d.c -> boundary_functions.c:20-31, 161-265: r ghosts
  *         (all k) and z ghosts (all j) at the centroid (get_centroid_arr)
  * then subtract_omega (rotframe.c:15-17);
+ *   bc 6  Boundary/accrete3d.c: the outer r ghosts and the z ghosts as bc 2
+ *         (boundary_fixed_rout / _zbot / _ztop; the inner r ghosts are
+ *         zero-gradient, k_zerograd)
+ * then subtract_omega (rotframe.c:15-17);
  *   bc 3  Boundary/polar.c: outer r ghosts and z ghosts at the centroid,
  *         without subtract_omega.  Returns whether prim was set. */
 template<int Q, int NC>
@@ -1008,6 +1012,11 @@ __device__ __forceinline__ bool fixed_ghost_init(const DiskParams &P, int bc, in
       double x[3] = { .5*(rj[j]+rj[j-1]), piph - .5*dphi, .5*(zk[k]+zk[k-1]) };
       initial<Q,NC>(P, prim, x);
    }else if( bc == 2 && (rghost || zghost) ){
+      double x[3] = { centroid_r(rj[j], rj[j-1]), 0.5*(piph + (piph - dphi)), 0.5*(zk[k]+zk[k-1]) };
+      initial<Q,NC>(P, prim, x);
+   }else if( bc == 6 && (j >= P.Nr - P.NgRb || zghost) ){
+      /* accrete3d: boundary_fixed_rout, _zbot, _ztop (set_cell_init); the
+       * inner r ghosts are zero-gradient */
       double x[3] = { centroid_r(rj[j], rj[j-1]), 0.5*(piph + (piph - dphi)), 0.5*(zk[k]+zk[k-1]) };
       initial<Q,NC>(P, prim, x);
    }else if( bc == 3 && (j >= P.Nr - P.NgRb || zghost) ){
@@ -1211,9 +1220,16 @@ __device__ __forceinline__ int zg_walk(const double *sp, const double *sd, const
  * the two annuli's edges in shared memory and records, per ghost cell, the
  * source cell it starts from and how many it visits; then every thread sums
  * its ghost cell's overlaps in that order and divides by its dphi.  Loops
- * are capped; a cap hit raises ERRF_WRAP. */
+ * are capped; a cap hit raises ERRF_WRAP.  sides[] names each pair's
+ * boundary (0 inner r, 1 outer r, 2 lower z, 3 upper z); with `diode` the
+ * copied normal velocity may only point out of the domain (the diode
+ * argument of the same functions, used by outflow3d, zerograd_omk and
+ * accrete3d), with `omk` the r ghosts then take Omega from the Initial
+ * module (boundary_fixed_q_rinn / _rout with q = UPP, :662-718,
+ * set_cell_init_q :33-47; zerograd_omk). */
 template<int Q, class R>
-__global__ void k_zerograd(ViewT<R> v, const int2 *pairs){
+__global__ void k_zerograd(ViewT<R> v, const int2 *pairs, const unsigned char *sides, int diode,
+                           int omk){
    extern __shared__ __align__(16) unsigned char zg_smem[];
    int2 pr = pairs[blockIdx.x];
    const int a = pr.x, a1 = pr.y;
@@ -1306,7 +1322,29 @@ __global__ void k_zerograd(ViewT<R> v, const int2 *pairs){
          i1 = i1 < np1-1 ? i1+1 : 0;
       }
 #pragma unroll
-      for( int q=0 ; q<Q ; ++q ) v.prim[q*N + c0 + i] = (R)(acc[q]/sd[i]);
+      for( int q=0 ; q<Q ; ++q ) acc[q] = acc[q]/sd[i];
+      const int side = sides[blockIdx.x];
+      R out[Q];
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) out[q] = (R)acc[q];
+      if( diode ){
+         if( side == 0 && out[URR] > R(0) ) out[URR] = R(0);
+         if( side == 1 && out[URR] < R(0) ) out[URR] = R(0);
+         if( side == 2 && out[UZZ] > R(0) ) out[UZZ] = R(0);
+         if( side == 3 && out[UZZ] < R(0) ) out[UZZ] = R(0);
+      }
+      if( omk && side <= 1 ){
+         const int j = v.ann_j[a], k = v.ann_k[a];
+         const double *rj = v.rj + P.rj0 + 1;
+         const double *zk = v.zk + P.zk0 + 1;
+         double x[3] = { centroid_r(rj[j], rj[j-1]), phip - 0.5*sd[i], centroid_z(zk[k], zk[k-1]) };
+         double tp[Q];
+         initial<Q, (Q > 6 ? 8 : 5)>(P, tp, x);
+         if( P.rotframe ) tp[UPP] -= P.RotOmega;
+         out[UPP] = (R)tp[UPP];
+      }
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) v.prim[q*N + c0 + i] = out[q];
    }
 }
 

@@ -141,7 +141,8 @@ static int put_string(disco_npz *z, const char *name, const char *v){
 /* writeOpts (h5out.c:91-160): the module selection */
 static int put_opts(disco_npz *z, const disco_modules &m){
    static const char *const hydro[] = {"euler", "mhd"};
-   static const char *const bc[] = {"fixed", "zerograd", "fixed3d", "polar"};
+   static const char *const bc[] = {"fixed", "zerograd", "fixed3d", "polar", "outflow3d",
+                                    "zerograd_omk", "accrete3d"};
    static const char *const pl[] = {"none", "sun", "cm2", "binary_soft"};
    static const char *const ic[] = {"kepler_noise", "mhd_shear_noise"};
    CKS(put_string(z, "Opts/HYDRO", hydro[m.hydro]));

@@ -68,13 +68,14 @@ static void fail(const char *what, int s){
 
 static void gpu_init(struct domain *d){
    static const char *const hydros[] = {"euler", "mhd"};
-   static const char *const bcs[] = {"fixed", "zerograd", "fixed3d", "polar"};
+   static const char *const bcs[] = {"fixed", "zerograd", "fixed3d", "polar", "outflow3d",
+                                     "zerograd_omk", "accrete3d"};
    static const char *const pls[] = {"none", "sun", "cm2", "binary_soft"};
    static const char *const ics[] = {"kepler_noise", "mhd_shear_noise"};
    disco_modules m;
    memset(&m, 0, sizeof m);
    m.hydro = module_id(HYDRO, hydros, 2);
-   m.boundary = module_id(BOUNDARY, bcs, 4);
+   m.boundary = module_id(BOUNDARY, bcs, 7);
    m.planets = module_id(PLANETS, pls, 4);
    m.initial = module_id(INITIAL, ics, 2);
    m.analysis = strcmp(ANALYSIS, "diag_disk2d") == 0 ? DISCO_DIAG_DISK2D : DISCO_DIAG_NONE;

@@ -55,7 +55,8 @@ enum disco_status {
  * match the reference's module file names. */
 enum disco_hydro    { DISCO_HYDRO_EULER = 0, DISCO_HYDRO_MHD = 1 };
 enum disco_boundary { DISCO_BC_FIXED = 0, DISCO_BC_ZEROGRAD = 1, DISCO_BC_FIXED3D = 2,
-                      DISCO_BC_POLAR = 3 };
+                      DISCO_BC_POLAR = 3, DISCO_BC_OUTFLOW3D = 4, DISCO_BC_ZEROGRAD_OMK = 5,
+                      DISCO_BC_ACCRETE3D = 6 };
 enum disco_planets  { DISCO_PLANETS_NONE = 0, DISCO_PLANETS_SUN = 1, DISCO_PLANETS_CM2 = 2,
                       DISCO_PLANETS_BINARY_SOFT = 3 };
 enum disco_initial  { DISCO_IC_KEPLER_NOISE = 0, DISCO_IC_MHD_SHEAR_NOISE = 1 };

@@ -85,13 +85,24 @@ CASES = {
     "c1_polar3d": ("c1_polar3d", {"Num_R": 8, "Num_Z": 6, "R_Min": 0.0, "R_Max": 2.0,
                                   "NoBC_Rmin": 1, "Init_Par2": 1, "Init_Par4": 10.0,
                                   "Constrained_Transport": 1, "Init_Par5": 20.0}, 5),
+    # boundary modules composed from boundary_functions.c: outflow3d
+    # (zero-gradient, outflow diode, every side), zerograd_omk (the same with
+    # Omega of the r ghosts from the Initial module), accrete3d (outflow
+    # inner r, fixed outer r and z; with CT)
+    "c0_outflow3d": ("c0_outflow3d", {"Num_R": 10, "Num_Z": 4, "Z_Min": -0.3, "Z_Max": 0.3,
+                                      "Log_Zoning": 0, "Init_Par2": 1, "Init_Par1": 0.05,
+                                      "Energy_Omega": 0, "Mach_Number": 5.0}, 5),
+    "c1_omk3d": ("c1_omk3d", {"Num_R": 8, "Num_Z": 6, "Init_Par2": 1, "Init_Par4": 10.0}, 5),
+    "c1_accrete3d": ("c1_accrete3d", {"Num_R": 8, "Num_Z": 6, "Init_Par2": 1, "Init_Par4": 10.0,
+                                      "Constrained_Transport": 1, "Init_Par5": 20.0}, 5),
 }
 
 # the in.par template each module configuration starts from
 BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": "c0_kepler2d",
             "c1_mhd2d": "c1_mhd2d", "c1_mhd2d_nograv": "c1_mhd2d", "c0_zerograd": "c0_kepler2d", "c0_fixed3d": "c0_kepler2d",
             "c1_mhd3d": "c1_mhd3d", "c1_mhd3d_nograv": "c1_mhd3d", "c0_polar": "c0_kepler2d",
-            "c1_polar": "c1_mhd2d", "c1_polar3d": "c1_mhd3d"}
+            "c1_polar": "c1_mhd2d", "c1_polar3d": "c1_mhd3d", "c0_outflow3d": "c0_kepler2d",
+            "c1_omk3d": "c1_mhd3d", "c1_accrete3d": "c1_mhd3d"}
 
 
 def par_text(cfg_par, overrides):

@@ -1,13 +1,23 @@
-"""Grids down to the axis (NoBC_Rmin 1, R_Min 0) with the polar boundary
-module (Boundary/polar.c), against the reference binary: no inner ghosts,
-the first annulus's r slopes fixed by plm_geom_boundary -> geom_grad
-(plm.c:184-185, cylindrical.c:141-173), the polar source terms (euler.c,
-mhd.c, planet.c with NoBC_Rmin), and the outer r and z ghosts re-evaluated
-from the Initial module each substep.  2D hydro, 2D MHD with constrained
-transport and 3D MHD with constrained transport, rigid rotation without
-gravity.  The polar source terms call sin(dphi/2), whose CUDA and glibc
-values may differ in the last bit, so the state is compared at 1e-12
-relative L1 (in practice far below); the face lists bit for bit."""
+"""Boundary modules beyond fixed / fixed3d / zerograd, against the reference
+binary built with the same module (rigid rotation without gravity, so the
+fixtures depend on no libm call except where noted):
+
+- polar (Boundary/polar.c) on grids down to the axis (NoBC_Rmin 1, R_Min 0):
+  no inner ghosts, the first annulus's r slopes fixed by plm_geom_boundary ->
+  geom_grad (plm.c:184-185, cylindrical.c:141-173), the polar source terms
+  (euler.c, mhd.c, planet.c with NoBC_Rmin; they call sin(dphi/2), whose
+  CUDA and glibc values may differ in the last bit), and the outer r and z
+  ghosts re-evaluated from the Initial module each substep.  2D hydro, 2D
+  MHD with CT, 3D MHD with CT.
+- outflow3d: zero-gradient copies with the outflow diode on every side
+  (boundary_functions.c:269-440), 3D hydro.
+- zerograd_omk: the same with Omega of the r ghosts from the Initial module
+  (boundary_fixed_q_rinn / _rout), 3D MHD.
+- accrete3d: outflow inner r, fixed outer r and z (set_cell_init), 3D MHD
+  with CT.
+
+State compared at 1e-12 relative L1 (in practice far below), face lists bit
+for bit, ghost cells included at set-up."""
 import os
 
 import numpy as np
@@ -18,15 +28,17 @@ from helpers import case_disk, observed_slots, par_with, rel_l1, rel_l1_cols
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["c0_polar", "c1_polar_ct", "c1_polar3d"]
+POLAR = ["c0_polar", "c1_polar_ct", "c1_polar3d"]
+CASES = POLAR + ["c0_outflow3d", "c1_omk3d", "c1_accrete3d"]
 TOL = 1e-12
 
 
 @pytest.mark.parametrize("case", CASES)
-def test_polar_setup(case):
-    """setupCells and the polar boundary's ghost values on the device."""
+def test_module_setup(case):
+    """setupCells and the module's ghost values on the device."""
     disk, g = case_disk(case)
-    assert disk.Ng[0] == 0 and disk.r_jph[0] == 0.0
+    if case in POLAR:
+        assert disk.Ng[0] == 0 and disk.r_jph[0] == 0.0
     b = db.Batch([disk])
     st = b.get_cells()
     r = disk.real == 1
@@ -40,7 +52,7 @@ def test_polar_setup(case):
 
 
 @pytest.mark.parametrize("case", CASES)
-def test_polar_steps(case):
+def test_module_steps(case):
     disk, g = case_disk(case)
     b = db.Batch([disk], setup=False)
     b.set_cells(g["s0_prim"], g["s0_cons"], g["s0_piph"], g["s0_dphi"], g["s0_wiph"], g["real"],
@@ -61,9 +73,12 @@ def test_polar_steps(case):
     ec = rel_l1_cols(st["cons"][r], g["sN_cons"][r])
     print("%s: prim %.2e cons %.2e" % (case, max(ep), max(ec)))
     assert max(ep) <= TOL and max(ec) <= TOL
-    # the axis annulus itself (its slopes are the geometric ones)
-    a0 = slice(0, int(disk.Np[0]))
-    assert max(rel_l1_cols(st["prim"][a0], g["sN_prim"][a0])) <= TOL
+    # the axis annulus itself (its slopes are the geometric ones); the ghosts
+    if case in POLAR:
+        a0 = slice(0, int(disk.Np[0]))
+        assert max(rel_l1_cols(st["prim"][a0], g["sN_prim"][a0])) <= TOL
+    gh = ~r
+    assert max(rel_l1_cols(st["prim"][gh], g["sN_prim"][gh])) <= TOL
     if "sN_Phi" in g:
         m = observed_slots(disk, b.num_faces)
         for s in range(m.shape[1]):
