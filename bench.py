@@ -43,6 +43,14 @@ def peaks():
         return 6650.0, "fallback"
 
 
+# dram__bytes_read.sum + dram__bytes_write.sum of one first-substep launch on
+# the ragged8 workload (1,049,795 cells, 2,089,252 r-faces), from the ncu
+# captures summarised in profiles/k_update_ragged8_fp64.md and
+# profiles/k_flux_t_ragged8_fp64.md: (bytes, units the launch processed)
+DRAM_UPDATE_RAGGED8 = (289.8e6 + 53.7e6, 1049795)
+DRAM_FLUX_RAGGED8 = (216.2e6 + 72.5e6, 2089252)
+
+
 def kernel_bytes(name, first, N, Nf, Na):
     """Algorithmic (compulsory, each element once) HBM bytes of one launch.
     N cells, Nf r-faces, Na annuli; Q doubles per cell."""
@@ -584,16 +592,15 @@ def run_ours(args, world, rank, local):
         byt[name] = byt.get(name, 0) + kernel_bytes(name, first, ncell, nf, na)
     dom = max(tot, key=tot.get)
     achieved = byt[dom] / (tot[dom] / 1e3) / 1e9
+    # DRAM bytes of one launch of the dominant kernel: the ncu capture of the
+    # same kernel on the smaller ragged8 workload, scaled by the cells (r-faces
+    # for k_flux_r) one launch here processes -- the ragged workloads' traffic
+    # grows with the cells, each cell's state crossing HBM once
+    per_unit = {"k_update": (DRAM_UPDATE_RAGGED8, "cells"), "k_flux_r": (DRAM_FLUX_RAGGED8, "faces")}
     traffic = None
-    tfile = os.path.join(REPO, "profiles", "traffic.json")
-    if os.path.exists(tfile):
-        try:
-            tj = json.load(open(tfile))
-            ent = tj.get(args.workload, {}).get(dom)
-            if ent:
-                traffic = ent["bytes_per_launch"]
-        except Exception:
-            traffic = None
+    if dom in per_unit and args.workload.startswith("ragged"):
+        (b8, units8), kind = per_unit[dom]
+        traffic = b8 / units8 * (ncell if kind == "cells" else nf)
     step_gbs = B_ALG_STEP * (value / world) / 1e9
 
     # end to end through the C ABI with host buffers: upload the state from
@@ -695,6 +702,10 @@ def run_ours(args, world, rank, local):
                        "parallelism": "independent disks per GPU" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                         "traffic_source": ("ncu dram bytes of one launch on ragged8, scaled by the "
+                                            "units processed (profiles/%s_ragged8_fp64.md)"
+                                            % ("k_update" if dom == "k_update" else "k_flux_t"))
+                         if traffic is not None else None,
                          "peak_kind": peak_kind},
             "step_roofline": {"bytes_per_zone_update": B_ALG_STEP, "achieved": step_gbs, "peak": hbm,
                               "unit": "GB/s", "frac": step_gbs / hbm},
