@@ -65,6 +65,8 @@ class Params(C.Structure):
         ("Disk_Mach", C.c_double), ("Mass_Ratio", C.c_double),
         ("grav2D", C.c_int), ("CT", C.c_int), ("initPar0", C.c_int),
         ("initPar", C.c_double * 9), ("metricPar", C.c_double * 5), ("t_min", C.c_double),
+        ("include_atmos", C.c_int), ("noiseType", C.c_int), ("noiseAbs", C.c_double),
+        ("noiseRel", C.c_double),
     ]
 
 
@@ -118,6 +120,8 @@ def library():
         "disco_setup_phi": (_I, [C.POINTER(Params), _I, _I, _IP, _IP, _D, _D, _IP]),
         "disco_sizeof": (_I, [_I]),
         "disco_batch_set_time": (_I, [_P, _I, C.c_double]),
+        "disco_batch_set_noise": (_I, [_P, _D]),
+        "disco_setup_noise": (_I, [C.POINTER(Params), _I, _I, _IP, _IP, _D]),
         "disco_batch_get_planets": (_I, [_P, _I, _D, _I, _IP]),
         "disco_batch_set_planets": (_I, [_P, _I, _D, _I]),
         "disco_batch_restart_cells": (_I, [_P, _D, _D, _D]),
@@ -194,6 +198,12 @@ class Disk:
         _check(lib.disco_setup_phi(C.byref(params), self.Nr, self.Nz, iptr(self.Ng), iptr(self.Np),
                                    dptr(self.piph), dptr(self.dphi), iptr(self.real)),
                "disco_setup_phi")
+        # addNoise's draws (Noise_Type 1-3), from the same rand() stream
+        self.noise = None
+        if params.noiseType in (1, 2, 3):
+            self.noise = np.zeros((self.ncell, 4))
+            _check(lib.disco_setup_noise(C.byref(params), self.Nr, self.Nz, iptr(self.Ng),
+                                         iptr(self.Np), dptr(self.noise)), "disco_setup_noise")
 
     @classmethod
     def from_files(cls, par_path, opt_path):
@@ -241,6 +251,7 @@ class Batch:
             real = np.concatenate([d.real for d in self.disks]).astype(np.int32)
             _check(lib.disco_batch_set_cells(self.h, None, None, dptr(piph), dptr(dphi), None,
                                              iptr(real), None), "disco_batch_set_cells")
+            self._upload_noise()
             _check(lib.disco_batch_setup_cells(self.h), "disco_batch_setup_cells")
 
     def close(self):
@@ -376,6 +387,15 @@ class Batch:
         _check(library().disco_batch_report(self.h, disk, dptr(out)), "disco_batch_report")
         return out
 
+    def _upload_noise(self):
+        """addNoise's draws of every disk with Noise_Type 1-3 (zeros for the others)."""
+        if all(d.noise is None for d in self.disks):
+            return
+        nz = np.concatenate([d.noise if d.noise is not None else np.zeros((d.ncell, 4))
+                             for d in self.disks])
+        _check(library().disco_batch_set_noise(self.h, dptr(np.ascontiguousarray(nz))),
+               "disco_batch_set_noise")
+
     def set_time(self, t, disk=0):
         """Set the disk's simulation time (a restart's T)."""
         _check(library().disco_batch_set_time(self.h, disk, float(t)), "disco_batch_set_time")
@@ -406,6 +426,7 @@ class Batch:
         Phi = None if Phi is None else np.ascontiguousarray(Phi, np.float64)
         if prim.shape != (self.ncell, self.q) or piph.shape != (self.ncell,):
             raise ValueError("restart_cells: prim must be ncell x q, piph ncell")
+        self._upload_noise()
         _check(library().disco_batch_restart_cells(self.h, dptr(prim), dptr(Phi), dptr(piph)),
                "disco_batch_restart_cells")
 

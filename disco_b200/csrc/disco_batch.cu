@@ -74,6 +74,9 @@ static void fill_disk_params(DiskParams &D, const disco_params &p, const disco_m
    D.mesh_om = p.Exact_Mesh_Omega; D.isothermal = p.isothermal_flag;
    D.cs2_profile = p.Cs2_Profile; D.grav2D = p.grav2D; D.polar = p.NoBC_Rmin == 1;
    D.timestep = p.Timestep;
+   D.atmos = p.include_atmos ? 1 : 0;
+   D.noise_type = (p.noiseType >= 1 && p.noiseType <= 3) ? p.noiseType : 0;
+   D.noise_abs = p.noiseAbs; D.noise_rel = p.noiseRel;
    D.rotframe = p.RotFrame;
    D.planets_move = (m.planets == DISCO_PLANETS_CM2 || m.planets == DISCO_PLANETS_BINARY_SOFT);
    D.ic.mach = p.Disk_Mach; D.ic.amp = p.initPar[1];
@@ -195,6 +198,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
                  mods->boundary == DISCO_BC_ACCRETE3D;
    b->zg_omk = mods->boundary == DISCO_BC_ZEROGRAD_OMK;
    b->d_zg_side = NULL;
+   b->d_noise = NULL;
    b->d_zg_pairs = NULL;
    b->zg_smem = 0;
    b->nq = mods->analysis == DISCO_DIAG_DISK2D ? 5 : 0;
@@ -595,8 +599,30 @@ static int launch_mindt(disco_batch *b){
    return cuda_status(cudaGetLastError());
 }
 
+/* a disk with Noise_Type 1-3 needs its addNoise draws (disco_batch_set_noise) */
+static bool noise_missing(const disco_batch *b){
+   if( b->vd.noise ) return false;
+   for( int d=0 ; d<b->ndisk ; ++d ) if( b->dparams[d].noise_type ) return true;
+   return false;
+}
+
+extern "C" int disco_batch_set_noise(disco_batch *b, const double *noise){
+   if( !b ) return DISCO_ERR_ARG;
+   CK(cudaSetDevice(b->device));
+   if( !noise ){ b->vd.noise = NULL; b->vf.noise = NULL; return DISCO_OK; }
+   size_t bytes = sizeof(double)*4*(size_t)b->ncell;
+   if( !b->d_noise ){
+      b->d_noise = (double *)dalloc_bytes(b, bytes);
+      if( !b->d_noise ) return DISCO_ERR_CUDA;
+   }
+   CK(xfer(b, b->d_noise, noise, bytes, cudaMemcpyHostToDevice));
+   b->vd.noise = b->d_noise; b->vf.noise = b->d_noise;
+   return DISCO_OK;
+}
+
 extern "C" int disco_batch_setup_cells(disco_batch *b){
    if( !b ) return DISCO_ERR_ARG;
+   if( noise_missing(b) ) return DISCO_ERR_STATE;
    CK(cudaSetDevice(b->device));
    CK(cudaMemsetAsync(b->vd.topo, 0, sizeof(int), b->stream));
    if( b->prec == DISCO_PREC_MIXED ) mixed_launch_setup(b);
@@ -741,6 +767,7 @@ extern "C" int disco_batch_set_time(disco_batch *b, int disk, double t){
 extern "C" int disco_batch_restart_cells(disco_batch *b, const double *prim, const double *Phi,
                                          const double *piph){
    if( !b || !prim || !piph || (b->ct && !Phi) ) return DISCO_ERR_ARG;
+   if( noise_missing(b) ) return DISCO_ERR_STATE;
    CK(cudaSetDevice(b->device));
    size_t N = b->ncell;
    int s;

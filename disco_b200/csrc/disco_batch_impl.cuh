@@ -52,6 +52,7 @@ struct disco_batch {
    double *d_Qrz;
    double *d_stage;          /* Q x ncell FP64, set/get_cells staging (lazy) */
    double *d_rpart, *d_rout; /* report partials per cell block, lines per disk (lazy) */
+   double *d_noise;          /* addNoise draws, 4 per cell (lazy) */
    int *d_err;
    cudaStream_t stream;
    cudaStream_t own_stream;

@@ -53,7 +53,10 @@ struct DiskParams {
    int face_r0;       /* first global r-face */
    int trz0, ntrz;    /* first global z-track, count (Nr*(Nz-1)) */
    int ln0;           /* first global (r, z) edge line, (Nr-1)*(Nz-1) of them (3D CT) */
-   int pad_ln;
+   int atmos;         /* Include_Atmos: adjust_gas at set-up */
+   int noise_type;    /* Noise_Type 0..3 (addNoise) */
+   int pad_noise;
+   double noise_abs, noise_rel;
    int npl;
    int ic_module;     /* DISCO_IC_KEPLER_NOISE or DISCO_IC_MHD_SHEAR_NOISE */
    int pad_ic;
@@ -692,6 +695,36 @@ __device__ __forceinline__ double fgrav(double M, double r, double eps, int type
       return( M*r/(x*sqrt(x)) );
    }
    return 0.0;
+}
+/* adjust_gas (planet.c:76-96) with phigrav of a point mass, PHI_ORDER 2
+ * (planet.c:36-42): the set-up gas of Include_Atmos */
+__device__ __forceinline__ void adjust_gas(const Planet &pl, const double *x, double *prim, double gam){
+   double r = x[0], phi = x[1];
+   double cosp = cos(phi), sinp = sin(phi);
+   double dx = r*cosp - pl.r*cos(pl.phi);
+   double dy = r*sinp - pl.r*sin(pl.phi);
+   double script_r = sqrt(dx*dx + dy*dy);
+   double pot = pl.type == 0 ? pl.M/pow(pow(script_r, 2.0) + pow(pl.eps, 2.0), 1./2.0) : 0.0;
+   double c2 = gam*prim[PPP]/prim[RHO];
+   double factor = 1. + (gam-1.)*pot/c2;
+   prim[RHO] *= factor;
+   prim[PPP] *= pow(factor, gam);
+}
+/* addNoise (noise.c:15-50) with the cell's draws x[0..3] (made on the host
+ * from glibc's rand() in the reference's order); cylindrical covariant
+ * phi velocity r*Omega for type 3 (geometry_functions.c:19-24) */
+__device__ __forceinline__ void add_noise(int type, double absMag, double relMag, double *prim,
+                                          const double *x, const double *xr){
+   if( type == 1 ){
+      prim[URR] = (1.0+xr[0]*relMag)*prim[URR] + xr[1]*absMag;
+      prim[UPP] = (1.0+xr[2]*relMag)*prim[UPP] + xr[3]*absMag;
+   }else if( type == 2 ){
+      prim[PPP] = (1.0+xr[0]*relMag)*prim[PPP] + xr[1]*absMag;
+   }else if( type == 3 ){
+      double Vc1 = prim[UPP]*x[0];
+      prim[URR] = xr[0]*relMag*Vc1 + xr[1]*absMag;
+      prim[UZZ] = xr[2]*relMag*Vc1 + xr[3]*absMag;
+   }
 }
 /* planetaryForce(), planet.c:99-150, modes 0 and 1 */
 __device__ __forceinline__ void planetary_force(int grav2D, const Planet &pl, double r,

@@ -106,6 +106,7 @@ struct ViewT {
    int *consL, *consR;                /* r-tracks outside / inside the cell */
    int *consZL, *consZR;              /* z-tracks above / below the cell */
    double *diag_part;   /* per cell block: nq sums + volume */
+   const double *noise; /* addNoise draws, 4 per cell (set-up and restart), or NULL */
    /* *topo = 1 when the face lists and geometry were built from the current
     * piph (the second RK2 substep builds them after the cells have moved, so
     * the next step's first substep, with the same piph, keeps them and only
@@ -1608,6 +1609,10 @@ __global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc){
       double x[3] = {r, piph - .5*dphi, z};
       initial<Q,NC>(P, prim, x);
       if( P.rotframe ) prim[UPP] -= P.RotOmega;
+      if( P.atmos )                                   /* domain.c:193-200 */
+         for( int p=0 ; p<P.npl ; ++p ) adjust_gas(v.ds[d].pl[p], x, prim, P.gam);
+      if( P.noise_type && v.noise )                   /* domain.c:202-203 */
+         add_noise(P.noise_type, P.noise_abs, P.noise_rel, prim, x, v.noise + 4*(size_t)c);
       double om = get_om(P, r);
       prim2cons<Q,NC,double>(P, prim, cons, r, om, dV);
       /* with CT, cons2prim follows set_B_fields (domain.c:211-237): k_c2p */
@@ -1673,6 +1678,10 @@ __global__ void __launch_bounds__(CB) k_restart(ViewT<R> v, int bc){
       double dV = dV_of(rj[j], rj[j-1], dph, zk[k], zk[k-1]);
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N+c];
+      if( P.noise_type && v.noise ){                  /* domain.c:202-203, restart too */
+         double x[3] = {r, piph - .5*dphi, z};
+         add_noise(P.noise_type, P.noise_abs, P.noise_rel, prim, x, v.noise + 4*(size_t)c);
+      }
       double om = get_om(P, r);
       prim2cons<Q,NC,double>(P, prim, cons, r, om, dV);
       cons2prim<Q,NC>(P, cons, prim, r, om, dV);

@@ -386,6 +386,23 @@ extern "C" int disco_batch_restart(disco_batch *b, const char *const *paths){
       disco_npz_close(z);
       if( s ) return s;
    }
+   /* setupCells adds noise on restart as well (domain.c:202-203): the same
+    * draws as at the start, from glibc's rand() stream */
+   bool any_noise = false;
+   for( int d=0 ; d<b->ndisk ; ++d ) any_noise = any_noise || b->dparams[d].noise_type;
+   if( any_noise ){
+      std::vector<double> nz((size_t)4*N, 0.0);
+      for( int d=0 ; d<b->ndisk ; ++d ){
+         if( !b->dparams[d].noise_type ) continue;
+         const DiskParams &D = b->dparams[d];
+         int Ng[4] = {D.NgRa, D.NgRb, D.NgZa, D.NgZb};
+         size_t c0, n;
+         disk_cells(b, d, &c0, &n);
+         CKS(disco_setup_noise(&b->params[d], D.Nr, D.Nz, Ng, b->ann_np.data() + D.ann0,
+                               nz.data() + 4*c0));
+      }
+      CKS(disco_batch_set_noise(b, nz.data()));
+   }
    for( int d=0 ; d<b->ndisk ; ++d ){
       CKS(disco_batch_set_time(b, d, T[d]));
       CKS(disco_batch_set_planets(b, d, pl[d].data(), b->dparams[d].npl));

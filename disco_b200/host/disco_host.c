@@ -79,7 +79,7 @@ int disco_read_par(const char *path, disco_params *p, int *nmissing){
    RI("Initial_Regrid", tmp);        RI("Restart", tmp);
    RI("Use_Viscosity", p->visc_flag); RD("Viscosity", p->viscosity);
    RI("Use_As_Alpha", p->alpha_flag);
-   RI("Include_Atmos", tmp);
+   RI("Include_Atmos", p->include_atmos);
    RI("T_Times_2pi", tT);            RI("P_Times_2pi", pT);
    RI("Z_Times_pi", zT);
    RD("Mach_Number", p->Disk_Mach);  RD("Mass_Ratio", p->Mass_Ratio);
@@ -95,6 +95,8 @@ int disco_read_par(const char *path, disco_params *p, int *nmissing){
    RD("Init_Par3", p->initPar[3]);   RD("Init_Par4", p->initPar[4]);
    RD("Init_Par5", p->initPar[5]);   RD("Init_Par6", p->initPar[6]);
    RD("Init_Par7", p->initPar[7]);   RD("Init_Par8", p->initPar[8]);
+   RI("Noise_Type", p->noiseType);
+   RD("Noise_Abs", p->noiseAbs);     RD("Noise_Rel", p->noiseRel);
 #undef RI
 #undef RD
    /* readpar.c:162-172 */
@@ -217,9 +219,46 @@ int disco_setup_grid(const disco_params *p, int *pNr, int *pNz, int *Ng,
    return DISCO_OK;
 }
 
+/* The draws of addNoise (noise.c:15-50) for each real cell, in setupCells'
+ * order (domain.c:183-205: k, then j, then i), continuing glibc's rand()
+ * stream where setupDomain left it: 4 per cell for types 1 and 3, 2 for
+ * type 2, each 2*rand()/RAND_MAX - 1. */
+static void noise_draws(const disco_params *p, int Nr, int Nz, const int *Ng, const int *Np,
+                        const int *coff, double *noise){
+   int per = p->noiseType == 2 ? 2 : (p->noiseType == 1 || p->noiseType == 3) ? 4 : 0;
+   int j, k, i, m;
+   for( k=Ng[2] ; k<Nz-Ng[3] ; ++k ) for( j=Ng[0] ; j<Nr-Ng[1] ; ++j ){
+      int jk = j + Nr*k;
+      for( i=0 ; i<Np[jk] ; ++i ) for( m=0 ; m<per ; ++m )
+         noise[4*(coff[jk]+i) + m] = 2 * ((double)rand() / (double)(RAND_MAX)) - 1;
+   }
+}
+
+static int setup_phi(const disco_params *p, int Nr, int Nz, const int *Ng,
+                     const int *Np, double *piph, double *dphi, int *real, double *noise);
+
 /* domain.c:172-233 (serial), then calc_dp (misc.c:271-288). */
 int disco_setup_phi(const disco_params *p, int Nr, int Nz, const int *Ng,
                     const int *Np, double *piph, double *dphi, int *real){
+   return setup_phi(p, Nr, Nz, Ng, Np, piph, dphi, real, NULL);
+}
+
+int disco_setup_noise(const disco_params *p, int Nr, int Nz, const int *Ng,
+                      const int *Np, double *noise){
+   if( !p || !Ng || !Np || !noise ) return DISCO_ERR_ARG;
+   size_t n = 0;
+   int jk;
+   for( jk=0 ; jk<Nr*Nz ; ++jk ) n += (size_t)Np[jk];
+   double *piph = malloc(sizeof(double)*(n ? n : 1)), *dphi = malloc(sizeof(double)*(n ? n : 1));
+   if( !piph || !dphi ){ free(piph); free(dphi); return DISCO_ERR_ARG; }
+   memset(noise, 0, sizeof(double)*4*n);
+   int s = setup_phi(p, Nr, Nz, Ng, Np, piph, dphi, NULL, noise);
+   free(piph); free(dphi);
+   return s;
+}
+
+static int setup_phi(const disco_params *p, int Nr, int Nz, const int *Ng,
+                     const int *Np, double *piph, double *dphi, int *real, double *noise){
    if( !p || !Ng || !Np || !piph || !dphi ) return DISCO_ERR_ARG;
    double Pmax = p->phimax;
    const int NG = 2;
@@ -250,6 +289,7 @@ int disco_setup_phi(const disco_params *p, int Nr, int Nz, const int *Ng,
       }
       for( j=N0r+Nr ; j<N0r_glob+Nr_glob ; ++j ) rand();                  /* :227-231 */
    }
+   if( noise ) noise_draws(p, Nr, Nz, Ng, Np, coff, noise);
    for( j=0 ; j<Nr*Nz ; ++j ){
       for( i=0 ; i<Np[j] ; ++i ){
          int im = i==0 ? Np[j]-1 : i-1;

@@ -59,6 +59,8 @@ static void fill_params(const struct domain *d, disco_params *p){
    p->metricPar[1] = L->metricPar1; p->metricPar[2] = L->metricPar2;
    p->metricPar[3] = L->metricPar3; p->metricPar[4] = L->metricPar4;
    p->t_min = d->t;
+   p->include_atmos = L->include_atmos;
+   p->noiseType = L->noiseType; p->noiseAbs = L->noiseAbs; p->noiseRel = L->noiseRel;
 }
 
 static void fail(const char *what, int s){

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define DISCO_ABI_VERSION 1
+#define DISCO_ABI_VERSION 2
 
 enum disco_status {
    DISCO_OK = 0,
@@ -103,6 +103,12 @@ typedef struct disco_params {
    double initPar[9];          /* initPar[1..8] = Init_Par1..8; [0] unused */
    double metricPar[5];        /* metricPar[1..4] = Metric_Par1..4 */
    double t_min;
+   /* set-up options of setupCells (domain.c:144-205): Include_Atmos
+    * (adjust_gas, planet.c:76-96) and Noise_Type / Noise_Abs / Noise_Rel
+    * (addNoise, noise.c:15-50) */
+   int    include_atmos;
+   int    noiseType;
+   double noiseAbs, noiseRel;
 } disco_params;
 
 typedef struct disco_batch disco_batch;   /* opaque device-resident batch */
@@ -165,6 +171,18 @@ int disco_batch_get_cells(disco_batch *b, double *prim, double *cons,
  * been uploaded (the reference draws them from rand(), domain.c:206-233).
  */
 int disco_batch_setup_cells(disco_batch *b);
+
+/*
+ * The random numbers of addNoise (noise.c:15-50) for in.par Noise_Type 1-3:
+ * 4 doubles per cell (annulus order, disk-major), made on the host by
+ * disco_setup_noise (include/disco_host.h) from glibc's rand() stream in
+ * the reference's cell order.  setupCells applies them after the Initial
+ * module (and adjust_gas), and again on restart, so set them before
+ * disco_batch_setup_cells / _restart_cells of a batch with noise (those
+ * return DISCO_ERR_STATE otherwise); disco_batch_restart makes them itself.
+ * NULL clears them.
+ */
+int disco_batch_set_noise(disco_batch *b, const double *noise);
 
 /* getmindt (misc.c:39-84) for every disk: dt[d] = CFL * min over real cells. */
 int disco_batch_mindt(disco_batch *b, double *dt);

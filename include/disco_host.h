@@ -49,6 +49,16 @@ int disco_setup_grid(const disco_params *p, int *Nr, int *Nz, int *Ng,
 int disco_setup_phi(const disco_params *p, int Nr, int Nz, const int *Ng,
                     const int *Np, double *piph, double *dphi, int *real);
 
+/*
+ * The random numbers addNoise (noise.c:15-50) draws for Noise_Type 1, 2 or
+ * 3: glibc's rand() stream of disco_setup_phi continued, in setupCells'
+ * cell order (domain.c:183-205, real cells only), each 2*rand()/RAND_MAX-1.
+ * noise[4*c + m] for cell c (annulus order), m < 4 (2 for type 2); zero
+ * elsewhere.  Upload with disco_batch_set_noise before set-up or restart.
+ */
+int disco_setup_noise(const disco_params *p, int Nr, int Nz, const int *Ng,
+                      const int *Np, double *noise);
+
 /* sizeof(disco_params) for which = 0, sizeof(disco_modules) for 1: lets a
  * foreign-language mirror of the structs check its layout. */
 int disco_sizeof(int which);

@@ -95,6 +95,20 @@ CASES = {
     "c1_omk3d": ("c1_omk3d", {"Num_R": 8, "Num_Z": 6, "Init_Par2": 1, "Init_Par4": 10.0}, 5),
     "c1_accrete3d": ("c1_accrete3d", {"Num_R": 8, "Num_Z": 6, "Init_Par2": 1, "Init_Par4": 10.0,
                                       "Constrained_Transport": 1, "Init_Par5": 20.0}, 5),
+    # setupCells options: addNoise (noise.c, glibc rand() in cell order)
+    # types 1 (v_r, Omega), 2 (P) and 3 (v_r, v_z from r Omega), libm-free;
+    # Include_Atmos (adjust_gas with the binary's potential)
+    "c0_noise1": ("c0_nograv", {"Num_R": 16, "Log_Zoning": 0, "Init_Par2": 1, "Energy_Omega": 0,
+                                "Mach_Number": 5.0, "Noise_Type": 1, "Noise_Abs": 1.0e-3,
+                                "Noise_Rel": 1.0e-2}, 6),
+    "c0_noise2": ("c0_nograv", {"Num_R": 16, "Log_Zoning": 0, "Init_Par2": 1, "Energy_Omega": 0,
+                                "Mach_Number": 5.0, "Noise_Type": 2, "Noise_Abs": 1.0e-4,
+                                "Noise_Rel": 2.0e-2}, 6),
+    "c1_noise3": ("c1_mhd3d_nograv", {"Num_R": 8, "Num_Z": 6, "Init_Par2": 1, "Init_Par4": 10.0,
+                                      "Noise_Type": 3, "Noise_Abs": 1.0e-3,
+                                      "Noise_Rel": 1.0e-2}, 5),
+    "c0_atmos": ("c0_cm2", {"Num_R": 24, "Mass_Ratio": 1.0e-3, "Energy_Omega": 0,
+                            "Include_Atmos": 1}, 6),
 }
 
 # the in.par template each module configuration starts from
@@ -129,6 +143,10 @@ CKPT_CASES = {
     "ck_ct_rigid": ("c1_mhd2d_nograv", {"Num_R": 14, "Init_Par2": 1, "Init_Par4": 10.0,
                                         "Constrained_Transport": 1, "Init_Par5": 20.0,
                                         "Init_Par6": 0.05}, 8, 4),
+    # setupCells adds noise on restart too (domain.c:202-203)
+    "ck_noise": ("c0_nograv", {"Num_R": 16, "Log_Zoning": 0, "Init_Par2": 1, "Energy_Omega": 0,
+                               "Mach_Number": 5.0, "Noise_Type": 1, "Noise_Abs": 1.0e-3,
+                               "Noise_Rel": 1.0e-2}, 6, 3),
     "ck_ct3d_rigid": ("c1_mhd3d_nograv", {"Num_R": 6, "Num_Z": 5, "Init_Par2": 1,
                                           "Init_Par4": 10.0, "Constrained_Transport": 1,
                                           "Init_Par5": 20.0, "Init_Par6": 0.05}, 4, 3),

@@ -79,7 +79,7 @@ def rel_l1_cols(a, b):
     return [rel_l1(a[:, q], b[:, q]) for q in range(a.shape[1])]
 
 
-CKPT_CASES = ["ck_cm2", "ck_rigid", "ck_ct_rigid", "ck_ct3d_rigid"]
+CKPT_CASES = ["ck_cm2", "ck_rigid", "ck_ct_rigid", "ck_ct3d_rigid", "ck_noise"]
 CK_NAMES = {"T": "Grid/T", "r_jph": "Grid/r_jph", "z_kph": "Grid/z_kph", "Index": "Grid/Index",
             "Np": "Grid/Np", "Id_phi0": "Grid/Id_phi0", "Cells": "Data/Cells",
             "Planets": "Data/Planets", "Diagnostics": "Data/Diagnostics"}

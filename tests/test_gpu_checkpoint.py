@@ -29,7 +29,7 @@ from helpers import (CKPT_CASES, CK_NAMES, GOLDEN, TEMPLATES, ck_to_npz, golden,
 
 pytestmark = pytest.mark.gpu
 
-EXACT = {"ck_rigid", "ck_ct_rigid", "ck_ct3d_rigid"}
+EXACT = {"ck_rigid", "ck_ct_rigid", "ck_ct3d_rigid", "ck_noise"}
 TOL = 1e-11            # point-mass force: CUDA's libm against glibc's, as the other fixtures
 
 
