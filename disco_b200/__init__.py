@@ -34,7 +34,7 @@ HYDRO = {"euler": 0, "mhd": 1}
 BOUNDARY = {"fixed": 0, "zerograd": 1, "fixed3d": 2, "polar": 3, "outflow3d": 4, "zerograd_omk": 5,
             "accrete3d": 6}
 PLANETS = {"none": 0, "sun": 1, "cm2": 2, "binary_soft": 3}
-INITIAL = {"kepler_noise": 0, "mhd_shear_noise": 1}
+INITIAL = {"kepler_noise": 0, "mhd_shear_noise": 1, "host": 2}
 PREC_FP64, PREC_MIXED = 0, 1
 
 

@@ -173,7 +173,12 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
     * with inner ghosts their prims would never be set */
    if( mods->boundary == DISCO_BC_POLAR )
       for( int d=0 ; d<ndisk ; ++d ) if( Ng[4*d+0] != 0 ) return DISCO_ERR_UNSUPPORTED;
-   if( mods->initial != DISCO_IC_KEPLER_NOISE && mods->initial != DISCO_IC_MHD_SHEAR_NOISE )
+   if( mods->initial != DISCO_IC_KEPLER_NOISE && mods->initial != DISCO_IC_MHD_SHEAR_NOISE &&
+       mods->initial != DISCO_IC_HOST )
+      return DISCO_ERR_UNSUPPORTED;
+   /* a host-evaluated Initial module cannot refill ghosts on the device */
+   if( mods->initial == DISCO_IC_HOST && mods->boundary != DISCO_BC_ZEROGRAD &&
+       mods->boundary != DISCO_BC_OUTFLOW3D )
       return DISCO_ERR_UNSUPPORTED;
    for( int d=0 ; d<ndisk ; ++d ){
       if( Nr[d] < 2 ) return DISCO_ERR_ARG;
@@ -622,6 +627,7 @@ extern "C" int disco_batch_set_noise(disco_batch *b, const double *noise){
 
 extern "C" int disco_batch_setup_cells(disco_batch *b){
    if( !b ) return DISCO_ERR_ARG;
+   if( b->mods.initial == DISCO_IC_HOST ) return DISCO_ERR_UNSUPPORTED;   /* set up on the host */
    if( noise_missing(b) ) return DISCO_ERR_STATE;
    CK(cudaSetDevice(b->device));
    CK(cudaMemsetAsync(b->vd.topo, 0, sizeof(int), b->stream));

@@ -154,7 +154,7 @@ int disco_read_opt(const char *path, disco_modules *m){
    if( opt_value(path, "INITIAL", v, sizeof v) ) return DISCO_ERR_ARG;
    if( !strcmp(v, "kepler_noise") ) m->initial = DISCO_IC_KEPLER_NOISE;
    else if( !strcmp(v, "mhd_shear_noise") ) m->initial = DISCO_IC_MHD_SHEAR_NOISE;
-   else return DISCO_ERR_UNSUPPORTED;
+   else m->initial = DISCO_IC_HOST;      /* another module: its state comes from the host */
    if( opt_value(path, "ANALYSIS", v, sizeof v) ) m->analysis = DISCO_DIAG_NONE;
    else if( !strcmp(v, "diag_disk2d") ) m->analysis = DISCO_DIAG_DISK2D;
    else m->analysis = DISCO_DIAG_NONE;

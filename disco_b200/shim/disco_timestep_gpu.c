@@ -80,6 +80,9 @@ static void gpu_init(struct domain *d){
    m.boundary = module_id(BOUNDARY, bcs, 7);
    m.planets = module_id(PLANETS, pls, 4);
    m.initial = module_id(INITIAL, ics, 2);
+   /* any other Initial module: setupCells evaluated it here on the host, and
+    * boundaries that do not call it again (zerograd, outflow3d) run as is */
+   if( m.initial < 0 ) m.initial = DISCO_IC_HOST;
    m.analysis = strcmp(ANALYSIS, "diag_disk2d") == 0 ? DISCO_DIAG_DISK2D : DISCO_DIAG_NONE;
    m.num_c = NUM_C; m.num_n = NUM_N; m.ct_mode = CT_MODE;
    if( m.hydro < 0 || m.boundary < 0 || m.planets < 0 || m.initial < 0 )

@@ -59,7 +59,11 @@ enum disco_boundary { DISCO_BC_FIXED = 0, DISCO_BC_ZEROGRAD = 1, DISCO_BC_FIXED3
                       DISCO_BC_ACCRETE3D = 6 };
 enum disco_planets  { DISCO_PLANETS_NONE = 0, DISCO_PLANETS_SUN = 1, DISCO_PLANETS_CM2 = 2,
                       DISCO_PLANETS_BINARY_SOFT = 3 };
-enum disco_initial  { DISCO_IC_KEPLER_NOISE = 0, DISCO_IC_MHD_SHEAR_NOISE = 1 };
+/* DISCO_IC_HOST: the Initial module is the host's own (a drop-in evaluating
+ * any reference IC in setupCells): the state must come from set_cells, and
+ * only boundaries that never re-evaluate initial() during the steps
+ * (zerograd, outflow3d) are accepted. */
+enum disco_initial  { DISCO_IC_KEPLER_NOISE = 0, DISCO_IC_MHD_SHEAR_NOISE = 1, DISCO_IC_HOST = 2 };
 enum disco_analysis { DISCO_DIAG_NONE = 0, DISCO_DIAG_DISK2D = 1 };
 enum disco_precision{ DISCO_PREC_FP64 = 0, DISCO_PREC_MIXED = 1 };
 

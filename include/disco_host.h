@@ -25,7 +25,9 @@ int disco_read_par(const char *path, disco_params *p, int *nmissing);
 /*
  * Parse a Makefile_opt.in module selection (INITIAL, HYDRO, BOUNDARY,
  * PLANETS, ANALYSIS, NUM_C, NUM_N, CT_MODE; Makefile:11-26).  Unknown module
- * names give DISCO_ERR_UNSUPPORTED.
+ * names give DISCO_ERR_UNSUPPORTED, except INITIAL: a module other than
+ * kepler_noise / mhd_shear_noise reads as DISCO_IC_HOST (its state must be
+ * uploaded, disco_batch_setup_cells refuses it).
  */
 int disco_read_opt(const char *path, disco_modules *m);
 

@@ -109,6 +109,10 @@ CASES = {
                                       "Noise_Rel": 1.0e-2}, 5),
     "c0_atmos": ("c0_cm2", {"Num_R": 24, "Mass_Ratio": 1.0e-3, "Energy_Omega": 0,
                             "Include_Atmos": 1}, 6),
+    # a reference Initial module (Initial/rigid.c), evaluated by the host
+    # set-up only: the drop-in with zero-gradient boundaries (the par file is
+    # what tests/test_gpu_dropin.py runs both binaries on)
+    "c0_rigid_zg": ("c0_rigid_zg", {"Num_R": 32, "Log_Zoning": 0, "Energy_Omega": 0}, 8),
 }
 
 # the in.par template each module configuration starts from
@@ -116,7 +120,7 @@ BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": 
             "c1_mhd2d": "c1_mhd2d", "c1_mhd2d_nograv": "c1_mhd2d", "c0_zerograd": "c0_kepler2d", "c0_fixed3d": "c0_kepler2d",
             "c1_mhd3d": "c1_mhd3d", "c1_mhd3d_nograv": "c1_mhd3d", "c0_polar": "c0_kepler2d",
             "c1_polar": "c1_mhd2d", "c1_polar3d": "c1_mhd3d", "c0_outflow3d": "c0_kepler2d",
-            "c1_omk3d": "c1_mhd3d", "c1_accrete3d": "c1_mhd3d"}
+            "c1_omk3d": "c1_mhd3d", "c1_accrete3d": "c1_mhd3d", "c0_rigid_zg": "c0_kepler2d"}
 
 
 def par_text(cfg_par, overrides):

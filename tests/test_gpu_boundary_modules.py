@@ -95,3 +95,27 @@ def test_polar_needs_the_axis():
     with pytest.raises(db.DiscoError) as e:
         db.Batch([disk])
     assert e.value.status == 3
+
+
+def test_host_initial_module():
+    """The same reference Initial module through the Python API: the disk
+    reads as DISCO_IC_HOST, the device set-up refuses it, and from the
+    reference's uploaded step-0 state the steps match the reference bit for
+    bit (zero-gradient boundaries)."""
+    disk, g = case_disk("c0_rigid_zg")
+    assert disk.modules.initial == db.INITIAL["host"]
+    with pytest.raises(db.DiscoError) as e:
+        db.Batch([disk])
+    assert e.value.status == 3
+    b = db.Batch([disk], setup=False)
+    b.set_cells(g["s0_prim"], g["s0_cons"], g["s0_piph"], g["s0_dphi"], g["s0_wiph"], g["real"])
+    dts = []
+    for _ in range(int(g["nsteps"])):
+        dt = b.mindt()[0]
+        dts.append(dt)
+        b.timestep(dt)
+    b.sync()
+    st = b.get_cells()
+    r = disk.real == 1
+    assert np.array_equal(np.array(dts), g["dt"])
+    assert np.array_equal(st["prim"][r], g["sN_prim"][r])

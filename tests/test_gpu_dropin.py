@@ -174,3 +174,17 @@ def test_dropin_polar():
     assert max(rel_l1_cols(b["prim"][r], a["prim"][r])) < 1e-12
     for k in ("iL", "iR", "LRtype"):
         assert np.array_equal(a["faces_1"][k], b["faces_1"][k]), k
+
+
+def test_dropin_reference_initial_module():
+    """A reference Initial module (Initial/rigid.c) the device does not have:
+    the host set-up evaluates it, the shim runs the steps with zero-gradient
+    boundaries (which never call initial() again) -- bit for bit with the
+    reference binary over 10 steps (no libm call in the steps)."""
+    ref, hyb = _binaries("c0_rigid_zg")
+    par = os.path.join(GOLDEN, "c0_rigid_zg.par")
+    a, b = _run(ref, par, 10), _run(hyb, par, 10)
+    assert np.array_equal(a["dt"], b["dt"])
+    r = a["real"] == 1
+    for k in ("prim", "piph", "dphi"):
+        assert np.array_equal(a[k][r], b[k][r]), k
