@@ -75,6 +75,9 @@ static void fill_disk_params(DiskParams &D, const disco_params &p, const disco_m
    D.cs2_profile = p.Cs2_Profile; D.grav2D = p.grav2D; D.polar = p.NoBC_Rmin == 1;
    D.timestep = p.Timestep;
    D.atmos = p.include_atmos ? 1 : 0;
+   D.visc = p.visc_flag ? 1 : 0;
+   D.visc_alpha = p.alpha_flag ? 1 : 0;
+   D.visc_nu = p.viscosity;
    D.noise_type = (p.noiseType >= 1 && p.noiseType <= 3) ? p.noiseType : 0;
    D.noise_abs = p.noiseAbs; D.noise_rel = p.noiseRel;
    D.rotframe = p.RotFrame;
@@ -185,7 +188,8 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       if( params[d].Timestep != params[0].Timestep ) return DISCO_ERR_ARG;
       if( params[d].R_Periodic ) return DISCO_ERR_UNSUPPORTED;
       if( params[d].Riemann_Solver > (mhd ? 2 : 1) ) return DISCO_ERR_UNSUPPORTED;   /* HLLD needs B */
-      if( params[d].visc_flag || params[d].RotFrame ) return DISCO_ERR_UNSUPPORTED;
+      /* viscosity is the Euler module's (Hydro/mhd.c has none) */
+      if( (params[d].visc_flag && mhd) || params[d].RotFrame ) return DISCO_ERR_UNSUPPORTED;
    }
    CK(cudaSetDevice(device));
    disco_batch *b = new disco_batch();

@@ -54,6 +54,8 @@ struct DiskParams {
    int trz0, ntrz;    /* first global z-track, count (Nr*(Nz-1)) */
    int ln0;           /* first global (r, z) edge line, (Nr-1)*(Nz-1) of them (3D CT) */
    int atmos;         /* Include_Atmos: adjust_gas at set-up */
+   int visc, visc_alpha;  /* Use_Viscosity, Use_As_Alpha (euler.c:217-295) */
+   double visc_nu;        /* Viscosity: nu, or alpha */
    int noise_type;    /* Noise_Type 0..3 (addNoise) */
    int pad_noise;
    double noise_abs, noise_rel;
@@ -626,10 +628,69 @@ __device__ __forceinline__ void hlld_solve(const DiskParams &P, R w, const R *pr
  * subtracted from cons_L and added to cons_R (riemann.c:312-315), and, when
  * eb is given (MHD), the inputs of flux_to_E (Hydro/mhd.c:293-316):
  * eb = (Flux[BRR], Flux[BPP], Ustr[BRR], Flux[BZZ], Ustr[BZZ]). */
+/* Kinematic viscosity of euler.c's visc_flux / visc_source / mindt:
+ * Viscosity, or with Use_As_Alpha alpha c h, h = c r^1.5 (euler.c:224-229) */
+__device__ __forceinline__ double visc_nu(const DiskParams &P, const double *prim, double r){
+   if( !P.visc_alpha ) return P.visc_nu;
+   double c = sqrt(P.gam*prim[PPP]/prim[RHO]);
+   double h = c*pow(r, 1.5);
+   return P.visc_nu*c*h;
+}
+
+/* the viscous limit of euler.c's mindt (:357-375): dt <= dx^2 / (2 nu),
+ * dx the cell's shortest get_dL (cylindrical: r dphi with r the mid radius,
+ * dr, dz) */
+__device__ __forceinline__ double visc_dt_limit(const DiskParams &P, const double *prim, double r,
+                                                double dt, double rp, double rm, double zp,
+                                                double zm, double dph){
+   double dL0 = (.5*(rp+rm))*dph, dL1 = rp - rm, dL2 = zp - zm;
+   double dx = dL0;
+   if( dx > dL1 ) dx = dL1;
+   if( dx > dL2 ) dx = dL2;
+   double nu = visc_nu(P, prim, r);
+   double dt_visc = 0.5*dx*dx/nu;
+   if( dt > dt_visc ) dt = dt_visc;
+   return dt;
+}
+
+/* visc_flux (euler.c:217-259) at a face with centre x, normal n (orthonormal
+ * basis), from the averaged state and gradients (riemann.c:295-309); om is
+ * the energy frame's Omega at x (get_om) */
+template<int Q>
+__device__ __forceinline__ void visc_flux(const DiskParams &P, const double *prim,
+                                          const double *gradr, const double *gradp,
+                                          const double *gradz, double r, double om,
+                                          const double *n, double *vF){
+   double nu = visc_nu(P, prim, r);
+   double rho = prim[RHO];
+   double vr = prim[URR];
+   double omg = prim[UPP];
+   double om_off = omg - om;
+   double vz = prim[UZZ];
+   double divV_o_d = (gradr[URR] + gradp[UPP] + gradz[UZZ] + vr/r) / 3.0;
+   double srr = gradr[URR] - divV_o_d;
+   double spp = r*(r*gradp[UPP] + vr - r*divV_o_d);
+   double szz = gradz[UZZ] - divV_o_d;
+   double srp = 0.5*(r*r*gradr[UPP] + gradp[URR]);
+   double srz = 0.5*(gradr[UZZ] + gradz[URR]);
+   double spz = 0.5*(gradp[UZZ] + r*r*gradz[UPP]);
+   double nc[3] = {n[0], n[1]/r, n[2]};
+   double srn = srr*nc[0] + srp*nc[1] + srz*nc[2];
+   double spn = srp*nc[0] + spp*nc[1] + spz*nc[2];
+   double szn = srz*nc[0] + spz*nc[1] + szz*nc[2];
+#pragma unroll
+   for( int q=0 ; q<Q ; ++q ) vF[q] = 0.0;
+   vF[SRR] = -2 * nu * rho * srn;
+   vF[LLL] = -2 * nu * rho * spn;
+   vF[SZZ] = -2 * nu * rho * szn;
+   vF[TAU] = -2 * nu * rho * ( vr*srn + om_off*spn + vz*szn);
+}
+
 template<int Q, int NC, int DIM, class R>
 __device__ __forceinline__ void solve_riemann(const DiskParams &P, const R *primL,
                                               const R *primR, R r, R om,
-                                              R w, R dAdt, R *G, R *eb = nullptr){
+                                              R w, R dAdt, R *G, R *eb = nullptr,
+                                              const double *vF = nullptr){
    R Flux[Q], Ustr[Q];
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ){ Flux[q] = R(0.0); Ustr[q] = R(0.0); }
@@ -672,6 +733,10 @@ __device__ __forceinline__ void solve_riemann(const DiskParams &P, const R *prim
       flux<Q,NC,DIM,R>(P, pk, Fk, r, om);
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ) Flux[q] = Fk[q] + Sk*( Ustr[q] - Uk[q] );
+   }
+   if( vF ){                                     /* riemann.c:295-310 */
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) Flux[q] += (R)vF[q];
    }
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) G[q] = (Flux[q] - w*Ustr[q])*dAdt;

@@ -658,7 +658,27 @@ __global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R
          solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G);
       }
    }else{
-      solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G);
+      if( P.visc ){                  /* riemann_trans (riemann.c:127-131, 158-167) + visc */
+         double pa[Q], gr[Q], gp[Q], gz[Q], vF[Q];
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ){
+            double g = (((double)v.prim[q*N+cR] - (double)v.gradp[q*N+cR]*(double)dpR)
+                        - ((double)v.prim[q*N+cL] + (double)v.gradp[q*N+cL]*(double)dpL))
+                       / ((double)dxL + (double)dxR);
+            double zL = v.gradz ? (double)v.gradz[q*N+cL] : 0.0;
+            double zR = v.gradz ? (double)v.gradz[q*N+cR] : 0.0;
+            pa[q] = .5*((double)primL[q] + (double)primR[q]);
+            gp[q] = .5*((double)v.gradp[q*N+cL] + (double)v.gradp[q*N+cR]);
+            if( DIM == 1 ){ gr[q] = .5*(g + g); gz[q] = .5*(zL + zR); }
+            else { gr[q] = .5*((double)v.gradr[q*N+cL] + (double)v.gradr[q*N+cR]); gz[q] = .5*(g + g); }
+         }
+         const double n[3] = {DIM == 1 ? 1.0 : 0.0, 0.0, DIM == 2 ? 1.0 : 0.0};
+         visc_flux<Q>(P, pa, gr, gp, gz, r, v.tr_om[t], n, vF);
+         solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G,
+                                   nullptr, vF);
+      }else{
+         solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G);
+      }
    }
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) v.fG[(size_t)q*v.Nf + f] = G[q];
@@ -695,7 +715,8 @@ __device__ __forceinline__ void phi_face_flux(const ViewT<R> &v, const DiskParam
 template<int Q, int NC, class R>
 __device__ __forceinline__ void phi_face_flux_states(const ViewT<R> &v, const DiskParams &P, int a,
                                                      int cL, double r, double dAdt, const R *eL,
-                                                     R *primR, R *G, R *eb = nullptr){
+                                                     R *primR, R *G, R *eb = nullptr,
+                                                     int cR = -1){
    R primL[Q];
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) primL[q] = eL[q];
@@ -704,6 +725,23 @@ __device__ __forceinline__ void phi_face_flux_states(const ViewT<R> &v, const Di
       primL[BPP] = Bp; primR[BPP] = Bp;
    }
    double w = r*v.wiph[cL];
+   if( P.visc && cR >= 0 ){          /* riemann_phi (riemann.c:45-64) + visc_flux */
+      const int N = v.Ncell;
+      double pa[Q], gr[Q], gp[Q], gz[Q], vF[Q];
+      double dh = 0.5*(v.dphi[cR] + v.dphi[cL]);
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ){
+         double g = ((double)v.prim[q*N+cR] - (double)v.prim[q*N+cL]) / dh;
+         pa[q] = .5*((double)primL[q] + (double)primR[q]);
+         gr[q] = .5*((double)v.gradr[q*N+cL] + (double)v.gradr[q*N+cR]);
+         gp[q] = .5*(g + g);
+         gz[q] = v.gradz ? .5*((double)v.gradz[q*N+cL] + (double)v.gradz[q*N+cR]) : 0.0;
+      }
+      const double n[3] = {0.0, 1.0, 0.0};
+      visc_flux<Q>(P, pa, gr, gp, gz, r, v.ann_om[a], n, vF);
+      solve_riemann<Q,NC,0,R>(P, primL, primR, (R)r, (R)v.ann_om[a], (R)w, (R)dAdt, G, eb, vF);
+      return;
+   }
    solve_riemann<Q,NC,0,R>(P, primL, primR, (R)r, (R)v.ann_om[a], (R)w, (R)dAdt, G, eb);
 }
 
@@ -791,7 +829,8 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
                if( v.ct == 2 ){ v.pEr[cprev] = -eb[3]; v.pBz[cprev] = eb[4]; }
             }
          }else{
-            phi_face_flux_states<Q,NC,R>(v, P, a, cprev, rc, dAdtp, eR, primR, G);
+            phi_face_flux_states<Q,NC,R>(v, P, a, cprev, rc, dAdtp, eR, primR, G, nullptr,
+                                         c0 + (i == np ? 0 : i));
          }
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) sG[q][threadIdx.x] = G[q];
@@ -908,6 +947,26 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
          acc<R>(cons[LLL], cc[LLL], rho*hp*F1*dVdt);
          acc<R>(cons[SZZ], cc[SZZ], rho*hz*F2*dVdt);
          acc<R>(cons[TAU], cc[TAU], rho*( hr*F0*vr + hz*F2*vz + hp*F1*omega )*dVdt);
+      }
+      if constexpr ( NC == 5 ){
+         if( P.visc ){                  /* visc_source, euler.c:261-295 */
+            double gr[Q], gp[Q], gz[Q];
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ){
+               gr[q] = (double)v.gradr[q*N + c];
+               gp[q] = (double)v.gradp[q*N + c];
+               gz[q] = v.gradz ? (double)v.gradz[q*N + c] : 0.0;
+            }
+            double nu = visc_nu(P, prim, r);
+            double rho = prim[RHO], vr = prim[URR];
+            double divV_o_d = (gr[URR] + gp[UPP] + gz[UZZ] + vr/r) / 3.0;
+            double spp = (r*gp[UPP] + vr - r*divV_o_d) / (r*r*r);
+            acc<R>(cons[SRR], cc[SRR], (-2 * r * rho * nu * spp) * dVdt);
+            double srp = 0.5*(r*r*gr[UPP] + gp[URR]);
+            double spz = 0.5*(gp[UZZ] + r*r*gz[UPP]);
+            double om_r = v.ann_om1[a], om_z = 0.0;
+            acc<R>(cons[TAU], cc[TAU], (2 * rho * nu * (srp * om_r + spz * om_z)) * dVdt);
+         }
       }
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){
@@ -1106,6 +1165,8 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
             double dtm = dtr;
             if( dtm > dtp ) dtm = dtp;
             if( dtm > dtz ) dtm = dtz;
+            if( P.visc ) dtm = visc_dt_limit(P, prim, r, dtm, rp, rm, zp, zm,
+                                             get_dp(piph, phim, P.Pmax, &err));
             if( dtm == dtm ) dtc = dtm;
          }
          if( v.nq && diag ) diag_cell(P, v.ds[d], prim, rp, rm, zp, zm, piph, phim, dq, &err);
@@ -1790,6 +1851,12 @@ __global__ void __launch_bounds__(CB) k_mindt(ViewT<R> v){
       double dtm = dtr;
       if( dtm > dtp ) dtm = dtp;
       if( dtm > dtz ) dtm = dtz;
+      if( P.visc ){
+         double pc[Q];
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ) pc[q] = (double)v.prim[q*N+c];
+         dtm = visc_dt_limit(P, pc, r, dtm, rp, rm, zp, zm, get_dp(piph, phim, P.Pmax, &err));
+      }
       if( dtm == dtm ) dtc = dtm;
    }
    raise_err(v, err);

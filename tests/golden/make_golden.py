@@ -109,6 +109,13 @@ CASES = {
                                       "Noise_Rel": 1.0e-2}, 5),
     "c0_atmos": ("c0_cm2", {"Num_R": 24, "Mass_Ratio": 1.0e-3, "Energy_Omega": 0,
                             "Include_Atmos": 1}, 6),
+    # viscosity (euler.c visc_flux / visc_source / mindt): constant nu large
+    # enough that the viscous dt limit binds (libm-free), and alpha viscosity
+    # on the Keplerian disk (pow)
+    "c0_visc": ("c0_nograv", {"Num_R": 16, "Log_Zoning": 0, "Init_Par2": 1, "Energy_Omega": 0,
+                              "Mach_Number": 5.0, "Use_Viscosity": 1, "Viscosity": 0.5}, 6),
+    "c0_visc_alpha": ("c0_kepler2d", {"Num_R": 24, "Use_Viscosity": 1, "Use_As_Alpha": 1,
+                                      "Viscosity": 0.01}, 6),
     # a reference Initial module (Initial/rigid.c), evaluated by the host
     # set-up only: the drop-in with zero-gradient boundaries (the par file is
     # what tests/test_gpu_dropin.py runs both binaries on)
