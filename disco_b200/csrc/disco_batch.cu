@@ -81,7 +81,11 @@ static void fill_disk_params(DiskParams &D, const disco_params &p, const disco_m
    D.noise_type = (p.noiseType >= 1 && p.noiseType <= 3) ? p.noiseType : 0;
    D.noise_abs = p.noiseAbs; D.noise_rel = p.noiseRel;
    D.rotframe = p.RotFrame;
-   D.planets_move = (m.planets == DISCO_PLANETS_CM2 || m.planets == DISCO_PLANETS_BINARY_SOFT);
+   D.planets_move = (m.planets == DISCO_PLANETS_CM2 || m.planets == DISCO_PLANETS_BINARY_SOFT ||
+                     m.planets == DISCO_PLANETS_CIRCULAR || m.planets == DISCO_PLANETS_CM);
+   /* Planets/cm.c:47-53: the softening relaxes as smooth + exp(-t/30) */
+   D.pl_eps_decay = m.planets == DISCO_PLANETS_CM;
+   D.pl_smooth = 0.5/p.Disk_Mach;
    D.ic.mach = p.Disk_Mach; D.ic.amp = p.initPar[1];
    D.ic.rmin = p.rmin; D.ic.rmax = p.rmax; D.ic.phimax = p.phimax;
    D.ic.seed = (uint64_t)(int64_t)p.initPar0;
@@ -113,6 +117,17 @@ static void init_planets(DiskState &S, DiskParams &D, const disco_params &p, con
          double om = 1.0/(a*sqrt(a));
          S.pl[0].M = 0.5; S.pl[0].omega = om; S.pl[0].r = 0.5*a; S.pl[0].phi = M_PI; S.pl[0].eps = eps;
          S.pl[1].M = 0.5; S.pl[1].omega = om; S.pl[1].r = 0.5*a; S.pl[1].phi = 0.0;  S.pl[1].eps = eps;
+         break; }
+      case DISCO_PLANETS_CIRCULAR: {                   /* Planets/circular.c:19-39 */
+         D.npl = 2;
+         S.pl[0].M = 1.0;
+         S.pl[1].M = p.Mass_Ratio; S.pl[1].omega = 1.0; S.pl[1].r = 1.0; S.pl[1].eps = 0.5/p.Disk_Mach;
+         break; }
+      case DISCO_PLANETS_CM: {                         /* Planets/cm.c:21-45 */
+         D.npl = 2;
+         double a = 1.0, q = p.Mass_Ratio, mu = q/(1.+q), om = pow(a,-1.5), sm = 0.5/p.Disk_Mach;
+         S.pl[0].M = 1.-mu; S.pl[0].omega = om; S.pl[0].r = a*mu; S.pl[0].phi = M_PI; S.pl[0].eps = sm;
+         S.pl[1].M = mu;    S.pl[1].omega = om; S.pl[1].r = a*(1.-mu); S.pl[1].eps = sm;
          break; }
       default:                                          /* Planets/none.c:9-17 */
          D.npl = 1; S.pl[0].M = 0.0; S.pl[0].eps = 1.0; break;

@@ -55,6 +55,8 @@ struct DiskParams {
    int ln0;           /* first global (r, z) edge line, (Nr-1)*(Nz-1) of them (3D CT) */
    int atmos;         /* Include_Atmos: adjust_gas at set-up */
    int visc, visc_alpha;  /* Use_Viscosity, Use_As_Alpha (euler.c:217-295) */
+   int pl_eps_decay, pad_pl;  /* Planets/cm.c: eps = pl_smooth + exp(-t/30) when moved */
+   double pl_smooth;
    double visc_nu;        /* Viscosity: nu, or alpha */
    int noise_type;    /* Noise_Type 0..3 (addNoise) */
    int pad_noise;

@@ -1457,6 +1457,7 @@ __global__ void k_disk_mid(ViewT<R> v, int ndisk, double RK, int first, int adva
          pl.omega = (1.-RK)*pl.omega + RK*pl.RK_omega;
          pl.vr    = (1.-RK)*pl.vr    + RK*pl.RK_vr;
          if( P.planets_move ) pl.phi += pl.omega*dts;
+         if( P.pl_eps_decay ) pl.eps = P.pl_smooth + exp(-S.t/30.);   /* movePlanets(t = t_n) */
       }
    }
    for( int p=0 ; p<P.npl ; ++p ){

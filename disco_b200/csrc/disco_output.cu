@@ -143,7 +143,7 @@ static int put_opts(disco_npz *z, const disco_modules &m){
    static const char *const hydro[] = {"euler", "mhd"};
    static const char *const bc[] = {"fixed", "zerograd", "fixed3d", "polar", "outflow3d",
                                     "zerograd_omk", "accrete3d"};
-   static const char *const pl[] = {"none", "sun", "cm2", "binary_soft"};
+   static const char *const pl[] = {"none", "sun", "cm2", "binary_soft", "circular", "cm"};
    static const char *const ic[] = {"kepler_noise", "mhd_shear_noise", "host"};
    CKS(put_string(z, "Opts/HYDRO", hydro[m.hydro]));
    CKS(put_string(z, "Opts/GEOMETRY", "cylindrical"));

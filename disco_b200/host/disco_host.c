@@ -150,6 +150,8 @@ int disco_read_opt(const char *path, disco_modules *m){
    else if( !strcmp(v, "sun") ) m->planets = DISCO_PLANETS_SUN;
    else if( !strcmp(v, "cm2") ) m->planets = DISCO_PLANETS_CM2;
    else if( !strcmp(v, "binary_soft") ) m->planets = DISCO_PLANETS_BINARY_SOFT;
+   else if( !strcmp(v, "circular") ) m->planets = DISCO_PLANETS_CIRCULAR;
+   else if( !strcmp(v, "cm") ) m->planets = DISCO_PLANETS_CM;
    else return DISCO_ERR_UNSUPPORTED;
    if( opt_value(path, "INITIAL", v, sizeof v) ) return DISCO_ERR_ARG;
    if( !strcmp(v, "kepler_noise") ) m->initial = DISCO_IC_KEPLER_NOISE;

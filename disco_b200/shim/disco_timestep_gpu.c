@@ -72,13 +72,13 @@ static void gpu_init(struct domain *d){
    static const char *const hydros[] = {"euler", "mhd"};
    static const char *const bcs[] = {"fixed", "zerograd", "fixed3d", "polar", "outflow3d",
                                      "zerograd_omk", "accrete3d"};
-   static const char *const pls[] = {"none", "sun", "cm2", "binary_soft"};
+   static const char *const pls[] = {"none", "sun", "cm2", "binary_soft", "circular", "cm"};
    static const char *const ics[] = {"kepler_noise", "mhd_shear_noise"};
    disco_modules m;
    memset(&m, 0, sizeof m);
    m.hydro = module_id(HYDRO, hydros, 2);
    m.boundary = module_id(BOUNDARY, bcs, 7);
-   m.planets = module_id(PLANETS, pls, 4);
+   m.planets = module_id(PLANETS, pls, 6);
    m.initial = module_id(INITIAL, ics, 2);
    /* any other Initial module: setupCells evaluated it here on the host, and
     * boundaries that do not call it again (zerograd, outflow3d) run as is */

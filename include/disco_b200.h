@@ -58,7 +58,8 @@ enum disco_boundary { DISCO_BC_FIXED = 0, DISCO_BC_ZEROGRAD = 1, DISCO_BC_FIXED3
                       DISCO_BC_POLAR = 3, DISCO_BC_OUTFLOW3D = 4, DISCO_BC_ZEROGRAD_OMK = 5,
                       DISCO_BC_ACCRETE3D = 6 };
 enum disco_planets  { DISCO_PLANETS_NONE = 0, DISCO_PLANETS_SUN = 1, DISCO_PLANETS_CM2 = 2,
-                      DISCO_PLANETS_BINARY_SOFT = 3 };
+                      DISCO_PLANETS_BINARY_SOFT = 3, DISCO_PLANETS_CIRCULAR = 4,
+                      DISCO_PLANETS_CM = 5 };
 /* DISCO_IC_HOST: the Initial module is the host's own (a drop-in evaluating
  * any reference IC in setupCells): the state must come from set_cells, and
  * only boundaries that never re-evaluate initial() during the steps

@@ -116,6 +116,17 @@ CASES = {
                               "Mach_Number": 5.0, "Use_Viscosity": 1, "Viscosity": 0.5}, 6),
     "c0_visc_alpha": ("c0_kepler2d", {"Num_R": 24, "Use_Viscosity": 1, "Use_As_Alpha": 1,
                                       "Viscosity": 0.01}, 6),
+    # Planets/circular.c (star + planet on a circular orbit) and Planets/cm.c
+    # (binary about the centre of mass, softening relaxing as exp(-t/30))
+    "c0_circular": ("c0_circular", {"Num_R": 24, "Mass_Ratio": 1.0e-3, "Energy_Omega": 0}, 6),
+    # (started at t = 300, where the softening has relaxed: from t = 0 the
+    # eps ~ 1 binary cannot hold the Keplerian disk and the reference blows up)
+    "c0_cm": ("c0_cm", {"Num_R": 24, "Mass_Ratio": 1.0e-3, "Energy_Omega": 0, "T_Start": 300.0,
+                        "Mach_Number": 5.0}, 6),
+    # from t = 0, where eps = 0.5/Mach + exp(-t/30) ~ 1 changes every step: a
+    # rigidly rotating, pressure-held disk that needs no Keplerian balance
+    "c0_cm_t0": ("c0_cm", {"Num_R": 20, "Log_Zoning": 0, "Init_Par2": 1, "Energy_Omega": 0,
+                           "Mach_Number": 5.0, "Mass_Ratio": 0.5}, 6),
     # a reference Initial module (Initial/rigid.c), evaluated by the host
     # set-up only: the drop-in with zero-gradient boundaries (the par file is
     # what tests/test_gpu_dropin.py runs both binaries on)
@@ -127,7 +138,8 @@ BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": 
             "c1_mhd2d": "c1_mhd2d", "c1_mhd2d_nograv": "c1_mhd2d", "c0_zerograd": "c0_kepler2d", "c0_fixed3d": "c0_kepler2d",
             "c1_mhd3d": "c1_mhd3d", "c1_mhd3d_nograv": "c1_mhd3d", "c0_polar": "c0_kepler2d",
             "c1_polar": "c1_mhd2d", "c1_polar3d": "c1_mhd3d", "c0_outflow3d": "c0_kepler2d",
-            "c1_omk3d": "c1_mhd3d", "c1_accrete3d": "c1_mhd3d", "c0_rigid_zg": "c0_kepler2d"}
+            "c1_omk3d": "c1_mhd3d", "c1_accrete3d": "c1_mhd3d", "c0_rigid_zg": "c0_kepler2d",
+            "c0_circular": "c0_kepler2d", "c0_cm": "c0_kepler2d"}
 
 
 def par_text(cfg_par, overrides):
