@@ -225,7 +225,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->d_noise = NULL;
    b->d_zg_pairs = NULL;
    b->zg_smem = 0;
-   b->nq = mods->analysis == DISCO_DIAG_DISK2D ? 5 : 0;
+   b->nq = mods->analysis == DISCO_DIAG_DISK2D ? 5 : mods->analysis == DISCO_DIAG_EULER ? 8 : 0;
    b->params.assign(params, params + ndisk);
    b->any_mm3 = 0;
    b->any_3d = 0;
@@ -430,10 +430,10 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.fL = dalloc<int>(b, face); v.fR = dalloc<int>(b, face);
    v.fLR = dalloc<unsigned char>(b, face);
    v.fphic = dalloc<double>(b, face); v.fdA = dalloc<double>(b, face); v.fdp = dalloc<double>(b, face);
-   v.diag_part = dalloc<double>(b, b->cblk.size()*6);
+   v.diag_part = dalloc<double>(b, b->cblk.size()*DIAG_SLOTS);
    v.ann_om = dalloc<double>(b, ann); v.ann_om1 = dalloc<double>(b, ann);
    v.tr_om = dalloc<double>(b, v.Ntr);
-   b->d_Qrz = dalloc<double>(b, (size_t)ann*5);
+   b->d_Qrz = dalloc<double>(b, (size_t)ann*(b->nq ? b->nq : 1));
    v.err = dalloc<int>(b, 1);
    b->d_err = v.err;
    v.topo = dalloc<int>(b, 1);
@@ -811,7 +811,7 @@ extern "C" int disco_batch_restart_cells(disco_batch *b, const double *prim, con
    CK(xfer(b, st.data(), b->vd.ds, sizeof(DiskState)*b->ndisk, cudaMemcpyDeviceToHost));
    for( int d=0 ; d<b->ndisk ; ++d ){ st[d].t_avg = 0.0; st[d].count_steps = 0; }
    CK(xfer(b, b->vd.ds, st.data(), sizeof(DiskState)*b->ndisk, cudaMemcpyHostToDevice));
-   if( b->nq ) CK(cudaMemsetAsync(b->d_Qrz, 0, sizeof(double)*5*b->ann_np.size(), b->stream));
+   if( b->nq ) CK(cudaMemsetAsync(b->d_Qrz, 0, sizeof(double)*b->nq*b->ann_np.size(), b->stream));
    if( b->prec == DISCO_PREC_MIXED ) mixed_launch_restart(b);
    else launch_restart_t(b, b->vd);
    CK(cudaGetLastError());
@@ -906,7 +906,8 @@ extern "C" int disco_batch_get_diagnostics(disco_batch *b, int disk, double *Qrz
    if( nq ) *nq = b->nq;
    const DiskParams &D = b->dparams[disk];
    int na = b->disk_Nr[disk]*b->disk_Nz[disk];
-   if( Qrz && b->nq ) CK(xfer(b, Qrz, b->d_Qrz + (size_t)D.ann0*5, sizeof(double)*na*5, cudaMemcpyDeviceToHost));
+   if( Qrz && b->nq ) CK(xfer(b, Qrz, b->d_Qrz + (size_t)D.ann0*b->nq, sizeof(double)*na*b->nq,
+                              cudaMemcpyDeviceToHost));
    if( t_avg ){
       DiskState st;
       CK(xfer(b, &st, b->vd.ds + disk, sizeof st, cudaMemcpyDeviceToHost));

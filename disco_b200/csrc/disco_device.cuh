@@ -38,6 +38,11 @@ struct Planet {
    int pad;
 };
 
+/* Per-cell-block diagnostic partials: up to 8 quantities of the Analysis
+ * module (diag_disk2d 5, diag_euler 8) and the volume in the last slot. */
+#define DIAG_SLOTS 9
+#define DIAG_VOL 8
+
 /* Per-disk constants (read-only inside a step). */
 struct DiskParams {
    double gam, PLM, CFL, maxDT, Pmax;

@@ -985,24 +985,41 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
 /* One cell's terms of add_diagnostics (analysis.c:52-107) with the
  * diag_disk2d quantities (Diagnostics/diag_disk2d.c:17-38), times dV, and
  * dV itself: every cell of the annulus, ghosts included, at the midpoint xc. */
-__device__ __forceinline__ void diag_cell(const DiskParams &P, const DiskState &S, const double *prim,
+__device__ __forceinline__ void diag_cell(const DiskParams &P, const DiskState &S, int nq,
+                                          const double *prim,
                                           double rp, double rm, double zp, double zm,
                                           double piph, double phim, double *dq, int *err){
    double dph = get_dp(piph, phim, P.Pmax, err);
    double dV = dV_of(rp, rm, dph, zp, zm);
-   double r = .5*(rp+rm), phi = .5*(piph+phim);
+   double r = .5*(rp+rm), phi = .5*(piph+phim), z = .5*(zp+zm);
    double rho = prim[RHO], vr = prim[URR], omega = prim[UPP];
    double Fp = 0.0;
-   if( P.npl > 1 ){
-      double Fr, Fz;
-      planetary_force(P.grav2D, S.pl[1], r, phi, 0.0, &Fr, &Fp, &Fz);
+   if( nq == 5 ){                     /* Diagnostics/diag_disk2d.c:17-40 */
+      if( P.npl > 1 ){
+         double Fr, Fz;
+         planetary_force(P.grav2D, S.pl[1], r, phi, 0.0, &Fr, &Fp, &Fz);
+      }
+      dq[0] = rho*dV;
+      dq[1] = 2.*DISCO_PI*r*rho*vr*dV;
+      dq[2] = 2.*DISCO_PI*r*rho*(r*Fp)*dV;
+      dq[3] = 2.*DISCO_PI*r*rho*( r*r*omega*vr )*dV;
+      dq[4] = omega*dV;
+   }else{                             /* Diagnostics/diag_euler.c:17-45 */
+      double vz = prim[UZZ], Pp = prim[PPP];
+      if( P.npl > 1 ){
+         double Fr, Fz;
+         planetary_force(P.grav2D, S.pl[1], r, phi, z, &Fr, &Fp, &Fz);
+      }
+      dq[0] = rho*dV;
+      dq[1] = 2.*DISCO_PI*r*rho*vr*dV;
+      dq[2] = 2.*DISCO_PI*r*rho*vz*dV;
+      dq[3] = 2.*DISCO_PI*r*rho*(r*Fp)*dV;
+      dq[4] = 2.*DISCO_PI*r*rho*( r*r*omega*vr )*dV;
+      dq[5] = omega*dV;
+      dq[6] = 2*DISCO_PI*r * rho*r*r*omega*dV;
+      dq[7] = Pp*dV;
    }
-   dq[0] = rho*dV;
-   dq[1] = 2.*DISCO_PI*r*rho*vr*dV;
-   dq[2] = 2.*DISCO_PI*r*rho*(r*Fp)*dV;
-   dq[3] = 2.*DISCO_PI*r*rho*( r*r*omega*vr )*dV;
-   dq[4] = omega*dV;
-   dq[5] = dV;
+   dq[DIAG_VOL] = dV;
 }
 
 /* The per-block diagnostic sums as a pass of their own, for boundaries that
@@ -1010,7 +1027,7 @@ __device__ __forceinline__ void diag_cell(const DiskParams &P, const DiskState &
  * state after the last boundary pass (timestep.c:40-42). */
 template<int Q, class R>
 __global__ void __launch_bounds__(CB) k_diag_part(ViewT<R> v){
-   __shared__ double s_red[CB/32][6];
+   __shared__ double s_red[CB/32][DIAG_SLOTS];
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -1020,7 +1037,7 @@ __global__ void __launch_bounds__(CB) k_diag_part(ViewT<R> v){
    int j = v.ann_j[a], k = v.ann_k[a];
    const double *rj = v.rj + P.rj0 + 1;
    const double *zk = v.zk + P.zk0 + 1;
-   double dq[6] = {0,0,0,0,0,0};
+   double dq[DIAG_SLOTS] = {0,0,0,0,0,0,0,0,0};
    int err = 0;
    if( i < np ){
       int c = v.ann_off[a] + i;
@@ -1028,12 +1045,12 @@ __global__ void __launch_bounds__(CB) k_diag_part(ViewT<R> v){
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N + c];
       double piph = v.piph[c];
-      diag_cell(P, v.ds[d], prim, rj[j], rj[j-1], zk[k], zk[k-1], piph, piph - v.dphi[c], dq, &err);
+      diag_cell(P, v.ds[d], v.nq, prim, rj[j], rj[j-1], zk[k], zk[k-1], piph, piph - v.dphi[c], dq, &err);
    }
    raise_err(v, err);
    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-   for( int m=0 ; m<6 ; ++m ){
+   for( int m=0 ; m<DIAG_SLOTS ; ++m ){
       double x = dq[m];
 #pragma unroll
       for( int o=16 ; o>0 ; o>>=1 ) x += __shfl_down_sync(0xffffffffu, x, o);
@@ -1041,10 +1058,10 @@ __global__ void __launch_bounds__(CB) k_diag_part(ViewT<R> v){
    }
    __syncthreads();
    if( threadIdx.x == 0 ){
-      for( int m=0 ; m<6 ; ++m ){
+      for( int m=0 ; m<DIAG_SLOTS ; ++m ){
          double x = 0.0;
          for( int w=0 ; w<CB/32 ; ++w ) x += s_red[w][m];
-         v.diag_part[(size_t)blockIdx.x*6 + m] = x;
+         v.diag_part[(size_t)blockIdx.x*DIAG_SLOTS + m] = x;
       }
    }
 }
@@ -1111,14 +1128,14 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
                                          int c0, int np, int i, int j, int k, int d, bool real,
                                          bool active, double piph, double dphi, double *cons,
                                          int last, int bc, int diag, int err){
-   __shared__ double s_red[CB/32][8];
+   __shared__ double s_red[CB/32][DIAG_SLOTS];
    __shared__ unsigned long long s_dt[CB/32];
    const int N = v.Ncell;
    const double *rj = v.rj + P.rj0 + 1;
    const double *zk = v.zk + P.zk0 + 1;
    double prim[Q];
    double dtc = 1.0e300;
-   double dq[6] = {0,0,0,0,0,0};
+   double dq[DIAG_SLOTS] = {0,0,0,0,0,0,0,0,0};
    double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
    if( active ){
       double phim = piph - dphi;
@@ -1169,7 +1186,7 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
                                              get_dp(piph, phim, P.Pmax, &err));
             if( dtm == dtm ) dtc = dtm;
          }
-         if( v.nq && diag ) diag_cell(P, v.ds[d], prim, rp, rm, zp, zm, piph, phim, dq, &err);
+         if( v.nq && diag ) diag_cell(P, v.ds[d], v.nq, prim, rp, rm, zp, zm, piph, phim, dq, &err);
       }
    }
    raise_err(v, err);
@@ -1186,7 +1203,8 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
    if( lane == 0 ) s_dt[wid] = bits;
    if( v.nq && diag ){
 #pragma unroll
-      for( int m=0 ; m<6 ; ++m ){
+      for( int m=0 ; m<DIAG_SLOTS ; ++m ){
+         if( m >= v.nq && m != DIAG_VOL ) continue;
          double x = dq[m];
 #pragma unroll
          for( int o=16 ; o>0 ; o>>=1 ) x += __shfl_down_sync(0xffffffffu, x, o);
@@ -1199,10 +1217,11 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
       for( int w=1 ; w<CB/32 ; ++w ) mb = s_dt[w] < mb ? s_dt[w] : mb;
       if( real ) atomicMin(&v.ds[d].dtmin, mb);
       if( v.nq && diag ){
-         for( int m=0 ; m<6 ; ++m ){
+         for( int m=0 ; m<DIAG_SLOTS ; ++m ){
+            if( m >= v.nq && m != DIAG_VOL ) continue;
             double x = 0.0;
             for( int w=0 ; w<CB/32 ; ++w ) x += s_red[w][m];
-            v.diag_part[(size_t)blockIdx.x*6 + m] = x;
+            v.diag_part[(size_t)blockIdx.x*DIAG_SLOTS + m] = x;
          }
       }
    }
@@ -1495,12 +1514,13 @@ __global__ void k_diag_finish(ViewT<R> v, double *Qrz, const int *ann_blk0, cons
    if( a >= v.Nann ) return;
    int d = v.ann_disk[a];
    double dt = v.ds[d].dt;
-   double s[6] = {0,0,0,0,0,0};
+   double s[DIAG_SLOTS] = {0,0,0,0,0,0,0,0,0};
+   const int nq = v.nq;
    for( int bb=0 ; bb<ann_nblk[a] ; ++bb ){
-      const double *p = v.diag_part + (size_t)(ann_blk0[a]+bb)*6;
-      for( int m=0 ; m<6 ; ++m ) s[m] += p[m];
+      const double *p = v.diag_part + (size_t)(ann_blk0[a]+bb)*DIAG_SLOTS;
+      for( int m=0 ; m<DIAG_SLOTS ; ++m ) if( m < nq || m == DIAG_VOL ) s[m] += p[m];
    }
-   for( int m=0 ; m<5 ; ++m ) Qrz[(size_t)a*5 + m] += s[m]*dt / s[5];
+   for( int m=0 ; m<nq ; ++m ) Qrz[(size_t)a*nq + m] += s[m]*dt / s[DIAG_VOL];
 }
 
 /* ------------------------------------------------------------------ report

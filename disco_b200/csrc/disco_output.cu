@@ -150,7 +150,8 @@ static int put_opts(disco_npz *z, const disco_modules &m){
    CKS(put_string(z, "Opts/BOUNDARY", bc[m.boundary]));
    CKS(put_string(z, "Opts/PLANETS", pl[m.planets]));
    CKS(put_string(z, "Opts/INITIAL", ic[m.initial]));
-   CKS(put_string(z, "Opts/ANALYSIS", m.analysis == DISCO_DIAG_DISK2D ? "diag_disk2d" : "none"));
+   CKS(put_string(z, "Opts/ANALYSIS", m.analysis == DISCO_DIAG_DISK2D ? "diag_disk2d" :
+                                      m.analysis == DISCO_DIAG_EULER ? "diag_euler" : "none"));
    int64_t one = 1;
    int v[3] = {m.num_c, m.num_n, m.ct_mode};
    CKS(disco_npz_put(z, "Opts/NUM_C", "<i4", 1, &one, &v[0]));
@@ -215,7 +216,7 @@ static int write_checkpoint(disco_batch *b, int disk, disco_npz *z){
    int nq = b->nq;
    std::vector<double> Qrz((size_t)na*nq);
    if( nq ){
-      CK(batch_xfer(b, Qrz.data(), b->d_Qrz + (size_t)a0*5, sizeof(double)*na*5, cudaMemcpyDeviceToHost));
+      CK(batch_xfer(b, Qrz.data(), b->d_Qrz + (size_t)a0*nq, sizeof(double)*na*nq, cudaMemcpyDeviceToHost));
       double dt = st.t_avg;
       for( size_t i=0 ; i<Qrz.size() ; ++i ) Qrz[i] /= dt;
    }
@@ -230,7 +231,7 @@ static int write_checkpoint(disco_batch *b, int disk, disco_npz *z){
    CKS(put_opts(z, b->mods));
 
    /* zero_diagnostics */
-   if( nq ) CK(cudaMemsetAsync(b->d_Qrz + (size_t)a0*5, 0, sizeof(double)*na*5, b->stream));
+   if( nq ) CK(cudaMemsetAsync(b->d_Qrz + (size_t)a0*nq, 0, sizeof(double)*na*nq, b->stream));
    CK(batch_xfer(b, &st, b->vd.ds + disk, sizeof st, cudaMemcpyDeviceToHost));
    st.t_avg = 0.0;
    CK(batch_xfer(b, b->vd.ds + disk, &st, sizeof st, cudaMemcpyHostToDevice));

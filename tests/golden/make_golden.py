@@ -127,6 +127,12 @@ CASES = {
     # rigidly rotating, pressure-held disk that needs no Keplerian balance
     "c0_cm_t0": ("c0_cm", {"Num_R": 20, "Log_Zoning": 0, "Init_Par2": 1, "Energy_Omega": 0,
                            "Mach_Number": 5.0, "Mass_Ratio": 0.5}, 6),
+    # Diagnostics/diag_euler.c (8 annulus averages: the flux of vz, the
+    # angular momentum and the pressure beside diag_disk2d's), with the
+    # planet torque term (cm2) and in 3D
+    "c0_diag_euler": ("c0_diag_euler", {"Num_R": 24, "Mass_Ratio": 1.0e-3, "Energy_Omega": 0}, 6),
+    "c0_diag_euler3d": ("c0_diag_euler3d", {"Num_R": 10, "Num_Z": 4, "Grav2D": 1, "Z_Min": -0.3,
+                                            "Z_Max": 0.3}, 4),
     # a reference Initial module (Initial/rigid.c), evaluated by the host
     # set-up only: the drop-in with zero-gradient boundaries (the par file is
     # what tests/test_gpu_dropin.py runs both binaries on)
@@ -139,7 +145,8 @@ BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": 
             "c1_mhd3d": "c1_mhd3d", "c1_mhd3d_nograv": "c1_mhd3d", "c0_polar": "c0_kepler2d",
             "c1_polar": "c1_mhd2d", "c1_polar3d": "c1_mhd3d", "c0_outflow3d": "c0_kepler2d",
             "c1_omk3d": "c1_mhd3d", "c1_accrete3d": "c1_mhd3d", "c0_rigid_zg": "c0_kepler2d",
-            "c0_circular": "c0_kepler2d", "c0_cm": "c0_kepler2d"}
+            "c0_circular": "c0_kepler2d", "c0_cm": "c0_kepler2d", "c0_diag_euler": "c0_kepler2d",
+            "c0_diag_euler3d": "c0_kepler2d"}
 
 
 def par_text(cfg_par, overrides):
