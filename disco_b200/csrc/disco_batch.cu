@@ -223,6 +223,8 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->zg_omk = mods->boundary == DISCO_BC_ZEROGRAD_OMK;
    b->d_zg_side = NULL;
    b->d_noise = NULL;
+   b->any_visc = 0;
+   for( int d=0 ; d<ndisk ; ++d ) if( params[d].visc_flag ) b->any_visc = 1;
    b->d_zg_pairs = NULL;
    b->zg_smem = 0;
    b->nq = mods->analysis == DISCO_DIAG_DISK2D ? 5 : mods->analysis == DISCO_DIAG_EULER ? 8 : 0;

@@ -27,6 +27,7 @@ struct disco_batch {
    std::vector<unsigned char> zg_side;  /* per pair: 0 inner r, 1 outer r, 2 lower z, 3 upper z */
    unsigned char *d_zg_side;
    int zg_diode, zg_omk;                /* outflow diode; Omega from initial() in r ghosts */
+   int any_visc;                        /* some disk has Use_Viscosity (Euler) */
    std::vector<int> zg_off;             /* layer groups: r layers, then z layers */
    int2 *d_zg_pairs;
    size_t zg_smem;                      /* dynamic shared memory of k_zerograd */
@@ -133,6 +134,31 @@ static void launch_restart_qt(disco_batch *b, const ViewT<R> &v){
    launch_zerograd<Q,R>(b, v);
 }
 
+/* k_c2p with the Analysis module's number of diagnostics (diag_disk2d 5,
+ * diag_euler 8) and, for Euler, the viscous dt limit compiled in only when a
+ * disk is viscous */
+template<int Q, int NC, class R, int NQD>
+static void launch_c2p_nq(disco_batch *b, const ViewT<R> &v, int last, int diag){
+   unsigned ncb = (unsigned)b->cblk.size();
+   if constexpr ( NC == 5 ){
+      if( b->any_visc ){ k_c2p<Q,NC,R,NQD,true><<<ncb, CB, 0, b->stream>>>(v, last, b->bc_fixed, diag); return; }
+   }
+   k_c2p<Q,NC,R,NQD,false><<<ncb, CB, 0, b->stream>>>(v, last, b->bc_fixed, diag);
+}
+template<int Q, int NC, class R>
+static void launch_c2p(disco_batch *b, const ViewT<R> &v, int last, int diag){
+   if( b->nq == 8 ) launch_c2p_nq<Q,NC,R,8>(b, v, last, diag);
+   else launch_c2p_nq<Q,NC,R,5>(b, v, last, diag);
+}
+template<int Q, int NC, int DIM, class R>
+static void launch_flux_t(disco_batch *b, const ViewT<R> &v){
+   unsigned nfb = (unsigned)b->fblk.size();
+   if constexpr ( NC == 5 ){
+      if( b->any_visc ){ k_flux_t<Q,NC,DIM,R,true><<<nfb, FB, 0, b->stream>>>(v); return; }
+   }
+   k_flux_t<Q,NC,DIM,R,false><<<nfb, FB, 0, b->stream>>>(v);
+}
+
 /* One substep of onestep() (onestep.c:84-229). */
 template<int Q, int NC, class R>
 static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int last, double dtfac){
@@ -149,9 +175,16 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    k_faces<Q,R><<<nfb, FB, 0, s>>>(v, 1);                             mark(b, "k_faces");
    k_grad<Q,1,R><<<ncb, CB, 0, s>>>(v);                               mark(b, "k_gradr");
    if( b->any_3d ){ k_grad<Q,2,R><<<ncb, CB, 0, s>>>(v);              mark(b, "k_gradz"); }
-   k_flux_t<Q,NC,1,R><<<nfb, FB, 0, s>>>(v);                          mark(b, "k_flux_r");
-   if( b->any_3d ){ k_flux_t<Q,NC,2,R><<<nfb, FB, 0, s>>>(v);         mark(b, "k_flux_z"); }
-   k_update<Q,NC,R><<<(unsigned)b->ublk.size(), CB, 0, s>>>(v, first); mark(b, "k_update");
+   launch_flux_t<Q,NC,1,R>(b, v);                                     mark(b, "k_flux_r");
+   if( b->any_3d ){ launch_flux_t<Q,NC,2,R>(b, v);                    mark(b, "k_flux_z"); }
+   bool upd_visc = false;
+   if constexpr ( NC == 5 ) upd_visc = b->any_visc;
+   if( upd_visc ){
+      if constexpr ( NC == 5 ) k_update<Q,NC,R,true><<<(unsigned)b->ublk.size(), CB, 0, s>>>(v, first);
+   }else{
+      k_update<Q,NC,R,false><<<(unsigned)b->ublk.size(), CB, 0, s>>>(v, first);
+   }
+   mark(b, "k_update");
    if constexpr ( NC == 8 ){
       if( b->ct ){                  /* onestep.c:140-146 and 160-167 */
          k_ct_edges<R><<<ncb, CB, 0, s>>>(v);                           mark(b, "k_ct_edges");
@@ -166,10 +199,12 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
          }
       }
    }
-   k_c2p<Q,NC,R><<<ncb, CB, 0, s>>>(v, last, b->bc_fixed, !b->bc_zerograd); mark(b, "k_c2p");
+   launch_c2p<Q,NC,R>(b, v, last, !b->bc_zerograd);                   mark(b, "k_c2p");
    launch_zerograd<Q,R>(b, v);
    if( last && b->nq && b->bc_zerograd ){
-      k_diag_part<Q,R><<<ncb, CB, 0, s>>>(v);                         mark(b, "k_diag_part");
+      if( b->nq == 8 ) k_diag_part<Q,R,8><<<ncb, CB, 0, s>>>(v);
+      else k_diag_part<Q,R,5><<<ncb, CB, 0, s>>>(v);
+      mark(b, "k_diag_part");
    }
 }
 

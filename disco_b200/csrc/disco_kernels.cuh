@@ -596,13 +596,91 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_GRAD) k_grad(ViewT<R> 
    raise_err(v, err);
 }
 
+/* The viscous flux of a face, compiled only into the viscous instances of
+ * k_flux_t / k_update (template VISC) so that the inviscid kernels keep
+ * their registers.  trans_visc_flux: riemann_trans's
+ * averaged state and gradients (riemann.c:127-131, 158-167, 295-309), the
+ * face's own difference slope in the face's direction; phi_visc_flux:
+ * riemann_phi's (riemann.c:45-64). */
+template<int Q, int DIM, class R>
+__device__ __forceinline__ void trans_visc_flux(const ViewT<R> &v, const DiskParams &P, int cL, int cR,
+                                             R dpL, R dpR, R dxL, R dxR, const R *primL,
+                                             const R *primR, double r, double om, double *vF){
+   const int N = v.Ncell;
+   double pa[Q], gr[Q], gp[Q], gz[Q];
+   for( int q=0 ; q<Q ; ++q ){
+      double g = (((double)v.prim[q*N+cR] - (double)v.gradp[q*N+cR]*(double)dpR)
+                  - ((double)v.prim[q*N+cL] + (double)v.gradp[q*N+cL]*(double)dpL))
+                 / ((double)dxL + (double)dxR);
+      double zL = v.gradz ? (double)v.gradz[q*N+cL] : 0.0;
+      double zR = v.gradz ? (double)v.gradz[q*N+cR] : 0.0;
+      pa[q] = .5*((double)primL[q] + (double)primR[q]);
+      gp[q] = .5*((double)v.gradp[q*N+cL] + (double)v.gradp[q*N+cR]);
+      if( DIM == 1 ){ gr[q] = .5*(g + g); gz[q] = .5*(zL + zR); }
+      else { gr[q] = .5*((double)v.gradr[q*N+cL] + (double)v.gradr[q*N+cR]); gz[q] = .5*(g + g); }
+   }
+   const double n[3] = {DIM == 1 ? 1.0 : 0.0, 0.0, DIM == 2 ? 1.0 : 0.0};
+   visc_flux<Q>(P, pa, gr, gp, gz, r, om, n, vF);
+}
+template<int Q, class R>
+__device__ __forceinline__ void phi_visc_flux(const ViewT<R> &v, const DiskParams &P, int cL, int cR,
+                                           const R *primL, const R *primR, double r, double om,
+                                           double *vF){
+   const int N = v.Ncell;
+   double pa[Q], gr[Q], gp[Q], gz[Q];
+   double dh = 0.5*(v.dphi[cR] + v.dphi[cL]);
+   for( int q=0 ; q<Q ; ++q ){
+      double g = ((double)v.prim[q*N+cR] - (double)v.prim[q*N+cL]) / dh;
+      pa[q] = .5*((double)primL[q] + (double)primR[q]);
+      gr[q] = .5*((double)v.gradr[q*N+cL] + (double)v.gradr[q*N+cR]);
+      gp[q] = .5*(g + g);
+      gz[q] = v.gradz ? .5*((double)v.gradz[q*N+cL] + (double)v.gradz[q*N+cR]) : 0.0;
+   }
+   const double n[3] = {0.0, 1.0, 0.0};
+   visc_flux<Q>(P, pa, gr, gp, gz, r, om, n, vF);
+}
+/* riemann_trans's solve with the viscous flux */
+template<int Q, int NC, int DIM, class R>
+__device__ __forceinline__ void trans_face_flux_visc(const ViewT<R> &v, const DiskParams &P, int cL,
+                                                  int cR, R dpL, R dpR, R dxL, R dxR,
+                                                  const R *primL, const R *primR, double r,
+                                                  double om, double dAdt, R *G){
+   double vF[Q];
+   trans_visc_flux<Q,DIM,R>(v, P, cL, cR, dpL, dpR, dxL, dxR, primL, primR, r, om, vF);
+   solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)om, R(0.0), (R)dAdt, G, nullptr, vF);
+}
+/* visc_source (euler.c:261-295) for cell c: the increments of cons[SRR]
+ * and cons[TAU] */
+template<int Q, class R>
+__device__ __forceinline__ double2 visc_source_cell(const ViewT<R> &v, const DiskParams &P, int c,
+                                                 int a, double r, double dVdt){
+   const int N = v.Ncell;
+   double gr[Q], gp[Q], gz[Q], prim[Q];
+   for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N + c];
+   for( int q=0 ; q<Q ; ++q ){
+      gr[q] = (double)v.gradr[q*N + c];
+      gp[q] = (double)v.gradp[q*N + c];
+      gz[q] = v.gradz ? (double)v.gradz[q*N + c] : 0.0;
+   }
+   double nu = visc_nu(P, prim, r);
+   double rho = prim[RHO], vr = prim[URR];
+   double divV_o_d = (gr[URR] + gp[UPP] + gz[UZZ] + vr/r) / 3.0;
+   double spp = (r*gp[UPP] + vr - r*divV_o_d) / (r*r*r);
+   double dS = (-2 * r * rho * nu * spp) * dVdt;
+   double srp = 0.5*(r*r*gr[UPP] + gp[URR]);
+   double spz = 0.5*(gp[UZZ] + r*r*gz[UPP]);
+   double om_r = v.ann_om1[a], om_z = 0.0;
+   double dT = (2 * rho * nu * (srp * om_r + spz * om_z)) * dVdt;
+   return make_double2(dS, dT);
+}
+
 /* ------------------------------------------------------------------ k_flux_t
  * trans_flux (misc.c:431-509) -> riemann_trans (riemann.c:114-170) ->
  * solve_riemann for the faces of r-tracks (DIM 1) or z-tracks (DIM 2);
  * G_q = (F - w U*) dA dt per face.  The face centre cm is (r_{j+1/2}, phic,
  * z centroid) for r-faces and (r centroid, phic, z_{k+1/2}) for z-faces
  * (addFace, faces_alt.c:10-16). */
-template<int Q, int NC, int DIM, class R>
+template<int Q, int NC, int DIM, class R, bool VISC = false>
 __global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R> v){
    int2 b = v.fblk[blockIdx.x];
    int t = b.x;
@@ -658,24 +736,11 @@ __global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R
          solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G);
       }
    }else{
-      if( P.visc ){                  /* riemann_trans (riemann.c:127-131, 158-167) + visc */
-         double pa[Q], gr[Q], gp[Q], gz[Q], vF[Q];
-#pragma unroll
-         for( int q=0 ; q<Q ; ++q ){
-            double g = (((double)v.prim[q*N+cR] - (double)v.gradp[q*N+cR]*(double)dpR)
-                        - ((double)v.prim[q*N+cL] + (double)v.gradp[q*N+cL]*(double)dpL))
-                       / ((double)dxL + (double)dxR);
-            double zL = v.gradz ? (double)v.gradz[q*N+cL] : 0.0;
-            double zR = v.gradz ? (double)v.gradz[q*N+cR] : 0.0;
-            pa[q] = .5*((double)primL[q] + (double)primR[q]);
-            gp[q] = .5*((double)v.gradp[q*N+cL] + (double)v.gradp[q*N+cR]);
-            if( DIM == 1 ){ gr[q] = .5*(g + g); gz[q] = .5*(zL + zR); }
-            else { gr[q] = .5*((double)v.gradr[q*N+cL] + (double)v.gradr[q*N+cR]); gz[q] = .5*(g + g); }
-         }
-         const double n[3] = {DIM == 1 ? 1.0 : 0.0, 0.0, DIM == 2 ? 1.0 : 0.0};
-         visc_flux<Q>(P, pa, gr, gp, gz, r, v.tr_om[t], n, vF);
-         solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G,
-                                   nullptr, vF);
+      bool visc = false;
+      if constexpr ( VISC ) visc = P.visc;
+      if( visc ){                    /* riemann_trans (riemann.c:127-131, 158-167) + visc */
+         trans_face_flux_visc<Q,NC,DIM,R>(v, P, cL, cR, dpL, dpR, dxL, dxR, primL, primR, r,
+                                          v.tr_om[t], dAdt, G);
       }else{
          solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G);
       }
@@ -715,8 +780,7 @@ __device__ __forceinline__ void phi_face_flux(const ViewT<R> &v, const DiskParam
 template<int Q, int NC, class R>
 __device__ __forceinline__ void phi_face_flux_states(const ViewT<R> &v, const DiskParams &P, int a,
                                                      int cL, double r, double dAdt, const R *eL,
-                                                     R *primR, R *G, R *eb = nullptr,
-                                                     int cR = -1){
+                                                     R *primR, R *G, R *eb = nullptr){
    R primL[Q];
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) primL[q] = eL[q];
@@ -725,24 +789,33 @@ __device__ __forceinline__ void phi_face_flux_states(const ViewT<R> &v, const Di
       primL[BPP] = Bp; primR[BPP] = Bp;
    }
    double w = r*v.wiph[cL];
-   if( P.visc && cR >= 0 ){          /* riemann_phi (riemann.c:45-64) + visc_flux */
-      const int N = v.Ncell;
-      double pa[Q], gr[Q], gp[Q], gz[Q], vF[Q];
-      double dh = 0.5*(v.dphi[cR] + v.dphi[cL]);
-#pragma unroll
-      for( int q=0 ; q<Q ; ++q ){
-         double g = ((double)v.prim[q*N+cR] - (double)v.prim[q*N+cL]) / dh;
-         pa[q] = .5*((double)primL[q] + (double)primR[q]);
-         gr[q] = .5*((double)v.gradr[q*N+cL] + (double)v.gradr[q*N+cR]);
-         gp[q] = .5*(g + g);
-         gz[q] = v.gradz ? .5*((double)v.gradz[q*N+cL] + (double)v.gradz[q*N+cR]) : 0.0;
-      }
-      const double n[3] = {0.0, 1.0, 0.0};
-      visc_flux<Q>(P, pa, gr, gp, gz, r, v.ann_om[a], n, vF);
-      solve_riemann<Q,NC,0,R>(P, primL, primR, (R)r, (R)v.ann_om[a], (R)w, (R)dAdt, G, eb, vF);
-      return;
-   }
    solve_riemann<Q,NC,0,R>(P, primL, primR, (R)r, (R)v.ann_om[a], (R)w, (R)dAdt, G, eb);
+}
+
+/* Q values passed to and from the out-of-line viscous paths by value, so
+ * that no array of the calling kernel has its address taken */
+template<int Q, class R> struct QVec { R q[Q]; };
+
+/* The phi face with the viscous flux (riemann_phi, riemann.c:45-64, +
+ * visc_flux), in the viscous instance of k_update only.  The edge states
+ * are extrapolated again here exactly as k_update does (cL's right edge,
+ * cR's left edge). */
+template<int Q, int NC, class R>
+__device__ __forceinline__ QVec<Q,R> phi_face_flux_visc(const ViewT<R> &v, const DiskParams &P, int a,
+                                                     int cL, int cR, double r, double dAdt){
+   const int N = v.Ncell;
+   R primL[Q], primR[Q];
+   R dL = (R)v.dphi[cL], dR = (R)v.dphi[cR];
+   for( int q=0 ; q<Q ; ++q ){
+      primL[q] = v.prim[q*N + cL] + R(.5)*v.gradp[q*N + cL]*dL;
+      primR[q] = v.prim[q*N + cR] - R(.5)*v.gradp[q*N + cR]*dR;
+   }
+   double w = r*v.wiph[cL];
+   double vF[Q];
+   phi_visc_flux<Q,R>(v, P, cL, cR, primL, primR, r, v.ann_om[a], vF);
+   QVec<Q,R> G;
+   solve_riemann<Q,NC,0,R>(P, primL, primR, (R)r, (R)v.ann_om[a], (R)w, (R)dAdt, G.q, nullptr, vF);
+   return G;
 }
 
 /* ------------------------------------------------------------------ k_update
@@ -754,7 +827,7 @@ __device__ __forceinline__ void phi_face_flux_states(const ViewT<R> &v, const Di
  * calc_prim, the boundary, and the fused getmindt / diagnostics follow in
  * k_c2p (run inside this kernel instead, the extra registers cost more than
  * the saved re-read of cons: 1.73 against 1.69 ms per ragged64 step). */
-template<int Q, int NC, class R>
+template<int Q, int NC, class R, bool VISC = false>
 __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT<R> v, int first){
    /* The block updates CB-1 cells i0 .. i0+CB-2 and its thread t solves the
     * phi face (i0+t-1, i0+t) into sG[.][t]: every thread one face, the
@@ -829,8 +902,16 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
                if( v.ct == 2 ){ v.pEr[cprev] = -eb[3]; v.pBz[cprev] = eb[4]; }
             }
          }else{
-            phi_face_flux_states<Q,NC,R>(v, P, a, cprev, rc, dAdtp, eR, primR, G, nullptr,
-                                         c0 + (i == np ? 0 : i));
+            bool visc = false;
+            if constexpr ( VISC ) visc = P.visc;
+            if( visc ){
+               QVec<Q,R> Gv = phi_face_flux_visc<Q,NC,R>(v, P, a, cprev, c0 + (i == np ? 0 : i),
+                                                         rc, dAdtp);
+#pragma unroll
+               for( int q=0 ; q<Q ; ++q ) G[q] = Gv.q[q];
+            }else{
+               phi_face_flux_states<Q,NC,R>(v, P, a, cprev, rc, dAdtp, eR, primR, G);
+            }
          }
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) sG[q][threadIdx.x] = G[q];
@@ -948,24 +1029,11 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
          acc<R>(cons[SZZ], cc[SZZ], rho*hz*F2*dVdt);
          acc<R>(cons[TAU], cc[TAU], rho*( hr*F0*vr + hz*F2*vz + hp*F1*omega )*dVdt);
       }
-      if constexpr ( NC == 5 ){
+      if constexpr ( NC == 5 && VISC ){
          if( P.visc ){                  /* visc_source, euler.c:261-295 */
-            double gr[Q], gp[Q], gz[Q];
-#pragma unroll
-            for( int q=0 ; q<Q ; ++q ){
-               gr[q] = (double)v.gradr[q*N + c];
-               gp[q] = (double)v.gradp[q*N + c];
-               gz[q] = v.gradz ? (double)v.gradz[q*N + c] : 0.0;
-            }
-            double nu = visc_nu(P, prim, r);
-            double rho = prim[RHO], vr = prim[URR];
-            double divV_o_d = (gr[URR] + gp[UPP] + gz[UZZ] + vr/r) / 3.0;
-            double spp = (r*gp[UPP] + vr - r*divV_o_d) / (r*r*r);
-            acc<R>(cons[SRR], cc[SRR], (-2 * r * rho * nu * spp) * dVdt);
-            double srp = 0.5*(r*r*gr[UPP] + gp[URR]);
-            double spz = 0.5*(gp[UZZ] + r*r*gz[UPP]);
-            double om_r = v.ann_om1[a], om_z = 0.0;
-            acc<R>(cons[TAU], cc[TAU], (2 * rho * nu * (srp * om_r + spz * om_z)) * dVdt);
+            double2 st = visc_source_cell<Q,R>(v, P, c, a, r, dVdt);
+            acc<R>(cons[SRR], cc[SRR], st.x);
+            acc<R>(cons[TAU], cc[TAU], st.y);
          }
       }
 #pragma unroll
@@ -985,16 +1053,17 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
 /* One cell's terms of add_diagnostics (analysis.c:52-107) with the
  * diag_disk2d quantities (Diagnostics/diag_disk2d.c:17-38), times dV, and
  * dV itself: every cell of the annulus, ghosts included, at the midpoint xc. */
-__device__ __forceinline__ void diag_cell(const DiskParams &P, const DiskState &S, int nq,
+template<int NQD>
+__device__ __forceinline__ void diag_cell(const DiskParams &P, const DiskState &S,
                                           const double *prim,
                                           double rp, double rm, double zp, double zm,
                                           double piph, double phim, double *dq, int *err){
    double dph = get_dp(piph, phim, P.Pmax, err);
    double dV = dV_of(rp, rm, dph, zp, zm);
-   double r = .5*(rp+rm), phi = .5*(piph+phim), z = .5*(zp+zm);
+   double r = .5*(rp+rm), phi = .5*(piph+phim);
    double rho = prim[RHO], vr = prim[URR], omega = prim[UPP];
    double Fp = 0.0;
-   if( nq == 5 ){                     /* Diagnostics/diag_disk2d.c:17-40 */
+   if constexpr ( NQD == 5 ){         /* Diagnostics/diag_disk2d.c:17-40 */
       if( P.npl > 1 ){
          double Fr, Fz;
          planetary_force(P.grav2D, S.pl[1], r, phi, 0.0, &Fr, &Fp, &Fz);
@@ -1005,6 +1074,7 @@ __device__ __forceinline__ void diag_cell(const DiskParams &P, const DiskState &
       dq[3] = 2.*DISCO_PI*r*rho*( r*r*omega*vr )*dV;
       dq[4] = omega*dV;
    }else{                             /* Diagnostics/diag_euler.c:17-45 */
+      double z = .5*(zp+zm);
       double vz = prim[UZZ], Pp = prim[PPP];
       if( P.npl > 1 ){
          double Fr, Fz;
@@ -1019,15 +1089,19 @@ __device__ __forceinline__ void diag_cell(const DiskParams &P, const DiskState &
       dq[6] = 2*DISCO_PI*r * rho*r*r*omega*dV;
       dq[7] = Pp*dV;
    }
-   dq[DIAG_VOL] = dV;
+   dq[NQD] = dV;
 }
+
+/* the global slot of local diagnostic m (the volume goes to DIAG_VOL) */
+template<int NQD>
+__device__ __forceinline__ int diag_slot(int m){ return m == NQD ? DIAG_VOL : m; }
 
 /* The per-block diagnostic sums as a pass of their own, for boundaries that
  * change ghost prims after calc_prim (zerograd): add_diagnostics sees the
  * state after the last boundary pass (timestep.c:40-42). */
-template<int Q, class R>
+template<int Q, class R, int NQD>
 __global__ void __launch_bounds__(CB) k_diag_part(ViewT<R> v){
-   __shared__ double s_red[CB/32][DIAG_SLOTS];
+   __shared__ double s_red[CB/32][NQD+1];
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
@@ -1037,7 +1111,9 @@ __global__ void __launch_bounds__(CB) k_diag_part(ViewT<R> v){
    int j = v.ann_j[a], k = v.ann_k[a];
    const double *rj = v.rj + P.rj0 + 1;
    const double *zk = v.zk + P.zk0 + 1;
-   double dq[DIAG_SLOTS] = {0,0,0,0,0,0,0,0,0};
+   double dq[NQD+1];
+#pragma unroll
+   for( int m=0 ; m<=NQD ; ++m ) dq[m] = 0.0;
    int err = 0;
    if( i < np ){
       int c = v.ann_off[a] + i;
@@ -1045,12 +1121,12 @@ __global__ void __launch_bounds__(CB) k_diag_part(ViewT<R> v){
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N + c];
       double piph = v.piph[c];
-      diag_cell(P, v.ds[d], v.nq, prim, rj[j], rj[j-1], zk[k], zk[k-1], piph, piph - v.dphi[c], dq, &err);
+      diag_cell<NQD>(P, v.ds[d], prim, rj[j], rj[j-1], zk[k], zk[k-1], piph, piph - v.dphi[c], dq, &err);
    }
    raise_err(v, err);
    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-   for( int m=0 ; m<DIAG_SLOTS ; ++m ){
+   for( int m=0 ; m<=NQD ; ++m ){
       double x = dq[m];
 #pragma unroll
       for( int o=16 ; o>0 ; o>>=1 ) x += __shfl_down_sync(0xffffffffu, x, o);
@@ -1058,10 +1134,10 @@ __global__ void __launch_bounds__(CB) k_diag_part(ViewT<R> v){
    }
    __syncthreads();
    if( threadIdx.x == 0 ){
-      for( int m=0 ; m<DIAG_SLOTS ; ++m ){
+      for( int m=0 ; m<=NQD ; ++m ){
          double x = 0.0;
          for( int w=0 ; w<CB/32 ; ++w ) x += s_red[w][m];
-         v.diag_part[(size_t)blockIdx.x*DIAG_SLOTS + m] = x;
+         v.diag_part[(size_t)blockIdx.x*DIAG_SLOTS + diag_slot<NQD>(m)] = x;
       }
    }
 }
@@ -1123,19 +1199,21 @@ __device__ void ct_cons_B(const ViewT<R> &v, const DiskParams &P, int a, int c0,
  * per-block sums of add_diagnostics (analysis.c:52-107).  Every thread of the
  * block (one annulus chunk) must call it: it ends in block reductions.
  * piph / dphi are the moved cell's; cons is read only on real cells. */
-template<int Q, int NC, class R>
+template<int Q, int NC, class R, int NQD, bool VISC>
 __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P, int a, int c,
                                          int c0, int np, int i, int j, int k, int d, bool real,
                                          bool active, double piph, double dphi, double *cons,
                                          int last, int bc, int diag, int err){
-   __shared__ double s_red[CB/32][DIAG_SLOTS];
+   __shared__ double s_red[CB/32][NQD+1];
    __shared__ unsigned long long s_dt[CB/32];
    const int N = v.Ncell;
    const double *rj = v.rj + P.rj0 + 1;
    const double *zk = v.zk + P.zk0 + 1;
    double prim[Q];
    double dtc = 1.0e300;
-   double dq[DIAG_SLOTS] = {0,0,0,0,0,0,0,0,0};
+   double dq[NQD+1];
+#pragma unroll
+   for( int m=0 ; m<=NQD ; ++m ) dq[m] = 0.0;
    double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
    if( active ){
       double phim = piph - dphi;
@@ -1182,11 +1260,13 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
             double dtm = dtr;
             if( dtm > dtp ) dtm = dtp;
             if( dtm > dtz ) dtm = dtz;
-            if( P.visc ) dtm = visc_dt_limit(P, prim, r, dtm, rp, rm, zp, zm,
-                                             get_dp(piph, phim, P.Pmax, &err));
+            if constexpr ( VISC ){
+               if( P.visc ) dtm = visc_dt_limit(P, prim, r, dtm, rp, rm, zp, zm,
+                                                get_dp(piph, phim, P.Pmax, &err));
+            }
             if( dtm == dtm ) dtc = dtm;
          }
-         if( v.nq && diag ) diag_cell(P, v.ds[d], v.nq, prim, rp, rm, zp, zm, piph, phim, dq, &err);
+         if( v.nq && diag ) diag_cell<NQD>(P, v.ds[d], prim, rp, rm, zp, zm, piph, phim, dq, &err);
       }
    }
    raise_err(v, err);
@@ -1203,8 +1283,7 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
    if( lane == 0 ) s_dt[wid] = bits;
    if( v.nq && diag ){
 #pragma unroll
-      for( int m=0 ; m<DIAG_SLOTS ; ++m ){
-         if( m >= v.nq && m != DIAG_VOL ) continue;
+      for( int m=0 ; m<=NQD ; ++m ){
          double x = dq[m];
 #pragma unroll
          for( int o=16 ; o>0 ; o>>=1 ) x += __shfl_down_sync(0xffffffffu, x, o);
@@ -1217,11 +1296,10 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
       for( int w=1 ; w<CB/32 ; ++w ) mb = s_dt[w] < mb ? s_dt[w] : mb;
       if( real ) atomicMin(&v.ds[d].dtmin, mb);
       if( v.nq && diag ){
-         for( int m=0 ; m<DIAG_SLOTS ; ++m ){
-            if( m >= v.nq && m != DIAG_VOL ) continue;
+         for( int m=0 ; m<=NQD ; ++m ){
             double x = 0.0;
             for( int w=0 ; w<CB/32 ; ++w ) x += s_red[w][m];
-            v.diag_part[(size_t)blockIdx.x*DIAG_SLOTS + m] = x;
+            v.diag_part[(size_t)blockIdx.x*DIAG_SLOTS + diag_slot<NQD>(m)] = x;
          }
       }
    }
@@ -1230,7 +1308,7 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
 /* ------------------------------------------------------------------ k_c2p
  * c2p_tail on each cell after k_update, with constrained transport first
  * rebuilding B from the face fluxes (onestep.c:183-185). */
-template<int Q, int NC, class R>
+template<int Q, int NC, class R, int NQD = 5, bool VISC = false>
 __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v, int last, int bc, int diag){
    int2 b = v.cblk[blockIdx.x];
    int a = b.x, i = b.y + threadIdx.x;
@@ -1262,8 +1340,8 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v,
          }
       }
    }
-   c2p_tail<Q,NC,R>(v, P, a, c, c0, np, i, j, k, d, real, active, piph, dphi, cons, last, bc, diag,
-                    err);
+   c2p_tail<Q,NC,R,NQD,VISC>(v, P, a, c, c0, np, i, j, k, d, real, active, piph, dphi, cons, last,
+                             bc, diag, err);
 }
 
 /* The sequential walk of set_cells_copy_distant (boundary_functions.c:
