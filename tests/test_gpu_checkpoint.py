@@ -280,3 +280,27 @@ def test_restart_refusals(tmp_path):
     # the state is unchanged by the refusals and a good file still restarts
     b.restart(path)
     assert b.time()[0] == g["ck_T"][0]
+
+
+def test_run_cli_checkpoint_and_restart(tmp_path):
+    """python -m disco_b200.run writes a checkpoint after its steps and a
+    second run restarts from it: the time carries over, the step count
+    starts again, and the ascii file has one line per cell."""
+    import json
+    import subprocess
+    import sys
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    ck = str(tmp_path / "checkpoint_0001")
+    base = [sys.executable, "-m", "disco_b200.run", "--template", "c0_kepler2d", "--set", "Num_R=32"]
+    r1 = subprocess.run(base + ["--steps", "4", "--warmup", "1", "--checkpoint", ck,
+                                "--ascii", str(tmp_path / "out")],
+                        cwd=repo, check=True, capture_output=True, text=True, timeout=600)
+    a = json.loads(r1.stdout.strip().splitlines()[-1])
+    assert a["count_steps"] == 5 and os.path.exists(ck + ".npz")
+    with open(str(tmp_path / "out.dat")) as f:
+        assert sum(1 for _ in f) == a["cells"]
+    r2 = subprocess.run(base + ["--steps", "4", "--warmup", "1", "--restart", ck + ".npz"],
+                        cwd=repo, check=True, capture_output=True, text=True, timeout=600)
+    b = json.loads(r2.stdout.strip().splitlines()[-1])
+    assert b["count_steps"] == 5 and b["t"] > a["t"]
+    assert np.load(ck + ".npz")["Grid/T"][0] == a["t"]
