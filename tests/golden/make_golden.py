@@ -133,6 +133,10 @@ CASES = {
     "c0_diag_euler": ("c0_diag_euler", {"Num_R": 24, "Mass_Ratio": 1.0e-3, "Energy_Omega": 0}, 6),
     "c0_diag_euler3d": ("c0_diag_euler3d", {"Num_R": 10, "Num_Z": 4, "Grav2D": 1, "Z_Min": -0.3,
                                             "Z_Max": 0.3}, 4),
+    # an outer edge without ghost annuli (NoBC_Rmax 1): the last real
+    # annulus has no outer track
+    "c0_nobc_rmax": ("c0_nograv", {"Num_R": 16, "Log_Zoning": 0, "Init_Par2": 1,
+                                   "Energy_Omega": 0, "Mach_Number": 5.0, "NoBC_Rmax": 1}, 8),
     # a reference Initial module (Initial/rigid.c), evaluated by the host
     # set-up only: the drop-in with zero-gradient boundaries (the par file is
     # what tests/test_gpu_dropin.py runs both binaries on)
