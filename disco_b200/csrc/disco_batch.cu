@@ -202,6 +202,9 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       if( Nr[d] < 2 ) return DISCO_ERR_ARG;
       if( params[d].Timestep != params[0].Timestep ) return DISCO_ERR_ARG;
       if( params[d].R_Periodic ) return DISCO_ERR_UNSUPPORTED;
+      /* periodic z is MPI's exchangeData (exchange.c:174-175): in the serial
+       * reference it copies nothing and the z ghosts are never set */
+      if( params[d].Z_Periodic && Nz[d] > 1 ) return DISCO_ERR_UNSUPPORTED;
       if( params[d].Riemann_Solver > (mhd ? 2 : 1) ) return DISCO_ERR_UNSUPPORTED;   /* HLLD needs B */
       /* viscosity is the Euler module's (Hydro/mhd.c has none) */
       if( (params[d].visc_flag && mhd) || params[d].RotFrame ) return DISCO_ERR_UNSUPPORTED;
