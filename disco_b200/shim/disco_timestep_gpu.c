@@ -205,3 +205,23 @@ void disco_gpu_sync_to_host( struct domain * theDomain ){
        disco_batch_get_diagnostics(g_batch, 0, theDomain->theTools.Qrz, &nq, &tavg) == DISCO_OK )
       theDomain->theTools.t_avg = tavg;
 }
+
+/* The rest of the drop-in's surface: the face lists of the resident state
+ * (for a bit-exact comparison with the reference's buildfaces: fIndex has
+ * N_ftracks+1 entries, iL / iR cell indices in annulus order, LR the
+ * LRtype; any pointer may be NULL, *nfaces receives the count), the
+ * device error word since the last call, and releasing the device state. */
+int disco_gpu_get_faces( struct domain * theDomain , int dim , int *nfaces ,
+                         int *fIndex , int *iL , int *iR , int *LR ){
+   if( !g_batch ) gpu_init(theDomain);
+   return disco_batch_get_faces(g_batch, 0, dim, nfaces, fIndex, iL, iR, LR, NULL);
+}
+
+int disco_gpu_last_error( void ){
+   return g_batch ? disco_batch_last_error(g_batch) : DISCO_OK;
+}
+
+void disco_gpu_free( void ){
+   if( g_batch ) disco_batch_destroy(g_batch);
+   g_batch = NULL;
+}

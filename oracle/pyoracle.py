@@ -67,6 +67,8 @@ def load_dump(d):
                dt_next=rd("dt_next.f64", np.float64)[0])
     if os.path.exists(os.path.join(d, "planets.f64")):
         out["planets"] = rd("planets.f64", np.float64).reshape(-1, 7)
+    if os.path.exists(os.path.join(d, "gpu_faces_1.i32")):      # the drop-in's own face lists
+        out["gpu_faces_1"] = dict(iL=rd("gpu_faces_1.i32", np.int32), iR=rd("gpu_facesR_1.i32", np.int32))
     if meta.get("num_faces", 0) > 0 and os.path.exists(os.path.join(d, "Phi.f64")):
         out["Phi"] = rd("Phi.f64", np.float64).reshape(N, meta["num_faces"])
     for dim in (1, 2):

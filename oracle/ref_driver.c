@@ -40,6 +40,9 @@ void freeDomain( struct domain * );
 /* Present only when this driver is linked with the GPU drop-in
  * (disco_b200/shim): copies the device state back into the cells. */
 void disco_gpu_sync_to_host( struct domain * ) __attribute__((weak));
+int disco_gpu_get_faces( struct domain * , int , int * , int * , int * , int * , int * ) __attribute__((weak));
+int disco_gpu_last_error( void ) __attribute__((weak));
+void disco_gpu_free( void ) __attribute__((weak));
 /* oracle/ref_checkpoint.c: h5out.c's datasets as raw files */
 void disco_ref_checkpoint( struct domain * , const char * );
 /* the output module (Output/ascii.c in the oracle build) */
@@ -238,5 +241,18 @@ int main(int argc, char *argv[]){
    double dt_next = getmindt(&theDomain);
    dump(absdump, "dt_next.f64", &dt_next, sizeof(double));
    if( ckpt ) disco_ref_checkpoint( &theDomain , ckpt );
+   /* through the drop-in: its own face lists equal the host's, rebuilt from
+    * the synced cells above, and the device state is released */
+   if( disco_gpu_get_faces && Nr > 1 ){
+      int nf = 0;
+      disco_gpu_get_faces( &theDomain , 1 , &nf , NULL , NULL , NULL , NULL );
+      int *gL = malloc(sizeof(int)*(nf>0?nf:1)), *gR = malloc(sizeof(int)*(nf>0?nf:1));
+      disco_gpu_get_faces( &theDomain , 1 , &nf , NULL , gL , gR , NULL );
+      dump(absdump, "gpu_faces_1.i32", gL, sizeof(int)*(size_t)nf);
+      dump(absdump, "gpu_facesR_1.i32", gR, sizeof(int)*(size_t)nf);
+      free(gL); free(gR);
+   }
+   if( disco_gpu_last_error && disco_gpu_last_error() != 0 ){ fprintf(stderr, "device error\n"); return 3; }
+   if( disco_gpu_free ) disco_gpu_free();
    return 0;
 }

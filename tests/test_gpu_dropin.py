@@ -64,6 +64,10 @@ def test_dropin_bitexact_libm_free():
     for k in ("iL", "iR", "LRtype"):
         assert np.array_equal(a["faces_1"][k], b["faces_1"][k]), k
     assert a["dt_next"] == b["dt_next"]
+    # the shim's own exports: the device's face lists (disco_gpu_get_faces)
+    # equal the reference's, and disco_gpu_last_error / disco_gpu_free ran
+    for k in ("iL", "iR"):
+        assert np.array_equal(b["gpu_faces_1"][k], a["faces_1"][k]), k
 
 
 def test_dropin_config0_20_steps():
