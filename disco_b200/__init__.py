@@ -455,7 +455,7 @@ class Batch:
 
     def diagnostics(self, disk=0):
         d = self.disks[disk]
-        Qrz = np.zeros(d.Nr * d.Nz * 8)
+        Qrz = np.zeros(d.Nr * d.Nz * 18)
         nq = C.c_int(); tav = C.c_double()
         _check(library().disco_batch_get_diagnostics(self.h, disk, dptr(Qrz), C.byref(nq),
                                                      C.byref(tav)), "disco_batch_get_diagnostics")

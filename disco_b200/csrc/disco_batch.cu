@@ -191,6 +191,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
     * with inner ghosts their prims would never be set */
    if( mods->boundary == DISCO_BC_POLAR )
       for( int d=0 ; d<ndisk ; ++d ) if( Ng[4*d+0] != 0 ) return DISCO_ERR_UNSUPPORTED;
+   if( mods->analysis == DISCO_DIAG_MHDMRI && !mhd ) return DISCO_ERR_UNSUPPORTED;   /* reads B */
    if( mods->initial != DISCO_IC_KEPLER_NOISE && mods->initial != DISCO_IC_MHD_SHEAR_NOISE &&
        mods->initial != DISCO_IC_HOST )
       return DISCO_ERR_UNSUPPORTED;
@@ -230,7 +231,8 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    for( int d=0 ; d<ndisk ; ++d ) if( params[d].visc_flag ) b->any_visc = 1;
    b->d_zg_pairs = NULL;
    b->zg_smem = 0;
-   b->nq = mods->analysis == DISCO_DIAG_DISK2D ? 5 : mods->analysis == DISCO_DIAG_EULER ? 8 : 0;
+   b->nq = mods->analysis == DISCO_DIAG_DISK2D ? 5 : mods->analysis == DISCO_DIAG_EULER ? 8 :
+           mods->analysis == DISCO_DIAG_MHDMRI ? 18 : 0;
    b->params.assign(params, params + ndisk);
    b->any_mm3 = 0;
    b->any_3d = 0;

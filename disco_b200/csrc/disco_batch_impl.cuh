@@ -147,6 +147,9 @@ static void launch_c2p_nq(disco_batch *b, const ViewT<R> &v, int last, int diag)
 }
 template<int Q, int NC, class R>
 static void launch_c2p(disco_batch *b, const ViewT<R> &v, int last, int diag){
+   if constexpr ( NC == 8 ){
+      if( b->nq == 18 ){ launch_c2p_nq<Q,NC,R,18>(b, v, last, diag); return; }
+   }
    if( b->nq == 8 ) launch_c2p_nq<Q,NC,R,8>(b, v, last, diag);
    else launch_c2p_nq<Q,NC,R,5>(b, v, last, diag);
 }
@@ -202,7 +205,11 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    launch_c2p<Q,NC,R>(b, v, last, !b->bc_zerograd);                   mark(b, "k_c2p");
    launch_zerograd<Q,R>(b, v);
    if( last && b->nq && b->bc_zerograd ){
-      if( b->nq == 8 ) k_diag_part<Q,R,8><<<ncb, CB, 0, s>>>(v);
+      bool mri = false;
+      if constexpr ( Q == 9 ) mri = b->nq == 18;
+      if( mri ){
+         if constexpr ( Q == 9 ) k_diag_part<Q,R,18><<<ncb, CB, 0, s>>>(v);
+      }else if( b->nq == 8 ) k_diag_part<Q,R,8><<<ncb, CB, 0, s>>>(v);
       else k_diag_part<Q,R,5><<<ncb, CB, 0, s>>>(v);
       mark(b, "k_diag_part");
    }

@@ -38,10 +38,11 @@ struct Planet {
    int pad;
 };
 
-/* Per-cell-block diagnostic partials: up to 8 quantities of the Analysis
- * module (diag_disk2d 5, diag_euler 8) and the volume in the last slot. */
-#define DIAG_SLOTS 9
-#define DIAG_VOL 8
+/* Per-cell-block diagnostic partials: up to 18 quantities of the Analysis
+ * module (diag_disk2d 5, diag_euler 8, diag_mhdmri 18) and the volume in
+ * the last slot. */
+#define DIAG_SLOTS 19
+#define DIAG_VOL 18
 
 /* Per-disk constants (read-only inside a step). */
 struct DiskParams {

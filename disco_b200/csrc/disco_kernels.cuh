@@ -1073,6 +1073,21 @@ __device__ __forceinline__ void diag_cell(const DiskParams &P, const DiskState &
       dq[2] = 2.*DISCO_PI*r*rho*(r*Fp)*dV;
       dq[3] = 2.*DISCO_PI*r*rho*( r*r*omega*vr )*dV;
       dq[4] = omega*dV;
+   }else if constexpr ( NQD == 18 ){  /* Diagnostics/diag_mhdmri.c:17-59 */
+      double Pp = prim[PPP], vp = prim[UPP], vz = prim[UZZ];
+      double Br = prim[BRR], Bp = prim[BPP], Bz = prim[BZZ];
+      double gam = P.gam;
+      double cs2 = gam * Pp / rho;
+      double B2 = Br*Br + Bp*Bp + Bz*Bz;
+      double sr = rho*vr;
+      double sp = r*r*rho*vp;
+      double sz = rho*vz;
+      double e = 0.5*rho*(vr*vr + r*r*vp*vp + vz*vz) + Pp/(gam-1.0) + 0.5*B2;
+      const double qv[18] = {rho, Pp, vr, vp, vz, Br, Bp, Bz, rho, e, sr, sp, sz, rho*vr*vp,
+                             Br*Bp, B2, sqrt(cs2), sqrt(B2/rho)};
+#pragma unroll
+      for( int m=0 ; m<18 ; ++m ) dq[m] = qv[m]*dV;
+      (void)omega; (void)phi; (void)Fp;
    }else{                             /* Diagnostics/diag_euler.c:17-45 */
       double z = .5*(zp+zm);
       double vz = prim[UZZ], Pp = prim[PPP];

@@ -151,7 +151,8 @@ static int put_opts(disco_npz *z, const disco_modules &m){
    CKS(put_string(z, "Opts/PLANETS", pl[m.planets]));
    CKS(put_string(z, "Opts/INITIAL", ic[m.initial]));
    CKS(put_string(z, "Opts/ANALYSIS", m.analysis == DISCO_DIAG_DISK2D ? "diag_disk2d" :
-                                      m.analysis == DISCO_DIAG_EULER ? "diag_euler" : "none"));
+                                      m.analysis == DISCO_DIAG_EULER ? "diag_euler" :
+                                      m.analysis == DISCO_DIAG_MHDMRI ? "diag_mhdmri" : "none"));
    int64_t one = 1;
    int v[3] = {m.num_c, m.num_n, m.ct_mode};
    CKS(disco_npz_put(z, "Opts/NUM_C", "<i4", 1, &one, &v[0]));

@@ -160,6 +160,7 @@ int disco_read_opt(const char *path, disco_modules *m){
    if( opt_value(path, "ANALYSIS", v, sizeof v) ) m->analysis = DISCO_DIAG_NONE;
    else if( !strcmp(v, "diag_disk2d") ) m->analysis = DISCO_DIAG_DISK2D;
    else if( !strcmp(v, "diag_euler") ) m->analysis = DISCO_DIAG_EULER;
+   else if( !strcmp(v, "diag_mhdmri") ) m->analysis = DISCO_DIAG_MHDMRI;
    else m->analysis = DISCO_DIAG_NONE;
    if( opt_value(path, "GEOMETRY", v, sizeof v) || strcmp(v, "cylindrical") )
       return DISCO_ERR_UNSUPPORTED;

@@ -84,7 +84,8 @@ static void gpu_init(struct domain *d){
     * boundaries that do not call it again (zerograd, outflow3d) run as is */
    if( m.initial < 0 ) m.initial = DISCO_IC_HOST;
    m.analysis = strcmp(ANALYSIS, "diag_disk2d") == 0 ? DISCO_DIAG_DISK2D :
-                strcmp(ANALYSIS, "diag_euler") == 0 ? DISCO_DIAG_EULER : DISCO_DIAG_NONE;
+                strcmp(ANALYSIS, "diag_euler") == 0 ? DISCO_DIAG_EULER :
+                strcmp(ANALYSIS, "diag_mhdmri") == 0 ? DISCO_DIAG_MHDMRI : DISCO_DIAG_NONE;
    m.num_c = NUM_C; m.num_n = NUM_N; m.ct_mode = CT_MODE;
    if( m.hydro < 0 || m.boundary < 0 || m.planets < 0 || m.initial < 0 )
       fail("module selection", DISCO_ERR_UNSUPPORTED);

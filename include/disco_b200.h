@@ -65,7 +65,8 @@ enum disco_planets  { DISCO_PLANETS_NONE = 0, DISCO_PLANETS_SUN = 1, DISCO_PLANE
  * only boundaries that never re-evaluate initial() during the steps
  * (zerograd, outflow3d) are accepted. */
 enum disco_initial  { DISCO_IC_KEPLER_NOISE = 0, DISCO_IC_MHD_SHEAR_NOISE = 1, DISCO_IC_HOST = 2 };
-enum disco_analysis { DISCO_DIAG_NONE = 0, DISCO_DIAG_DISK2D = 1, DISCO_DIAG_EULER = 2 };
+enum disco_analysis { DISCO_DIAG_NONE = 0, DISCO_DIAG_DISK2D = 1, DISCO_DIAG_EULER = 2,
+                      DISCO_DIAG_MHDMRI = 3 };
 enum disco_precision{ DISCO_PREC_FP64 = 0, DISCO_PREC_MIXED = 1 };
 
 /* Compile-time module selection (Makefile_opt.in).  num_c/num_n/ct_mode are

@@ -133,6 +133,8 @@ CASES = {
     "c0_diag_euler": ("c0_diag_euler", {"Num_R": 24, "Mass_Ratio": 1.0e-3, "Energy_Omega": 0}, 6),
     "c0_diag_euler3d": ("c0_diag_euler3d", {"Num_R": 10, "Num_Z": 4, "Grav2D": 1, "Z_Min": -0.3,
                                             "Z_Max": 0.3}, 4),
+    # Diagnostics/diag_mhdmri.c (18 annulus averages of the MHD state)
+    "c1_diag_mhdmri": ("c1_diag_mhdmri", {"Num_R": 12}, 6),
     # an outer edge without ghost annuli (NoBC_Rmax 1): the last real
     # annulus has no outer track
     "c0_nobc_rmax": ("c0_nograv", {"Num_R": 16, "Log_Zoning": 0, "Init_Par2": 1,
@@ -150,7 +152,7 @@ BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": 
             "c1_polar": "c1_mhd2d", "c1_polar3d": "c1_mhd3d", "c0_outflow3d": "c0_kepler2d",
             "c1_omk3d": "c1_mhd3d", "c1_accrete3d": "c1_mhd3d", "c0_rigid_zg": "c0_kepler2d",
             "c0_circular": "c0_kepler2d", "c0_cm": "c0_kepler2d", "c0_diag_euler": "c0_kepler2d",
-            "c0_diag_euler3d": "c0_kepler2d"}
+            "c0_diag_euler3d": "c0_kepler2d", "c1_diag_mhdmri": "c1_mhd2d"}
 
 
 def par_text(cfg_par, overrides):

@@ -16,7 +16,7 @@ CASES = ["c0_log16", "c0_lin20", "c0_hll_fe_mm3", "c0_cm2", "c0_rigid"]
 MHD_CASES = ["c1_mhd_hlld", "c1_mhd_hllc", "c1_mhd_hll_fe", "c1_mhd_rigid"]
 # zero-gradient boundaries and 3D (z faces), also pinned to the reference binary
 EXT_CASES = ["c0_zg", "c0_3d", "c1_mhd3d", "c1_mhd3d_rigid", "c0_circular", "c0_cm", "c0_cm_t0",
-             "c0_diag_euler", "c0_diag_euler3d", "c0_nobc_rmax"]
+             "c0_diag_euler", "c0_diag_euler3d", "c0_nobc_rmax", "c1_diag_mhdmri"]
 
 
 def golden(case):

@@ -25,7 +25,8 @@ TOL = 1e-12          # relative L1, FP64 fields (north_star)
 # libm-free twin (c1_mhd_rigid) is held to bit equality.
 CASE_TOL = {"c0_hll_fe_mm3": 1e-11, "c1_mhd_hlld": 1e-11, "c1_mhd_hllc": 1e-11,
             "c1_mhd_hll_fe": 1e-11, "c1_mhd3d": 1e-11, "c0_3d": 1e-11,
-            "c0_circular": 1e-11, "c0_cm": 1e-11, "c0_cm_t0": 1e-11, "c0_diag_euler3d": 1e-11}
+            "c0_circular": 1e-11, "c0_cm": 1e-11, "c0_cm_t0": 1e-11, "c0_diag_euler3d": 1e-11,
+            "c1_diag_mhdmri": 1e-11}
 BITEXACT = ("c0_rigid", "c1_mhd_rigid", "c1_mhd3d_rigid", "c0_nobc_rmax")
 
 
