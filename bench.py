@@ -44,9 +44,9 @@ def peaks():
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one first-substep launch on
-# the ragged8 workload (1,049,795 cells, 2,089,252 r-faces), from the ncu
-# captures summarised in profiles/k_update_ragged8_fp64.md and
-# profiles/k_flux_t_ragged8_fp64.md: (bytes, units the launch processed)
+# the ragged8 workload (1,049,795 cells, 2,089,252 r-faces), from an ncu
+# capture of k_update and k_flux_t on that workload: (bytes, units the
+# launch processed)
 DRAM_UPDATE_RAGGED8 = (289.8e6 + 53.7e6, 1049795)
 DRAM_FLUX_RAGGED8 = (216.2e6 + 72.5e6, 2089252)
 
@@ -150,23 +150,71 @@ def make_disks(workload, rank):
     return workloads.ragged_disks(64, rank=rank)
 
 
-def reference_pars(workload, rank=0):
-    from disco_b200 import workloads, template_paths
+# The reference arm builds its in.par files here, in plain Python, so that it
+# imports nothing of the disco_b200 package: the same seeded draws as
+# disco_b200.workloads.ragged_specs (tests/test_bench_config.py checks that
+# they agree) written into the same template.
+TEMPLATE_PAR = os.path.join(REPO, "disco_b200", "templates", "c0_kepler2d.par")
+NDISK = {"ragged64": 64, "ragged8": 8, "config0": 1}
+
+
+def ragged_specs(ndisk, seed=314159, rank=0):
+    """(Num_R, Mach_Number, noise seed) per disk of a ragged workload."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    nr = rng.integers(32, 257, size=ndisk)
+    mach = rng.uniform(10.0, 40.0, size=ndisk)
+    seeds = seed + np.arange(ndisk) + rank * ndisk
+    return [(int(a), float(b), int(c)) for a, b, c in zip(nr, mach, seeds)]
+
+
+def template_par(overrides, directory):
+    """The config-0 template in.par with some keys replaced, written to a
+    new file in `directory`; returns its path."""
+    out = []
+    with open(TEMPLATE_PAR) as f:
+        for line in f:
+            tok = line.split()
+            if tok and tok[0] in overrides:
+                line = "%s\t\t%s\n" % (tok[0], overrides[tok[0]])
+            out.append(line)
+    fd, path = tempfile.mkstemp(suffix=".par", dir=directory)
+    with os.fdopen(fd, "w") as f:
+        f.write("".join(out))
+    return path
+
+
+def reference_pars(workload, directory, rank=0):
     if workload == "config0":
-        return [template_paths("c0_kepler2d")[0]], False
-    _, pars = workloads.ragged_disks(8 if workload == "ragged8" else 64, rank=rank, keep_pars=True)
-    return pars, True
+        return [template_par({}, directory)]
+    return [template_par({"Num_R": nr, "Mach_Number": repr(mach), "Init_Par0": s}, directory)
+            for nr, mach, s in ragged_specs(NDISK[workload], rank=rank)]
+
+
+def workload_config(workload, nreal):
+    """The `config` object of both arms' lines: the workload, nothing of
+    either implementation."""
+    base = ("64 2D Keplerian hydro disks" if workload == "ragged64" else
+            "8 2D Keplerian hydro disks" if workload == "ragged8" else "the config-0 2D Keplerian hydro disk")
+    grid = ("Num_R drawn from [32, 256] per disk (seeded), log r in [0.5, 3], Np constant per disk"
+            if workload.startswith("ragged") else "Num_R 128, log r in [0.5, 3], Np 452")
+    return {"workload": workload, "description": base, "disks_per_gpu": NDISK[workload],
+            "real_cells_per_gpu": int(nreal), "grid": grid,
+            "physics": "Euler, HLLC, PLM 1.5, RK2, CFL 0.5, sun gravity, fixed boundaries, Mesh_Motion 1",
+            "precision": "fp64",
+            "l2_policy": "inputs larger than L2 (%.2f GB of prim+cons state per GPU)" % (nreal * 8 * 2 * Q / 1e9)}
 
 
 def time_reference(workload, nsteps, max_workers=None):
     """The reference's serial CPU code on every disk of the workload, one
     process per disk, statically spread over the host cores.  Returns
-    (zone-updates/s, cores, sample description)."""
+    (zone-updates/s, cores, sample description, real cells)."""
     import pyoracle
     binary = pyoracle.ref_binary("c0_kepler2d")
     if not os.path.exists(binary):
         pyoracle.build_ref("c0_kepler2d")
-    pars, tmp = reference_pars(workload)
+    pdir = tempfile.mkdtemp(prefix="dpar_")
+    pars = reference_pars(workload, pdir)
     cores = max_workers or min(os.cpu_count() or 1, len(pars))
     work = []
     for p in pars:
@@ -180,7 +228,7 @@ def time_reference(workload, nsteps, max_workers=None):
         jobs = work[w::cores]
         cmd = " ; ".join("%s %s %d --time" % (binary, d, nsteps) for d in jobs)
         procs.append(subprocess.Popen(["bash", "-c", cmd], stdout=subprocess.PIPE, text=True))
-    per_worker, zones = [], 0
+    per_worker, zones, nreal = [], 0, 0
     for pr in procs:
         out, _ = pr.communicate()
         s = 0.0
@@ -189,27 +237,26 @@ def time_reference(workload, nsteps, max_workers=None):
                 r = json.loads(line)
                 s += r["seconds"]
                 zones += r["real_cells"] * r["steps"]
+                nreal += r["real_cells"]
         per_worker.append(s)
-    for d in work:
+    for d in work + [pdir]:
         subprocess.run(["rm", "-rf", d])
-    if tmp:
-        for p in pars:
-            os.unlink(p)
     wall = max(per_worker)
     sample = "%s: all %d disks x %d step(s), %d processes on %d cores, step-loop time only" % (
         workload, len(pars), nsteps, len(pars), cores)
-    return zones / wall, cores, sample
+    return zones / wall, cores, sample, nreal
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    v, cores, sample = time_reference(args.workload, max(1, args.steps // 4))
+    v, cores, sample, nreal = time_reference(args.workload, max(1, args.steps // 4))
     line = {"metric": METRIC, "value": v, "unit": "zone-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": args.workload, "parallelism": "one process per disk"},
+            "config": workload_config(args.workload, nreal),
+            "parallelism": "one host process per disk",
             "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
@@ -681,7 +728,7 @@ def run_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            v, cores, sample = time_reference(args.workload, 1)
+            v, cores, sample, _ = time_reference(args.workload, 1)
             cpu = {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "reference",
                    "sample": sample}
         except Exception as ex:  # reference binary missing on this machine
@@ -694,17 +741,14 @@ def run_ours(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": args.workload, "disks_per_gpu": len(disks), "real_cells_per_gpu": nreal,
-                       "cells_per_gpu_incl_ghosts": ncell, "r_faces_per_gpu": nf,
-                       "precision": "fp64 plain", "riemann": "HLLC", "timestepper": "RK2",
-                       "l2_policy": "inputs larger than L2 (%.1f GB of cell state per GPU)" %
-                                    (ncell * 8 * (6 * Q + 4) / 1e9),
-                       "parallelism": "independent disks per GPU" if world > 1 else "single GPU"},
+            "config": workload_config(args.workload, nreal),
+            "layout": {"cells_per_gpu_incl_ghosts": ncell, "r_faces_per_gpu": nf,
+                       "precision": "fp64 plain path"},
+            "parallelism": "independent disks per GPU" if world > 1 else "single GPU",
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                         "traffic_source": ("ncu dram bytes of one launch on ragged8, scaled by the "
-                                            "units processed (profiles/%s_ragged8_fp64.md)"
-                                            % ("k_update" if dom == "k_update" else "k_flux_t"))
+                         "traffic_source": ("ncu capture on ragged8 (dram bytes of one %s launch), "
+                                            "scaled by the units processed" % dom)
                          if traffic is not None else None,
                          "peak_kind": peak_kind},
             "step_roofline": {"bytes_per_zone_update": B_ALG_STEP, "achieved": step_gbs, "peak": hbm,

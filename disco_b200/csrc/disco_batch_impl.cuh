@@ -170,6 +170,7 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
     * substep built from the same piph; that substep marks them valid */
    v.topo_reuse = first && b->timestep_mode == 0;
    v.topo_set = !first;
+   v.move_c2p = first && !b->ct;
    cudaStream_t s = b->stream;
    unsigned ncb = (unsigned)b->cblk.size(), nfb = (unsigned)b->fblk.size();
    k_begin<Q,NC,R><<<ncb, CB, 0, s>>>(v, RK, first);                  mark(b, "k_begin");

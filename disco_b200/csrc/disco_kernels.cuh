@@ -114,6 +114,10 @@ struct ViewT {
     * behaviour of one launch sequence. */
    int *topo;
    int topo_reuse, topo_set;
+   /* move_cells + calc_dp of the first substep, done by k_c2p (1) or by the
+    * constrained-transport update (0): k_update reads the neighbour cells'
+    * pre-move dphi across its chunk edges, so it must not move any cell */
+   int move_c2p;
    /* energy-frame Omega of omega.c:62-110, evaluated once by k_precompute at
     * the radii the step uses (same device expressions, so bit-identical to
     * evaluating them in place): annulus centroid (om, dOm/dr) and r-face */
@@ -823,7 +827,10 @@ __device__ __forceinline__ QVec<Q,R> phi_face_flux_visc(const ViewT<R> &v, const
  *   flux gather  riemann.c:312-315 applied as phi_flux then trans_flux do
  *   add_source   misc.c:538-580 (euler source + planet_src), pre-move cell,
  *                FP64 in both forms (the disk's force balance)
- *   move/clean/calc_dp   misc.c:256-288 (first substep; piph_new from k_begin)
+ * The move of the first substep (move_cells / clean_pi / calc_dp,
+ * misc.c:256-288, to piph_new from k_begin) follows in k_c2p: the phi-face
+ * states here read the pre-move dphi of the cells next to the chunk, which
+ * another block owns, so no block of this kernel may move a cell.
  * calc_prim, the boundary, and the fused getmindt / diagnostics follow in
  * k_c2p (run inside this kernel instead, the extra registers cost more than
  * the saved re-read of cons: 1.73 against 1.69 ms per ragged64 step). */
@@ -1042,11 +1049,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
          if constexpr ( sizeof(R) != sizeof(double) ) v.ccarry[q*N + c] = (float)cc[q];
       }
    }
-   if( first && !v.ct ){            /* with CT the edge fields read the old piph first */
-      piph = v.piph_new[c];
-      dphi = get_dp(piph, v.piph_new[cprev], P.Pmax, &err);
-      v.piph[c] = piph; v.dphi[c] = dphi;
-   }
+   (void)first;                     /* the move follows in k_c2p (or k_ct_update) */
    raise_err(v, err);
 }
 
@@ -1208,6 +1211,8 @@ __device__ void ct_cons_B(const ViewT<R> &v, const DiskParams &P, int a, int c0,
                           int *err);
 
 /* ------------------------------------------------------------------ c2p
+ *   move         move_cells / calc_dp (misc.c:256-288) in the first substep
+ *                without constrained transport (v.move_c2p; k_c2p)
  *   calc_prim    misc.c:290-325 (cons2prim, FP64) on real cells, from cons
  *   boundary     Boundary/fixed.c:11-60 / fixed3d (ghosts re-initialised)
  * and, on the last substep, the next step's getmindt (misc.c:39-84) and the
@@ -1339,7 +1344,13 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v,
    double cons[Q];
    double piph = 0.0, dphi = 0.0;
    if( active ){
-      piph = v.piph[c]; dphi = v.dphi[c];
+      if( v.move_c2p ){             /* move_cells + calc_dp (misc.c:256-288) */
+         piph = v.piph_new[c];
+         dphi = get_dp(piph, v.piph_new[c0 + (i == 0 ? np-1 : i-1)], P.Pmax, &err);
+         v.piph[c] = piph; v.dphi[c] = dphi;
+      }else{
+         piph = v.piph[c]; dphi = v.dphi[c];
+      }
       if( real ){
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) cons[q] = v.cons[q*N + c];

@@ -29,7 +29,8 @@
 
 using namespace disco;
 
-/* Limits of the static scratch (all must hold for a call to be accepted). */
+/* Limits of the static scratch (all must hold for a call to be accepted;
+ * otherwise the call prints the limit and returns DISCO_ERR_ARG). */
 #define NA_MAX_ANN    65536          /* annuli (Nr*Nz)                        */
 #define NA_MAX_EDGES  8192           /* r_jph / z_kph entries each            */
 #define NA_BLOCK      256
@@ -50,10 +51,15 @@ static __device__ __align__(256) NoAllocScratch disco_noalloc_scratch;
 #define NA_MAX_DEV 64
 static NoAllocScratch *g_scratch_addr[NA_MAX_DEV];
 
+/* The viscous limit of euler.c's mindt (:357-375) needs only these
+ * parameters of the disk: Use_Viscosity, Use_As_Alpha, Viscosity. */
+struct NoAllocVisc { int visc, alpha; double nu; };
+
 __global__ void k_noalloc_mindt(NoAllocScratch *S, int nann, int ncell,
                                 const double *prim, const double *piph, const double *dphi,
                                 const double *wiph, double gam, double Pmax,
-                                int NgRa, int NgRb, int NgZa, int NgZb, int Nr, int Nz){
+                                int NgRa, int NgRb, int NgZa, int NgZb, int Nr, int Nz,
+                                NoAllocVisc vp_){
    __shared__ unsigned long long s_min[NA_BLOCK/32];
    int c = blockIdx.x*blockDim.x + threadIdx.x;
    double dtc = 1.0e300;
@@ -85,6 +91,13 @@ __global__ void k_noalloc_mindt(NoAllocScratch *S, int nann, int ncell,
          double dtm = dtr;
          if( dtm > dtp ) dtm = dtp;
          if( dtm > dtz ) dtm = dtz;
+         if( vp_.visc ){                           /* euler.c:357-375 */
+            DiskParams P;
+            P.gam = gam; P.visc = 1; P.visc_alpha = vp_.alpha; P.visc_nu = vp_.nu;
+            double pc[6];
+            for( int q=0 ; q<6 ; ++q ) pc[q] = prim[q*ncell + c];
+            dtm = visc_dt_limit(P, pc, r, dtm, rp, rm, zp, zm, get_dp(ph, phim, Pmax, &err));
+         }
          if( dtm == dtm ) dtc = dtm;
       }
    }
@@ -129,17 +142,32 @@ extern "C" int disco_mindt_noalloc(const disco_params *p, int hydro, int Nr, int
    if( !p || !Ng || !Np || !r_jph || !z_kph || !prim || !piph || !dphi || !wiph || !dt )
       return DISCO_ERR_ARG;
    if( hydro != DISCO_HYDRO_EULER ) return DISCO_ERR_UNSUPPORTED;
-   int nann = Nr*Nz;
-   if( Nr < 1 || Nz < 1 || nann > NA_MAX_ANN || Nr+1 > NA_MAX_EDGES || Nz+1 > NA_MAX_EDGES ){
+   /* the sizes are checked before any product of them is formed */
+   if( Nr < 1 || Nz < 1 || Nr > NA_MAX_EDGES-1 || Nz > NA_MAX_EDGES-1 ||
+       (long long)Nr*(long long)Nz > NA_MAX_ANN ){
       fprintf(stderr, "disco_mindt_noalloc: grid of %d x %d annuli exceeds the scratch limits "
                       "(%d annuli, %d edges per direction)\n", Nr, Nz, NA_MAX_ANN, NA_MAX_EDGES);
       return DISCO_ERR_ARG;
    }
+   const int nann = Nr*Nz;
    long long ncell = 0;
    int4 tab[1024];
    int dev = 0;
    if( cudaGetDevice(&dev) != cudaSuccess ) return DISCO_ERR_NO_DEVICE;
    if( dev < 0 || dev >= NA_MAX_DEV ) return DISCO_ERR_ARG;
+   /* The scratch used below is the current device's copy, so the caller's
+    * arrays must live on that device too (a stream of another device would
+    * fail at the first copy; an array of another device would be read
+    * through the wrong device's scratch). */
+   {
+      const void *arrs[4] = {prim, piph, dphi, wiph};
+      for( int m=0 ; m<4 ; ++m ){
+         cudaPointerAttributes at;
+         if( cudaPointerGetAttributes(&at, arrs[m]) != cudaSuccess ){ cudaGetLastError(); return DISCO_ERR_ARG; }
+         if( at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged ) return DISCO_ERR_ARG;
+         if( at.device != dev ) return DISCO_ERR_ARG;
+      }
+   }
    for( int a=0 ; a<nann ; ++a ){
       if( Np[a] < 1 ) return DISCO_ERR_ARG;
       ncell += Np[a];
@@ -178,7 +206,10 @@ extern "C" int disco_mindt_noalloc(const disco_params *p, int hydro, int Nr, int
       return DISCO_ERR_CUDA;
    k_noalloc_mindt<<<(unsigned)nblocks, NA_BLOCK, 0, s>>>(S, nann, (int)ncell, prim, piph, dphi, wiph,
                                                          p->Adiabatic_Index, p->phimax,
-                                                         Ng[0], Ng[1], Ng[2], Ng[3], Nr, Nz);
+                                                         Ng[0], Ng[1], Ng[2], Ng[3], Nr, Nz,
+                                                         NoAllocVisc{p->visc_flag ? 1 : 0,
+                                                                     p->alpha_flag ? 1 : 0,
+                                                                     p->viscosity});
    double dt0 = p->maxDT / p->CFL;                       /* misc.c:52-54 */
    if( dt0 <= 0.0 ) dt0 = 1.0e100;
    k_noalloc_finish<<<1, NA_BLOCK, 0, s>>>(S, (int)nblocks, dt0);

@@ -7,8 +7,12 @@
  * link time:
  *     void   timestep( struct domain * , double )   timestep.c:7-45
  *     double getmindt( struct domain * )            misc.c:39-84
- * main.c's loop (main.c:69-83) is unchanged.  The first call uploads the
- * domain (cells, grid, parameters) to the GPU; afterwards the state stays on
+ * main.c's loop (main.c:69-83) is unchanged.  disco_gpu_init(), called once
+ * after setupCells (main.c:47-62), uploads the domain (cells, grid,
+ * parameters) to the GPU and returns a status, so a host can catch a module
+ * selection the device does not run, or a CUDA error, before its loop; a
+ * host that does not call it gets the same upload from the first getmindt()
+ * or timestep(), which then exits on error.  Afterwards the state stays on
  * the device and struct domain's cells and planets are stale until
  * disco_gpu_sync_to_host() copies them back (call it before output, e.g. at
  * the top of possiblyOutput, domain.c:317; report() is replaced here and
@@ -68,12 +72,27 @@ static void fail(const char *what, int s){
    exit(1);
 }
 
-static void gpu_init(struct domain *d){
+static void report_err(const char *what, int s){
+   fprintf(stderr, "disco_b200 shim: %s: %s\n", what, disco_strerror(s));
+}
+
+/* Upload the domain after setupCells; returns DISCO_OK or the status of the
+ * step that failed (the batch is then released).  The module selection is
+ * checked first: a Hydro / Boundary / Planets module the device does not
+ * run, and an Analysis module whose diagnostics it does not compute
+ * (analysis.c:52-107 would fill theTools.Qrz every step), are refused with
+ * DISCO_ERR_UNSUPPORTED rather than run without them.  Calling it again
+ * re-uploads the domain. */
+int disco_gpu_init( const struct domain * d ){
    static const char *const hydros[] = {"euler", "mhd"};
    static const char *const bcs[] = {"fixed", "zerograd", "fixed3d", "polar", "outflow3d",
                                      "zerograd_omk", "accrete3d"};
    static const char *const pls[] = {"none", "sun", "cm2", "binary_soft", "circular", "cm"};
    static const char *const ics[] = {"kepler_noise", "mhd_shear_noise"};
+   static const char *const diags[] = {"diag_disk2d", "diag_euler", "diag_mhdmri"};
+   static const int diag_ids[] = {DISCO_DIAG_DISK2D, DISCO_DIAG_EULER, DISCO_DIAG_MHDMRI};
+   if( !d ) return DISCO_ERR_ARG;
+   if( g_batch ){ disco_batch_destroy(g_batch); g_batch = NULL; }
    disco_modules m;
    memset(&m, 0, sizeof m);
    m.hydro = module_id(HYDRO, hydros, 2);
@@ -83,19 +102,18 @@ static void gpu_init(struct domain *d){
    /* any other Initial module: setupCells evaluated it here on the host, and
     * boundaries that do not call it again (zerograd, outflow3d) run as is */
    if( m.initial < 0 ) m.initial = DISCO_IC_HOST;
-   m.analysis = strcmp(ANALYSIS, "diag_disk2d") == 0 ? DISCO_DIAG_DISK2D :
-                strcmp(ANALYSIS, "diag_euler") == 0 ? DISCO_DIAG_EULER :
-                strcmp(ANALYSIS, "diag_mhdmri") == 0 ? DISCO_DIAG_MHDMRI : DISCO_DIAG_NONE;
+   int ia = module_id(ANALYSIS, diags, 3);
+   m.analysis = ia >= 0 ? diag_ids[ia] : DISCO_DIAG_NONE;
    m.num_c = NUM_C; m.num_n = NUM_N; m.ct_mode = CT_MODE;
-   if( m.hydro < 0 || m.boundary < 0 || m.planets < 0 || m.initial < 0 )
-      fail("module selection", DISCO_ERR_UNSUPPORTED);
+   if( m.hydro < 0 || m.boundary < 0 || m.planets < 0 || m.initial < 0 ) return DISCO_ERR_UNSUPPORTED;
+   if( ia < 0 && d->num_tools > 0 ) return DISCO_ERR_UNSUPPORTED;
    disco_params p;
    fill_params(d, &p);
    int Nr = d->Nr, Nz = d->Nz, jk, i, q;
    int Ng[4] = {d->NgRa, d->NgRb, d->NgZa, d->NgZb};
    int s = disco_batch_create(0, &m, DISCO_PREC_FP64, 1, &p, &Nr, &Nz, Ng, d->Np,
                               d->r_jph - 1, d->z_kph - 1, &g_batch);
-   if( s ) fail("disco_batch_create", s);
+   if( s ){ g_batch = NULL; return s; }
    int64_t ncell;
    disco_batch_sizes(g_batch, &ncell, NULL, NULL);
    double *prim = malloc(sizeof(double)*NUM_Q*ncell), *cons = malloc(sizeof(double)*NUM_Q*ncell);
@@ -104,19 +122,25 @@ static void gpu_init(struct domain *d){
    int *real = malloc(sizeof(int)*ncell);
    /* the constrained-transport face fluxes, cell->Phi[NUM_FACES] */
    double *phis = NUM_FACES > 0 && d->theParList.CT ? malloc(sizeof(double)*(NUM_FACES > 0 ? NUM_FACES : 1)*ncell) : NULL;
+   if( !prim || !cons || !piph || !dphi || !wiph || !real || (NUM_FACES > 0 && d->theParList.CT && !phis) ){
+      free(prim); free(cons); free(piph); free(dphi); free(wiph); free(real); free(phis);
+      disco_batch_destroy(g_batch); g_batch = NULL;
+      return DISCO_ERR_ARG;
+   }
    int64_t n = 0;
    for( jk=0 ; jk<Nr*Nz ; ++jk ) for( i=0 ; i<d->Np[jk] ; ++i, ++n ){
-      struct cell *c = &d->theCells[jk][i];
+      const struct cell *c = &d->theCells[jk][i];
       for( q=0 ; q<NUM_Q ; ++q ){ prim[NUM_Q*n+q] = c->prim[q]; cons[NUM_Q*n+q] = c->cons[q]; }
       piph[n] = c->piph; dphi[n] = c->dphi; wiph[n] = c->wiph; real[n] = c->real;
       if( phis ) for( q=0 ; q<NUM_FACES ; ++q ) phis[NUM_FACES*n+q] = c->Phi[q];
    }
    s = disco_batch_set_cells(g_batch, prim, cons, piph, dphi, wiph, real, phis);
    free(prim); free(cons); free(piph); free(dphi); free(wiph); free(real); free(phis);
-   if( s ) fail("disco_batch_set_cells", s);
+   if( s ){ disco_batch_destroy(g_batch); g_batch = NULL; return s; }
    /* the planets as the host domain holds them: a restart reads them from
     * the checkpoint (h5in.c:291-318), not from initializePlanets */
    double *pl = malloc(sizeof(double)*DISCO_PLANET_COLS*(d->Npl > 0 ? d->Npl : 1));
+   if( !pl ){ disco_batch_destroy(g_batch); g_batch = NULL; return DISCO_ERR_ARG; }
    int ip;
    for( ip=0 ; ip<d->Npl ; ++ip ){
       const struct planet *P = d->thePlanets + ip;
@@ -126,7 +150,14 @@ static void gpu_init(struct domain *d){
    }
    s = disco_batch_set_planets(g_batch, 0, pl, d->Npl);
    free(pl);
-   if( s ) fail("disco_batch_set_planets", s);
+   if( s ){ disco_batch_destroy(g_batch); g_batch = NULL; return s; }
+   return DISCO_OK;
+}
+
+/* the implicit upload of a host that did not call disco_gpu_init() */
+static void gpu_init(struct domain *d){
+   int s = disco_gpu_init(d);
+   if( s ){ report_err("disco_gpu_init", s); exit(1); }
 }
 
 /* getmindt replacement (misc.c:39-84): the device min-reduction. */

@@ -337,7 +337,10 @@ int disco_batch_kernel_times(disco_batch *b, float *ms, const char **names, int 
  * z_kph[Nz+1]) and device pointers to its cells in annulus order: prim as
  * structure-of-arrays (prim[q*ncell + c], q < 6), piph, dphi, wiph.  Work is
  * issued on `stream` (a cudaStream_t; NULL = default stream) and *dt (host)
- * receives CFL * min over real cells, the reference's getmindt value.
+ * receives CFL * min over real cells, the reference's getmindt value,
+ * including the viscous limit of Use_Viscosity (euler.c:357-375).  The
+ * arrays and the stream must belong to the current device; device arrays
+ * of another device return DISCO_ERR_ARG.
  *
  * Limits: Nr*Nz <= 65536 annuli, Nr+1 and Nz+1 <= 8192, ncell <= 2^26;
  * larger grids return DISCO_ERR_ARG.  Working memory is one static device

@@ -18,7 +18,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "liboracle_c2p.so")
 REF_LIB = os.path.join(HERE, "_ref", "c2p", "libc2p_ref.so")
-REF_SRC = "/root/reference"
+# the reference source tree the oracle builds compile; DISCO_REF overrides it
+REF_SRC = os.environ.get("DISCO_REF", "/root/reference")
 
 NPARAM = 64 * 8 + 64 + 64 * 64 + 64 + 2 * 64 + 2
 NNORM = 2 * 8 + 2 * 2
@@ -46,7 +47,7 @@ def build_c2p_ref():
         if os.path.exists(REF_LIB):
             return REF_LIB
         raise FileNotFoundError("reference tree absent and oracle/_ref/c2p not built")
-    subprocess.run(["make", "-s", "-C", HERE, "c2p"], check=True, stdout=subprocess.DEVNULL)
+    subprocess.run(["make", "-s", "-C", HERE, "c2p", "REF=" + REF_SRC], check=True, stdout=subprocess.DEVNULL)
     return REF_LIB
 
 

@@ -16,7 +16,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "liboracle.so")
-REF_SRC = "/root/reference"
+# the reference source tree the oracle builds compile; DISCO_REF overrides it
+REF_SRC = os.environ.get("DISCO_REF", "/root/reference")
 
 
 def build_oracle(force=False):
@@ -45,7 +46,7 @@ def build_ref(cfg):
         if os.path.exists(ref_binary(cfg)):
             return ref_binary(cfg)
         raise FileNotFoundError("reference tree absent and oracle/_ref/%s not built" % cfg)
-    subprocess.run(["make", "-s", "-C", HERE, "CFG=" + cfg, "-j8"], check=True,
+    subprocess.run(["make", "-s", "-C", HERE, "CFG=" + cfg, "REF=" + REF_SRC, "-j8"], check=True,
                    stdout=subprocess.DEVNULL)
     return ref_binary(cfg)
 

@@ -40,6 +40,7 @@ void freeDomain( struct domain * );
 /* Present only when this driver is linked with the GPU drop-in
  * (disco_b200/shim): copies the device state back into the cells. */
 void disco_gpu_sync_to_host( struct domain * ) __attribute__((weak));
+int disco_gpu_init( const struct domain * ) __attribute__((weak));
 int disco_gpu_get_faces( struct domain * , int , int * , int * , int * , int * , int * ) __attribute__((weak));
 int disco_gpu_last_error( void ) __attribute__((weak));
 void disco_gpu_free( void ) __attribute__((weak));
@@ -133,6 +134,12 @@ int main(int argc, char *argv[]){
    if( theDomain.Nz > 1 ){
       exchangeData( &theDomain , 1 );
       if( !theDomain.theParList.Z_Periodic ) boundary_trans( &theDomain , 2 );
+   }
+
+   /* the drop-in's explicit upload, after main.c's set-up and boundaries */
+   if( disco_gpu_init ){
+      int st = disco_gpu_init( &theDomain );
+      if( st != 0 ){ fprintf(stderr, "disco_gpu_init: status %d\n", st); return 4; }
    }
 
    int Nr = theDomain.Nr, Nz = theDomain.Nz;

@@ -1,7 +1,8 @@
 """The drop-in: the reference's own host code (read_par_file, setupGrid,
 setupDomain, setupCells, boundary_trans -- everything but timestep() and
-getmindt()) linked with disco_b200/shim, i.e. exactly the link-time
-substitution of INTEGRATION.md, against the unmodified reference binary.
+getmindt()) linked with disco_b200/shim, i.e. the link-time substitution
+a Disco maintainer makes, against the unmodified reference binary.  The
+driver calls the shim's disco_gpu_init after set-up, as a host would.
 
 Both binaries are built from the reference sources by oracle/Makefile
 (targets disco_ref and hybrid) wherever the reference tree is available."""
