@@ -36,6 +36,7 @@ BOUNDARY = {"fixed": 0, "zerograd": 1, "fixed3d": 2, "polar": 3, "outflow3d": 4,
 PLANETS = {"none": 0, "sun": 1, "cm2": 2, "binary_soft": 3, "circular": 4, "cm": 5}
 INITIAL = {"kepler_noise": 0, "mhd_shear_noise": 1, "host": 2}
 PREC_FP64, PREC_MIXED = 0, 1
+SCHED_KERNELS, SCHED_PERSISTENT = 0, 1
 
 
 class DiscoError(RuntimeError):
@@ -113,6 +114,8 @@ def library():
         "disco_batch_last_error": (_I, [_P]),
         "disco_batch_kernel_times": (_I, [_P, C.POINTER(C.c_float), C.POINTER(C.c_char_p), _I, _IP]),
         "disco_batch_set_stream": (_I, [_P, _P]),
+        "disco_batch_set_schedule": (_I, [_P, _I]),
+        "disco_batch_get_schedule": (_I, [_P, _IP]),
         "disco_batch_debug_get": (_I, [_P, _I, _D]),
         "disco_read_par": (_I, [C.c_char_p, C.POINTER(Params), _IP]),
         "disco_read_opt": (_I, [C.c_char_p, C.POINTER(Modules)]),
@@ -333,6 +336,17 @@ class Batch:
         """Launch on an external cudaStream_t (an int handle; 0/None = own stream)."""
         _check(library().disco_batch_set_stream(self.h, C.c_void_p(stream_handle or None)),
                "disco_batch_set_stream")
+
+    @property
+    def schedule(self):
+        """SCHED_PERSISTENT (the step as one launch) or SCHED_KERNELS."""
+        x = C.c_int()
+        _check(library().disco_batch_get_schedule(self.h, C.byref(x)), "disco_batch_get_schedule")
+        return x.value
+
+    @schedule.setter
+    def schedule(self, sched):
+        _check(library().disco_batch_set_schedule(self.h, int(sched)), "disco_batch_set_schedule")
 
     def kernel_times(self, cap=64):
         """One instrumented step: [(kernel name, device ms), ...] in launch order."""

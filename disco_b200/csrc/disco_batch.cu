@@ -149,6 +149,148 @@ static void make_float_view(disco_batch *b){
 
 extern "C" void disco_batch_destroy(disco_batch *b);
 
+/* ---- the one-launch step (disco_step_persist.cuh) ---------------------- */
+
+/* the module selections the persistent step covers */
+static bool persist_eligible(const disco_batch *b){
+   return !b->ct && !b->any_3d && !b->bc_zerograd && !b->any_mm3 && !b->any_visc &&
+          b->timestep_mode == 0 && (b->bc_fixed == 0 || b->bc_fixed == 1 || b->bc_fixed == 3);
+}
+
+/* The work list: every block of both substeps and the per-disk items, each
+ * with a position P in its disk's pipeline such that everything an item
+ * reads from has a smaller P: with W = 16 positions per annulus, substep
+ * base B (8, or W (Nr+4) + 8 for the second substep) and j the annulus (for
+ * a track, its inner annulus):
+ *   begin(j) B + Wj      I0(j..)  B + Wj + 1       faces(j,j+1) B + W(j+1) + 2
+ *   grad(j)  B + W(j+1) + 3   flux(j,j+1) B + W(j+2) + 4
+ *   update(j) B + W(j+2) + 5  c2p(j) B + W(j+2) + 6
+ *   timestep() start 0, planets after substep 1 W(Nr+4) + 4,
+ *   diagnostics of annuli ..j  second B + W(j+2) + 7, end 2W(Nr+4) + 16.
+ * Keys are P over the disk's total (all disks advance together), cut into
+ * tiles of about 8 grids' worth of items; inside a tile the order is
+ * (substep, stage, key).  Every dependency has a smaller key and an earlier
+ * (substep, stage), so it comes earlier in the list. */
+static int build_persist_plan(disco_batch *b){
+   b->persist_ok = 0;
+   int bps = b->prec == DISCO_PREC_MIXED ? mixed_persist_blocks_per_sm(b) : persist_blocks_per_sm_t<double>(b);
+   int nsm = 0;
+   if( cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess ) return DISCO_ERR_CUDA;
+   if( bps < 1 || nsm < 1 ) return DISCO_OK;           /* not resident: keep the kernels */
+   const long G = (long)bps*nsm;
+   const int nann = (int)b->ann_np.size(), ntr = (int)b->tr_a.size(), nd = b->ndisk;
+   std::vector<int> nu(nann, 0), nf(ntr, 0), ndc(nd, 0);
+   for( const int2 &u : b->ublk ) nu[u.x]++;
+   for( const int2 &f : b->fblk ) nf[f.x]++;
+   for( int a=0 ; a<nann ; ++a ) ndc[b->ann_disk[a]] += b->ann_nblk[a];
+   struct It { int4 w; int sub, rank, disk, tile; double key; };
+   std::vector<It> L;
+   L.reserve(2*(3*b->cblk.size() + 2*b->fblk.size() + b->ublk.size()) + 4*nd + nann);
+   const long W = 16;
+   auto add = [&](int stage, int sub, int rank, int x, int n, int d, long P){
+      long Nr = b->disk_Nr[d];
+      double tot = (double)(2*W*(Nr+4) + 16);
+      It it;
+      it.w = make_int4(stage | (sub << 4), x, n, 0);
+      it.sub = sub; it.rank = rank; it.disk = d; it.tile = 0;
+      it.key = (double)P / tot;
+      L.push_back(it);
+   };
+   auto base = [&](int sub, int d){ return sub ? W*((long)b->disk_Nr[d] + 4) + 8 : 8L; };
+   for( int d=0 ; d<nd ; ++d ) add(PS_DBEGIN, 0, 0, d, 1, d, 0);
+   for( int sub=0 ; sub<2 ; ++sub ){
+      for( int cb=0 ; cb<(int)b->cblk.size() ; ++cb ){
+         int a = b->cblk[cb].x, d = b->ann_disk[a];
+         long j = b->ann_j[a], B = base(sub, d);
+         add(PS_BEGIN, sub, 1, cb, 1, d, B + W*j);
+         add(PS_GRAD, sub, 4, cb, 1, d, B + W*(j+1) + 3);
+         add(PS_C2P, sub, 7, cb, 1, d, B + W*(j+2) + 6);
+      }
+      for( int d=0 ; d<nd ; ++d ){
+         int a0 = b->dparams[d].ann0, na = b->disk_Nr[d]*b->disk_Nz[d];
+         for( int a=a0 ; a<a0+na ; a+=4 ){
+            int n = a0 + na - a < 4 ? a0 + na - a : 4;
+            add(PS_I0, sub, 2, a, n, d, base(sub, d) + W*b->ann_j[a] + 1);
+         }
+      }
+      for( int fb=0 ; fb<(int)b->fblk.size() ; ++fb ){
+         int t = b->fblk[fb].x, d = b->ann_disk[b->tr_a[t]];
+         long j = b->tr_j[t], B = base(sub, d);
+         add(PS_FACES, sub, 3, fb, 1, d, B + W*(j+1) + 2);
+         add(PS_FLUX, sub, 5, fb, 1, d, B + W*(j+2) + 4);
+      }
+      for( int ub=0 ; ub<(int)b->ublk.size() ; ++ub ){
+         int a = b->ublk[ub].x, d = b->ann_disk[a];
+         add(PS_UPDATE, sub, 6, ub, 1, d, base(sub, d) + W*(long)(b->ann_j[a]+2) + 5);
+      }
+   }
+   for( int d=0 ; d<nd ; ++d ) add(PS_DMID, 0, 8, d, 1, d, W*((long)b->disk_Nr[d] + 4) + 4);
+   if( b->nq ){
+      for( int d=0 ; d<nd ; ++d ){
+         int a0 = b->dparams[d].ann0, na = b->disk_Nr[d]*b->disk_Nz[d];
+         for( int a=a0 ; a<a0+na ; a+=CB ){
+            int n = a0 + na - a < CB ? a0 + na - a : CB;
+            add(PS_DIAGFIN, 1, 8, a, n, d, base(1, d) + W*(long)(b->ann_j[a+n-1]+2) + 7);
+         }
+      }
+   }
+   for( int d=0 ; d<nd ; ++d ) add(PS_DTAIL, 1, 9, d, 1, d, 2*W*((long)b->disk_Nr[d] + 4) + 16);
+   long NT = (long)L.size() / (8*G);
+   if( NT < 1 ) NT = 1;
+   for( It &it : L ){
+      long tl = (long)(it.key*(double)NT);
+      it.tile = (int)(tl < NT-1 ? tl : NT-1);
+   }
+   std::stable_sort(L.begin(), L.end(), [](const It &x, const It &y){
+      if( x.tile != y.tile ) return x.tile < y.tile;
+      if( x.sub != y.sub ) return x.sub < y.sub;
+      if( x.rank != y.rank ) return x.rank < y.rank;
+      if( x.key != y.key ) return x.key < y.key;
+      if( x.disk != y.disk ) return x.disk < y.disk;
+      return x.w.y < y.w.y;
+   });
+   std::vector<int4> items(L.size());
+   for( size_t i=0 ; i<L.size() ; ++i ) items[i] = L[i].w;
+   /* completion counters */
+   PersistArgs &pa = b->pargs;
+   memset(&pa, 0, sizeof pa);
+   int o = 0;
+   for( int sub=0 ; sub<2 ; ++sub ){
+      pa.o_begin[sub] = o; o += nann;
+      pa.o_I0[sub] = o;    o += nann;
+      pa.o_faces[sub] = o; o += ntr;
+      pa.o_grad[sub] = o;  o += nann;
+      pa.o_flux[sub] = o;  o += ntr;
+      pa.o_upd[sub] = o;   o += nann;
+      pa.o_c2p[sub] = o;   o += nann;
+      pa.o_c2pd[sub] = o;  o += nd;
+   }
+   pa.o_d0 = o; o += nd;
+   pa.o_d1 = o; o += nd;
+   int octl = o; o += 2;
+   b->d_pcnt = dalloc<int>(b, (size_t)o);
+   b->pcnt_bytes = (size_t)o*sizeof(int);
+   b->d_pitems = dupload(b, items);
+   b->pnitems = (int)items.size();
+   b->pgrid = (int)G;
+   pa.items = b->d_pitems;
+   pa.nitems = b->pnitems;
+   pa.cnt = b->d_pcnt;
+   pa.ctl = b->d_pcnt + octl;
+   pa.nc = b->d_ann_nblk;
+   pa.nu = dupload(b, nu);
+   pa.nf = dupload(b, nf);
+   pa.ndc = dupload(b, ndc);
+   pa.Qrz = b->d_Qrz;
+   pa.ann_blk0 = b->d_ann_blk0;
+   pa.ann_nblk = b->d_ann_nblk;
+   pa.bc = b->bc_fixed;
+   pa.diag = !b->bc_zerograd;
+   if( !b->d_pcnt || !b->d_pitems || !pa.nu || !pa.nf || !pa.ndc ) return DISCO_ERR_CUDA;
+   b->persist_ok = 1;
+   return DISCO_OK;
+}
+
 extern "C" int disco_batch_create(int device, const disco_modules *mods, int precision,
                                   int ndisk, const disco_params *params,
                                   const int *Nr, const int *Nz, const int *Ng,
@@ -484,8 +626,31 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       k_precompute<<<nblk(nx, 128), 128, 0, b->stream>>>(v);
       k_planet_trig<double><<<nblk(ndisk, 64), 64, 0, b->stream>>>(v, ndisk);
    }
+   b->sched = DISCO_SCHED_KERNELS;
+   if( persist_eligible(b) ){
+      if( build_persist_plan(b) != DISCO_OK ){ disco_batch_destroy(b); return DISCO_ERR_CUDA; }
+      if( b->persist_ok ) b->sched = DISCO_SCHED_PERSISTENT;
+   }
    if( cudaDeviceSynchronize() != cudaSuccess ){ disco_batch_destroy(b); return DISCO_ERR_CUDA; }
    *out = b;
+   return DISCO_OK;
+}
+
+extern "C" int disco_batch_set_schedule(disco_batch *b, int sched){
+   if( !b ) return DISCO_ERR_ARG;
+   if( sched != DISCO_SCHED_KERNELS && sched != DISCO_SCHED_PERSISTENT ) return DISCO_ERR_ARG;
+   if( sched == DISCO_SCHED_PERSISTENT && !b->persist_ok ) return DISCO_ERR_UNSUPPORTED;
+   if( sched == b->sched ) return DISCO_OK;
+   CK(cudaSetDevice(b->device));
+   CK(cudaStreamSynchronize(b->stream));
+   if( b->graph ){ cudaGraphExecDestroy(b->graph); b->graph = NULL; }   /* recaptured on the next run */
+   b->sched = sched;
+   return DISCO_OK;
+}
+
+extern "C" int disco_batch_get_schedule(const disco_batch *b, int *sched){
+   if( !b || !sched ) return DISCO_ERR_ARG;
+   *sched = b->sched;
    return DISCO_OK;
 }
 
@@ -676,7 +841,7 @@ static int read_err(disco_batch *b){
    }
    if( e & ERRF_WRAP ) return DISCO_ERR_PHI_WRAP;
    if( e & ERRF_NONFINITE ) return DISCO_ERR_NONFINITE;
-   if( e & ERRF_INTERNAL ) return DISCO_ERR_INTERNAL;
+   if( e & (ERRF_INTERNAL | ERRF_TIMEOUT) ) return DISCO_ERR_INTERNAL;
    return DISCO_OK;
 }
 

@@ -10,6 +10,7 @@
 #include "disco_b200.h"
 #include "disco_kernels.cuh"
 #include "disco_ct.cuh"
+#include "disco_step_persist.cuh"
 
 using namespace disco;
 
@@ -65,6 +66,17 @@ struct disco_batch {
    int nfs;                  /* face-flux slots per cell (NUM_FACES: 3 or 5) */
    std::vector<int> line_off;           /* edge lines of 3D CT, offsets into lineX */
    int line_ne;
+   /* the one-launch step (disco_step_persist.cuh): schedule in use, whether
+    * the batch's modules allow it, its sorted work list, completion
+    * counters (zeroed before each launch) and resident grid */
+   int sched;
+   int persist_ok;
+   int4 *d_pitems;
+   int pnitems;
+   int *d_pcnt;
+   size_t pcnt_bytes;
+   int pgrid;
+   PersistArgs pargs;
 };
 
 static inline unsigned nblk(size_t n, unsigned t){ return (unsigned)((n + t - 1)/t); }
@@ -216,9 +228,51 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    }
 }
 
+/* timestep() as one cooperative launch of k_step (the counters zeroed first) */
+template<int Q, int NC, class R, int NQD>
+static void launch_persist_nq(disco_batch *b, const ViewT<R> &v, int use_next){
+   PersistArgs pa = b->pargs;
+   pa.use_next = use_next;
+   cudaMemsetAsync(b->d_pcnt, 0, b->pcnt_bytes, b->stream);
+   cudaLaunchConfig_t cfg = {};
+   cfg.gridDim = dim3((unsigned)b->pgrid);
+   cfg.blockDim = dim3(CB);
+   cfg.dynamicSmemBytes = 0;
+   cfg.stream = b->stream;
+   cudaLaunchAttribute at[1];
+   at[0].id = cudaLaunchAttributeCooperative;
+   at[0].val.cooperative = 1;
+   cfg.attrs = at;
+   cfg.numAttrs = 1;
+   cudaLaunchKernelEx(&cfg, k_step<Q,NC,R,NQD>, v, pa);
+   mark(b, "k_step");
+}
+template<int Q, int NC, class R>
+static void launch_persist(disco_batch *b, const ViewT<R> &v, int use_next){
+   if constexpr ( NC == 8 ){
+      if( b->nq == 18 ){ launch_persist_nq<Q,NC,R,18>(b, v, use_next); return; }
+   }
+   if( b->nq == 8 ) launch_persist_nq<Q,NC,R,8>(b, v, use_next);
+   else launch_persist_nq<Q,NC,R,5>(b, v, use_next);
+}
+/* resident k_step CTAs per SM for the batch's instantiation */
+template<int Q, int NC, class R, int NQD>
+static int persist_occ_nq(){
+   int nb = 0;
+   if( cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<Q,NC,R,NQD>, CB, 0) != cudaSuccess ) return 0;
+   return nb;
+}
+template<class R>
+static int persist_blocks_per_sm_t(const disco_batch *b){
+   if( b->NC == 8 ) return b->nq == 18 ? persist_occ_nq<9,8,R,18>() : b->nq == 8 ? persist_occ_nq<9,8,R,8>()
+                                                                                  : persist_occ_nq<9,8,R,5>();
+   return b->nq == 8 ? persist_occ_nq<6,5,R,8>() : persist_occ_nq<6,5,R,5>();
+}
+
 /* timestep() (timestep.c:7-45). */
 template<int Q, int NC, class R>
 static void launch_step_qt(disco_batch *b, const ViewT<R> &v, int use_next){
+   if( b->sched == DISCO_SCHED_PERSISTENT ){ launch_persist<Q,NC,R>(b, v, use_next); return; }
    cudaStream_t s = b->stream;
    unsigned nd = nblk(b->ndisk, 64);
    k_disk_begin<R><<<nd, 64, 0, s>>>(v, b->ndisk, use_next);          mark(b, "k_disk_begin");
@@ -281,6 +335,7 @@ void mixed_launch_step(disco_batch *b, int use_next);
 void mixed_launch_prim2cons(disco_batch *b);
 void mixed_launch_faces(disco_batch *b);
 int mixed_prepare_zerograd(disco_batch *b);
+int mixed_persist_blocks_per_sm(const disco_batch *b);
 
 /* host <-> device copy on the batch's stream, completed on return
  * (disco_batch.cu; used by the writers of disco_output.cu) */

@@ -21,3 +21,4 @@ void mixed_launch_faces(disco_batch *b){
 int mixed_prepare_zerograd(disco_batch *b){
    return prepare_zerograd<6,float>(b) || prepare_zerograd<9,float>(b);
 }
+int mixed_persist_blocks_per_sm(const disco_batch *b){ return persist_blocks_per_sm_t<float>(b); }

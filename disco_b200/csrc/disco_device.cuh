@@ -27,7 +27,8 @@ namespace disco {
 
 enum { RHO = 0, PPP = 1, URR = 2, UPP = 3, UZZ = 4, BRR = 5, BPP = 6, BZZ = 7 };
 enum { DDD = 0, TAU = 1, SRR = 2, LLL = 3, SZZ = 4 };
-enum { ERRF_WRAP = 1, ERRF_NONFINITE = 2, ERRF_INTERNAL = 4 };
+enum { ERRF_WRAP = 1, ERRF_NONFINITE = 2, ERRF_INTERNAL = 4,
+       ERRF_TIMEOUT = 8 /* a bounded device wait ran out (persistent step) */ };
 
 struct Planet {
    double r, phi, M, omega, vr;

@@ -170,12 +170,12 @@ __device__ __forceinline__ void acc(double &s, double &cc, double x){
  * move_cells + clean_pi (misc.c:256-268, 8-26) into piph_new.
  * Every substep: adjust_RK_cons (misc.c:226-244) and plm_phi (plm.c:15-51). */
 template<int Q, int NC, class R>
-__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_BEGIN) k_begin(ViewT<R> v, double RK, int first){
+__device__ __forceinline__ void begin_body(const ViewT<R> &v, double RK, int first, int bid){
    /* the chunk's prims and dphi staged once, with one neighbour cell on each
     * side (slot t+1 = cell i0+t) */
    __shared__ R sp[Q][CB+2];
    __shared__ double sd[CB+2];
-   int2 b = v.cblk[blockIdx.x];
+   int2 b = v.cblk[bid];
    int a = b.x, i0 = b.y, t = threadIdx.x, i = i0 + t;
    int np = v.ann_np[a];
    const int N = v.Ncell;
@@ -260,6 +260,10 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_BEGIN) k_begin(ViewT<R
       v.gradp[q*N + c] = m;
    }
 }
+template<int Q, int NC, class R>
+__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_BEGIN) k_begin(ViewT<R> v, double RK, int first){
+   begin_body<Q,NC,R>(v, RK, first, blockIdx.x);
+}
 
 /* Energy-frame Omega at the radii the step evaluates it (omega.c:62-110):
  * annulus centroids (sources, phi faces, c2p) and r-faces (trans_flux). */
@@ -328,11 +332,9 @@ __global__ void __launch_bounds__(32*WM_WARPS) k_wmean(ViewT<R> v, int move){
  * quadrant IV (the cell whose upper edge is just past phi = 0).  One warp
  * per annulus, ballots over 32-cell chunks. */
 template<class R>
-__global__ void k_I0(ViewT<R> v){
-   int warp = (blockIdx.x*blockDim.x + threadIdx.x) >> 5;
-   int lane = threadIdx.x & 31;
+__device__ __forceinline__ void I0_body(const ViewT<R> &v, int topo_reuse, int warp, int lane){
    if( warp >= v.Nann ) return;
-   if( v.topo_reuse && *v.topo ) return;
+   if( topo_reuse && *v.topo ) return;
    int a = warp;
    int np = v.ann_np[a], c0 = v.ann_off[a];
    const DiskParams &P = v.dp[v.ann_disk[a]];
@@ -360,6 +362,10 @@ __global__ void k_I0(ViewT<R> v){
    }
    if( lane == 0 ) v.I0[a] = res;
 }
+template<class R>
+__global__ void k_I0(ViewT<R> v){
+   I0_body<R>(v, v.topo_reuse, (blockIdx.x*blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31);
+}
 
 /* ------------------------------------------------------------------ faces
  * buildfaces (faces_alt.c:102-177) as a merge path: face d of a track is
@@ -373,8 +379,8 @@ __global__ void k_I0(ViewT<R> v){
  * gather reads each twice (sum, limiter), and recomputing them there from
  * the two cells' scattered states was measured 5x slower than storing. */
 template<int Q, class R>
-__global__ void __launch_bounds__(FB, MB_FACES) k_faces(ViewT<R> v, int with_slopes){
-   int2 b = v.fblk[blockIdx.x];
+__device__ __forceinline__ void faces_body(const ViewT<R> &v, int with_slopes, int topo_reuse, int bid){
+   int2 b = v.fblk[bid];
    int t = b.x, dd = b.y + threadIdx.x;
    int A = v.tr_a[t], B = v.tr_b[t];
    int NA = v.ann_np[A], NB = v.ann_np[B];
@@ -387,7 +393,7 @@ __global__ void __launch_bounds__(FB, MB_FACES) k_faces(ViewT<R> v, int with_slo
    double Pmax = P.Pmax;
    int err = 0;
 
-   if( v.topo_reuse && *v.topo ){   /* same piph as the last build: slopes only */
+   if( topo_reuse && *v.topo ){     /* same piph as the last build: slopes only */
       if( !with_slopes ) return;
       int cL = v.fL[f], cR = v.fR[f];
       double phic = v.fphic[f];
@@ -467,6 +473,10 @@ __global__ void __launch_bounds__(FB, MB_FACES) k_faces(ViewT<R> v, int with_slo
    }
    raise_err(v, err);
 }
+template<int Q, class R>
+__global__ void __launch_bounds__(FB, MB_FACES) k_faces(ViewT<R> v, int with_slopes){
+   faces_body<Q,R>(v, with_slopes, v.topo_reuse, blockIdx.x);
+}
 
 /* The faces of track t in which cell c (k-th edge from I0 of its annulus,
  * cell index i) is the head on its side, in face order: run 1 is
@@ -498,8 +508,8 @@ __device__ __forceinline__ Runs cell_runs(const ViewT<R> &v, const int *cons, in
  * then outer / upper), divide by the cell's two face areas, then apply
  * every face's limiter. */
 template<int Q, int DIM, class R>
-__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_GRAD) k_grad(ViewT<R> v){
-   int2 b = v.cblk[blockIdx.x];
+__device__ __forceinline__ void grad_body(const ViewT<R> &v, int bid){
+   int2 b = v.cblk[bid];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
    if( i >= np ) return;
@@ -599,6 +609,10 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_GRAD) k_grad(ViewT<R> 
    for( int q=0 ; q<Q ; ++q ) grad[q*N + c] = g[q];
    raise_err(v, err);
 }
+template<int Q, int DIM, class R>
+__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_GRAD) k_grad(ViewT<R> v){
+   grad_body<Q,DIM,R>(v, blockIdx.x);
+}
 
 /* The viscous flux of a face, compiled only into the viscous instances of
  * k_flux_t / k_update (template VISC) so that the inviscid kernels keep
@@ -685,8 +699,8 @@ __device__ __forceinline__ double2 visc_source_cell(const ViewT<R> &v, const Dis
  * z centroid) for r-faces and (r centroid, phic, z_{k+1/2}) for z-faces
  * (addFace, faces_alt.c:10-16). */
 template<int Q, int NC, int DIM, class R, bool VISC = false>
-__global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R> v){
-   int2 b = v.fblk[blockIdx.x];
+__device__ __forceinline__ void flux_body(const ViewT<R> &v, double dtfac, int bid){
+   int2 b = v.fblk[bid];
    int t = b.x;
    if( v.tr_dim[t] != DIM || !v.tr_flux[t] ) return;
    int dd = b.y + threadIdx.x;
@@ -697,7 +711,7 @@ __global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R
    int d = v.ann_disk[v.tr_a[t]];
    const DiskParams &P = v.dp[d];
    int err = 0;
-   double dt = v.ds[d].dt*v.dtfac;
+   double dt = v.ds[d].dt*dtfac;
    double dAdt = v.fdA[f]*dt;
    R dxL = (R)v.tr_dxL[t], dxR = (R)v.tr_dxR[t];
    double phi = v.fphic[f];
@@ -752,6 +766,10 @@ __global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) v.fG[(size_t)q*v.Nf + f] = G[q];
    raise_err(v, err);
+}
+template<int Q, int NC, int DIM, class R, bool VISC = false>
+__global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R> v){
+   flux_body<Q,NC,DIM,R,VISC>(v, v.dtfac, blockIdx.x);
 }
 
 /* ------------------------------------------------------------------ phi faces
@@ -835,14 +853,14 @@ __device__ __forceinline__ QVec<Q,R> phi_face_flux_visc(const ViewT<R> &v, const
  * k_c2p (run inside this kernel instead, the extra registers cost more than
  * the saved re-read of cons: 1.73 against 1.69 ms per ragged64 step). */
 template<int Q, int NC, class R, bool VISC = false>
-__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT<R> v, int first){
+__device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double dtfac, int bid){
    /* The block updates CB-1 cells i0 .. i0+CB-2 and its thread t solves the
     * phi face (i0+t-1, i0+t) into sG[.][t]: every thread one face, the
     * chunk's two outer faces included (the left one is also the previous
     * chunk's last). */
    __shared__ R sG[Q][CB];
    __shared__ R sW[Q][CB+1];      /* sW[.][s]: left-edge state of cell i0+s-1 */
-   int2 b = v.ublk[blockIdx.x];
+   int2 b = v.ublk[bid];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
    const int N = v.Ncell;
@@ -867,7 +885,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
    }
    if( real || ctE ){               /* uniform over the block: one annulus */
       double dA = (rj[j]-rj[j-1])*(zk[k]-zk[k-1]);       /* get_dA(.,.,0) */
-      double dAdtp = dA*(v.ds[d].dt*v.dtfac);
+      double dAdtp = dA*(v.ds[d].dt*dtfac);
       double rc = centroid_r(rj[j], rj[j-1]);
       /* riemann_phi's edge states (riemann.c:45-50): thread t extrapolates
        * cell i-1 to both of its phi edges; the left-edge state goes to its
@@ -930,7 +948,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
    double piph = v.piph[c], dphi = v.dphi[c];
    if( real ){
       const DiskState &S = v.ds[d];
-      double dt = S.dt*v.dtfac;
+      double dt = S.dt*dtfac;
       double cons[Q], cc[Q];
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){
@@ -1051,6 +1069,10 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT
    }
    (void)first;                     /* the move follows in k_c2p (or k_ct_update) */
    raise_err(v, err);
+}
+template<int Q, int NC, class R, bool VISC = false>
+__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT<R> v, int first){
+   update_body<Q,NC,R,VISC>(v, first, v.dtfac, blockIdx.x);
 }
 
 /* One cell's terms of add_diagnostics (analysis.c:52-107) with the
@@ -1223,7 +1245,8 @@ template<int Q, int NC, class R, int NQD, bool VISC>
 __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P, int a, int c,
                                          int c0, int np, int i, int j, int k, int d, bool real,
                                          bool active, double piph, double dphi, double *cons,
-                                         int last, int bc, int diag, int err){
+                                         int last, int bc, int diag, int err, int topo_set,
+                                         int bid){
    __shared__ double s_red[CB/32][NQD+1];
    __shared__ unsigned long long s_dt[CB/32];
    const int N = v.Ncell;
@@ -1290,7 +1313,7 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
       }
    }
    raise_err(v, err);
-   if( v.topo_set && blockIdx.x == 0 && threadIdx.x == 0 ) *v.topo = 1;
+   if( topo_set && bid == 0 && threadIdx.x == 0 ) *v.topo = 1;
    if( !last ) return;
    /* block reductions (one annulus per block) */
    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1319,7 +1342,7 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
          for( int m=0 ; m<=NQD ; ++m ){
             double x = 0.0;
             for( int w=0 ; w<CB/32 ; ++w ) x += s_red[w][m];
-            v.diag_part[(size_t)blockIdx.x*DIAG_SLOTS + diag_slot<NQD>(m)] = x;
+            v.diag_part[(size_t)bid*DIAG_SLOTS + diag_slot<NQD>(m)] = x;
          }
       }
    }
@@ -1329,8 +1352,9 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
  * c2p_tail on each cell after k_update, with constrained transport first
  * rebuilding B from the face fluxes (onestep.c:183-185). */
 template<int Q, int NC, class R, int NQD = 5, bool VISC = false>
-__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v, int last, int bc, int diag){
-   int2 b = v.cblk[blockIdx.x];
+__device__ __forceinline__ void c2p_body(const ViewT<R> &v, int last, int bc, int diag, int move_c2p,
+                                         int topo_set, int bid){
+   int2 b = v.cblk[bid];
    int a = b.x, i = b.y + threadIdx.x;
    int np = v.ann_np[a];
    bool active = i < np;
@@ -1344,7 +1368,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v,
    double cons[Q];
    double piph = 0.0, dphi = 0.0;
    if( active ){
-      if( v.move_c2p ){             /* move_cells + calc_dp (misc.c:256-288) */
+      if( move_c2p ){               /* move_cells + calc_dp (misc.c:256-288) */
          piph = v.piph_new[c];
          dphi = get_dp(piph, v.piph_new[c0 + (i == 0 ? np-1 : i-1)], P.Pmax, &err);
          v.piph[c] = piph; v.dphi[c] = dphi;
@@ -1367,7 +1391,11 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v,
       }
    }
    c2p_tail<Q,NC,R,NQD,VISC>(v, P, a, c, c0, np, i, j, k, d, real, active, piph, dphi, cons, last,
-                             bc, diag, err);
+                             bc, diag, err, topo_set, bid);
+}
+template<int Q, int NC, class R, int NQD = 5, bool VISC = false>
+__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v, int last, int bc, int diag){
+   c2p_body<Q,NC,R,NQD,VISC>(v, last, bc, diag, v.move_c2p, v.topo_set, blockIdx.x);
 }
 
 /* The sequential walk of set_cells_copy_distant (boundary_functions.c:
@@ -1536,9 +1564,7 @@ __global__ void k_zerograd(ViewT<R> v, const int2 *pairs, const unsigned char *s
 /* ------------------------------------------------------------------ per disk */
 /* Start of timestep(): planet_RK_copy, reset of the dt reduction. */
 template<class R>
-__global__ void k_disk_begin(ViewT<R> v, int ndisk, int use_next){
-   int d = blockIdx.x*blockDim.x + threadIdx.x;
-   if( d >= ndisk ) return;
+__device__ __forceinline__ void disk_begin_body(const ViewT<R> &v, int d, int use_next){
    DiskState &S = v.ds[d];
    const DiskParams &P = v.dp[d];
    if( use_next ) S.dt = S.dt_next;
@@ -1550,6 +1576,11 @@ __global__ void k_disk_begin(ViewT<R> v, int ndisk, int use_next){
    double dt0 = P.maxDT / P.CFL;
    if( dt0 <= 0.0 ) dt0 = 1.0e100;
    S.dtmin = dbits(dt0);
+}
+template<class R>
+__global__ void k_disk_begin(ViewT<R> v, int ndisk, int use_next){
+   int d = blockIdx.x*blockDim.x + threadIdx.x;
+   if( d < ndisk ) disk_begin_body<R>(v, d, use_next);
 }
 
 /* cos / sin of the planets' phi at set-up (later kept by k_disk_begin/mid) */
@@ -1564,9 +1595,7 @@ __global__ void k_planet_trig(ViewT<R> v, int ndisk){
 /* After substep 1 (onestep.c:163-166, timestep.c:38): planet adjust/move,
  * planet phi wrap (clean_pi, misc.c:27-34), t += dt. */
 template<class R>
-__global__ void k_disk_mid(ViewT<R> v, int ndisk, double RK, int first, int advance_t){
-   int d = blockIdx.x*blockDim.x + threadIdx.x;
-   if( d >= ndisk ) return;
+__device__ __forceinline__ void disk_mid_body(const ViewT<R> &v, int d, double RK, int first, int advance_t){
    DiskState &S = v.ds[d];
    const DiskParams &P = v.dp[d];
    double dt = S.dt;
@@ -1594,13 +1623,16 @@ __global__ void k_disk_mid(ViewT<R> v, int ndisk, double RK, int first, int adva
    }
    if( advance_t ) S.t += dt;
 }
+template<class R>
+__global__ void k_disk_mid(ViewT<R> v, int ndisk, double RK, int first, int advance_t){
+   int d = blockIdx.x*blockDim.x + threadIdx.x;
+   if( d < ndisk ) disk_mid_body<R>(v, d, RK, first, advance_t);
+}
 
 /* End of timestep(): dt of the next step, diagnostics time (analysis.c:105),
  * count_steps. */
 template<class R>
-__global__ void k_disk_end(ViewT<R> v, int ndisk){
-   int d = blockIdx.x*blockDim.x + threadIdx.x;
-   if( d >= ndisk ) return;
+__device__ __forceinline__ void disk_end_body(const ViewT<R> &v, int d){
    DiskState &S = v.ds[d];
    const DiskParams &P = v.dp[d];
    double mn = __longlong_as_double((long long)S.dtmin);
@@ -1610,12 +1642,16 @@ __global__ void k_disk_end(ViewT<R> v, int ndisk){
    if( !(S.dt_next > 0.0) || S.dt_next != S.dt_next || S.dt_next >= 1.0e99 )
       atomicOr(v.err, ERRF_NONFINITE);
 }
+template<class R>
+__global__ void k_disk_end(ViewT<R> v, int ndisk){
+   int d = blockIdx.x*blockDim.x + threadIdx.x;
+   if( d < ndisk ) disk_end_body<R>(v, d);
+}
 
 /* Per annulus: sum its blocks' diagnostic partials in block order. */
 template<class R>
-__global__ void k_diag_finish(ViewT<R> v, double *Qrz, const int *ann_blk0, const int *ann_nblk){
-   int a = blockIdx.x*blockDim.x + threadIdx.x;
-   if( a >= v.Nann ) return;
+__device__ __forceinline__ void diag_finish_body(const ViewT<R> &v, double *Qrz, const int *ann_blk0,
+                                                 const int *ann_nblk, int a){
    int d = v.ann_disk[a];
    double dt = v.ds[d].dt;
    double s[DIAG_SLOTS] = {0,0,0,0,0,0,0,0,0};
@@ -1625,6 +1661,11 @@ __global__ void k_diag_finish(ViewT<R> v, double *Qrz, const int *ann_blk0, cons
       for( int m=0 ; m<DIAG_SLOTS ; ++m ) if( m < nq || m == DIAG_VOL ) s[m] += p[m];
    }
    for( int m=0 ; m<nq ; ++m ) Qrz[(size_t)a*nq + m] += s[m]*dt / s[DIAG_VOL];
+}
+template<class R>
+__global__ void k_diag_finish(ViewT<R> v, double *Qrz, const int *ann_blk0, const int *ann_nblk){
+   int a = blockIdx.x*blockDim.x + threadIdx.x;
+   if( a < v.Nann ) diag_finish_body<R>(v, Qrz, ann_blk0, ann_nblk, a);
 }
 
 /* ------------------------------------------------------------------ report

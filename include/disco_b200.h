@@ -68,6 +68,11 @@ enum disco_initial  { DISCO_IC_KEPLER_NOISE = 0, DISCO_IC_MHD_SHEAR_NOISE = 1, D
 enum disco_analysis { DISCO_DIAG_NONE = 0, DISCO_DIAG_DISK2D = 1, DISCO_DIAG_EULER = 2,
                       DISCO_DIAG_MHDMRI = 3 };
 enum disco_precision{ DISCO_PREC_FP64 = 0, DISCO_PREC_MIXED = 1 };
+/* How a batch's step is launched (disco_batch_set_schedule): one kernel per
+ * pass of onestep(), or the whole RK2 step as one persistent launch whose
+ * blocks wait only for the blocks they read from.  Both run the same block
+ * bodies, so their results are identical bit for bit. */
+enum disco_schedule { DISCO_SCHED_KERNELS = 0, DISCO_SCHED_PERSISTENT = 1 };
 
 /* Compile-time module selection (Makefile_opt.in).  num_c/num_n/ct_mode are
  * the reference's NUM_C, NUM_N and CT_MODE (paul.h:26-49). */
@@ -315,6 +320,17 @@ int disco_batch_debug_get(disco_batch *b, int which, double *out);
  * own stream).  Lets a caller time the step with events on its own stream.
  */
 int disco_batch_set_stream(disco_batch *b, void *stream);
+
+/*
+ * Choose how the step is launched (enum disco_schedule).  A new batch uses
+ * DISCO_SCHED_PERSISTENT whenever its modules allow it: hydro or MHD without
+ * constrained transport, 2D disks, RK2, fixed / polar boundaries, no
+ * Mesh_Motion 3, no viscosity; DISCO_ERR_UNSUPPORTED otherwise.  No
+ * counterpart in the reference (its onestep() is one sequence of loops);
+ * disco_batch_get_schedule returns the schedule in use.
+ */
+int disco_batch_set_schedule(disco_batch *b, int sched);
+int disco_batch_get_schedule(const disco_batch *b, int *sched);
 
 /*
  * Run one full step with a CUDA event between every kernel launch and
