@@ -51,10 +51,13 @@ DRAM_UPDATE_RAGGED8 = (289.8e6 + 53.7e6, 1049795)
 DRAM_FLUX_RAGGED8 = (216.2e6 + 72.5e6, 2089252)
 
 
-def kernel_bytes(name, first, N, Nf, Na):
+def kernel_bytes(name, first, N, Nf, Na, nreal=0):
     """Algorithmic (compulsory, each element once) HBM bytes of one launch.
-    N cells, Nf r-faces, Na annuli; Q doubles per cell."""
+    N cells, Nf r-faces, Na annuli; Q doubles per cell.  k_step, the whole
+    RK2 step as one launch, moves the step's 576 bytes per real zone-update."""
     w = 8
+    if name == "k_step":
+        return B_ALG_STEP * nreal
     if name == "k_begin":
         return N * w * ((5 * Q + 4) if first else (5 * Q + 1))
     if name == "k_c2p":
@@ -636,7 +639,7 @@ def run_ours(args, world, rank, local):
         first = seen.get(name, 0) == 0
         seen[name] = seen.get(name, 0) + 1
         tot[name] = tot.get(name, 0.0) + t
-        byt[name] = byt.get(name, 0) + kernel_bytes(name, first, ncell, nf, na)
+        byt[name] = byt.get(name, 0) + kernel_bytes(name, first, ncell, nf, na, nreal)
     dom = max(tot, key=tot.get)
     achieved = byt[dom] / (tot[dom] / 1e3) / 1e9
     # DRAM bytes of one launch of the dominant kernel: the ncu capture of the
@@ -649,6 +652,36 @@ def run_ours(args, world, rank, local):
         (b8, units8), kind = per_unit[dom]
         traffic = b8 / units8 * (ncell if kind == "cells" else nf)
     step_gbs = B_ALG_STEP * (value / world) / 1e9
+
+    # the same step as one persistent launch (disco_batch_set_schedule), for
+    # comparison with the default multi-kernel step timed above
+    sched_cmp = None
+    try:
+        b.schedule = db.SCHED_PERSISTENT
+    except db.DiscoError:
+        pass
+    if b.schedule == db.SCHED_PERSISTENT:
+        b.run(args.warmup)
+        b.sync()
+        kt_k = b.kernel_times()
+        barrier()
+        h0 = torch.cuda.Event(enable_timing=True)
+        h1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            h0.record(stream)
+            b.run(args.steps)
+            h1.record(stream)
+        h1.synchronize()
+        barrier()
+        kms = allmax(h0.elapsed_time(h1))
+        ktot = {}
+        for name, t in kt_k:
+            ktot[name] = ktot.get(name, 0.0) + t
+        sched_cmp = {"schedule": "persistent one-launch step", "ms_per_step": kms / args.steps,
+                     "value": job_rate(world, nreal, args.steps, kms),
+                     "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(ktot.items(), key=lambda x: -x[1])},
+                     "launches_per_step": len(kt_k)}
+        b.schedule = db.SCHED_KERNELS
 
     # end to end through the C ABI with host buffers: upload the state from
     # host memory, K x {dt = getmindt() -> host; timestep(dt) from host},
@@ -754,6 +787,8 @@ def run_ours(args, world, rank, local):
             "step_roofline": {"bytes_per_zone_update": B_ALG_STEP, "achieved": step_gbs, "peak": hbm,
                               "unit": "GB/s", "frac": step_gbs / hbm},
             "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(tot.items(), key=lambda x: -x[1])},
+            "schedule": "persistent one-launch step" if dom == "k_step" else "one kernel per pass",
+            "persistent_schedule": sched_cmp,
             "e2e": {"value": e2e, "unit": "zone-updates/s",
                     "h2d_bytes_per_step": (h2d + 8 * len(disks) * args.steps) / args.steps,
                     "d2h_bytes_per_step": (d2h + 8 * len(disks) * args.steps) / args.steps},

@@ -74,6 +74,12 @@ __device__ __forceinline__ int ld_acquire(const int *p){
    return x;
 }
 
+__device__ __forceinline__ int ld_relaxed(const int *p){
+   int x;
+   asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(x) : "l"(p) : "memory");
+   return x;
+}
+
 /* Bounded wait until *p >= target; false on time-out or abort. */
 __device__ __forceinline__ bool wait_ge(const int *p, int target, const int *abortp){
    if( ld_acquire(p) >= target ) return true;
@@ -83,6 +89,29 @@ __device__ __forceinline__ bool wait_ge(const int *p, int target, const int *abo
       if( (it & 63) == 63 && ld_acquire(abortp) ) return false;
    }
    return false;
+}
+
+/* Up to four counters at once: one round of independent loads first (the
+ * usual case, every input already done), the bounded waits only for what is
+ * not; then an acquire fence for the reads that follow. */
+__device__ __forceinline__ bool wait4(const int *const *p, const int *t, int n, const int *abortp){
+   int x[4];
+#pragma unroll
+   for( int m=0 ; m<4 ; ++m ) x[m] = m < n ? ld_relaxed(p[m]) : 0;
+   bool ok = true;
+#pragma unroll
+   for( int m=0 ; m<4 ; ++m ) if( m < n && x[m] < t[m] ) ok = false;
+   if( !ok ){
+      for( int m=0 ; m<n ; ++m ) if( !wait_ge(p[m], t[m], abortp) ) return false;
+   }
+   asm volatile("fence.acq_rel.gpu;" ::: "memory");
+   return true;
+}
+
+/* counter += 1 with release semantics (orders the CTA's prior writes, made
+ * visible to thread 0 by the barrier before it) */
+__device__ __forceinline__ void red_release(int *p){
+   asm volatile("red.release.gpu.global.add.s32 [%0], 1;" :: "l"(p) : "memory");
 }
 
 /* the r-tracks inside / outside annulus a (-1: none) */
@@ -104,70 +133,83 @@ template<class R>
 __device__ bool persist_wait(const ViewT<R> &v, const PersistArgs &pa, int stage, int sub, int x, int n){
    const int *ab = pa.ctl;
    const int *C = pa.cnt;
+   const int *p[4];
+   int t[4], m = 0;
+   auto need = [&](int off, int idx, int target){ p[m] = C + off + idx; t[m] = target; ++m; };
    switch( stage ){
    case PS_BEGIN: {
       int a = v.cblk[x].x, d = v.ann_disk[a];
-      if( sub == 0 ) return wait_ge(C + pa.o_d0 + d, 1, ab);
-      return wait_ge(C + pa.o_c2p[0] + a, pa.nc[a], ab) && wait_ge(C + pa.o_d1 + d, 1, ab);
+      if( sub == 0 ) need(pa.o_d0, d, 1);
+      else { need(pa.o_c2p[0], a, pa.nc[a]); need(pa.o_d1, d, 1); }
+      break;
    }
    case PS_I0:
       if( sub == 0 ) return true;
-      for( int a=x ; a<x+n ; ++a ) if( !wait_ge(C + pa.o_c2p[0] + a, pa.nc[a], ab) ) return false;
-      return true;
+      for( int a=x ; a<x+n ; ++a ) need(pa.o_c2p[0], a, pa.nc[a]);
+      break;
    case PS_FACES: {
-      int t = v.fblk[x].x, A = v.tr_a[t], B = v.tr_b[t];
-      return wait_ge(C + pa.o_begin[sub] + A, pa.nc[A], ab) && wait_ge(C + pa.o_begin[sub] + B, pa.nc[B], ab) &&
-             wait_ge(C + pa.o_I0[sub] + A, 1, ab) && wait_ge(C + pa.o_I0[sub] + B, 1, ab);
+      int tr = v.fblk[x].x, A = v.tr_a[tr], B = v.tr_b[tr];
+      need(pa.o_begin[sub], A, pa.nc[A]); need(pa.o_begin[sub], B, pa.nc[B]);
+      need(pa.o_I0[sub], A, 1); need(pa.o_I0[sub], B, 1);
+      break;
    }
    case PS_GRAD: {
       int a = v.cblk[x].x, ti = track_in(v, a), to = track_out(v, a);
-      return (ti < 0 || wait_ge(C + pa.o_faces[sub] + ti, pa.nf[ti], ab)) &&
-             (to < 0 || wait_ge(C + pa.o_faces[sub] + to, pa.nf[to], ab));
+      if( ti >= 0 ) need(pa.o_faces[sub], ti, pa.nf[ti]);
+      if( to >= 0 ) need(pa.o_faces[sub], to, pa.nf[to]);
+      break;
    }
    case PS_FLUX: {
-      int t = v.fblk[x].x, A = v.tr_a[t], B = v.tr_b[t];
-      return wait_ge(C + pa.o_grad[sub] + A, pa.nc[A], ab) && wait_ge(C + pa.o_grad[sub] + B, pa.nc[B], ab);
+      int tr = v.fblk[x].x, A = v.tr_a[tr], B = v.tr_b[tr];
+      need(pa.o_grad[sub], A, pa.nc[A]); need(pa.o_grad[sub], B, pa.nc[B]);
+      break;
    }
    case PS_UPDATE: {
       int a = v.ublk[x].x, ti = track_in(v, a), to = track_out(v, a);
-      return (ti < 0 || wait_ge(C + pa.o_flux[sub] + ti, pa.nf[ti], ab)) &&
-             (to < 0 || wait_ge(C + pa.o_flux[sub] + to, pa.nf[to], ab));
+      if( ti >= 0 ) need(pa.o_flux[sub], ti, pa.nf[ti]);
+      if( to >= 0 ) need(pa.o_flux[sub], to, pa.nf[to]);
+      break;
    }
    case PS_C2P: {
       int a = v.cblk[x].x;
-      return wait_ge(C + pa.o_upd[sub] + a, pa.nu[a], ab);
+      need(pa.o_upd[sub], a, pa.nu[a]);
+      break;
    }
    case PS_DMID:
-      return wait_ge(C + pa.o_c2pd[0] + x, pa.ndc[x], ab);
+      need(pa.o_c2pd[0], x, pa.ndc[x]);
+      break;
    case PS_DIAGFIN:
       for( int a=x ; a<x+n ; ++a ) if( !wait_ge(C + pa.o_c2p[1] + a, pa.nc[a], ab) ) return false;
+      asm volatile("fence.acq_rel.gpu;" ::: "memory");
       return true;
    case PS_DTAIL:
-      return wait_ge(C + pa.o_c2pd[1] + x, pa.ndc[x], ab);
+      need(pa.o_c2pd[1], x, pa.ndc[x]);
+      break;
    default:
       return true;
    }
+   return m == 0 || wait4(p, t, m, ab);
 }
 
-/* Thread 0, after the block's writes and a fence: mark the item done. */
+/* Thread 0, after the block's barrier: mark the item done (release). */
 template<class R>
 __device__ void persist_signal(const ViewT<R> &v, const PersistArgs &pa, int stage, int sub, int x, int n){
    int *C = pa.cnt;
    switch( stage ){
-   case PS_DBEGIN: atomicAdd(C + pa.o_d0 + x, 1); break;
-   case PS_BEGIN:  atomicAdd(C + pa.o_begin[sub] + v.cblk[x].x, 1); break;
-   case PS_I0:     for( int a=x ; a<x+n ; ++a ) atomicAdd(C + pa.o_I0[sub] + a, 1); break;
-   case PS_FACES:  atomicAdd(C + pa.o_faces[sub] + v.fblk[x].x, 1); break;
-   case PS_GRAD:   atomicAdd(C + pa.o_grad[sub] + v.cblk[x].x, 1); break;
-   case PS_FLUX:   atomicAdd(C + pa.o_flux[sub] + v.fblk[x].x, 1); break;
-   case PS_UPDATE: atomicAdd(C + pa.o_upd[sub] + v.ublk[x].x, 1); break;
+   case PS_DBEGIN: red_release(C + pa.o_d0 + x); break;
+   case PS_BEGIN:  red_release(C + pa.o_begin[sub] + v.cblk[x].x); break;
+   case PS_I0:     for( int a=x ; a<x+n ; ++a ) red_release(C + pa.o_I0[sub] + a); break;
+   case PS_FACES:  red_release(C + pa.o_faces[sub] + v.fblk[x].x); break;
+   case PS_GRAD:   red_release(C + pa.o_grad[sub] + v.cblk[x].x); break;
+   case PS_FLUX:   red_release(C + pa.o_flux[sub] + v.fblk[x].x); break;
+   case PS_UPDATE: red_release(C + pa.o_upd[sub] + v.ublk[x].x); break;
    case PS_C2P: {
       int a = v.cblk[x].x;
-      atomicAdd(C + pa.o_c2p[sub] + a, 1);
-      atomicAdd(C + pa.o_c2pd[sub] + v.ann_disk[a], 1);
+      red_release(C + pa.o_c2p[sub] + a);
+      red_release(C + pa.o_c2pd[sub] + v.ann_disk[a]);
       break;
    }
-   case PS_DMID:   atomicAdd(C + pa.o_d1 + x, 1); break;
+   case PS_DMID:   red_release(C + pa.o_d1 + x); break;
    default: break;
    }
 }
@@ -215,7 +257,6 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_PERSIST) k_step(ViewT<
             atomicExch(pa.ctl, 1);
             atomicOr(v.err, ERRF_TIMEOUT);
          }
-         __threadfence();
          s_go = ok;
       }
       __syncthreads();
@@ -223,7 +264,7 @@ __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_PERSIST) k_step(ViewT<
       persist_run<Q,NC,R,NQD>(v, pa, stage, sub, w.y, w.z);
       __syncthreads();
       if( tid == 0 ){
-         __threadfence();
+         __threadfence();        /* the block's writes, ordered by the barrier, before the counter */
          persist_signal<R>(v, pa, stage, sub, w.y, w.z);
       }
    }

@@ -228,6 +228,12 @@ def test_nonfinite_piph_reports_error_status():
 def test_kernel_times_cover_the_step():
     disk, g = case_disk("c0_lin20")
     b = _batch_from_golden(disk, g)
+    # the persistent schedule: the whole step is one launch
+    b.schedule = db.SCHED_PERSISTENT
+    kt = b.kernel_times()
+    assert [k for k, _ in kt] == ["k_step"] and kt[0][1] > 0
+    # the multi-kernel schedule: every pass of both substeps
+    b.schedule = db.SCHED_KERNELS
     kt = b.kernel_times()
     names = [k for k, _ in kt]
     for k in ("k_begin", "k_I0", "k_faces", "k_gradr", "k_flux_r", "k_update", "k_c2p"):

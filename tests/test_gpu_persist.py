@@ -47,8 +47,10 @@ def test_persistent_step_equals_kernels(prec):
     assert np.array_equal(a["diag"], p["diag"])
 
 
-def test_persistent_is_default_where_supported():
+def test_schedule_selection():
     b = db.Batch([workloads.config0_disk()])
+    assert b.schedule == db.SCHED_KERNELS          # the default
+    b.schedule = db.SCHED_PERSISTENT
     assert b.schedule == db.SCHED_PERSISTENT
     b.close()
     # 3D (z faces) runs on the multi-kernel path and refuses the persistent one
