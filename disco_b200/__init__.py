@@ -30,11 +30,12 @@ STATUS = {0: "ok", 1: "bad argument", 2: "CUDA runtime error", 3: "module combin
           4: "phi wrap loop hit its cap (non-finite piph)", 5: "non-finite or non-positive dt",
           6: "no CUDA device", 7: "call out of order", 8: "device consistency check failed",
           9: "file not written, read or parsed"}
-HYDRO = {"euler": 0, "mhd": 1}
+HYDRO = {"euler": 0, "mhd": 1, "grmhd2": 2}
+METRIC = {"schw_ks_rpz": 0, "kerr_ks_rpz": 1}
 BOUNDARY = {"fixed": 0, "zerograd": 1, "fixed3d": 2, "polar": 3, "outflow3d": 4, "zerograd_omk": 5,
             "accrete3d": 6}
 PLANETS = {"none": 0, "sun": 1, "cm2": 2, "binary_soft": 3, "circular": 4, "cm": 5}
-INITIAL = {"kepler_noise": 0, "mhd_shear_noise": 1, "host": 2}
+INITIAL = {"kepler_noise": 0, "mhd_shear_noise": 1, "host": 2, "gr_torus_noise": 3}
 PREC_FP64, PREC_MIXED = 0, 1
 SCHED_KERNELS, SCHED_PERSISTENT = 0, 1
 
@@ -75,7 +76,7 @@ class Modules(C.Structure):
     """Mirror of disco_modules."""
     _fields_ = [("hydro", C.c_int), ("boundary", C.c_int), ("planets", C.c_int),
                 ("initial", C.c_int), ("analysis", C.c_int),
-                ("num_c", C.c_int), ("num_n", C.c_int), ("ct_mode", C.c_int)]
+                ("num_c", C.c_int), ("num_n", C.c_int), ("ct_mode", C.c_int), ("metric", C.c_int)]
 
 
 _lib = None

@@ -90,7 +90,18 @@ static void fill_disk_params(DiskParams &D, const disco_params &p, const disco_m
    D.ic.rmin = p.rmin; D.ic.rmax = p.rmax; D.ic.phimax = p.phimax;
    D.ic.seed = (uint64_t)(int64_t)p.initPar0;
    D.ic.kind = (int)p.initPar[2];
-   D.ic_module = m.initial == DISCO_IC_MHD_SHEAR_NOISE ? 1 : 0;
+   D.ic_module = m.initial == DISCO_IC_MHD_SHEAR_NOISE ? 1 : m.initial == DISCO_IC_GR_TORUS_NOISE ? 2 : 0;
+   D.gr = m.hydro == DISCO_HYDRO_GRMHD ? 1 : 0;
+   D.gr_metric = m.metric == DISCO_METRIC_KERR_KS_RPZ ? 1 : 0;
+   D.gr_M = p.metricPar[2];
+   D.gr_a = m.metric == DISCO_METRIC_KERR_KS_RPZ ? p.metricPar[3] : 0.0;
+   D.ic_gr.seed = (uint64_t)(int64_t)p.initPar0; D.ic_gr.amp = p.initPar[1];
+   D.ic_gr.rc = p.initPar[2]; D.ic_gr.wr = p.initPar[3]; D.ic_gr.hr = p.initPar[4];
+   D.ic_gr.beta = p.initPar[5]; D.ic_gr.rho_atm = p.initPar[6]; D.ic_gr.p_atm = p.initPar[7];
+   D.ic_gr.s_cut = p.initPar[8];
+   D.ic_gr.M = p.metricPar[2]; D.ic_gr.a = D.gr_a;
+   D.ic_gr.rmin = p.rmin; D.ic_gr.rmax = p.rmax; D.ic_gr.zmin = p.zmin; D.ic_gr.zmax = p.zmax;
+   D.ic_gr.phimax = p.phimax;
    D.ic_mhd.seed = (uint64_t)(int64_t)p.initPar0; D.ic_mhd.amp = p.initPar[1];
    D.ic_mhd.cs = p.initPar[3]; D.ic_mhd.beta = p.initPar[4]; D.ic_mhd.gam = p.Adiabatic_Index;
    D.ic_mhd.rmin = p.rmin; D.ic_mhd.rmax = p.rmax; D.ic_mhd.zmin = p.zmin; D.ic_mhd.zmax = p.zmax;
@@ -320,10 +331,21 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
     * flag and the next cell's prims), so it is accepted.  Constrained
     * transport itself is built in both forms, for every disk of the batch
     * or none. */
-   bool mhd = mods->hydro == DISCO_HYDRO_MHD;
+   /* grmhd2 (HYDRO = grmhd2, NUM_C 8) carries B like mhd; it is built for
+    * the FP64 path with the HLL solver, without constrained transport or
+    * point masses, for the schw_ks_rpz metric and the Kerr-Schild one */
+   const bool gr = mods->hydro == DISCO_HYDRO_GRMHD;
+   bool mhd = mods->hydro == DISCO_HYDRO_MHD || gr;
    if( !((mods->hydro == DISCO_HYDRO_EULER && mods->num_c == 5) || (mhd && mods->num_c == 8)) ||
        mods->num_n != 1 || mods->ct_mode < 0 || mods->ct_mode > 2 )
       return DISCO_ERR_UNSUPPORTED;
+   if( gr ){
+      if( precision != DISCO_PREC_FP64 || params[0].CT || mods->planets != DISCO_PLANETS_NONE ||
+          mods->analysis == DISCO_DIAG_MHDMRI ||
+          (mods->metric != DISCO_METRIC_SCHW_KS_RPZ && mods->metric != DISCO_METRIC_KERR_KS_RPZ) )
+         return DISCO_ERR_UNSUPPORTED;
+      for( int d=0 ; d<ndisk ; ++d ) if( params[d].Riemann_Solver != 0 ) return DISCO_ERR_UNSUPPORTED;
+   }
    int ct = params[0].CT ? mods->ct_mode : 0;
    for( int d=0 ; d<ndisk ; ++d ) if( (params[d].CT ? 1 : 0) != (params[0].CT ? 1 : 0) ) return DISCO_ERR_ARG;
    if( params[0].CT ){
@@ -344,8 +366,9 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       for( int d=0 ; d<ndisk ; ++d ) if( Ng[4*d+0] != 0 ) return DISCO_ERR_UNSUPPORTED;
    if( mods->analysis == DISCO_DIAG_MHDMRI && !mhd ) return DISCO_ERR_UNSUPPORTED;   /* reads B */
    if( mods->initial != DISCO_IC_KEPLER_NOISE && mods->initial != DISCO_IC_MHD_SHEAR_NOISE &&
-       mods->initial != DISCO_IC_HOST )
+       mods->initial != DISCO_IC_GR_TORUS_NOISE && mods->initial != DISCO_IC_HOST )
       return DISCO_ERR_UNSUPPORTED;
+   if( mods->initial == DISCO_IC_GR_TORUS_NOISE && !gr ) return DISCO_ERR_UNSUPPORTED;
    /* a host-evaluated Initial module cannot refill ghosts on the device */
    if( mods->initial == DISCO_IC_HOST && mods->boundary != DISCO_BC_ZEROGRAD &&
        mods->boundary != DISCO_BC_OUTFLOW3D )
@@ -380,6 +403,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->d_noise = NULL;
    b->any_visc = 0;
    for( int d=0 ; d<ndisk ; ++d ) if( params[d].visc_flag ) b->any_visc = 1;
+   b->gr = gr ? 1 : 0;
    b->d_zg_pairs = NULL;
    b->zg_smem = 0;
    b->nq = mods->analysis == DISCO_DIAG_DISK2D ? 5 : mods->analysis == DISCO_DIAG_EULER ? 8 :

@@ -29,6 +29,7 @@ struct disco_batch {
    unsigned char *d_zg_side;
    int zg_diode, zg_omk;                /* outflow diode; Omega from initial() in r ghosts */
    int any_visc;                        /* some disk has Use_Viscosity (Euler) */
+   int gr;                              /* HYDRO = grmhd2 (FP64, no constrained transport) */
    std::vector<int> zg_off;             /* layer groups: r layers, then z layers */
    int2 *d_zg_pairs;
    size_t zg_smem;                      /* dynamic shared memory of k_zerograd */
@@ -149,33 +150,33 @@ static void launch_restart_qt(disco_batch *b, const ViewT<R> &v){
 /* k_c2p with the Analysis module's number of diagnostics (diag_disk2d 5,
  * diag_euler 8) and, for Euler, the viscous dt limit compiled in only when a
  * disk is viscous */
-template<int Q, int NC, class R, int NQD>
+template<int Q, int NC, class R, int NQD, bool GR>
 static void launch_c2p_nq(disco_batch *b, const ViewT<R> &v, int last, int diag){
    unsigned ncb = (unsigned)b->cblk.size();
    if constexpr ( NC == 5 ){
       if( b->any_visc ){ k_c2p<Q,NC,R,NQD,true><<<ncb, CB, 0, b->stream>>>(v, last, b->bc_fixed, diag); return; }
    }
-   k_c2p<Q,NC,R,NQD,false><<<ncb, CB, 0, b->stream>>>(v, last, b->bc_fixed, diag);
+   k_c2p<Q,NC,R,NQD,false,GR><<<ncb, CB, 0, b->stream>>>(v, last, b->bc_fixed, diag);
 }
-template<int Q, int NC, class R>
+template<int Q, int NC, class R, bool GR = false>
 static void launch_c2p(disco_batch *b, const ViewT<R> &v, int last, int diag){
-   if constexpr ( NC == 8 ){
-      if( b->nq == 18 ){ launch_c2p_nq<Q,NC,R,18>(b, v, last, diag); return; }
+   if constexpr ( NC == 8 && !GR ){
+      if( b->nq == 18 ){ launch_c2p_nq<Q,NC,R,18,false>(b, v, last, diag); return; }
    }
-   if( b->nq == 8 ) launch_c2p_nq<Q,NC,R,8>(b, v, last, diag);
-   else launch_c2p_nq<Q,NC,R,5>(b, v, last, diag);
+   if( b->nq == 8 ) launch_c2p_nq<Q,NC,R,8,GR>(b, v, last, diag);
+   else launch_c2p_nq<Q,NC,R,5,GR>(b, v, last, diag);
 }
-template<int Q, int NC, int DIM, class R>
+template<int Q, int NC, int DIM, class R, bool GR = false>
 static void launch_flux_t(disco_batch *b, const ViewT<R> &v){
    unsigned nfb = (unsigned)b->fblk.size();
    if constexpr ( NC == 5 ){
       if( b->any_visc ){ k_flux_t<Q,NC,DIM,R,true><<<nfb, FB, 0, b->stream>>>(v); return; }
    }
-   k_flux_t<Q,NC,DIM,R,false><<<nfb, FB, 0, b->stream>>>(v);
+   k_flux_t<Q,NC,DIM,R,false,GR><<<nfb, FB, 0, b->stream>>>(v);
 }
 
-/* One substep of onestep() (onestep.c:84-229). */
-template<int Q, int NC, class R>
+/* One substep of onestep() (onestep.c:84-229); GR: the grmhd2 module. */
+template<int Q, int NC, class R, bool GR = false>
 static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int last, double dtfac){
    v.dtfac = dtfac;
    /* RK2: the first substep keeps the faces the previous step's second
@@ -185,20 +186,20 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    v.move_c2p = first && !b->ct;
    cudaStream_t s = b->stream;
    unsigned ncb = (unsigned)b->cblk.size(), nfb = (unsigned)b->fblk.size();
-   k_begin<Q,NC,R><<<ncb, CB, 0, s>>>(v, RK, first);                  mark(b, "k_begin");
+   k_begin<Q,NC,R,GR><<<ncb, CB, 0, s>>>(v, RK, first);               mark(b, "k_begin");
    if( first && b->any_mm3 ){ k_wmean<R><<<nblk(v.Nann, WM_WARPS), 32*WM_WARPS, 0, s>>>(v, 1); mark(b, "k_wmean"); }
    k_I0<R><<<nblk((size_t)v.Nann*32, 128), 128, 0, s>>>(v);           mark(b, "k_I0");
    k_faces<Q,R><<<nfb, FB, 0, s>>>(v, 1);                             mark(b, "k_faces");
    k_grad<Q,1,R><<<ncb, CB, 0, s>>>(v);                               mark(b, "k_gradr");
    if( b->any_3d ){ k_grad<Q,2,R><<<ncb, CB, 0, s>>>(v);              mark(b, "k_gradz"); }
-   launch_flux_t<Q,NC,1,R>(b, v);                                     mark(b, "k_flux_r");
-   if( b->any_3d ){ launch_flux_t<Q,NC,2,R>(b, v);                    mark(b, "k_flux_z"); }
+   launch_flux_t<Q,NC,1,R,GR>(b, v);                                  mark(b, "k_flux_r");
+   if( b->any_3d ){ launch_flux_t<Q,NC,2,R,GR>(b, v);                 mark(b, "k_flux_z"); }
    bool upd_visc = false;
    if constexpr ( NC == 5 ) upd_visc = b->any_visc;
    if( upd_visc ){
       if constexpr ( NC == 5 ) k_update<Q,NC,R,true><<<(unsigned)b->ublk.size(), CB, 0, s>>>(v, first);
    }else{
-      k_update<Q,NC,R,false><<<(unsigned)b->ublk.size(), CB, 0, s>>>(v, first);
+      k_update<Q,NC,R,false,GR><<<(unsigned)b->ublk.size(), CB, 0, s>>>(v, first);
    }
    mark(b, "k_update");
    if constexpr ( NC == 8 ){
@@ -215,7 +216,7 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
          }
       }
    }
-   launch_c2p<Q,NC,R>(b, v, last, !b->bc_zerograd);                   mark(b, "k_c2p");
+   launch_c2p<Q,NC,R,GR>(b, v, last, !b->bc_zerograd);                mark(b, "k_c2p");
    launch_zerograd<Q,R>(b, v);
    if( last && b->nq && b->bc_zerograd ){
       bool mri = false;
@@ -270,19 +271,19 @@ static int persist_blocks_per_sm_t(const disco_batch *b){
 }
 
 /* timestep() (timestep.c:7-45). */
-template<int Q, int NC, class R>
+template<int Q, int NC, class R, bool GR = false>
 static void launch_step_qt(disco_batch *b, const ViewT<R> &v, int use_next){
    if( b->sched == DISCO_SCHED_PERSISTENT ){ launch_persist<Q,NC,R>(b, v, use_next); return; }
    cudaStream_t s = b->stream;
    unsigned nd = nblk(b->ndisk, 64);
    k_disk_begin<R><<<nd, 64, 0, s>>>(v, b->ndisk, use_next);          mark(b, "k_disk_begin");
    if( b->timestep_mode == 1 ){
-      launch_substep<Q,NC,R>(b, v, 0.0, 1, 1, 1.0);
+      launch_substep<Q,NC,R,GR>(b, v, 0.0, 1, 1, 1.0);
       k_disk_mid<R><<<nd, 64, 0, s>>>(v, b->ndisk, 0.0, 1, 1);       mark(b, "k_disk_mid");
    }else{
-      launch_substep<Q,NC,R>(b, v, 0.0, 1, 0, 1.0);
+      launch_substep<Q,NC,R,GR>(b, v, 0.0, 1, 0, 1.0);
       k_disk_mid<R><<<nd, 64, 0, s>>>(v, b->ndisk, 0.0, 1, 1);       mark(b, "k_disk_mid");
-      launch_substep<Q,NC,R>(b, v, 0.5, 0, 1, 0.5);
+      launch_substep<Q,NC,R,GR>(b, v, 0.5, 0, 1, 0.5);
       k_disk_mid<R><<<nd, 64, 0, s>>>(v, b->ndisk, 0.5, 0, 0);       mark(b, "k_disk_mid");
    }
    if( b->nq ){
@@ -307,6 +308,9 @@ static void launch_restart_t(disco_batch *b, const ViewT<R> &v){
 }
 template<class R>
 static void launch_step_t(disco_batch *b, const ViewT<R> &v, int use_next){
+   if constexpr ( sizeof(R) == sizeof(double) ){
+      if( b->gr ){ launch_step_qt<9,8,R,true>(b, v, use_next); return; }
+   }
    if( b->NC == 8 ) launch_step_qt<9,8,R>(b, v, use_next); else launch_step_qt<6,5,R>(b, v, use_next);
 }
 template<class R>

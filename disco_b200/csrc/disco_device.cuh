@@ -18,6 +18,7 @@
 #include <stdint.h>
 #include "ic_kepler_noise.h"
 #include "ic_mhd_shear.h"
+#include "ic_gr_torus.h"
 
 namespace disco {
 
@@ -69,10 +70,15 @@ struct DiskParams {
    int pad_noise;
    double noise_abs, noise_rel;
    int npl;
-   int ic_module;     /* DISCO_IC_KEPLER_NOISE or DISCO_IC_MHD_SHEAR_NOISE */
+   int ic_module;     /* 0 kepler_noise, 1 mhd_shear_noise, 2 gr_torus_noise */
    int pad_ic;
    disco_ic_kepler_noise ic;
    disco_ic_mhd_shear ic_mhd;
+   disco_ic_gr_torus ic_gr;
+   /* grmhd2 (HYDRO = grmhd2): the metric module (0 schw_ks_rpz, 1 the
+    * Kerr-Schild kerr_ks_rpz) and its Metric_Par2 (M) / Metric_Par3 (a) */
+   int gr, gr_metric;
+   double gr_M, gr_a;
 };
 
 /* Per-disk mutable state (device resident across steps). */
@@ -835,6 +841,7 @@ __device__ __forceinline__ void planetary_force(int grav2D, const Planet &pl, do
 template<int Q, int NC>
 __device__ __forceinline__ void initial(const DiskParams &P, double *prim, const double *x){
    if( P.ic_module == 1 ) disco_ic_mhd_shear_eval(&P.ic_mhd, NC, Q, prim, x);
+   else if( P.ic_module == 2 ) disco_ic_gr_torus_eval(&P.ic_gr, NC, Q, prim, x);
    else disco_ic_kepler_noise_eval(&P.ic, NC, Q, prim, x);
 }
 

@@ -32,6 +32,7 @@
  */
 #pragma once
 #include "disco_device.cuh"
+#include "grmhd_step.cuh"
 
 #include "tuned.h"
 
@@ -169,7 +170,7 @@ __device__ __forceinline__ void acc(double &s, double &cc, double x){
  * modes 0/1/2/4; mode 3's mean is k_wmean), the moved-and-wrapped piph of
  * move_cells + clean_pi (misc.c:256-268, 8-26) into piph_new.
  * Every substep: adjust_RK_cons (misc.c:226-244) and plm_phi (plm.c:15-51). */
-template<int Q, int NC, class R>
+template<int Q, int NC, class R, bool GR = false>
 __device__ __forceinline__ void begin_body(const ViewT<R> &v, double RK, int first, int bid){
    /* the chunk's prims and dphi staged once, with one neighbour cell on each
     * side (slot t+1 = cell i0+t) */
@@ -201,7 +202,19 @@ __device__ __forceinline__ void begin_body(const ViewT<R> &v, double RK, int fir
    }
    if( first ){
       double w = 0.0;
-      if( P.mesh_motion ) w = .5*((double)pC[UPP] + (double)pR[UPP]);   /* get_omega = prim[UPP] */
+      if constexpr ( GR ){          /* get_omega of grmhd2, grmhd2.c:64-86 (set_wcell's x) */
+         if( P.mesh_motion ){
+            int j = v.ann_j[a], k = v.ann_k[a];
+            const double *rj = v.rj + P.rj0 + 1, *zk = v.zk + P.zk0 + 1;
+            double x[3] = {centroid_r(rj[j], rj[j-1]), 0.0, centroid_z(zk[k], zk[k-1])};
+            double pc[Q], pr[Q];
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ){ pc[q] = (double)pC[q]; pr[q] = (double)pR[q]; }
+            w = .5*(gr_omega(P, pc, x) + gr_omega(P, pr, x));
+         }
+      }else{
+         if( P.mesh_motion ) w = .5*((double)pC[UPP] + (double)pR[UPP]);   /* get_omega = prim[UPP] */
+      }
       if( P.mesh_motion == 4 ){
          int j = v.ann_j[a];
          const double *rj = v.rj + P.rj0 + 1;
@@ -260,9 +273,9 @@ __device__ __forceinline__ void begin_body(const ViewT<R> &v, double RK, int fir
       v.gradp[q*N + c] = m;
    }
 }
-template<int Q, int NC, class R>
+template<int Q, int NC, class R, bool GR = false>
 __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_BEGIN) k_begin(ViewT<R> v, double RK, int first){
-   begin_body<Q,NC,R>(v, RK, first, blockIdx.x);
+   begin_body<Q,NC,R,GR>(v, RK, first, blockIdx.x);
 }
 
 /* Energy-frame Omega at the radii the step evaluates it (omega.c:62-110):
@@ -698,7 +711,7 @@ __device__ __forceinline__ double2 visc_source_cell(const ViewT<R> &v, const Dis
  * G_q = (F - w U*) dA dt per face.  The face centre cm is (r_{j+1/2}, phic,
  * z centroid) for r-faces and (r centroid, phic, z_{k+1/2}) for z-faces
  * (addFace, faces_alt.c:10-16). */
-template<int Q, int NC, int DIM, class R, bool VISC = false>
+template<int Q, int NC, int DIM, class R, bool VISC = false, bool GR = false>
 __device__ __forceinline__ void flux_body(const ViewT<R> &v, double dtfac, int bid){
    int2 b = v.fblk[bid];
    int t = b.x;
@@ -735,7 +748,18 @@ __device__ __forceinline__ void flux_body(const ViewT<R> &v, double dtfac, int b
    const double *rj = v.rj + P.rj0 + 1;
    double r = DIM == 1 ? .5*(rj[j]+rj[j]) : centroid_r(rj[j], rj[j-1]);    /* face cm[0] */
    R G[Q];
-   if constexpr ( NC == 8 ){
+   if constexpr ( GR ){              /* grmhd2 + HLL at the face centre (addFace, faces_alt.c:10-16) */
+      const double *zk = v.zk + P.zk0 + 1;
+      int k = v.tr_k[t];
+      double x[3] = {r, phi, DIM == 1 ? 0.5*(zk[k]+zk[k-1]) : 0.5*(zk[k]+zk[k])};
+      const double n[3] = {DIM == 1 ? 1.0 : 0.0, 0.0, DIM == 2 ? 1.0 : 0.0};
+      double pl[Q], pr[Q], g[Q];
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ){ pl[q] = (double)primL[q]; pr[q] = (double)primR[q]; }
+      gr_hll(P, pl, pr, x, n, 0.0, dAdt, g);
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) G[q] = (R)g[q];
+   }else if constexpr ( NC == 8 ){
       if( v.ct ){                    /* flux_to_E dim 1 / 2, Hydro/mhd.c:304-314 */
          R eb[5];
          solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G, eb);
@@ -767,9 +791,9 @@ __device__ __forceinline__ void flux_body(const ViewT<R> &v, double dtfac, int b
    for( int q=0 ; q<Q ; ++q ) v.fG[(size_t)q*v.Nf + f] = G[q];
    raise_err(v, err);
 }
-template<int Q, int NC, int DIM, class R, bool VISC = false>
+template<int Q, int NC, int DIM, class R, bool VISC = false, bool GR = false>
 __global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R> v){
-   flux_body<Q,NC,DIM,R,VISC>(v, v.dtfac, blockIdx.x);
+   flux_body<Q,NC,DIM,R,VISC,GR>(v, v.dtfac, blockIdx.x);
 }
 
 /* ------------------------------------------------------------------ phi faces
@@ -852,7 +876,7 @@ __device__ __forceinline__ QVec<Q,R> phi_face_flux_visc(const ViewT<R> &v, const
  * calc_prim, the boundary, and the fused getmindt / diagnostics follow in
  * k_c2p (run inside this kernel instead, the extra registers cost more than
  * the saved re-read of cons: 1.73 against 1.69 ms per ragged64 step). */
-template<int Q, int NC, class R, bool VISC = false>
+template<int Q, int NC, class R, bool VISC = false, bool GR = false>
 __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double dtfac, int bid){
    /* The block updates CB-1 cells i0 .. i0+CB-2 and its thread t solves the
     * phi face (i0+t-1, i0+t) into sG[.][t]: every thread one face, the
@@ -917,7 +941,18 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
          R primR[Q];
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ) primR[q] = sW[q][tt+1];
-         if( ctE ){                 /* flux_to_E dim 0, Hydro/mhd.c:298-303 */
+         if constexpr ( GR ){      /* riemann_phi with grmhd2 + HLL, x = (r, piph, z) */
+            double pl[Q], pr[Q], g[Q];
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ){ pl[q] = (double)eR[q]; pr[q] = (double)primR[q]; }
+            double Bp = .5*(pl[BPP]+pr[BPP]);                 /* riemann.c:54-58 */
+            pl[BPP] = Bp; pr[BPP] = Bp;
+            double x[3] = {rc, v.piph[cprev], centroid_z(zk[k], zk[k-1])};
+            const double n[3] = {0.0, 1.0, 0.0};
+            gr_hll(P, pl, pr, x, n, rc*v.wiph[cprev], dAdtp, g);
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ) G[q] = (R)g[q];
+         }else if( ctE ){           /* flux_to_E dim 0, Hydro/mhd.c:298-303 */
             R eb[5];
             phi_face_flux_states<Q,NC,R>(v, P, a, cprev, rc, dAdtp, eR, primR, G, eb);
             if( threadIdx.x > 0 ){  /* stored once: t = 0's face is the previous chunk's */
@@ -1009,7 +1044,10 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
       double dV = dV_of(rp, rm, dph, zp, zm);
       double dVdt = dV*dt;
       double r = centroid_r(rp, rm);
-      if constexpr ( NC == 8 ){  /* mhd source, mhd.c:225-263 */
+      if constexpr ( GR ){       /* grmhd2 source, grmhd2.c:383-478 */
+         double xp[3] = {rp, piph, zp}, xm[3] = {rm, phim, zm};
+         gr_source(P, prim, cons, xp, xm, dVdt);
+      }else if constexpr ( NC == 8 ){  /* mhd source, mhd.c:225-263 */
          double rho = prim[RHO], Pp = prim[PPP];
          double r_1 = .5*(rp+rm);
          double r2_3 = (rp*rp + rp*rm + rm*rm)/3.;
@@ -1070,9 +1108,9 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
    (void)first;                     /* the move follows in k_c2p (or k_ct_update) */
    raise_err(v, err);
 }
-template<int Q, int NC, class R, bool VISC = false>
+template<int Q, int NC, class R, bool VISC = false, bool GR = false>
 __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT<R> v, int first){
-   update_body<Q,NC,R,VISC>(v, first, v.dtfac, blockIdx.x);
+   update_body<Q,NC,R,VISC,GR>(v, first, v.dtfac, blockIdx.x);
 }
 
 /* One cell's terms of add_diagnostics (analysis.c:52-107) with the
@@ -1241,7 +1279,7 @@ __device__ void ct_cons_B(const ViewT<R> &v, const DiskParams &P, int a, int c0,
  * per-block sums of add_diagnostics (analysis.c:52-107).  Every thread of the
  * block (one annulus chunk) must call it: it ends in block reductions.
  * piph / dphi are the moved cell's; cons is read only on real cells. */
-template<int Q, int NC, class R, int NQD, bool VISC>
+template<int Q, int NC, class R, int NQD, bool VISC, bool GR = false>
 __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P, int a, int c,
                                          int c0, int np, int i, int j, int k, int d, bool real,
                                          bool active, double piph, double dphi, double *cons,
@@ -1263,7 +1301,14 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
       if( real ){
          double dph2 = get_dp(piph, phim, P.Pmax, &err);
          double dV2 = dV_of(rp, rm, dph2, zp, zm);
-         cons2prim<Q,NC>(P, cons, prim, centroid_r(rp, rm), v.ann_om[a], dV2);
+         if constexpr ( GR ){       /* grmhd2 cons2prim from the cell's current prims */
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N + c];
+            double x[3] = {centroid_r(rp, rm), 0.5*(phim+piph), centroid_z(zp, zm)};
+            gr_cons2prim(P, cons, prim, x, dV2);
+         }else{
+            cons2prim<Q,NC>(P, cons, prim, centroid_r(rp, rm), v.ann_om[a], dV2);
+         }
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ){
             R pq = (R)prim[q];
@@ -1284,7 +1329,13 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
          }
       }
       if( last ){
-         if( real ){                              /* mindt, euler.c:332-380, mhd.c:452-486 */
+         if( real && GR ){                        /* mindt, grmhd2.c:748-832 */
+            int cprev = c0 + (i == 0 ? np-1 : i-1);
+            double w = .5*(v.wiph[cprev] + v.wiph[c]);
+            double xp[3] = {rp, piph, zp}, xm[3] = {rm, phim, zm};
+            double dtm = gr_mindt(P, prim, w, xp, xm, &err);
+            if( dtm == dtm ) dtc = dtm;
+         }else if( real ){                        /* mindt, euler.c:332-380, mhd.c:452-486 */
             int cprev = c0 + (i == 0 ? np-1 : i-1);
             double w = .5*(v.wiph[cprev] + v.wiph[c]);
             double r = centroid_r(rp, rm);
@@ -1351,7 +1402,7 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
 /* ------------------------------------------------------------------ k_c2p
  * c2p_tail on each cell after k_update, with constrained transport first
  * rebuilding B from the face fluxes (onestep.c:183-185). */
-template<int Q, int NC, class R, int NQD = 5, bool VISC = false>
+template<int Q, int NC, class R, int NQD = 5, bool VISC = false, bool GR = false>
 __device__ __forceinline__ void c2p_body(const ViewT<R> &v, int last, int bc, int diag, int move_c2p,
                                          int topo_set, int bid){
    int2 b = v.cblk[bid];
@@ -1390,12 +1441,12 @@ __device__ __forceinline__ void c2p_body(const ViewT<R> &v, int last, int bc, in
          }
       }
    }
-   c2p_tail<Q,NC,R,NQD,VISC>(v, P, a, c, c0, np, i, j, k, d, real, active, piph, dphi, cons, last,
-                             bc, diag, err, topo_set, bid);
+   c2p_tail<Q,NC,R,NQD,VISC,GR>(v, P, a, c, c0, np, i, j, k, d, real, active, piph, dphi, cons, last,
+                                bc, diag, err, topo_set, bid);
 }
-template<int Q, int NC, class R, int NQD = 5, bool VISC = false>
+template<int Q, int NC, class R, int NQD = 5, bool VISC = false, bool GR = false>
 __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v, int last, int bc, int diag){
-   c2p_body<Q,NC,R,NQD,VISC>(v, last, bc, diag, v.move_c2p, v.topo_set, blockIdx.x);
+   c2p_body<Q,NC,R,NQD,VISC,GR>(v, last, bc, diag, v.move_c2p, v.topo_set, blockIdx.x);
 }
 
 /* The sequential walk of set_cells_copy_distant (boundary_functions.c:
@@ -1841,9 +1892,22 @@ __global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc){
       if( P.noise_type && v.noise )                   /* domain.c:202-203 */
          add_noise(P.noise_type, P.noise_abs, P.noise_rel, prim, x, v.noise + 4*(size_t)c);
       double om = get_om(P, r);
-      prim2cons<Q,NC,double>(P, prim, cons, r, om, dV);
-      /* with CT, cons2prim follows set_B_fields (domain.c:211-237): k_c2p */
-      if( !v.ct ) cons2prim<Q,NC>(P, cons, prim, r, om, dV);
+      bool done = false;
+      if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+         if( P.gr ){                /* grmhd2 prim2cons / cons2prim at x (domain.c:205, 237) */
+            const GRParams G = gr_params(P);
+            Metric3 g;
+            metric_at(G, x, g);
+            gr_prim2cons(G, g, prim, cons, x, dV);
+            gr_cons2prim(P, cons, prim, x, dV);
+            done = true;
+         }
+      }
+      if( !done ){
+         prim2cons<Q,NC,double>(P, prim, cons, r, om, dV);
+         /* with CT, cons2prim follows set_B_fields (domain.c:211-237): k_c2p */
+         if( !v.ct ) cons2prim<Q,NC>(P, cons, prim, r, om, dV);
+      }
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){ v.prim[q*N+c] = (R)prim[q]; v.cons[q*N+c] = cons[q]; }
    }else{
@@ -1910,8 +1974,22 @@ __global__ void __launch_bounds__(CB) k_restart(ViewT<R> v, int bc){
          add_noise(P.noise_type, P.noise_abs, P.noise_rel, prim, x, v.noise + 4*(size_t)c);
       }
       double om = get_om(P, r);
-      prim2cons<Q,NC,double>(P, prim, cons, r, om, dV);
-      cons2prim<Q,NC>(P, cons, prim, r, om, dV);
+      bool done = false;
+      if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+         if( P.gr ){
+            double x[3] = {r, piph - .5*dphi, z};
+            const GRParams G = gr_params(P);
+            Metric3 g;
+            metric_at(G, x, g);
+            gr_prim2cons(G, g, prim, cons, x, dV);
+            gr_cons2prim(P, cons, prim, x, dV);
+            done = true;
+         }
+      }
+      if( !done ){
+         prim2cons<Q,NC,double>(P, prim, cons, r, om, dV);
+         cons2prim<Q,NC>(P, cons, prim, r, om, dV);
+      }
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){ v.prim[q*N+c] = (R)prim[q]; v.cons[q*N+c] = cons[q]; }
    }else{
@@ -1950,7 +2028,18 @@ __global__ void __launch_bounds__(CB) k_prim2cons(ViewT<R> v){
    double prim[Q], cons[Q];
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N+c];
-   prim2cons<Q,NC,double>(P, prim, cons, r, get_om(P, r), dV);
+   bool done = false;
+   if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ){
+      if( P.gr ){                   /* calc_cons with grmhd2 at the centroid */
+         double x[3] = {r, piph - .5*dphi, centroid_z(zk[k], zk[k-1])};
+         const GRParams G = gr_params(P);
+         Metric3 g;
+         metric_at(G, x, g);
+         gr_prim2cons(G, g, prim, cons, x, dV);
+         done = true;
+      }
+   }
+   if( !done ) prim2cons<Q,NC,double>(P, prim, cons, r, get_om(P, r), dV);
 #pragma unroll
    for( int q=0 ; q<Q ; ++q ) v.cons[q*N+c] = cons[q];
    raise_err(v, err);
@@ -1968,7 +2057,18 @@ __global__ void __launch_bounds__(CB) k_wcell(ViewT<R> v){
    int cp = c0 + (i+1 == np ? 0 : i+1);
    const DiskParams &P = v.dp[v.ann_disk[a]];
    double w = 0.0;
-   if( P.mesh_motion ) w = .5*((double)v.prim[UPP*N + c] + (double)v.prim[UPP*N + cp]);
+   bool gr = false;
+   if constexpr ( Q == 9 && sizeof(R) == sizeof(double) ) gr = P.gr;
+   if( gr ){                        /* set_wcell with grmhd2's get_omega */
+      if( P.mesh_motion ){
+         int j = v.ann_j[a], k = v.ann_k[a];
+         const double *rj = v.rj + P.rj0 + 1, *zk = v.zk + P.zk0 + 1;
+         double x[3] = {centroid_r(rj[j], rj[j-1]), 0.0, centroid_z(zk[k], zk[k-1])};
+         double pc[Q], pr[Q];
+         for( int q=0 ; q<Q ; ++q ){ pc[q] = (double)v.prim[q*N + c]; pr[q] = (double)v.prim[q*N + cp]; }
+         w = .5*(gr_omega(P, pc, x) + gr_omega(P, pr, x));
+      }
+   }else if( P.mesh_motion ) w = .5*((double)v.prim[UPP*N + c] + (double)v.prim[UPP*N + cp]);
    if( P.mesh_motion == 4 ){
       int j = v.ann_j[a];
       const double *rj = v.rj + P.rj0 + 1;
@@ -2001,29 +2101,39 @@ __global__ void __launch_bounds__(CB) k_mindt(ViewT<R> v){
       int cprev = c0 + (i == 0 ? np-1 : i-1);
       double w = .5*(v.wiph[cprev] + v.wiph[c]);
       double r = centroid_r(rp, rm);
-      double vp = ((double)v.prim[UPP*N+c]-w)*r;
-      double cs = sqrt(P.gam*(double)v.prim[PPP*N+c]/(double)v.prim[RHO*N+c]);
-      if constexpr ( NC == 8 ){                  /* mhd.c:452-486: fast speed */
-         double Br = v.prim[BRR*N+c], Bp = v.prim[BPP*N+c], Bz = v.prim[BZZ*N+c];
-         double b2 = (Br*Br+Bp*Bp+Bz*Bz)/(double)v.prim[RHO*N+c];
-         cs = sqrt(cs*cs + b2);
-      }
-      double maxvr = cs + fabs((double)v.prim[URR*N+c]);
-      double maxvp = cs + fabs(vp);
-      double maxvz = cs + fabs((double)v.prim[UZZ*N+c]);
-      double dtr = (rp-rm)/maxvr;
-      double dtp = (.5*(rp+rm))*get_dp(piph, phim, P.Pmax, &err)/maxvp;
-      double dtz = (zp-zm)/maxvz;
-      double dtm = dtr;
-      if( dtm > dtp ) dtm = dtp;
-      if( dtm > dtz ) dtm = dtz;
-      if( P.visc ){
+      bool gr = false;
+      if constexpr ( NC == 8 && sizeof(R) == sizeof(double) ) gr = P.gr;
+      if( gr ){                     /* mindt of grmhd2, grmhd2.c:748-832 */
          double pc[Q];
-#pragma unroll
          for( int q=0 ; q<Q ; ++q ) pc[q] = (double)v.prim[q*N+c];
-         dtm = visc_dt_limit(P, pc, r, dtm, rp, rm, zp, zm, get_dp(piph, phim, P.Pmax, &err));
+         double xp[3] = {rp, piph, zp}, xm[3] = {rm, phim, zm};
+         double dtg = gr_mindt(P, pc, w, xp, xm, &err);
+         if( dtg == dtg ) dtc = dtg;
+      }else{
+         double vp = ((double)v.prim[UPP*N+c]-w)*r;
+         double cs = sqrt(P.gam*(double)v.prim[PPP*N+c]/(double)v.prim[RHO*N+c]);
+         if constexpr ( NC == 8 ){               /* mhd.c:452-486: fast speed */
+            double Br = v.prim[BRR*N+c], Bp = v.prim[BPP*N+c], Bz = v.prim[BZZ*N+c];
+            double b2 = (Br*Br+Bp*Bp+Bz*Bz)/(double)v.prim[RHO*N+c];
+            cs = sqrt(cs*cs + b2);
+         }
+         double maxvr = cs + fabs((double)v.prim[URR*N+c]);
+         double maxvp = cs + fabs(vp);
+         double maxvz = cs + fabs((double)v.prim[UZZ*N+c]);
+         double dtr = (rp-rm)/maxvr;
+         double dtp = (.5*(rp+rm))*get_dp(piph, phim, P.Pmax, &err)/maxvp;
+         double dtz = (zp-zm)/maxvz;
+         double dtm = dtr;
+         if( dtm > dtp ) dtm = dtp;
+         if( dtm > dtz ) dtm = dtz;
+         if( P.visc ){
+            double pc[Q];
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ) pc[q] = (double)v.prim[q*N+c];
+            dtm = visc_dt_limit(P, pc, r, dtm, rp, rm, zp, zm, get_dp(piph, phim, P.Pmax, &err));
+         }
+         if( dtm == dtm ) dtc = dtm;
       }
-      if( dtm == dtm ) dtc = dtm;
    }
    raise_err(v, err);
    unsigned long long bits = dbits(dtc);

@@ -109,10 +109,10 @@ __host__ __device__ __forceinline__ void metric_at(const GRParams &P, const doub
    else metric_schw(x, P.M, g);
 }
 
-/* prim2cons, grmhd2.c:88-180 (dV = 1) */
+/* prim2cons, grmhd2.c:88-180 (per volume dV; 1 for the Riemann states) */
 __host__ __device__ __forceinline__ void gr_prim2cons(const GRParams &P, const Metric3 &g,
                                                        const double *prim, double *cons,
-                                                       const double *x){
+                                                       const double *x, double dV = 1.0){
    double r = x[0];
    double gl = P.gam;
    double al = g.al, jac = g.jac, sqrtgam = g.sqrtgam;
@@ -145,15 +145,15 @@ __host__ __device__ __forceinline__ void gr_prim2cons(const GRParams &P, const M
    Ub = (UB + uU*uB) / w;
    double rhoh = rho + gl/(gl-1.0)*Pp + b2;
    double rhoe = Pp / (gl-1.0);
-   cons[DDD] = jac * rho*u0 * 1.0;
-   cons[SRR] = jac * (rhoh*u0*l[0] - b0*bd[0]) * 1.0;
-   cons[LLL] = jac * (rhoh*u0*l[1] - b0*bd[1]) * 1.0;
-   cons[SZZ] = jac * (rhoh*u0*l[2] - b0*bd[2]) * 1.0;
+   cons[DDD] = jac * rho*u0 * dV;
+   cons[SRR] = jac * (rhoh*u0*l[0] - b0*bd[0]) * dV;
+   cons[LLL] = jac * (rhoh*u0*l[1] - b0*bd[1]) * dV;
+   cons[SZZ] = jac * (rhoh*u0*l[2] - b0*bd[2]) * dV;
    cons[TAU] = jac * (-(rhoe+0.5*b2)*uU*u0 - (Pp+0.5*b2)*(uU*u0+U[0])
-                           - rho*(uU+1.0)*u0 + Ub*b0) * 1.0;
-   cons[BRR] = sqrtgam * B[0]/r * 1.0;
-   cons[BPP] = sqrtgam * B[1] * 1.0;
-   cons[BZZ] = sqrtgam * B[2] * 1.0;
+                           - rho*(uU+1.0)*u0 + Ub*b0) * dV;
+   cons[BRR] = sqrtgam * B[0]/r * dV;
+   cons[BPP] = sqrtgam * B[1] * dV;
+   cons[BZZ] = sqrtgam * B[2] * dV;
    cons[8] = prim[8]*cons[DDD];
 }
 

@@ -135,7 +135,16 @@ int disco_read_opt(const char *path, disco_modules *m){
    if( opt_value(path, "HYDRO", v, sizeof v) ) return DISCO_ERR_ARG;
    if( !strcmp(v, "euler") ) m->hydro = DISCO_HYDRO_EULER;
    else if( !strcmp(v, "mhd") ) m->hydro = DISCO_HYDRO_MHD;
+   else if( !strcmp(v, "grmhd2") ) m->hydro = DISCO_HYDRO_GRMHD;
    else return DISCO_ERR_UNSUPPORTED;
+   m->metric = DISCO_METRIC_SCHW_KS_RPZ;
+   if( m->hydro == DISCO_HYDRO_GRMHD ){
+      if( opt_value(path, "METRIC", v, sizeof v) ) return DISCO_ERR_ARG;
+      if( !strcmp(v, "schw_ks_rpz") ) m->metric = DISCO_METRIC_SCHW_KS_RPZ;
+      else if( !strcmp(v, "kerr_ks_rpz") ) m->metric = DISCO_METRIC_KERR_KS_RPZ;
+      else return DISCO_ERR_UNSUPPORTED;
+      if( opt_value(path, "FRAME", v, sizeof v) || strcmp(v, "normal") ) return DISCO_ERR_UNSUPPORTED;
+   }
    if( opt_value(path, "BOUNDARY", v, sizeof v) ) return DISCO_ERR_ARG;
    if( !strcmp(v, "fixed") ) m->boundary = DISCO_BC_FIXED;
    else if( !strcmp(v, "zerograd") ) m->boundary = DISCO_BC_ZEROGRAD;
@@ -156,6 +165,7 @@ int disco_read_opt(const char *path, disco_modules *m){
    if( opt_value(path, "INITIAL", v, sizeof v) ) return DISCO_ERR_ARG;
    if( !strcmp(v, "kepler_noise") ) m->initial = DISCO_IC_KEPLER_NOISE;
    else if( !strcmp(v, "mhd_shear_noise") ) m->initial = DISCO_IC_MHD_SHEAR_NOISE;
+   else if( !strcmp(v, "gr_torus_noise") ) m->initial = DISCO_IC_GR_TORUS_NOISE;
    else m->initial = DISCO_IC_HOST;      /* another module: its state comes from the host */
    if( opt_value(path, "ANALYSIS", v, sizeof v) ) m->analysis = DISCO_DIAG_NONE;
    else if( !strcmp(v, "diag_disk2d") ) m->analysis = DISCO_DIAG_DISK2D;

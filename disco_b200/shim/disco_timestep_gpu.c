@@ -84,21 +84,28 @@ static void report_err(const char *what, int s){
  * DISCO_ERR_UNSUPPORTED rather than run without them.  Calling it again
  * re-uploads the domain. */
 int disco_gpu_init( const struct domain * d ){
-   static const char *const hydros[] = {"euler", "mhd"};
+   static const char *const hydros[] = {"euler", "mhd", "grmhd2"};
    static const char *const bcs[] = {"fixed", "zerograd", "fixed3d", "polar", "outflow3d",
                                      "zerograd_omk", "accrete3d"};
    static const char *const pls[] = {"none", "sun", "cm2", "binary_soft", "circular", "cm"};
-   static const char *const ics[] = {"kepler_noise", "mhd_shear_noise"};
+   static const char *const ics[] = {"kepler_noise", "mhd_shear_noise", "gr_torus_noise"};
+   static const int ic_ids[] = {DISCO_IC_KEPLER_NOISE, DISCO_IC_MHD_SHEAR_NOISE, DISCO_IC_GR_TORUS_NOISE};
+   static const char *const metrics[] = {"schw_ks_rpz", "kerr_ks_rpz"};
    static const char *const diags[] = {"diag_disk2d", "diag_euler", "diag_mhdmri"};
    static const int diag_ids[] = {DISCO_DIAG_DISK2D, DISCO_DIAG_EULER, DISCO_DIAG_MHDMRI};
    if( !d ) return DISCO_ERR_ARG;
    if( g_batch ){ disco_batch_destroy(g_batch); g_batch = NULL; }
    disco_modules m;
    memset(&m, 0, sizeof m);
-   m.hydro = module_id(HYDRO, hydros, 2);
+   m.hydro = module_id(HYDRO, hydros, 3);
    m.boundary = module_id(BOUNDARY, bcs, 7);
    m.planets = module_id(PLANETS, pls, 6);
-   m.initial = module_id(INITIAL, ics, 2);
+   int ii = module_id(INITIAL, ics, 3);
+   m.initial = ii >= 0 ? ic_ids[ii] : -1;
+   m.metric = module_id(METRIC, metrics, 2);
+   if( m.hydro == DISCO_HYDRO_GRMHD && (m.metric < 0 || strcmp(FRAME, "normal") != 0) )
+      return DISCO_ERR_UNSUPPORTED;
+   if( m.metric < 0 ) m.metric = DISCO_METRIC_SCHW_KS_RPZ;     /* not read without grmhd2 */
    /* any other Initial module: setupCells evaluated it here on the host, and
     * boundaries that do not call it again (zerograd, outflow3d) run as is */
    if( m.initial < 0 ) m.initial = DISCO_IC_HOST;

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define DISCO_ABI_VERSION 2
+#define DISCO_ABI_VERSION 3
 
 enum disco_status {
    DISCO_OK = 0,
@@ -53,7 +53,10 @@ enum disco_status {
 
 /* Module choices, one per Makefile_opt.in line (Makefile:11-26).  The names
  * match the reference's module file names. */
-enum disco_hydro    { DISCO_HYDRO_EULER = 0, DISCO_HYDRO_MHD = 1 };
+enum disco_hydro    { DISCO_HYDRO_EULER = 0, DISCO_HYDRO_MHD = 1, DISCO_HYDRO_GRMHD = 2 };
+/* METRIC of a grmhd2 build: Hydro/Metric/schw_ks_rpz.c, or the new Kerr-Schild
+ * module kerr_ks_rpz (spin Metric_Par3; the reference has no Kerr metric) */
+enum disco_metric   { DISCO_METRIC_SCHW_KS_RPZ = 0, DISCO_METRIC_KERR_KS_RPZ = 1 };
 enum disco_boundary { DISCO_BC_FIXED = 0, DISCO_BC_ZEROGRAD = 1, DISCO_BC_FIXED3D = 2,
                       DISCO_BC_POLAR = 3, DISCO_BC_OUTFLOW3D = 4, DISCO_BC_ZEROGRAD_OMK = 5,
                       DISCO_BC_ACCRETE3D = 6 };
@@ -64,7 +67,8 @@ enum disco_planets  { DISCO_PLANETS_NONE = 0, DISCO_PLANETS_SUN = 1, DISCO_PLANE
  * any reference IC in setupCells): the state must come from set_cells, and
  * only boundaries that never re-evaluate initial() during the steps
  * (zerograd, outflow3d) are accepted. */
-enum disco_initial  { DISCO_IC_KEPLER_NOISE = 0, DISCO_IC_MHD_SHEAR_NOISE = 1, DISCO_IC_HOST = 2 };
+enum disco_initial  { DISCO_IC_KEPLER_NOISE = 0, DISCO_IC_MHD_SHEAR_NOISE = 1, DISCO_IC_HOST = 2,
+                      DISCO_IC_GR_TORUS_NOISE = 3 };
 enum disco_analysis { DISCO_DIAG_NONE = 0, DISCO_DIAG_DISK2D = 1, DISCO_DIAG_EULER = 2,
                       DISCO_DIAG_MHDMRI = 3 };
 enum disco_precision{ DISCO_PREC_FP64 = 0, DISCO_PREC_MIXED = 1 };
@@ -79,6 +83,7 @@ enum disco_schedule { DISCO_SCHED_KERNELS = 0, DISCO_SCHED_PERSISTENT = 1 };
 typedef struct disco_modules {
    int hydro, boundary, planets, initial, analysis;
    int num_c, num_n, ct_mode;
+   int metric;                 /* enum disco_metric, for HYDRO = grmhd2 */
 } disco_modules;
 
 /* Run-time parameters: the subset of struct param_list (paul.h:51-127) that

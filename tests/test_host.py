@@ -66,7 +66,7 @@ def test_struct_layouts_match_library():
     lib = db.library()
     assert lib.disco_sizeof(0) == C.sizeof(db.Params)
     assert lib.disco_sizeof(1) == C.sizeof(db.Modules)
-    assert lib.disco_abi_version() == 2
+    assert lib.disco_abi_version() == 3
 
 
 def test_library_exports_every_declared_symbol():
