@@ -477,6 +477,97 @@ def face_flux_div(disk, batch):
     return div, float(np.abs(Phi).max())
 
 
+B_ALG_GR = 8 * (10 * 9 + 12)            # HBM bytes per zone-update, Q = 9 without face fluxes (816)
+C3_GRID = {"Num_R": 192, "Num_Z": 96, "aspect": 0.75}          # Np 463 per annulus
+
+
+def config3_leg(args, local, stream):
+    """Config 3: the GRMHD torus timestep (grmhd2, Kerr-Schild a = 0.9, HLL,
+    noble2d cons->prim, fixed3d), 192 x 96 annuli of 463 cells (8.53M real
+    cells), FP64; throughput, step roofline against the 816 B/zone-update of
+    the Q = 9 state without face fluxes, and the reference's serial CPU code
+    on a reduced-Nz slice of the same grid (Schwarzschild, a = 0: the
+    reference has no Kerr metric)."""
+    import numpy as np
+    import torch
+    import disco_b200 as db
+    from disco_b200.workloads import write_par
+    hbm, kind = peaks()
+    over = dict(C3_GRID, Metric_Par3=0.9)
+    p = write_par(over, base="c3_grtorus")
+    disk = db.Disk.from_files(p, os.path.join(db.TEMPLATES, "c3_grtorus_kerr.in"))
+    os.unlink(p)
+    nsteps = 10
+    out = {"workload": "GRMHD torus, Kerr-Schild a=0.9, HLL, Nr=%d Nz=%d (real), Np %d, %d real cells"
+                       % (C3_GRID["Num_R"], C3_GRID["Num_Z"], int(np.max(disk.Np)), disk.nreal),
+           "steps": nsteps, "warmup": 3}
+    b = db.Batch([disk], device=local)
+    b.set_stream(stream.cuda_stream)
+    b.run(3)
+    b.sync()
+    kt = {}
+    for name, t in b.kernel_times():
+        kt[name] = kt.get(name, 0.0) + t
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.run(nsteps)
+    e1.record(stream)
+    e1.synchronize()
+    if b.last_error() != 0:
+        raise RuntimeError("device error in the config-3 leg")
+    ms = e0.elapsed_time(e1)
+    zu = disk.nreal * nsteps / (ms / 1e3)
+    st = b.get_cells()
+    r = disk.real == 1
+    out["fp64"] = {"zone_updates_per_s": zu, "ms_per_step": ms / nsteps,
+                   "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(kt.items(), key=lambda x: -x[1])},
+                   "step_roofline": {"bytes_per_zone_update": B_ALG_GR, "achieved": B_ALG_GR * zu / 1e9,
+                                     "peak": hbm, "unit": "GB/s", "frac": B_ALG_GR * zu / 1e9 / hbm,
+                                     "peak_kind": kind},
+                   "finite": bool(np.isfinite(st["prim"][r]).all())}
+    del st
+    b.close()
+    if rank0_cpu(args):
+        try:
+            import pyoracle
+            binary = pyoracle.ref_binary("c3_grtorus")
+            if not os.path.exists(binary):
+                pyoracle.build_ref("c3_grtorus")
+            d = tempfile.mkdtemp(prefix="dref3_")
+            pdir = tempfile.mkdtemp(prefix="dpar3_")
+            sl = dict(C3_GRID, Num_Z=8, Z_Min=-20.0 * 8 / 96, Z_Max=20.0 * 8 / 96)
+            src = write_par_text("c3_grtorus", sl)
+            with open(os.path.join(d, "in.par"), "w") as f:
+                f.write(src)
+            res = subprocess.run([binary, d, "2", "--time"], capture_output=True, text=True, timeout=600)
+            rr = json.loads([l for l in res.stdout.splitlines() if l.startswith("{")][0])
+            out["cpu_baseline"] = {"value": rr["zone_updates_per_s"], "unit": "zone-updates/s", "cores": 1,
+                                   "kind": "reference",
+                                   "sample": "reference grmhd2 + schw_ks_rpz (a = 0), %d x 8 annuli of the "
+                                             "same r grid and Np, 2 steps, one process" % C3_GRID["Num_R"]}
+            subprocess.run(["rm", "-rf", d, pdir])
+        except Exception as ex:
+            out["cpu_baseline"] = {"value": None, "sample": "unavailable: %s" % ex}
+    return out
+
+
+def rank0_cpu(args):
+    return not args.no_cpu_baseline and int(os.environ.get("RANK", "0")) == 0
+
+
+def write_par_text(base, overrides):
+    """A bundled template in.par with keys replaced, as text."""
+    out = []
+    with open(os.path.join(REPO, "disco_b200", "templates", base + ".par")) as f:
+        for line in f:
+            tok = line.split()
+            if tok and tok[0] in overrides:
+                line = "%s\t\t%s\n" % (tok[0], overrides[tok[0]])
+            out.append(line)
+    return "".join(out)
+
+
 C2P_GRID = {"Nr": 192, "Nz": 96, "Np": 462, "rmin": 1.5, "rmax": 50.0, "zmin": -20.0, "zmax": 20.0}
 C2P_TOL, C2P_NEXTRA, C2P_MAXIT = 1e-10, 10, 30
 C2P_BYTES = 8 * (9 + 3 + 5 + 9)         # read cons, x, the 5 prims of the warm start; write prims
@@ -753,6 +844,11 @@ def run_ours(args, world, rank, local):
         config4 = config4_leg(args, local, stream)
         barrier()
 
+    config3 = None
+    if not args.no_config3:
+        config3 = config3_leg(args, local, stream)
+        barrier()
+
     c2p = None
     if not args.no_c2p:
         c2p = c2p_leg(args, local, stream)
@@ -795,6 +891,7 @@ def run_ours(args, world, rank, local):
             "gpu_launches": launches_per_step * args.steps,
             "mixed_form": mixed,
             "config1_mhd3d": config1,
+            "config3_grtorus": config3,
             "config4_binary3d": config4,
             "c2p": c2p,
             "clocks": ck,
@@ -817,6 +914,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--no-c2p", action="store_true", help="skip the GRMHD cons->prim leg")
     ap.add_argument("--no-config1", action="store_true", help="skip the 3D MHD (config 1) leg")
+    ap.add_argument("--no-config3", action="store_true", help="skip the GRMHD torus (config 3) leg")
     ap.add_argument("--no-config4", action="store_true",
                     help="skip the 40M-cell 3D MHD circumbinary (config 4) leg")
     args = ap.parse_args()

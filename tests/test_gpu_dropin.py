@@ -71,6 +71,24 @@ def test_dropin_bitexact_libm_free():
         assert np.array_equal(b["gpu_faces_1"][k], a["faces_1"][k]), k
 
 
+def test_dropin_grmhd_bitexact():
+    """The GRMHD module selection (grmhd2, schw_ks_rpz, normal frame, HLL,
+    fixed3d, the gr_torus_noise torus) through the drop-in: the reference's
+    own setupCells and boundaries on the host, every step on the device."""
+    ref, hyb = _binaries("c3_grtorus")
+    par = os.path.join(GOLDEN, "c3_grtorus.par")
+    a, b = _run(ref, par, 5), _run(hyb, par, 5)
+    assert np.array_equal(a["dt"], b["dt"])
+    r = a["real"] == 1
+    for k in ("prim", "cons"):
+        assert np.array_equal(a[k][r], b[k][r]), k
+    for k in ("piph", "dphi"):
+        assert np.array_equal(a[k], b[k]), k
+    for k in ("iL", "iR", "LRtype"):
+        assert np.array_equal(a["faces_1"][k], b["faces_1"][k]), k
+    assert a["dt_next"] == b["dt_next"]
+
+
 def test_dropin_config0_20_steps():
     ref, hyb = _binaries("c0_kepler2d")
     import disco_b200 as db
