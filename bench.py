@@ -417,7 +417,8 @@ def config4_leg(args, local, stream):
     nsteps = 50
     hbm, kind = peaks()
     out = {"workload": "3D MHD circumbinary disk, softened equal-mass binary, HLLD + CT, zerograd, "
-                       "Nr=%d Nz=%d (incl. ghosts), Np max %d, %d real cells"
+                       "Nr=%d Nz=%d (incl. ghosts), Np max %d, %d real cells (the configuration's "
+                       "'about 50M' is not reachable with Np <= 1536 on 384 x 128 annuli)"
                        % (disk.Nr, disk.Nz, int(np.max(disk.Np)), disk.nreal),
            "steps": nsteps, "warmup": 3}
     ref = None
@@ -453,7 +454,34 @@ def config4_leg(args, local, stream):
         del st
         b.close()
     out["mixed_speedup_vs_fp64"] = out["mixed"]["zone_updates_per_s"] / out["fp64"]["zone_updates_per_s"]
+    if rank0_cpu(args):
+        out["cpu_baseline"] = reference_slice_rate("c4_binary3d", {"Num_Z": 4, "Z_Min": -0.5 * 4 / 128,
+                                                                  "Z_Max": 0.5 * 4 / 128}, 1,
+                                                   "reference mhd + hlld + 3D CT + binary_soft, the full "
+                                                   "384-annulus r grid and Np on 4 z layers, 1 step, one "
+                                                   "process")
     return out
+
+
+def reference_slice_rate(cfg, overrides, nsteps, sample):
+    """The reference binary of a module configuration on a reduced slice of
+    a workload (its template in.par with overrides), one process: the
+    cpu_baseline object."""
+    try:
+        import pyoracle
+        binary = pyoracle.ref_binary(cfg)
+        if not os.path.exists(binary):
+            pyoracle.build_ref(cfg)
+        d = tempfile.mkdtemp(prefix="dref_")
+        with open(os.path.join(d, "in.par"), "w") as f:
+            f.write(write_par_text(cfg, overrides))
+        res = subprocess.run([binary, d, str(nsteps), "--time"], capture_output=True, text=True, timeout=900)
+        subprocess.run(["rm", "-rf", d])
+        rr = json.loads([l for l in res.stdout.splitlines() if l.startswith("{")][0])
+        return {"value": rr["zone_updates_per_s"], "unit": "zone-updates/s", "cores": 1, "kind": "reference",
+                "sample": sample + " (%d real cells)" % rr["real_cells"]}
+    except Exception as ex:
+        return {"value": None, "sample": "unavailable: %s" % ex}
 
 
 def face_flux_div(disk, batch):
@@ -529,26 +557,10 @@ def config3_leg(args, local, stream):
     del st
     b.close()
     if rank0_cpu(args):
-        try:
-            import pyoracle
-            binary = pyoracle.ref_binary("c3_grtorus")
-            if not os.path.exists(binary):
-                pyoracle.build_ref("c3_grtorus")
-            d = tempfile.mkdtemp(prefix="dref3_")
-            pdir = tempfile.mkdtemp(prefix="dpar3_")
-            sl = dict(C3_GRID, Num_Z=8, Z_Min=-20.0 * 8 / 96, Z_Max=20.0 * 8 / 96)
-            src = write_par_text("c3_grtorus", sl)
-            with open(os.path.join(d, "in.par"), "w") as f:
-                f.write(src)
-            res = subprocess.run([binary, d, "2", "--time"], capture_output=True, text=True, timeout=600)
-            rr = json.loads([l for l in res.stdout.splitlines() if l.startswith("{")][0])
-            out["cpu_baseline"] = {"value": rr["zone_updates_per_s"], "unit": "zone-updates/s", "cores": 1,
-                                   "kind": "reference",
-                                   "sample": "reference grmhd2 + schw_ks_rpz (a = 0), %d x 8 annuli of the "
-                                             "same r grid and Np, 2 steps, one process" % C3_GRID["Num_R"]}
-            subprocess.run(["rm", "-rf", d, pdir])
-        except Exception as ex:
-            out["cpu_baseline"] = {"value": None, "sample": "unavailable: %s" % ex}
+        out["cpu_baseline"] = reference_slice_rate(
+            "c3_grtorus", dict(C3_GRID, Num_Z=8, Z_Min=-20.0 * 8 / 96, Z_Max=20.0 * 8 / 96), 2,
+            "reference grmhd2 + schw_ks_rpz (a = 0; the reference has no Kerr metric), the full r grid "
+            "and Np on 8 z layers, 2 steps, one process")
     return out
 
 

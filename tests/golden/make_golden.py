@@ -147,6 +147,10 @@ CASES = {
     # schw_ks_rpz and the normal frame, HLL): the gr_torus_noise torus with
     # its loop field and pressure noise, fixed3d ghosts; by-cell mesh motion
     # (get_omega of grmhd2) and a fixed mesh.  Only +, -, *, /, sqrt occur.
+    # config 4's module set (MHD, HLLD, 3D CT, zerograd) with the softened
+    # equal-mass binary (Planets/binary_soft.c of this repo, compiled into the
+    # reference build): point-mass forces use libm (1e-11)
+    "c4_binary3d": ("c4_binary3d", {"Num_R": 12, "Num_Z": 6, "Constrained_Transport": 1}, 5),
     "c3_grtorus": ("c3_grtorus", {"Num_R": 16, "Num_Z": 8}, 5),
     "c3_grtorus_mm0": ("c3_grtorus", {"Num_R": 12, "Num_Z": 6, "Mesh_Motion": 0,
                                       "Init_Par0": 2718}, 4),
@@ -159,7 +163,7 @@ BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": 
             "c1_polar": "c1_mhd2d", "c1_polar3d": "c1_mhd3d", "c0_outflow3d": "c0_kepler2d",
             "c1_omk3d": "c1_mhd3d", "c1_accrete3d": "c1_mhd3d", "c0_rigid_zg": "c0_kepler2d",
             "c0_circular": "c0_kepler2d", "c0_cm": "c0_kepler2d", "c0_diag_euler": "c0_kepler2d",
-            "c0_diag_euler3d": "c0_kepler2d", "c1_diag_mhdmri": "c1_mhd2d", "c3_grtorus": "c3_grtorus"}
+            "c0_diag_euler3d": "c0_kepler2d", "c1_diag_mhdmri": "c1_mhd2d", "c3_grtorus": "c3_grtorus", "c4_binary3d": "c4_binary3d"}
 
 
 def par_text(cfg_par, overrides):

@@ -31,8 +31,10 @@ from helpers import case_disk, observed_slots as _observed_slots, par_with, rel_
 
 pytestmark = pytest.mark.gpu
 
-CT_CASES = ["c1_ct2d", "c1_ct_rigid", "c1_ct_hll_fe", "c1_ct3d", "c1_ct3d_rigid"]
-CT_TOL = {"c1_ct2d": 1e-11, "c1_ct_hll_fe": 1e-11, "c1_ct3d": 1e-11}
+# c4_binary3d: config 4's module set with the softened binary
+# (Planets/binary_soft.c in the reference build)
+CT_CASES = ["c1_ct2d", "c1_ct_rigid", "c1_ct_hll_fe", "c1_ct3d", "c1_ct3d_rigid", "c4_binary3d"]
+CT_TOL = {"c1_ct2d": 1e-11, "c1_ct_hll_fe": 1e-11, "c1_ct3d": 1e-11, "c4_binary3d": 1e-11}
 
 
 def _from_golden(disk, g):
