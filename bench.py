@@ -522,12 +522,14 @@ def config3_leg(args, local, stream):
     from disco_b200.workloads import write_par
     hbm, kind = peaks()
     over = dict(C3_GRID, Metric_Par3=0.9)
+    if args.c3_nz != C3_GRID["Num_Z"]:           # a slice of the torus (profiling runs)
+        over.update(Num_Z=args.c3_nz, Z_Min=-20.0 * args.c3_nz / 96, Z_Max=20.0 * args.c3_nz / 96)
     p = write_par(over, base="c3_grtorus")
     disk = db.Disk.from_files(p, os.path.join(db.TEMPLATES, "c3_grtorus_kerr.in"))
     os.unlink(p)
     nsteps = 10
     out = {"workload": "GRMHD torus, Kerr-Schild a=0.9, HLL, Nr=%d Nz=%d (real), Np %d, %d real cells"
-                       % (C3_GRID["Num_R"], C3_GRID["Num_Z"], int(np.max(disk.Np)), disk.nreal),
+                       % (C3_GRID["Num_R"], over["Num_Z"], int(np.max(disk.Np)), disk.nreal),
            "steps": nsteps, "warmup": 3}
     b = db.Batch([disk], device=local)
     b.set_stream(stream.cuda_stream)
@@ -927,12 +929,22 @@ def main():
     ap.add_argument("--no-c2p", action="store_true", help="skip the GRMHD cons->prim leg")
     ap.add_argument("--no-config1", action="store_true", help="skip the 3D MHD (config 1) leg")
     ap.add_argument("--no-config3", action="store_true", help="skip the GRMHD torus (config 3) leg")
+    ap.add_argument("--c3-nz", type=int, default=96, help="z layers of the config-3 torus (96)")
+    ap.add_argument("--only-config3", action="store_true",
+                    help="run the config-3 leg alone (no headline line), e.g. for profiling")
     ap.add_argument("--no-config4", action="store_true",
                     help="skip the 40M-cell 3D MHD circumbinary (config 4) leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = dist_setup()
+    if args.only_config3:
+        import torch
+        torch.cuda.set_device(local)
+        args.no_cpu_baseline = True
+        print(json.dumps({"config3_grtorus": config3_leg(args, local, torch.cuda.Stream(device=local))}),
+              flush=True)
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
     else:
