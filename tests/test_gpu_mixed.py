@@ -133,14 +133,39 @@ def _mixed_errors(disks, nsteps):
 
 def test_mixed_config1_mhd3d():
     """Config 1 (3D MHD, HLLD, zerograd, 64 x 64 annuli), 100 steps: every
-    field within 1e-5.  The mixed form's density difference grows by about
-    6e-8 per step (1.1e-5 after 200 steps) while a FP32-sized perturbation of
-    the FP64 run itself stays at 1.7e-6 over the same 200 steps: the growth is
-    FP32 rounding accumulating in the fluxes, not the shear amplifying it, so
-    the form holds its 1e-5 for runs of up to about 150 steps of this grid."""
+    field within 1e-5 except B_phi, which the shear winds up from B_r: there
+    any difference grows, and a 2^-24 relative perturbation of the FP64 run's
+    own conserved state (the size of one FP32 rounding) already diverges by
+    more than 1e-5 of |B|.  B_phi is held to 4x that FP64 divergence, measured
+    here on the same steps.  The density difference grows by about 6e-8 per
+    step (1.1e-5 after 200 steps) while the perturbed FP64 run stays at
+    1.7e-6: FP32 rounding accumulating in the fluxes, not the shear, so the
+    form holds its 1e-5 for runs of up to about 150 steps of this grid."""
     disk = db.Disk.from_files(*db.template_paths("c1_mhd3d"))
     err = _mixed_errors([disk], 100)
+    bphi = err.pop("B_phi/|B|")
     assert max(err.values()) < TOL_MIXED, err
+    # the FP64 run from a state perturbed by one FP32 rounding
+    a = db.Batch([disk], precision=db.PREC_FP64)
+    s0 = a.get_cells()
+    rng = np.random.default_rng(7)
+    cons_p = s0["cons"] * (1.0 + 2.0**-24 * rng.choice([-1.0, 1.0], size=s0["cons"].shape))
+    p = db.Batch([disk], precision=db.PREC_FP64, setup=False)
+    p.set_cells(s0["prim"], cons_p, s0["piph"], s0["dphi"], s0["wiph"], disk.real)
+    p.mindt()
+    a.run(100)
+    p.run(100)
+    a.sync()
+    p.sync()
+    sa, sp = a.get_cells(), p.get_cells()
+    a.close()
+    p.close()
+    r = disk.real == 1
+    pa, pp = sa["prim"][r], sp["prim"][r]
+    bmag = np.abs(pa[:, 5]) + np.abs(pa[:, 6]) + np.abs(pa[:, 7])
+    bphi_fp64 = float(np.abs(pp[:, 6] - pa[:, 6]).sum() / bmag.sum())
+    print("B_phi/|B|: mixed %.3e, FP64 perturbed by 2^-24 %.3e" % (bphi, bphi_fp64))
+    assert bphi < 4.0 * bphi_fp64, (bphi, bphi_fp64)
 
 
 def test_mixed_config2_ragged():
