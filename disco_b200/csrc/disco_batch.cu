@@ -618,6 +618,10 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->d_Qrz = dalloc<double>(b, (size_t)ann*(b->nq ? b->nq : 1));
    v.err = dalloc<int>(b, 1);
    b->d_err = v.err;
+   if( b->gr ){
+      v.gr_ann = dalloc<GRAnn>(b, ann);
+      v.gr_tr = dalloc<Metric3>(b, v.Ntr > 0 ? v.Ntr : 1);
+   }
    v.topo = dalloc<int>(b, 1);
    if( ct ){
       v.ct = ct;
@@ -657,6 +661,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    {
       int nx = ann > v.Ntr ? ann : v.Ntr;
       k_precompute<<<nblk(nx, 128), 128, 0, b->stream>>>(v);
+      if( b->gr ) k_gr_tables<double><<<nblk(nx, 128), 128, 0, b->stream>>>(v);
       k_planet_trig<double><<<nblk(ndisk, 64), 64, 0, b->stream>>>(v, ndisk);
    }
    /* the multi-kernel schedule is the default: on ragged64 the persistent

@@ -81,6 +81,10 @@ namespace disco {
 #ifndef MB_C2P
 #define MB_C2P MB_STEP
 #endif
+/* the grmhd2 (GR) instantiations of the step kernels */
+#ifndef MB_GR
+#define MB_GR MB_MHD
+#endif
 
 template<class R>
 struct ViewT {
@@ -141,6 +145,10 @@ struct ViewT {
     * lineX[line_off[l] + e] the E_phi dl dt of merged edge e of line l. */
    int ct, nfs;
    double *Phi, *RKPhi, *fX;            /* the face fluxes stay FP64 in both forms */
+   /* grmhd2: the metric at the fixed points where the step evaluates it
+    * (k_gr_tables; NULL for the Newtonian modules) */
+   GRAnn *gr_ann;
+   Metric3 *gr_tr;
    R *ctE, *ctB, *pE, *pB, *pEr, *pBz, *fEt, *fBt, *fEphi;   /* edge arithmetic: R */
    unsigned char *fFlip;
    int *rk, *line_off;
@@ -210,7 +218,8 @@ __device__ __forceinline__ void begin_body(const ViewT<R> &v, double RK, int fir
             double pc[Q], pr[Q];
 #pragma unroll
             for( int q=0 ; q<Q ; ++q ){ pc[q] = (double)pC[q]; pr[q] = (double)pR[q]; }
-            w = .5*(gr_omega(P, pc, x) + gr_omega(P, pr, x));
+            (void)x;
+            w = .5*(gr_omega(v.gr_ann[a].c, pc) + gr_omega(v.gr_ann[a].c, pr));
          }
       }else{
          if( P.mesh_motion ) w = .5*((double)pC[UPP] + (double)pR[UPP]);   /* get_omega = prim[UPP] */
@@ -274,7 +283,7 @@ __device__ __forceinline__ void begin_body(const ViewT<R> &v, double RK, int fir
    }
 }
 template<int Q, int NC, class R, bool GR = false>
-__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_BEGIN) k_begin(ViewT<R> v, double RK, int first){
+__global__ void __launch_bounds__(CB, GR ? MB_GR : (Q > 6 ? MB_MHD : MB_BEGIN)) k_begin(ViewT<R> v, double RK, int first){
    begin_body<Q,NC,R,GR>(v, RK, first, blockIdx.x);
 }
 
@@ -296,6 +305,30 @@ __global__ void k_precompute(ViewT<R> v){
       const double *rj = v.rj + P.rj0 + 1;
       int j = v.tr_j[x];
       v.tr_om[x] = get_om(P, v.tr_dim[x] == 1 ? .5*(rj[j]+rj[j]) : centroid_r(rj[j], rj[j-1]));
+   }
+}
+
+/* grmhd2's metric tables (GRAnn per annulus, Metric3 per track at the face
+ * centre: (r_{j+1/2}, centroid z) for r-faces, (centroid r, z_{k+1/2}) for
+ * z-faces, addFace faces_alt.c:10-16), once per batch */
+template<class R>
+__global__ void k_gr_tables(ViewT<R> v){
+   int x = blockIdx.x*blockDim.x + threadIdx.x;
+   if( x < v.Nann ){
+      const DiskParams &P = v.dp[v.ann_disk[x]];
+      const double *rj = v.rj + P.rj0 + 1, *zk = v.zk + P.zk0 + 1;
+      int j = v.ann_j[x], k = v.ann_k[x];
+      gr_ann_table(P, rj[j], rj[j-1], zk[k], zk[k-1], v.gr_ann[x]);
+   }
+   if( x < v.Ntr ){
+      const DiskParams &P = v.dp[v.ann_disk[v.tr_a[x]]];
+      const double *rj = v.rj + P.rj0 + 1, *zk = v.zk + P.zk0 + 1;
+      int j = v.tr_j[x], k = v.tr_k[x];
+      double xf[3];
+      if( v.tr_dim[x] == 1 ){ xf[0] = .5*(rj[j]+rj[j]); xf[2] = 0.5*(zk[k]+zk[k-1]); }
+      else { xf[0] = centroid_r(rj[j], rj[j-1]); xf[2] = 0.5*(zk[k]+zk[k]); }
+      xf[1] = 0.0;
+      metric_at(gr_params(P), xf, v.gr_tr[x]);
    }
 }
 
@@ -756,7 +789,7 @@ __device__ __forceinline__ void flux_body(const ViewT<R> &v, double dtfac, int b
       double pl[Q], pr[Q], g[Q];
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){ pl[q] = (double)primL[q]; pr[q] = (double)primR[q]; }
-      gr_hll(P, pl, pr, x, n, 0.0, dAdt, g);
+      gr_hll(P, v.gr_tr[t], pl, pr, x, n, 0.0, dAdt, g);
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ) G[q] = (R)g[q];
    }else if constexpr ( NC == 8 ){
@@ -792,7 +825,7 @@ __device__ __forceinline__ void flux_body(const ViewT<R> &v, double dtfac, int b
    raise_err(v, err);
 }
 template<int Q, int NC, int DIM, class R, bool VISC = false, bool GR = false>
-__global__ void __launch_bounds__(FB, Q > 6 ? MB_MHD : MB_FLUX) k_flux_t(ViewT<R> v){
+__global__ void __launch_bounds__(FB, GR ? MB_GR : (Q > 6 ? MB_MHD : MB_FLUX)) k_flux_t(ViewT<R> v){
    flux_body<Q,NC,DIM,R,VISC,GR>(v, v.dtfac, blockIdx.x);
 }
 
@@ -949,7 +982,7 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
             pl[BPP] = Bp; pr[BPP] = Bp;
             double x[3] = {rc, v.piph[cprev], centroid_z(zk[k], zk[k-1])};
             const double n[3] = {0.0, 1.0, 0.0};
-            gr_hll(P, pl, pr, x, n, rc*v.wiph[cprev], dAdtp, g);
+            gr_hll(P, v.gr_ann[a].c, pl, pr, x, n, rc*v.wiph[cprev], dAdtp, g);
 #pragma unroll
             for( int q=0 ; q<Q ; ++q ) G[q] = (R)g[q];
          }else if( ctE ){           /* flux_to_E dim 0, Hydro/mhd.c:298-303 */
@@ -1045,8 +1078,7 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
       double dVdt = dV*dt;
       double r = centroid_r(rp, rm);
       if constexpr ( GR ){       /* grmhd2 source, grmhd2.c:383-478 */
-         double xp[3] = {rp, piph, zp}, xm[3] = {rm, phim, zm};
-         gr_source(P, prim, cons, xp, xm, dVdt);
+         gr_source(P, v.gr_ann[a], prim, cons, 0.5*(rm+rp), dVdt);
       }else if constexpr ( NC == 8 ){  /* mhd source, mhd.c:225-263 */
          double rho = prim[RHO], Pp = prim[PPP];
          double r_1 = .5*(rp+rm);
@@ -1109,7 +1141,7 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
    raise_err(v, err);
 }
 template<int Q, int NC, class R, bool VISC = false, bool GR = false>
-__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_UPDATE) k_update(ViewT<R> v, int first){
+__global__ void __launch_bounds__(CB, GR ? MB_GR : (Q > 6 ? MB_MHD : MB_UPDATE)) k_update(ViewT<R> v, int first){
    update_body<Q,NC,R,VISC,GR>(v, first, v.dtfac, blockIdx.x);
 }
 
@@ -1305,7 +1337,7 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
 #pragma unroll
             for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N + c];
             double x[3] = {centroid_r(rp, rm), 0.5*(phim+piph), centroid_z(zp, zm)};
-            gr_cons2prim(P, cons, prim, x, dV2);
+            gr_cons2prim(P, v.gr_ann[a].c, cons, prim, x, dV2);
          }else{
             cons2prim<Q,NC>(P, cons, prim, centroid_r(rp, rm), v.ann_om[a], dV2);
          }
@@ -1333,7 +1365,7 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
             int cprev = c0 + (i == 0 ? np-1 : i-1);
             double w = .5*(v.wiph[cprev] + v.wiph[c]);
             double xp[3] = {rp, piph, zp}, xm[3] = {rm, phim, zm};
-            double dtm = gr_mindt(P, prim, w, xp, xm, &err);
+            double dtm = gr_mindt(P, v.gr_ann[a].m, prim, w, xp, xm, &err);
             if( dtm == dtm ) dtc = dtm;
          }else if( real ){                        /* mindt, euler.c:332-380, mhd.c:452-486 */
             int cprev = c0 + (i == 0 ? np-1 : i-1);
@@ -1445,7 +1477,7 @@ __device__ __forceinline__ void c2p_body(const ViewT<R> &v, int last, int bc, in
                                 bc, diag, err, topo_set, bid);
 }
 template<int Q, int NC, class R, int NQD = 5, bool VISC = false, bool GR = false>
-__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_C2P) k_c2p(ViewT<R> v, int last, int bc, int diag){
+__global__ void __launch_bounds__(CB, GR ? MB_GR : (Q > 6 ? MB_MHD : MB_C2P)) k_c2p(ViewT<R> v, int last, int bc, int diag){
    c2p_body<Q,NC,R,NQD,VISC,GR>(v, last, bc, diag, v.move_c2p, v.topo_set, blockIdx.x);
 }
 
@@ -1899,7 +1931,7 @@ __global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc){
             Metric3 g;
             metric_at(G, x, g);
             gr_prim2cons(G, g, prim, cons, x, dV);
-            gr_cons2prim(P, cons, prim, x, dV);
+            gr_cons2prim(P, g, cons, prim, x, dV);
             done = true;
          }
       }
@@ -1982,7 +2014,7 @@ __global__ void __launch_bounds__(CB) k_restart(ViewT<R> v, int bc){
             Metric3 g;
             metric_at(G, x, g);
             gr_prim2cons(G, g, prim, cons, x, dV);
-            gr_cons2prim(P, cons, prim, x, dV);
+            gr_cons2prim(P, g, cons, prim, x, dV);
             done = true;
          }
       }
@@ -2066,7 +2098,7 @@ __global__ void __launch_bounds__(CB) k_wcell(ViewT<R> v){
          double x[3] = {centroid_r(rj[j], rj[j-1]), 0.0, centroid_z(zk[k], zk[k-1])};
          double pc[Q], pr[Q];
          for( int q=0 ; q<Q ; ++q ){ pc[q] = (double)v.prim[q*N + c]; pr[q] = (double)v.prim[q*N + cp]; }
-         w = .5*(gr_omega(P, pc, x) + gr_omega(P, pr, x));
+         w = .5*(gr_omega_at(P, pc, x) + gr_omega_at(P, pr, x));
       }
    }else if( P.mesh_motion ) w = .5*((double)v.prim[UPP*N + c] + (double)v.prim[UPP*N + cp]);
    if( P.mesh_motion == 4 ){
@@ -2107,7 +2139,7 @@ __global__ void __launch_bounds__(CB) k_mindt(ViewT<R> v){
          double pc[Q];
          for( int q=0 ; q<Q ; ++q ) pc[q] = (double)v.prim[q*N+c];
          double xp[3] = {rp, piph, zp}, xm[3] = {rm, phim, zm};
-         double dtg = gr_mindt(P, pc, w, xp, xm, &err);
+         double dtg = gr_mindt(P, v.gr_ann[a].m, pc, w, xp, xm, &err);
          if( dtg == dtg ) dtc = dtg;
       }else{
          double vp = ((double)v.prim[UPP*N+c]-w)*r;

@@ -89,6 +89,82 @@ __device__ __forceinline__ void gr_flux(const GRParams &G, const Metric3 &g, con
    F[8] = prim[8]*F[DDD];
 }
 
+/* flux() and prim2cons(dV = 1) of the same state at the same point: the two
+ * reference functions compute the same intermediates (u^i, w, b^mu, b^2,
+ * ...) with the same expressions, so evaluating them once gives both results
+ * bit for bit */
+__device__ __forceinline__ void gr_flux_cons(const GRParams &G, const Metric3 &g, const double *prim,
+                                             const double *x, const double *n, double *F, double *Uc){
+   const double r = x[0];
+   const double al = g.al, jac = g.jac, sqrtgam = g.sqrtgam;
+   const double *be = g.be, *gam = g.gam, *igam = g.igam, *U = g.U;
+   const double rho = prim[RHO], Pp = prim[PPP];
+   const double l[3] = {prim[URR], prim[UPP], prim[UZZ]};
+   const double B[3] = {prim[BRR]/sqrtgam, prim[BPP]/(r*sqrtgam), prim[BZZ]/sqrtgam};
+   double igaml[3], u[3], v[3];
+#pragma unroll
+   for( int i=0 ; i<3 ; ++i ){
+      igaml[i] = 0.0;
+#pragma unroll
+      for( int j=0 ; j<3 ; ++j ) igaml[i] += igam[3*i+j]*l[j];
+   }
+   const double u2 = l[0]*igaml[0] + l[1]*igaml[1] + l[2]*igaml[2];
+   const double w = sqrt(1.0 + u2);
+   const double u0 = w/al;
+#pragma unroll
+   for( int i=0 ; i<3 ; ++i ) u[i] = igaml[i] - be[i]*u0;
+#pragma unroll
+   for( int i=0 ; i<3 ; ++i ) v[i] = u[i]/u0;
+   const double lt = -al*w + be[0]*l[0] + be[1]*l[1] + be[2]*l[2];
+   const double uU = U[0]*lt + U[1]*l[0] + U[2]*l[1] + U[3]*l[2];
+   const double uB = l[0]*B[0] + l[1]*B[1] + l[2]*B[2];
+   const double b0 = uB / al;
+   double bd[3];
+#pragma unroll
+   for( int k=0 ; k<3 ; ++k ) bd[k] = (gam[3*k]*B[0] + gam[3*k+1]*B[1] + gam[3*k+2]*B[2] + l[k]*uB) / w;
+   double B2 = 0.0, UB = 0.0;
+#pragma unroll
+   for( int i=0 ; i<3 ; ++i )
+#pragma unroll
+      for( int j=0 ; j<3 ; ++j ){
+         B2 += gam[3*i+j]*B[i]*B[j];
+         UB += gam[3*i+j] * B[i] * (U[0]*be[j] + U[j+1]);
+      }
+   const double b2 = (B2 + uB*uB) / (w*w);
+   const double Ub = (UB + uU*uB) / w;
+   const double gl = G.gam;
+   const double rhoh = rho + gl/(gl-1.0)*Pp + b2;
+   const double rhoe = Pp / (gl-1.0);
+   /* prim2cons, grmhd2.c:88-180 */
+   Uc[DDD] = jac * rho*u0 * 1.0;
+   Uc[SRR] = jac * (rhoh*u0*l[0] - b0*bd[0]) * 1.0;
+   Uc[LLL] = jac * (rhoh*u0*l[1] - b0*bd[1]) * 1.0;
+   Uc[SZZ] = jac * (rhoh*u0*l[2] - b0*bd[2]) * 1.0;
+   Uc[TAU] = jac * (-(rhoe+0.5*b2)*uU*u0 - (Pp+0.5*b2)*(uU*u0+U[0])
+                         - rho*(uU+1.0)*u0 + Ub*b0) * 1.0;
+   Uc[BRR] = sqrtgam * B[0]/r * 1.0;
+   Uc[BPP] = sqrtgam * B[1] * 1.0;
+   Uc[BZZ] = sqrtgam * B[2] * 1.0;
+   Uc[8] = prim[8]*Uc[DDD];
+   /* flux, grmhd2.c:272-335 */
+   const double un = u[0]*n[0] + u[1]*n[1] + u[2]*n[2];
+   const double Bn = B[0]*n[0] + B[1]*n[1] + B[2]*n[2];
+   const double Un = U[1]*n[0] + U[2]*n[1] + U[3]*n[2];
+   const double vn = v[0]*n[0] + v[1]*n[1] + v[2]*n[2];
+   const double hn = n[0] + r*n[1] + n[2];
+   const double bn = (Bn + uB*un)/w;
+   const double Pt = Pp + 0.5*b2;
+   F[DDD] = jac * hn * rho*un;
+   F[SRR] = jac * hn * (rhoh*un*l[0] + Pt*n[0] - bd[0]*bn);
+   F[LLL] = jac * hn * (rhoh*un*l[1] + Pt*n[1] - bd[1]*bn);
+   F[SZZ] = jac * hn * (rhoh*un*l[2] + Pt*n[2] - bd[2]*bn);
+   F[TAU] = jac * hn * (-(rhoe+0.5*b2)*uU*un - Pt*(uU*un+Un) - rho*(uU+1.0)*un + Ub*bn);
+   F[BRR] = sqrtgam * hn * (B[0]*vn - Bn*v[0])/r;
+   F[BPP] = sqrtgam * hn * (B[1]*vn - Bn*v[1]);
+   F[BZZ] = sqrtgam * hn * (B[2]*vn - Bn*v[2]);
+   F[8] = prim[8]*F[DDD];
+}
+
 /* ------------------------------------------------------------- HLL speeds */
 /* one side's fast speeds along n (grmhd2.c:551-612 for one of the two states) */
 __device__ __forceinline__ void gr_side_speeds(const GRParams &G, const Metric3 &g, double sqrtgam_v,
@@ -140,29 +216,24 @@ __device__ __forceinline__ void gr_hll_speeds(const GRParams &G, const Metric3 &
 
 /* ------------------------------------------------------------- HLL flux */
 /* G[q] = (F - w U*) dA dt of one face, solve_riemann with Riemann_Solver 0:
- * the upwind state's flux outside the fan, the HLL average inside. */
-__device__ __forceinline__ void gr_hll(const DiskParams &P, const double *primL, const double *primR,
-                                       const double *x, const double *n, double w, double dAdt,
-                                       double *Gq){
+ * the upwind state's flux outside the fan, the HLL average inside.  g is
+ * the metric at x (a per-annulus or per-track table: it depends on r, z). */
+__device__ __forceinline__ void gr_hll(const DiskParams &P, const Metric3 &g, const double *primL,
+                                       const double *primR, const double *x, const double *n,
+                                       double w, double dAdt, double *Gq){
    const GRParams G = gr_params(P);
-   Metric3 g;
-   metric_at(G, x, g);
    double Sl, Sr;
    gr_hll_speeds(G, g, primL, primR, n, x, &Sl, &Sr);
    double Flux[GR_Q], Ustr[GR_Q];
    if( w < Sl ){
-      gr_flux(G, g, primL, x, n, Flux);
-      gr_prim2cons(G, g, primL, Ustr, x);
+      gr_flux_cons(G, g, primL, x, n, Flux, Ustr);
    }else if( w > Sr ){
-      gr_flux(G, g, primR, x, n, Flux);
-      gr_prim2cons(G, g, primR, Ustr, x);
+      gr_flux_cons(G, g, primR, x, n, Flux, Ustr);
    }else{
       double Fl[GR_Q], Fr[GR_Q], Ul[GR_Q], Ur[GR_Q];
       const double aL = Sr, aR = -Sl;
-      gr_prim2cons(G, g, primL, Ul, x);
-      gr_prim2cons(G, g, primR, Ur, x);
-      gr_flux(G, g, primL, x, n, Fl);
-      gr_flux(G, g, primR, x, n, Fr);
+      gr_flux_cons(G, g, primL, x, n, Fl, Ul);
+      gr_flux_cons(G, g, primR, x, n, Fr, Ur);
 #pragma unroll
       for( int q=0 ; q<GR_Q ; ++q ){
          Flux[q] = ( aL*Fl[q] + aR*Fr[q] + aL*aR*( Ul[q] - Ur[q] ) )/( aL + aR );
@@ -271,52 +342,68 @@ __device__ __forceinline__ void kerr_der(const double *x, double M, double a, in
    for( int i=0 ; i<3 ; ++i ) dbe[i] = be[i].d;
 }
 
+/* ------------------------------------------------------------- tables */
+/* The metric depends on (r, z) only, so every place the step evaluates it
+ * is a fixed point of the grid: per annulus its centroid (phi faces,
+ * cons->prim, mesh Omega) and the midpoint of its corners (source, mindt,
+ * with the frame's and the 4-metric's derivatives there), per r- or z-track
+ * the face centre.  They are computed once per batch into these tables with
+ * the same functions, so the step reads bit-identical values. */
+struct GRAnn {
+   Metric3 c;            /* at (centroid r, centroid z) */
+   Metric3 m;            /* at (midpoint r, midpoint z) */
+   double dU[16];        /* frame_der_U at the midpoint */
+   double dgr[16], dgz[16];   /* d g_{mu nu}/dr, /dz at the midpoint */
+};
+
+__device__ __forceinline__ void gr_ann_table(const DiskParams &P, double rp, double rm, double zp,
+                                             double zm, GRAnn &T){
+   const GRParams G = gr_params(P);
+   const double xc[3] = {centroid_r(rp, rm), 0.0, centroid_z(zp, zm)};
+   metric_at(G, xc, T.c);
+   const double x[3] = {0.5*(rm+rp), 0.0, 0.5*(zm+zp)};
+   metric_at(G, x, T.m);
+   double da[4], db[12];
+   if( G.metric == GR_METRIC_KERR ){
+      double b1[3], b3[3];
+      kerr_der(x, G.M, G.a, 1, T.dgr, &da[1], b1);
+      kerr_der(x, G.M, G.a, 3, T.dgz, &da[3], b3);
+      da[0] = 0.0; da[2] = 0.0;
+      for( int j=0 ; j<3 ; ++j ){ db[j] = 0.0; db[3+j] = b1[j]; db[6+j] = 0.0; db[9+j] = b3[j]; }
+   }else{
+      schw_der_g(x, G.M, 1, T.dgr);
+      schw_der_g(x, G.M, 3, T.dgz);
+      schw_der_lapse(x, G.M, da);
+      schw_der_shift(x, G.M, db);
+   }
+   /* frame_der_U (Frame/normal.c:23-44): killing directions t and phi */
+   const double ia = 1.0/T.m.al;
+   for( int i=0 ; i<16 ; ++i ) T.dU[i] = 0.0;
+   for( int i=1 ; i<4 ; i+=2 ){
+      T.dU[4*i] = -ia*ia*da[i];
+      for( int j=0 ; j<3 ; ++j ) T.dU[4*i+j+1] = T.m.be[j]*ia*ia*da[i] - db[3*i+j]*ia;
+   }
+}
+
 /* ------------------------------------------------------------- source */
 /* source() of grmhd2.c:383-478 into cons (SRR, LLL, SZZ, TAU), at the
- * midpoint of the cell's corners xp, xm, with the normal frame's
- * derivative (Frame/normal.c:23-44). */
-__device__ __forceinline__ void gr_source(const DiskParams &P, const double *prim, double *cons,
-                                          const double *xp, const double *xm, double dVdt){
-   const GRParams G = gr_params(P);
-   const double x[3] = {0.5*(xm[0]+xp[0]), 0.5*(xm[1]+xp[1]), 0.5*(xm[2]+xp[2])};
-   Metric3 g;
-   metric_at(G, x, g);
-   const double r = x[0];
+ * midpoint of the cell's corners, from the annulus table. */
+__device__ __forceinline__ void gr_source(const DiskParams &P, const GRAnn &T, const double *prim,
+                                          double *cons, double r, double dVdt){
+   const Metric3 &g = T.m;
    const double al = g.al, jac = g.jac, sqrtgam = g.sqrtgam;
    const double *be = g.be, *gam = g.gam, *igam = g.igam, *U = g.U;
-   /* frame_der_U with the metric's derivatives: killing directions 0, 2 */
-   double dU[16];
-   double dgr[16], dgz[16];
-   {
-      double da[4], db[12];
-      if( G.metric == GR_METRIC_KERR ){
-         double b1[3], b3[3];
-         kerr_der(x, G.M, G.a, 1, dgr, &da[1], b1);
-         kerr_der(x, G.M, G.a, 3, dgz, &da[3], b3);
-         da[0] = 0.0; da[2] = 0.0;
-         for( int j=0 ; j<3 ; ++j ){ db[j] = 0.0; db[3+j] = b1[j]; db[6+j] = 0.0; db[9+j] = b3[j]; }
-      }else{
-         schw_der_g(x, G.M, 1, dgr);
-         schw_der_g(x, G.M, 3, dgz);
-         schw_der_lapse(x, G.M, da);
-         schw_der_shift(x, G.M, db);
-      }
-      const double ia = 1.0/al;
-      for( int i=0 ; i<16 ; ++i ) dU[i] = 0.0;
-      for( int i=1 ; i<4 ; i+=2 ){
-         dU[4*i] = -ia*ia*da[i];
-         for( int j=0 ; j<3 ; ++j ) dU[4*i+j+1] = be[j]*ia*ia*da[i] - db[3*i+j]*ia;
-      }
-   }
    const double rho = prim[RHO], Pp = prim[PPP];
    double l[4] = {0.0, prim[URR], prim[UPP], prim[UZZ]};
    const double B[3] = {prim[BRR]/sqrtgam, prim[BPP]/(r*sqrtgam), prim[BZZ]/sqrtgam};
    double ig[16];
    const double ia2 = 1.0/(al*al);
    ig[0] = -ia2;
+#pragma unroll
    for( int mu=0 ; mu<3 ; ++mu ){
       ig[mu+1] = be[mu]*ia2;
       ig[4*(mu+1)] = ig[mu+1];
+#pragma unroll
       for( int nu=0 ; nu<3 ; ++nu ) ig[4*(mu+1)+nu+1] = igam[3*mu+nu]-be[mu]*be[nu]*ia2;
    }
    double igaml[3];
@@ -327,6 +414,7 @@ __device__ __forceinline__ void gr_source(const DiskParams &P, const double *pri
    const double w = sqrt(1.0 + u2);
    double u[4];
    u[0] = w/al;
+#pragma unroll
    for( int i=0 ; i<3 ; ++i ) u[i+1] = igaml[i] - be[i]*u[0];
    l[0] = -al*w + be[0]*l[1] + be[1]*l[2] + be[2]*l[3];
    const double uB = l[1]*B[0] + l[2]*B[1] + l[3]*B[2];
@@ -339,29 +427,39 @@ __device__ __forceinline__ void gr_source(const DiskParams &P, const double *pri
    bd[2] = (gam[3]*B[0] + gam[4]*B[1] + gam[5]*B[2] + l[2]*uB) / w;
    bd[3] = (gam[6]*B[0] + gam[7]*B[1] + gam[8]*B[2] + l[3]*uB) / w;
    double B2 = 0.0, beB = 0.0;
-   for( int i=0 ; i<3 ; ++i ) for( int j=0 ; j<3 ; ++j ){
-      beB += gam[3*i+j]*be[i]*B[j];
-      B2 += gam[3*i+j]*B[i]*B[j];
-   }
+#pragma unroll
+   for( int i=0 ; i<3 ; ++i )
+#pragma unroll
+      for( int j=0 ; j<3 ; ++j ){
+         beB += gam[3*i+j]*be[i]*B[j];
+         B2 += gam[3*i+j]*B[i]*B[j];
+      }
    bd[0] = (beB + l[0]*uB) / w;
    const double b2 = (B2 + uB*uB) / (w*w);
-   const double gl = G.gam;
+   const double gl = P.gam;
    const double rhoh = rho + gl/(gl-1.0)*Pp + b2;
    const double Pt = Pp + 0.5*b2;
-   double Sk[3];
-   for( int i=0 ; i<3 ; ++i ){
-      Sk[i] = 0.0;
-      if( i == 1 ) continue;                      /* metric_killing(2): phi */
-      const double *dg = i == 0 ? dgr : dgz;
-      for( int mu=0 ; mu<4 ; ++mu ) for( int nu=0 ; nu<4 ; ++nu )
-         Sk[i] += (rhoh*u[mu]*u[nu] + ig[4*mu+nu]*Pt - b[mu]*b[nu]) * dg[4*mu+nu];
-      Sk[i] *= 0.5;
-   }
+   double Sk[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+   for( int mu=0 ; mu<4 ; ++mu )
+#pragma unroll
+      for( int nu=0 ; nu<4 ; ++nu )
+         Sk[0] += (rhoh*u[mu]*u[nu] + ig[4*mu+nu]*Pt - b[mu]*b[nu]) * T.dgr[4*mu+nu];
+   Sk[0] *= 0.5;                                   /* Sk[1]: phi is a killing direction */
+#pragma unroll
+   for( int mu=0 ; mu<4 ; ++mu )
+#pragma unroll
+      for( int nu=0 ; nu<4 ; ++nu )
+         Sk[2] += (rhoh*u[mu]*u[nu] + ig[4*mu+nu]*Pt - b[mu]*b[nu]) * T.dgz[4*mu+nu];
+   Sk[2] *= 0.5;
    double S0 = -U[1]*Sk[0] - U[2]*Sk[1] - U[3]*Sk[2];
-   for( int mu=0 ; mu<4 ; ++mu ) for( int nu=0 ; nu<4 ; ++nu ){
-      if( mu == nu ) S0 += -(rhoh*u[mu]*l[nu] + Pt - b[mu]*bd[nu]) * dU[4*mu+nu];
-      else           S0 += -(rhoh*u[mu]*l[nu] - b[mu]*bd[nu]) * dU[4*mu+nu];
-   }
+#pragma unroll
+   for( int mu=0 ; mu<4 ; ++mu )
+#pragma unroll
+      for( int nu=0 ; nu<4 ; ++nu ){
+         if( mu == nu ) S0 += -(rhoh*u[mu]*l[nu] + Pt - b[mu]*bd[nu]) * T.dU[4*mu+nu];
+         else           S0 += -(rhoh*u[mu]*l[nu] - b[mu]*bd[nu]) * T.dU[4*mu+nu];
+      }
    cons[SRR] += jac * Sk[0] * dVdt;
    cons[LLL] += jac * Sk[1] * dVdt;
    cons[SZZ] += jac * Sk[2] * dVdt;
@@ -369,25 +467,31 @@ __device__ __forceinline__ void gr_source(const DiskParams &P, const double *pri
 }
 
 /* ------------------------------------------------------------- mesh Omega */
-__device__ __forceinline__ double gr_omega(const DiskParams &P, const double *prim, const double *x){
-   const GRParams G = gr_params(P);
-   Metric3 g;
-   metric_at(G, x, g);
+__device__ __forceinline__ double gr_omega(const Metric3 &g, const double *prim){
    const double l[3] = {prim[URR], prim[UPP], prim[UZZ]};
    double u2 = 0.0;
-   for( int i=0 ; i<3 ; ++i ) for( int j=0 ; j<3 ; ++j ) u2 += g.igam[3*i+j]*l[i]*l[j];
+#pragma unroll
+   for( int i=0 ; i<3 ; ++i )
+#pragma unroll
+      for( int j=0 ; j<3 ; ++j ) u2 += g.igam[3*i+j]*l[i]*l[j];
    const double w = sqrt(1.0 + u2);
    return g.al*(g.igam[3]*l[0]+g.igam[4]*l[1]+g.igam[5]*l[2])/w - g.be[1];
 }
+/* the same with the metric evaluated at x (set-up kernels) */
+__device__ __forceinline__ double gr_omega_at(const DiskParams &P, const double *prim, const double *x){
+   const GRParams G = gr_params(P);
+   Metric3 g;
+   metric_at(G, x, g);
+   return gr_omega(g, prim);
+}
 
 /* ------------------------------------------------------------- mindt */
-__device__ __forceinline__ double gr_mindt(const DiskParams &P, const double *prim, double wc,
-                                           const double *xp, const double *xm, int *err){
+/* g: the metric at the midpoint of the corners (GRAnn::m) */
+__device__ __forceinline__ double gr_mindt(const DiskParams &P, const Metric3 &g, const double *prim,
+                                           double wc, const double *xp, const double *xm, int *err){
    const GRParams G = gr_params(P);
    const double x[3] = {0.5*(xm[0]+xp[0]), 0.5*(xm[1]+xp[1]), 0.5*(xm[2]+xp[2])};
    const double r = x[0];
-   Metric3 g;
-   metric_at(G, x, g);
    const double al = g.al, *be = g.be, *gam = g.gam, *igam = g.igam;
    const double sqrtgam = gr_jacobian(x) / (r*al);
    const double gl = G.gam;
@@ -438,11 +542,9 @@ __device__ __forceinline__ double gr_mindt(const DiskParams &P, const double *pr
  * warm-started from the cell's current prim (grmhd2.c:1167-1175), then the
  * recovery.  prim is read as the guess and overwritten; returns the
  * Newton iterations. */
-__device__ __forceinline__ int gr_cons2prim(const DiskParams &P, const double *cons, double *prim,
-                                            const double *x, double dV){
+__device__ __forceinline__ int gr_cons2prim(const DiskParams &P, const Metric3 &g, const double *cons,
+                                            double *prim, const double *x, double dV){
    const GRParams G = gr_params(P);
-   Metric3 g;
-   metric_at(G, x, g);
    double c1[GR_Q];
 #pragma unroll
    for( int q=0 ; q<GR_Q ; ++q ) c1[q] = cons[q]/dV;
