@@ -81,9 +81,16 @@ namespace disco {
 #ifndef MB_C2P
 #define MB_C2P MB_STEP
 #endif
-/* the grmhd2 (GR) instantiations of the step kernels */
+/* the grmhd2 (GR) instantiations of the step kernels: resident blocks per
+ * SM measured on the config-3 torus (192 x 16 x 462 slice, Kerr a = 0.9)
+ * for 2-6 blocks: 5 for the flux kernels and k_update (2-4 spill less but
+ * hide less latency: 8.4-10.1 ms per step at 2-3 against 7.4 at 5), 6 for
+ * k_begin and k_c2p */
 #ifndef MB_GR
-#define MB_GR MB_MHD
+#define MB_GR 5
+#endif
+#ifndef MB_GR_LIGHT
+#define MB_GR_LIGHT 6
 #endif
 
 template<class R>
@@ -283,7 +290,7 @@ __device__ __forceinline__ void begin_body(const ViewT<R> &v, double RK, int fir
    }
 }
 template<int Q, int NC, class R, bool GR = false>
-__global__ void __launch_bounds__(CB, GR ? MB_GR : (Q > 6 ? MB_MHD : MB_BEGIN)) k_begin(ViewT<R> v, double RK, int first){
+__global__ void __launch_bounds__(CB, GR ? MB_GR_LIGHT : (Q > 6 ? MB_MHD : MB_BEGIN)) k_begin(ViewT<R> v, double RK, int first){
    begin_body<Q,NC,R,GR>(v, RK, first, blockIdx.x);
 }
 
@@ -1477,7 +1484,7 @@ __device__ __forceinline__ void c2p_body(const ViewT<R> &v, int last, int bc, in
                                 bc, diag, err, topo_set, bid);
 }
 template<int Q, int NC, class R, int NQD = 5, bool VISC = false, bool GR = false>
-__global__ void __launch_bounds__(CB, GR ? MB_GR : (Q > 6 ? MB_MHD : MB_C2P)) k_c2p(ViewT<R> v, int last, int bc, int diag){
+__global__ void __launch_bounds__(CB, GR ? MB_GR_LIGHT : (Q > 6 ? MB_MHD : MB_C2P)) k_c2p(ViewT<R> v, int last, int bc, int diag){
    c2p_body<Q,NC,R,NQD,VISC,GR>(v, last, bc, diag, v.move_c2p, v.topo_set, blockIdx.x);
 }
 
