@@ -102,6 +102,7 @@ static void fill_disk_params(DiskParams &D, const disco_params &p, const disco_m
    D.ic_gr.M = p.metricPar[2]; D.ic_gr.a = D.gr_a;
    D.ic_gr.rmin = p.rmin; D.ic_gr.rmax = p.rmax; D.ic_gr.zmin = p.zmin; D.ic_gr.zmax = p.zmax;
    D.ic_gr.phimax = p.phimax;
+   D.bc_horizon = m.boundary == DISCO_BC_HORIZON ? 8 : m.boundary == DISCO_BC_HORIZON3D ? 9 : 0;
    D.ic_mhd.seed = (uint64_t)(int64_t)p.initPar0; D.ic_mhd.amp = p.initPar[1];
    D.ic_mhd.cs = p.initPar[3]; D.ic_mhd.beta = p.initPar[4]; D.ic_mhd.gam = p.Adiabatic_Index;
    D.ic_mhd.rmin = p.rmin; D.ic_mhd.rmax = p.rmax; D.ic_mhd.zmin = p.zmin; D.ic_mhd.zmax = p.zmax;
@@ -357,8 +358,13 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
             return DISCO_ERR_UNSUPPORTED;
       }
    }
-   if( mods->boundary < DISCO_BC_FIXED || mods->boundary > DISCO_BC_ACCRETE3D )
+   if( mods->boundary < DISCO_BC_FIXED || mods->boundary > DISCO_BC_HORIZON3D )
       return DISCO_ERR_UNSUPPORTED;
+   /* polar3d, horizon and horizon3d set the outer r and the z ghosts only
+    * (Boundary/polar3d.c, horizon.c, horizon3d.c): grids without inner ghosts */
+   if( mods->boundary == DISCO_BC_POLAR3D || mods->boundary == DISCO_BC_HORIZON ||
+       mods->boundary == DISCO_BC_HORIZON3D )
+      for( int d=0 ; d<ndisk ; ++d ) if( Ng[4*d+0] != 0 ) return DISCO_ERR_UNSUPPORTED;
    /* Boundary/polar.c sets the outer r and the z ghosts only: it is meant
     * for a grid whose inner edge is the axis (NoBC_Rmin 1, no inner ghosts);
     * with inner ghosts their prims would never be set */
@@ -389,8 +395,12 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->device = device; b->mods = *mods; b->prec = precision; b->ndisk = ndisk;
    b->NC = mods->num_c; b->Q = mods->num_c + mods->num_n;
    b->timestep_mode = params[0].Timestep == 1 ? 1 : 0;
+   /* the fixed ghost sets of fixed_ghost_init: polar3d is accrete3d's fixed
+    * set (boundary_fixed_rout / _zbot / _ztop) without its inner copy */
    b->bc_fixed = mods->boundary == DISCO_BC_FIXED ? 1 : mods->boundary == DISCO_BC_FIXED3D ? 2 :
-                 mods->boundary == DISCO_BC_POLAR ? 3 : mods->boundary == DISCO_BC_ACCRETE3D ? 6 : 0;
+                 mods->boundary == DISCO_BC_POLAR ? 3 :
+                 (mods->boundary == DISCO_BC_ACCRETE3D || mods->boundary == DISCO_BC_POLAR3D) ? 6 :
+                 mods->boundary == DISCO_BC_HORIZON ? 8 : mods->boundary == DISCO_BC_HORIZON3D ? 9 : 0;
    /* modules built from boundary_functions.c's zero-gradient copies: all four
     * sides (zerograd; with the diode outflow3d, zerograd_omk), or the inner r
     * side only (accrete3d, whose other sides are fixed) */

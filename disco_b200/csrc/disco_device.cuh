@@ -79,6 +79,8 @@ struct DiskParams {
     * Kerr-Schild kerr_ks_rpz) and its Metric_Par2 (M) / Metric_Par3 (a) */
    int gr, gr_metric;
    double gr_M, gr_a;
+   int bc_horizon;    /* 8 (Boundary/horizon.c) or 9 (horizon3d) when cells are excised, else 0 */
+   int pad_hz;
 };
 
 /* Per-disk mutable state (device resident across steps). */

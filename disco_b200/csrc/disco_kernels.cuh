@@ -1271,13 +1271,62 @@ __global__ void __launch_bounds__(CB) k_diag_part(ViewT<R> v){
  *         zero-gradient, k_zerograd)
  * then subtract_omega (rotframe.c:15-17);
  *   bc 3  Boundary/polar.c: outer r ghosts and z ghosts at the centroid,
- *         without subtract_omega.  Returns whether prim was set. */
+ *         without subtract_omega;
+ *   bc 8  Boundary/horizon.c:26-67: outer r ghosts and z ghosts at (midpoint r,
+ *         piph - dphi/2, midpoint z), without subtract_omega;
+ *   bc 9  Boundary/horizon3d.c: outer r ghosts and z ghosts as bc 6
+ *         (Boundary/polar3d.c is bc 6 on a grid without inner ghosts);
+ * plus, for bc 8 and 9, every annulus inside the excised region
+ * (horizon_cut) re-initialised as the module does it.  Returns whether
+ * prim was set. */
+/* Whether annulus (j, k) lies in a horizon module's excised region: the
+ * cells Boundary/horizon.c:70-109 re-initialises and marks not real inside
+ * 0.7 * 2M (M = 1 there), or boundary_fixed_horizon's R < R_HOR = 1
+ * (boundary_functions.c:622-656, horizon3d).  rj, zk are the disk's edge
+ * arrays (index -1 valid). */
+__device__ __forceinline__ bool horizon_cut(const DiskParams &P, int bc, int j, int k,
+                                            const double *rj, const double *zk){
+   if( bc == 8 ){
+      const double rh = 2*1.0, cut = 0.7*rh;
+      if( !(rj[-1] < cut && zk[-1] < cut && zk[P.Nz-1] > -cut) ) return false;
+      double zp = zk[k], zm = zk[k-1];
+      double zc = fabs(zp) < fabs(zm) ? zp : zm;
+      if( fabs(zc) > cut && P.Nz > 1 ) return false;
+      /* the reference walks j outwards and stops at the first annulus
+       * outside; the test is monotone in j, so it is this annulus's own */
+      double rp = rj[j], rm = rj[j-1];
+      double rc = fabs(rp) < fabs(rm) ? rp : rm;
+      return !((rc*rc+zc*zc > cut*cut && P.Nz > 1) || rc > cut);
+   }
+   if( bc == 9 ){
+      const double R_HOR = 1.0;
+      double zm = zk[k-1], zp = zk[k];
+      double zo = fabs(zp) > fabs(zm) ? zp : zm;
+      if( fabs(zo) > R_HOR ) return false;
+      double ro = rj[j];
+      double R = sqrt(zo*zo + ro*ro);
+      return R < R_HOR;
+   }
+   return false;
+}
 template<int Q, int NC>
 __device__ __forceinline__ bool fixed_ghost_init(const DiskParams &P, int bc, int j, int k,
                                                  const double *rj, const double *zk,
                                                  double piph, double dphi, double *prim){
    bool rghost = j < P.NgRa || j >= P.Nr - P.NgRb;
    bool zghost = k < P.NgZa || k >= P.Nz - P.NgZb;
+   if( bc == 8 && (j >= P.Nr - P.NgRb || zghost || horizon_cut(P, bc, j, k, rj, zk)) ){
+      double x[3] = { .5*(rj[j]+rj[j-1]), piph - .5*dphi, .5*(zk[k]+zk[k-1]) };
+      initial<Q,NC>(P, prim, x);
+      return true;
+   }
+   if( bc == 9 && (j >= P.Nr - P.NgRb || zghost || horizon_cut(P, bc, j, k, rj, zk)) ){
+      /* set_cell_init (boundary_functions.c:21-31) */
+      double x[3] = { centroid_r(rj[j], rj[j-1]), 0.5*(piph + (piph - dphi)), 0.5*(zk[k]+zk[k-1]) };
+      initial<Q,NC>(P, prim, x);
+      if( P.rotframe ) prim[UPP] -= P.RotOmega;
+      return true;
+   }
    if( bc == 1 && rghost ){
       double x[3] = { .5*(rj[j]+rj[j-1]), piph - .5*dphi, .5*(zk[k]+zk[k-1]) };
       initial<Q,NC>(P, prim, x);
@@ -1335,6 +1384,7 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
 #pragma unroll
    for( int m=0 ; m<=NQD ; ++m ) dq[m] = 0.0;
    double rp = rj[j], rm = rj[j-1], zp = zk[k], zm = zk[k-1];
+   bool excised = false;
    if( active ){
       double phim = piph - dphi;
       if( real ){
@@ -1347,6 +1397,12 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
             gr_cons2prim(P, v.gr_ann[a].c, cons, prim, x, dV2);
          }else{
             cons2prim<Q,NC>(P, cons, prim, centroid_r(rp, rm), v.ann_om[a], dV2);
+         }
+         /* a horizon module then re-initialises the excised annuli (after
+          * calc_prim, as boundary_trans follows it) and getmindt skips them */
+         if( (bc == 8 || bc == 9) && horizon_cut(P, bc, j, k, rj, zk) ){
+            fixed_ghost_init<Q,NC>(P, bc, j, k, rj, zk, piph, dphi, prim);
+            excised = true;
          }
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ){
@@ -1368,13 +1424,13 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
          }
       }
       if( last ){
-         if( real && GR ){                        /* mindt, grmhd2.c:748-832 */
+         if( real && !excised && GR ){            /* mindt, grmhd2.c:748-832 */
             int cprev = c0 + (i == 0 ? np-1 : i-1);
             double w = .5*(v.wiph[cprev] + v.wiph[c]);
             double xp[3] = {rp, piph, zp}, xm[3] = {rm, phim, zm};
             double dtm = gr_mindt(P, v.gr_ann[a].m, prim, w, xp, xm, &err);
             if( dtm == dtm ) dtc = dtm;
-         }else if( real ){                        /* mindt, euler.c:332-380, mhd.c:452-486 */
+         }else if( real && !excised ){            /* mindt, euler.c:332-380, mhd.c:452-486 */
             int cprev = c0 + (i == 0 ? np-1 : i-1);
             double w = .5*(v.wiph[cprev] + v.wiph[c]);
             double r = centroid_r(rp, rm);
@@ -1947,6 +2003,10 @@ __global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc){
          /* with CT, cons2prim follows set_B_fields (domain.c:211-237): k_c2p */
          if( !v.ct ) cons2prim<Q,NC>(P, cons, prim, r, om, dV);
       }
+      /* main.c's boundary pass: a horizon module re-initialises the
+       * excised annuli's prims (their cons stay set-up's) */
+      if( P.bc_horizon && horizon_cut(P, P.bc_horizon, j, k, rj, zk) )
+         fixed_ghost_init<Q,NC>(P, bc, j, k, rj, zk, piph, dphi, prim);
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){ v.prim[q*N+c] = (R)prim[q]; v.cons[q*N+c] = cons[q]; }
    }else{
@@ -2029,6 +2089,8 @@ __global__ void __launch_bounds__(CB) k_restart(ViewT<R> v, int bc){
          prim2cons<Q,NC,double>(P, prim, cons, r, om, dV);
          cons2prim<Q,NC>(P, cons, prim, r, om, dV);
       }
+      if( P.bc_horizon && horizon_cut(P, P.bc_horizon, j, k, rj, zk) )
+         fixed_ghost_init<Q,NC>(P, bc, j, k, rj, zk, piph, dphi, prim);
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){ v.prim[q*N+c] = (R)prim[q]; v.cons[q*N+c] = cons[q]; }
    }else{
@@ -2131,7 +2193,9 @@ __global__ void __launch_bounds__(CB) k_mindt(ViewT<R> v){
    bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
    double dtc = 1.0e300;
    int err = 0;
-   if( i < np && real ){
+   bool excised = P.bc_horizon &&
+                  horizon_cut(P, P.bc_horizon, j, k, v.rj + P.rj0 + 1, v.zk + P.zk0 + 1);
+   if( i < np && real && !excised ){
       int c = c0 + i;
       const double *rj = v.rj + P.rj0 + 1;
       const double *zk = v.zk + P.zk0 + 1;

@@ -153,6 +153,9 @@ int disco_read_opt(const char *path, disco_modules *m){
    else if( !strcmp(v, "outflow3d") ) m->boundary = DISCO_BC_OUTFLOW3D;
    else if( !strcmp(v, "zerograd_omk") ) m->boundary = DISCO_BC_ZEROGRAD_OMK;
    else if( !strcmp(v, "accrete3d") ) m->boundary = DISCO_BC_ACCRETE3D;
+   else if( !strcmp(v, "polar3d") ) m->boundary = DISCO_BC_POLAR3D;
+   else if( !strcmp(v, "horizon") ) m->boundary = DISCO_BC_HORIZON;
+   else if( !strcmp(v, "horizon3d") ) m->boundary = DISCO_BC_HORIZON3D;
    else return DISCO_ERR_UNSUPPORTED;
    if( opt_value(path, "PLANETS", v, sizeof v) ) return DISCO_ERR_ARG;
    if( !strcmp(v, "none") ) m->planets = DISCO_PLANETS_NONE;

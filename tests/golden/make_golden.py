@@ -154,6 +154,21 @@ CASES = {
     "c3_grtorus": ("c3_grtorus", {"Num_R": 16, "Num_Z": 8}, 5),
     "c3_grtorus_mm0": ("c3_grtorus", {"Num_R": 12, "Num_Z": 6, "Mesh_Motion": 0,
                                       "Init_Par0": 2718}, 4),
+    # the excising boundary modules: horizon3d (boundary_fixed_horizon, the
+    # annuli inside R < 1 re-initialised by set_cell_init every substep and
+    # left out of the dt minimum) on a 3D hydro grid down to the axis, and
+    # horizon (Boundary/horizon.c: inside 0.7 r_H of M = 1, midpoint
+    # re-initialisation) under the GRMHD torus with its inner edge at
+    # r = 0.5 and no inner ghosts; polar3d (outer r and z ghosts from
+    # set_cell_init, no inner ghosts) with 3D CT
+    "c0_horizon3d": ("c0_horizon3d", {"Num_R": 10, "Num_Z": 6, "Z_Min": -0.6, "Z_Max": 0.6,
+                                      "R_Min": 0.0, "R_Max": 2.0, "NoBC_Rmin": 1,
+                                      "Log_Zoning": 0, "Init_Par2": 1, "Init_Par1": 0.05,
+                                      "Energy_Omega": 0, "Mach_Number": 5.0}, 5),
+    "c1_polar3dbc": ("c1_polar3dbc", {"Num_R": 8, "Num_Z": 6, "R_Min": 0.0, "R_Max": 2.0,
+                                      "NoBC_Rmin": 1, "Init_Par2": 1, "Init_Par4": 10.0,
+                                      "Constrained_Transport": 1, "Init_Par5": 20.0}, 5),
+    "c3_grhorizon": ("c3_grhorizon", {"Num_R": 16, "Num_Z": 8, "R_Min": 0.5, "NoBC_Rmin": 1}, 5),
 }
 
 # the in.par template each module configuration starts from
@@ -163,7 +178,8 @@ BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": 
             "c1_polar": "c1_mhd2d", "c1_polar3d": "c1_mhd3d", "c0_outflow3d": "c0_kepler2d",
             "c1_omk3d": "c1_mhd3d", "c1_accrete3d": "c1_mhd3d", "c0_rigid_zg": "c0_kepler2d",
             "c0_circular": "c0_kepler2d", "c0_cm": "c0_kepler2d", "c0_diag_euler": "c0_kepler2d",
-            "c0_diag_euler3d": "c0_kepler2d", "c1_diag_mhdmri": "c1_mhd2d", "c3_grtorus": "c3_grtorus", "c4_binary3d": "c4_binary3d"}
+            "c0_diag_euler3d": "c0_kepler2d", "c1_diag_mhdmri": "c1_mhd2d", "c3_grtorus": "c3_grtorus", "c4_binary3d": "c4_binary3d",
+            "c0_horizon3d": "c0_kepler2d", "c1_polar3dbc": "c1_mhd3d", "c3_grhorizon": "c3_grtorus"}
 
 
 def par_text(cfg_par, overrides):

@@ -15,6 +15,12 @@ fixtures depend on no libm call except where noted):
   (boundary_fixed_q_rinn / _rout), 3D MHD.
 - accrete3d: outflow inner r, fixed outer r and z (set_cell_init), 3D MHD
   with CT.
+- polar3d: fixed outer r and z (set_cell_init) on an axis grid, 3D MHD with
+  CT.
+- horizon3d: polar3d's ghosts plus boundary_fixed_horizon
+  (boundary_functions.c:622-656): every annulus whose outer corner lies
+  inside R = 1 is re-initialised by set_cell_init each substep and left out
+  of the dt minimum, 3D hydro on an axis grid.
 
 State compared at 1e-12 relative L1 (in practice far below), face lists bit
 for bit, ghost cells included at set-up."""
@@ -28,7 +34,7 @@ from helpers import case_disk, observed_slots, par_with, rel_l1, rel_l1_cols
 
 pytestmark = pytest.mark.gpu
 
-POLAR = ["c0_polar", "c1_polar_ct", "c1_polar3d"]
+POLAR = ["c0_polar", "c1_polar_ct", "c1_polar3d", "c1_polar3dbc", "c0_horizon3d"]
 CASES = POLAR + ["c0_outflow3d", "c1_omk3d", "c1_accrete3d"]
 TOL = 1e-12
 
@@ -95,6 +101,34 @@ def test_polar_needs_the_axis():
     with pytest.raises(db.DiscoError) as e:
         db.Batch([disk])
     assert e.value.status == 3
+
+
+@pytest.mark.parametrize("module", ["polar3d", "horizon3d"])
+def test_axis_modules_need_no_inner_ghosts(module):
+    """polar3d and horizon3d set no inner r ghosts (Boundary/polar3d.c,
+    horizon3d.c): refused on a grid that has them."""
+    p = par_with({"Num_R": 12, "Num_Z": 4}, base="c1_mhd3d")
+    cfg = {"polar3d": "c1_polar3dbc", "horizon3d": "c0_horizon3d"}[module]
+    disk = db.Disk.from_files(p, os.path.join(db.TEMPLATES, cfg + ".in"))
+    os.unlink(p)
+    assert disk.modules.boundary == db.BOUNDARY[module]
+    with pytest.raises(db.DiscoError) as e:
+        db.Batch([disk])
+    assert e.value.status == 3
+
+
+def test_horizon3d_excises():
+    """The fixture's excised annuli (the reference marks them not real) are
+    inside R = 1, and after the steps their prims are the set_cell_init values
+    the device left there too."""
+    disk, g = case_disk("c0_horizon3d")
+    geo = disk.real == 1
+    ex = geo & (g["real"] == 0)
+    assert ex.sum() > 0 and (g["real"][~geo] == 0).all()
+    b = db.Batch([disk])
+    st = b.get_cells()
+    assert max(rel_l1_cols(st["prim"][ex], g["s0_prim"][ex])) <= TOL
+    b.close()
 
 
 def test_host_initial_module():

@@ -6,7 +6,11 @@ Every operation of the step with this module set is +, -, *, / or sqrt, all
 correctly rounded on both sides, and the device keeps the reference's
 operation order (--fmad=false), so the set-up, the dt sequence, every field
 after N steps and the face lists are compared bit for bit: the torus with
-the by-cell mesh (get_omega of grmhd2 moves the cells) and on a fixed mesh."""
+the by-cell mesh (get_omega of grmhd2 moves the cells) and on a fixed mesh,
+and with the horizon boundary (Boundary/horizon.c): no inner ghosts at
+r = 0.5, every annulus inside 0.7 r_H re-initialised at its midpoint each
+substep and left out of the dt minimum.  The comparison covers every cell the
+grid calls real, the excised ones included."""
 import numpy as np
 import pytest
 
@@ -15,11 +19,14 @@ from helpers import case_disk
 
 pytestmark = pytest.mark.gpu
 
-GR_CASES = ["c3_grtorus", "c3_grtorus_mm0"]
+GR_CASES = ["c3_grtorus", "c3_grtorus_mm0", "c3_grhorizon"]
 
 
-def _real(g):
-    return g["real"] == 1
+def _real(disk, g):
+    """The grid's real cells; the reference's flag also drops the excised ones."""
+    r = disk.real == 1
+    assert (g["real"][~r] == 0).all()
+    return r
 
 
 @pytest.mark.parametrize("case", GR_CASES)
@@ -28,11 +35,15 @@ def test_grmhd_setup_matches_reference(case):
     assert disk.modules.hydro == db.HYDRO["grmhd2"]
     b = db.Batch([disk])
     st = b.get_cells()
-    r = _real(g)
+    r = _real(disk, g)
     assert np.array_equal(st["prim"][r], g["s0_prim"][r])
     assert np.array_equal(st["cons"][r], g["s0_cons"][r])
     assert np.array_equal(st["wiph"][r], g["s0_wiph"][r])
     assert np.array_equal(st["piph"], g["s0_piph"])
+    if case == "c3_grhorizon":
+        ex = r & (g["real"] == 0)
+        assert ex.sum() > 0
+        assert np.array_equal(st["prim"], g["s0_prim"])
     b.close()
 
 
@@ -49,7 +60,7 @@ def test_grmhd_steps_bitexact(case):
     b.sync()
     assert np.array_equal(np.array(dts), g["dt"]), (np.array(dts) - g["dt"])
     st = b.get_cells()
-    r = _real(g)
+    r = _real(disk, g)
     for k in ("prim", "cons"):
         assert np.array_equal(st[k][r], g["sN_" + k][r]), k
     assert np.array_equal(st["piph"], g["sN_piph"])

@@ -55,6 +55,21 @@ def test_grid_and_phi_match_reference(case):
     assert np.array_equal(disk.real, g["real"])
 
 
+@pytest.mark.parametrize("case,module", [("c0_horizon3d", "horizon3d"), ("c1_polar3dbc", "polar3d"),
+                                         ("c3_grhorizon", "horizon")])
+def test_axis_and_horizon_modules_parse(case, module):
+    """The excising boundary modules read from Makefile_opt.in; the grid
+    matches the reference, whose real flag also drops the excised annuli."""
+    disk, g = case_disk(case)
+    assert disk.modules.boundary == db.BOUNDARY[module]
+    assert disk.Ng[0] == 0
+    assert np.array_equal(disk.Np, g["Np"]) and np.array_equal(disk.r_jph, g["r_jph"])
+    r = disk.real == 1
+    assert (g["real"][~r] == 0).all()
+    excised = r & (g["real"] == 0)
+    assert excised.any() == module.startswith("horizon")
+
+
 def test_np_floor_minimum_four():
     path = par_with({"Num_R": 4, "aspect": 100.0})
     disk = db.Disk(db.read_par(path), db.read_opt(db.template_paths("c0_kepler2d")[1]))
