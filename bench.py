@@ -2,19 +2,28 @@
 """Benchmark of the B200 Disco RK timestep (zone-updates/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ragged64|config0]
+                    [--workload config4|ragged64|ragged8|config0]
 
 A step is one full RK2 timestep (two substeps, fused getmindt) of every disk
-of the workload, inputs resident in HBM.  Default workload `ragged64`: 64
-ragged 2D hydro disks (~5.7M cells, the config-2 batch, FP64 plain path).
-Multi-GPU: one process per GPU (torchrun), each GPU advances its own 64
-disks (same sizes, own noise seeds): the disks are independent, so there is
-no data-path collective ("scaling": "weak"); only a barrier and a max of the
-timings over ranks.
+of the workload, inputs resident in HBM.  Default workload `config4`, the
+largest single-GPU configuration: the 3D MHD circumbinary disk (HLLD,
+constrained transport, softened equal-mass binary, zerograd; 384 x 128
+annuli, Np up to 1536, 39.5M real cells) in its stated form -- FP32 bulk
+(prims, slopes, fluxes, edge fields) with FP64 cell positions, mesh motion,
+dt and a Kahan-compensated FP64 conserved update -- with the FP64 plain path
+on the same set-up beside it (throughput, roofline, L1 error and drifts of
+the FP32 form against it).  The other configurations run as side legs:
+config 1 (3D MHD shearing disk), config 2 (`ragged64`, 64 ragged 2D hydro
+disks in one batch), config 3 (GRMHD torus) and the cons->prim leg.
+Multi-GPU: one process per GPU (torchrun), each GPU advances its own copy of
+the workload (independent disks, no data-path collective, "scaling":
+"weak"); only a barrier and a max of the timings over ranks.
 
 --impl reference times the reference Disco serial CPU code itself
-(oracle/_ref, built from the reference's own sources) on the same disks, one
-process per disk spread over all host cores.
+(oracle/_ref, built from the reference's own sources) on the same module
+set, spread over all host cores: for config4 one process per core, each on
+the full r grid and Np of the workload on a 4-layer z slab; for the ragged
+workloads one process per disk.
 """
 import argparse
 import json
@@ -32,6 +41,9 @@ sys.path.insert(0, os.path.join(REPO, "oracle"))
 METRIC = "zone-updates/s"
 Q = 6                                   # NUM_C 5 + NUM_N 1 (hydro)
 B_ALG_STEP = 576                        # HBM bytes per zone-update, FP64 hydro (10Q+12 words)
+B_ALG_MHD_CT = {"fp64": 1056, "mixed": 1200}   # HBM bytes per zone-update, MHD Q=9 with CT (5 faces)
+C4_NZ = 128
+C4_REAL_PER_LAYER = 308974              # real cells of one z layer of config 4 (Np depends on r only)
 
 
 def peaks():
@@ -83,6 +95,45 @@ def kernel_bytes(name, first, N, Nf, Na, nreal=0):
         # indices and the r-face fluxes; writes cons (+ piph_new -> piph,
         # dphi in the first substep)
         return N * w * (4 * Q + (6 if first else 3)) + N * 8 + Nf * w * Q
+    return 0
+
+
+def kernel_bytes_mhd(name, first, N, Nfr, Nfz, mixed):
+    """Algorithmic HBM bytes of one launch of a step kernel on a 3D MHD grid
+    with constrained transport (Q = 9, 5 face-flux slots per cell): every
+    array element the kernel must read or write, once.  N cells (ghosts
+    included), Nfr / Nfz r- and z-faces.  In the mixed form the prims, slopes
+    and fluxes are FP32 and the conserved update carries an FP32 Kahan term;
+    cons, RKcons, piph, dphi, wiph and the face fluxes Phi stay FP64."""
+    q, w = 9, 8
+    wr = 4 if mixed else 8
+    ck = 4 if mixed else 0               # Kahan carry per conserved variable
+    phi = 5 * w
+    if name == "k_update":
+        # cons (+carry) read and written, prim and gradp, piph / dphi / wiph,
+        # the four consume indices, the phi-face EMFs written (4); the r- and
+        # z-face fluxes read
+        return N * (2 * q * (w + ck) + 2 * q * wr + 3 * w + 16 + 4 * wr) + (Nfr + Nfz) * q * wr
+    if name in ("k_flux_r", "k_flux_z"):
+        nf = Nfr if name == "k_flux_r" else Nfz
+        # per face: its two cells, its geometry, the flux and the two edge
+        # terms written; per cell once: prim, the slope in this direction, gradp
+        return nf * (8 + 3 * w + q * wr + 2 * wr) + N * (3 * q * wr + 2 * w)
+    if name == "k_c2p":
+        # cons (+carry), piph / dphi (moved in the first substep), the face
+        # fluxes rebuilt into the cell field, the prims written (+wiph last)
+        return N * (q * (w + ck) + 2 * w + phi + 3 * w + q * wr) + (0 if first else N * w)
+    if name == "k_begin":
+        rk = q * w if first else q * (w + 2 * ck)
+        return N * (2 * q * wr + 2 * q * w + rk + 2 * w + (2 * w if first else 0) + 3 * phi)
+    if name in ("k_gradr", "k_gradz"):
+        nf = Nfr if name == "k_gradr" else Nfz
+        return nf * (q * wr + w) + N * (q * wr + 2 * w + 8)
+    if name == "k_faces":
+        nf = Nfr + Nfz
+        if first:
+            return N * (2 * w + 2 * q * wr) + nf * (8 + w + q * wr)
+        return N * (2 * w + 2 * q * wr + 16) + nf * (9 + 3 * w + q * wr)
     return 0
 
 
@@ -144,8 +195,24 @@ def dist_setup():
     return world, rank, local
 
 
-def make_disks(workload, rank):
+def c4_disk(nz=C4_NZ):
+    """The config-4 disk; nz < 128 takes the mid-plane slab of nz layers
+    (the same dz) for reduced profiling runs."""
+    import disco_b200 as db
+    par, opt = db.template_paths("c4_binary3d")
+    if nz == C4_NZ:
+        return db.Disk.from_files(par, opt)
+    from disco_b200.workloads import write_par
+    p = write_par({"Num_Z": nz, "Z_Min": -0.5 * nz / C4_NZ, "Z_Max": 0.5 * nz / C4_NZ}, base="c4_binary3d")
+    d = db.Disk.from_files(p, opt)
+    os.unlink(p)
+    return d
+
+
+def make_disks(workload, rank, c4_nz=C4_NZ):
     from disco_b200 import workloads
+    if workload == "config4":
+        return [c4_disk(c4_nz)]
     if workload == "config0":
         return [workloads.config0_disk()]
     if workload == "ragged8":
@@ -158,7 +225,7 @@ def make_disks(workload, rank):
 # disco_b200.workloads.ragged_specs (tests/test_bench_config.py checks that
 # they agree) written into the same template.
 TEMPLATE_PAR = os.path.join(REPO, "disco_b200", "templates", "c0_kepler2d.par")
-NDISK = {"ragged64": 64, "ragged8": 8, "config0": 1}
+NDISK = {"ragged64": 64, "ragged8": 8, "config0": 1, "config4": 1}
 
 
 def ragged_specs(ndisk, seed=314159, rank=0):
@@ -194,9 +261,23 @@ def reference_pars(workload, directory, rank=0):
             for nr, mach, s in ragged_specs(NDISK[workload], rank=rank)]
 
 
-def workload_config(workload, nreal):
+def workload_config(workload, nreal, c4_nz=C4_NZ):
     """The `config` object of both arms' lines: the workload, nothing of
     either implementation."""
+    if workload == "config4":
+        return {"workload": "config4" + ("" if c4_nz == C4_NZ else "_nz%d" % c4_nz),
+                "description": "3D MHD circumbinary disk, softened equal-mass binary (eps 0.05, "
+                               "separation 1), HLLD + constrained transport",
+                "disks_per_gpu": 1, "real_cells_per_gpu": int(nreal),
+                "grid": "Nr 384 (r in [0.5, 10], linear) x Nz %d (z in [-0.5, 0.5] at 128), aspect 1.66, "
+                        "Np up to 1536: %d real cells (changed from the configuration's 'about 50M', "
+                        "which Np <= 1536 on 384 x 128 annuli cannot reach)" % (c4_nz, nreal),
+                "physics": "MHD, HLLD, PLM 1.5, RK2, CFL 0.2, CT_MODE 2, binary_soft planets, "
+                           "zerograd boundaries, Mesh_Motion 3, diag_disk2d",
+                "precision": "FP32 bulk (prims, slopes, fluxes, edge fields), FP64 piph / mesh / dt / "
+                             "Kahan-compensated conserved update and face fluxes",
+                "l2_policy": "inputs larger than L2 (%.1f GB of prim+cons state per GPU)"
+                             % (nreal * (4 + 8) * 9 / 1e9)}
     base = ("64 2D Keplerian hydro disks" if workload == "ragged64" else
             "8 2D Keplerian hydro disks" if workload == "ragged8" else "the config-0 2D Keplerian hydro disk")
     grid = ("Num_R drawn from [32, 256] per disk (seeded), log r in [0.5, 3], Np constant per disk"
@@ -250,16 +331,61 @@ def time_reference(workload, nsteps, max_workers=None):
     return zones / wall, cores, sample, nreal
 
 
+C4_SLAB_NZ = 4
+
+
+def time_reference_c4(nsteps, max_workers=None):
+    """The reference's serial CPU code on the config-4 module set (mhd,
+    hlld, CT_MODE 2, binary_soft, zerograd): one process per host core,
+    each the full 384-annulus r grid and Np on a 4-layer mid-plane z slab
+    (the slabs a z decomposition of the workload would give each core).
+    Returns (zone-updates/s summed over the processes over the slowest
+    process's step-loop time, cores, sample description, real cells of one
+    slab)."""
+    import pyoracle
+    binary = pyoracle.ref_binary("c4_binary3d")
+    if not os.path.exists(binary):
+        pyoracle.build_ref("c4_binary3d")
+    cores = max_workers or min(os.cpu_count() or 1, 32)
+    text = write_par_text("c4_binary3d", {"Num_Z": C4_SLAB_NZ, "Z_Min": -0.5 * C4_SLAB_NZ / C4_NZ,
+                                          "Z_Max": 0.5 * C4_SLAB_NZ / C4_NZ})
+    work, procs = [], []
+    for w in range(cores):
+        d = tempfile.mkdtemp(prefix="dref4_")
+        with open(os.path.join(d, "in.par"), "w") as f:
+            f.write(text)
+        work.append(d)
+        procs.append(subprocess.Popen([binary, d, str(nsteps), "--time"], stdout=subprocess.PIPE, text=True))
+    secs, zones, cells = [], 0, 0
+    for pr in procs:
+        out, _ = pr.communicate(timeout=1800)
+        r = json.loads([l for l in out.splitlines() if l.startswith("{")][0])
+        secs.append(r["seconds"])
+        zones += r["real_cells"] * r["steps"]
+        cells = r["real_cells"]
+    for d in work:
+        subprocess.run(["rm", "-rf", d])
+    sample = ("config4 module set, %d processes on %d cores, each the full r grid and Np on a %d-layer "
+              "z slab (%d real cells) for %d step(s), step-loop time only"
+              % (cores, cores, C4_SLAB_NZ, cells, nsteps))
+    return zones / max(secs), cores, sample, cells
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    v, cores, sample, nreal = time_reference(args.workload, max(1, args.steps // 4))
+    if args.workload == "config4":
+        v, cores, sample, _ = time_reference_c4(max(1, args.steps // 10))
+        nreal = C4_REAL_PER_LAYER * args.c4_nz
+    else:
+        v, cores, sample, nreal = time_reference(args.workload, max(1, args.steps // 4))
     line = {"metric": METRIC, "value": v, "unit": "zone-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": workload_config(args.workload, nreal),
-            "parallelism": "one host process per disk",
+            "config": workload_config(args.workload, nreal, args.c4_nz),
+            "parallelism": ("one host process per core (z slabs)" if args.workload == "config4"
+                            else "one host process per disk"),
             "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
@@ -399,9 +525,6 @@ def config1_leg(args, local, stream):
                       "note": "max over real cells of |net face flux(t) - net face flux(0)| / max |Phi|"}
     b.close()
     return out
-
-
-B_ALG_MHD_CT = {"fp64": 1056, "mixed": 1200}   # HBM bytes per zone-update, MHD Q=9 with CT (5 faces)
 
 
 def config4_leg(args, local, stream):
@@ -683,6 +806,149 @@ def c2p_leg(args, local, stream):
     return out
 
 
+def face_counts(disks):
+    """(r-faces, z-faces) of the disks' face lists: each track's face count
+    is the sum of its two annuli's Np (fIndex, faces_alt.c:97-100)."""
+    nfr = nfz = 0
+    for d in disks:
+        Np = d.Np.reshape(d.Nz, d.Nr)
+        nfr += int((Np[:, :-1] + Np[:, 1:]).sum())
+        if d.Nz > 1:
+            nfz += int((Np[:-1, :] + Np[1:, :]).sum())
+    return nfr, nfz
+
+
+def timed_run(b, stream, steps, barrier, allmax, clocks=None):
+    """b.run(steps) between CUDA events on the batch's stream, barriers on
+    both sides; returns (max over ranks of the ms, clock record)."""
+    import torch
+    barrier()
+    if clocks:
+        clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        b.run(steps)
+        e1.record(stream)
+    e1.synchronize()
+    ck = clocks.stop() if clocks else None
+    barrier()
+    if b.last_error() != 0:
+        import disco_b200 as db
+        raise RuntimeError("device error during the timed region: %s" % db.STATUS.get(b.last_error()))
+    return allmax(e0.elapsed_time(e1)), ck
+
+
+def kernel_table(kt):
+    tot, cnt = {}, {}
+    for name, t in kt:
+        tot[name] = tot.get(name, 0.0) + t
+        cnt[name] = cnt.get(name, 0) + 1
+    return tot, cnt
+
+
+def dominant_roofline(kt, bytes_of, traffic_of):
+    """Roofline object of the kernel with the largest device time in one
+    instrumented step: algorithmic bytes of its launches over their time."""
+    hbm, peak_kind = peaks()
+    tot, byt, seen = {}, {}, {}
+    for name, t in kt:
+        first = seen.get(name, 0) == 0
+        seen[name] = seen.get(name, 0) + 1
+        tot[name] = tot.get(name, 0.0) + t
+        byt[name] = byt.get(name, 0) + bytes_of(name, first)
+    dom = max(tot, key=tot.get)
+    achieved = byt[dom] / (tot[dom] / 1e3) / 1e9 if byt[dom] else None
+    traffic, src = traffic_of(dom, seen[dom])
+    return {"bound": "hbm", "kernel": dom, "launches_per_step": seen[dom],
+            "bytes_per_launch": byt[dom] / seen[dom] if byt[dom] else None,
+            "ms_per_launch": tot[dom] / seen[dom],
+            "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm if achieved else None, "traffic": traffic, "traffic_source": src,
+            "peak_kind": peak_kind}, tot
+
+
+def ragged_leg(args, local, stream, barrier, allmax, rank, world):
+    """Config 2: 64 ragged 2D hydro disks in one batch, FP64 plain path (the
+    graph-replayed kernel-per-pass step and the persistent one-launch
+    schedule), the mixed form, per-kernel times, the dominant kernel's
+    roofline and the step roofline; the reference on the same 64 disks."""
+    import disco_b200 as db
+    disks = make_disks("ragged64", rank)
+    b = db.Batch(disks, device=local)
+    nreal, ncell = sum(d.nreal for d in disks), b.ncell
+    nf, _ = face_counts(disks)
+    na = sum(d.Nr * d.Nz for d in disks)
+    b.set_stream(stream.cuda_stream)
+    b.run(args.warmup)
+    b.sync()
+    kt = b.kernel_times()
+    ms, _ = timed_run(b, stream, args.steps, barrier, allmax)
+    value = world * nreal * args.steps / (ms / 1e3)
+
+    def traffic_of(dom, n):
+        per_unit = {"k_update": (DRAM_UPDATE_RAGGED8, ncell), "k_flux_r": (DRAM_FLUX_RAGGED8, nf)}
+        if dom not in per_unit:
+            return None, None
+        (b8, u8), units = per_unit[dom]
+        return b8 / u8 * units, ("ncu capture on ragged8 (dram bytes of one %s launch), scaled by the "
+                                 "units processed" % dom)
+    roof, tot = dominant_roofline(kt, lambda nm, first: kernel_bytes(nm, first, ncell, nf, na, nreal),
+                                  traffic_of)
+    hbm, _ = peaks()
+    step_gbs = B_ALG_STEP * (value / world) / 1e9
+    out = {"workload": workload_config("ragged64", nreal), "value": value, "unit": "zone-updates/s",
+           "ms_per_step": ms / args.steps, "steps": args.steps, "warmup": args.warmup, "dtype": "f64",
+           "layout": {"cells_per_gpu_incl_ghosts": ncell, "r_faces_per_gpu": nf},
+           "roofline": roof,
+           "step_roofline": {"bytes_per_zone_update": B_ALG_STEP, "achieved": step_gbs, "peak": hbm,
+                             "unit": "GB/s", "frac": step_gbs / hbm},
+           "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(tot.items(), key=lambda x: -x[1])},
+           "launches_per_step": len(kt)}
+    # the same step as one persistent launch (disco_batch_set_schedule)
+    try:
+        b.schedule = db.SCHED_PERSISTENT
+    except db.DiscoError:
+        pass
+    if b.schedule == db.SCHED_PERSISTENT:
+        b.run(args.warmup)
+        b.sync()
+        ktot, _ = kernel_table(b.kernel_times())
+        kms, _ = timed_run(b, stream, args.steps, barrier, allmax)
+        out["persistent_schedule"] = {
+            "schedule": "persistent one-launch step", "ms_per_step": kms / args.steps,
+            "value": world * nreal * args.steps / (kms / 1e3),
+            "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(ktot.items(), key=lambda x: -x[1])}}
+        b.schedule = db.SCHED_KERNELS
+    b.close()
+    if not args.no_mixed:
+        bm = db.Batch(disks, device=local, precision=db.PREC_MIXED)
+        bm.set_stream(stream.cuda_stream)
+        bm.run(args.warmup)
+        bm.sync()
+        mms, _ = timed_run(bm, stream, args.steps, barrier, allmax)
+        mv = world * nreal * args.steps / (mms / 1e3)
+        out["mixed_form"] = {"value": mv, "unit": "zone-updates/s", "ms_per_step": mms / args.steps,
+                             "speedup_vs_fp64": mv / value,
+                             "precision": "FP32 prim/slopes/fluxes, FP64 mesh/dt/Kahan cons"}
+        bm.close()
+    if rank0_cpu(args) and world == 1:
+        try:
+            v, cores, sample, _ = time_reference("ragged64", 1)
+            out["cpu_baseline"] = {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "reference",
+                                   "sample": sample}
+        except Exception as ex:
+            out["cpu_baseline"] = {"value": None, "sample": "unavailable: %s" % ex}
+    return out
+
+
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_update launch of the
+# mixed form on the config-4 slab of 12 z layers (4,995,072 cells with
+# ghosts), from an ncu capture: (bytes, cells of that slab)
+DRAM_UPDATE_C4 = (1665111808 + 450670080, 4995072)
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -701,99 +967,104 @@ def run_ours(args, world, rank, local):
             pg.barrier()
         torch.cuda.synchronize()
 
-    from disco_b200.replicas import job_rate, max_over_ranks
+    from disco_b200.replicas import max_over_ranks
 
     def allmax(x):
         return max_over_ranks(x, pg, device="cuda")
 
-    disks = make_disks(args.workload, rank)
-    b = db.Batch(disks, device=local)
+    c4 = args.workload == "config4"
+    disks = make_disks(args.workload, rank, args.c4_nz)
+    prec = db.PREC_MIXED if c4 else db.PREC_FP64
+    b = db.Batch(disks, device=local, precision=prec)
     nreal = sum(d.nreal for d in disks)
     ncell = b.ncell
-    nf = sum(int(sum(d.Np[j] + d.Np[j + 1] for j in range(d.Nr - 1))) for d in disks)
+    nfr, nfz = face_counts(disks)
     na = sum(d.Nr * d.Nz for d in disks)
 
     stream = torch.cuda.Stream(device=local)
     b.set_stream(stream.cuda_stream)
     b.run(args.warmup)
     b.sync()
-
     # per-kernel device times of one step (events between launches, same stream)
-    kt = b.kernel_times()
+    kt = b.kernel_times(cap=128)
     launches_per_step = len(kt)
-
-    barrier()
     clocks = Clocks(local)
-    clocks.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        e0.record(stream)
-        b.run(args.steps)
-        e1.record(stream)
-    e1.synchronize()
-    ck = clocks.stop()
-    barrier()
-    if b.last_error() != 0:
-        raise RuntimeError("device error during the timed region: %s" % db.STATUS.get(b.last_error()))
-    ms = allmax(e0.elapsed_time(e1))
-    value = job_rate(world, nreal, args.steps, ms)
-
-    # roofline of the dominant kernel (sum over its launches in the step)
+    ms, ck = timed_run(b, stream, args.steps, barrier, allmax, clocks)
+    value = world * nreal * args.steps / (ms / 1e3)
     hbm, peak_kind = peaks()
-    tot, byt, seen = {}, {}, {}
-    for name, t in kt:
-        first = seen.get(name, 0) == 0
-        seen[name] = seen.get(name, 0) + 1
-        tot[name] = tot.get(name, 0.0) + t
-        byt[name] = byt.get(name, 0) + kernel_bytes(name, first, ncell, nf, na, nreal)
-    dom = max(tot, key=tot.get)
-    achieved = byt[dom] / (tot[dom] / 1e3) / 1e9
-    # DRAM bytes of one launch of the dominant kernel: the ncu capture of the
-    # same kernel on the smaller ragged8 workload, scaled by the cells (r-faces
-    # for k_flux_r) one launch here processes -- the ragged workloads' traffic
-    # grows with the cells, each cell's state crossing HBM once
-    per_unit = {"k_update": (DRAM_UPDATE_RAGGED8, "cells"), "k_flux_r": (DRAM_FLUX_RAGGED8, "faces")}
-    traffic = None
-    if dom in per_unit and args.workload.startswith("ragged"):
-        (b8, units8), kind = per_unit[dom]
-        traffic = b8 / units8 * (ncell if kind == "cells" else nf)
-    step_gbs = B_ALG_STEP * (value / world) / 1e9
 
-    # the same step as one persistent launch (disco_batch_set_schedule), for
-    # comparison with the default multi-kernel step timed above
-    sched_cmp = None
-    try:
-        b.schedule = db.SCHED_PERSISTENT
-    except db.DiscoError:
-        pass
-    if b.schedule == db.SCHED_PERSISTENT:
-        b.run(args.warmup)
-        b.sync()
-        kt_k = b.kernel_times()
-        barrier()
-        h0 = torch.cuda.Event(enable_timing=True)
-        h1 = torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            h0.record(stream)
-            b.run(args.steps)
-            h1.record(stream)
-        h1.synchronize()
-        barrier()
-        kms = allmax(h0.elapsed_time(h1))
-        ktot = {}
-        for name, t in kt_k:
-            ktot[name] = ktot.get(name, 0.0) + t
-        sched_cmp = {"schedule": "persistent one-launch step", "ms_per_step": kms / args.steps,
-                     "value": job_rate(world, nreal, args.steps, kms),
-                     "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(ktot.items(), key=lambda x: -x[1])},
-                     "launches_per_step": len(kt_k)}
-        b.schedule = db.SCHED_KERNELS
+    if c4:
+        def bytes_of(name, first):
+            return kernel_bytes_mhd(name, first, ncell, nfr, nfz, mixed=True)
+
+        def traffic_of(dom, n):
+            if dom != "k_update" or DRAM_UPDATE_C4 is None:
+                return None, None
+            bb, cells = DRAM_UPDATE_C4
+            return bb / cells * ncell, ("ncu capture of one k_update launch on the 12-layer config-4 "
+                                        "slab, scaled by the cells processed")
+        b_step = B_ALG_MHD_CT["mixed"]
+    else:
+        def bytes_of(name, first):
+            return kernel_bytes(name, first, ncell, nfr, na, nreal)
+
+        def traffic_of(dom, n):
+            per_unit = {"k_update": (DRAM_UPDATE_RAGGED8, ncell), "k_flux_r": (DRAM_FLUX_RAGGED8, nfr)}
+            if dom not in per_unit or not args.workload.startswith("ragged"):
+                return None, None
+            (b8, u8), units = per_unit[dom]
+            return b8 / u8 * units, ("ncu capture on ragged8 (dram bytes of one %s launch), scaled by "
+                                     "the units processed" % dom)
+        b_step = B_ALG_STEP
+    roof, tot = dominant_roofline(kt, bytes_of, traffic_of)
+    step_gbs = b_step * (value / world) / 1e9
+
+    # the FP64 plain path on the same set-up and the same step sequence
+    # (config 4): its throughput and roofline, and the FP32 form's error and
+    # drifts against it
+    fp64 = None
+    if c4:
+        r = np.concatenate([d.real for d in disks]) == 1
+        sm = b.get_cells()
+        b64 = db.Batch(disks, device=local)
+        b64.set_stream(stream.cuda_stream)
+        s0 = b64.get_cells()
+        tot0 = {q: float(s0["cons"][r, q].sum()) for q in (0, 3)}
+        del s0
+        b64.run(args.warmup)
+        b64.sync()
+        kt64 = b64.kernel_times(cap=128)
+        ms64, _ = timed_run(b64, stream, args.steps, barrier, allmax)
+        v64 = world * nreal * args.steps / (ms64 / 1e3)
+        roof64, tot64 = dominant_roofline(kt64, lambda nm, first: kernel_bytes_mhd(nm, first, ncell, nfr, nfz,
+                                                                                   mixed=False),
+                                          lambda dom, n: (None, None))
+        sa = b64.get_cells()
+        b64.close()
+        names = ["rho", "P", "v_r", "omega", "v_z", "B_r", "B_phi", "B_z", "X"]
+        err = {}
+        for q, nm in enumerate(names):
+            den = np.abs(sa["prim"][r, q]).sum()
+            err[nm] = float(np.abs(sm["prim"][r, q] - sa["prim"][r, q]).sum() / den) if den > 0 else None
+        ctot = lambda st, q: float(st["cons"][r, q].sum())
+        g64 = B_ALG_MHD_CT["fp64"] * (v64 / world) / 1e9
+        fp64 = {"value": v64, "unit": "zone-updates/s", "ms_per_step": ms64 / args.steps,
+                "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(tot64.items(), key=lambda x: -x[1])},
+                "roofline": roof64,
+                "step_roofline": {"bytes_per_zone_update": B_ALG_MHD_CT["fp64"], "achieved": g64, "peak": hbm,
+                                  "unit": "GB/s", "frac": g64 / hbm},
+                "mixed_speedup_vs_fp64": value / v64,
+                "mixed_rel_l1_vs_fp64": err,
+                "drift": {"mass_fp64": ctot(sa, 0) / tot0[0] - 1.0, "mass_mixed": ctot(sm, 0) / tot0[0] - 1.0,
+                          "ang_mom_fp64": ctot(sa, 3) / tot0[3] - 1.0,
+                          "ang_mom_mixed": ctot(sm, 3) / tot0[3] - 1.0},
+                "note": "both forms from the same set-up after %d warm-up + 1 instrumented + %d timed steps"
+                        % (args.warmup, args.steps)}
+        del sa, sm
 
     # end to end through the C ABI with host buffers: upload the state from
-    # host memory, K x {dt = getmindt() -> host; timestep(dt) from host},
-    # download the state.
-    # Host buffers are pinned (the state a host code keeps between outputs).
+    # pinned host memory, K x {dt = getmindt() -> host; timestep(dt) from
+    # host}, download the state into the same buffers.
     keep = []
 
     def pinned(a):
@@ -803,77 +1074,64 @@ def run_ours(args, world, rank, local):
         n[...] = a
         return n
     st = {k: pinned(v) for k, v in b.get_cells().items()}
-    out_bufs = {k: pinned(np.zeros_like(v)) for k, v in st.items()}
-    h2d = (st["prim"].nbytes + st["cons"].nbytes + st["piph"].nbytes + st["dphi"].nbytes
-           + st["wiph"].nbytes + 4 * ncell)
-    d2h = h2d - 4 * ncell
     real = pinned(np.concatenate([d.real for d in disks]).astype(np.int32))
+    h2d = sum(st[k].nbytes for k in st) + real.nbytes
+    d2h = sum(st[k].nbytes for k in st)
     barrier()
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     t_wall = time.perf_counter()
-    b.set_cells(st["prim"], st["cons"], st["piph"], st["dphi"], st["wiph"], real)
+    b.set_cells(st["prim"], st["cons"], st["piph"], st["dphi"], st["wiph"], real, Phi=st.get("Phi"))
     for _ in range(args.steps):
         dt = b.mindt()
         b.timestep(dt)
-    out = b.get_cells(out=out_bufs)
+    b.get_cells(out=st)
     f1.record(stream)
     f1.synchronize()
     t_wall = time.perf_counter() - t_wall
     e2e_ms = allmax(max(f0.elapsed_time(f1), t_wall * 1e3))
     e2e = world * nreal * args.steps / (e2e_ms / 1e3)
-    del out
+    del st, keep
+    b.close()
 
-    # the mixed-precision form on the same disks, timed the same way
     mixed = None
-    if not args.no_mixed:
+    if not c4 and not args.no_mixed:
         bm = db.Batch(disks, device=local, precision=db.PREC_MIXED)
         bm.set_stream(stream.cuda_stream)
         bm.run(args.warmup)
         bm.sync()
-        barrier()
-        g0 = torch.cuda.Event(enable_timing=True)
-        g1 = torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            g0.record(stream)
-            bm.run(args.steps)
-            g1.record(stream)
-        g1.synchronize()
-        barrier()
-        if bm.last_error() != 0:
-            raise RuntimeError("device error in the mixed-form timed region")
-        mms = allmax(g0.elapsed_time(g1))
+        mms, _ = timed_run(bm, stream, args.steps, barrier, allmax)
         mv = world * nreal * args.steps / (mms / 1e3)
         mixed = {"value": mv, "unit": "zone-updates/s", "ms_per_step": mms / args.steps,
                  "speedup_vs_fp64": mv / value,
                  "precision": "FP32 prim/slopes/fluxes, FP64 mesh/dt/Kahan cons"}
         bm.close()
 
-    config1 = None
+    side = {}
+    if c4 and not args.no_config2:
+        side["config2_ragged64"] = ragged_leg(args, local, stream, barrier, allmax, rank, world)
+        barrier()
     if not args.no_config1:
-        config1 = config1_leg(args, local, stream)
+        side["config1_mhd3d"] = config1_leg(args, local, stream)
         barrier()
-
-    config4 = None
-    if not args.no_config4:
-        config4 = config4_leg(args, local, stream)
+    if not c4 and not args.no_config4:
+        side["config4_binary3d"] = config4_leg(args, local, stream)
         barrier()
-
-    config3 = None
     if not args.no_config3:
-        config3 = config3_leg(args, local, stream)
+        side["config3_grtorus"] = config3_leg(args, local, stream)
         barrier()
-
-    c2p = None
     if not args.no_c2p:
-        c2p = c2p_leg(args, local, stream)
+        side["c2p"] = c2p_leg(args, local, stream)
         barrier()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            v, cores, sample, _ = time_reference(args.workload, 1)
+            if c4:
+                v, cores, sample, _ = time_reference_c4(1)
+            else:
+                v, cores, sample, _ = time_reference(args.workload, 1)
             cpu = {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "reference",
                    "sample": sample}
         except Exception as ex:  # reference binary missing on this machine
@@ -884,37 +1142,28 @@ def run_ours(args, world, rank, local):
         line = {
             "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": workload_config(args.workload, nreal),
-            "layout": {"cells_per_gpu_incl_ghosts": ncell, "r_faces_per_gpu": nf,
-                       "precision": "fp64 plain path"},
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if c4 else "f64", "data": "synthetic",
+            "config": workload_config(args.workload, nreal, args.c4_nz),
+            "layout": {"cells_per_gpu_incl_ghosts": ncell, "r_faces_per_gpu": nfr, "z_faces_per_gpu": nfz,
+                       "precision": "mixed form" if c4 else "fp64 plain path"},
             "parallelism": "independent disks per GPU" if world > 1 else "single GPU",
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                         "traffic_source": ("ncu capture on ragged8 (dram bytes of one %s launch), "
-                                            "scaled by the units processed" % dom)
-                         if traffic is not None else None,
-                         "peak_kind": peak_kind},
-            "step_roofline": {"bytes_per_zone_update": B_ALG_STEP, "achieved": step_gbs, "peak": hbm,
+            "roofline": roof,
+            "step_roofline": {"bytes_per_zone_update": b_step, "achieved": step_gbs, "peak": hbm,
                               "unit": "GB/s", "frac": step_gbs / hbm},
             "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(tot.items(), key=lambda x: -x[1])},
-            "schedule": "persistent one-launch step" if dom == "k_step" else "one kernel per pass",
-            "persistent_schedule": sched_cmp,
+            "schedule": "one kernel per pass, CUDA-graph replay",
             "e2e": {"value": e2e, "unit": "zone-updates/s",
                     "h2d_bytes_per_step": (h2d + 8 * len(disks) * args.steps) / args.steps,
                     "d2h_bytes_per_step": (d2h + 8 * len(disks) * args.steps) / args.steps},
             "gpu_launches": launches_per_step * args.steps,
+            "fp64_plain": fp64,
             "mixed_form": mixed,
-            "config1_mhd3d": config1,
-            "config3_grtorus": config3,
-            "config4_binary3d": config4,
-            "c2p": c2p,
             "clocks": ck,
             "cpu_baseline": cpu,
         }
+        line.update(side)
         print(json.dumps(line), flush=True)
-    b.close()
     if pg:
         pg.destroy_process_group()
 
@@ -925,7 +1174,10 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ragged64", choices=["ragged64", "ragged8", "config0"])
+    ap.add_argument("--workload", default="config4", choices=["config4", "ragged64", "ragged8", "config0"])
+    ap.add_argument("--c4-nz", type=int, default=C4_NZ,
+                    help="z layers of the config-4 disk (128; fewer for profiling captures)")
+    ap.add_argument("--no-config2", action="store_true", help="skip the ragged64 (config 2) leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--no-c2p", action="store_true", help="skip the GRMHD cons->prim leg")

@@ -31,3 +31,23 @@ def test_config_is_implementation_free():
     c = bench.workload_config("ragged64", 5490132)
     assert c["real_cells_per_gpu"] == 5490132 and c["disks_per_gpu"] == 64
     assert bench.workload_config("ragged64", 5490132) == c
+
+
+def test_config4_cell_count_without_the_library():
+    """The reference arm names the config-4 workload's real cells from a
+    per-layer constant (Np depends on r only), without building the disk."""
+    d = bench.c4_disk()
+    assert d.nreal == bench.C4_REAL_PER_LAYER * bench.C4_NZ
+    assert bench.c4_disk(8).nreal == bench.C4_REAL_PER_LAYER * 8
+    c = bench.workload_config("config4", d.nreal)
+    assert c["workload"] == "config4" and c["real_cells_per_gpu"] == d.nreal
+
+
+def test_config4_slab_par_text():
+    """The reference arm's 4-layer slab of config 4: the template with the
+    z extent of 4 of the 128 layers."""
+    text = bench.write_par_text("c4_binary3d", {"Num_Z": bench.C4_SLAB_NZ,
+                                               "Z_Min": -0.5 * bench.C4_SLAB_NZ / bench.C4_NZ,
+                                               "Z_Max": 0.5 * bench.C4_SLAB_NZ / bench.C4_NZ})
+    kv = {l.split()[0]: l.split()[1] for l in text.splitlines() if l.split()}
+    assert kv["Num_Z"] == "4" and float(kv["Z_Max"]) == 0.015625 and kv["Num_R"] == "384"
