@@ -198,15 +198,8 @@ def dist_setup():
 def c4_disk(nz=C4_NZ):
     """The config-4 disk; nz < 128 takes the mid-plane slab of nz layers
     (the same dz) for reduced profiling runs."""
-    import disco_b200 as db
-    par, opt = db.template_paths("c4_binary3d")
-    if nz == C4_NZ:
-        return db.Disk.from_files(par, opt)
-    from disco_b200.workloads import write_par
-    p = write_par({"Num_Z": nz, "Z_Min": -0.5 * nz / C4_NZ, "Z_Max": 0.5 * nz / C4_NZ}, base="c4_binary3d")
-    d = db.Disk.from_files(p, opt)
-    os.unlink(p)
-    return d
+    from disco_b200.workloads import config4_disk
+    return config4_disk(nz)
 
 
 def make_disks(workload, rank, c4_nz=C4_NZ):

@@ -10,6 +10,8 @@ import os
 import shutil
 import subprocess
 import sys
+import time
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
@@ -25,11 +27,13 @@ def nvcc_path():
 
 
 def _run(cmd, verbose):
-    if verbose:
-        print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
+    if verbose:
+        # the command, then ptxas's register / spill report of each kernel
+        print(" ".join(cmd) + "\n" + r.stdout + r.stderr, flush=True)
     if r.returncode != 0:
-        sys.stderr.write(r.stdout + r.stderr)
+        if not verbose:
+            sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("build step failed: " + " ".join(cmd[:3]))
     return r
 
@@ -59,28 +63,34 @@ def build(force=False, verbose=False):
     """Build disco_b200/libdisco_b200.so (sm_100a).  Returns its path."""
     if not force and not needs_build():
         return LIB
+    t0 = time.time()
     nvcc = nvcc_path()
     bdir = os.path.join(HERE, "_build")
     os.makedirs(bdir, exist_ok=True)
     inc = ["-I" + os.path.join(REPO, "include"), "-I" + os.path.join(HERE, "csrc")]
     cu, c = sources()
-    objs = []
+    jobs, objs = [], []
     for src in cu:
         obj = os.path.join(bdir, os.path.basename(src) + ".o")
         # the FP64 parity path must not contract a*b+c into FMA (the reference's
         # x86-64 build does not); the FP32 mixed form (*_mixed.cu) may
         fmad = "--fmad=true" if src.endswith("_mixed.cu") else "--fmad=false"
-        _run([nvcc] + ARCH + ["-O3", "-lineinfo", fmad, "-std=c++17",
-                              "-Xcompiler", "-fPIC", "-Xptxas", "-v"] + inc +
-             ["-c", src, "-o", obj], verbose)
+        jobs.append([nvcc] + ARCH + ["-O3", "-lineinfo", fmad, "-std=c++17",
+                                     "-Xcompiler", "-fPIC", "-Xptxas", "-v"] + inc + ["-c", src, "-o", obj])
         objs.append(obj)
     for src in c:
         obj = os.path.join(bdir, os.path.basename(src) + ".o")
-        _run(["gcc", "-O2", "-fPIC", "-std=gnu11"] + inc + ["-c", src, "-o", obj], verbose)
+        jobs.append(["gcc", "-O2", "-fPIC", "-std=gnu11"] + inc + ["-c", src, "-o", obj])
         objs.append(obj)
+    # the translation units compile independently: all at once
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, j, verbose) for j in jobs]:
+            f.result()
     tmp = LIB + ".tmp"
     _run([nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lm", "-lz"], verbose)
     os.replace(tmp, LIB)
+    # dated to the build's start, so a source edited during it is newer
+    os.utime(LIB, (t0, t0))
     return LIB
 
 

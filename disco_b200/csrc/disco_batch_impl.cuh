@@ -129,7 +129,7 @@ static void launch_setup_qt(disco_batch *b, const ViewT<R> &v){
          k_I0<R><<<nblk((size_t)v.Nann*32, 128), 128, 0, b->stream>>>(v);
          k_faces<Q,R><<<nfb, FB, 0, b->stream>>>(v, 0);
          k_ct_face_init<Q,NC,R><<<nfb, FB, 0, b->stream>>>(v);
-         k_c2p<Q,NC,R><<<ncb, CB, 0, b->stream>>>(v, 0, b->bc_fixed, 0);
+         k_c2p<Q,NC,R,5,false,false,0><<<ncb, CB, 0, b->stream>>>(v, b->bc_fixed, 0);
       }
    }
    k_wcell<Q,R><<<ncb, CB, 0, b->stream>>>(v);
@@ -154,9 +154,14 @@ template<int Q, int NC, class R, int NQD, bool GR>
 static void launch_c2p_nq(disco_batch *b, const ViewT<R> &v, int last, int diag){
    unsigned ncb = (unsigned)b->cblk.size();
    if constexpr ( NC == 5 ){
-      if( b->any_visc ){ k_c2p<Q,NC,R,NQD,true><<<ncb, CB, 0, b->stream>>>(v, last, b->bc_fixed, diag); return; }
+      if( b->any_visc ){
+         if( last ) k_c2p<Q,NC,R,NQD,true,false,1><<<ncb, CB, 0, b->stream>>>(v, b->bc_fixed, diag);
+         else       k_c2p<Q,NC,R,NQD,true,false,0><<<ncb, CB, 0, b->stream>>>(v, b->bc_fixed, diag);
+         return;
+      }
    }
-   k_c2p<Q,NC,R,NQD,false,GR><<<ncb, CB, 0, b->stream>>>(v, last, b->bc_fixed, diag);
+   if( last ) k_c2p<Q,NC,R,NQD,false,GR,1><<<ncb, CB, 0, b->stream>>>(v, b->bc_fixed, diag);
+   else       k_c2p<Q,NC,R,NQD,false,GR,0><<<ncb, CB, 0, b->stream>>>(v, b->bc_fixed, diag);
 }
 template<int Q, int NC, class R, bool GR = false>
 static void launch_c2p(disco_batch *b, const ViewT<R> &v, int last, int diag){

@@ -132,7 +132,8 @@ __global__ void __launch_bounds__(CB) k_ct_edges(ViewT<R> v){
          }
       }
    }
-   for( int s=0 ; s<ne ; ++s ){ v.ctE[s*N + c] = E[s]; v.ctB[s*N + c] = B[s]; }
+#pragma unroll
+   for( int s=0 ; s<8 ; ++s ) if( s < ne ){ v.ctE[s*N + c] = E[s]; v.ctB[s*N + c] = B[s]; }
 }
 
 /* next / previous cell of annulus a (cyclic) */
@@ -293,15 +294,12 @@ __global__ void __launch_bounds__(CB) k_ct_line(ViewT<R> v){
             cnt[n] = f - v.tr_off[tz] - t;
          }else{                       /* diagonal: cells of list n before this one */
             int o = v.ann_off[an[n]], nn = v.ann_np[an[n]], I0n = v.I0[an[n]];
-            int lo = 0, hi = nn;
-            while( lo < hi ){
-               int mid = (lo + hi) >> 1;
+            /* both lists unrolled from I0: the count is near t nn / np */
+            cnt[n] = gallop_lb(0, nn, (int)(((long long)t*nn)/np), [&](int mid){
                int s = I0n + mid; if( s >= nn ) s -= nn;
                double uy = v.piph[o + s];
-               bool before = n < m ? uy <= ux : uy < ux;
-               if( before ) lo = mid + 1; else hi = mid;
-            }
-            cnt[n] = lo;
+               return !(n < m ? uy <= ux : uy < ux);
+            });
          }
       }
       int e = cnt[0] + cnt[1] + cnt[2] + cnt[3];

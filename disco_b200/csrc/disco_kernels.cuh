@@ -35,6 +35,9 @@
 #include "grmhd_step.cuh"
 
 #include "tuned.h"
+#if __has_include("tuned_mhd.h")
+#include "tuned_mhd.h"
+#endif
 
 namespace disco {
 
@@ -56,7 +59,9 @@ namespace disco {
  * autotuner (disco_b200/autotune.py) measured on a B200, per precision
  * (DISCO_MIXED_TU marks the FP32 translation unit); a -DMB_x on the
  * command line overrides them, and the defaults below fill the rest.  The
- * MHD instantiations (HLLD needs about 160 registers) keep MB_MHD. */
+ * MHD instantiations (HLLD needs about 160 registers) take MB_MHD_* from
+ * tuned_mhd.h, the same autotuner's values for Q = 9 measured on the
+ * config-4 slab, else MB_MHD. */
 #ifndef MB_FACES
 #define MB_FACES 1
 #endif
@@ -65,6 +70,22 @@ namespace disco {
 #endif
 #ifndef MB_MHD
 #define MB_MHD 4
+#endif
+/* per kernel, for the MHD instantiations */
+#ifndef MB_MHD_BEGIN
+#define MB_MHD_BEGIN MB_MHD
+#endif
+#ifndef MB_MHD_GRAD
+#define MB_MHD_GRAD MB_MHD
+#endif
+#ifndef MB_MHD_FLUX
+#define MB_MHD_FLUX MB_MHD
+#endif
+#ifndef MB_MHD_UPDATE
+#define MB_MHD_UPDATE MB_MHD
+#endif
+#ifndef MB_MHD_C2P
+#define MB_MHD_C2P MB_MHD
 #endif
 #ifndef MB_BEGIN
 #define MB_BEGIN 10
@@ -290,7 +311,7 @@ __device__ __forceinline__ void begin_body(const ViewT<R> &v, double RK, int fir
    }
 }
 template<int Q, int NC, class R, bool GR = false>
-__global__ void __launch_bounds__(CB, GR ? MB_GR_LIGHT : (Q > 6 ? MB_MHD : MB_BEGIN)) k_begin(ViewT<R> v, double RK, int first){
+__global__ void __launch_bounds__(CB, GR ? MB_GR_LIGHT : (Q > 6 ? MB_MHD_BEGIN : MB_BEGIN)) k_begin(ViewT<R> v, double RK, int first){
    begin_body<Q,NC,R,GR>(v, RK, first, blockIdx.x);
 }
 
@@ -420,6 +441,37 @@ __global__ void k_I0(ViewT<R> v){
    I0_body<R>(v, v.topo_reuse, (blockIdx.x*blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31);
 }
 
+/* The first x in [lo, hi) where the monotone predicate p turns true (hi if
+ * it never does) -- the binary search's answer -- found by galloping out
+ * from a guess g and bisecting the bracket: a few probes when g is close,
+ * as the position of a face or edge in the other annulus usually is. */
+template<class Pr>
+__device__ __forceinline__ int gallop_lb(int lo, int hi, int g, Pr p){
+   if( g < lo ) g = lo;
+   if( g > hi ) g = hi;
+   int a, b;
+   if( g < hi && !p(g) ){            /* the answer lies above g */
+      a = g + 1; b = hi;
+      for( int step=1 ; a + step - 1 < hi ; step <<= 1 ){
+         const int x = a + step - 1;
+         if( p(x) ){ b = x; break; }
+         a = x + 1;
+      }
+   }else{                            /* at or below g */
+      a = lo; b = g;
+      for( int step=1 ; b - step >= lo ; step <<= 1 ){
+         const int x = b - step;
+         if( !p(x) ){ a = x + 1; break; }
+         b = x;
+      }
+   }
+   while( a < b ){
+      const int mid = (a + b) >> 1;
+      if( p(mid) ) b = mid; else a = mid + 1;
+   }
+   return a;
+}
+
 /* ------------------------------------------------------------------ faces
  * buildfaces (faces_alt.c:102-177) as a merge path: face d of a track is
  * the d-th step of the reference's two-pointer merge, found by binary
@@ -465,12 +517,13 @@ __device__ __forceinline__ void faces_body(const ViewT<R> &v, int with_slopes, i
    }
    int lo = dd - NB > 0 ? dd - NB : 0;
    int hi = dd < NA ? dd : NA;
-   while( lo < hi ){
-      int mid = (lo + hi) >> 1;
+   /* the diagonal's split: both annuli's edges are unrolled from I0, so face
+    * dd lies near phi = dd/(NA+NB) of the turn in both */
+   lo = gallop_lb(lo, hi, (int)(((long long)dd*NA)/(NA+NB)), [&](int mid){
       int ia = IA + mid;       if( ia >= NA ) ia -= NA;
       int ib = IB + dd - mid - 1; if( ib >= NB ) ib -= NB;
-      if( v.piph[cA0+ia] > v.piph[cB0+ib] ) hi = mid; else lo = mid + 1;
-   }
+      return v.piph[cA0+ia] > v.piph[cB0+ib];
+   });
    int ka = lo, kb = dd - lo;
    int ia = IA + ka; while( ia >= NA ) ia -= NA;
    int ib = IB + kb; while( ib >= NB ) ib -= NB;
@@ -663,7 +716,7 @@ __device__ __forceinline__ void grad_body(const ViewT<R> &v, int bid){
    raise_err(v, err);
 }
 template<int Q, int DIM, class R>
-__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD : MB_GRAD) k_grad(ViewT<R> v){
+__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD_GRAD : MB_GRAD) k_grad(ViewT<R> v){
    grad_body<Q,DIM,R>(v, blockIdx.x);
 }
 
@@ -832,7 +885,7 @@ __device__ __forceinline__ void flux_body(const ViewT<R> &v, double dtfac, int b
    raise_err(v, err);
 }
 template<int Q, int NC, int DIM, class R, bool VISC = false, bool GR = false>
-__global__ void __launch_bounds__(FB, GR ? MB_GR : (Q > 6 ? MB_MHD : MB_FLUX)) k_flux_t(ViewT<R> v){
+__global__ void __launch_bounds__(FB, GR ? MB_GR : (Q > 6 ? MB_MHD_FLUX : MB_FLUX)) k_flux_t(ViewT<R> v){
    flux_body<Q,NC,DIM,R,VISC,GR>(v, v.dtfac, blockIdx.x);
 }
 
@@ -1148,7 +1201,7 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
    raise_err(v, err);
 }
 template<int Q, int NC, class R, bool VISC = false, bool GR = false>
-__global__ void __launch_bounds__(CB, GR ? MB_GR : (Q > 6 ? MB_MHD : MB_UPDATE)) k_update(ViewT<R> v, int first){
+__global__ void __launch_bounds__(CB, GR ? MB_GR : (Q > 6 ? MB_MHD_UPDATE : MB_UPDATE)) k_update(ViewT<R> v, int first){
    update_body<Q,NC,R,VISC,GR>(v, first, v.dtfac, blockIdx.x);
 }
 
@@ -1539,9 +1592,12 @@ __device__ __forceinline__ void c2p_body(const ViewT<R> &v, int last, int bc, in
    c2p_tail<Q,NC,R,NQD,VISC,GR>(v, P, a, c, c0, np, i, j, k, d, real, active, piph, dphi, cons, last,
                                 bc, diag, err, topo_set, bid);
 }
-template<int Q, int NC, class R, int NQD = 5, bool VISC = false, bool GR = false>
-__global__ void __launch_bounds__(CB, GR ? MB_GR_LIGHT : (Q > 6 ? MB_MHD : MB_C2P)) k_c2p(ViewT<R> v, int last, int bc, int diag){
-   c2p_body<Q,NC,R,NQD,VISC,GR>(v, last, bc, diag, v.move_c2p, v.topo_set, blockIdx.x);
+/* LAST: 1 for the last substep (the next step's getmindt and the
+ * diagnostics), 0 otherwise -- one instantiation each, so that the
+ * substeps without the reductions keep fewer registers */
+template<int Q, int NC, class R, int NQD = 5, bool VISC = false, bool GR = false, int LAST = 1>
+__global__ void __launch_bounds__(CB, GR ? MB_GR_LIGHT : (Q > 6 ? MB_MHD_C2P : MB_C2P)) k_c2p(ViewT<R> v, int bc, int diag){
+   c2p_body<Q,NC,R,NQD,VISC,GR>(v, LAST, bc, diag, v.move_c2p, v.topo_set, blockIdx.x);
 }
 
 /* The sequential walk of set_cells_copy_distant (boundary_functions.c:
@@ -1605,8 +1661,13 @@ __global__ void k_zerograd(ViewT<R> v, const int2 *pairs, const unsigned char *s
    __shared__ int s_first;
    for( int i=threadIdx.x ; i<np ; i+=blockDim.x ){ sp[i] = v.piph[c0+i]; sd[i] = v.dphi[c0+i]; }
    for( int i=threadIdx.x ; i<np1 ; i+=blockDim.x ){ sp1[i] = v.piph[c10+i]; sd1[i] = v.dphi[c10+i]; }
-   if( threadIdx.x == 0 ) s_first = np1;
+   __shared__ int s_rot;
+   if( threadIdx.x == 0 ){ s_first = np1; s_rot = 0; }
    __syncthreads();
+   /* the source annulus's edges are increasing from its smallest one on
+    * (cyclically): that cell's index, for the binary searches below */
+   for( int k=threadIdx.x+1 ; k<np1 ; k+=blockDim.x )
+      if( sp1[k] < sp1[k-1] ) atomicMax(&s_rot, k);
    {  /* the first source cell (in index order) containing the ghost
        * annulus's first edge: every thread tests its cells, the minimum
        * index wins, as the reference's search loop would stop there */
@@ -1638,11 +1699,20 @@ __global__ void k_zerograd(ViewT<R> v, const int2 *pairs, const unsigned char *s
          if( lane == 0 ){
             start = s_first < np1 ? s_first : 0;
          }else{
+            /* a guess only (checked below): the source cell whose edge is
+             * the first at or after the upper edge of the cell before the
+             * run, by binary search over the source edges unrolled from
+             * the smallest; past the largest it is the cell that wraps */
             const double pt = sp[lo-1];
-            for( int k=0 ; k<np1 ; ++k ){
-               double dd = get_signed_dp(sp1[k], pt, Pmax, &err);
-               if( dd >= 0.0 && dd - sd1[k] < 0.0 ){ start = k; break; }
+            const int rot = s_rot;
+            int l0 = 0, h0 = np1;
+            while( l0 < h0 ){
+               int mid = (l0 + h0) >> 1;
+               int k = rot + mid; if( k >= np1 ) k -= np1;
+               if( sp1[k] < pt ) l0 = mid + 1; else h0 = mid;
             }
+            start = rot + (l0 < np1 ? l0 : 0);
+            if( start >= np1 ) start -= np1;
          }
       }
       s_guess[lane] = start;

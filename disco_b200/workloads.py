@@ -58,3 +58,16 @@ def ragged_disks(ndisk=64, seed=314159, rank=0, keep_pars=False):
 
 def config0_disk():
     return Disk.from_files(*template_paths("c0_kepler2d"))
+
+
+def config4_disk(nz=128):
+    """The config-4 disk (3D MHD circumbinary, CT, 384 x 128 annuli); nz < 128
+    takes the mid-plane slab of nz layers with the same dz."""
+    par, opt = template_paths("c4_binary3d")
+    if nz == 128:
+        return Disk.from_files(par, opt)
+    p = write_par({"Num_Z": nz, "Z_Min": -0.5 * nz / 128, "Z_Max": 0.5 * nz / 128}, base="c4_binary3d")
+    try:
+        return Disk.from_files(p, opt)
+    finally:
+        os.unlink(p)
