@@ -627,6 +627,21 @@ B_ALG_GR = 8 * (10 * 9 + 12)            # HBM bytes per zone-update, Q = 9 witho
 C3_GRID = {"Num_R": 192, "Num_Z": 96, "aspect": 0.75}          # Np 463 per annulus
 
 
+def c3_disk(nz=96):
+    """The config-3 torus disk (Kerr-Schild a = 0.9); nz < 96 takes the
+    mid-plane slice of nz layers (profiling runs).  Returns (disk, overrides)."""
+    import disco_b200 as db
+    from disco_b200.workloads import write_par
+    over = dict(C3_GRID, Metric_Par3=0.9)
+    if nz != C3_GRID["Num_Z"]:
+        over.update(Num_Z=nz, Z_Min=-20.0 * nz / 96, Z_Max=20.0 * nz / 96)
+    p = write_par(over, base="c3_grtorus")
+    try:
+        return db.Disk.from_files(p, os.path.join(db.TEMPLATES, "c3_grtorus_kerr.in")), over
+    finally:
+        os.unlink(p)
+
+
 def config3_leg(args, local, stream):
     """Config 3: the GRMHD torus timestep (grmhd2, Kerr-Schild a = 0.9, HLL,
     noble2d cons->prim, fixed3d), 192 x 96 annuli of 463 cells (8.53M real
@@ -637,14 +652,8 @@ def config3_leg(args, local, stream):
     import numpy as np
     import torch
     import disco_b200 as db
-    from disco_b200.workloads import write_par
     hbm, kind = peaks()
-    over = dict(C3_GRID, Metric_Par3=0.9)
-    if args.c3_nz != C3_GRID["Num_Z"]:           # a slice of the torus (profiling runs)
-        over.update(Num_Z=args.c3_nz, Z_Min=-20.0 * args.c3_nz / 96, Z_Max=20.0 * args.c3_nz / 96)
-    p = write_par(over, base="c3_grtorus")
-    disk = db.Disk.from_files(p, os.path.join(db.TEMPLATES, "c3_grtorus_kerr.in"))
-    os.unlink(p)
+    disk, over = c3_disk(args.c3_nz)
     nsteps = 10
     out = {"workload": "GRMHD torus, Kerr-Schild a=0.9, HLL, Nr=%d Nz=%d (real), Np %d, %d real cells"
                        % (C3_GRID["Num_R"], over["Num_Z"], int(np.max(disk.Np)), disk.nreal),
@@ -700,39 +709,61 @@ def write_par_text(base, overrides):
     return "".join(out)
 
 
-C2P_GRID = {"Nr": 192, "Nz": 96, "Np": 462, "rmin": 1.5, "rmax": 50.0, "zmin": -20.0, "zmax": 20.0}
 C2P_TOL, C2P_NEXTRA, C2P_MAXIT = 1e-10, 10, 30
 C2P_BYTES = 8 * (9 + 3 + 5 + 9)         # read cons, x, the 5 prims of the warm start; write prims
+C2P_DUMPS = 4                           # steps dumped: 3 for training pairs, the last for timing
 
 
 def c2p_leg(args, local, stream):
-    """GRMHD cons -> prim on the torus workload (Kerr-KS a = 0.9): the
-    network is trained on pairs written by plain solves of four perturbation
-    sizes, then plain (previous prims) and learned guesses are timed on fresh
-    states, both finished by Newton to |d eta/eta| < 1e-10 with the
-    reference's tail of 10 and cap of 30."""
+    """GRMHD cons -> prim on the states of the config-3 run (the Kerr-Schild
+    a = 0.9 torus, 192 x 96 annuli of 463 cells): after 3 warm-up steps the
+    step's own cons->prim inputs of 4 consecutive steps are dumped
+    (disco_batch_set_gr_dump: cons / dV, the warm-start prims, x of every
+    real cell).  The plain solver writes the training pairs on the first
+    three; the network is trained on them; on the fourth, plain (the cell's
+    previous prims, as the step starts) and learned guesses are timed, both
+    finished by Newton to |d eta/eta| < 1e-10 with the reference's tail of
+    10 (and without it) and cap of 30; "jump" starts both from prims
+    perturbed by 30% instead, where the previous state is far."""
     import numpy as np
     import torch
+    import disco_b200 as db
     from disco_b200.gr import GR
 
-    g = C2P_GRID
-    gr = GR(device=local, metric="kerr", a=0.9, tol=C2P_TOL, nextra=C2P_NEXTRA, max_iter=C2P_MAXIT)
-    gr.set_stream(stream)
+    disk, over = c3_disk(args.c3_nz)
+    r = torch.from_numpy(disk.real == 1).to("cuda:%d" % local)
+    idx = torch.nonzero(r).squeeze(1)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    out = {"workload": "GRMHD torus, Kerr-KS a=0.9, %dx%dx%d cells (r %.1f-%.0f log, z +-%.0f)" %
-                       (g["Nr"], g["Nz"], g["Np"], g["rmin"], g["rmax"], g["zmax"]),
+    out = {"workload": "cons->prim inputs of the config-3 GRMHD torus step (Kerr-Schild a=0.9, Nr=%d "
+                       "Nz=%d, Np %d), dumped from %d consecutive steps after 3 warm-up steps"
+                       % (C3_GRID["Num_R"], over["Num_Z"], int(np.max(disk.Np)), C2P_DUMPS),
            "tol": C2P_TOL, "nextra": C2P_NEXTRA, "max_iter": C2P_MAXIT}
     with torch.cuda.stream(stream):
-        x = gr.grid(g["Nr"], g["Nz"], g["Np"], g["rmin"], g["rmax"], g["zmin"], g["zmax"])
-        p0 = gr.torus(x)
-        n = x.shape[1]
+        b = db.Batch([disk], device=local)
+        b.set_stream(stream.cuda_stream)
+        b.run(3)
+        b.sync()
+        buf = torch.zeros((db.GR_DUMP_ROWS, b.ncell), dtype=torch.float64, device=idx.device)
+        b.set_gr_dump(buf)
+        dumps = []
+        for _ in range(C2P_DUMPS):
+            b.timestep(b.mindt()[0])
+            torch.cuda.current_stream().wait_stream(stream)
+            b.sync()
+            dumps.append(buf[:, idx].contiguous())
+        b.set_gr_dump(None)
+        b.close()
+        del buf
+        n = int(idx.numel())
         out["ncell"] = n
+        gr = GR(device=local, gamma_law=1.3333333333333, rho_floor=0.0, p_floor=0.0, M=1.0, a=0.9,
+                metric="kerr", tol=C2P_TOL, nextra=C2P_NEXTRA, max_iter=C2P_MAXIT)
+        gr.set_stream(stream)
         pairs = []
-        for seed, eps in ((101, 1e-3), (102, 3e-2), (103, 0.1), (104, 0.3)):
-            cons = gr.prim2cons(gr.perturb(p0, seed, eps), x)
-            pr = p0.clone()
-            pairs.append(gr.cons2prim(cons, x, pr, pairs=True, stats=False)["pairs"])
-            del cons, pr
+        for dmp in dumps[:-1]:
+            pr = dmp[9:18].clone()
+            pairs.append(gr.cons2prim(dmp[0:9], dmp[18:21], pr, pairs=True, stats=False)["pairs"])
+            del pr
         pairs = torch.cat(pairs)
         gr.mlp_init(3)
         gr.mlp_fit_norm(pairs)
@@ -741,60 +772,66 @@ def c2p_leg(args, local, stream):
         hist = gr.mlp_train(pairs, steps=steps, batch=batch, lr=2e-3, seed=9)
         ev[1].record(stream)
         ev[1].synchronize()
-        out["train"] = {"pairs": int(pairs.shape[0]), "steps": steps, "batch": batch,
+        out["train"] = {"pairs": int(pairs.shape[0]), "source": "the plain solver on the step's own inputs "
+                        "of the first %d dumped steps" % (C2P_DUMPS - 1), "steps": steps, "batch": batch,
                         "ms": ev[0].elapsed_time(ev[1]), "loss_first": float(hist[:10].mean()),
                         "loss_last": float(hist[-50:].mean())}
         del pairs
         # the same network in a solver without the tail (tol only)
-        gr0 = GR(device=local, metric="kerr", a=0.9, tol=C2P_TOL, nextra=0, max_iter=C2P_MAXIT)
+        gr0 = GR(device=local, gamma_law=1.3333333333333, rho_floor=0.0, p_floor=0.0, M=1.0, a=0.9,
+                 metric="kerr", tol=C2P_TOL, nextra=0, max_iter=C2P_MAXIT)
         gr0.set_stream(stream)
         gr0.mlp_set(*gr.mlp_get())
-        work = torch.empty_like(p0)
+        test = dumps[-1]
+        cons, x, warm = test[0:9], test[18:21], test[9:18].contiguous()
+        jump = gr.perturb(warm, 777, 0.3)
+        work = torch.empty_like(warm)
         hbm, _ = peaks()
-        for name, eps in (("warm", 1e-3), ("jump", 0.3)):
-            cons = gr.prim2cons(gr.perturb(p0, 777, eps), x)
+        for name, start in (("step", warm), ("jump", jump)):
             for solver, tail in ((gr, ""), (gr0, "_tail0")):
-                row = {"eps": eps, "nextra": C2P_NEXTRA if solver is gr else 0}
+                row = {"start": "the previous prims" if name == "step" else "the previous prims x (1 + 0.3 u)",
+                       "nextra": C2P_NEXTRA if solver is gr else 0}
                 for guess, key in (("previous", "plain"), ("learned", "learned")):
                     ts = []
-                    for r in range(4):
-                        work.copy_(p0)
+                    for rep in range(4):
+                        work.copy_(start)
                         ev[0].record(stream)
                         solver.cons2prim(cons, x, work, guess=guess, stats=False)
                         ev[1].record(stream)
                         ev[1].synchronize()
-                        if r:
+                        if rep:
                             ts.append(ev[0].elapsed_time(ev[1]))
-                    work.copy_(p0)
-                    rep = solver.cons2prim(cons, x, work, guess=guess)
+                    work.copy_(start)
+                    rep_ = solver.cons2prim(cons, x, work, guess=guess)
                     ms = statistics.median(ts)
                     gbs = C2P_BYTES * n / (ms / 1e3) / 1e9
-                    row[key] = {"ms": ms, "cells_per_s": n / (ms / 1e3), "iters_mean": rep["iters_mean"],
-                                "iters_max": rep["iters_max"], "n_fallback": rep["n_fallback"],
-                                "n_fail": rep["n_fail"], "hbm_gbs": gbs, "hbm_frac": gbs / hbm}
+                    row[key] = {"ms": ms, "cells_per_s": n / (ms / 1e3), "iters_mean": rep_["iters_mean"],
+                                "iters_max": rep_["iters_max"], "n_fallback": rep_["n_fallback"],
+                                "n_fail": rep_["n_fail"], "hbm_gbs": gbs, "hbm_frac": gbs / hbm}
                 row["learned_speedup"] = row["plain"]["ms"] / row["learned"]["ms"]
                 row["learned_iteration_ratio"] = row["learned"]["iters_mean"] / row["plain"]["iters_mean"]
                 out[name + tail] = row
-            del cons
-        del gr0
+        del gr0, jump, work
         out["bytes_per_cell"] = C2P_BYTES
         # CPU baseline: the oracle restatement (same tol/tail/cap), one core,
-        # on the first 50k cells of the warm case
+        # on 50k cells of the timed dump
         if not args.no_cpu_baseline:
             try:
                 from oracle import pyc2p
                 m = 50000
                 xs = x[:, :m].T.cpu().numpy().copy()
-                pp = p0[:, :m].T.cpu().numpy().copy()
-                cs = gr.prim2cons(gr.perturb(p0, 777, 1e-3), x)[:, :m].T.cpu().numpy().copy()
-                orc = pyc2p.C2POracle(metric=1, a=0.9, tol=C2P_TOL, nextra=C2P_NEXTRA, max_iter=C2P_MAXIT)
+                pp = warm[:, :m].T.cpu().numpy().copy()
+                cs = cons[:, :m].T.cpu().numpy().copy()
+                orc = pyc2p.C2POracle(metric=1, a=0.9, gam=1.3333333333333, rho_floor=0.0, p_floor=0.0,
+                                      tol=C2P_TOL, nextra=C2P_NEXTRA, max_iter=C2P_MAXIT)
                 t0 = time.perf_counter()
                 orc.cons2prim(cs, xs, pp)
                 dt = time.perf_counter() - t0
                 out["cpu_baseline"] = {"value": m / dt, "unit": "cells/s", "cores": 1, "kind": "port",
-                                       "sample": "%d cells of the warm case, oracle restatement" % m}
+                                       "sample": "%d cells of the timed dump, oracle restatement" % m}
             except Exception as ex:
                 out["cpu_baseline"] = {"value": None, "sample": "unavailable: %s" % ex}
+        del dumps, test
     del gr
     return out
 
@@ -1179,6 +1216,8 @@ def main():
     ap.add_argument("--c3-nz", type=int, default=96, help="z layers of the config-3 torus (96)")
     ap.add_argument("--only-config3", action="store_true",
                     help="run the config-3 leg alone (no headline line), e.g. for profiling")
+    ap.add_argument("--only-c2p", action="store_true",
+                    help="run the cons->prim leg alone (no headline line)")
     ap.add_argument("--no-config4", action="store_true",
                     help="skip the 40M-cell 3D MHD circumbinary (config 4) leg")
     args = ap.parse_args()
@@ -1191,6 +1230,11 @@ def main():
         args.no_cpu_baseline = True
         print(json.dumps({"config3_grtorus": config3_leg(args, local, torch.cuda.Stream(device=local))}),
               flush=True)
+        return
+    if args.only_c2p:
+        import torch
+        torch.cuda.set_device(local)
+        print(json.dumps({"c2p": c2p_leg(args, local, torch.cuda.Stream(device=local))}), flush=True)
         return
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -38,6 +38,7 @@ PLANETS = {"none": 0, "sun": 1, "cm2": 2, "binary_soft": 3, "circular": 4, "cm":
 INITIAL = {"kepler_noise": 0, "mhd_shear_noise": 1, "host": 2, "gr_torus_noise": 3}
 PREC_FP64, PREC_MIXED = 0, 1
 SCHED_KERNELS, SCHED_PERSISTENT = 0, 1
+GR_DUMP_ROWS = 21                 # DISCO_GR_DUMP_ROWS: cons / dV (9), warm-start prims (9), x (3)
 
 
 class DiscoError(RuntimeError):
@@ -116,6 +117,7 @@ def library():
         "disco_batch_kernel_times": (_I, [_P, C.POINTER(C.c_float), C.POINTER(C.c_char_p), _I, _IP]),
         "disco_batch_set_stream": (_I, [_P, _P]),
         "disco_batch_set_schedule": (_I, [_P, _I]),
+        "disco_batch_set_gr_dump": (_I, [_P, _P]),
         "disco_batch_get_schedule": (_I, [_P, _IP]),
         "disco_batch_debug_get": (_I, [_P, _I, _D]),
         "disco_read_par": (_I, [C.c_char_p, C.POINTER(Params), _IP]),
@@ -348,6 +350,22 @@ class Batch:
     @schedule.setter
     def schedule(self, sched):
         _check(library().disco_batch_set_schedule(self.h, int(sched)), "disco_batch_set_schedule")
+
+    def set_gr_dump(self, buf):
+        """GRMHD batches: each cons->prim of the following steps writes its
+        inputs (cons / dV, warm-start prims, x: GR_DUMP_ROWS x ncell float64,
+        a CUDA tensor on the batch's device, e.g. torch.zeros) for the real
+        cells into `buf`; None stops it.  The buffer must outlive its use."""
+        if buf is None:
+            ptr = None
+        else:
+            if tuple(buf.shape) != (GR_DUMP_ROWS, self.ncell) or not buf.is_contiguous() \
+                    or str(buf.dtype) != "torch.float64" or not buf.is_cuda:
+                raise ValueError("dump buffer must be a contiguous float64 CUDA tensor of shape (%d, %d)"
+                                 % (GR_DUMP_ROWS, self.ncell))
+            ptr = C.c_void_p(buf.data_ptr())
+        _check(library().disco_batch_set_gr_dump(self.h, ptr), "disco_batch_set_gr_dump")
+        self._gr_dump = buf
 
     def kernel_times(self, cap=64):
         """One instrumented step: [(kernel name, device ms), ...] in launch order."""

@@ -699,6 +699,24 @@ extern "C" int disco_batch_set_schedule(disco_batch *b, int sched){
    return DISCO_OK;
 }
 
+extern "C" int disco_batch_set_gr_dump(disco_batch *b, double *dev){
+   if( !b ) return DISCO_ERR_ARG;
+   if( !b->gr ) return DISCO_ERR_UNSUPPORTED;
+   CK(cudaSetDevice(b->device));
+   if( dev ){                       /* device memory of this batch's GPU */
+      cudaPointerAttributes at;
+      if( cudaPointerGetAttributes(&at, dev) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
+          at.device != b->device ){
+         cudaGetLastError();
+         return DISCO_ERR_ARG;
+      }
+   }
+   CK(cudaStreamSynchronize(b->stream));
+   if( b->graph ){ cudaGraphExecDestroy(b->graph); b->graph = NULL; }   /* recaptured on the next run */
+   b->vd.gr_dump = dev;
+   return DISCO_OK;
+}
+
 extern "C" int disco_batch_get_schedule(const disco_batch *b, int *sched){
    if( !b || !sched ) return DISCO_ERR_ARG;
    *sched = b->sched;

@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(CB) k_ct_line(ViewT<R> v){
          }else{                       /* diagonal: cells of list n before this one */
             int o = v.ann_off[an[n]], nn = v.ann_np[an[n]], I0n = v.I0[an[n]];
             /* both lists unrolled from I0: the count is near t nn / np */
-            cnt[n] = gallop_lb(0, nn, (int)(((long long)t*nn)/np), [&](int mid){
+            cnt[n] = gallop_lb(0, nn, __float2int_rz(__fdividef((float)t*(float)nn, (float)np)), [&](int mid){
                int s = I0n + mid; if( s >= nn ) s -= nn;
                double uy = v.piph[o + s];
                return !(n < m ? uy <= ux : uy < ux);

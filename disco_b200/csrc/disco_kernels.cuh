@@ -177,6 +177,10 @@ struct ViewT {
     * (k_gr_tables; NULL for the Newtonian modules) */
    GRAnn *gr_ann;
    Metric3 *gr_tr;
+   /* cons->prim inputs of the real cells, SoA [21][Ncell]: cons / dV (9), the
+    * warm-start prims (9), x (3), written by each GR c2p when set
+    * (disco_batch_set_gr_dump; NULL otherwise) */
+   double *gr_dump;
    R *ctE, *ctB, *pE, *pB, *pEr, *pBz, *fEt, *fBt, *fEphi;   /* edge arithmetic: R */
    unsigned char *fFlip;
    int *rk, *line_off;
@@ -444,7 +448,9 @@ __global__ void k_I0(ViewT<R> v){
 /* The first x in [lo, hi) where the monotone predicate p turns true (hi if
  * it never does) -- the binary search's answer -- found by galloping out
  * from a guess g and bisecting the bracket: a few probes when g is close,
- * as the position of a face or edge in the other annulus usually is. */
+ * as the position of a face or edge in the other annulus usually is.  The
+ * guess only sets where the search starts (computed in FP32, it may be off
+ * by one either way); the answer is the bisection's whatever it is. */
 template<class Pr>
 __device__ __forceinline__ int gallop_lb(int lo, int hi, int g, Pr p){
    if( g < lo ) g = lo;
@@ -519,7 +525,7 @@ __device__ __forceinline__ void faces_body(const ViewT<R> &v, int with_slopes, i
    int hi = dd < NA ? dd : NA;
    /* the diagonal's split: both annuli's edges are unrolled from I0, so face
     * dd lies near phi = dd/(NA+NB) of the turn in both */
-   lo = gallop_lb(lo, hi, (int)(((long long)dd*NA)/(NA+NB)), [&](int mid){
+   lo = gallop_lb(lo, hi, __float2int_rz(__fdividef((float)dd*(float)NA, (float)(NA+NB))), [&](int mid){
       int ia = IA + mid;       if( ia >= NA ) ia -= NA;
       int ib = IB + dd - mid - 1; if( ib >= NB ) ib -= NB;
       return v.piph[cA0+ia] > v.piph[cB0+ib];
@@ -1447,6 +1453,13 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
 #pragma unroll
             for( int q=0 ; q<Q ; ++q ) prim[q] = (double)v.prim[q*N + c];
             double x[3] = {centroid_r(rp, rm), 0.5*(phim+piph), centroid_z(zp, zm)};
+            if( v.gr_dump ){         /* the solve's inputs, as gr_cons2prim forms them */
+               double *o = v.gr_dump + c;
+#pragma unroll
+               for( int q=0 ; q<Q ; ++q ){ o[(size_t)q*N] = cons[q]/dV2; o[(size_t)(Q+q)*N] = prim[q]; }
+#pragma unroll
+               for( int m=0 ; m<3 ; ++m ) o[(size_t)(2*Q+m)*N] = x[m];
+            }
             gr_cons2prim(P, v.gr_ann[a].c, cons, prim, x, dV2);
          }else{
             cons2prim<Q,NC>(P, cons, prim, centroid_r(rp, rm), v.ann_om[a], dV2);

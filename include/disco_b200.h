@@ -340,6 +340,19 @@ int disco_batch_set_stream(disco_batch *b, void *stream);
 int disco_batch_set_schedule(disco_batch *b, int sched);
 int disco_batch_get_schedule(const disco_batch *b, int *sched);
 
+/* GRMHD batches: from the next step on, every cons->prim of the step writes
+ * its inputs for each real cell into dev (device memory of the batch's GPU,
+ * DISCO_GR_DUMP_ROWS x ncell doubles, row-major: cons / dV in rows 0-8, the
+ * warm-start prims -- the cell's prims before the solve -- in rows 9-17, the
+ * cell centre x in rows 18-20); rows of other cells are left as they were,
+ * and each substep overwrites the last.  These are exactly the arguments
+ * the step's noble2d solve sees (disco_gr_cons2prim with dV = 1 solves them
+ * to the same bits), so the plain solver's training pairs (include/disco_c2p.h)
+ * can be written from the states of the run itself.  dev = NULL stops it.
+ * Returns DISCO_ERR_UNSUPPORTED for a batch without HYDRO grmhd2. */
+#define DISCO_GR_DUMP_ROWS 21
+int disco_batch_set_gr_dump(disco_batch *b, double *dev);
+
 /*
  * Run one full step with a CUDA event between every kernel launch and
  * return each launch's device time: ms[i] and the kernel's name in

@@ -94,3 +94,45 @@ def test_grmhd_graph_run_equals_steps():
         b.close()
     for k in ("prim", "cons", "piph"):
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+def test_grmhd_c2p_dump_reproduces_the_step():
+    """disco_batch_set_gr_dump: the cons->prim inputs the step's last
+    substep solved, handed to the standalone solver (disco_gr_cons2prim with
+    the step's metric, gamma, floors, tol 1e-12, tail 10, cap 30), give the
+    step's prims of every real cell bit for bit -- so training pairs written
+    by the plain solver on these dumps are pairs of the run itself."""
+    import torch
+    from disco_b200.gr import GR
+    disk, g = case_disk("c3_grtorus")
+    b = db.Batch([disk], setup=False)
+    b.set_cells(g["s0_prim"], g["s0_cons"], g["s0_piph"], g["s0_dphi"], g["s0_wiph"], g["real"])
+    buf = torch.zeros((db.GR_DUMP_ROWS, b.ncell), dtype=torch.float64, device="cuda")
+    b.set_gr_dump(buf)
+    for _ in range(2):
+        b.timestep(b.mindt()[0])
+    b.sync()
+    st = b.get_cells()
+    b.set_gr_dump(None)
+    b.close()
+    r = disk.real == 1
+    idx = torch.nonzero(torch.from_numpy(r)).squeeze(1).cuda()
+    cons = buf[0:9][:, idx].contiguous()
+    prim = buf[9:18][:, idx].contiguous()
+    x = buf[18:21][:, idx].contiguous()
+    assert torch.isfinite(cons).all() and (x[0] > 0).all()
+    gr = GR(gamma_law=1.3333333333333, rho_floor=0.0, p_floor=0.0, M=1.0, a=0.0, metric="schw",
+            tol=1e-12, nextra=10, max_iter=30)
+    gr.cons2prim(cons, x, prim)
+    assert np.array_equal(prim.cpu().numpy().T, st["prim"][r])
+
+
+def test_grmhd_dump_needs_grmhd():
+    import torch
+    disk, _ = case_disk("c0_log16")
+    b = db.Batch([disk])
+    buf = torch.zeros((db.GR_DUMP_ROWS, b.ncell), dtype=torch.float64, device="cuda")
+    with pytest.raises(db.DiscoError) as e:
+        b.set_gr_dump(buf)
+    assert e.value.status == 3
+    b.close()
