@@ -96,8 +96,7 @@ def build_variants(cache=DEFAULT_CACHE, mbs=DEFAULT_MB, cbs=(128,), verbose=Fals
         objs = []
         for name in tuned:
             obj = os.path.join(vdir, name + ".o")
-            fmad = "--fmad=true" if name.endswith("_mixed.cu") else "--fmad=false"
-            jobs.append([nvcc] + native.ARCH + ["-O3", "-lineinfo", fmad, "-std=c++17",
+            jobs.append([nvcc] + native.ARCH + ["-O3", "-lineinfo"] + native.precision_flags(name) + ["-std=c++17",
                                                 "-Xcompiler", "-fPIC"] + defs + inc +
                         ["-c", os.path.join(CSRC, name), "-o", obj])
             objs.append(obj)
