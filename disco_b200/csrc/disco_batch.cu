@@ -350,13 +350,10 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    int ct = params[0].CT ? mods->ct_mode : 0;
    for( int d=0 ; d<ndisk ; ++d ) if( (params[d].CT ? 1 : 0) != (params[0].CT ? 1 : 0) ) return DISCO_ERR_ARG;
    if( params[0].CT ){
-      /* CT_MODE 1 stores no z-face fluxes, so it is built for 2D disks; in 3D
-       * (CT_MODE 2) avg_Efields' z-pole branch (NgZa or NgZb = 0) is not */
+      /* CT_MODE 1 stores no z-face fluxes, so it is built for 2D disks */
       if( !mhd || mods->ct_mode < 1 ) return DISCO_ERR_UNSUPPORTED;
-      for( int d=0 ; d<ndisk ; ++d ){
-         if( Nz[d] > 1 && (mods->ct_mode != 2 || Ng[4*d+2] == 0 || Ng[4*d+3] == 0) )
-            return DISCO_ERR_UNSUPPORTED;
-      }
+      for( int d=0 ; d<ndisk ; ++d )
+         if( Nz[d] > 1 && mods->ct_mode != 2 ) return DISCO_ERR_UNSUPPORTED;
    }
    if( mods->boundary < DISCO_BC_FIXED || mods->boundary > DISCO_BC_HORIZON3D )
       return DISCO_ERR_UNSUPPORTED;
@@ -647,6 +644,20 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       if( ct == 2 ){
          v.pEr = ralloc(N); v.pBz = ralloc(N);
          v.fEphi = ralloc(face);
+         /* avg_Efields' z-pole branch: the annuli of a z boundary without
+          * ghosts (bottom layer when NgZa = 0, top when NgZb = 0) */
+         for( int d=0 ; d<ndisk ; ++d ){
+            const DiskParams &D = b->dparams[d];
+            if( D.Nz < 2 ) continue;
+            for( int j=0 ; j<D.Nr ; ++j ){
+               if( D.NgZa == 0 ) b->zpole.push_back(make_int2(D.ann0 + j, 0));
+               if( D.NgZb == 0 ) b->zpole.push_back(make_int2(D.ann0 + j + D.Nr*(D.Nz-1), 1));
+            }
+         }
+         if( !b->zpole.empty() ){
+            v.ctPole = dalloc<double>(b, N);
+            b->d_zpole = dupload(b, b->zpole);
+         }
          if( b->any_3d ){
             v.rk = dalloc<int>(b, 4*N);
             v.lineX = dalloc<double>(b, (size_t)b->line_ne);

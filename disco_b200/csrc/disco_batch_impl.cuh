@@ -33,6 +33,8 @@ struct disco_batch {
    std::vector<int> zg_off;             /* layer groups: r layers, then z layers */
    int2 *d_zg_pairs;
    size_t zg_smem;                      /* dynamic shared memory of k_zerograd */
+   std::vector<int2> zpole;             /* 3D CT z-pole annuli (annulus, 0 bottom / 1 top) */
+   int2 *d_zpole;
    int nq;
    std::vector<disco_params> params;
    /* topology (host) */
@@ -211,6 +213,9 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
       if( b->ct ){                  /* onestep.c:140-146 and 160-167 */
          k_ct_edges<R><<<ncb, CB, 0, s>>>(v);                           mark(b, "k_ct_edges");
          k_ct_faces<R><<<nfb, FB, 0, s>>>(v);                           mark(b, "k_ct_faces");
+         if( !b->zpole.empty() ){
+            k_ct_zpole<R><<<(unsigned)b->zpole.size(), CB, 0, s>>>(v, b->d_zpole); mark(b, "k_ct_zpole");
+         }
          if( b->ct == 2 && b->any_3d ){
             k_ct_line<R><<<ncb, CB, 0, s>>>(v);                         mark(b, "k_ct_line");
          }

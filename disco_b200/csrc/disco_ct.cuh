@@ -43,8 +43,10 @@
  * faces outside the CT flux ranges) are zero here; they reach only slots of
  * ghost cells' faces that no real cell reads.  The r-pole branches of
  * avg_Efields (NgRa/NgRb = 0) write edges that no face owns, so they are not
- * evaluated; the z-pole branches do reach owned edges, so CT in 3D needs
- * z ghost layers (checked at create).
+ * evaluated; the z-pole branches (NgZa/NgZb = 0 in 3D) reach the z faces the
+ * bottom layer's cells own above them and the top layer's own below them:
+ * k_ct_faces keeps those faces' E per owner and k_ct_zpole writes their X
+ * from the annulus mean.
  */
 #pragma once
 #include "disco_kernels.cuh"
@@ -205,8 +207,45 @@ __global__ void __launch_bounds__(FB) k_ct_faces(ViewT<R> v){
       dl = rj[j]-rj[j-1];                         /* z-face dl = dr */
    }
    double dt = v.ds[d].dt*v.dtfac;
-   v.fX[f] = (double)Ef*dl*dt;
+   /* avg_Efields' z-pole branch (bfields.c:580-617): without z ghosts the
+    * bottom layer's E[5] and the top layer's E[4] become their annulus's
+    * mean and B 0 -- the owner's value is kept for k_ct_zpole, which writes
+    * these faces' X */
+   if( zf && v.ctPole && ((lr == 0 && k == 0 && P.NgZa == 0) ||
+                          (lr == 1 && k+1 == P.Nz-1 && P.NgZb == 0)) ){
+      v.ctPole[o] = (double)fE;
+   }else{
+      v.fX[f] = (double)Ef*dl*dt;
+   }
    raise_err(v, err);
+}
+
+/* The z-pole average (bfields.c:580-617) of pole annulus pl[blockIdx.x]
+ * (x: annulus, y: 0 the bottom layer, its cells' upper faces; 1 the top
+ * layer, their lower faces): E = the sum of the cells' owned-face E in cell
+ * order over Np, B = 0, so the advective term vanishes and each owned face
+ * takes X = E dl dt. */
+template<class R>
+__global__ void __launch_bounds__(CB) k_ct_zpole(ViewT<R> v, const int2 *pl){
+   __shared__ double s_E;
+   const int2 pa = pl[blockIdx.x];
+   const int a = pa.x, top = pa.y;
+   const int np = v.ann_np[a], c0 = v.ann_off[a];
+   const int d = v.ann_disk[a];
+   const DiskParams &P = v.dp[d];
+   if( threadIdx.x == 0 ){
+      double E = 0.0;
+      for( int i=0 ; i<np ; ++i ) E += v.ctPole[c0 + i];
+      s_E = E/np;
+   }
+   __syncthreads();
+   const int j = v.ann_j[a];
+   const double *rj = v.rj + P.rj0 + 1;
+   const double dl = rj[j]-rj[j-1];                   /* z-face dl = dr */
+   const double dt = v.ds[d].dt*v.dtfac;
+   const R E = (R)s_E;
+   const int *own = top ? v.consZR : v.consZL;
+   for( int i=threadIdx.x ; i<np ; i+=blockDim.x ) v.fX[own[c0 + i]] = (double)E*dl*dt;
 }
 
 /* get_which4 (bfields.c:834-885): which of four phi edges is smallest (mode

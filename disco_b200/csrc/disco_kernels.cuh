@@ -182,6 +182,9 @@ struct ViewT {
     * (disco_batch_set_gr_dump; NULL otherwise) */
    double *gr_dump;
    R *ctE, *ctB, *pE, *pB, *pEr, *pBz, *fEt, *fBt, *fEphi;   /* edge arithmetic: R */
+   /* 3D CT with a z boundary without ghosts: each pole cell's owned z-face
+    * E (avg_Efields' z-pole average, k_ct_zpole); NULL otherwise */
+   double *ctPole;
    unsigned char *fFlip;
    int *rk, *line_off;
    double *lineX;
@@ -279,7 +282,9 @@ __device__ __forceinline__ void begin_body(const ViewT<R> &v, double RK, int fir
       double rk;
       if( first ){ rk = cq; v.RKcons[q*N + c] = cq; }
       else rk = v.RKcons[q*N + c];
-      v.cons[q*N + c] = (1.-RK)*cq + RK*rk;
+      /* with RK = 0 (the first substep) the average returns a finite cq
+       * bit for bit, so the store is skipped */
+      if( !(RK == 0.0 && isfinite(cq)) ) v.cons[q*N + c] = (1.-RK)*cq + RK*rk;
       if constexpr ( sizeof(R) != sizeof(double) ){
          /* the carry belongs to cons; averaged with it (RKcons keeps none) */
          if( !first ) v.ccarry[q*N + c] = (float)((1.-RK)*(double)v.ccarry[q*N + c]);
@@ -294,7 +299,7 @@ __device__ __forceinline__ void begin_body(const ViewT<R> &v, double RK, int fir
             double rk;
             if( first ){ rk = ph; v.RKPhi[s*N + c] = ph; }
             else rk = v.RKPhi[s*N + c];
-            v.Phi[s*N + c] = (1.-RK)*ph + RK*rk;
+            if( !(RK == 0.0 && isfinite(ph)) ) v.Phi[s*N + c] = (1.-RK)*ph + RK*rk;
          }
       }
    }

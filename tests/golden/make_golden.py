@@ -169,6 +169,18 @@ CASES = {
                                       "NoBC_Rmin": 1, "Init_Par2": 1, "Init_Par4": 10.0,
                                       "Constrained_Transport": 1, "Init_Par5": 20.0}, 5),
     "c3_grhorizon": ("c3_grhorizon", {"Num_R": 16, "Num_Z": 8, "R_Min": 0.5, "NoBC_Rmin": 1}, 5),
+    # 3D constrained transport with z boundaries without ghost layers
+    # (NoBC_Zmin / NoBC_Zmax 1): avg_Efields' z-pole branch (bfields.c:580-617)
+    # averages the bottom layer's E[5] and the top layer's E[4] over each
+    # annulus; libm-free rigid HLLD with zerograd r ghosts, and with the polar
+    # module down to the axis (both poles of the domain at once)
+    "c1_ct3d_zpole": ("c1_mhd3d_nograv", {"Num_R": 8, "Num_Z": 6, "Init_Par2": 1, "Init_Par4": 10.0,
+                                          "Constrained_Transport": 1, "Init_Par5": 20.0,
+                                          "Init_Par6": 0.05, "NoBC_Zmin": 1, "NoBC_Zmax": 1}, 6),
+    "c1_polar3d_zpole": ("c1_polar3d", {"Num_R": 8, "Num_Z": 6, "R_Min": 0.0, "R_Max": 2.0,
+                                        "NoBC_Rmin": 1, "Init_Par2": 1, "Init_Par4": 10.0,
+                                        "Constrained_Transport": 1, "Init_Par5": 20.0,
+                                        "NoBC_Zmin": 1, "NoBC_Zmax": 1}, 5),
 }
 
 # the in.par template each module configuration starts from

@@ -33,8 +33,13 @@ pytestmark = pytest.mark.gpu
 
 # c4_binary3d: config 4's module set with the softened binary
 # (Planets/binary_soft.c in the reference build)
-CT_CASES = ["c1_ct2d", "c1_ct_rigid", "c1_ct_hll_fe", "c1_ct3d", "c1_ct3d_rigid", "c4_binary3d"]
-CT_TOL = {"c1_ct2d": 1e-11, "c1_ct_hll_fe": 1e-11, "c1_ct3d": 1e-11, "c4_binary3d": 1e-11}
+# c1_ct3d_zpole, c1_polar3d_zpole: 3D CT with z boundaries without ghost
+# layers (avg_Efields' z-pole average, k_ct_zpole); the polar one also down
+# to the axis (polar sources call sin: 1e-12)
+CT_CASES = ["c1_ct2d", "c1_ct_rigid", "c1_ct_hll_fe", "c1_ct3d", "c1_ct3d_rigid", "c4_binary3d",
+            "c1_ct3d_zpole", "c1_polar3d_zpole"]
+CT_TOL = {"c1_ct2d": 1e-11, "c1_ct_hll_fe": 1e-11, "c1_ct3d": 1e-11, "c4_binary3d": 1e-11,
+          "c1_polar3d_zpole": 1e-12}
 
 
 def _from_golden(disk, g):
