@@ -102,7 +102,8 @@ static void fill_disk_params(DiskParams &D, const disco_params &p, const disco_m
    D.ic_gr.M = p.metricPar[2]; D.ic_gr.a = D.gr_a;
    D.ic_gr.rmin = p.rmin; D.ic_gr.rmax = p.rmax; D.ic_gr.zmin = p.zmin; D.ic_gr.zmax = p.zmax;
    D.ic_gr.phimax = p.phimax;
-   D.bc_horizon = m.boundary == DISCO_BC_HORIZON ? 8 : m.boundary == DISCO_BC_HORIZON3D ? 9 : 0;
+   D.bc_horizon = m.boundary == DISCO_BC_HORIZON ? 8 : m.boundary == DISCO_BC_HORIZON3D ? 9 :
+                  m.boundary == DISCO_BC_HORIZON_BIN ? 10 : 0;
    D.ic_mhd.seed = (uint64_t)(int64_t)p.initPar0; D.ic_mhd.amp = p.initPar[1];
    D.ic_mhd.cs = p.initPar[3]; D.ic_mhd.beta = p.initPar[4]; D.ic_mhd.gam = p.Adiabatic_Index;
    D.ic_mhd.rmin = p.rmin; D.ic_mhd.rmax = p.rmax; D.ic_mhd.zmin = p.zmin; D.ic_mhd.zmax = p.zmax;
@@ -355,12 +356,13 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       for( int d=0 ; d<ndisk ; ++d )
          if( Nz[d] > 1 && mods->ct_mode != 2 ) return DISCO_ERR_UNSUPPORTED;
    }
-   if( mods->boundary < DISCO_BC_FIXED || mods->boundary > DISCO_BC_HORIZON3D )
+   if( mods->boundary < DISCO_BC_FIXED || mods->boundary > DISCO_BC_HORIZON_BIN )
       return DISCO_ERR_UNSUPPORTED;
-   /* polar3d, horizon and horizon3d set the outer r and the z ghosts only
-    * (Boundary/polar3d.c, horizon.c, horizon3d.c): grids without inner ghosts */
+   /* polar3d, horizon, horizon3d and horizon_bin set the outer r and the z
+    * ghosts only (Boundary/polar3d.c, horizon.c, horizon3d.c,
+    * horizon_bin.c): grids without inner ghosts */
    if( mods->boundary == DISCO_BC_POLAR3D || mods->boundary == DISCO_BC_HORIZON ||
-       mods->boundary == DISCO_BC_HORIZON3D )
+       mods->boundary == DISCO_BC_HORIZON3D || mods->boundary == DISCO_BC_HORIZON_BIN )
       for( int d=0 ; d<ndisk ; ++d ) if( Ng[4*d+0] != 0 ) return DISCO_ERR_UNSUPPORTED;
    /* Boundary/polar.c sets the outer r and the z ghosts only: it is meant
     * for a grid whose inner edge is the axis (NoBC_Rmin 1, no inner ghosts);
@@ -397,7 +399,8 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->bc_fixed = mods->boundary == DISCO_BC_FIXED ? 1 : mods->boundary == DISCO_BC_FIXED3D ? 2 :
                  mods->boundary == DISCO_BC_POLAR ? 3 :
                  (mods->boundary == DISCO_BC_ACCRETE3D || mods->boundary == DISCO_BC_POLAR3D) ? 6 :
-                 mods->boundary == DISCO_BC_HORIZON ? 8 : mods->boundary == DISCO_BC_HORIZON3D ? 9 : 0;
+                 mods->boundary == DISCO_BC_HORIZON ? 8 : mods->boundary == DISCO_BC_HORIZON3D ? 9 :
+                 mods->boundary == DISCO_BC_HORIZON_BIN ? 10 : 0;
    /* modules built from boundary_functions.c's zero-gradient copies: all four
     * sides (zerograd; with the diode outflow3d, zerograd_omk), or the inner r
     * side only (accrete3d, whose other sides are fixed) */
@@ -630,6 +633,8 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       v.gr_tr = dalloc<Metric3>(b, v.Ntr > 0 ? v.Ntr : 1);
    }
    v.topo = dalloc<int>(b, 1);
+   if( mods->boundary == DISCO_BC_HORIZON_BIN )        /* the sticky not-real flags (zeroed) */
+      v.xflag = dalloc<unsigned char>(b, N);
    if( ct ){
       v.ct = ct;
       v.nfs = b->nfs;

@@ -181,6 +181,9 @@ struct ViewT {
     * warm-start prims (9), x (3), written by each GR c2p when set
     * (disco_batch_set_gr_dump; NULL otherwise) */
    double *gr_dump;
+   /* horizon_bin: a cell once excised stays out of the dt minimum (the
+    * reference's real flag is never set back); NULL for other modules */
+   unsigned char *xflag;
    R *ctE, *ctB, *pE, *pB, *pEr, *pBz, *fEt, *fBt, *fEphi;   /* edge arithmetic: R */
    /* 3D CT with a z boundary without ghosts: each pole cell's owned z-face
     * E (avg_Efields' z-pole average, k_ct_zpole); NULL otherwise */
@@ -1373,13 +1376,57 @@ __device__ __forceinline__ bool horizon_cut(const DiskParams &P, int bc, int j, 
    }
    return false;
 }
+/* Boundary/horizon_bin.c:83-171: cell (j, k) at phi inside one of the two
+ * excision spheres of the module's fixed binary (M = 1, separation 10, q = 1:
+ * centres at x = 5 and x = -5 in the plane, radius 0.8 r_H of each member),
+ * tested in the module's order with its nearest-edge radius rc and z; the
+ * per-annulus pre-checks first, then the cell's own distance. */
+__device__ __forceinline__ bool horizon_bin_cut(const DiskParams &P, int j, int k, const double *rj,
+                                                const double *zk, double phi){
+   const double M = 1.0, a = 1.0e1, q = 1.0;
+   const double M1 = M/(1+q), M2 = q*M/(1+q);
+   const double a1 = q*a/(1+q), a2 = -a/(1+q);
+   const double cuts[2] = {0.8*(2*M1), 0.8*(2*M2)};
+   const double zp = zk[k], zm = zk[k-1];
+   const double zc = fabs(zp) < fabs(zm) ? zp : zm;
+   const double rp = rj[j], rm = rj[j-1];
+   for( int s=0 ; s<2 ; ++s ){
+      const double cut = cuts[s];
+      /* the member's centre at x = as; its |x| = xs */
+      const double as = s == 0 ? a1 : a2, xs = s == 0 ? a1 : -a2;
+      if( !(rj[-1] < xs+cut && rj[P.Nr-1] > xs-cut && zk[-1] < cut && zk[P.Nz-1] > -cut) ) continue;
+      if( fabs(zc) > cut && P.Nz > 1 ) continue;
+      double rc, dr;
+      if( s == 0 ){ rc = fabs(rp-a1) < fabs(rm-a1) ? rp : rm; dr = rc-a1; }
+      else        { rc = fabs(rp+a2) < fabs(rm+a2) ? rp : rm; dr = rc+a2; }
+      if( (dr*dr+zc*zc > cut*cut && P.Nz > 1) || fabs(dr) > cut ) continue;
+      double sn, cs;
+      sincos(phi, &sn, &cs);
+      const double xc = rc*cs, yc = rc*sn;
+      double d2;
+      if( P.Nz > 1 ) d2 = (xc-as)*(xc-as) + yc*yc + zc*zc;
+      else           d2 = (xc-as)*(xc-as) + yc*yc;
+      if( d2 < cut*cut ) return true;
+   }
+   return false;
+}
+
+/* Whether a horizon module re-initialises cell (j, k, phi) and marks it not
+ * real: horizon / horizon3d by annulus, horizon_bin by cell. */
+__device__ __forceinline__ bool cell_excised(const DiskParams &P, int bc, int j, int k, const double *rj,
+                                             const double *zk, double piph, double dphi){
+   if( bc == 10 ) return horizon_bin_cut(P, j, k, rj, zk, piph - .5*dphi);
+   return (bc == 8 || bc == 9) && horizon_cut(P, bc, j, k, rj, zk);
+}
+
 template<int Q, int NC>
 __device__ __forceinline__ bool fixed_ghost_init(const DiskParams &P, int bc, int j, int k,
                                                  const double *rj, const double *zk,
                                                  double piph, double dphi, double *prim){
    bool rghost = j < P.NgRa || j >= P.Nr - P.NgRb;
    bool zghost = k < P.NgZa || k >= P.Nz - P.NgZb;
-   if( bc == 8 && (j >= P.Nr - P.NgRb || zghost || horizon_cut(P, bc, j, k, rj, zk)) ){
+   if( (bc == 8 && (j >= P.Nr - P.NgRb || zghost || horizon_cut(P, bc, j, k, rj, zk))) ||
+       (bc == 10 && (j >= P.Nr - P.NgRb || zghost || horizon_bin_cut(P, j, k, rj, zk, piph - .5*dphi))) ){
       double x[3] = { .5*(rj[j]+rj[j-1]), piph - .5*dphi, .5*(zk[k]+zk[k-1]) };
       initial<Q,NC>(P, prim, x);
       return true;
@@ -1471,10 +1518,12 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
          }
          /* a horizon module then re-initialises the excised annuli (after
           * calc_prim, as boundary_trans follows it) and getmindt skips them */
-         if( (bc == 8 || bc == 9) && horizon_cut(P, bc, j, k, rj, zk) ){
+         if( cell_excised(P, bc, j, k, rj, zk, piph, dphi) ){
             fixed_ghost_init<Q,NC>(P, bc, j, k, rj, zk, piph, dphi, prim);
             excised = true;
+            if( v.xflag ) v.xflag[c] = 1;   /* horizon_bin: not real from now on */
          }
+         if( v.xflag && v.xflag[c] ) excised = true;
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ){
             R pq = (R)prim[q];
@@ -2092,9 +2141,12 @@ __global__ void __launch_bounds__(CB) k_setup(ViewT<R> v, int bc){
          if( !v.ct ) cons2prim<Q,NC>(P, cons, prim, r, om, dV);
       }
       /* main.c's boundary pass: a horizon module re-initialises the
-       * excised annuli's prims (their cons stay set-up's) */
-      if( P.bc_horizon && horizon_cut(P, P.bc_horizon, j, k, rj, zk) )
-         fixed_ghost_init<Q,NC>(P, bc, j, k, rj, zk, piph, dphi, prim);
+       * excised cells' prims (their cons stay set-up's) */
+      {
+         const bool ex = P.bc_horizon && cell_excised(P, P.bc_horizon, j, k, rj, zk, piph, dphi);
+         if( ex ) fixed_ghost_init<Q,NC>(P, bc, j, k, rj, zk, piph, dphi, prim);
+         if( v.xflag ) v.xflag[c] = ex ? 1 : 0;
+      }
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){ v.prim[q*N+c] = (R)prim[q]; v.cons[q*N+c] = cons[q]; }
    }else{
@@ -2177,8 +2229,11 @@ __global__ void __launch_bounds__(CB) k_restart(ViewT<R> v, int bc){
          prim2cons<Q,NC,double>(P, prim, cons, r, om, dV);
          cons2prim<Q,NC>(P, cons, prim, r, om, dV);
       }
-      if( P.bc_horizon && horizon_cut(P, P.bc_horizon, j, k, rj, zk) )
-         fixed_ghost_init<Q,NC>(P, bc, j, k, rj, zk, piph, dphi, prim);
+      {
+         const bool ex = P.bc_horizon && cell_excised(P, P.bc_horizon, j, k, rj, zk, piph, dphi);
+         if( ex ) fixed_ghost_init<Q,NC>(P, bc, j, k, rj, zk, piph, dphi, prim);
+         if( v.xflag ) v.xflag[c] = ex ? 1 : 0;     /* setupCells marks the real cells anew */
+      }
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ){ v.prim[q*N+c] = (R)prim[q]; v.cons[q*N+c] = cons[q]; }
    }else{
@@ -2281,8 +2336,9 @@ __global__ void __launch_bounds__(CB) k_mindt(ViewT<R> v){
    bool real = j >= P.NgRa && j < P.Nr - P.NgRb && k >= P.NgZa && k < P.Nz - P.NgZb;
    double dtc = 1.0e300;
    int err = 0;
-   bool excised = P.bc_horizon &&
-                  horizon_cut(P, P.bc_horizon, j, k, v.rj + P.rj0 + 1, v.zk + P.zk0 + 1);
+   bool excised = P.bc_horizon && i < np &&
+                  (v.xflag ? v.xflag[c0 + i] != 0
+                           : horizon_cut(P, P.bc_horizon, j, k, v.rj + P.rj0 + 1, v.zk + P.zk0 + 1));
    if( i < np && real && !excised ){
       int c = c0 + i;
       const double *rj = v.rj + P.rj0 + 1;

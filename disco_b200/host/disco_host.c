@@ -156,6 +156,7 @@ int disco_read_opt(const char *path, disco_modules *m){
    else if( !strcmp(v, "polar3d") ) m->boundary = DISCO_BC_POLAR3D;
    else if( !strcmp(v, "horizon") ) m->boundary = DISCO_BC_HORIZON;
    else if( !strcmp(v, "horizon3d") ) m->boundary = DISCO_BC_HORIZON3D;
+   else if( !strcmp(v, "horizon_bin") ) m->boundary = DISCO_BC_HORIZON_BIN;
    else return DISCO_ERR_UNSUPPORTED;
    if( opt_value(path, "PLANETS", v, sizeof v) ) return DISCO_ERR_ARG;
    if( !strcmp(v, "none") ) m->planets = DISCO_PLANETS_NONE;

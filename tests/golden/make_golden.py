@@ -177,6 +177,17 @@ CASES = {
     "c1_ct3d_zpole": ("c1_mhd3d_nograv", {"Num_R": 8, "Num_Z": 6, "Init_Par2": 1, "Init_Par4": 10.0,
                                           "Constrained_Transport": 1, "Init_Par5": 20.0,
                                           "Init_Par6": 0.05, "NoBC_Zmin": 1, "NoBC_Zmax": 1}, 6),
+    # horizon_bin (Boundary/horizon_bin.c): two excision spheres of radius 0.8
+    # at x = +-5 -- cells inside are re-initialised each substep and, once
+    # excised, stay out of the dt minimum (the reference's real flag is never
+    # set back); rigid rotation moves cells through them.  2D and 3D hydro,
+    # no inner ghosts (the module sets none); the test is per cell with cos
+    # and sin of the cell's phi
+    "c0_hbin": ("c0_hbin", {"Num_R": 24, "R_Min": 3.5, "R_Max": 7.0, "NoBC_Rmin": 1, "Log_Zoning": 0,
+                            "Init_Par2": 1, "Init_Par1": 0.05, "Energy_Omega": 0, "Mach_Number": 5.0}, 8),
+    "c0_hbin3d": ("c0_hbin", {"Num_R": 16, "Num_Z": 6, "Z_Min": -0.6, "Z_Max": 0.6, "R_Min": 3.5,
+                              "R_Max": 7.0, "NoBC_Rmin": 1, "Log_Zoning": 0, "Init_Par2": 1,
+                              "Init_Par1": 0.05, "Energy_Omega": 0, "Mach_Number": 5.0}, 5),
     "c1_polar3d_zpole": ("c1_polar3d", {"Num_R": 8, "Num_Z": 6, "R_Min": 0.0, "R_Max": 2.0,
                                         "NoBC_Rmin": 1, "Init_Par2": 1, "Init_Par4": 10.0,
                                         "Constrained_Transport": 1, "Init_Par5": 20.0,
@@ -191,7 +202,8 @@ BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": 
             "c1_omk3d": "c1_mhd3d", "c1_accrete3d": "c1_mhd3d", "c0_rigid_zg": "c0_kepler2d",
             "c0_circular": "c0_kepler2d", "c0_cm": "c0_kepler2d", "c0_diag_euler": "c0_kepler2d",
             "c0_diag_euler3d": "c0_kepler2d", "c1_diag_mhdmri": "c1_mhd2d", "c3_grtorus": "c3_grtorus", "c4_binary3d": "c4_binary3d",
-            "c0_horizon3d": "c0_kepler2d", "c1_polar3dbc": "c1_mhd3d", "c3_grhorizon": "c3_grtorus"}
+            "c0_horizon3d": "c0_kepler2d", "c1_polar3dbc": "c1_mhd3d", "c3_grhorizon": "c3_grtorus",
+            "c0_hbin": "c0_kepler2d"}
 
 
 def par_text(cfg_par, overrides):

@@ -17,6 +17,11 @@ fixtures depend on no libm call except where noted):
   with CT.
 - polar3d: fixed outer r and z (set_cell_init) on an axis grid, 3D MHD with
   CT.
+- horizon_bin: outer r and z ghosts at the midpoint, and every cell inside
+  one of two spheres of radius 0.8 at x = +-5 re-initialised there each
+  substep, out of the dt minimum from its first excision on (the
+  reference's real flag is never set back); 2D and 3D hydro.  The test is
+  per cell with sin and cos of the cell's phi (libm).
 - horizon3d: polar3d's ghosts plus boundary_fixed_horizon
   (boundary_functions.c:622-656): every annulus whose outer corner lies
   inside R = 1 is re-initialised by set_cell_init each substep and left out
@@ -35,7 +40,7 @@ from helpers import case_disk, observed_slots, par_with, rel_l1, rel_l1_cols
 pytestmark = pytest.mark.gpu
 
 POLAR = ["c0_polar", "c1_polar_ct", "c1_polar3d", "c1_polar3dbc", "c0_horizon3d"]
-CASES = POLAR + ["c0_outflow3d", "c1_omk3d", "c1_accrete3d"]
+CASES = POLAR + ["c0_outflow3d", "c1_omk3d", "c1_accrete3d", "c0_hbin", "c0_hbin3d"]
 TOL = 1e-12
 
 

@@ -56,7 +56,8 @@ def test_grid_and_phi_match_reference(case):
 
 
 @pytest.mark.parametrize("case,module", [("c0_horizon3d", "horizon3d"), ("c1_polar3dbc", "polar3d"),
-                                         ("c3_grhorizon", "horizon")])
+                                         ("c3_grhorizon", "horizon"), ("c0_hbin", "horizon_bin"),
+                                         ("c0_hbin3d", "horizon_bin")])
 def test_axis_and_horizon_modules_parse(case, module):
     """The excising boundary modules read from Makefile_opt.in; the grid
     matches the reference, whose real flag also drops the excised annuli."""
