@@ -768,14 +768,26 @@ def c2p_leg(args, local, stream):
         gr.mlp_init(3)
         gr.mlp_fit_norm(pairs)
         steps, batch = 3000, 8192
+        # the CUDA-core backward first (timing only), then the tensor-core
+        # (tcgen05) one whose network is used below
+        gr.mlp_backend("cuda")
+        ev[0].record(stream)
+        hist_c = gr.mlp_train(pairs, steps=steps, batch=batch, lr=2e-3, seed=9)
+        ev[1].record(stream)
+        ev[1].synchronize()
+        ms_cuda = ev[0].elapsed_time(ev[1])
+        gr.mlp_init(3)
+        gr.mlp_fit_norm(pairs)
+        gr.mlp_backend("tensor")
         ev[0].record(stream)
         hist = gr.mlp_train(pairs, steps=steps, batch=batch, lr=2e-3, seed=9)
         ev[1].record(stream)
         ev[1].synchronize()
         out["train"] = {"pairs": int(pairs.shape[0]), "source": "the plain solver on the step's own inputs "
                         "of the first %d dumped steps" % (C2P_DUMPS - 1), "steps": steps, "batch": batch,
-                        "ms": ev[0].elapsed_time(ev[1]), "loss_first": float(hist[:10].mean()),
-                        "loss_last": float(hist[-50:].mean())}
+                        "backend": "tcgen05 tensor cores", "ms": ev[0].elapsed_time(ev[1]),
+                        "loss_first": float(hist[:10].mean()), "loss_last": float(hist[-50:].mean()),
+                        "cuda_cores_ms": ms_cuda, "cuda_cores_loss_last": float(hist_c[-50:].mean())}
         del pairs
         # the same network in a solver without the tail (tol only)
         gr0 = GR(device=local, gamma_law=1.3333333333333, rho_floor=0.0, p_floor=0.0, M=1.0, a=0.9,

@@ -14,10 +14,13 @@
  * tensor-core operands with FP32 accumulation (mma.sync m16n8k16; a warp
  * evaluates its 32 cells as two 16-row tiles, the FP32 accumulator fragment
  * of one layer becoming, packed to BF16, the A fragment of the next).
- * Training: the same forward, then the backward on the FP32 CUDA cores over
- * 128-sample groups held in shared memory (per-thread register accumulators
- * for dW, one atomic per weight per block), then Adam on FP32 master weights
- * which writes the BF16 copy the kernels read.
+ * Training: by default the forward and backward contractions of each
+ * 128-sample group on the tensor cores through tcgen05.mma with tensor-
+ * memory accumulators (mlp_tcgen05.cuh); or the same forward and the
+ * backward on the FP32 CUDA cores over 128-sample groups held in shared
+ * memory (per-thread register accumulators for dW, one atomic per weight
+ * per block).  Then Adam on FP32 master weights, which writes the BF16
+ * copy the kernels read.
  */
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
@@ -512,6 +515,8 @@ k_mlp_grad(const MlpPacked *__restrict__ mlp, long n, const float *__restrict__ 
    if( lane == 0 && lsum != 0.0 ) atomicAdd(loss, lsum/(2.0*(double)nsamp));
 }
 
+#include "mlp_tcgen05.cuh"
+
 /* Write a parameter into the packed image (W rounded to BF16) */
 __device__ __forceinline__ void pack_param(MlpPacked *P, int p, float w){
    if( p < OFF_B1 )      P->W1[p >> 3][p & 7] = __float2bfloat16_rn(w);
@@ -585,6 +590,8 @@ struct disco_gr {
    float h_norm[MLP_NNORM];
    bool have_mlp;
    long adam_t;
+   int backend;               /* DISCO_MLP_TENSOR or DISCO_MLP_CUDA_CORES */
+   int *d_err;                /* a tensor-core wait ran out */
    int c2p_blocks[4];
    std::string err;
 };
@@ -635,6 +642,8 @@ int disco_gr_create(int device, const disco_gr_params *p, disco_gr **out){
    h->stream = 0;
    h->have_mlp = false;
    h->adam_t = 0;
+   h->backend = DISCO_MLP_TENSOR;
+   h->d_err = nullptr;
    int rc = DISCO_OK;
    do{
       if( cudaSetDevice(device) != cudaSuccess ){ rc = DISCO_ERR_CUDA; break; }
@@ -653,6 +662,10 @@ int disco_gr_create(int device, const disco_gr_params *p, disco_gr **out){
       if( (rc = c2p_setup_attr<true, true>(h, 3)) ) break;
       if( cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(TrainSmem)) != cudaSuccess ){ rc = DISCO_ERR_CUDA; break; }
+      if( cudaFuncSetAttribute(k_mlp_grad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(TcSmem)) != cudaSuccess ){ rc = DISCO_ERR_CUDA; break; }
+      if( cudaMalloc(&h->d_err, sizeof(int)) != cudaSuccess ||
+          cudaMemset(h->d_err, 0, sizeof(int)) != cudaSuccess ){ rc = DISCO_ERR_CUDA; break; }
    }while(0);
    if( rc != DISCO_OK ){ disco_gr_destroy(h); return rc; }
    for( int k=0 ; k<8 ; ++k ){ h->h_norm[k] = 0.f; h->h_norm[8+k] = 1.f; }
@@ -665,6 +678,7 @@ void disco_gr_destroy(disco_gr *h){
    if( !h ) return;
    cudaSetDevice(h->device);
    cudaFree(h->d_mlp); cudaFree(h->d_master); cudaFree(h->d_loss); cudaFree(h->d_stats);
+   cudaFree(h->d_err);
    delete h;
 }
 
@@ -847,9 +861,31 @@ static int launch_grad(disco_gr *h, long n, const float *pairs, long nsamp, int 
                        uint64_t seed, int step, double *loss_slot){
    unsigned grid = nb(nsamp, TR_BLOCK);
    if( grid > (unsigned)(2*h->nsm) ) grid = 2*h->nsm;
-   k_mlp_grad<<<grid, TR_BLOCK, sizeof(TrainSmem), h->stream>>>(h->d_mlp, n, pairs, nsamp, sampled,
-                                                               seed, step, h->d_grad, loss_slot);
+   if( h->backend == DISCO_MLP_TENSOR )
+      k_mlp_grad_tc<<<grid, TC_BLOCK, sizeof(TcSmem), h->stream>>>(h->d_mlp, n, pairs, nsamp, sampled,
+                                                                  seed, step, h->d_grad, loss_slot,
+                                                                  h->d_err);
+   else
+      k_mlp_grad<<<grid, TR_BLOCK, sizeof(TrainSmem), h->stream>>>(h->d_mlp, n, pairs, nsamp, sampled,
+                                                                  seed, step, h->d_grad, loss_slot);
    GR_CK(cudaGetLastError());
+   return DISCO_OK;
+}
+
+/* after a synchronisation: a tensor-core wait that ran out */
+static int tc_status(disco_gr *h){
+   int e = 0;
+   GR_CK(cudaMemcpy(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+   if( e ){
+      cudaMemset(h->d_err, 0, sizeof(int));
+      return fail(h, DISCO_ERR_INTERNAL, "tensor-core training kernel: an MMA wait ran out");
+   }
+   return DISCO_OK;
+}
+
+int disco_gr_mlp_set_backend(disco_gr *h, int backend){
+   if( !h || (backend != DISCO_MLP_TENSOR && backend != DISCO_MLP_CUDA_CORES) ) return DISCO_ERR_ARG;
+   h->backend = backend;
    return DISCO_OK;
 }
 
@@ -865,7 +901,7 @@ int disco_gr_mlp_grad(disco_gr *h, long n, const float *pairs, float *grad, doub
    GR_CK(cudaMemcpyAsync(loss, h->d_loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
    GR_CK(cudaMemsetAsync(h->d_grad, 0, MLP_NPARAM*sizeof(float), h->stream));
    GR_CK(cudaStreamSynchronize(h->stream));
-   return DISCO_OK;
+   return tc_status(h);
 }
 
 int disco_gr_mlp_train(disco_gr *h, long n, const float *pairs, int steps, int batch, float lr,
@@ -897,6 +933,7 @@ int disco_gr_mlp_train(disco_gr *h, long n, const float *pairs, int steps, int b
                           h->stream) != cudaSuccess ) rc = fail(h, DISCO_ERR_CUDA, "loss history copy");
    cudaFreeAsync(d_hist, h->stream);
    GR_CK(cudaStreamSynchronize(h->stream));
+   if( rc == DISCO_OK ) rc = tc_status(h);
    return rc;
 }
 

@@ -90,6 +90,7 @@ def _lib():
         "disco_gr_mlp_fit_norm": (I, [P, L, P]),
         "disco_gr_mlp_grad": (I, [P, L, P, C.POINTER(C.c_float), C.POINTER(C.c_double)]),
         "disco_gr_mlp_train": (I, [P, L, P, I, I, C.c_float, C.c_uint64, C.POINTER(C.c_double)]),
+        "disco_gr_mlp_set_backend": (I, [P, I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -225,6 +226,12 @@ class GR:
                                                g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)),
                     "mlp_grad")
         return loss.value, g
+
+    def mlp_backend(self, backend):
+        """"tensor" (tcgen05 MMAs, the default) or "cuda" (the FP32 CUDA-core
+        backward) for mlp_grad / mlp_train."""
+        self._check(self.lib.disco_gr_mlp_set_backend(self.h, {"cuda": 0, "tensor": 1}[backend]),
+                    "mlp_set_backend")
 
     def mlp_train(self, pairs, steps, batch=4096, lr=2e-3, seed=1):
         hist = np.zeros(steps)

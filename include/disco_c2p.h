@@ -132,6 +132,14 @@ int  disco_gr_mlp_grad(disco_gr *h, long n, const float *pairs, float *grad, dou
  * loss_hist (nullable, host, `steps` doubles) receives each step's loss. */
 int  disco_gr_mlp_train(disco_gr *h, long n, const float *pairs, int steps, int batch,
                         float lr, unsigned long long seed, double *loss_hist);
+/* Which kernel disco_gr_mlp_grad / _train run: DISCO_MLP_TENSOR (the
+ * default: the 128-sample group's four contractions as tcgen05.mma on the
+ * tensor cores, BF16 operands, FP32 accumulation in tensor memory) or
+ * DISCO_MLP_CUDA_CORES (the backward on the FP32 CUDA cores).  A tensor-
+ * core wait that runs out (a bounded wait) returns DISCO_ERR_INTERNAL. */
+#define DISCO_MLP_CUDA_CORES 0
+#define DISCO_MLP_TENSOR 1
+int  disco_gr_mlp_set_backend(disco_gr *h, int backend);
 
 #ifdef __cplusplus
 }

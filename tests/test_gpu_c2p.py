@@ -109,8 +109,16 @@ def _pairs_from_runs(gr, x, p0, seeds_eps):
     return torch.cat(out)
 
 
-def test_mlp_gradient_vs_oracle():
+# gradient tolerances against the oracle's double forward / backward: the
+# CUDA-core backward keeps dA2 / dA1 in FP32; the tensor-core one
+# (tcgen05.mma) takes them as BF16 operands, as the forward's activations
+GRAD_TOL = {"cuda": (1e-3, 2e-3), "tensor": (1e-3, 5e-3)}
+
+
+@pytest.mark.parametrize("backend", ["tensor", "cuda"])
+def test_mlp_gradient_vs_oracle(backend):
     gr = _gr(metric="kerr", a=0.9, tol=1e-10)
+    gr.mlp_backend(backend)
     x = gr.grid(16, 8, 64, 1.5, 50.0, -20.0, 20.0)
     p0 = gr.torus(x)
     pairs = _pairs_from_runs(gr, x, p0, [(5, 1e-2), (6, 0.3)])
@@ -124,12 +132,43 @@ def test_mlp_gradient_vs_oracle():
     orc = pyc2p.C2POracle()
     loss_o, grad_o, _ = orc.mlp_loss_grad(param, norm, s[:, :8], t)
     assert abs(loss_g / loss_o - 1) < 1e-5, (loss_g, loss_o)
+    tol, tol_block = GRAD_TOL[backend]
     rel = np.linalg.norm(grad_g - grad_o) / np.linalg.norm(grad_o)
-    assert rel < 1e-3, rel
+    print(backend, "gradient rel L2 %.2e" % rel)
+    assert rel < tol, rel
     # each layer's block on its own
     for lo, hi in [(0, 512), (512, 576), (576, 4672), (4672, 4736), (4736, 4864), (4864, 4866)]:
         r = np.linalg.norm(grad_g[lo:hi] - grad_o[lo:hi]) / max(np.linalg.norm(grad_o[lo:hi]), 1e-30)
-        assert r < 2e-3, (lo, hi, r)
+        assert r < tol_block, (lo, hi, r)
+
+
+def test_mlp_tensor_core_gradient_matches_cuda_cores():
+    """The tcgen05 backward against the CUDA-core one on the same pairs and
+    network, over many 128-sample groups per block (the tensor-memory
+    accumulators carry across groups), and both trainings converge."""
+    gr = _gr(metric="kerr", a=0.9, tol=1e-10)
+    x = gr.grid(32, 16, 96, 1.5, 50.0, -20.0, 20.0)
+    p0 = gr.torus(x)
+    pairs = _pairs_from_runs(gr, x, p0, [(11, 1e-2), (12, 0.3)])
+    gr.mlp_init(5)
+    gr.mlp_fit_norm(pairs)
+    sel = pairs[torch.isfinite(pairs).all(dim=1)].contiguous()
+    assert sel.shape[0] > 128 * 2 * 148 * 2          # several groups per block
+    out = {}
+    for backend in ("cuda", "tensor"):
+        gr.mlp_backend(backend)
+        out[backend] = gr.mlp_grad(sel)
+    (lc, gc), (lt, gt) = out["cuda"], out["tensor"]
+    assert abs(lt / lc - 1) < 1e-5, (lt, lc)
+    rel = np.linalg.norm(gt - gc) / np.linalg.norm(gc)
+    print("tensor vs CUDA cores: rel L2 %.2e" % rel)
+    assert rel < 1e-2, rel
+    for backend in ("tensor", "cuda"):
+        gr.mlp_init(5)
+        gr.mlp_fit_norm(pairs)
+        gr.mlp_backend(backend)
+        hist = gr.mlp_train(sel, steps=300, batch=4096, lr=2e-3, seed=3)
+        assert hist[-20:].mean() < 0.2 * hist[:5].mean(), (backend, hist[:5], hist[-20:])
 
 
 def test_learned_without_network_is_refused():
