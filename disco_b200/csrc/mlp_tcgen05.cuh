@@ -12,12 +12,15 @@
  *   D  = H1 W2^T      N = 64, K = 64                           -> H2 = tanh(D + b2)
  *   (Y = H2 W3^T + b3, dY, dA2 = (dY W3)(1 - H2^2) on the CUDA cores)
  *   D  = dA2 W2       N = 64, K = 64                           -> dA1 = D (1 - H1^2)
- *   G2 += dA2^T H1    rows k (64 of 128, the rest zero rows), N = 64, K = 128 samples
- *   G1 += dA1^T X     rows j (64 of 128), N = 16 (8 used), K = 128 samples
- * G2 and G1 accumulate in tensor memory over the block's groups and are
- * added to the gradient once at the end; the bias gradients and dW3 are
- * warp-shuffle sums.  The transposed products read the same shared-memory
- * tiles as the forward ones, through MN-major descriptors.
+ *   G2 += dA2^T [H1 1] rows k (64 of 128, the rest zero rows), N = 80, K = 128 samples
+ *   G1 += dA1^T [X 1]  rows j (64 of 128), N = 16, K = 128 samples
+ *   G3 += [H2 1]^T dY  rows k (65 of 128), N = 16 (2 used), K = 128 samples
+ * A column of ones beside H1 and X, and a row of ones under H2^T, make the
+ * same products give the bias gradients (db2, db1, db3) with the weight
+ * gradients (dW2, dW1, dW3).  G1-G3 accumulate in tensor memory over the
+ * block's groups and are added to the gradient once at the end.  The
+ * transposed products read the same shared-memory tiles as the forward
+ * ones, through MN-major descriptors.
  *
  * Operand tiles are the canonical no-swizzle layout: 8 x 8 BF16 core
  * matrices of 128 contiguous bytes (row r at byte 16 r), a descriptor's
@@ -32,7 +35,7 @@
 namespace disco {
 
 #define TC_BLOCK 128
-#define TC_COLS 256            /* TMEM columns per block: D 0-63, G2 64-127, G1 128-143 */
+#define TC_COLS 256            /* TMEM columns per block: D 0-63, G2 64-143, G1 144-159, G3 160-175 */
 #define TC_WAIT_CYCLES (1ll << 31)   /* about one second at the SM clock */
 
 struct TcSmem {
@@ -40,12 +43,13 @@ struct TcSmem {
    __nv_bfloat16 W1b[8*2*64];    /* B of X W1^T:  N = j (8 groups), K = i (2) */
    __nv_bfloat16 W2b[8*8*64];    /* B of H1 W2^T: N = k, K = j */
    __nv_bfloat16 W2t[8*8*64];    /* B of dA2 W2:  N = j, K = k */
-   __nv_bfloat16 Xb[16*2*64];    /* [s group][i group]; i 8..15 zero */
-   __nv_bfloat16 H1b[16*8*64];   /* [s group][j group] */
+   __nv_bfloat16 Xb[16*2*64];    /* [s group][i group]; i 8 = 1, i 9..15 zero */
+   __nv_bfloat16 H1b[16*10*64];  /* [s group][j group]; j 64 = 1, j 65..79 zero */
    __nv_bfloat16 DA2b[16*16*64]; /* [s group][k group]; k groups 8..15 zero (the padded M of G2) */
    __nv_bfloat16 DA1b[16*16*64]; /* [s group][j group]; j groups 8..15 zero */
+   __nv_bfloat16 H2b[16*16*64];  /* [s group][k group]; k 64 = 1, the rest of 8..15 zero */
+   __nv_bfloat16 DYb[16*2*64];   /* [s group][o group]; o 2..15 zero */
    float b1[MLP_H], b2[MLP_H], W3[2][MLP_H], b3[2], norm[MLP_NNORM];
-   float g_b1[MLP_H], g_b2[MLP_H], g_W3[2][MLP_H], g_b3[2];
    uint64_t bar;
    uint32_t tmem;
    int abort;
@@ -123,12 +127,6 @@ __device__ __forceinline__ void tc_put8(__nv_bfloat16 *tile, int r, int cg, int 
    *reinterpret_cast<uint4*>(reinterpret_cast<char*>(tile) + tc_off(r, cg*8, ncg)) = u;
 }
 
-__device__ __forceinline__ float tc_wsum(float x){
-#pragma unroll
-   for( int o=16 ; o>0 ; o>>=1 ) x += __shfl_xor_sync(0xffffffffu, x, o);
-   return x;
-}
-
 /* Loss and gradient over nsamp samples (as k_mlp_grad); err: wait timed out */
 __global__ void __launch_bounds__(TC_BLOCK, 1)
 k_mlp_grad_tc(const MlpPacked *__restrict__ mlp, long n, const float *__restrict__ pairs, long nsamp,
@@ -150,21 +148,28 @@ k_mlp_grad_tc(const MlpPacked *__restrict__ mlp, long n, const float *__restrict
       *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<char*>(S.W2b) + tc_off(k, j, 8)) = w;
       *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<char*>(S.W2t) + tc_off(j, k, 8)) = w;
    }
-   {  /* zero the padded tiles (their pad groups stay zero) */
+   {  /* the pad groups: zero, and the ones of the bias products (each
+       * thread its own sample row; the rows are rewritten per group only in
+       * their data groups) */
       uint4 z = make_uint4(0, 0, 0, 0);
-      for( int e=tid ; e<(int)(sizeof(S.Xb)/16) ; e+=TC_BLOCK ) reinterpret_cast<uint4*>(S.Xb)[e] = z;
       for( int e=tid ; e<(int)(sizeof(S.DA2b)/16) ; e+=TC_BLOCK ){
          reinterpret_cast<uint4*>(S.DA2b)[e] = z;
          reinterpret_cast<uint4*>(S.DA1b)[e] = z;
+         reinterpret_cast<uint4*>(S.H2b)[e] = z;
       }
+      float one[8] = {1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, zero[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      tc_put8(S.Xb, tid, 1, 2, one);
+      tc_put8(S.H1b, tid, 8, 10, one);
+      tc_put8(S.H1b, tid, 9, 10, zero);
+      tc_put8(S.H2b, tid, 8, 16, one);
+      tc_put8(S.DYb, tid, 1, 2, zero);
    }
    if( tid < MLP_H ){
       S.b1[tid] = mlp->b1[tid]; S.b2[tid] = mlp->b2[tid];
       S.W3[0][tid] = __bfloat162float(mlp->W3[0][tid]); S.W3[1][tid] = __bfloat162float(mlp->W3[1][tid]);
-      S.g_b1[tid] = 0.f; S.g_b2[tid] = 0.f; S.g_W3[0][tid] = 0.f; S.g_W3[1][tid] = 0.f;
    }
    if( tid < MLP_NNORM ) S.norm[tid] = mlp->norm[tid];
-   if( tid < 2 ){ S.b3[tid] = mlp->b3[tid]; S.g_b3[tid] = 0.f; }
+   if( tid < 2 ) S.b3[tid] = mlp->b3[tid];
    if( tid == 0 ){
       S.abort = 0;
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&S.bar)), "r"(1) : "memory");
@@ -188,7 +193,7 @@ k_mlp_grad_tc(const MlpPacked *__restrict__ mlp, long n, const float *__restrict
 
    const uint32_t aX = smem_u32(S.Xb), aH1 = smem_u32(S.H1b), aDA2 = smem_u32(S.DA2b),
                   aDA1 = smem_u32(S.DA1b), aW1 = smem_u32(S.W1b), aW2 = smem_u32(S.W2b),
-                  aW2t = smem_u32(S.W2t);
+                  aW2t = smem_u32(S.W2t), aH2 = smem_u32(S.H2b), aDY = smem_u32(S.DYb);
    /* wait for the MMAs just committed; every thread learns whether to go on */
    auto sync_mma = [&]() -> bool {
       const bool ok = tc_wait(&S.bar, parity);
@@ -224,7 +229,7 @@ k_mlp_grad_tc(const MlpPacked *__restrict__ mlp, long n, const float *__restrict
       float x[8];
 #pragma unroll
       for( int q=0 ; q<8 ; ++q ) x[q] = valid ? (f[q] - S.norm[q])*S.norm[8+q] : 0.f;
-      tc_put8(S.Xb, tid, 0, 2, x);
+      tc_put8(S.Xb, tid, 0, 2, x);           /* group 1 holds the ones column */
       publish();
       if( tid == 0 ){
          tc_mma(tm, tc_desc(aX, 128, 256), tc_desc(aW1, 128, 256), tc_idesc(64, false, false), 0);
@@ -239,12 +244,12 @@ k_mlp_grad_tc(const MlpPacked *__restrict__ mlp, long n, const float *__restrict
 #pragma unroll
       for( int j=0 ; j<MLP_H ; ++j ) h1[j] = tanhf(h1[j] + S.b1[j]);
 #pragma unroll
-      for( int jg=0 ; jg<8 ; ++jg ) tc_put8(S.H1b, tid, jg, 8, h1 + 8*jg);
+      for( int jg=0 ; jg<8 ; ++jg ) tc_put8(S.H1b, tid, jg, 10, h1 + 8*jg);
       publish();
       if( tid == 0 ){
 #pragma unroll
          for( int q=0 ; q<4 ; ++q )
-            tc_mma(tm, tc_desc(aH1 + 256*q, 128, 1024), tc_desc(aW2 + 256*q, 128, 1024),
+            tc_mma(tm, tc_desc(aH1 + 256*q, 128, 1280), tc_desc(aW2 + 256*q, 128, 1024),
                    tc_idesc(64, false, false), q > 0);
          tc_commit(&S.bar);
       }
@@ -269,31 +274,32 @@ k_mlp_grad_tc(const MlpPacked *__restrict__ mlp, long n, const float *__restrict
       const float dy0 = valid ? d0*invn : 0.f, dy1 = valid ? d1*invn : 0.f;
       float da2[MLP_H];
 #pragma unroll
-      for( int k=0 ; k<MLP_H ; ++k ){
-         const float hb = __bfloat162float(__float2bfloat16_rn(h2[k]));
-         float gw0 = tc_wsum(dy0*hb), gw1 = tc_wsum(dy1*hb);
-         if( lane == 0 ){ atomicAdd(&S.g_W3[0][k], gw0); atomicAdd(&S.g_W3[1][k], gw1); }
-         da2[k] = (S.W3[0][k]*dy0 + S.W3[1][k]*dy1)*(1.f - h2[k]*h2[k]);
-         const float gb = tc_wsum(da2[k]);
-         if( lane == 0 ) atomicAdd(&S.g_b2[k], gb);
+      for( int k=0 ; k<MLP_H ; ++k ) da2[k] = (S.W3[0][k]*dy0 + S.W3[1][k]*dy1)*(1.f - h2[k]*h2[k]);
+#pragma unroll
+      for( int kg=0 ; kg<8 ; ++kg ){
+         tc_put8(S.DA2b, tid, kg, 16, da2 + 8*kg);
+         tc_put8(S.H2b, tid, kg, 16, h2 + 8*kg);
       }
       {
-         const float g0 = tc_wsum(dy0), g1 = tc_wsum(dy1);
-         if( lane == 0 ){ atomicAdd(&S.g_b3[0], g0); atomicAdd(&S.g_b3[1], g1); }
+         float dy[8] = {dy0, dy1, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+         tc_put8(S.DYb, tid, 0, 2, dy);
       }
-#pragma unroll
-      for( int kg=0 ; kg<8 ; ++kg ) tc_put8(S.DA2b, tid, kg, 16, da2 + 8*kg);
       publish();
       if( tid == 0 ){
-         /* dA2 W2 -> D; G2 += dA2^T H1 (MN-major: rows k, 16 groups, 8 of them zero) */
+         /* dA2 W2 -> D; G2 += dA2^T [H1 1] (MN-major: rows k, 16 groups, 8 of
+          * them zero); G3 += [H2 1]^T dY (rows k and the ones row 64) */
 #pragma unroll
          for( int q=0 ; q<4 ; ++q )
             tc_mma(tm, tc_desc(aDA2 + 256*q, 128, 2048), tc_desc(aW2t + 256*q, 128, 1024),
                    tc_idesc(64, false, false), q > 0);
 #pragma unroll
-         for( int q=0 ; q<8 ; ++q )
-            tc_mma(tm + 64, tc_desc(aDA2 + 4096*q, 2048, 128), tc_desc(aH1 + 2048*q, 1024, 128),
-                   tc_idesc(64, true, true), (g > 0 || q > 0) ? 1 : 0);
+         for( int q=0 ; q<8 ; ++q ){
+            const int acc = (g > 0 || q > 0) ? 1 : 0;
+            tc_mma(tm + 64, tc_desc(aDA2 + 4096*q, 2048, 128), tc_desc(aH1 + 2560*q, 1280, 128),
+                   tc_idesc(80, true, true), acc);
+            tc_mma(tm + 160, tc_desc(aH2 + 4096*q, 2048, 128), tc_desc(aDY + 512*q, 256, 128),
+                   tc_idesc(16, true, true), acc);
+         }
          tc_commit(&S.bar);
       }
       if( !sync_mma() ){ live = false; break; }
@@ -303,18 +309,14 @@ k_mlp_grad_tc(const MlpPacked *__restrict__ mlp, long n, const float *__restrict
 #pragma unroll
       for( int c=0 ; c<4 ; ++c ) tc_ld16(lane_base + 16*c, da1 + 16*c);
 #pragma unroll
-      for( int j=0 ; j<MLP_H ; ++j ){
-         da1[j] *= (1.f - h1[j]*h1[j]);
-         const float gb = tc_wsum(da1[j]);
-         if( lane == 0 ) atomicAdd(&S.g_b1[j], gb);
-      }
+      for( int j=0 ; j<MLP_H ; ++j ) da1[j] *= (1.f - h1[j]*h1[j]);
 #pragma unroll
       for( int jg=0 ; jg<8 ; ++jg ) tc_put8(S.DA1b, tid, jg, 16, da1 + 8*jg);
       publish();
       if( tid == 0 ){
 #pragma unroll
          for( int q=0 ; q<8 ; ++q )
-            tc_mma(tm + 128, tc_desc(aDA1 + 4096*q, 2048, 128), tc_desc(aX + 512*q, 256, 128),
+            tc_mma(tm + 144, tc_desc(aDA1 + 4096*q, 2048, 128), tc_desc(aX + 512*q, 256, 128),
                    tc_idesc(16, true, true), (g > 0 || q > 0) ? 1 : 0);
          tc_commit(&S.bar);
       }
@@ -323,28 +325,39 @@ k_mlp_grad_tc(const MlpPacked *__restrict__ mlp, long n, const float *__restrict
 
    if( S.abort ){
       if( tid == 0 ) atomicOr(err, 1);
-   }else if( g > 0 && warp < 2 ){
-      /* G2 rows k = lane (warps 0, 1), columns j; G1 rows j, columns i < 8 */
+   }else if( g > 0 && warp < 3 ){
+      /* rows r = lane of warps 0-2: G2 row k: dW2[k][j] (columns 0-63) and
+       * db2[k] (column 64); G1 row j: dW1[j][i] (columns 0-7) and db1[j]
+       * (column 8); G3 row k: dW3[o][k] (columns 0, 1), row 64: db3 */
       const int r = 32*warp + lane;
       float v[16];
+      if( r < MLP_H ){
 #pragma unroll
-      for( int c=0 ; c<4 ; ++c ){
-         tc_ld16(lane_base + 64 + 16*c, v);
+         for( int c=0 ; c<4 ; ++c ){
+            tc_ld16(lane_base + 64 + 16*c, v);
 #pragma unroll
-         for( int q=0 ; q<16 ; ++q ) atomicAdd(&grad[OFF_W2 + r*MLP_H + 16*c + q], v[q]);
+            for( int q=0 ; q<16 ; ++q ) atomicAdd(&grad[OFF_W2 + r*MLP_H + 16*c + q], v[q]);
+         }
+         tc_ld16(lane_base + 128, v);
+         atomicAdd(&grad[OFF_B2 + r], v[0]);
+         tc_ld16(lane_base + 144, v);
+#pragma unroll
+         for( int q=0 ; q<8 ; ++q ) atomicAdd(&grad[OFF_W1 + r*8 + q], v[q]);
+         atomicAdd(&grad[OFF_B1 + r], v[8]);
+         tc_ld16(lane_base + 160, v);
+         atomicAdd(&grad[OFF_W3 + r], v[0]);
+         atomicAdd(&grad[OFF_W3 + MLP_H + r], v[1]);
+      }else{
+         /* warp 2: the tcgen05.ld is warp-wide; lane 0 (row 64) keeps db3 */
+#pragma unroll
+         for( int c=0 ; c<4 ; ++c ) tc_ld16(lane_base + 64 + 16*c, v);
+         tc_ld16(lane_base + 128, v);
+         tc_ld16(lane_base + 144, v);
+         tc_ld16(lane_base + 160, v);
+         if( r == MLP_H ){ atomicAdd(&grad[OFF_B3], v[0]); atomicAdd(&grad[OFF_B3 + 1], v[1]); }
       }
-      tc_ld16(lane_base + 128, v);
-#pragma unroll
-      for( int q=0 ; q<8 ; ++q ) atomicAdd(&grad[OFF_W1 + r*8 + q], v[q]);
    }
    if( !S.abort ){
-      if( tid < MLP_H ){
-         atomicAdd(&grad[OFF_B1 + tid], S.g_b1[tid]);
-         atomicAdd(&grad[OFF_B2 + tid], S.g_b2[tid]);
-         atomicAdd(&grad[OFF_W3 + tid], S.g_W3[0][tid]);
-         atomicAdd(&grad[OFF_W3 + MLP_H + tid], S.g_W3[1][tid]);
-      }
-      if( tid < 2 ) atomicAdd(&grad[OFF_B3 + tid], S.g_b3[tid]);
 #pragma unroll
       for( int o=16 ; o>0 ; o>>=1 ) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
       if( lane == 0 && lsum != 0.0 ) atomicAdd(loss, lsum/(2.0*(double)nsamp));
