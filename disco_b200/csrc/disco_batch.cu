@@ -64,6 +64,41 @@ extern "C" const char *disco_strerror(int s){
    return "unknown status";
 }
 
+/* Each side of the modules composed from boundary_functions.c (0 inner r,
+ * 1 outer r, 2 lower z, 3 upper z): fixed (set_cell_init, boundary_fixed_*),
+ * zero-gradient copy (boundary_zerograd_*, diode 0 or 1), mirror copy
+ * (boundary_reflect_*: the annulus as far inside as the ghost is outside,
+ * then reflect_prims' normal velocity negated), or nothing. */
+enum { SIDE_NONE = 0, SIDE_FIXED, SIDE_ZG, SIDE_ZG_DIODE, SIDE_REFLECT };
+static int side_mode(int boundary, int s){
+   static const int zg[4] = {SIDE_ZG, SIDE_ZG, SIDE_ZG, SIDE_ZG};
+   static const int zgd[4] = {SIDE_ZG_DIODE, SIDE_ZG_DIODE, SIDE_ZG_DIODE, SIDE_ZG_DIODE};
+   static const int acc3[4] = {SIDE_ZG_DIODE, SIDE_FIXED, SIDE_FIXED, SIDE_FIXED};
+   static const int frz[4] = {SIDE_FIXED, SIDE_FIXED, SIDE_REFLECT, SIDE_REFLECT};      /* fixRrefZ.c */
+   static const int tube[4] = {SIDE_NONE, SIDE_REFLECT, SIDE_ZG, SIDE_ZG};             /* tube.c */
+   static const int sgb[4] = {SIDE_REFLECT, SIDE_REFLECT, SIDE_REFLECT, SIDE_ZG_DIODE}; /* surfaceGravBox.c */
+   static const int gap[4] = {SIDE_ZG_DIODE, SIDE_FIXED, SIDE_ZG_DIODE, SIDE_ZG_DIODE}; /* fixed_gap.c */
+   switch( boundary ){
+      case DISCO_BC_ZEROGRAD: return zg[s];
+      case DISCO_BC_OUTFLOW3D: case DISCO_BC_ZEROGRAD_OMK: return zgd[s];
+      case DISCO_BC_ACCRETE3D: return acc3[s];
+      case DISCO_BC_FIXRREFZ: return frz[s];
+      case DISCO_BC_TUBE: return tube[s];
+      case DISCO_BC_SURFACEGRAVBOX: return sgb[s];
+      case DISCO_BC_FIXED_GAP: return gap[s];
+   }
+   return SIDE_NONE;
+}
+static bool side_copies(int m){ return m == SIDE_ZG || m == SIDE_ZG_DIODE || m == SIDE_REFLECT; }
+/* the fixed sides of the newer composed modules (fixed_ghost_init bc 11) */
+static int side_fixed_mask(int boundary){
+   if( boundary != DISCO_BC_FIXRREFZ && boundary != DISCO_BC_TUBE &&
+       boundary != DISCO_BC_SURFACEGRAVBOX && boundary != DISCO_BC_FIXED_GAP ) return 0;
+   int m = 0;
+   for( int s=0 ; s<4 ; ++s ) if( side_mode(boundary, s) == SIDE_FIXED ) m |= 1 << s;
+   return m ? m : 16;          /* 16: composed, no fixed side */
+}
+
 static void fill_disk_params(DiskParams &D, const disco_params &p, const disco_modules &m){
    memset(&D, 0, sizeof D);
    D.gam = p.Adiabatic_Index; D.PLM = p.PLM; D.CFL = p.CFL; D.maxDT = p.maxDT;
@@ -104,6 +139,7 @@ static void fill_disk_params(DiskParams &D, const disco_params &p, const disco_m
    D.ic_gr.phimax = p.phimax;
    D.bc_horizon = m.boundary == DISCO_BC_HORIZON ? 8 : m.boundary == DISCO_BC_HORIZON3D ? 9 :
                   m.boundary == DISCO_BC_HORIZON_BIN ? 10 : 0;
+   D.side_fixed = side_fixed_mask(m.boundary) & 15;
    D.ic_mhd.seed = (uint64_t)(int64_t)p.initPar0; D.ic_mhd.amp = p.initPar[1];
    D.ic_mhd.cs = p.initPar[3]; D.ic_mhd.beta = p.initPar[4]; D.ic_mhd.gam = p.Adiabatic_Index;
    D.ic_mhd.rmin = p.rmin; D.ic_mhd.rmax = p.rmax; D.ic_mhd.zmin = p.zmin; D.ic_mhd.zmax = p.zmax;
@@ -356,8 +392,11 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       for( int d=0 ; d<ndisk ; ++d )
          if( Nz[d] > 1 && mods->ct_mode != 2 ) return DISCO_ERR_UNSUPPORTED;
    }
-   if( mods->boundary < DISCO_BC_FIXED || mods->boundary > DISCO_BC_HORIZON_BIN )
+   if( mods->boundary < DISCO_BC_FIXED || mods->boundary > DISCO_BC_FIXED_GAP )
       return DISCO_ERR_UNSUPPORTED;
+   /* tube sets no inner r ghosts (Boundary/tube.c): grids without them */
+   if( mods->boundary == DISCO_BC_TUBE )
+      for( int d=0 ; d<ndisk ; ++d ) if( Ng[4*d+0] != 0 ) return DISCO_ERR_UNSUPPORTED;
    /* polar3d, horizon, horizon3d and horizon_bin set the outer r and the z
     * ghosts only (Boundary/polar3d.c, horizon.c, horizon3d.c,
     * horizon_bin.c): grids without inner ghosts */
@@ -400,14 +439,14 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
                  mods->boundary == DISCO_BC_POLAR ? 3 :
                  (mods->boundary == DISCO_BC_ACCRETE3D || mods->boundary == DISCO_BC_POLAR3D) ? 6 :
                  mods->boundary == DISCO_BC_HORIZON ? 8 : mods->boundary == DISCO_BC_HORIZON3D ? 9 :
-                 mods->boundary == DISCO_BC_HORIZON_BIN ? 10 : 0;
-   /* modules built from boundary_functions.c's zero-gradient copies: all four
-    * sides (zerograd; with the diode outflow3d, zerograd_omk), or the inner r
-    * side only (accrete3d, whose other sides are fixed) */
-   b->bc_zerograd = mods->boundary == DISCO_BC_ZEROGRAD || mods->boundary == DISCO_BC_OUTFLOW3D ||
-                    mods->boundary == DISCO_BC_ZEROGRAD_OMK || mods->boundary == DISCO_BC_ACCRETE3D;
-   b->zg_diode = mods->boundary == DISCO_BC_OUTFLOW3D || mods->boundary == DISCO_BC_ZEROGRAD_OMK ||
-                 mods->boundary == DISCO_BC_ACCRETE3D;
+                 mods->boundary == DISCO_BC_HORIZON_BIN ? 10 :
+                 side_fixed_mask(mods->boundary) ? 11 : 0;
+   /* modules built from boundary_functions.c's copies (zero-gradient, with
+    * or without the outflow diode, and mirror copies): the sides whose
+    * ghosts k_zerograd fills */
+   b->bc_zerograd = 0;
+   for( int s=0 ; s<4 ; ++s ) if( side_copies(side_mode(mods->boundary, s)) ) b->bc_zerograd = 1;
+   b->zg_diode = 0;                          /* per pair (zg_side) */
    b->zg_omk = mods->boundary == DISCO_BC_ZEROGRAD_OMK;
    b->d_zg_side = NULL;
    b->d_noise = NULL;
@@ -539,7 +578,11 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
     * cells outwards, then z ghosts (all j, ghosts included); sides[] of each
     * pair: 0 inner r, 1 outer r, 2 lower z, 3 upper z */
    if( b->bc_zerograd ){
-      const bool acc3 = mods->boundary == DISCO_BC_ACCRETE3D;
+      int smode[4];
+      for( int s=0 ; s<4 ; ++s ) smode[s] = side_mode(mods->boundary, s);
+      /* zg_side: the side, | 4 with the diode, | 8 for a mirror copy */
+      auto flags = [&](int s){ return (unsigned char)(s | (smode[s] == SIDE_ZG_DIODE ? 4 : 0) |
+                                                      (smode[s] == SIDE_REFLECT ? 8 : 0)); };
       int maxr = 0, maxz = 0;
       for( int d=0 ; d<ndisk ; ++d ){
          const DiskParams &D = b->dparams[d];
@@ -552,13 +595,18 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
             const DiskParams &D = b->dparams[d];
             for( int k=0 ; k<D.Nz ; ++k ){
                int base = D.ann0 + D.Nr*k;
-               /* accrete3d: the z ghost layers end fixed (boundary_fixed_zbot /
-                * _ztop run after the r copies), so their inner r ghosts need no copy */
-               if( acc3 && (k < D.NgZa || k >= D.Nz - D.NgZb) ) continue;
-               if( l < D.NgRa ){ int j = D.NgRa-1-l; b->zg_pairs.push_back(make_int2(base+j, base+j+1));
-                                 b->zg_side.push_back(0); }
-               if( l < D.NgRb && !acc3 ){ int j = D.Nr-D.NgRb+l;
-                                 b->zg_pairs.push_back(make_int2(base+j, base+j-1)); b->zg_side.push_back(1); }
+               /* a z ghost layer of a fixed z side ends fixed (the z pass runs
+                * after the r copies), so its r ghosts need no copy */
+               if( (k < D.NgZa && smode[2] == SIDE_FIXED) || (k >= D.Nz - D.NgZb && smode[3] == SIDE_FIXED) )
+                  continue;
+               if( l < D.NgRa && side_copies(smode[0]) ){
+                  int j = D.NgRa-1-l, j1 = smode[0] == SIDE_REFLECT ? 2*D.NgRa-j-1 : j+1;
+                  b->zg_pairs.push_back(make_int2(base+j, base+j1)); b->zg_side.push_back(flags(0));
+               }
+               if( l < D.NgRb && side_copies(smode[1]) ){
+                  int j = D.Nr-D.NgRb+l, j1 = smode[1] == SIDE_REFLECT ? 2*(D.Nr-D.NgRb)-j-1 : j-1;
+                  b->zg_pairs.push_back(make_int2(base+j, base+j1)); b->zg_side.push_back(flags(1));
+               }
             }
          }
       }
@@ -566,14 +614,18 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
          b->zg_off.push_back((int)b->zg_pairs.size());
          for( int d=0 ; d<ndisk ; ++d ){
             const DiskParams &D = b->dparams[d];
-            if( D.Nz < 2 || params[d].Z_Periodic || acc3 ) continue;
+            if( D.Nz < 2 || params[d].Z_Periodic ) continue;
             for( int j=0 ; j<D.Nr ; ++j ){
-               if( l < D.NgZa ){ int k = D.NgZa-1-l;
-                  b->zg_pairs.push_back(make_int2(D.ann0 + j + D.Nr*k, D.ann0 + j + D.Nr*(k+1)));
-                  b->zg_side.push_back(2); }
-               if( l < D.NgZb ){ int k = D.Nz-D.NgZb+l;
-                  b->zg_pairs.push_back(make_int2(D.ann0 + j + D.Nr*k, D.ann0 + j + D.Nr*(k-1)));
-                  b->zg_side.push_back(3); }
+               if( l < D.NgZa && side_copies(smode[2]) ){
+                  int k = D.NgZa-1-l, k1 = smode[2] == SIDE_REFLECT ? 2*D.NgZa-k-1 : k+1;
+                  b->zg_pairs.push_back(make_int2(D.ann0 + j + D.Nr*k, D.ann0 + j + D.Nr*k1));
+                  b->zg_side.push_back(flags(2));
+               }
+               if( l < D.NgZb && side_copies(smode[3]) ){
+                  int k = D.Nz-D.NgZb+l, k1 = smode[3] == SIDE_REFLECT ? 2*(D.Nz-D.NgZb)-k-1 : k-1;
+                  b->zg_pairs.push_back(make_int2(D.ann0 + j + D.Nr*k, D.ann0 + j + D.Nr*k1));
+                  b->zg_side.push_back(flags(3));
+               }
             }
          }
       }

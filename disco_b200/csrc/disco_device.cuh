@@ -80,7 +80,7 @@ struct DiskParams {
    int gr, gr_metric;
    double gr_M, gr_a;
    int bc_horizon;    /* 8 (Boundary/horizon.c) or 9 (horizon3d) when cells are excised, else 0 */
-   int pad_hz;
+   int side_fixed;    /* bc 11: the fixed sides (bit 0 inner r, 1 outer r, 2 lower z, 3 upper z) */
 };
 
 /* Per-disk mutable state (device resident across steps). */

@@ -1444,6 +1444,12 @@ __device__ __forceinline__ bool fixed_ghost_init(const DiskParams &P, int bc, in
    }else if( bc == 2 && (rghost || zghost) ){
       double x[3] = { centroid_r(rj[j], rj[j-1]), 0.5*(piph + (piph - dphi)), 0.5*(zk[k]+zk[k-1]) };
       initial<Q,NC>(P, prim, x);
+   }else if( bc == 11 && ((j < P.NgRa && (P.side_fixed & 1)) || (j >= P.Nr - P.NgRb && (P.side_fixed & 2)) ||
+                          (k < P.NgZa && (P.side_fixed & 4)) || (k >= P.Nz - P.NgZb && (P.side_fixed & 8))) ){
+      /* the fixed sides of fixRrefZ, fixed_gap (boundary_fixed_rinn / _rout /
+       * _zbot / _ztop: set_cell_init) */
+      double x[3] = { centroid_r(rj[j], rj[j-1]), 0.5*(piph + (piph - dphi)), 0.5*(zk[k]+zk[k-1]) };
+      initial<Q,NC>(P, prim, x);
    }else if( bc == 6 && (j >= P.Nr - P.NgRb || zghost) ){
       /* accrete3d: boundary_fixed_rout, _zbot, _ztop (set_cell_init); the
        * inner r ghosts are zero-gradient */
@@ -1819,11 +1825,16 @@ __global__ void k_zerograd(ViewT<R> v, const int2 *pairs, const unsigned char *s
       }
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ) acc[q] = acc[q]/sd[i];
-      const int side = sides[blockIdx.x];
+      const int sflags = sides[blockIdx.x];
+      const int side = sflags & 3;
       R out[Q];
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ) out[q] = (R)acc[q];
-      if( diode ){
+      if( sflags & 8 ){               /* mirror copy: reflect_prims (euler.c:405, mhd.c:507) */
+         if( side <= 1 ) out[URR] = -out[URR];
+         else            out[UZZ] = -out[UZZ];
+      }
+      if( diode || (sflags & 4) ){
          if( side == 0 && out[URR] > R(0) ) out[URR] = R(0);
          if( side == 1 && out[URR] < R(0) ) out[URR] = R(0);
          if( side == 2 && out[UZZ] > R(0) ) out[UZZ] = R(0);

@@ -157,6 +157,10 @@ int disco_read_opt(const char *path, disco_modules *m){
    else if( !strcmp(v, "horizon") ) m->boundary = DISCO_BC_HORIZON;
    else if( !strcmp(v, "horizon3d") ) m->boundary = DISCO_BC_HORIZON3D;
    else if( !strcmp(v, "horizon_bin") ) m->boundary = DISCO_BC_HORIZON_BIN;
+   else if( !strcmp(v, "fixRrefZ") ) m->boundary = DISCO_BC_FIXRREFZ;
+   else if( !strcmp(v, "tube") ) m->boundary = DISCO_BC_TUBE;
+   else if( !strcmp(v, "surfaceGravBox") ) m->boundary = DISCO_BC_SURFACEGRAVBOX;
+   else if( !strcmp(v, "fixed_gap") ) m->boundary = DISCO_BC_FIXED_GAP;
    else return DISCO_ERR_UNSUPPORTED;
    if( opt_value(path, "PLANETS", v, sizeof v) ) return DISCO_ERR_ARG;
    if( !strcmp(v, "none") ) m->planets = DISCO_PLANETS_NONE;

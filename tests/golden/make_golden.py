@@ -28,6 +28,10 @@ import pyoracle  # noqa: E402
 
 TEMPLATES = os.path.join(REPO, "disco_b200", "templates")
 
+# the 3D rigid disk of the composed boundary modules' fixtures
+BC3D = {"Num_R": 10, "Num_Z": 4, "Z_Min": -0.3, "Z_Max": 0.3, "Log_Zoning": 0, "Init_Par2": 1,
+        "Init_Par1": 0.05, "Energy_Omega": 0, "Mach_Number": 5.0}
+
 # case -> (module config, in.par overrides, steps)
 CASES = {
     "c0_log16": ("c0_kepler2d", {"Num_R": 16}, 8),
@@ -188,6 +192,16 @@ CASES = {
     "c0_hbin3d": ("c0_hbin", {"Num_R": 16, "Num_Z": 6, "Z_Min": -0.6, "Z_Max": 0.6, "R_Min": 3.5,
                               "R_Max": 7.0, "NoBC_Rmin": 1, "Log_Zoning": 0, "Init_Par2": 1,
                               "Init_Par1": 0.05, "Energy_Omega": 0, "Mach_Number": 5.0}, 5),
+    # the other modules composed from boundary_functions.c, with mirror
+    # copies (boundary_reflect_*: the annulus as far inside as the ghost is
+    # outside, normal velocity negated by reflect_prims): fixRrefZ (fixed r,
+    # reflecting z), tube (reflecting outer r, zero-gradient z; no inner
+    # ghosts), surfaceGravBox (reflecting r and lower z, outflow upper z),
+    # fixed_gap (outflow inner r and z, fixed outer r); 3D hydro, rigid
+    "c0_bc_fixRrefZ": ("c0_bc_fixRrefZ", dict(BC3D), 5),
+    "c0_bc_tube": ("c0_bc_tube", dict(BC3D, NoBC_Rmin=1), 5),
+    "c0_bc_surfaceGravBox": ("c0_bc_surfaceGravBox", dict(BC3D), 5),
+    "c0_bc_fixed_gap": ("c0_bc_fixed_gap", dict(BC3D), 5),
     "c1_polar3d_zpole": ("c1_polar3d", {"Num_R": 8, "Num_Z": 6, "R_Min": 0.0, "R_Max": 2.0,
                                         "NoBC_Rmin": 1, "Init_Par2": 1, "Init_Par4": 10.0,
                                         "Constrained_Transport": 1, "Init_Par5": 20.0,
@@ -203,7 +217,8 @@ BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": 
             "c0_circular": "c0_kepler2d", "c0_cm": "c0_kepler2d", "c0_diag_euler": "c0_kepler2d",
             "c0_diag_euler3d": "c0_kepler2d", "c1_diag_mhdmri": "c1_mhd2d", "c3_grtorus": "c3_grtorus", "c4_binary3d": "c4_binary3d",
             "c0_horizon3d": "c0_kepler2d", "c1_polar3dbc": "c1_mhd3d", "c3_grhorizon": "c3_grtorus",
-            "c0_hbin": "c0_kepler2d"}
+            "c0_hbin": "c0_kepler2d", "c0_bc_fixRrefZ": "c0_kepler2d", "c0_bc_tube": "c0_kepler2d",
+            "c0_bc_surfaceGravBox": "c0_kepler2d", "c0_bc_fixed_gap": "c0_kepler2d"}
 
 
 def par_text(cfg_par, overrides):

@@ -107,3 +107,12 @@ def test_no_device_is_a_clean_error():
         db.Batch([disk])
     assert e.value.status == 6
     assert db.library().disco_strerror(6) == b"no CUDA device"
+
+
+@pytest.mark.parametrize("case,module", [("c0_bc_fixRrefZ", "fixRrefZ"), ("c0_bc_tube", "tube"),
+                                         ("c0_bc_surfaceGravBox", "surfaceGravBox"),
+                                         ("c0_bc_fixed_gap", "fixed_gap")])
+def test_composed_boundary_modules_parse(case, module):
+    disk, g = case_disk(case)
+    assert disk.modules.boundary == db.BOUNDARY[module]
+    assert np.array_equal(disk.Np, g["Np"]) and np.array_equal(disk.real, g["real"])
