@@ -34,7 +34,7 @@ HYDRO = {"euler": 0, "mhd": 1, "grmhd2": 2}
 METRIC = {"schw_ks_rpz": 0, "kerr_ks_rpz": 1}
 BOUNDARY = {"fixed": 0, "zerograd": 1, "fixed3d": 2, "polar": 3, "outflow3d": 4, "zerograd_omk": 5,
             "accrete3d": 6, "polar3d": 7, "horizon": 8, "horizon3d": 9, "horizon_bin": 10,
-            "fixRrefZ": 11, "tube": 12, "surfaceGravBox": 13, "fixed_gap": 14}
+            "fixRrefZ": 11, "tube": 12, "surfaceGravBox": 13, "fixed_gap": 14, "flowthrough": 15}
 PLANETS = {"none": 0, "sun": 1, "cm2": 2, "binary_soft": 3, "circular": 4, "cm": 5}
 INITIAL = {"kepler_noise": 0, "mhd_shear_noise": 1, "host": 2, "gr_torus_noise": 3}
 PREC_FP64, PREC_MIXED = 0, 1

@@ -69,7 +69,9 @@ extern "C" const char *disco_strerror(int s){
  * zero-gradient copy (boundary_zerograd_*, diode 0 or 1), mirror copy
  * (boundary_reflect_*: the annulus as far inside as the ghost is outside,
  * then reflect_prims' normal velocity negated), or nothing. */
-enum { SIDE_NONE = 0, SIDE_FIXED, SIDE_ZG, SIDE_ZG_DIODE, SIDE_REFLECT };
+enum { SIDE_NONE = 0, SIDE_FIXED, SIDE_ZG, SIDE_ZG_DIODE, SIDE_REFLECT,
+       SIDE_NOSLIP,             /* mirror copy, all three velocity components negated */
+       SIDE_ZG_DIODE_PHIWIN };  /* zero-gradient with the diode, then fixed on 0.3 pi < phi < 1.7 pi */
 static int side_mode(int boundary, int s){
    static const int zg[4] = {SIDE_ZG, SIDE_ZG, SIDE_ZG, SIDE_ZG};
    static const int zgd[4] = {SIDE_ZG_DIODE, SIDE_ZG_DIODE, SIDE_ZG_DIODE, SIDE_ZG_DIODE};
@@ -78,6 +80,7 @@ static int side_mode(int boundary, int s){
    static const int tube[4] = {SIDE_NONE, SIDE_REFLECT, SIDE_ZG, SIDE_ZG};             /* tube.c */
    static const int sgb[4] = {SIDE_REFLECT, SIDE_REFLECT, SIDE_REFLECT, SIDE_ZG_DIODE}; /* surfaceGravBox.c */
    static const int gap[4] = {SIDE_ZG_DIODE, SIDE_FIXED, SIDE_ZG_DIODE, SIDE_ZG_DIODE}; /* fixed_gap.c */
+   static const int flow[4] = {SIDE_NOSLIP, SIDE_ZG_DIODE_PHIWIN, SIDE_FIXED, SIDE_FIXED}; /* flowthrough.c */
    switch( boundary ){
       case DISCO_BC_ZEROGRAD: return zg[s];
       case DISCO_BC_OUTFLOW3D: case DISCO_BC_ZEROGRAD_OMK: return zgd[s];
@@ -86,13 +89,18 @@ static int side_mode(int boundary, int s){
       case DISCO_BC_TUBE: return tube[s];
       case DISCO_BC_SURFACEGRAVBOX: return sgb[s];
       case DISCO_BC_FIXED_GAP: return gap[s];
+      case DISCO_BC_FLOWTHROUGH: return flow[s];
    }
    return SIDE_NONE;
 }
-static bool side_copies(int m){ return m == SIDE_ZG || m == SIDE_ZG_DIODE || m == SIDE_REFLECT; }
+static bool side_copies(int m){
+   return m == SIDE_ZG || m == SIDE_ZG_DIODE || m == SIDE_REFLECT || m == SIDE_NOSLIP ||
+          m == SIDE_ZG_DIODE_PHIWIN;
+}
+static bool side_mirror(int m){ return m == SIDE_REFLECT || m == SIDE_NOSLIP; }
 /* the fixed sides of the newer composed modules (fixed_ghost_init bc 11) */
 static int side_fixed_mask(int boundary){
-   if( boundary != DISCO_BC_FIXRREFZ && boundary != DISCO_BC_TUBE &&
+   if( boundary != DISCO_BC_FIXRREFZ && boundary != DISCO_BC_TUBE && boundary != DISCO_BC_FLOWTHROUGH &&
        boundary != DISCO_BC_SURFACEGRAVBOX && boundary != DISCO_BC_FIXED_GAP ) return 0;
    int m = 0;
    for( int s=0 ; s<4 ; ++s ) if( side_mode(boundary, s) == SIDE_FIXED ) m |= 1 << s;
@@ -392,7 +400,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
       for( int d=0 ; d<ndisk ; ++d )
          if( Nz[d] > 1 && mods->ct_mode != 2 ) return DISCO_ERR_UNSUPPORTED;
    }
-   if( mods->boundary < DISCO_BC_FIXED || mods->boundary > DISCO_BC_FIXED_GAP )
+   if( mods->boundary < DISCO_BC_FIXED || mods->boundary > DISCO_BC_FLOWTHROUGH )
       return DISCO_ERR_UNSUPPORTED;
    /* tube sets no inner r ghosts (Boundary/tube.c): grids without them */
    if( mods->boundary == DISCO_BC_TUBE )
@@ -580,9 +588,16 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    if( b->bc_zerograd ){
       int smode[4];
       for( int s=0 ; s<4 ; ++s ) smode[s] = side_mode(mods->boundary, s);
-      /* zg_side: the side, | 4 with the diode, | 8 for a mirror copy */
-      auto flags = [&](int s){ return (unsigned char)(s | (smode[s] == SIDE_ZG_DIODE ? 4 : 0) |
-                                                      (smode[s] == SIDE_REFLECT ? 8 : 0)); };
+      /* zg_side: the side, | 4 with the diode, | 8 for a mirror copy, | 16
+       * negating all three velocity components (no-slip); 32 marks a
+       * window-only entry (pair (ghost, ghost)): flowthrough's azimuthal
+       * fixed window, run as its own layer after every r copy, since the
+       * second ghost layer copies the first before the window is set */
+      auto flags = [&](int s){
+         const int m = smode[s];
+         return (unsigned char)(s | ((m == SIDE_ZG_DIODE || m == SIDE_ZG_DIODE_PHIWIN) ? 4 : 0) |
+                                (side_mirror(m) ? 8 : 0) | (m == SIDE_NOSLIP ? 16 : 0));
+      };
       int maxr = 0, maxz = 0;
       for( int d=0 ; d<ndisk ; ++d ){
          const DiskParams &D = b->dparams[d];
@@ -600,12 +615,26 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
                if( (k < D.NgZa && smode[2] == SIDE_FIXED) || (k >= D.Nz - D.NgZb && smode[3] == SIDE_FIXED) )
                   continue;
                if( l < D.NgRa && side_copies(smode[0]) ){
-                  int j = D.NgRa-1-l, j1 = smode[0] == SIDE_REFLECT ? 2*D.NgRa-j-1 : j+1;
+                  int j = D.NgRa-1-l, j1 = side_mirror(smode[0]) ? 2*D.NgRa-j-1 : j+1;
                   b->zg_pairs.push_back(make_int2(base+j, base+j1)); b->zg_side.push_back(flags(0));
                }
                if( l < D.NgRb && side_copies(smode[1]) ){
-                  int j = D.Nr-D.NgRb+l, j1 = smode[1] == SIDE_REFLECT ? 2*(D.Nr-D.NgRb)-j-1 : j-1;
+                  int j = D.Nr-D.NgRb+l, j1 = side_mirror(smode[1]) ? 2*(D.Nr-D.NgRb)-j-1 : j-1;
                   b->zg_pairs.push_back(make_int2(base+j, base+j1)); b->zg_side.push_back(flags(1));
+               }
+            }
+         }
+      }
+      if( smode[1] == SIDE_ZG_DIODE_PHIWIN ){
+         b->zg_off.push_back((int)b->zg_pairs.size());
+         for( int d=0 ; d<ndisk ; ++d ){
+            const DiskParams &D = b->dparams[d];
+            for( int k=0 ; k<D.Nz ; ++k ){
+               if( (k < D.NgZa && smode[2] == SIDE_FIXED) || (k >= D.Nz - D.NgZb && smode[3] == SIDE_FIXED) )
+                  continue;
+               for( int j=D.Nr-D.NgRb ; j<D.Nr ; ++j ){
+                  int A = D.ann0 + j + D.Nr*k;
+                  b->zg_pairs.push_back(make_int2(A, A)); b->zg_side.push_back((unsigned char)(1 | 32));
                }
             }
          }
@@ -617,12 +646,12 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
             if( D.Nz < 2 || params[d].Z_Periodic ) continue;
             for( int j=0 ; j<D.Nr ; ++j ){
                if( l < D.NgZa && side_copies(smode[2]) ){
-                  int k = D.NgZa-1-l, k1 = smode[2] == SIDE_REFLECT ? 2*D.NgZa-k-1 : k+1;
+                  int k = D.NgZa-1-l, k1 = side_mirror(smode[2]) ? 2*D.NgZa-k-1 : k+1;
                   b->zg_pairs.push_back(make_int2(D.ann0 + j + D.Nr*k, D.ann0 + j + D.Nr*k1));
                   b->zg_side.push_back(flags(2));
                }
                if( l < D.NgZb && side_copies(smode[3]) ){
-                  int k = D.Nz-D.NgZb+l, k1 = smode[3] == SIDE_REFLECT ? 2*(D.Nz-D.NgZb)-k-1 : k-1;
+                  int k = D.Nz-D.NgZb+l, k1 = side_mirror(smode[3]) ? 2*(D.Nz-D.NgZb)-k-1 : k-1;
                   b->zg_pairs.push_back(make_int2(D.ann0 + j + D.Nr*k, D.ann0 + j + D.Nr*k1));
                   b->zg_side.push_back(flags(3));
                }

@@ -30,7 +30,7 @@ struct disco_batch {
    int zg_diode, zg_omk;                /* outflow diode; Omega from initial() in r ghosts */
    int any_visc;                        /* some disk has Use_Viscosity (Euler) */
    int gr;                              /* HYDRO = grmhd2 (FP64, no constrained transport) */
-   std::vector<int> zg_off;             /* layer groups: r layers, then z layers */
+   std::vector<int> zg_off;             /* layer groups: r layers, a window layer, then z layers */
    int2 *d_zg_pairs;
    size_t zg_smem;                      /* dynamic shared memory of k_zerograd */
    std::vector<int2> zpole;             /* 3D CT z-pole annuli (annulus, 0 bottom / 1 top) */

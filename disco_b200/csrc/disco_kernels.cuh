@@ -1725,6 +1725,30 @@ __global__ void k_zerograd(ViewT<R> v, const int2 *pairs, const unsigned char *s
    const int c0 = v.ann_off[a], c10 = v.ann_off[a1];
    const DiskParams &P = v.dp[v.ann_disk[a]];
    const double Pmax = P.Pmax;
+   if( sides[blockIdx.x] & 32 ){
+      /* boundary_fixed_phi_rout(0.3 pi, 1.7 pi) (boundary_functions.c:809-843)
+       * on a ghost annulus whose copies are all done (flowthrough.c:10-12):
+       * set_cell_init on the cells whose centre lies in the window, no copy */
+      const double phia = 0.3*DISCO_PI, phib = 1.7*DISCO_PI;
+      const int j = v.ann_j[a], k = v.ann_k[a];
+      const double *rj = v.rj + P.rj0 + 1;
+      const double *zk = v.zk + P.zk0 + 1;
+      const int N = v.Ncell;
+      for( int i=threadIdx.x ; i<np ; i+=blockDim.x ){
+         const double phip = v.piph[c0+i], dp = v.dphi[c0+i];
+         double phi = phip - 0.5*dp;
+         for( int w=0 ; phi < phia && w <= WRAP_CAP ; ++w ) phi += Pmax;
+         if( phi < phib ){
+            double x[3] = { centroid_r(rj[j], rj[j-1]), 0.5*(phip + (phip - dp)), 0.5*(zk[k]+zk[k-1]) };
+            double tp[Q];
+            initial<Q, (Q > 6 ? 8 : 5)>(P, tp, x);
+            if( P.rotframe ) tp[UPP] -= P.RotOmega;
+#pragma unroll
+            for( int q=0 ; q<Q ; ++q ) v.prim[q*N + c0 + i] = (R)tp[q];
+         }
+      }
+      return;
+   }
    double *sp = reinterpret_cast<double*>(zg_smem);          /* ghost piph, dphi */
    double *sd = sp + np;
    double *sp1 = sd + np;                                    /* source piph, dphi */
@@ -1830,7 +1854,9 @@ __global__ void k_zerograd(ViewT<R> v, const int2 *pairs, const unsigned char *s
       R out[Q];
 #pragma unroll
       for( int q=0 ; q<Q ; ++q ) out[q] = (R)acc[q];
-      if( sflags & 8 ){               /* mirror copy: reflect_prims (euler.c:405, mhd.c:507) */
+      if( sflags & 16 ){              /* no-slip: reflect_prims in r, phi and z */
+         out[URR] = -out[URR]; out[UPP] = -out[UPP]; out[UZZ] = -out[UZZ];
+      }else if( sflags & 8 ){         /* mirror copy: reflect_prims (euler.c:405, mhd.c:507) */
          if( side <= 1 ) out[URR] = -out[URR];
          else            out[UZZ] = -out[UZZ];
       }

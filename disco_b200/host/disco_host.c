@@ -161,6 +161,7 @@ int disco_read_opt(const char *path, disco_modules *m){
    else if( !strcmp(v, "tube") ) m->boundary = DISCO_BC_TUBE;
    else if( !strcmp(v, "surfaceGravBox") ) m->boundary = DISCO_BC_SURFACEGRAVBOX;
    else if( !strcmp(v, "fixed_gap") ) m->boundary = DISCO_BC_FIXED_GAP;
+   else if( !strcmp(v, "flowthrough") ) m->boundary = DISCO_BC_FLOWTHROUGH;
    else return DISCO_ERR_UNSUPPORTED;
    if( opt_value(path, "PLANETS", v, sizeof v) ) return DISCO_ERR_ARG;
    if( !strcmp(v, "none") ) m->planets = DISCO_PLANETS_NONE;

@@ -88,7 +88,7 @@ int disco_gpu_init( const struct domain * d ){
    static const char *const bcs[] = {"fixed", "zerograd", "fixed3d", "polar", "outflow3d",
                                      "zerograd_omk", "accrete3d", "polar3d", "horizon",
                                      "horizon3d", "horizon_bin", "fixRrefZ", "tube",
-                                     "surfaceGravBox", "fixed_gap"};
+                                     "surfaceGravBox", "fixed_gap", "flowthrough"};
    static const char *const pls[] = {"none", "sun", "cm2", "binary_soft", "circular", "cm"};
    static const char *const ics[] = {"kepler_noise", "mhd_shear_noise", "gr_torus_noise"};
    static const int ic_ids[] = {DISCO_IC_KEPLER_NOISE, DISCO_IC_MHD_SHEAR_NOISE, DISCO_IC_GR_TORUS_NOISE};
@@ -100,7 +100,7 @@ int disco_gpu_init( const struct domain * d ){
    disco_modules m;
    memset(&m, 0, sizeof m);
    m.hydro = module_id(HYDRO, hydros, 3);
-   m.boundary = module_id(BOUNDARY, bcs, 15);
+   m.boundary = module_id(BOUNDARY, bcs, 16);
    m.planets = module_id(PLANETS, pls, 6);
    int ii = module_id(INITIAL, ics, 3);
    m.initial = ii >= 0 ? ic_ids[ii] : -1;

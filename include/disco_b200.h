@@ -61,7 +61,8 @@ enum disco_boundary { DISCO_BC_FIXED = 0, DISCO_BC_ZEROGRAD = 1, DISCO_BC_FIXED3
                       DISCO_BC_POLAR = 3, DISCO_BC_OUTFLOW3D = 4, DISCO_BC_ZEROGRAD_OMK = 5,
                       DISCO_BC_ACCRETE3D = 6, DISCO_BC_POLAR3D = 7, DISCO_BC_HORIZON = 8,
                       DISCO_BC_HORIZON3D = 9, DISCO_BC_HORIZON_BIN = 10, DISCO_BC_FIXRREFZ = 11,
-                      DISCO_BC_TUBE = 12, DISCO_BC_SURFACEGRAVBOX = 13, DISCO_BC_FIXED_GAP = 14 };
+                      DISCO_BC_TUBE = 12, DISCO_BC_SURFACEGRAVBOX = 13, DISCO_BC_FIXED_GAP = 14,
+                      DISCO_BC_FLOWTHROUGH = 15 };
 enum disco_planets  { DISCO_PLANETS_NONE = 0, DISCO_PLANETS_SUN = 1, DISCO_PLANETS_CM2 = 2,
                       DISCO_PLANETS_BINARY_SOFT = 3, DISCO_PLANETS_CIRCULAR = 4,
                       DISCO_PLANETS_CM = 5 };

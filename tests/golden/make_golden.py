@@ -202,6 +202,10 @@ CASES = {
     "c0_bc_tube": ("c0_bc_tube", dict(BC3D, NoBC_Rmin=1), 5),
     "c0_bc_surfaceGravBox": ("c0_bc_surfaceGravBox", dict(BC3D), 5),
     "c0_bc_fixed_gap": ("c0_bc_fixed_gap", dict(BC3D), 5),
+    # flowthrough: a no-slip inner wall (mirror copy, all three velocity
+    # components negated), outflow outer r fixed again on 0.3 pi < phi < 1.7 pi
+    # after the copy, fixed z
+    "c0_bc_flowthrough": ("c0_bc_flowthrough", dict(BC3D), 5),
     "c1_polar3d_zpole": ("c1_polar3d", {"Num_R": 8, "Num_Z": 6, "R_Min": 0.0, "R_Max": 2.0,
                                         "NoBC_Rmin": 1, "Init_Par2": 1, "Init_Par4": 10.0,
                                         "Constrained_Transport": 1, "Init_Par5": 20.0,
@@ -218,7 +222,8 @@ BASE_PAR = {"c0_kepler2d": "c0_kepler2d", "c0_cm2": "c0_kepler2d", "c0_nograv": 
             "c0_diag_euler3d": "c0_kepler2d", "c1_diag_mhdmri": "c1_mhd2d", "c3_grtorus": "c3_grtorus", "c4_binary3d": "c4_binary3d",
             "c0_horizon3d": "c0_kepler2d", "c1_polar3dbc": "c1_mhd3d", "c3_grhorizon": "c3_grtorus",
             "c0_hbin": "c0_kepler2d", "c0_bc_fixRrefZ": "c0_kepler2d", "c0_bc_tube": "c0_kepler2d",
-            "c0_bc_surfaceGravBox": "c0_kepler2d", "c0_bc_fixed_gap": "c0_kepler2d"}
+            "c0_bc_surfaceGravBox": "c0_kepler2d", "c0_bc_fixed_gap": "c0_kepler2d",
+            "c0_bc_flowthrough": "c0_kepler2d"}
 
 
 def par_text(cfg_par, overrides):

@@ -17,10 +17,12 @@ fixtures depend on no libm call except where noted):
   with CT.
 - polar3d: fixed outer r and z (set_cell_init) on an axis grid, 3D MHD with
   CT.
-- fixRrefZ, tube, surfaceGravBox, fixed_gap: composed per side from fixed
+- fixRrefZ, tube, surfaceGravBox, fixed_gap, flowthrough: composed per side from fixed
   (set_cell_init), zero-gradient (with or without the outflow diode) and
   mirror copies (boundary_reflect_*: the annulus as far inside as the ghost
-  is outside, normal velocity negated), r sides before z sides; 3D hydro.
+  is outside, normal velocity negated; no-slip: all three), r sides before z
+  sides (flowthrough's outer r fixed again on an azimuthal window after its
+  copy); 3D hydro.
 - horizon_bin: outer r and z ghosts at the midpoint, and every cell inside
   one of two spheres of radius 0.8 at x = +-5 re-initialised there each
   substep, out of the dt minimum from its first excision on (the
@@ -44,7 +46,8 @@ from helpers import case_disk, observed_slots, par_with, rel_l1, rel_l1_cols
 pytestmark = pytest.mark.gpu
 
 POLAR = ["c0_polar", "c1_polar_ct", "c1_polar3d", "c1_polar3dbc", "c0_horizon3d"]
-COMPOSED = ["c0_bc_fixRrefZ", "c0_bc_tube", "c0_bc_surfaceGravBox", "c0_bc_fixed_gap"]
+COMPOSED = ["c0_bc_fixRrefZ", "c0_bc_tube", "c0_bc_surfaceGravBox", "c0_bc_fixed_gap",
+            "c0_bc_flowthrough"]
 CASES = POLAR + ["c0_outflow3d", "c1_omk3d", "c1_accrete3d", "c0_hbin", "c0_hbin3d"] + COMPOSED
 TOL = 1e-12
 

@@ -111,7 +111,8 @@ def test_no_device_is_a_clean_error():
 
 @pytest.mark.parametrize("case,module", [("c0_bc_fixRrefZ", "fixRrefZ"), ("c0_bc_tube", "tube"),
                                          ("c0_bc_surfaceGravBox", "surfaceGravBox"),
-                                         ("c0_bc_fixed_gap", "fixed_gap")])
+                                         ("c0_bc_fixed_gap", "fixed_gap"),
+                                         ("c0_bc_flowthrough", "flowthrough")])
 def test_composed_boundary_modules_parse(case, module):
     disk, g = case_disk(case)
     assert disk.modules.boundary == db.BOUNDARY[module]
