@@ -1714,7 +1714,9 @@ __device__ __forceinline__ int zg_walk(const double *sp, const double *sd, const
  * argument of the same functions, used by outflow3d, zerograd_omk and
  * accrete3d), with `omk` the r ghosts then take Omega from the Initial
  * module (boundary_fixed_q_rinn / _rout with q = UPP, :662-718,
- * set_cell_init_q :33-47; zerograd_omk). */
+ * set_cell_init_q :33-47; zerograd_omk).  Higher bits of sides[]: 4 the
+ * diode on this side only, 8 a mirror copy (boundary_reflect_*), 16 no-slip
+ * (boundary_noslip_*, :914-1100), 32 a window-only entry with no copy. */
 template<int Q, class R>
 __global__ void k_zerograd(ViewT<R> v, const int2 *pairs, const unsigned char *sides, int diode,
                            int omk){
