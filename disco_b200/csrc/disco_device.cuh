@@ -592,47 +592,46 @@ __device__ __forceinline__ void hlld_solve(const DiskParams &P, R w, const R *pr
    pL[UZZ] *= hz; pR[UZZ] *= hz;
    R vel[5], Pt_star;
    hlld_velocities<R>(P, pL, pR, n0, n1, n2, vel, &Pt_star);
-   if( w < vel[2] ){
-      R UL[8];
-      hlld_flux<R>(P, pL, F, n0, n1, n2);
-      hlld_prim_to_cons<R>(P, pL, UL);
-      if( w < vel[0] ){
-         hlld_prim_to_cons<R>(P, pL, U);
-      }else if( w < vel[1] ){
-         hlld_single_star<R>(P, pL, U, vel[0], vel[2], Pt_star, n0, n1, n2);
+   /* The two sides of the contact run the same operations on mirrored
+    * inputs, so they are one code path here on the side K the face's frame
+    * lies on (left: w < S_M) and the other side O: neighbouring faces on
+    * different sides (w close to S_M, the common case on a moving mesh) do
+    * not serialise the warp, and every value is the one the branch of that
+    * side computes. */
+   const bool left = w < vel[2];
+   R pK[Q], pO[Q];
 #pragma unroll
-         for( int q=0 ; q<8 ; ++q ) F[q] += vel[0]*( U[q] - UL[q] );
-      }else{
-         R UsL[8], UsR[8];
-         hlld_single_star<R>(P, pL, UsL, vel[0], vel[2], Pt_star, n0, n1, n2);
-         hlld_single_star<R>(P, pR, UsR, vel[4], vel[2], Pt_star, n0, n1, n2);
-         hlld_double_star<R>(UsL, UsR, U, vel, n0, n1, n2, 0);
+   for( int q=0 ; q<Q ; ++q ){ pK[q] = left ? pL[q] : pR[q]; pO[q] = left ? pR[q] : pL[q]; }
+   const R S_K = left ? vel[0] : vel[4], S_O = left ? vel[4] : vel[0];
+   const R Ss_K = left ? vel[1] : vel[3];
+   /* 0: outside the fast wave, 1: between the fast and the Alfven wave,
+    * 2: between the Alfven wave and the contact */
+   const int region = left ? ( w < vel[0] ? 0 : ( w < vel[1] ? 1 : 2 ) )
+                           : ( w > vel[4] ? 0 : ( w > vel[3] ? 1 : 2 ) );
+   R UK[8];
+   hlld_flux<R>(P, pK, F, n0, n1, n2);
+   hlld_prim_to_cons<R>(P, pK, UK);
+   if( region == 0 ){
 #pragma unroll
-         for( int q=0 ; q<8 ; ++q ) F[q] += vel[1]*( U[q] - UsL[q] ) + vel[0]*( UsL[q] - UL[q] );
-      }
-#pragma unroll
-      for( int q=8 ; q<Q ; ++q ){ U[q] = pL[q]*U[DDD]; F[q] = pL[q]*F[DDD]; }
+      for( int q=0 ; q<8 ; ++q ) U[q] = UK[q];
    }else{
-      R UR[8];
-      hlld_flux<R>(P, pR, F, n0, n1, n2);
-      hlld_prim_to_cons<R>(P, pR, UR);
-      if( w > vel[4] ){
-         hlld_prim_to_cons<R>(P, pR, U);
-      }else if( w > vel[3] ){
-         hlld_single_star<R>(P, pR, U, vel[4], vel[2], Pt_star, n0, n1, n2);
+      R UsK[8];
+      hlld_single_star<R>(P, pK, UsK, S_K, vel[2], Pt_star, n0, n1, n2);
+      if( region == 1 ){
 #pragma unroll
-         for( int q=0 ; q<8 ; ++q ) F[q] += vel[4]*( U[q] - UR[q] );
+         for( int q=0 ; q<8 ; ++q ){ U[q] = UsK[q]; F[q] += S_K*( U[q] - UK[q] ); }
       }else{
-         R UsL[8], UsR[8];
-         hlld_single_star<R>(P, pL, UsL, vel[0], vel[2], Pt_star, n0, n1, n2);
-         hlld_single_star<R>(P, pR, UsR, vel[4], vel[2], Pt_star, n0, n1, n2);
-         hlld_double_star<R>(UsL, UsR, U, vel, n0, n1, n2, 1);
+         R UsO[8], UsL[8], UsR[8];
+         hlld_single_star<R>(P, pO, UsO, S_O, vel[2], Pt_star, n0, n1, n2);
 #pragma unroll
-         for( int q=0 ; q<8 ; ++q ) F[q] += vel[3]*( U[q] - UsR[q] ) + vel[4]*( UsR[q] - UR[q] );
+         for( int q=0 ; q<8 ; ++q ){ UsL[q] = left ? UsK[q] : UsO[q]; UsR[q] = left ? UsO[q] : UsK[q]; }
+         hlld_double_star<R>(UsL, UsR, U, vel, n0, n1, n2, left ? 0 : 1);
+#pragma unroll
+         for( int q=0 ; q<8 ; ++q ) F[q] += Ss_K*( U[q] - UsK[q] ) + S_K*( UsK[q] - UK[q] );
       }
-#pragma unroll
-      for( int q=8 ; q<Q ; ++q ){ U[q] = pR[q]*U[DDD]; F[q] = pR[q]*F[DDD]; }
    }
+#pragma unroll
+   for( int q=8 ; q<Q ; ++q ){ U[q] = pK[q]*U[DDD]; F[q] = pK[q]*F[DDD]; }
    const R brfac = R(1.0)/r, bpfac = R(1.0), bzfac = R(1.0);   /* bfield_scale_factor */
    F[SRR] *= hr; F[LLL] *= hp; F[SZZ] *= hz;
    F[BRR] *= brfac/hr; F[BPP] *= bpfac/hp; F[BZZ] *= bzfac/hz;

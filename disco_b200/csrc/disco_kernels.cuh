@@ -1098,19 +1098,30 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
          if constexpr ( sizeof(R) != sizeof(double) ) cc[q] = (double)v.ccarry[q*N + c];
          else cc[q] = 0.0;
       }
+      /* The face fluxes: in the FP64 path added to cons one by one in the
+       * reference's order; in the mixed form (FP32 fluxes) summed in a plain
+       * FP64 accumulator, exact for a handful of FP32 values whose exponents
+       * lie within 29 binades, then added to cons once, compensated. */
+      double fs[Q];
+#pragma unroll
+      for( int q=0 ; q<Q ; ++q ) fs[q] = 0.0;
+      auto addf = [&](int q, double x){
+         if constexpr ( sizeof(R) == sizeof(double) ) cons[q] += x;
+         else fs[q] += x;
+      };
       /* phi faces: loop order of phi_flux */
       const int t = threadIdx.x;
       if( i > 0 ){
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ){
-            acc<R>(cons[q], cc[q], (double)sG[q][t]);
-            acc<R>(cons[q], cc[q], -(double)sG[q][t+1]);
+            addf(q, (double)sG[q][t]);
+            addf(q, -(double)sG[q][t+1]);
          }
       }else{
 #pragma unroll
          for( int q=0 ; q<Q ; ++q ){
-            acc<R>(cons[q], cc[q], -(double)sG[q][t+1]);
-            acc<R>(cons[q], cc[q], (double)sG[q][t]);
+            addf(q, -(double)sG[q][t+1]);
+            addf(q, (double)sG[q][t]);
          }
       }
       /* r faces: inner track (cell is R) then outer track (cell is L) */
@@ -1122,7 +1133,7 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
       if( j <= P.Nr-2 ) Rout = cell_runs(v, v.consL, P.trr0 + j + (P.Nr-1)*k, c0, np, i, I0);
       const size_t Nf = v.Nf;
 #define ADD_RUN(s,e,sg) for( int f=(s) ; f<=(e) ; ++f ){ \
-      _Pragma("unroll") for( int q=0 ; q<Q ; ++q ) acc<R>(cons[q], cc[q], sg (double)v.fG[q*Nf + f]); }
+      _Pragma("unroll") for( int q=0 ; q<Q ; ++q ) addf(q, sg (double)v.fG[q*Nf + f]); }
       ADD_RUN(Rin.s1, Rin.e1, +)
       ADD_RUN(Rin.s2, Rin.e2, +)
       ADD_RUN(Rout.s1, Rout.e1, -)
@@ -1141,6 +1152,10 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
          }
       }
 #undef ADD_RUN
+      if constexpr ( sizeof(R) != sizeof(double) ){
+#pragma unroll
+         for( int q=0 ; q<Q ; ++q ) acc<R>(cons[q], cc[q], fs[q]);
+      }
       /* add_source with the pre-move cell */
       double prim[Q];
 #pragma unroll
