@@ -865,15 +865,17 @@ __global__ void k_soa_to_aos(const T *src, double *dst, size_t N, int Q){
 }
 static int staging(disco_batch *b){
    if( b->d_stage ) return DISCO_OK;
-   if( cudaMalloc(&b->d_stage, (size_t)b->Q*b->ncell*sizeof(double)) != cudaSuccess ){
+   const size_t w = (size_t)(b->Q > b->nfs ? b->Q : b->nfs);
+   if( cudaMalloc(&b->d_stage, w*b->ncell*sizeof(double)) != cudaSuccess ){
       b->d_stage = NULL;
       return DISCO_ERR_CUDA;
    }
    return DISCO_OK;
 }
 template<class T>
-static int upload_q(disco_batch *b, T *dst, const double *src){
-   size_t N = b->ncell; int Q = b->Q;
+static int upload_q(disco_batch *b, T *dst, const double *src, int Q = 0){
+   size_t N = b->ncell;
+   if( Q == 0 ) Q = b->Q;
    int s = staging(b);
    if( s ) return s;
    CK(cudaMemcpyAsync(b->d_stage, src, (size_t)Q*N*sizeof(double), cudaMemcpyHostToDevice, b->stream));
@@ -883,8 +885,9 @@ static int upload_q(disco_batch *b, T *dst, const double *src){
    return DISCO_OK;
 }
 template<class T>
-static int download_q(disco_batch *b, double *dst, const T *src){
-   size_t N = b->ncell; int Q = b->Q;
+static int download_q(disco_batch *b, double *dst, const T *src, int Q = 0){
+   size_t N = b->ncell;
+   if( Q == 0 ) Q = b->Q;
    int s = staging(b);
    if( s ) return s;
    k_soa_to_aos<T><<<nblk(N, 256), 256, 0, b->stream>>>(src, b->d_stage, N, Q);
@@ -913,10 +916,11 @@ extern "C" int disco_batch_set_cells(disco_batch *b, const double *prim, const d
    if( prim && (s = upload_r(b, b->vd.prim, prim)) ) return s;
    if( cons && (s = upload_q<double>(b, b->vd.cons, cons)) ) return s;
    if( b->ct ){                     /* Phi[0 .. num_faces-1] per cell, cell-major */
-      const int F = b->nfs;
-      std::vector<double> t(F*N, 0.0);
-      if( Phi ) for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<F ; ++q ) t[q*N + c] = Phi[F*c + q];
-      CK(xfer(b, b->vd.Phi, t.data(), t.size()*sizeof(double), cudaMemcpyHostToDevice));
+      if( Phi ){
+         if( (s = upload_q<double>(b, b->vd.Phi, Phi, b->nfs)) ) return s;
+      }else{
+         CK(cudaMemsetAsync(b->vd.Phi, 0, (size_t)b->nfs*N*sizeof(double), b->stream));
+      }
    }
    CK(xfer(b, b->vd.piph, piph, N*sizeof(double), cudaMemcpyHostToDevice));
    CK(xfer(b, b->vd.dphi, dphi, N*sizeof(double), cudaMemcpyHostToDevice));
@@ -941,12 +945,7 @@ extern "C" int disco_batch_get_cells(disco_batch *b, double *prim, double *cons,
    CK(cudaStreamSynchronize(b->stream));
    size_t N = b->ncell;
    int s;
-   if( Phi && b->ct ){
-      const int F = b->nfs;
-      std::vector<double> t(F*N);
-      CK(xfer(b, t.data(), b->vd.Phi, t.size()*sizeof(double), cudaMemcpyDeviceToHost));
-      for( size_t c=0 ; c<N ; ++c ) for( int q=0 ; q<F ; ++q ) Phi[F*c + q] = t[q*N + c];
-   }
+   if( Phi && b->ct && (s = download_q<double>(b, Phi, b->vd.Phi, b->nfs)) ) return s;
    if( prim && (s = download_r(b, prim, b->vd.prim)) ) return s;
    if( cons && (s = download_q<double>(b, cons, b->vd.cons)) ) return s;
    if( piph ) CK(xfer(b, piph, b->vd.piph, N*sizeof(double), cudaMemcpyDeviceToHost));

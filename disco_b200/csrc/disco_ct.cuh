@@ -347,11 +347,15 @@ __global__ void __launch_bounds__(CB) k_ct_line(ViewT<R> v){
       v.rk[m*N + c] = e;
       /* the reference's state at step e */
       int cur[4];
+      bool bad = false;
       for( int n=0 ; n<4 ; ++n ){
          int o = v.ann_off[an[n]], nn = v.ann_np[an[n]];
-         int s = (v.I0[an[n]] + cnt[n]) % nn;
+         int s = v.I0[an[n]] + cnt[n];          /* I0 < nn, 0 <= cnt <= nn */
+         if( s >= nn ) s -= nn;
+         if( s < 0 || s >= nn ){ bad = true; s = 0; }
          cur[n] = o + s;
       }
+      if( bad ){ err |= ERRF_INTERNAL; continue; }
       int LR_alt = 0, UD_alt = 0;
       int w4 = ct_which4(v.piph[cur[0]], v.piph[cur[1]], v.piph[cur[2]], v.piph[cur[3]],
                          &LR_alt, &UD_alt, 0, Pmax, &err);
