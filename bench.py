@@ -129,6 +129,9 @@ def kernel_bytes_mhd(name, first, N, Nfr, Nfz, mixed):
     if name in ("k_gradr", "k_gradz"):
         nf = Nfr if name == "k_gradr" else Nfz
         return nf * (q * wr + w) + N * (q * wr + 2 * w + 8)
+    if name == "k_grad":
+        # r and z in one launch: both face sets, both gradients written
+        return (Nfr + Nfz) * (q * wr + w) + N * (2 * q * wr + 2 * w + 16)
     if name == "k_faces":
         nf = Nfr + Nfz
         if first:

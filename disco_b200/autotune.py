@@ -138,7 +138,7 @@ def _child(lib, workload, precision, reps):
         tot = {}
         for name, ms in b.kernel_times(cap=128):
             tot[name] = tot.get(name, 0.0) + ms
-        tot["k_grad"] = tot.get("k_gradr", 0.0) + tot.get("k_gradz", 0.0)
+        tot["k_grad"] = tot.get("k_grad", 0.0) + tot.get("k_gradr", 0.0) + tot.get("k_gradz", 0.0)
         tot["k_flux"] = tot.get("k_flux_r", 0.0) + tot.get("k_flux_z", 0.0)
         for k, v in tot.items():
             per.setdefault(k, []).append(v)

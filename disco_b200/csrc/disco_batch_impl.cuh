@@ -197,8 +197,8 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    if( first && b->any_mm3 ){ k_wmean<R><<<nblk(v.Nann, WM_WARPS), 32*WM_WARPS, 0, s>>>(v, 1); mark(b, "k_wmean"); }
    k_I0<R><<<nblk((size_t)v.Nann*32, 128), 128, 0, s>>>(v);           mark(b, "k_I0");
    k_faces<Q,R><<<nfb, FB, 0, s>>>(v, 1);                             mark(b, "k_faces");
-   k_grad<Q,1,R><<<ncb, CB, 0, s>>>(v);                               mark(b, "k_gradr");
-   if( b->any_3d ){ k_grad<Q,2,R><<<ncb, CB, 0, s>>>(v);              mark(b, "k_gradz"); }
+   if( b->any_3d ){ k_grad_rz<Q,R><<<ncb, CB, 0, s>>>(v);             mark(b, "k_grad"); }
+   else{ k_grad<Q,1,R><<<ncb, CB, 0, s>>>(v);                         mark(b, "k_gradr"); }
    launch_flux_t<Q,NC,1,R,GR>(b, v);                                  mark(b, "k_flux_r");
    if( b->any_3d ){ launch_flux_t<Q,NC,2,R,GR>(b, v);                 mark(b, "k_flux_z"); }
    bool upd_visc = false;

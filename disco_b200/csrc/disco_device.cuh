@@ -808,12 +808,12 @@ __device__ __forceinline__ void add_noise(int type, double absMag, double relMag
    }
 }
 /* planetaryForce(), planet.c:99-150, modes 0 and 1 */
-__device__ __forceinline__ void planetary_force(int grav2D, const Planet &pl, double r,
-                                                double phi, double z, double *fr,
-                                                double *fp, double *fz, int mode = 0){
+/* the same with sin and cos of the cell's phi given (one sincos per cell
+ * for all planets) */
+__device__ __forceinline__ void planetary_force_sc(int grav2D, const Planet &pl, double r,
+                                                   double sinp, double cosp, double z, double *fr,
+                                                   double *fp, double *fz, int mode = 0){
    double rp = pl.r;
-   double sinp, cosp;
-   sincos(phi, &sinp, &cosp);
    double cpp = pl.cphi, spp = pl.sphi;             /* cos, sin of the planet's phi */
    if( grav2D == 1 ) z = 0.0;
    else if( grav2D == 2 ){ rp = r; cpp = cosp; spp = sinp; z = 1.0; }
@@ -836,6 +836,13 @@ __device__ __forceinline__ void planetary_force(int grav2D, const Planet &pl, do
    *fr = cosap*f1*sint;
    *fp = sinap*f1*sint;
    *fz = f1*cost;
+}
+__device__ __forceinline__ void planetary_force(int grav2D, const Planet &pl, double r,
+                                                double phi, double z, double *fr,
+                                                double *fp, double *fz, int mode = 0){
+   double sinp, cosp;
+   sincos(phi, &sinp, &cosp);
+   planetary_force_sc(grav2D, pl, r, sinp, cosp, z, fr, fp, fz, mode);
 }
 
 /* ------------------------------------------------------------ initial */

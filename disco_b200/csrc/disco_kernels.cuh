@@ -733,6 +733,13 @@ template<int Q, int DIM, class R>
 __global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD_GRAD : MB_GRAD) k_grad(ViewT<R> v){
    grad_body<Q,DIM,R>(v, blockIdx.x);
 }
+/* both directions of a 3D grid in one launch: the cell's annulus data are
+ * read once and the two gathers' loads overlap */
+template<int Q, class R>
+__global__ void __launch_bounds__(CB, Q > 6 ? MB_MHD_GRAD : MB_GRAD) k_grad_rz(ViewT<R> v){
+   grad_body<Q,1,R>(v, blockIdx.x);
+   grad_body<Q,2,R>(v, blockIdx.x);
+}
 
 /* The viscous flux of a face, compiled only into the viscous instances of
  * k_flux_t / k_update (template VISC) so that the inviscid kernels keep
@@ -1200,12 +1207,13 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
          double om_z = 0.0;
          acc<R>(cons[TAU], cc[TAU], dVdt*rho*( r*vr*om*om - r*r*(omega-om)*(vr*om_r + vz*om_z)));
       }
+      double sphi = 0.0, cphi = 1.0;
+      if( P.npl > 0 ) sincos(phim + 0.5*dph, &sphi, &cphi);   /* the cell's phi, all planets */
       for( int p=0 ; p<P.npl ; ++p ){   /* planet_src, planet.c:152-196 */
          double rho = prim[RHO], vr = prim[URR], vz = prim[UZZ], omega = prim[UPP];
-         double phi = phim + 0.5*dph;
          double x2 = centroid_z(zp, zm);
          double F0, F1, F2;
-         planetary_force(P.grav2D, S.pl[p], r, phi, x2, &F0, &F1, &F2);
+         planetary_force_sc(P.grav2D, S.pl[p], r, sphi, cphi, x2, &F0, &F1, &F2);
          double hr = 1.0, hp = r, hz = 1.0;
          if( P.polar ){ double adj = sin(0.5*dph)/(0.5*dph); F0 *= adj; F1 *= adj; }
          acc<R>(cons[SRR], cc[SRR], rho*hr*F0*dVdt);
