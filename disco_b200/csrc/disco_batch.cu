@@ -582,6 +582,25 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    b->line_off.push_back(b->line_ne);
    b->ncell = cell;
 
+   /* k_faces' block order: per disk and layer k, for each j the r track
+    * (j,k)-(j+1,k) and the z track (j,k)-(j,k+1), so that the tracks reading
+    * an annulus run close together and its cells are read from L2; and the
+    * flux kernels' blocks, per direction, of the tracks with fluxes */
+   for( int d=0 ; d<ndisk ; ++d ){
+      const DiskParams &D = b->dparams[d];
+      auto push = [&](int t){
+         int nf = b->ann_np[b->tr_a[t]] + b->ann_np[b->tr_b[t]];
+         for( int f0=0 ; f0<nf ; f0+=FB ) b->fblk_rz.push_back(make_int2(t, f0));
+      };
+      for( int k=0 ; k<D.Nz ; ++k ) for( int j=0 ; j<D.Nr ; ++j ){
+         if( j < D.Nr-1 ) push(D.trr0 + j + (D.Nr-1)*k);
+         if( k < D.Nz-1 ) push(D.trz0 + j + D.Nr*k);
+      }
+   }
+   if( b->fblk_rz.size() != b->fblk.size() ){ delete b; return DISCO_ERR_INTERNAL; }
+   for( const int2 &fb : b->fblk )
+      if( b->tr_flux[fb.x] ) b->fblk_fl[b->tr_dim[fb.x] - 1].push_back(fb);
+
    /* zerograd layers (boundary_functions.c:269-440): r ghosts from the real
     * cells outwards, then z ghosts (all j, ghosts included); sides[] of each
     * pair: 0 inner r, 1 outer r, 2 lower z, 3 upper z */
@@ -680,6 +699,8 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.tr_dxL = dupload(b, b->tr_dxL); v.tr_dxR = dupload(b, b->tr_dxR);
    v.tr_dim = dupload(b, b->tr_dim);
    v.cblk = dupload(b, b->cblk); v.fblk = dupload(b, b->fblk); v.ublk = dupload(b, b->ublk);
+   b->d_fblk_rz = dupload(b, b->fblk_rz);
+   b->d_fblk_fl[0] = dupload(b, b->fblk_fl[0]); b->d_fblk_fl[1] = dupload(b, b->fblk_fl[1]);
    v.rj = dupload(b, b->rj); v.zk = dupload(b, b->zk);
    v.dp = dupload(b, b->dparams);
    v.ds = dupload(b, dstate);

@@ -43,6 +43,10 @@ struct disco_batch {
    std::vector<unsigned char> tr_dim;
    std::vector<double> tr_dxL, tr_dxR;
    std::vector<int2> cblk, fblk;
+   /* the same face blocks in k_faces' order (per layer, the r and z tracks of
+    * each annulus together) and the blocks k_flux_t solves per direction */
+   std::vector<int2> fblk_rz, fblk_fl[2];
+   int2 *d_fblk_rz, *d_fblk_fl[2];
    std::vector<int2> ublk;              /* k_update's blocks: chunks of CB-1 cells */
    std::vector<int> ann_blk0, ann_nblk;
    std::vector<double> rj, zk;
@@ -174,8 +178,11 @@ static void launch_c2p(disco_batch *b, const ViewT<R> &v, int last, int diag){
    else launch_c2p_nq<Q,NC,R,5,GR>(b, v, last, diag);
 }
 template<int Q, int NC, int DIM, class R, bool GR = false>
-static void launch_flux_t(disco_batch *b, const ViewT<R> &v){
-   unsigned nfb = (unsigned)b->fblk.size();
+static void launch_flux_t(disco_batch *b, const ViewT<R> &v0){
+   /* only the blocks of this direction's tracks with trans_flux faces */
+   unsigned nfb = (unsigned)b->fblk_fl[DIM-1].size();
+   if( nfb == 0 ) return;
+   ViewT<R> v = v0; v.fblk = b->d_fblk_fl[DIM-1];
    if constexpr ( NC == 5 ){
       if( b->any_visc ){ k_flux_t<Q,NC,DIM,R,true><<<nfb, FB, 0, b->stream>>>(v); return; }
    }
@@ -196,7 +203,10 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    k_begin<Q,NC,R,GR><<<ncb, CB, 0, s>>>(v, RK, first);               mark(b, "k_begin");
    if( first && b->any_mm3 ){ k_wmean<R><<<nblk(v.Nann, WM_WARPS), 32*WM_WARPS, 0, s>>>(v, 1); mark(b, "k_wmean"); }
    k_I0<R><<<nblk((size_t)v.Nann*32, 128), 128, 0, s>>>(v);           mark(b, "k_I0");
-   k_faces<Q,R><<<nfb, FB, 0, s>>>(v, 1);                             mark(b, "k_faces");
+   {  /* the same blocks in the order that keeps an annulus's three tracks together */
+      ViewT<R> vf = v; vf.fblk = b->d_fblk_rz;
+      k_faces<Q,R><<<nfb, FB, 0, s>>>(vf, 1);                          mark(b, "k_faces");
+   }
    if( b->any_3d ){ k_grad_rz<Q,R><<<ncb, CB, 0, s>>>(v);             mark(b, "k_grad"); }
    else{ k_grad<Q,1,R><<<ncb, CB, 0, s>>>(v);                         mark(b, "k_gradr"); }
    launch_flux_t<Q,NC,1,R,GR>(b, v);                                  mark(b, "k_flux_r");
@@ -212,7 +222,8 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
    if constexpr ( NC == 8 ){
       if( b->ct ){                  /* onestep.c:140-146 and 160-167 */
          k_ct_edges<R><<<ncb, CB, 0, s>>>(v);                           mark(b, "k_ct_edges");
-         k_ct_faces<R><<<nfb, FB, 0, s>>>(v);                           mark(b, "k_ct_faces");
+         ViewT<R> vrz = v; vrz.fblk = b->d_fblk_rz;      /* per-face kernels, k_faces' order */
+         k_ct_faces<R><<<nfb, FB, 0, s>>>(vrz);                         mark(b, "k_ct_faces");
          if( !b->zpole.empty() ){
             k_ct_zpole<R><<<(unsigned)b->zpole.size(), CB, 0, s>>>(v, b->d_zpole); mark(b, "k_ct_zpole");
          }
@@ -221,7 +232,7 @@ static void launch_substep(disco_batch *b, ViewT<R> v, double RK, int first, int
          }
          k_ct_update<R><<<ncb, CB, 0, s>>>(v, first);                   mark(b, "k_ct_update");
          if( first ){
-            k_ct_flag<R><<<nfb, FB, 0, s>>>(v);                         mark(b, "k_ct_flag");
+            k_ct_flag<R><<<nfb, FB, 0, s>>>(vrz);                       mark(b, "k_ct_flag");
             k_ct_flip<R><<<nblk((size_t)v.Ntr*32, 128), 128, 0, s>>>(v); mark(b, "k_ct_flip");
          }
       }
