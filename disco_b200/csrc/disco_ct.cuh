@@ -570,12 +570,19 @@ __device__ void ct_cons_B(const ViewT<R> &v, const DiskParams &P, int a, int c0,
    int c = c0 + i, cm = c0 + (i == 0 ? np-1 : i-1);
    int I0 = v.I0[a];
    double S = 0.0, T = 0.0;
-   auto sum_r = [&](int f){
-      S += v.fLR[f] == 0 ? v.Phi[2*N + v.fL[f]] : v.Phi[N + v.fR[f]];
+   /* every face of the cell's run in its inner (lower) track has the cell as
+    * R, in its outer (upper) track as L; the other side's cell is read only
+    * when that one owns the face */
+   auto sum_rin = [&](int f){
+      S += v.fLR[f] == 0 ? v.Phi[2*N + v.fL[f]] : v.Phi[N + c];
       T += v.fdA[f];
    };
-   if( j >= 1 )      ct_over_runs(v, v.consR, P.trr0 + (j-1) + (P.Nr-1)*k, c0, np, i, I0, sum_r);
-   if( j <= P.Nr-2 ) ct_over_runs(v, v.consL, P.trr0 + j + (P.Nr-1)*k, c0, np, i, I0, sum_r);
+   auto sum_rout = [&](int f){
+      S += v.fLR[f] == 0 ? v.Phi[2*N + c] : v.Phi[N + v.fR[f]];
+      T += v.fdA[f];
+   };
+   if( j >= 1 )      ct_over_runs(v, v.consR, P.trr0 + (j-1) + (P.Nr-1)*k, c0, np, i, I0, sum_rin);
+   if( j <= P.Nr-2 ) ct_over_runs(v, v.consL, P.trr0 + j + (P.Nr-1)*k, c0, np, i, I0, sum_rout);
    double x0 = centroid_r(rp, rm);
    double dph = get_dp(v.piph[c], v.piph[cm], P.Pmax, err);
    double dV = dV_of(rp, rm, dph, zp, zm);
@@ -586,12 +593,16 @@ __device__ void ct_cons_B(const ViewT<R> &v, const DiskParams &P, int a, int c0,
    cons[BPP] = .5*(v.Phi[c]+v.Phi[cm])*dV/(dA * hp);
    if( v.ct == 2 && P.Nz > 1 ){
       double Sz = 0.0, Tz = 0.0;
-      auto sum_z = [&](int f){
-         Sz += v.fLR[f] == 0 ? v.Phi[4*N + v.fL[f]] : v.Phi[3*N + v.fR[f]];
+      auto sum_zin = [&](int f){
+         Sz += v.fLR[f] == 0 ? v.Phi[4*N + v.fL[f]] : v.Phi[3*N + c];
          Tz += v.fdA[f];
       };
-      if( k >= 1 )      ct_over_runs(v, v.consZR, P.trz0 + j + P.Nr*(k-1), c0, np, i, I0, sum_z);
-      if( k <= P.Nz-2 ) ct_over_runs(v, v.consZL, P.trz0 + j + P.Nr*k, c0, np, i, I0, sum_z);
+      auto sum_zout = [&](int f){
+         Sz += v.fLR[f] == 0 ? v.Phi[4*N + c] : v.Phi[3*N + v.fR[f]];
+         Tz += v.fdA[f];
+      };
+      if( k >= 1 )      ct_over_runs(v, v.consZR, P.trz0 + j + P.Nr*(k-1), c0, np, i, I0, sum_zin);
+      if( k <= P.Nz-2 ) ct_over_runs(v, v.consZL, P.trz0 + j + P.Nr*k, c0, np, i, I0, sum_zout);
       double zfac = 1.0, hz = 1.0;                      /* bfield_scale_factor(x2, 2) */
       cons[BZZ] = Sz * (dV*zfac/(Tz * hz));
    }

@@ -157,6 +157,9 @@ k_mlp_grad_tc(const MlpPacked *__restrict__ mlp, long n, const float *__restrict
          reinterpret_cast<uint4*>(S.DA1b)[e] = z;
          reinterpret_cast<uint4*>(S.H2b)[e] = z;
       }
+      /* the zeroing above covers other threads' rows: finish it before any
+       * thread writes its ones column into H2b */
+      __syncthreads();
       float one[8] = {1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, zero[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       tc_put8(S.Xb, tid, 1, 2, one);
       tc_put8(S.H1b, tid, 8, 10, one);
