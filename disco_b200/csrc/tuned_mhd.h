@@ -6,17 +6,17 @@
  * columns CB/MB):
  *
  *   fp64   kernel        128/4    128/5    128/6    128/7    128/8   128/10   128/12
- *          k_begin      2.0337   2.0335   1.8452   1.6906   1.6261   1.7644   1.8841   -> 8
- *          k_grad       2.5444   2.5455   2.4076   2.3245   2.2507   2.2590   2.5467   -> 8
- *          k_flux       6.5569   6.0407   6.5466   6.4051   7.0216   9.7142  12.0202   -> 5
- *          k_update     3.2236   3.1807   3.4487   3.7623   4.1120   5.7662   8.3289   -> 5
- *          k_c2p        1.9652   1.6211   1.4591   1.3302   1.2285   1.2634   1.3519   -> 8
+ *          k_begin      1.9414   1.9414   1.7468   1.5975   1.5166   1.5941   1.7050   -> 8
+ *          k_grad       2.7288   2.3407   2.2743   2.2546   2.2262   2.2681   2.6733   -> 8
+ *          k_flux       4.8046   4.2260   4.3233   4.4032   4.7350   6.6027   8.3230   -> 5
+ *          k_update     2.8222   2.6586   2.6642   2.7488   2.9839   3.9034   5.9269   -> 5
+ *          k_c2p        1.9937   1.5872   1.4421   1.3007   1.1989   1.2420   1.3012   -> 8
  *   mixed  kernel        128/4    128/5    128/6    128/7    128/8   128/10   128/12
- *          k_begin      1.5646   1.5637   1.5639   1.5644   1.5659   1.4716   1.4673   -> 12
- *          k_grad       1.6005   1.5995   1.5976   1.5986   1.4992   1.4417   1.3659   -> 12
- *          k_flux       3.6875   3.6885   3.3207   3.0425   2.9040   3.1497   3.7171   -> 8
- *          k_update     2.7862   2.5500   2.3829   2.3982   2.5538   3.4816   4.5682   -> 6
- *          k_c2p        1.9211   1.5964   1.4324   1.3035   1.1794   1.1940   1.2627   -> 8
+ *          k_begin      1.3866   1.3862   1.3865   1.3866   1.3866   1.2227   1.1776   -> 12
+ *          k_grad       1.3995   1.3988   1.4009   1.4008   1.3333   1.3728   1.2678   -> 12
+ *          k_flux       2.4134   2.4135   2.1352   2.0572   1.9460   1.8873   2.2928   -> 10
+ *          k_update     2.1891   2.0595   1.9458   1.8913   1.9089   2.0669   2.3853   -> 7
+ *          k_c2p        1.9393   1.5485   1.3977   1.2502   1.1611   1.1900   1.2116   -> 8
  *
  * Values given with -D on the command line win.
  */
@@ -29,10 +29,10 @@
 #define MB_MHD_GRAD 12
 #endif
 #ifndef MB_MHD_FLUX
-#define MB_MHD_FLUX 8
+#define MB_MHD_FLUX 10
 #endif
 #ifndef MB_MHD_UPDATE
-#define MB_MHD_UPDATE 6
+#define MB_MHD_UPDATE 7
 #endif
 #ifndef MB_MHD_C2P
 #define MB_MHD_C2P 8
