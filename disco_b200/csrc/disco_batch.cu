@@ -191,6 +191,22 @@ static void init_planets(DiskState &S, DiskParams &D, const disco_params &p, con
    }
 }
 
+/* The radius of a track's face centres, evaluated on the host with the
+ * device's operations and order (each an IEEE-rounded double operation, no
+ * contraction: the sum of products as in centroid_r), and 1/(1/r) for the
+ * B-field scale factor of the CT edge values. */
+static double host_centroid_r(double xp, double xm){
+   volatile double a = xp*xp, bb = xp*xm, c = xm*xm;
+   double s = (a + bb) + c;
+   volatile double num = 2.0*s, den = 3.0*(xp+xm);
+   return num / den;
+}
+static void push_track_r(disco_batch *b, double r){
+   b->tr_r.push_back(r);
+   volatile double inv = 1.0/r;
+   b->tr_irf.push_back(1.0/inv);
+}
+
 /* the FP32 view: same allocations, R* pointers reinterpreted */
 static void make_float_view(disco_batch *b){
    ViewT<double> &d = b->vd;
@@ -533,6 +549,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
          b->tr_dxL.push_back(rj[j] - rm);
          b->tr_dxR.push_back(rp - rj[j]);
          b->tr_dim.push_back(1);
+         push_track_r(b, .5*(rj[j]+rj[j]));              /* addFace cm[0], faces_alt.c:10-16 */
          int nf = b->ann_np[A] + b->ann_np[B];
          for( int f0=0 ; f0<nf ; f0+=FB ) b->fblk.push_back(make_int2(t, f0));
          face += nf;
@@ -559,6 +576,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
          b->tr_dxL.push_back(zkp[k] - zm);
          b->tr_dxR.push_back(zp - zkp[k]);
          b->tr_dim.push_back(2);
+         push_track_r(b, host_centroid_r(rj[j], rj[j-1]));
          int nf = b->ann_np[A] + b->ann_np[B];
          for( int f0=0 ; f0<nf ; f0+=FB ) b->fblk.push_back(make_int2(t, f0));
          face += nf;
@@ -698,6 +716,7 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.tr_flux = dupload(b, b->tr_flux); v.tr_j = dupload(b, b->tr_j); v.tr_k = dupload(b, b->tr_k);
    v.tr_dxL = dupload(b, b->tr_dxL); v.tr_dxR = dupload(b, b->tr_dxR);
    v.tr_dim = dupload(b, b->tr_dim);
+   v.tr_r = dupload(b, b->tr_r); v.tr_irf = dupload(b, b->tr_irf);
    v.cblk = dupload(b, b->cblk); v.fblk = dupload(b, b->fblk); v.ublk = dupload(b, b->ublk);
    b->d_fblk_rz = dupload(b, b->fblk_rz);
    b->d_fblk_fl[0] = dupload(b, b->fblk_fl[0]); b->d_fblk_fl[1] = dupload(b, b->fblk_fl[1]);

@@ -121,6 +121,7 @@ struct ViewT {
    const int *tr_a, *tr_b, *tr_off, *tr_flux, *tr_j, *tr_k;
    const unsigned char *tr_dim;      /* 1: r-track (j,k)-(j+1,k); 2: z-track (j,k)-(j,k+1) */
    const double *tr_dxL, *tr_dxR;
+   const double *tr_r, *tr_irf;       /* face centre radius of the track's faces, 1/(1/r) */
    const int2 *cblk, *fblk;
    const int2 *ublk;                  /* k_update: (annulus, first cell) of chunks of CB-1 cells */
    const double *rj, *zk;
@@ -858,9 +859,9 @@ __device__ __forceinline__ void flux_body(const ViewT<R> &v, double dtfac, int b
       R Bavg = R(.5)*(primL[BT]+primR[BT]);
       primL[BT] = Bavg; primR[BT] = Bavg;
    }
-   int j = v.tr_j[t];
-   const double *rj = v.rj + P.rj0 + 1;
-   double r = DIM == 1 ? .5*(rj[j]+rj[j]) : centroid_r(rj[j], rj[j-1]);    /* face cm[0] */
+   /* face cm[0]: .5 (r_j + r_j) on an r track, the annulus centroid on a z
+    * track (the same for every face of the track, tabulated at set-up) */
+   const double r = v.tr_r[t];
    R G[Q];
    if constexpr ( GR ){              /* grmhd2 + HLL at the face centre (addFace, faces_alt.c:10-16) */
       const double *zk = v.zk + P.zk0 + 1;
@@ -878,7 +879,7 @@ __device__ __forceinline__ void flux_body(const ViewT<R> &v, double dtfac, int b
          R eb[5];
          solve_riemann<Q,NC,DIM,R>(P, primL, primR, (R)r, (R)v.tr_om[t], R(0.0), (R)dAdt, G, eb);
          const R rr = (R)r;
-         const R irfac = (R)(1.0/(1.0/r));
+         const R irfac = (R)v.tr_irf[t];                /* 1/(1/r) */
          if( DIM == 1 ){
             v.fEt[f] = -eb[1]*rr;
             v.fBt[f] = eb[2]*irfac;
