@@ -717,6 +717,13 @@ extern "C" int disco_batch_create(int device, const disco_modules *mods, int pre
    v.tr_dxL = dupload(b, b->tr_dxL); v.tr_dxR = dupload(b, b->tr_dxR);
    v.tr_dim = dupload(b, b->tr_dim);
    v.tr_r = dupload(b, b->tr_r); v.tr_irf = dupload(b, b->tr_irf);
+   for( int a=0 ; a<ann ; ++a ){
+      const DiskParams &D = b->dparams[b->ann_disk[a]];
+      const double *rjd = b->rj.data() + D.rj0 + 1;
+      const int j = b->ann_j[a];
+      b->ann_rc.push_back(host_centroid_r(rjd[j], rjd[j-1]));
+   }
+   v.ann_rc = dupload(b, b->ann_rc);
    v.cblk = dupload(b, b->cblk); v.fblk = dupload(b, b->fblk); v.ublk = dupload(b, b->ublk);
    b->d_fblk_rz = dupload(b, b->fblk_rz);
    b->d_fblk_fl[0] = dupload(b, b->fblk_fl[0]); b->d_fblk_fl[1] = dupload(b, b->fblk_fl[1]);

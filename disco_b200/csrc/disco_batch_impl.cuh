@@ -43,6 +43,7 @@ struct disco_batch {
    std::vector<unsigned char> tr_dim;
    std::vector<double> tr_dxL, tr_dxR;
    std::vector<double> tr_r, tr_irf;    /* face centre radius per track, 1/(1/r) */
+   std::vector<double> ann_rc;          /* centroid radius per annulus */
    std::vector<int2> cblk, fblk;
    /* the same face blocks in k_faces' order (per layer, the r and z tracks of
     * each annulus together) and the blocks k_flux_t solves per direction */

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(FB) k_ct_faces(ViewT<R> v){
       Ef = fE - (R)(h*w)*fB;
       dl = zk[k]-zk[k-1];                         /* r-face dl = dz, faces_alt.c:26-27 */
    }else{
-      double h = centroid_r(rj[j], rj[j-1]);
+      double h = v.tr_r[t];                        /* centroid_r(r_j, r_j-1) */
       Ef = fE + (R)(h*w)*fB;
       dl = rj[j]-rj[j-1];                         /* z-face dl = dr */
    }
@@ -583,7 +583,7 @@ __device__ void ct_cons_B(const ViewT<R> &v, const DiskParams &P, int a, int c0,
    };
    if( j >= 1 )      ct_over_runs(v, v.consR, P.trr0 + (j-1) + (P.Nr-1)*k, c0, np, i, I0, sum_rin);
    if( j <= P.Nr-2 ) ct_over_runs(v, v.consL, P.trr0 + j + (P.Nr-1)*k, c0, np, i, I0, sum_rout);
-   double x0 = centroid_r(rp, rm);
+   double x0 = v.ann_rc[a];                          /* centroid_r(rp, rm) */
    double dph = get_dp(v.piph[c], v.piph[cm], P.Pmax, err);
    double dV = dV_of(rp, rm, dph, zp, zm);
    double dA = (rp-rm)*(zp-zm);

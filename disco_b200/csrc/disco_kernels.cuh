@@ -122,6 +122,7 @@ struct ViewT {
    const unsigned char *tr_dim;      /* 1: r-track (j,k)-(j+1,k); 2: z-track (j,k)-(j,k+1) */
    const double *tr_dxL, *tr_dxR;
    const double *tr_r, *tr_irf;       /* face centre radius of the track's faces, 1/(1/r) */
+   const double *ann_rc;              /* centroid radius of the annulus (get_centroid(.,.,1)) */
    const int2 *cblk, *fblk;
    const int2 *ublk;                  /* k_update: (annulus, first cell) of chunks of CB-1 cells */
    const double *rj, *zk;
@@ -1025,7 +1026,7 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
    if( real || ctE ){               /* uniform over the block: one annulus */
       double dA = (rj[j]-rj[j-1])*(zk[k]-zk[k-1]);       /* get_dA(.,.,0) */
       double dAdtp = dA*(v.ds[d].dt*dtfac);
-      double rc = centroid_r(rj[j], rj[j-1]);
+      double rc = v.ann_rc[a];                          /* centroid_r(r_j, r_j-1) */
       /* riemann_phi's edge states (riemann.c:45-50): thread t extrapolates
        * cell i-1 to both of its phi edges; the left-edge state goes to its
        * neighbour through shared memory (the last thread also does cell i) */
@@ -1173,7 +1174,7 @@ __device__ __forceinline__ void update_body(const ViewT<R> &v, int first, double
       double dph = get_dp(piph, phim, P.Pmax, &err);
       double dV = dV_of(rp, rm, dph, zp, zm);
       double dVdt = dV*dt;
-      double r = centroid_r(rp, rm);
+      double r = v.ann_rc[a];                            /* centroid_r(rp, rm) */
       if constexpr ( GR ){       /* grmhd2 source, grmhd2.c:383-478 */
          gr_source(P, v.gr_ann[a], prim, cons, 0.5*(rm+rp), dVdt);
       }else if constexpr ( NC == 8 ){  /* mhd source, mhd.c:225-263 */
@@ -1544,7 +1545,7 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
             }
             gr_cons2prim(P, v.gr_ann[a].c, cons, prim, x, dV2);
          }else{
-            cons2prim<Q,NC>(P, cons, prim, centroid_r(rp, rm), v.ann_om[a], dV2);
+            cons2prim<Q,NC>(P, cons, prim, v.ann_rc[a], v.ann_om[a], dV2);   /* centroid_r(rp, rm) */
          }
          /* a horizon module then re-initialises the excised annuli (after
           * calc_prim, as boundary_trans follows it) and getmindt skips them */
@@ -1583,7 +1584,7 @@ __device__ __forceinline__ void c2p_tail(const ViewT<R> &v, const DiskParams &P,
          }else if( real && !excised ){            /* mindt, euler.c:332-380, mhd.c:452-486 */
             int cprev = c0 + (i == 0 ? np-1 : i-1);
             double w = .5*(v.wiph[cprev] + v.wiph[c]);
-            double r = centroid_r(rp, rm);
+            double r = v.ann_rc[a];                      /* centroid_r(rp, rm) */
             double vp = (prim[UPP]-w)*r;
             double cs = sqrt(P.gam*prim[PPP]/prim[RHO]);
             if constexpr ( NC == 8 ){
